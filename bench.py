@@ -1,0 +1,372 @@
+#!/usr/bin/env python3
+"""Benchmark: supernodal Cholesky factor + solve on one or more B200s.
+
+Workload (one step): NumericFactorization + Solve with 16 right-hand sides of
+the 7-point Laplacian of a 64^3 grid (n = 262,144) with per-edge
+conductivities exp(N(0,1)) and a 1e-6 diagonal shift, nested-dissection
+ordering, plain FP64.  Inputs are seeded synthetic data (no dataset exists for
+this path).  Symbolic analysis is done once before timing, as in the
+reference's driver (Example_SparseCholesky/main.cpp:135 vs :147).
+
+The metric is factor+solve throughput in GFLOP/s, counting the reference's
+algorithmic flops once: factor Sum_s [n0^3/3 + n0^2 n1 + n0 n1^2] over the
+reference's supernodes plus solve 4 k nnz(U); ms_per_step is the factor+solve
+time.  Every run checks the relative residual ||B - A X|| / ||B|| on the
+device.
+
+Multi-GPU (torchrun): the workload is replicated -- each rank factors and
+solves its own system (weak scaling, no collective on the data path).
+
+`--impl reference` times the reference's own CPU implementation (compiled
+from its headers into oracle/_ref) on the host cores for the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = 64
+SEED = 0x5EED0002
+SHIFT = 1e-6
+NRHS = 16
+L2_FLUSH_BYTES = 256 << 20
+# The reference's CPU code needs about a minute per full 64^3 factor+solve on
+# 8 cores, so its timed runs use a bounded sample of the same workload: the
+# same generator and ordering on a 48^3 grid (same stencil, weights, shift,
+# RHS count); GFLOP/s is computed with the sample's own flop count.
+CPU_SAMPLE_GRID = 48
+
+
+def build_problem(grid: int = GRID):
+    from tensors_b200 import matrices, ordering
+
+    A = matrices.grid_laplacian_3d(grid, SEED, SHIFT)
+    perm = ordering.nested_dissection(A)
+    B = np.random.default_rng(SEED + 1).standard_normal((A.n, NRHS))
+    return A, perm, B
+
+
+def config_dict(extra=None):
+    c = {
+        "workload": f"3D 7-point Laplacian {GRID}^3 (n={GRID**3}), lognormal(0,1) edge conductivities, "
+                    f"shift {SHIFT:g}, nested dissection, {NRHS} RHS N(0,1), FP64 factor+solve",
+        "grid": GRID, "n": GRID ** 3, "nrhs": NRHS, "seed": SEED,
+        "supernode_strategy": "Maximal",
+        "l2": "256 MiB buffer written between timed steps (inputs and factor also exceed L2)",
+    }
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks / throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measure_dgemm_tflops(torch, dev):
+    """cuBLAS FP64 GEMM throughput (the FP64 tensor-core reference denominator)."""
+    n = 8192
+    a = torch.randn(n, n, device=dev, dtype=torch.float64)
+    b = torch.randn(n, n, device=dev, dtype=torch.float64)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def cpu_reference_run(A, perm, B, threads, steps=1, warmup=0, sample=None):
+    """Times the reference's own CPU factor+solve (oracle/_ref) on this host."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not oracle.ref_available():
+        return None
+    ref = oracle.RefCholesky(A.n, A.outer, A.inner, perm, "maximal", threads=threads, blas_threads=1)
+    ref.symbolic()
+    times = []
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        st = ref.factor(A.values, 0.0)
+        X = ref.solve(B, parallel=False)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    res = np.linalg.norm(B - A.to_scipy() @ X) / np.linalg.norm(B)
+    return {"seconds": times, "status": st, "relres": float(res)}
+
+
+def reference_flops(A, perm):
+    """Reference-supernode factor flops and nnz(U) (host-only symbolic)."""
+    from tensors_b200.cholesky import CholeskyDecomposition
+
+    c = CholeskyDecomposition(A.outer, A.inner, perm)
+    c.SymbolicFactorization()
+    f, nnz_u = c.FlopCount()
+    return f, nnz_u
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    A, perm, B = build_problem(CPU_SAMPLE_GRID)
+    f, nnz_u = reference_flops(A, perm)
+    flops = f + 4.0 * NRHS * nnz_u
+    threads = os.cpu_count() or 1
+    r = cpu_reference_run(A, perm, B, threads, steps=args.steps, warmup=args.warmup)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtb_ref.so not built (needs the reference checkout)"}))
+        return 0
+    t = statistics.mean(r["seconds"])
+    v = flops / t / 1e9
+    line = {
+        "impl": "reference",
+        "metric": "factor+solve GFLOP/s (FP64, 64^3 7-pt Laplacian, 16 RHS)",
+        "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded)",
+        "config": config_dict({"relres": r["relres"], "cpu_threads": threads}),
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "reference",
+                         "sample": f"same generator on a {CPU_SAMPLE_GRID}^3 grid (n={CPU_SAMPLE_GRID**3}), "
+                                   "one factor+solve per step"},
+        "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    from tensors_b200 import build as tb_build
+    from tensors_b200._lib import lib
+    from tensors_b200.cholesky import CholeskyDecomposition
+
+    tb_build.build()
+    lib().tb_set_device(local)
+
+    A, perm, B_host = build_problem()
+    t0 = time.perf_counter()
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    chol.SymbolicFactorization()
+    t_symbolic = time.perf_counter() - t0
+    F, nnz_u = chol.FlopCount()
+    flops = F + 4.0 * NRHS * nnz_u
+
+    vals = torch.tensor(A.values, device=dev)
+    B = torch.tensor(B_host, device=dev)
+    X = torch.empty_like(B)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    # one dedicated stream for the library's kernels, the L2 flush and the events
+    stream = torch.cuda.Stream(dev)
+    chol.SetStream(stream)
+    torch.cuda.set_stream(stream)
+
+    def step():
+        st = chol.NumericFactorization(vals, 0.0)
+        chol.Solve(B, X)
+        return st
+
+    for _ in range(args.warmup):
+        assert step() == 0
+    torch.cuda.synchronize(dev)
+
+    times = []
+    with ClockSampler(local) as clocks:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            step()
+            e.record(stream)
+            e.synchronize()
+            times.append(s.elapsed_time(e))
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+    t_ms = statistics.mean(times)
+    if world > 1:
+        tt = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+
+    # correctness of the timed result
+    R = chol.Residual(B, X)
+    torch.cuda.synchronize(dev)
+    relres = float(torch.linalg.norm(R) / torch.linalg.norm(B))
+    fl, sl = chol.LaunchCounts()
+
+    # end to end through the host-buffer C-ABI calls (copies inside the timing)
+    Xh = np.zeros_like(B_host)
+    e2e = []
+    for i in range(max(2, min(args.steps, 3)) + 1):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        chol.NumericFactorization(A.values, 0.0)
+        chol.Solve(B_host, Xh)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e.append(dt)
+    e2e_s = statistics.mean(e2e)
+
+    # per-kernel timing of the GEMM tiles (direct launches with events)
+    chol.SetProfiling(True)
+    prof = None
+    for _ in range(2):
+        chol.NumericFactorization(vals, 0.0)
+        prof = chol.KernelProfile()
+    chol.SetProfiling(False)
+    dgemm_peak = measure_dgemm_tflops(torch, dev)
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    g = prof["gemm"]
+    achieved = g["flops"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "gemm_tn_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        As, ps, Bs = build_problem(CPU_SAMPLE_GRID)
+        fs, zs = reference_flops(As, ps)
+        r = cpu_reference_run(As, ps, Bs, threads, steps=1, warmup=0)
+        if r is not None:
+            cpu = {"value": (fs + 4.0 * NRHS * zs) / r["seconds"][0] / 1e9, "unit": "GFLOP/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"reference's own code, one factor+solve of the same generator on a {CPU_SAMPLE_GRID}^3 "
+                             f"grid (OpenBLAS 1 thread per tree task, {threads} tree threads)",
+                   "seconds": r["seconds"][0], "relres": r["relres"]}
+
+    value = flops / (t_ms * 1e-3) / 1e9 * world
+    line = {
+        "metric": "factor+solve GFLOP/s (FP64, 64^3 7-pt Laplacian, 16 RHS)",
+        "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded)",
+        "config": config_dict({
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "relres": relres, "symbolic_s": t_symbolic,
+            "factor_gflop": F / 1e9, "solve_gflop": 4.0 * NRHS * nnz_u / 1e9,
+            "plan": chol.PlanStats(),
+            "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+        }),
+        "e2e": {"value": flops / e2e_s / 1e9 * world, "unit": "GFLOP/s",
+                "h2d_bytes_per_step": int(A.values.nbytes + B_host.nbytes),
+                "d2h_bytes_per_step": int(B_host.nbytes), "ms_per_step": e2e_s * 1e3},
+        "roofline": {"bound": "tensor", "kernel": "gemm_tn_kernel (FP64 DMMA tiles)",
+                     "achieved": achieved, "peak": dgemm_peak, "unit": "TFLOP/s",
+                     "frac": (achieved / dgemm_peak) if achieved else None, "traffic": traffic,
+                     "peak_source": "measured live: cuBLAS FP64 GEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)"},
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+        "gpu_launches": int((fl + sl) * args.steps),
+    }
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,184 @@
+/* tensors_b200 -- C-ABI of the B200 supernodal sparse Cholesky.
+ *
+ * A drop-in for the Sparse::CholeskyDecomposition<Scal,Int,LInt,parQ> path of
+ * HenrikSchumacher/Tensors (src/Sparse/CholeskyDecomposition.hpp).  The
+ * reference is a header-only C++ class with no C interface; every function
+ * here replaces one of its members, cited as file:line of the reference.
+ * Integer types follow the reference's driver (Example_SparseCholesky/
+ * main.cpp:31-32): Int = int32_t for rows/columns, LInt = int64_t for
+ * nonzero positions.  Scal = double.
+ *
+ * Conventions
+ *  - Every function returns an int status: TB_OK (0) on success, a positive
+ *    TB_NOT_SPD from the numeric factorization when a pivot is not positive
+ *    (the reference returns 1, CholeskyDecomposition/Numeric.hpp:99), and a
+ *    negative TB_ERR_* on misuse or a CUDA failure.  tb_last_error() gives a
+ *    message for the last failure on the calling thread.
+ *  - Matrices are CSR with the full symmetric pattern and a structurally
+ *    present diagonal (CholeskyDecomposition.hpp:63-65, :404-423).
+ *  - Right-hand sides and solutions are row-major n x nrhs blocks with leading
+ *    dimensions, as in CholeskyDecomposition/Solve.hpp:22-80.
+ *  - Functions without a _device suffix take HOST pointers and copy through
+ *    pinned staging buffers; _device variants take device pointers on the
+ *    handle's GPU and stream.
+ *  - A handle is not re-entrant (neither is the reference object): use one
+ *    handle per host thread / stream.
+ */
+#ifndef TENSORS_B200_H
+#define TENSORS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum tb_status {
+    TB_OK                      = 0,
+    TB_NOT_SPD                 = 1,
+    TB_ERR_INVALID_ARGUMENT    = -1,
+    TB_ERR_INVALID_PATTERN     = -2,
+    TB_ERR_INVALID_PERMUTATION = -3,
+    TB_ERR_MISSING_DIAGONAL    = -4,
+    TB_ERR_NOT_FACTORIZED      = -5,
+    TB_ERR_CUDA                = -6,
+    TB_ERR_OUT_OF_MEMORY       = -7,
+    TB_ERR_NO_DEVICE           = -8,
+    TB_ERR_TIMEOUT             = -9
+};
+
+/* Supernode strategies (CholeskyDecomposition.hpp:119-124). */
+enum tb_supernode_strategy { TB_SN_MAXIMAL = 0, TB_SN_FUNDAMENTAL = 1, TB_SN_AMALGAMATED = 2 };
+
+/* Factorization methods (CholeskyDecomposition.hpp:126-130).  Both compute
+ * the same factor; on the GPU both run the level-scheduled supernodal kernels. */
+enum tb_factorization_method { TB_MULTIFRONTAL = 0, TB_LEFT_LOOKING = 1 };
+
+/* Arrays of the symbolic structure, for tb_chol_array_size/_copy
+ * (getters of CholeskyDecomposition/InputOutput.hpp:304-367 and the trees). */
+enum tb_array {
+    TB_ARRAY_PERM = 0,            /* GetPermutation().GetPermutation()        */
+    TB_ARRAY_PERM_INV = 1,        /* GetPermutation().GetInversePermutation() */
+    TB_ARRAY_VALUE_PERM = 2,      /* GetValuePermutation()                    */
+    TB_ARRAY_SN_RP = 3,           /* SN_RowPointers()                         */
+    TB_ARRAY_SN_OUTER = 4,        /* SN_Outer()                               */
+    TB_ARRAY_SN_INNER = 5,        /* SN_Inner()                               */
+    TB_ARRAY_ROW_TO_SN = 6,       /* RowToSN()                                */
+    TB_ARRAY_SN_TRI_PTR = 7,      /* SN_TrianglePointers()                    */
+    TB_ARRAY_SN_REC_PTR = 8,      /* SN_RectanglePointers()                   */
+    TB_ARRAY_ATREE_PARENTS = 9,   /* AssemblyTree().Parents()                 */
+    TB_ARRAY_ETREE_PARENTS = 10,  /* EliminationTree().Parents()              */
+    TB_ARRAY_OUTER = 11,          /* GetA().Outer()  (permuted pattern)       */
+    TB_ARRAY_INNER = 12,          /* GetA().Inner()                           */
+    TB_ARRAY_ATREE_CHILD_PTR = 13,/* AssemblyTree().ChildPointers()           */
+    TB_ARRAY_ATREE_CHILD_IDX = 14 /* AssemblyTree().ChildIndices()            */
+};
+
+typedef struct tb_chol tb_chol;
+
+/* Message of the last failing call on this thread (never NULL). */
+const char * tb_last_error( void );
+
+/* Library / device information: CUDA device ordinal used by new handles. */
+int tb_set_device( int device );
+
+/* Constructors, CholeskyDecomposition.hpp:313-371.  The pattern is copied.
+ * perm == NULL: the matrix is already permuted (ctor :350).  Otherwise
+ * perm[i] is the original index placed at position i (ctor :336,
+ * Inverse::False).  thread_count is the host thread count of the symbolic
+ * phase (the reference's thread_count). */
+int tb_chol_create( tb_chol ** out, int32_t n, const int64_t * outer, const int32_t * inner,
+                    const int32_t * perm, int32_t thread_count );
+int tb_chol_destroy( tb_chol * h );
+
+/* Setters, CholeskyDecomposition/InputOutput.hpp:369-409. */
+int tb_chol_set_supernode_strategy( tb_chol * h, int32_t strategy );
+int tb_chol_set_amalgamation_threshold( tb_chol * h, int32_t threshold );
+int tb_chol_set_factorization_method( tb_chol * h, int32_t method );
+
+/* SymbolicFactorization(), CholeskyDecomposition/Symbolic.hpp:3-66.  Lazy and
+ * idempotent; also builds and uploads the device execution plan. */
+int tb_chol_symbolic( tb_chol * h );
+
+/* NumericFactorization(A_val, reg), CholeskyDecomposition/Numeric.hpp:3-24:
+ * values in the caller's original CSR order; reg is added to every diagonal
+ * entry.  Returns TB_OK, TB_NOT_SPD (the handle is still marked factorized,
+ * Numeric.hpp:95) or an error. */
+int tb_chol_numeric( tb_chol * h, const double * values, double reg );
+int tb_chol_numeric_device( tb_chol * h, const double * d_values, double reg );
+
+/* Solve: X = alpha * A^{-1} B + beta * X (Solve.hpp:22-80).  B and X are
+ * row-major n x nrhs with leading dimensions ldB, ldX >= nrhs; they may
+ * alias.  When beta == 0 the old X is not read. */
+int tb_chol_solve( tb_chol * h, double alpha, const double * B, int32_t ldB,
+                   double beta, double * X, int32_t ldX, int32_t nrhs );
+int tb_chol_solve_device( tb_chol * h, double alpha, const double * d_B, int32_t ldB,
+                          double beta, double * d_X, int32_t ldX, int32_t nrhs );
+
+/* Half solves (Solve.hpp:182-310) with the documented meaning:
+ * upper: X = alpha * P^T U^{-1} P B + beta X;  lower: X = alpha * P^T U^{-T} P B + beta X. */
+int tb_chol_upper_solve( tb_chol * h, double alpha, const double * B, int32_t ldB,
+                         double beta, double * X, int32_t ldX, int32_t nrhs );
+int tb_chol_lower_solve( tb_chol * h, double alpha, const double * B, int32_t ldB,
+                         double beta, double * X, int32_t ldX, int32_t nrhs );
+
+/* Residual helper: R = B - A X for the matrix passed to the last numeric
+ * factorization (values in caller order), on device buffers (row-major,
+ * leading dimension nrhs).  Used for iterative refinement and tests. */
+int tb_chol_residual_device( tb_chol * h, const double * d_B, const double * d_X,
+                             double * d_R, int32_t nrhs );
+
+/* Queries. */
+int tb_chol_sn_count( tb_chol * h, int32_t * out );
+int tb_chol_row_count( tb_chol * h, int32_t * out );
+int tb_chol_nonzero_count( tb_chol * h, int64_t * out );
+int tb_chol_array_size( tb_chol * h, int32_t which, int64_t * out );
+int tb_chol_array_copy( tb_chol * h, int32_t which, int64_t * out );
+int tb_chol_factorized( tb_chol * h, int32_t * factorized, int32_t * good );
+/* First supernode whose pivot failed, or -1. */
+int tb_chol_failed_supernode( tb_chol * h, int32_t * out );
+/* RequiredTriangularSize / RequiredRectangularSize (Numeric.hpp:193-215). */
+int tb_chol_factor_sizes( tb_chol * h, int64_t * tri_size, int64_t * rec_size );
+/* Copy the factor back in the reference's layout: SN_TriangleValues and
+ * SN_RectangleValues (InputOutput.hpp:339-352), row-major U0 / U1 blocks. */
+int tb_chol_factor_values( tb_chol * h, double * tri, double * rec );
+/* LogDeterminant (InputOutput.hpp:294-297) and WriteFactorDiagonal (:238-257). */
+int tb_chol_log_det( tb_chol * h, double * out );
+int tb_chol_factor_diagonal( tb_chol * h, double * diag );
+/* Factor flops Sum_s [n0^3/3 + n0^2 n1 + n0 n1^2] and nnz(U). */
+int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
+/* Plan statistics (host-only, after the symbolic phase): out[0] arena
+ * doubles (triangles + rectangles + update matrices), out[1] update-matrix
+ * doubles, out[2] levels, out[3] factorization launches, out[4] GEMM tile
+ * tasks, out[5] panel tasks, out[6] extend-add tasks, out[7] forward-solve
+ * launches, out[8] back-solve launches, out[9] supernodes, out[10] fronts
+ * (runs of supernodes merged for computation).  Returns the
+ * number of entries written (at most cap). */
+int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
+/* Host-side bounds check of every device task of the plan (also run before
+ * the plan is first uploaded).  TB_OK or TB_ERR_INVALID_ARGUMENT with the
+ * first violation in tb_last_error(). */
+int tb_chol_check_plan( tb_chol * h );
+/* Device bytes held by the handle. */
+int tb_chol_device_bytes( tb_chol * h, int64_t * out );
+
+/* Stream of the handle (a cudaStream_t; NULL = a stream the handle owns). */
+int tb_chol_set_stream( tb_chol * h, void * stream );
+/* Capture the numeric factorization into a CUDA graph on first use (default
+ * on); off runs the same kernels as individual launches. */
+int tb_chol_set_graph( tb_chol * h, int32_t enabled );
+/* Per-kernel timing: when enabled, factorizations run as direct launches
+ * bracketed by CUDA events and tb_chol_kernel_profile reports, per launch
+ * kind (0 zero, 1 extend-add, 2 panel, 3 GEMM tiles, 7 clear + assembly),
+ * the milliseconds and launches of the last factorization and the
+ * algorithmic flops of the GEMM tiles (8 entries each). */
+int tb_chol_set_profiling( tb_chol * h, int32_t enabled );
+int tb_chol_kernel_profile( tb_chol * h, double * ms, int64_t * launches, double * flops );
+/* Number of kernel launches the last numeric factorization / solve issued. */
+int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * solve_launches );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TENSORS_B200_H */

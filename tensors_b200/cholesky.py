@@ -1,0 +1,366 @@
+"""Python mirror of ``Sparse::CholeskyDecomposition`` over the C-ABI.
+
+Method names, argument meanings and return conventions follow the reference
+class (src/Sparse/CholeskyDecomposition.hpp and its CholeskyDecomposition/
+subfiles); every call goes through ``include/tensors_b200.h`` into the CUDA
+library.  Differences from the reference are deliberate and listed here:
+
+* errors raise :class:`TBError` instead of printing and continuing (the
+  reference ``eprint``s and returns, e.g. Solve.hpp:353-363);
+* ``NumericFactorization`` returns 0 / 1 like the reference (Numeric.hpp:99)
+  and additionally records the first failing supernode;
+* ``LowerSolve`` solves with L = U^T as documented; the reference's public
+  LowerSolve runs the upper solve (Solve.hpp:290-307).
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import numpy as np
+
+from ._lib import lib
+
+__all__ = ["CholeskyDecomposition", "TBError", "SupernodeStrategy", "FactorizationMethod"]
+
+
+class TBError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class SupernodeStrategy(enum.IntEnum):
+    """CholeskyDecomposition.hpp:119-124."""
+
+    Maximal = 0
+    Fundamental = 1
+    Amalgamated = 2
+
+
+class FactorizationMethod(enum.IntEnum):
+    """CholeskyDecomposition.hpp:126-130."""
+
+    Multifrontal = 0
+    LeftLooking = 1
+
+
+_ARRAYS = {
+    "perm": 0, "perm_inv": 1, "value_perm": 2, "SN_rp": 3, "SN_outer": 4, "SN_inner": 5,
+    "row_to_SN": 6, "SN_tri_ptr": 7, "SN_rec_ptr": 8, "aTree_parents": 9, "eTree_parents": 10,
+    "outer": 11, "inner": 12, "aTree_child_ptr": 13, "aTree_child_idx": 14,
+}
+
+
+def _check(status: int) -> int:
+    if status < 0:
+        raise TBError(status, lib().tb_last_error().decode())
+    return status
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class CholeskyDecomposition:
+    """Supernodal Cholesky A = U^T U of a sparse SPD matrix on the GPU.
+
+    ``CholeskyDecomposition(outer, inner, perm)`` mirrors the constructor with
+    a fill-reducing permutation (CholeskyDecomposition.hpp:336: perm[i] is the
+    original index placed at position i); ``perm=None`` means the matrix is
+    already permuted (:350).  The pattern must be the full symmetric pattern
+    with the diagonal present.
+    """
+
+    SupernodeStrategy_T = SupernodeStrategy
+    FactorizationMethod_T = FactorizationMethod
+
+    def __init__(self, outer, inner, perm=None, n: int | None = None, thread_count: int = 1):
+        self._outer = np.ascontiguousarray(outer, dtype=np.int64)
+        self._inner = np.ascontiguousarray(inner, dtype=np.int32)
+        self._n = int(n) if n is not None else len(self._outer) - 1
+        self._perm = None if perm is None else np.ascontiguousarray(perm, dtype=np.int32)
+        if self._perm is not None and self._perm.shape != (self._n,):
+            raise TBError(-1, "permutation has the wrong length")
+        h = ctypes.c_void_p()
+        _check(lib().tb_chol_create(ctypes.byref(h), self._n, self._outer.ctypes.data, self._inner.ctypes.data,
+                                    None if self._perm is None else self._perm.ctypes.data, int(thread_count)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().tb_chol_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---------------------------------------------------------------- setup
+    def SetSupernodeStrategy(self, strategy) -> None:
+        _check(lib().tb_chol_set_supernode_strategy(self._h, int(strategy)))
+
+    def SetAmalgamationThreshold(self, threshold: int) -> None:
+        _check(lib().tb_chol_set_amalgamation_threshold(self._h, int(threshold)))
+
+    def SetFactorizationMethod(self, method) -> None:
+        _check(lib().tb_chol_set_factorization_method(self._h, int(method)))
+
+    def SetUseGraph(self, enabled: bool) -> None:
+        _check(lib().tb_chol_set_graph(self._h, 1 if enabled else 0))
+
+    def SetStream(self, stream) -> None:
+        """Run on a torch.cuda.Stream (or raw handle); None = an owned stream."""
+        ptr = None if stream is None else int(getattr(stream, "cuda_stream", stream))
+        _check(lib().tb_chol_set_stream(self._h, ptr))
+
+    # -------------------------------------------------------------- phases
+    def SymbolicFactorization(self) -> None:
+        _check(lib().tb_chol_symbolic(self._h))
+
+    def NumericFactorization(self, values, reg: float = 0.0) -> int:
+        """Values in the caller's CSR order (host array or CUDA torch tensor)."""
+        if _is_cuda_tensor(values):
+            return _check(lib().tb_chol_numeric_device(self._h, values.data_ptr(), float(reg)))
+        v = _f64(values)
+        if v.shape != (self.NonzeroCount(),):
+            raise TBError(-1, "NumericFactorization: wrong number of values")
+        return _check(lib().tb_chol_numeric(self._h, v.ctypes.data, float(reg)))
+
+    def _solve(self, which: str, B, X=None, alpha=1.0, beta=0.0):
+        if _is_cuda_tensor(B):
+            return self._solve_device(which, B, X, alpha, beta)
+        B = _f64(B)
+        one_d = B.ndim == 1
+        k = 1 if one_d else B.shape[1]
+        if B.shape[0] != self._n:
+            raise TBError(-1, "Solve: B has the wrong number of rows")
+        if X is None:
+            X = np.zeros_like(B)
+            beta = 0.0
+        elif not (X.flags.c_contiguous and X.dtype == np.float64 and X.shape == B.shape):
+            raise TBError(-1, "Solve: X must be a C-contiguous float64 array shaped like B")
+        fn = {"full": lib().tb_chol_solve, "upper": lib().tb_chol_upper_solve, "lower": lib().tb_chol_lower_solve}[which]
+        _check(fn(self._h, float(alpha), B.ctypes.data, k, float(beta), X.ctypes.data, k, k))
+        return X
+
+    def _solve_device(self, which, B, X, alpha, beta):
+        import torch
+
+        if which != "full":
+            raise TBError(-1, "device half solves are not exposed")
+        B = B.contiguous()
+        k = 1 if B.dim() == 1 else B.shape[1]
+        if X is None:
+            X = torch.empty_like(B)
+            beta = 0.0
+        _check(lib().tb_chol_solve_device(self._h, float(alpha), B.data_ptr(), k, float(beta), X.data_ptr(), k, k))
+        return X
+
+    def Solve(self, B, X=None, alpha: float = 1.0, beta: float = 0.0):
+        """X = alpha * A^{-1} B + beta * X  (Solve.hpp:22-80); B is n or n x nrhs."""
+        return self._solve("full", B, X, alpha, beta)
+
+    def UpperSolve(self, B, X=None, alpha: float = 1.0, beta: float = 0.0):
+        """X = alpha * P^T U^{-1} P B + beta * X (Solve.hpp:182-243)."""
+        return self._solve("upper", B, X, alpha, beta)
+
+    def LowerSolve(self, B, X=None, alpha: float = 1.0, beta: float = 0.0):
+        """X = alpha * P^T U^{-T} P B + beta * X (documented meaning of Solve.hpp:248)."""
+        return self._solve("lower", B, X, alpha, beta)
+
+    def Residual(self, B, X):
+        """R = B - A X on CUDA tensors (row-major n x k), with the last factored values."""
+        import torch
+
+        k = 1 if B.dim() == 1 else B.shape[1]
+        R = torch.empty_like(B)
+        _check(lib().tb_chol_residual_device(self._h, B.data_ptr(), X.data_ptr(), R.data_ptr(), k))
+        return R
+
+    # ------------------------------------------------------------- getters
+    def _array(self, name: str) -> np.ndarray:
+        size = ctypes.c_int64()
+        _check(lib().tb_chol_array_size(self._h, _ARRAYS[name], ctypes.byref(size)))
+        out = np.zeros(size.value, dtype=np.int64)
+        if size.value:
+            _check(lib().tb_chol_array_copy(self._h, _ARRAYS[name], out.ctypes.data))
+        return out
+
+    def SymbolicArray(self, name: str) -> np.ndarray:
+        return self._array(name)
+
+    def RowCount(self) -> int:
+        return self._n
+
+    def ColCount(self) -> int:
+        return self._n
+
+    def NonzeroCount(self) -> int:
+        return int(self._outer[-1])
+
+    def SN_Count(self) -> int:
+        v = ctypes.c_int32()
+        _check(lib().tb_chol_sn_count(self._h, ctypes.byref(v)))
+        return v.value
+
+    def SN_RowPointers(self):
+        return self._array("SN_rp")
+
+    def SN_Outer(self):
+        return self._array("SN_outer")
+
+    def SN_Inner(self):
+        return self._array("SN_inner")
+
+    def RowToSN(self):
+        return self._array("row_to_SN")
+
+    def SN_TrianglePointers(self):
+        return self._array("SN_tri_ptr")
+
+    def SN_RectanglePointers(self):
+        return self._array("SN_rec_ptr")
+
+    def GetPermutation(self):
+        return self._array("perm")
+
+    def GetInversePermutation(self):
+        return self._array("perm_inv")
+
+    def GetValuePermutation(self):
+        return self._array("value_perm")
+
+    def AssemblyTreeParents(self):
+        return self._array("aTree_parents")
+
+    def EliminationTreeParents(self):
+        return self._array("eTree_parents")
+
+    def RequiredTriangularSize(self) -> int:
+        t, r = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().tb_chol_factor_sizes(self._h, ctypes.byref(t), ctypes.byref(r)))
+        return t.value
+
+    def RequiredRectangularSize(self) -> int:
+        t, r = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().tb_chol_factor_sizes(self._h, ctypes.byref(t), ctypes.byref(r)))
+        return r.value
+
+    def FactorValues(self):
+        """(SN_TriangleValues, SN_RectangleValues) in the reference layout."""
+        tri = np.zeros(self.RequiredTriangularSize())
+        rec = np.zeros(self.RequiredRectangularSize())
+        _check(lib().tb_chol_factor_values(self._h, tri.ctypes.data, rec.ctypes.data))
+        return tri, rec
+
+    def SN_TriangleValues(self):
+        return self.FactorValues()[0]
+
+    def SN_RectangleValues(self):
+        return self.FactorValues()[1]
+
+    def NumericallyFactorizedQ(self) -> bool:
+        f, g = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().tb_chol_factorized(self._h, ctypes.byref(f), ctypes.byref(g)))
+        return bool(f.value)
+
+    def NumericallyGoodQ(self) -> bool:
+        f, g = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().tb_chol_factorized(self._h, ctypes.byref(f), ctypes.byref(g)))
+        return bool(g.value)
+
+    def FailedSupernode(self) -> int:
+        v = ctypes.c_int32()
+        _check(lib().tb_chol_failed_supernode(self._h, ctypes.byref(v)))
+        return v.value
+
+    def LogDeterminant(self) -> float:
+        v = ctypes.c_double()
+        _check(lib().tb_chol_log_det(self._h, ctypes.byref(v)))
+        return v.value
+
+    def FactorLogDeterminant(self) -> float:
+        return 0.5 * self.LogDeterminant()
+
+    def WriteFactorDiagonal(self):
+        d = np.zeros(self._n)
+        _check(lib().tb_chol_factor_diagonal(self._h, d.ctypes.data))
+        return d
+
+    def FlopCount(self):
+        f, z = ctypes.c_double(), ctypes.c_double()
+        _check(lib().tb_chol_flop_count(self._h, ctypes.byref(f), ctypes.byref(z)))
+        return f.value, z.value
+
+    def PlanStats(self) -> dict:
+        out = np.zeros(16, dtype=np.int64)
+        m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 16))
+        keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
+                "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts"]
+        return {k: int(out[i]) for i, k in enumerate(keys[:m])}
+
+    def CheckPlan(self) -> None:
+        """Host-side bounds check of every device task (raises TBError)."""
+        _check(lib().tb_chol_check_plan(self._h))
+
+    def DeviceBytes(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().tb_chol_device_bytes(self._h, ctypes.byref(v)))
+        return v.value
+
+    def SetProfiling(self, enabled: bool) -> None:
+        _check(lib().tb_chol_set_profiling(self._h, 1 if enabled else 0))
+
+    def KernelProfile(self) -> dict:
+        """Per launch kind of the last profiled factorization: ms, launches, flops."""
+        ms = np.zeros(8)
+        ln = np.zeros(8, dtype=np.int64)
+        fl = np.zeros(8)
+        _check(lib().tb_chol_kernel_profile(self._h, ms.ctypes.data, ln.ctypes.data, fl.ctypes.data))
+        names = {0: "zero", 1: "extend", 2: "panel", 3: "gemm", 7: "assemble"}
+        return {names[k]: {"ms": float(ms[k]), "launches": int(ln[k]), "flops": float(fl[k])} for k in names}
+
+    def LaunchCounts(self):
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().tb_chol_launch_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def GetU(self):
+        """U as a scipy CSR matrix in the permuted ordering (InputOutput.hpp:116-217)."""
+        import scipy.sparse as sp
+
+        rp = self.SN_RowPointers()
+        so = self.SN_Outer()
+        si = self.SN_Inner()
+        tp = self.SN_TrianglePointers()
+        rcp = self.SN_RectanglePointers()
+        tri, rec = self.FactorValues()
+        rows, cols, vals = [], [], []
+        for s in range(len(rp) - 1):
+            i0, i1 = rp[s], rp[s + 1]
+            n0, n1 = i1 - i0, so[s + 1] - so[s]
+            U0 = tri[tp[s]: tp[s] + n0 * n0].reshape(n0, n0)
+            U1 = rec[rcp[s]: rcp[s] + n0 * n1].reshape(n0, n1)
+            r, c = np.triu_indices(n0)
+            rows.append(i0 + r); cols.append(i0 + c); vals.append(U0[r, c])
+            if n1:
+                rr = np.repeat(np.arange(n0), n1)
+                rows.append(i0 + rr); cols.append(np.tile(si[so[s]: so[s + 1]], n0)); vals.append(U1.ravel())
+        return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(self._n, self._n))
+
+
+def _is_cuda_tensor(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)

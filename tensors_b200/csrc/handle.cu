@@ -1,0 +1,830 @@
+// C-ABI of the library (include/tensors_b200.h): handle lifetime, device
+// memory, launch sequencing and CUDA-graph capture of the factorization.
+
+#include "common.hpp"
+#include "kernels.cuh"
+#include "plan.hpp"
+#include "plan_check.hpp"
+#include "symbolic.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace
+{
+
+thread_local std::string g_error = "no error";
+int g_device = 0;
+
+int fail( int code, const std::string & msg )
+{
+    g_error = msg;
+    return code;
+}
+
+#define TB_CUDA( call )                                                                              \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if( e_ != cudaSuccess )                                                                      \
+        {                                                                                            \
+            return fail( e_ == cudaErrorMemoryAllocation ? TB_ERR_OUT_OF_MEMORY : TB_ERR_CUDA,        \
+                         std::string( #call ) + ": " + cudaGetErrorString( e_ ) );                   \
+        }                                                                                            \
+    } while( 0 )
+
+#define TB_TRY( call )                         \
+    do {                                       \
+        const int s_ = (call);                 \
+        if( s_ != TB_OK ) { return s_; }       \
+    } while( 0 )
+
+template<typename T>
+struct DeviceArray
+{
+    T * ptr = nullptr;
+    std::int64_t size = 0;
+    ~DeviceArray() { release(); }
+    void release() { if( ptr ) { cudaFree( ptr ); ptr = nullptr; } size = 0; }
+    int reserve( std::int64_t n )
+    {
+        if( n <= size && ptr ) { return TB_OK; }
+        release();
+        TB_CUDA( cudaMalloc( &ptr, sizeof(T) * static_cast<size_t>( std::max<std::int64_t>( n, 1 ) ) ) );
+        size = n;
+        return TB_OK;
+    }
+    int upload( const std::vector<T> & v, cudaStream_t st )
+    {
+        TB_TRY( reserve( static_cast<std::int64_t>( v.size() ) ) );
+        if( !v.empty() ) { TB_CUDA( cudaMemcpyAsync( ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st ) ); }
+        return TB_OK;
+    }
+};
+
+struct PinnedBuffer
+{
+    void * ptr = nullptr;
+    size_t bytes = 0;
+    ~PinnedBuffer() { if( ptr ) { cudaFreeHost( ptr ); } }
+    int reserve( size_t n )
+    {
+        if( n <= bytes && ptr ) { return TB_OK; }
+        if( ptr ) { cudaFreeHost( ptr ); ptr = nullptr; }
+        TB_CUDA( cudaMallocHost( &ptr, std::max<size_t>( n, 64 ) ) );
+        bytes = n;
+        return TB_OK;
+    }
+    template<typename T> T * as() { return static_cast<T*>( ptr ); }
+};
+
+} // namespace
+
+struct tb_chol
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // input pattern (copied, CholeskyDecomposition.hpp:313-371)
+    std::int32_t n = 0;
+    std::vector<std::int64_t> outer;
+    std::vector<std::int32_t> inner;
+    std::vector<std::int32_t> perm;
+    bool has_perm = false;
+    std::int32_t threads = 1;
+
+    tb::SupernodeStrategy strategy = tb::SupernodeStrategy::Maximal;
+    std::int32_t amalgamation_threshold = 4;
+    std::int32_t method = TB_MULTIFRONTAL;
+
+    bool symbolic_done = false;
+    bool device_ready = false;
+    bool kernels_configured = false;
+    tb::Symbolic sym;
+    tb::Plan plan;
+
+    // device state
+    DeviceArray<double>             arena;
+    DeviceArray<std::int64_t>       asm_src, asm_dst, diag_off;
+    DeviceArray<std::int32_t>       lut, sn_inner, p, p_inv, colmap;
+    DeviceArray<tb::ZeroTask>       zero;
+    DeviceArray<tb::ExportTask>     exports;
+    DeviceArray<double>             exported;    // reference-layout factor (tri then rec)
+    DeviceArray<tb::GemmTask>       gemm;
+    DeviceArray<tb::PanelTask>      panel;
+    DeviceArray<tb::ExtendTask>     extend;
+    DeviceArray<tb::SolveDiagTask>  sdiag;
+    DeviceArray<tb::SolveRestTask>  srest;
+    DeviceArray<std::int64_t>       a_outer;     // caller-order pattern, for residuals
+    DeviceArray<std::int32_t>       a_inner;
+    DeviceArray<double>             values;      // caller-order values of the last factorization
+    DeviceArray<double>             reg;
+    DeviceArray<int>                status;
+    DeviceArray<double>             work, in, out, diag_vals;
+    PinnedBuffer                    pin_in, pin_out, pin_small;
+
+    cudaGraphExec_t factor_graph = nullptr;
+    bool use_graph = true;
+
+    // optional per-kernel timing of direct (non-graph) factorizations
+    bool profiling = false;
+    double kind_ms[8] = {};
+    std::int64_t kind_launches[8] = {};
+    std::vector<cudaEvent_t> events;
+
+    bool factorized = false;
+    bool good = false;
+    std::int32_t failed_sn = -1;
+    std::int64_t factor_launch_count = 0;
+    std::int64_t solve_launch_count = 0;
+
+    ~tb_chol()
+    {
+        for( cudaEvent_t e : events ) { cudaEventDestroy( e ); }
+        if( factor_graph ) { cudaGraphExecDestroy( factor_graph ); }
+        if( own_stream && stream ) { cudaStreamDestroy( stream ); }
+    }
+
+    void invalidate_symbolic()
+    {
+        symbolic_done = false;
+        device_ready = false;
+        factorized = false;
+        good = false;
+        if( factor_graph ) { cudaGraphExecDestroy( factor_graph ); factor_graph = nullptr; }
+    }
+};
+
+namespace
+{
+
+int check_handle( tb_chol * h )
+{
+    if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    return TB_OK;
+}
+
+int ensure_symbolic( tb_chol * h )
+{
+    if( h->symbolic_done ) { return TB_OK; }
+    tb::SymbolicInput in;
+    in.n = h->n;
+    in.outer = h->outer.data();
+    in.inner = h->inner.data();
+    in.perm = h->has_perm ? h->perm.data() : nullptr;
+    in.strategy = h->strategy;
+    in.amalgamation_threshold = h->amalgamation_threshold;
+    const int st = h->sym.analyze( in );
+    if( st != TB_OK )
+    {
+        const char * what = st == TB_ERR_INVALID_PERMUTATION ? "input is not a permutation"
+                          : st == TB_ERR_MISSING_DIAGONAL    ? "diagonal of input matrix is not marked as nonzero"
+                          : "invalid CSR pattern";
+        return fail( st, std::string( "SymbolicFactorization: " ) + what );
+    }
+    h->plan.build( h->sym );
+    h->symbolic_done = true;
+    h->device_ready = false;
+    h->factorized = false;
+    h->good = false;
+    return TB_OK;
+}
+
+// Binds the handle's device and stream and uploads the plan (once per
+// symbolic analysis).  Everything before this point is host-only, so the
+// symbolic phase and its getters work without a GPU.
+int ensure_device( tb_chol * h )
+{
+    TB_TRY( ensure_symbolic( h ) );
+    TB_CUDA( cudaSetDevice( h->device ) );
+    if( h->stream == nullptr )
+    {
+        TB_CUDA( cudaStreamCreateWithFlags( &h->stream, cudaStreamNonBlocking ) );
+        h->own_stream = true;
+    }
+    if( !h->kernels_configured )
+    {
+        TB_CUDA( tb::configure_kernels() );
+        h->kernels_configured = true;
+    }
+    if( h->device_ready ) { return TB_OK; }
+    {
+        const std::string msg = tb::check_plan( h->sym, h->plan );
+        if( !msg.empty() ) { return fail( TB_ERR_INVALID_ARGUMENT, "plan check: " + msg ); }
+    }
+
+    const tb::Symbolic & s = h->sym;
+    const tb::Plan & pl = h->plan;
+    cudaStream_t st_ = h->stream;
+    TB_TRY( h->arena.reserve( pl.arena_size() ) );
+    TB_TRY( h->asm_src.upload( pl.asm_src, st_ ) );
+    TB_TRY( h->asm_dst.upload( pl.asm_dst, st_ ) );
+    TB_TRY( h->lut.upload( pl.lut, st_ ) );
+    TB_TRY( h->sn_inner.upload( s.sn_inner, st_ ) );
+    TB_TRY( h->p.upload( s.p, st_ ) );
+    TB_TRY( h->p_inv.upload( s.p_inv, st_ ) );
+    TB_TRY( h->gemm.upload( pl.gemm, st_ ) );
+    TB_TRY( h->panel.upload( pl.panel, st_ ) );
+    TB_TRY( h->extend.upload( pl.extend, st_ ) );
+    TB_TRY( h->sdiag.upload( pl.sdiag, st_ ) );
+    TB_TRY( h->srest.upload( pl.srest, st_ ) );
+    TB_TRY( h->zero.upload( pl.zero, st_ ) );
+    TB_TRY( h->exports.upload( pl.exports, st_ ) );
+    TB_TRY( h->colmap.upload( pl.colmap, st_ ) );
+    TB_TRY( h->a_outer.upload( h->outer, st_ ) );
+    TB_TRY( h->a_inner.upload( h->inner, st_ ) );
+    TB_TRY( h->values.reserve( s.nnz ) );
+    TB_TRY( h->reg.reserve( 1 ) );
+    TB_TRY( h->status.reserve( 2 ) );
+    TB_TRY( h->diag_off.upload( pl.diag_offset, st_ ) );
+    TB_TRY( h->diag_vals.reserve( s.n ) );
+    TB_CUDA( cudaStreamSynchronize( st_ ) );
+    if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    h->device_ready = true;
+    return TB_OK;
+}
+
+// Issues the numeric factorization on h->stream (capturable).  With
+// `timed`, every launch is bracketed by events (kind index in `kinds`).
+std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * kinds = nullptr )
+{
+    const tb::Plan & pl = h->plan;
+    cudaStream_t st = h->stream;
+    double * A = h->arena.ptr;
+    std::int64_t launches = 0;
+    std::size_t ev = 0;
+    auto mark = [&]( int kind )
+    {
+        if( !timed ) { return; }
+        cudaEventRecord( h->events[ev++], st );
+        if( kind >= 0 ) { kinds->push_back( kind ); }
+    };
+    mark( -1 );
+    // ClearFactors (Numeric.hpp:256-268); update matrices are zeroed per level
+    cudaMemsetAsync( A, 0, sizeof(double) * static_cast<size_t>( pl.u0_size + pl.u1_size ), st );
+    tb::launch_init_status( h->status.ptr, st );
+    tb::launch_assemble( h->values.ptr, h->asm_src.ptr, h->asm_dst.ptr,
+                         static_cast<std::int64_t>( pl.asm_src.size() ), h->reg.ptr, A, st );
+    mark( 7 );
+    launches += 2;
+    for( const tb::Launch & L : pl.factor_launches )
+    {
+        switch( L.kind )
+        {
+            case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
+            case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
+            case tb::LaunchKind::Panel:  tb::launch_panel( h->panel.ptr + L.first, L.count, A, h->status.ptr, st ); break;
+            case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
+            default: break;
+        }
+        mark( static_cast<int>( L.kind ) );
+        ++launches;
+    }
+    return launches;
+}
+
+int run_factor( tb_chol * h, double reg )
+{
+    cudaStream_t st = h->stream;
+    TB_TRY( h->pin_small.reserve( 64 ) );
+    double * pr = h->pin_small.as<double>();
+    pr[0] = reg;
+    TB_CUDA( cudaMemcpyAsync( h->reg.ptr, pr, sizeof(double), cudaMemcpyHostToDevice, st ) );
+    if( h->profiling )
+    {
+        const std::size_t need = h->plan.factor_launches.size() + 2;
+        while( h->events.size() < need )
+        {
+            cudaEvent_t e;
+            TB_CUDA( cudaEventCreate( &e ) );
+            h->events.push_back( e );
+        }
+        std::vector<int> kinds;
+        h->factor_launch_count = issue_factor( h, true, &kinds );
+        TB_CUDA( cudaGetLastError() );
+        TB_CUDA( cudaStreamSynchronize( st ) );
+        for( int k = 0; k < 8; ++k ) { h->kind_ms[k] = 0.0; h->kind_launches[k] = 0; }
+        for( std::size_t i = 0; i < kinds.size(); ++i )
+        {
+            float ms = 0.0f;
+            TB_CUDA( cudaEventElapsedTime( &ms, h->events[i], h->events[i + 1] ) );
+            h->kind_ms[kinds[i]] += ms;
+            h->kind_launches[kinds[i]] += 1;
+        }
+    }
+    else if( h->use_graph )
+    {
+        if( h->factor_graph == nullptr )
+        {
+            cudaGraph_t g = nullptr;
+            TB_CUDA( cudaStreamBeginCapture( st, cudaStreamCaptureModeThreadLocal ) );
+            h->factor_launch_count = issue_factor( h );
+            const cudaError_t ce = cudaStreamEndCapture( st, &g );
+            if( ce != cudaSuccess ) { return fail( TB_ERR_CUDA, std::string( "graph capture: " ) + cudaGetErrorString( ce ) ); }
+            const cudaError_t ie = cudaGraphInstantiate( &h->factor_graph, g, 0 );
+            cudaGraphDestroy( g );
+            if( ie != cudaSuccess ) { h->factor_graph = nullptr; return fail( TB_ERR_CUDA, std::string( "graph instantiate: " ) + cudaGetErrorString( ie ) ); }
+        }
+        TB_CUDA( cudaGraphLaunch( h->factor_graph, st ) );
+    }
+    else
+    {
+        h->factor_launch_count = issue_factor( h );
+        TB_CUDA( cudaGetLastError() );
+    }
+    int * ps = reinterpret_cast<int*>( pr + 1 );
+    TB_CUDA( cudaMemcpyAsync( ps, h->status.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, st ) );
+    TB_CUDA( cudaStreamSynchronize( st ) );
+    h->factorized = true;                       // marked in any case, Numeric.hpp:94-95
+    h->good = (ps[0] == 0);
+    h->failed_sn = h->good ? -1 : h->sym.row_to_sn[std::min( std::max( ps[1], 0 ), h->n - 1 )];
+    if( !h->good )
+    {
+        g_error = "NumericFactorization: matrix is not (sufficiently) positive-definite; first failing supernode "
+                  + std::to_string( h->failed_sn );
+        return TB_NOT_SPD;
+    }
+    return TB_OK;
+}
+
+int require_factor( tb_chol * h )
+{
+    if( h->factorized ) { TB_CUDA( cudaSetDevice( h->device ) ); }
+    if( !h->factorized ) { return fail( TB_ERR_NOT_FACTORIZED, "Solve: nonzero values of matrix have not been passed, yet" ); }
+    if( !h->good ) { return fail( TB_ERR_NOT_FACTORIZED, "Solve: numerical factorization was not successful" ); }
+    return TB_OK;
+}
+
+// which: 0 lower only, 1 upper only, 2 both.  d_B (ldB) -> d_X (ldX), device.
+int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
+                      double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+{
+    const tb::Plan & pl = h->plan;
+    cudaStream_t st = h->stream;
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    TB_TRY( h->work.reserve( static_cast<std::int64_t>(n) * k ) );
+    double * W = h->work.ptr;
+    std::int64_t launches = 0;
+    tb::launch_gather_rows( d_B, ldB, h->p.ptr, W, k, n, k, st );            // ReadRightHandSide
+    ++launches;
+    for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
+    {
+        const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
+        double * Wc = W + c0;
+        if( which != 1 )
+        {
+            for( const tb::Launch & L : pl.lower_launches )
+            {
+                if( L.kind == tb::LaunchKind::SolveDiag ) { tb::launch_solve_diag( h->sdiag.ptr + L.first, L.count, false, h->arena.ptr, Wc, k, kc, st ); }
+                else { tb::launch_solve_rest( h->srest.ptr + L.first, L.count, false, h->arena.ptr, h->sn_inner.ptr, Wc, k, kc, st ); }
+                ++launches;
+            }
+        }
+        if( which != 0 )
+        {
+            for( const tb::Launch & L : pl.upper_launches )
+            {
+                if( L.kind == tb::LaunchKind::SolveDiag ) { tb::launch_solve_diag( h->sdiag.ptr + L.first, L.count, true, h->arena.ptr, Wc, k, kc, st ); }
+                else { tb::launch_solve_rest( h->srest.ptr + L.first, L.count, true, h->arena.ptr, h->sn_inner.ptr, Wc, k, kc, st ); }
+                ++launches;
+            }
+        }
+    }
+    tb::launch_scatter_rows( W, k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );   // WriteSolution
+    ++launches;
+    h->solve_launch_count = launches;
+    TB_CUDA( cudaGetLastError() );
+    return TB_OK;
+}
+
+// Host-buffer solve through pinned staging buffers.
+int run_solve_host( tb_chol * h, int which, double alpha, const double * B, std::int32_t ldB,
+                    double beta, double * X, std::int32_t ldX, std::int32_t nrhs )
+{
+    if( B == nullptr || X == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: null buffer" ); }
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    const size_t bytes = sizeof(double) * static_cast<size_t>(n) * k;
+    cudaStream_t st = h->stream;
+    TB_TRY( h->pin_in.reserve( bytes ) );
+    TB_TRY( h->pin_out.reserve( bytes ) );
+    TB_TRY( h->in.reserve( static_cast<std::int64_t>(n) * k ) );
+    TB_TRY( h->out.reserve( static_cast<std::int64_t>(n) * k ) );
+    double * pi = h->pin_in.as<double>();
+    double * po = h->pin_out.as<double>();
+    if( ldB == k ) { std::memcpy( pi, B, bytes ); }
+    else { for( std::int64_t i = 0; i < n; ++i ) { std::memcpy( pi + i * k, B + i * ldB, sizeof(double) * k ); } }
+    TB_CUDA( cudaMemcpyAsync( h->in.ptr, pi, bytes, cudaMemcpyHostToDevice, st ) );
+    if( beta != 0.0 )
+    {
+        if( ldX == k ) { std::memcpy( po, X, bytes ); }
+        else { for( std::int64_t i = 0; i < n; ++i ) { std::memcpy( po + i * k, X + i * ldX, sizeof(double) * k ); } }
+        TB_CUDA( cudaMemcpyAsync( h->out.ptr, po, bytes, cudaMemcpyHostToDevice, st ) );
+    }
+    TB_TRY( run_solve_device( h, which, alpha, h->in.ptr, k, beta, h->out.ptr, k, k ) );
+    TB_CUDA( cudaMemcpyAsync( po, h->out.ptr, bytes, cudaMemcpyDeviceToHost, st ) );
+    TB_CUDA( cudaStreamSynchronize( st ) );
+    if( ldX == k ) { std::memcpy( X, po, bytes ); }
+    else { for( std::int64_t i = 0; i < n; ++i ) { std::memcpy( X + i * ldX, po + i * k, sizeof(double) * k ); } }
+    return TB_OK;
+}
+
+int fetch_diagonal( tb_chol * h, std::vector<double> & d )
+{
+    TB_TRY( require_factor( h ) );
+    tb::launch_gather_diag( h->diag_off.ptr, h->arena.ptr, h->diag_vals.ptr, h->n, h->stream );
+    d.resize( static_cast<size_t>(h->n) );
+    TB_CUDA( cudaMemcpyAsync( d.data(), h->diag_vals.ptr, sizeof(double) * d.size(), cudaMemcpyDeviceToHost, h->stream ) );
+    TB_CUDA( cudaStreamSynchronize( h->stream ) );
+    return TB_OK;
+}
+
+} // namespace
+
+namespace
+{
+template<typename T>
+std::int64_t copy_array( const std::vector<T> & v, std::int64_t * out )
+{
+    if( out ) { for( size_t i = 0; i < v.size(); ++i ) { out[i] = static_cast<std::int64_t>( v[i] ); } }
+    return static_cast<std::int64_t>( v.size() );
+}
+
+int array_op( tb_chol * h, std::int32_t which, std::int64_t * size, std::int64_t * out )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( ensure_symbolic( h ) );
+    const tb::Symbolic & s = h->sym;
+    std::int64_t n = -1;
+    switch( which )
+    {
+        case TB_ARRAY_PERM:            n = copy_array( s.p, out ); break;
+        case TB_ARRAY_PERM_INV:        n = copy_array( s.p_inv, out ); break;
+        case TB_ARRAY_VALUE_PERM:      n = copy_array( s.value_perm, out ); break;
+        case TB_ARRAY_SN_RP:           n = copy_array( s.sn_rp, out ); break;
+        case TB_ARRAY_SN_OUTER:        n = copy_array( s.sn_outer, out ); break;
+        case TB_ARRAY_SN_INNER:        n = copy_array( s.sn_inner, out ); break;
+        case TB_ARRAY_ROW_TO_SN:       n = copy_array( s.row_to_sn, out ); break;
+        case TB_ARRAY_SN_TRI_PTR:      n = copy_array( s.sn_tri_ptr, out ); break;
+        case TB_ARRAY_SN_REC_PTR:      n = copy_array( s.sn_rec_ptr, out ); break;
+        case TB_ARRAY_ATREE_PARENTS:   n = copy_array( s.atree_parent, out ); break;
+        case TB_ARRAY_ETREE_PARENTS:   n = copy_array( s.etree_parent, out ); break;
+        case TB_ARRAY_OUTER:           n = copy_array( s.outer, out ); break;
+        case TB_ARRAY_INNER:           n = copy_array( s.inner, out ); break;
+        case TB_ARRAY_ATREE_CHILD_PTR: n = copy_array( s.atree_child_ptr, out ); break;
+        case TB_ARRAY_ATREE_CHILD_IDX: n = copy_array( s.atree_child_idx, out ); break;
+        default: return fail( TB_ERR_INVALID_ARGUMENT, "unknown array selector" );
+    }
+    if( size ) { *size = n; }
+    return TB_OK;
+}
+} // namespace
+
+extern "C" {
+
+const char * tb_last_error( void ) { return g_error.c_str(); }
+
+int tb_set_device( int device )
+{
+    int count = 0;
+    if( cudaGetDeviceCount( &count ) != cudaSuccess || count == 0 ) { return fail( TB_ERR_NO_DEVICE, "no CUDA device" ); }
+    if( device < 0 || device >= count ) { return fail( TB_ERR_INVALID_ARGUMENT, "device ordinal out of range" ); }
+    g_device = device;
+    return TB_OK;
+}
+
+int tb_chol_create( tb_chol ** out, std::int32_t n, const std::int64_t * outer, const std::int32_t * inner,
+                    const std::int32_t * perm, std::int32_t thread_count )
+{
+    if( out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output handle" ); }
+    *out = nullptr;
+    if( n <= 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "Size n of matrix is <= 0" ); }
+    if( outer == nullptr || inner == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null pattern" ); }
+    if( outer[0] != 0 || outer[n] < n ) { return fail( TB_ERR_INVALID_PATTERN, "invalid row pointers" ); }
+    auto * h = new tb_chol();
+    h->device = g_device;
+    h->n = n;
+    h->outer.assign( outer, outer + n + 1 );
+    h->inner.assign( inner, inner + outer[n] );
+    if( perm != nullptr ) { h->perm.assign( perm, perm + n ); h->has_perm = true; }
+    h->threads = std::max( 1, thread_count );
+    *out = h;
+    return TB_OK;
+}
+
+int tb_chol_destroy( tb_chol * h )
+{
+    if( h == nullptr ) { return TB_OK; }
+    if( h->stream ) { cudaSetDevice( h->device ); cudaStreamSynchronize( h->stream ); }
+    delete h;
+    return TB_OK;
+}
+
+int tb_chol_set_supernode_strategy( tb_chol * h, std::int32_t strategy )
+{
+    if( h == nullptr || strategy < 0 || strategy > 2 ) { return fail( TB_ERR_INVALID_ARGUMENT, "invalid supernode strategy" ); }
+    const auto s = static_cast<tb::SupernodeStrategy>( strategy );
+    if( s != h->strategy ) { h->strategy = s; h->invalidate_symbolic(); }
+    return TB_OK;
+}
+
+int tb_chol_set_amalgamation_threshold( tb_chol * h, std::int32_t threshold )
+{
+    if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    if( threshold != h->amalgamation_threshold ) { h->amalgamation_threshold = threshold; h->invalidate_symbolic(); }
+    return TB_OK;
+}
+
+int tb_chol_set_factorization_method( tb_chol * h, std::int32_t method )
+{
+    if( h == nullptr || (method != TB_MULTIFRONTAL && method != TB_LEFT_LOOKING) ) { return fail( TB_ERR_INVALID_ARGUMENT, "invalid factorization method" ); }
+    h->method = method;
+    return TB_OK;
+}
+
+int tb_chol_symbolic( tb_chol * h )
+{
+    TB_TRY( check_handle( h ) );
+    return ensure_symbolic( h );
+}
+
+int tb_chol_numeric( tb_chol * h, const double * values, double reg )
+{
+    TB_TRY( check_handle( h ) );
+    if( values == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "NumericFactorization: null values" ); }
+    TB_TRY( ensure_device( h ) );
+    const size_t bytes = sizeof(double) * static_cast<size_t>( h->sym.nnz );
+    TB_TRY( h->pin_in.reserve( bytes ) );
+    std::memcpy( h->pin_in.ptr, values, bytes );
+    TB_CUDA( cudaMemcpyAsync( h->values.ptr, h->pin_in.ptr, bytes, cudaMemcpyHostToDevice, h->stream ) );
+    return run_factor( h, reg );
+}
+
+int tb_chol_numeric_device( tb_chol * h, const double * d_values, double reg )
+{
+    TB_TRY( check_handle( h ) );
+    if( d_values == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "NumericFactorization: null values" ); }
+    TB_TRY( ensure_device( h ) );
+    if( d_values != h->values.ptr )
+    {
+        TB_CUDA( cudaMemcpyAsync( h->values.ptr, d_values, sizeof(double) * static_cast<size_t>( h->sym.nnz ),
+                                  cudaMemcpyDeviceToDevice, h->stream ) );
+    }
+    return run_factor( h, reg );
+}
+
+int tb_chol_solve( tb_chol * h, double alpha, const double * B, std::int32_t ldB,
+                   double beta, double * X, std::int32_t ldX, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    return run_solve_host( h, 2, alpha, B, ldB, beta, X, ldX, nrhs );
+}
+
+int tb_chol_solve_device( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
+                          double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    if( d_B == nullptr || d_X == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: null buffer" ); }
+    return run_solve_device( h, 2, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
+}
+
+int tb_chol_upper_solve( tb_chol * h, double alpha, const double * B, std::int32_t ldB,
+                         double beta, double * X, std::int32_t ldX, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    return run_solve_host( h, 1, alpha, B, ldB, beta, X, ldX, nrhs );
+}
+
+int tb_chol_lower_solve( tb_chol * h, double alpha, const double * B, std::int32_t ldB,
+                         double beta, double * X, std::int32_t ldX, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    return run_solve_host( h, 0, alpha, B, ldB, beta, X, ldX, nrhs );
+}
+
+int tb_chol_residual_device( tb_chol * h, const double * d_B, const double * d_X, double * d_R, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    tb::launch_residual( h->n, h->a_outer.ptr, h->a_inner.ptr, h->values.ptr, d_X, d_B, d_R, std::max( 1, nrhs ), h->stream );
+    TB_CUDA( cudaGetLastError() );
+    return TB_OK;
+}
+
+int tb_chol_sn_count( tb_chol * h, std::int32_t * out )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( ensure_symbolic( h ) );
+    *out = h->sym.sn_count;
+    return TB_OK;
+}
+
+int tb_chol_row_count( tb_chol * h, std::int32_t * out )
+{
+    if( h == nullptr || out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null argument" ); }
+    *out = h->n;
+    return TB_OK;
+}
+
+int tb_chol_nonzero_count( tb_chol * h, std::int64_t * out )
+{
+    if( h == nullptr || out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null argument" ); }
+    *out = h->outer[h->n];
+    return TB_OK;
+}
+
+
+int tb_chol_array_size( tb_chol * h, std::int32_t which, std::int64_t * out )
+{
+    if( out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    return array_op( h, which, out, nullptr );
+}
+
+int tb_chol_array_copy( tb_chol * h, std::int32_t which, std::int64_t * out )
+{
+    if( out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    return array_op( h, which, nullptr, out );
+}
+
+int tb_chol_factorized( tb_chol * h, std::int32_t * factorized, std::int32_t * good )
+{
+    if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    if( factorized ) { *factorized = h->factorized ? 1 : 0; }
+    if( good ) { *good = h->good ? 1 : 0; }
+    return TB_OK;
+}
+
+int tb_chol_failed_supernode( tb_chol * h, std::int32_t * out )
+{
+    if( h == nullptr || out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null argument" ); }
+    *out = h->failed_sn;
+    return TB_OK;
+}
+
+int tb_chol_factor_sizes( tb_chol * h, std::int64_t * tri_size, std::int64_t * rec_size )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( ensure_symbolic( h ) );
+    if( tri_size ) { *tri_size = h->sym.sn_tri_ptr[h->sym.sn_count]; }
+    if( rec_size ) { *rec_size = h->sym.sn_rec_ptr[h->sym.sn_count]; }
+    return TB_OK;
+}
+
+int tb_chol_factor_values( tb_chol * h, double * tri, double * rec )
+{
+    TB_TRY( check_handle( h ) );
+    if( !h->factorized ) { return fail( TB_ERR_NOT_FACTORIZED, "factor values requested before NumericFactorization" ); }
+    TB_CUDA( cudaSetDevice( h->device ) );
+    const std::int64_t ts = h->sym.sn_tri_ptr[h->sym.sn_count];
+    const std::int64_t rs = h->sym.sn_rec_ptr[h->sym.sn_count];
+    TB_TRY( h->exported.reserve( ts + rs ) );
+    tb::launch_export( h->exports.ptr, static_cast<int>( h->plan.exports.size() ), h->colmap.ptr, h->arena.ptr,
+                       h->exported.ptr, h->exported.ptr + ts, h->stream );
+    TB_CUDA( cudaGetLastError() );
+    if( tri && ts ) { TB_CUDA( cudaMemcpyAsync( tri, h->exported.ptr, sizeof(double) * ts, cudaMemcpyDeviceToHost, h->stream ) ); }
+    if( rec && rs ) { TB_CUDA( cudaMemcpyAsync( rec, h->exported.ptr + ts, sizeof(double) * rs, cudaMemcpyDeviceToHost, h->stream ) ); }
+    TB_CUDA( cudaStreamSynchronize( h->stream ) );
+    return TB_OK;
+}
+
+int tb_chol_log_det( tb_chol * h, double * out )
+{
+    TB_TRY( check_handle( h ) );
+    if( out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    std::vector<double> d;
+    TB_TRY( fetch_diagonal( h, d ) );
+    double s = 0.0;
+    for( double v : d ) { s += std::log( v ); }
+    *out = 2.0 * s;
+    return TB_OK;
+}
+
+int tb_chol_factor_diagonal( tb_chol * h, double * diag )
+{
+    TB_TRY( check_handle( h ) );
+    if( diag == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    std::vector<double> d;
+    TB_TRY( fetch_diagonal( h, d ) );
+    std::copy( d.begin(), d.end(), diag );
+    return TB_OK;
+}
+
+int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( ensure_symbolic( h ) );
+    if( factor_flops ) { *factor_flops = h->plan.factor_flops; }
+    if( nnz_u ) { *nnz_u = h->plan.nnz_u; }
+    return TB_OK;
+}
+
+int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
+{
+    TB_TRY( check_handle( h ) );
+    if( out == nullptr || cap < 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    TB_TRY( ensure_symbolic( h ) );
+    const tb::Plan & pl = h->plan;
+    const std::int64_t v[] = {
+        pl.arena_size(), pl.v_size, pl.levels, static_cast<std::int64_t>( pl.factor_launches.size() ) + 2,
+        static_cast<std::int64_t>( pl.gemm.size() ), static_cast<std::int64_t>( pl.panel.size() ),
+        static_cast<std::int64_t>( pl.extend.size() ), static_cast<std::int64_t>( pl.lower_launches.size() ),
+        static_cast<std::int64_t>( pl.upper_launches.size() ), h->sym.sn_count, pl.front_count };
+    const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
+    for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
+    return m;
+}
+
+int tb_chol_check_plan( tb_chol * h )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( ensure_symbolic( h ) );
+    const std::string msg = tb::check_plan( h->sym, h->plan );
+    if( !msg.empty() ) { return fail( TB_ERR_INVALID_ARGUMENT, "plan check: " + msg ); }
+    return TB_OK;
+}
+
+int tb_chol_device_bytes( tb_chol * h, std::int64_t * out )
+{
+    if( h == nullptr || out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null argument" ); }
+    std::int64_t b = 0;
+    b += h->arena.size * 8 + h->asm_src.size * 8 + h->asm_dst.size * 8 + h->diag_off.size * 8;
+    b += (h->lut.size + h->sn_inner.size + h->p.size + h->p_inv.size + h->a_inner.size) * 4;
+    b += h->gemm.size * (std::int64_t)sizeof(tb::GemmTask) + h->panel.size * (std::int64_t)sizeof(tb::PanelTask);
+    b += h->extend.size * (std::int64_t)sizeof(tb::ExtendTask) + h->sdiag.size * (std::int64_t)sizeof(tb::SolveDiagTask);
+    b += h->srest.size * (std::int64_t)sizeof(tb::SolveRestTask) + h->a_outer.size * 8;
+    b += h->zero.size * (std::int64_t)sizeof(tb::ZeroTask) + h->exports.size * (std::int64_t)sizeof(tb::ExportTask);
+    b += h->colmap.size * 4 + h->exported.size * 8;
+    b += (h->values.size + h->work.size + h->in.size + h->out.size + h->diag_vals.size) * 8;
+    *out = b;
+    return TB_OK;
+}
+
+int tb_chol_set_stream( tb_chol * h, void * stream )
+{
+    TB_TRY( check_handle( h ) );
+    TB_CUDA( cudaSetDevice( h->device ) );
+    if( h->stream ) { TB_CUDA( cudaStreamSynchronize( h->stream ) ); }
+    if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    if( h->own_stream && h->stream ) { cudaStreamDestroy( h->stream ); }
+    if( stream == nullptr )
+    {
+        TB_CUDA( cudaStreamCreateWithFlags( &h->stream, cudaStreamNonBlocking ) );
+        h->own_stream = true;
+    }
+    else
+    {
+        h->stream = static_cast<cudaStream_t>( stream );
+        h->own_stream = false;
+    }
+    return TB_OK;
+}
+
+int tb_chol_set_graph( tb_chol * h, std::int32_t enabled )
+{
+    if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    h->use_graph = (enabled != 0);
+    return TB_OK;
+}
+
+int tb_chol_set_profiling( tb_chol * h, std::int32_t enabled )
+{
+    if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    h->profiling = (enabled != 0);
+    return TB_OK;
+}
+
+int tb_chol_kernel_profile( tb_chol * h, double * ms, std::int64_t * launches, double * flops )
+{
+    if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    for( int k = 0; k < 8; ++k )
+    {
+        if( ms ) { ms[k] = h->kind_ms[k]; }
+        if( launches ) { launches[k] = h->kind_launches[k]; }
+        if( flops ) { flops[k] = 0.0; }
+    }
+    if( flops && h->symbolic_done ) { flops[static_cast<int>( tb::LaunchKind::Gemm )] = h->plan.gemm_flops; }
+    return TB_OK;
+}
+
+int tb_chol_launch_counts( tb_chol * h, std::int64_t * factor_launches, std::int64_t * solve_launches )
+{
+    if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    if( factor_launches ) { *factor_launches = h->factor_launch_count; }
+    if( solve_launches ) { *solve_launches = h->solve_launch_count; }
+    return TB_OK;
+}
+
+} // extern "C"

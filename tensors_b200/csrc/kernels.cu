@@ -1,0 +1,600 @@
+// FP64 kernels of the supernodal factorization and solves (sm_100a).
+//
+// Every kernel consumes a flat task array built by Plan::build (plan.cpp):
+// one CTA per task, no inter-CTA dependencies inside a launch, so a level's
+// work for all of its supernodes is a handful of launches regardless of how
+// many supernodes it has.  FP64 has no tcgen05 MMA kind, so the FP64 tile
+// products use DMMA (mma.sync.m8n8k4.f64), the only FP64 tensor-core path on
+// Blackwell.
+
+#include "kernels.cuh"
+
+#include <climits>
+
+namespace tb
+{
+namespace
+{
+
+constexpr int kGemmThreads  = 128;
+constexpr int kGemmK        = 16;
+constexpr int kGemmLd       = kTile + 4;   // padded smem row (2 wavefronts per fragment load)
+constexpr int kPanelThreads = kRestChunk;
+constexpr int kSolveThreads = 256;
+constexpr int kMaxRhs       = kSolveMaxRhs;   // columns per solve launch
+
+__device__ __forceinline__ void dmma_8x8x4( double (&d)[2], double a, double b )
+{
+    asm volatile( "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                  : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b) );
+}
+
+// ---------------------------------------------------------------- assembly
+// arena[dst] = values[src] (+ reg on the diagonal): ReadNonzeroValues
+// (Numeric.hpp:165-180) fused with FetchFromA (Multifrontal.hpp:249-321).
+__global__ void assemble_kernel( const double * __restrict__ values, const std::int64_t * __restrict__ src,
+                                 const std::int64_t * __restrict__ dst, std::int64_t count,
+                                 const double * __restrict__ reg, double * __restrict__ arena )
+{
+    const double r = *reg;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < count;
+         e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const std::uint64_t d = static_cast<std::uint64_t>( dst[e] );
+        double v = values[src[e]];
+        if( d & kDiagFlag ) { v += r; }
+        arena[d & (kDiagFlag - 1)] = v;
+    }
+}
+
+// ------------------------------------------------------------------ zeroing
+__global__ void zero_kernel( const ZeroTask * __restrict__ tasks, double * __restrict__ arena )
+{
+    const ZeroTask t = tasks[blockIdx.x];
+    double * p = arena + t.offset;
+    for( std::int64_t i = threadIdx.x; i < t.count; i += blockDim.x ) { p[i] = 0.0; }
+}
+
+// ---------------------------------------------------------------- export
+// Reference layout from the fronts: U0 of supernode s is the diagonal block
+// of its front at row offset roff; column l of its U1 is front U0 column
+// colmap[l] (>= 0) or front U1 column -colmap[l]-1.
+__global__ void export_kernel( const ExportTask * __restrict__ tasks, const std::int32_t * __restrict__ colmap_all,
+                               const double * __restrict__ arena, double * __restrict__ tri, double * __restrict__ rec )
+{
+    const ExportTask t = tasks[blockIdx.x];
+    const std::int32_t * colmap = colmap_all + t.colmap;
+    for( int r = t.r_begin; r < t.r_end; ++r )
+    {
+        const std::int64_t fr = t.roff + r;
+        const double * f0 = arena + t.fu0 + fr * t.fn0;
+        const double * f1 = arena + t.fu1 + fr * t.fn1;
+        double * d0 = tri + t.tri + (std::int64_t)r * t.n0s;
+        for( int c = threadIdx.x; c < t.n0s; c += blockDim.x ) { d0[c] = (c >= r) ? f0[t.roff + c] : 0.0; }
+        double * d1 = rec + t.rec + (std::int64_t)r * t.n1s;
+        for( int l = threadIdx.x; l < t.n1s; l += blockDim.x )
+        {
+            const int cm = colmap[l];
+            d1[l] = (cm >= 0) ? f0[cm] : f1[-cm - 1];
+        }
+    }
+}
+
+// ------------------------------------------------------------- extend-add
+// One warp per row of the child's update W; lanes walk the row's upper part
+// (coalesced reads of W, lut-indexed adds into the parent front).
+__global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restrict__ tasks,
+                                                      const std::int32_t * __restrict__ lut_all,
+                                                      double * __restrict__ arena )
+{
+    const ExtendTask t = tasks[blockIdx.x];
+    const std::int32_t * lut = lut_all + t.lut;
+    const double * W = arena + t.w;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for( int i = t.row_begin + warp; i < t.row_end; i += 8 )
+    {
+        const std::int64_t li = lut[i];
+        const double * Wi = W + (std::int64_t)i * t.m1;
+        if( i < t.mid )
+        {
+            double * row0 = arena + t.u0 + li * t.n0p;
+            double * row1 = arena + t.u1 + li * t.n1p;
+            for( int j = i + lane; j < t.m1; j += 32 )
+            {
+                const int lj = lut[j];
+                const double v = Wi[j];
+                if( j < t.mid ) { row0[lj] += v; } else { row1[lj] += v; }
+            }
+        }
+        else
+        {
+            double * rowv = arena + t.v + li * t.n1p;
+            for( int j = i + lane; j < t.m1; j += 32 ) { rowv[lut[j]] += Wi[j]; }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ panel
+// Cholesky of the panel's nb x nb diagonal block in shared memory (every CTA
+// of the panel repeats it; the write_diag CTA stores it), then each thread
+// solves one rest column D^T x = u with the column held in registers
+// (potrf + trsm of FactorizeSupernode, Multifrontal.hpp:438-475).  A row
+// that forms a 1 x 1 reference supernode takes sqrt(|a|) as the reference
+// does (:471) and never reports failure.
+__global__ __launch_bounds__(kPanelThreads, 1) void panel_kernel( const PanelTask * __restrict__ tasks,
+                                                               double * __restrict__ arena, int * __restrict__ status )
+{
+    const PanelTask t = tasks[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int nb = min( kPanel, t.n0 - t.r0 );
+    const int r1 = t.r0 + nb;
+    const int m = t.n0 - r1;
+    const int rest = m + t.n1;
+    __shared__ double D[kPanel][kPanel + 1];
+    __shared__ double inv_d[kPanel];
+    __shared__ int fail;
+
+    double * U0 = arena + t.u0;
+    double * U1 = arena + t.u1;
+    for( int idx = tid; idx < kPanel * kPanel; idx += kPanelThreads )
+    {
+        const int r = idx / kPanel, c = idx % kPanel;
+        double v = (r == c) ? 1.0 : 0.0;
+        if( r < nb && c < nb && c >= r ) { v = U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c]; }
+        D[r][c] = v;
+    }
+    if( tid == 0 ) { fail = -1; }
+    __syncthreads();
+
+    for( int j = 0; j < nb; ++j )
+    {
+        if( tid == 0 )
+        {
+            double d = D[j][j];
+            if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
+            else if( !(d > 0.0) && fail < 0 ) { fail = j; }
+            d = sqrt( d );
+            D[j][j] = d;
+            inv_d[j] = 1.0 / d;
+        }
+        __syncthreads();
+        for( int c = j + 1 + tid; c < nb; c += kPanelThreads ) { D[j][c] *= inv_d[j]; }
+        __syncthreads();
+        const int w = nb - j - 1;
+        for( int idx = tid; idx < w * w; idx += kPanelThreads )
+        {
+            const int r = j + 1 + idx / w, c = j + 1 + idx % w;
+            if( c >= r ) { D[r][c] -= D[j][r] * D[j][c]; }
+        }
+        __syncthreads();
+    }
+    for( int r = nb + tid; r < kPanel; r += kPanelThreads ) { inv_d[r] = 1.0; }
+    __syncthreads();
+
+    if( t.write_diag )
+    {
+        for( int idx = tid; idx < nb * nb; idx += kPanelThreads )
+        {
+            const int r = idx / nb, c = idx % nb;
+            if( c >= r ) { U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] = D[r][c]; }
+        }
+        if( tid == 0 && fail >= 0 )
+        {
+            atomicOr( status, 1 );
+            atomicMin( status + 1, t.row0 + t.r0 + fail );
+        }
+    }
+
+    const int col = t.c0 + tid;
+    if( col < rest )
+    {
+        double * base;
+        std::int64_t ld;
+        if( col < m ) { base = U0 + (std::int64_t)t.r0 * t.n0 + r1 + col; ld = t.n0; }
+        else          { base = U1 + (std::int64_t)t.r0 * t.n1 + (col - m); ld = t.n1; }
+        double x[kPanel];
+#pragma unroll
+        for( int r = 0; r < kPanel; ++r ) { x[r] = (r < nb) ? base[r * ld] : 0.0; }
+#pragma unroll
+        for( int r = 0; r < kPanel; ++r )
+        {
+            x[r] *= inv_d[r];
+#pragma unroll
+            for( int r2 = 0; r2 < kPanel; ++r2 ) { if( r2 > r ) { x[r2] -= D[r][r2] * x[r]; } }
+        }
+#pragma unroll
+        for( int r = 0; r < kPanel; ++r ) { if( r < nb ) { base[r * ld] = x[r]; } }
+    }
+}
+
+// ------------------------------------------------------------------- gemm
+// C[m0:m0+64, c0:c0+64] -= A[:, m0:]^T B[:, c0:] for row-major K x M / K x N
+// panels: 4 warps in a 2 x 2 arrangement, each a 32 x 32 block of 8 x 8
+// DMMA tiles; K staged through double-buffered shared memory 16 rows at a
+// time (register prefetch of the next chunk overlaps the MMAs).
+__global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask * __restrict__ tasks,
+                                                                double * __restrict__ arena )
+{
+    const GemmTask t = tasks[blockIdx.x];
+    __shared__ double As[2][kGemmK][kGemmLd];
+    __shared__ double Bs[2][kGemmK][kGemmLd];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1;
+    const double * A = arena + t.a;
+    const double * B = arena + t.b;
+
+    double acc[4][4][2];
+#pragma unroll
+    for( int i = 0; i < 4; ++i )
+#pragma unroll
+        for( int j = 0; j < 4; ++j ) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
+
+    constexpr int kPer = kGemmK * kTile / kGemmThreads;   // 8 elements per thread per operand
+    double ra[kPer], rb[kPer];
+    auto load = [&]( int k0 )
+    {
+#pragma unroll
+        for( int l = 0; l < kPer; ++l )
+        {
+            const int idx = tid + kGemmThreads * l;
+            const int r = idx / kTile, c = idx % kTile;
+            const int k = k0 + r;
+            ra[l] = (k < t.K && t.m0 + c < t.M) ? A[(std::int64_t)k * t.lda + t.m0 + c] : 0.0;
+            rb[l] = (k < t.K && t.c0 + c < t.N) ? B[(std::int64_t)k * t.ldb + t.c0 + c] : 0.0;
+        }
+    };
+    auto store = [&]( int buf )
+    {
+#pragma unroll
+        for( int l = 0; l < kPer; ++l )
+        {
+            const int idx = tid + kGemmThreads * l;
+            const int r = idx / kTile, c = idx % kTile;
+            As[buf][r][c] = ra[l];
+            Bs[buf][r][c] = rb[l];
+        }
+    };
+
+    const int nk = (t.K + kGemmK - 1) / kGemmK;
+    load( 0 );
+    store( 0 );
+    __syncthreads();
+    for( int kc = 0; kc < nk; ++kc )
+    {
+        const int buf = kc & 1;
+        if( kc + 1 < nk ) { load( (kc + 1) * kGemmK ); }
+#pragma unroll
+        for( int kk = 0; kk < kGemmK; kk += 4 )
+        {
+            double af[4], bf[4];
+#pragma unroll
+            for( int i = 0; i < 4; ++i ) { af[i] = As[buf][kk + (lane & 3)][wm * 32 + i * 8 + (lane >> 2)]; }
+#pragma unroll
+            for( int j = 0; j < 4; ++j ) { bf[j] = Bs[buf][kk + (lane & 3)][wn * 32 + j * 8 + (lane >> 2)]; }
+#pragma unroll
+            for( int i = 0; i < 4; ++i )
+#pragma unroll
+                for( int j = 0; j < 4; ++j ) { dmma_8x8x4( acc[i][j], af[i], bf[j] ); }
+        }
+        if( kc + 1 < nk ) { store( buf ^ 1 ); }
+        __syncthreads();
+    }
+
+    double * C = arena + t.c;
+#pragma unroll
+    for( int i = 0; i < 4; ++i )
+    {
+        const int row = t.m0 + wm * 32 + i * 8 + (lane >> 2);
+        if( row >= t.M ) { continue; }
+#pragma unroll
+        for( int j = 0; j < 4; ++j )
+        {
+#pragma unroll
+            for( int e = 0; e < 2; ++e )
+            {
+                const int col = t.c0 + wn * 32 + j * 8 + (lane & 3) * 2 + e;
+                if( col < t.N && (!t.upper || row <= col) )
+                {
+                    C[(std::int64_t)row * t.ldc + col] -= acc[i][j][e];
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ solves
+// Triangular solve with a panel's diagonal block for the panel's rows of X
+// (k <= 64 columns): D^T x = b forward (LowerSolver.hpp:183-197) or
+// D x = b backward (UpperSolver.hpp:190-200).
+__global__ __launch_bounds__(kSolveThreads) void solve_diag_kernel( const SolveDiagTask * __restrict__ tasks, int upper,
+                                                                    const double * __restrict__ arena,
+                                                                    double * __restrict__ X, int ldx, int k )
+{
+    extern __shared__ double smem[];
+    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem );
+    double * Xs = smem + kPanel * (kPanel + 1);        // [kPanel][k]
+    const SolveDiagTask t = tasks[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int nb = min( kPanel, t.n0 - t.r0 );
+    const double * U0 = arena + t.u0;
+    for( int idx = tid; idx < nb * nb; idx += kSolveThreads )
+    {
+        const int r = idx / nb, c = idx % nb;
+        D[r][c] = (c >= r) ? U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] : 0.0;
+    }
+    const std::int64_t row_base = (std::int64_t)t.row0 + t.r0;
+    for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+    {
+        const int r = idx / k, c = idx % k;
+        Xs[r * k + c] = X[(row_base + r) * ldx + c];
+    }
+    __syncthreads();
+    if( !upper )
+    {
+        for( int r = 0; r < nb; ++r )
+        {
+            if( tid < k ) { Xs[r * k + tid] /= D[r][r]; }
+            __syncthreads();
+            const int w = nb - r - 1;
+            for( int idx = tid; idx < w * k; idx += kSolveThreads )
+            {
+                const int r2 = r + 1 + idx / k, c = idx % k;
+                Xs[r2 * k + c] -= D[r][r2] * Xs[r * k + c];
+            }
+            __syncthreads();
+        }
+    }
+    else
+    {
+        for( int r = nb - 1; r >= 0; --r )
+        {
+            if( tid < k ) { Xs[r * k + tid] /= D[r][r]; }
+            __syncthreads();
+            for( int idx = tid; idx < r * k; idx += kSolveThreads )
+            {
+                const int r2 = idx / k, c = idx % k;
+                Xs[r2 * k + c] -= D[r2][r] * Xs[r * k + c];
+            }
+            __syncthreads();
+        }
+    }
+    for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+    {
+        const int r = idx / k, c = idx % k;
+        X[(row_base + r) * ldx + c] = Xs[r * k + c];
+    }
+}
+
+// The rest of a panel in the solves.  Forward: X[rest] -= P^T X_panel, with
+// rows of the supernode itself updated in place and ancestor rows (through
+// SN_inner) by atomic adds, since other supernodes of the level may target
+// them (LowerSolver.hpp:199-231).  Backward: X_panel -= P X[rest] gathered
+// from final rows (UpperSolver.hpp:151-188), reduced over rest chunks by
+// atomic adds.
+__global__ __launch_bounds__(kSolveThreads) void solve_rest_kernel( const SolveRestTask * __restrict__ tasks, int upper,
+                                                                    const double * __restrict__ arena,
+                                                                    const std::int32_t * __restrict__ sn_inner,
+                                                                    double * __restrict__ X, int ldx, int k )
+{
+    extern __shared__ double smem[];
+    double (*P)[kSolveRest + 1] = reinterpret_cast<double (*)[kSolveRest + 1]>( smem );   // [kPanel][kSolveRest+1]
+    double * Xs = smem + kPanel * (kSolveRest + 1);
+    const SolveRestTask t = tasks[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int nb = min( kPanel, t.n0 - t.r0 );
+    const int r1 = t.r0 + nb;
+    const int m = t.n0 - r1;
+    const int cw = t.c1 - t.c0;
+    const double * U0 = arena + t.u0;
+    const double * U1 = arena + t.u1;
+    for( int idx = tid; idx < nb * cw; idx += kSolveThreads )
+    {
+        const int i = idx / cw, jj = idx % cw;
+        const int j = t.c0 + jj;
+        P[i][jj] = (j < m) ? U0[(std::int64_t)(t.r0 + i) * t.n0 + r1 + j]
+                           : U1[(std::int64_t)(t.r0 + i) * t.n1 + (j - m)];
+    }
+    const std::int64_t panel_row = (std::int64_t)t.row0 + t.r0;
+    auto target_row = [&]( int j ) -> std::int64_t
+    {
+        return (j < m) ? (std::int64_t)t.row0 + r1 + j : (std::int64_t)sn_inner[t.inner + (j - m)];
+    };
+    if( !upper )
+    {
+        for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+        {
+            const int i = idx / k, c = idx % k;
+            Xs[i * k + c] = X[(panel_row + i) * ldx + c];
+        }
+        __syncthreads();
+        for( int idx = tid; idx < cw * k; idx += kSolveThreads )
+        {
+            const int jj = idx / k, c = idx % k;
+            double acc = 0.0;
+            for( int i = 0; i < nb; ++i ) { acc += P[i][jj] * Xs[i * k + c]; }
+            const int j = t.c0 + jj;
+            double * dst = X + target_row( j ) * ldx + c;
+            if( j < m ) { *dst -= acc; } else { atomicAdd( dst, -acc ); }
+        }
+    }
+    else
+    {
+        for( int idx = tid; idx < cw * k; idx += kSolveThreads )
+        {
+            const int jj = idx / k, c = idx % k;
+            Xs[jj * k + c] = X[target_row( t.c0 + jj ) * ldx + c];
+        }
+        __syncthreads();
+        for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+        {
+            const int i = idx / k, c = idx % k;
+            double acc = 0.0;
+            for( int jj = 0; jj < cw; ++jj ) { acc += P[i][jj] * Xs[jj * k + c]; }
+            atomicAdd( X + (panel_row + i) * ldx + c, -acc );
+        }
+    }
+}
+
+// ------------------------------------------------------ permutations, SpMV
+__global__ void gather_rows_kernel( const double * __restrict__ B, int ldB, const std::int32_t * __restrict__ p,
+                                    double * __restrict__ W, int ldw, int n, int k )
+{
+    const std::int64_t total = (std::int64_t)n * k;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const std::int64_t i = e / k;
+        const int c = static_cast<int>( e % k );
+        W[i * ldw + c] = B[(std::int64_t)p[i] * ldB + c];
+    }
+}
+
+__global__ void scatter_rows_kernel( const double * __restrict__ W, int ldw, const std::int32_t * __restrict__ p_inv,
+                                     double alpha, double beta, double * __restrict__ Y, int ldY, int n, int k )
+{
+    const std::int64_t total = (std::int64_t)n * k;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total;
+         e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const std::int64_t i = e / k;
+        const int c = static_cast<int>( e % k );
+        double y = (alpha == 0.0) ? 0.0 : alpha * W[(std::int64_t)p_inv[i] * ldw + c];
+        if( beta != 0.0 ) { y += beta * Y[i * ldY + c]; }
+        Y[i * ldY + c] = y;
+    }
+}
+
+// R = B - A X, one warp per row, lanes over the row's entries.
+__global__ void residual_kernel( int n, const std::int64_t * __restrict__ outer, const std::int32_t * __restrict__ inner,
+                                 const double * __restrict__ vals, const double * __restrict__ X,
+                                 const double * __restrict__ B, double * __restrict__ R, int k )
+{
+    const int lane = threadIdx.x & 31;
+    const std::int64_t warp = (blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x) >> 5;
+    const std::int64_t warps = ((std::int64_t)gridDim.x * blockDim.x) >> 5;
+    for( std::int64_t i = warp; i < n; i += warps )
+    {
+        for( int c = 0; c < k; ++c )
+        {
+            double s = 0.0;
+            for( std::int64_t e = outer[i] + lane; e < outer[i+1]; e += 32 ) { s += vals[e] * X[(std::int64_t)inner[e] * k + c]; }
+#pragma unroll
+            for( int o = 16; o > 0; o >>= 1 ) { s += __shfl_xor_sync( 0xffffffffu, s, o ); }
+            if( lane == 0 ) { R[i * k + c] = B[i * k + c] - s; }
+        }
+    }
+}
+
+__global__ void gather_diag_kernel( const std::int64_t * __restrict__ offsets, const double * __restrict__ arena,
+                                    double * __restrict__ out, int n )
+{
+    for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        out[i] = arena[offsets[i]];
+    }
+}
+
+__global__ void init_status_kernel( int * status )
+{
+    status[0] = 0;
+    status[1] = INT_MAX;
+}
+
+int grid_for( std::int64_t work, int threads )
+{
+    const std::int64_t blocks = (work + threads - 1) / threads;
+    return static_cast<int>( blocks < 1 ? 1 : (blocks > 148 * 32 ? 148 * 32 : blocks) );
+}
+
+} // namespace
+
+void launch_assemble( const double * values, const std::int64_t * src, const std::int64_t * dst,
+                      std::int64_t count, const double * reg, double * arena, cudaStream_t st )
+{
+    if( count <= 0 ) { return; }
+    assemble_kernel<<<grid_for( count, 256 ), 256, 0, st>>>( values, src, dst, count, reg, arena );
+}
+
+void launch_zero( const ZeroTask * tasks, int count, double * arena, cudaStream_t st )
+{
+    if( count > 0 ) { zero_kernel<<<count, 256, 0, st>>>( tasks, arena ); }
+}
+
+void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const double * arena,
+                    double * tri, double * rec, cudaStream_t st )
+{
+    if( count > 0 ) { export_kernel<<<count, 128, 0, st>>>( tasks, colmap, arena, tri, rec ); }
+}
+
+void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, double * arena, cudaStream_t st )
+{
+    if( count > 0 ) { extend_kernel<<<count, 256, 0, st>>>( tasks, lut, arena ); }
+}
+
+void launch_panel( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st )
+{
+    if( count > 0 ) { panel_kernel<<<count, kPanelThreads, 0, st>>>( tasks, arena, status ); }
+}
+
+void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st )
+{
+    if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, 0, st>>>( tasks, arena ); }
+}
+
+void launch_solve_diag( const SolveDiagTask * tasks, int count, bool upper, const double * arena,
+                        double * X, int ldx, int k, cudaStream_t st )
+{
+    if( count <= 0 ) { return; }
+    const size_t smem = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kMaxRhs);
+    solve_diag_kernel<<<count, kSolveThreads, smem, st>>>( tasks, upper ? 1 : 0, arena, X, ldx, k );
+}
+
+void launch_solve_rest( const SolveRestTask * tasks, int count, bool upper, const double * arena,
+                        const std::int32_t * sn_inner, double * X, int ldx, int k, cudaStream_t st )
+{
+    if( count <= 0 ) { return; }
+    const size_t smem = sizeof(double) * (kPanel * (kSolveRest + 1) + kSolveRest * kMaxRhs);
+    solve_rest_kernel<<<count, kSolveThreads, smem, st>>>( tasks, upper ? 1 : 0, arena, sn_inner, X, ldx, k );
+}
+
+void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
+                         int n, int k, cudaStream_t st )
+{
+    gather_rows_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( B, ldB, p, W, ldw, n, k );
+}
+
+void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv, double alpha, double beta,
+                          double * Y, int ldY, int n, int k, cudaStream_t st )
+{
+    scatter_rows_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( W, ldw, p_inv, alpha, beta, Y, ldY, n, k );
+}
+
+void launch_residual( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
+                      const double * X, const double * B, double * R, int k, cudaStream_t st )
+{
+    residual_kernel<<<grid_for( (std::int64_t)n * 32, 256 ), 256, 0, st>>>( n, outer, inner, vals, X, B, R, k );
+}
+
+cudaError_t configure_kernels()
+{
+    cudaError_t e = cudaFuncSetAttribute( solve_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)( sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kMaxRhs) ) );
+    if( e != cudaSuccess ) { return e; }
+    return cudaFuncSetAttribute( solve_rest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)( sizeof(double) * (kPanel * (kSolveRest + 1) + kSolveRest * kMaxRhs) ) );
+}
+
+void launch_gather_diag( const std::int64_t * offsets, const double * arena, double * out, int n, cudaStream_t st )
+{
+    gather_diag_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( offsets, arena, out, n );
+}
+
+void launch_init_status( int * status, cudaStream_t st )
+{
+    init_status_kernel<<<1, 1, 0, st>>>( status );
+}
+
+} // namespace tb

@@ -1,0 +1,43 @@
+// Kernel entry points of the FP64 supernodal factorization and solves.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "plan.hpp"
+
+namespace tb
+{
+
+// status[0]: bit 0 set when a pivot was not positive; status[1]: smallest
+// failing (permuted) row index (initialised to INT_MAX).
+void launch_assemble( const double * values, const std::int64_t * src, const std::int64_t * dst,
+                      std::int64_t count, const double * reg, double * arena, cudaStream_t st );
+void launch_zero( const ZeroTask * tasks, int count, double * arena, cudaStream_t st );
+void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const double * arena,
+                    double * tri, double * rec, cudaStream_t st );
+void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, double * arena, cudaStream_t st );
+void launch_panel( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st );
+void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st );
+
+void launch_solve_diag( const SolveDiagTask * tasks, int count, bool upper, const double * arena,
+                        double * X, int ldx, int k, cudaStream_t st );
+void launch_solve_rest( const SolveRestTask * tasks, int count, bool upper, const double * arena,
+                        const std::int32_t * sn_inner, double * X, int ldx, int k, cudaStream_t st );
+
+void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
+                         int n, int k, cudaStream_t st );
+void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv, double alpha, double beta,
+                          double * Y, int ldY, int n, int k, cudaStream_t st );
+void launch_residual( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
+                      const double * X, const double * B, double * R, int k, cudaStream_t st );
+void launch_init_status( int * status, cudaStream_t st );
+void launch_gather_diag( const std::int64_t * offsets, const double * arena, double * out, int n, cudaStream_t st );
+
+// Raises the dynamic shared-memory limits of the solve kernels on the
+// current device; call once per device before the first launch.
+cudaError_t configure_kernels();
+
+constexpr int kSolveMaxRhs = 64;   // right-hand sides per solve launch
+
+} // namespace tb

@@ -1,0 +1,489 @@
+// Device execution plan; see plan.hpp.
+
+#include "plan.hpp"
+#include "common.hpp"
+
+#include <algorithm>
+#include <map>
+
+namespace tb
+{
+namespace
+{
+using I32 = std::int32_t;
+using I64 = std::int64_t;
+
+constexpr I64 kExtendEntries = 8192;   // target entries of W per extend-add task
+constexpr I64 kExportEntries = 16384;  // target entries per export task
+
+void push_tiles( std::vector<GemmTask> & out, I64 a, I32 lda, I64 b, I32 ldb, I64 c, I32 ldc,
+                 I32 K, I32 M, I32 N, bool symmetric )
+{
+    for( I32 m0 = 0; m0 < M; m0 += kTile )
+    {
+        for( I32 c0 = symmetric ? m0 : 0; c0 < N; c0 += kTile )
+        {
+            GemmTask t{};
+            t.a = a; t.b = b; t.c = c;
+            t.lda = lda; t.ldb = ldb; t.ldc = ldc;
+            t.K = K; t.M = M; t.N = N;
+            t.m0 = m0; t.c0 = c0;
+            t.upper = (symmetric && m0 == c0) ? 1 : 0;
+            out.push_back( t );
+        }
+    }
+}
+
+// First-fit allocator over [0, capacity) with coalescing free list; grows
+// the capacity when nothing fits.
+class RegionAllocator
+{
+public:
+    I64 allocate( I64 size )
+    {
+        if( size <= 0 ) { return 0; }
+        for( auto it = free_.begin(); it != free_.end(); ++it )
+        {
+            if( it->second >= size )
+            {
+                const I64 off = it->first;
+                const I64 rest = it->second - size;
+                free_.erase( it );
+                if( rest > 0 ) { free_[off + size] = rest; }
+                return off;
+            }
+        }
+        // extend: reuse a free block that ends at the top
+        if( !free_.empty() )
+        {
+            auto last = std::prev( free_.end() );
+            if( last->first + last->second == top_ )
+            {
+                const I64 off = last->first;
+                free_.erase( last );
+                top_ = off + size;
+                return off;
+            }
+        }
+        const I64 off = top_;
+        top_ += size;
+        return off;
+    }
+    void release( I64 off, I64 size )
+    {
+        if( size <= 0 ) { return; }
+        auto it = free_.emplace( off, size ).first;
+        if( it != free_.begin() )
+        {
+            auto prev = std::prev( it );
+            if( prev->first + prev->second == it->first )
+            {
+                prev->second += it->second;
+                free_.erase( it );
+                it = prev;
+            }
+        }
+        auto next = std::next( it );
+        if( next != free_.end() && it->first + it->second == next->first )
+        {
+            it->second += next->second;
+            free_.erase( next );
+        }
+    }
+    I64 capacity() const { return top_; }
+
+private:
+    std::map<I64,I64> free_;
+    I64 top_ = 0;
+};
+
+} // namespace
+
+void Plan::build( const Symbolic & sym )
+{
+    const I32 S = sym.sn_count;
+    const I32 n = sym.n;
+
+    factor_flops = 0.0;
+    nnz_u = 0.0;
+    for( I32 s = 0; s < S; ++s )
+    {
+        const double a = sym.n0(s), b = sym.n1(s);
+        factor_flops += a * a * a / 3.0 + a * a * b + a * b * b;
+        nnz_u += a * (a + 1.0) / 2.0 + a * b;
+    }
+
+    // ---------------------------------------------------------------- fronts
+    // Walk supernodes in order; supernode s joins the front of s+1 when it is
+    // the last child of s+1 (aTree parent == s+1, so rows are contiguous) and
+    // the relaxation limits allow it.
+    std::vector<I32> merged_into( static_cast<size_t>(S), -1 );
+    {
+        std::vector<I64> rows( static_cast<size_t>(S) );
+        std::vector<double> zeros( static_cast<size_t>(S), 0.0 );
+        for( I32 s = 0; s < S; ++s ) { rows[s] = sym.n0(s); }
+        for( I32 s = 0; s + 1 < S; ++s )
+        {
+            const I32 p = sym.atree_parent[s];
+            if( p != s + 1 ) { continue; }
+            const double a0 = static_cast<double>(rows[s]), a1 = sym.n1(s);
+            const double b0 = sym.n0(p), b1 = sym.n1(p);
+            const double m0 = a0 + b0;
+            const double z = zeros[s] + zeros[p] + a0 * (b0 + b1 - a1);
+            const double total = m0 * (m0 + 1.0) / 2.0 + m0 * b1;
+            bool take;
+            if( m0 <= relax.nrelax[0] )      { take = true; }
+            else if( m0 <= relax.nrelax[1] ) { take = z < relax.zrelax[0] * total; }
+            else if( m0 <= relax.nrelax[2] ) { take = z < relax.zrelax[1] * total; }
+            else                             { take = z < relax.zrelax[2] * total; }
+            if( take )
+            {
+                merged_into[s] = p;
+                rows[p] = static_cast<I64>(m0);
+                zeros[p] = z;
+            }
+        }
+    }
+    front_of_sn.assign( static_cast<size_t>(S), -1 );
+    front_sn_first.clear(); front_sn_last.clear();
+    {
+        I32 first = 0;
+        for( I32 s = 0; s < S; ++s )
+        {
+            if( merged_into[s] >= 0 ) { continue; }
+            front_sn_first.push_back( first );
+            front_sn_last.push_back( s );
+            first = s + 1;
+        }
+    }
+    front_count = static_cast<I32>( front_sn_last.size() );
+    const I32 F = front_count;
+    front_row0.resize( static_cast<size_t>(F) );
+    front_n0.resize( static_cast<size_t>(F) );
+    front_n1.resize( static_cast<size_t>(F) );
+    front_cols.resize( static_cast<size_t>(F) );
+    front_parent.resize( static_cast<size_t>(F) );
+    for( I32 f = 0; f < F; ++f )
+    {
+        for( I32 s = front_sn_first[f]; s <= front_sn_last[f]; ++s ) { front_of_sn[s] = f; }
+        front_row0[f] = sym.sn_rp[front_sn_first[f]];
+        front_n0[f] = sym.sn_rp[front_sn_last[f] + 1] - front_row0[f];
+        front_n1[f] = sym.n1( front_sn_last[f] );
+        front_cols[f] = sym.sn_outer[front_sn_last[f]];
+    }
+    front_flops = 0.0;
+    front_entries = 0.0;
+    for( I32 f = 0; f < F; ++f )
+    {
+        const I32 p = sym.atree_parent[front_sn_last[f]];
+        front_parent[f] = (p < S) ? front_of_sn[p] : F;
+        const double a = front_n0[f], b = front_n1[f];
+        front_flops += a * a * a / 3.0 + a * a * b + a * b * b;
+        front_entries += a * (a + 1.0) / 2.0 + a * b;
+    }
+    std::vector<I32> child_ptr( static_cast<size_t>(F) + 2, 0 ), child_idx( static_cast<size_t>(F) );
+    for( I32 f = 0; f < F; ++f ) { ++child_ptr[front_parent[f] + 1]; }
+    for( I32 f = 0; f <= F; ++f ) { child_ptr[f+1] += child_ptr[f]; }
+    {
+        std::vector<I32> next( child_ptr.begin(), child_ptr.end() - 1 );
+        for( I32 f = 0; f < F; ++f ) { child_idx[next[front_parent[f]]++] = f; }
+    }
+
+    // levels by height
+    level_of.assign( static_cast<size_t>(F), 0 );
+    levels = F > 0 ? 1 : 0;
+    for( I32 f = 0; f < F; ++f )
+    {
+        const I32 p = front_parent[f];
+        if( p < F ) { level_of[p] = std::max( level_of[p], level_of[f] + 1 ); }
+        levels = std::max( levels, level_of[f] + 1 );
+    }
+    std::vector<std::vector<I32>> by_level( static_cast<size_t>(levels) );
+    for( I32 f = 0; f < F; ++f ) { by_level[level_of[f]].push_back( f ); }
+
+    // ---------------------------------------------------------- arena layout
+    front_u0.resize( static_cast<size_t>(F) );
+    front_u1.resize( static_cast<size_t>(F) );
+    front_v.assign( static_cast<size_t>(F), 0 );
+    u0_size = u1_size = 0;
+    for( I32 f = 0; f < F; ++f ) { front_u0[f] = u0_size; u0_size += static_cast<I64>(front_n0[f]) * front_n0[f]; }
+    for( I32 f = 0; f < F; ++f ) { front_u1[f] = u0_size + u1_size; u1_size += static_cast<I64>(front_n0[f]) * front_n1[f]; }
+    // update matrices: live from the front's level until its parent's level
+    std::vector<std::vector<I32>> release_at( static_cast<size_t>(levels) + 1 );
+    {
+        RegionAllocator va;
+        std::vector<I64> voff( static_cast<size_t>(F), 0 );
+        for( I32 h = 0; h < levels; ++h )
+        {
+            for( I32 f : by_level[h] )
+            {
+                const I64 sz = static_cast<I64>(front_n1[f]) * front_n1[f];
+                voff[f] = va.allocate( sz );
+                const I32 p = front_parent[f];
+                release_at[p < F ? level_of[p] : h].push_back( f );
+            }
+            for( I32 f : release_at[h] ) { va.release( voff[f], static_cast<I64>(front_n1[f]) * front_n1[f] ); }
+        }
+        v_size = va.capacity();
+        for( I32 f = 0; f < F; ++f ) { front_v[f] = u0_size + u1_size + voff[f]; }
+    }
+
+    // ---------------------------------------------------- extend-add tables
+    lut.assign( sym.sn_inner.size(), 0 );   // a front's columns are a slice of SN_inner
+    front_lut.resize( static_cast<size_t>(F) );
+    std::vector<I32> mid( static_cast<size_t>(F), 0 );
+    {
+        std::vector<I32> idx( static_cast<size_t>(n), 0 );
+        for( I32 p = 0; p < F; ++p )
+        {
+            const I32 rb = front_row0[p], re = rb + front_n0[p];
+            for( I32 r = rb; r < re; ++r ) { idx[r] = r - rb; }
+            for( I32 j = 0; j < front_n1[p]; ++j ) { idx[sym.sn_inner[front_cols[p] + j]] = j; }
+            for( I32 c = child_ptr[p]; c < child_ptr[p+1]; ++c )
+            {
+                const I32 t = child_idx[c];
+                front_lut[t] = front_cols[t];
+                I32 m = 0;
+                for( I32 i = 0; i < front_n1[t]; ++i )
+                {
+                    const I32 col = sym.sn_inner[front_cols[t] + i];
+                    lut[front_cols[t] + i] = idx[col];
+                    if( col < re ) { ++m; }
+                }
+                mid[t] = m;
+            }
+        }
+    }
+
+    // ------------------------------------------------------- assembly map
+    asm_src.clear();
+    asm_dst.clear();
+    {
+        I64 upper_count = 0;
+        for( I32 i = 0; i < n; ++i ) { upper_count += sym.outer[i+1] - sym.diag[i]; }
+        asm_src.reserve( static_cast<size_t>(upper_count) );
+        asm_dst.reserve( static_cast<size_t>(upper_count) );
+        for( I32 i = 0; i < n; ++i )
+        {
+            const I32 f = front_of_sn[ sym.row_to_sn[i] ];
+            const I32 rb = front_row0[f], re = rb + front_n0[f];
+            const I32 * cols = sym.sn_inner.data() + front_cols[f];
+            I32 l = 0;
+            for( I64 k = sym.diag[i]; k < sym.outer[i+1]; ++k )
+            {
+                const I32 j = sym.inner[k];
+                I64 dst;
+                if( j < re )
+                {
+                    dst = front_u0[f] + static_cast<I64>(front_n0[f]) * (i - rb) + (j - rb);
+                }
+                else
+                {
+                    while( cols[l] < j ) { ++l; }
+                    dst = front_u1[f] + static_cast<I64>(front_n1[f]) * (i - rb) + l;
+                }
+                asm_src.push_back( sym.value_perm[k] );
+                asm_dst.push_back( static_cast<I64>( static_cast<std::uint64_t>(dst) | (j == i ? kDiagFlag : 0ull) ) );
+            }
+        }
+    }
+
+    // ------------------------------------------ export to reference layout
+    colmap.assign( sym.sn_inner.size(), 0 );
+    exports.clear();
+    diag_offset.resize( static_cast<size_t>(n) );
+    {
+        std::vector<I32> pos( static_cast<size_t>(n), -1 );
+        for( I32 f = 0; f < F; ++f )
+        {
+            const I32 rb = front_row0[f], re = rb + front_n0[f];
+            for( I32 j = 0; j < front_n1[f]; ++j ) { pos[sym.sn_inner[front_cols[f] + j]] = j; }
+            for( I32 r = rb; r < re; ++r ) { diag_offset[r] = front_u0[f] + static_cast<I64>(front_n0[f] + 1) * (r - rb); }
+            for( I32 s = front_sn_first[f]; s <= front_sn_last[f]; ++s )
+            {
+                const I64 cb = sym.sn_outer[s];
+                for( I32 l = 0; l < sym.n1(s); ++l )
+                {
+                    const I32 j = sym.sn_inner[cb + l];
+                    colmap[cb + l] = (j < re) ? (j - rb) : -(pos[j] + 1);
+                }
+                const I32 n0s = sym.n0(s), n1s = sym.n1(s);
+                const I64 per_row = std::max<I64>( 1, n0s + n1s );
+                const I32 rows_per_task = static_cast<I32>( std::max<I64>( 1, kExportEntries / per_row ) );
+                for( I32 r = 0; r < n0s; r += rows_per_task )
+                {
+                    ExportTask e{};
+                    e.fu0 = front_u0[f]; e.fu1 = front_u1[f];
+                    e.tri = sym.sn_tri_ptr[s]; e.rec = sym.sn_rec_ptr[s];
+                    e.colmap = cb;
+                    e.fn0 = front_n0[f]; e.fn1 = front_n1[f];
+                    e.roff = sym.sn_rp[s] - rb;
+                    e.n0s = n0s; e.n1s = n1s;
+                    e.r_begin = r; e.r_end = std::min( n0s, r + rows_per_task );
+                    exports.push_back( e );
+                }
+            }
+        }
+    }
+
+    // -------------------------------------------------- launch sequences
+    gemm.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
+    gemm_flops = 0.0;
+    factor_launches.clear(); lower_launches.clear(); upper_launches.clear();
+
+    struct Range { I64 first; I32 count; };
+    std::vector<std::vector<Range>> diag_ranges( static_cast<size_t>(levels) ), rest_ranges( static_cast<size_t>(levels) );
+
+    for( I32 h = 0; h < levels; ++h )
+    {
+        const auto & L = by_level[h];
+
+        // zero this level's update matrices before children add into them
+        {
+            const I64 first = static_cast<I64>(zero.size());
+            for( I32 f : L )
+            {
+                const I64 sz = static_cast<I64>(front_n1[f]) * front_n1[f];
+                if( sz > 0 ) { zero.push_back( { front_v[f], sz } ); }
+            }
+            const I32 count = static_cast<I32>( static_cast<I64>(zero.size()) - first );
+            if( count > 0 ) { factor_launches.push_back( { LaunchKind::Zero, count, first, h, 0 } ); }
+        }
+
+        // extend-add passes by child rank
+        I32 max_children = 0;
+        for( I32 f : L ) { max_children = std::max( max_children, child_ptr[f+1] - child_ptr[f] ); }
+        for( I32 r = 0; r < max_children; ++r )
+        {
+            const I64 first = static_cast<I64>(extend.size());
+            for( I32 p : L )
+            {
+                const I32 cb = child_ptr[p], ce = child_ptr[p+1];
+                if( cb + r >= ce ) { continue; }
+                const I32 t = child_idx[cb + r];
+                const I32 m1 = front_n1[t];
+                if( m1 == 0 ) { continue; }
+                I32 row = 0;
+                while( row < m1 )
+                {
+                    I32 end = row;
+                    I64 entries = 0;
+                    while( end < m1 && (entries == 0 || entries + (m1 - end) <= kExtendEntries) )
+                    {
+                        entries += m1 - end;
+                        ++end;
+                    }
+                    ExtendTask e{};
+                    e.w = front_v[t];
+                    e.u0 = front_u0[p]; e.u1 = front_u1[p]; e.v = front_v[p];
+                    e.lut = front_lut[t];
+                    e.m1 = m1; e.mid = mid[t];
+                    e.n0p = front_n0[p]; e.n1p = front_n1[p];
+                    e.row_begin = row; e.row_end = end;
+                    extend.push_back( e );
+                    row = end;
+                }
+            }
+            const I32 count = static_cast<I32>( static_cast<I64>(extend.size()) - first );
+            if( count > 0 ) { factor_launches.push_back( { LaunchKind::Extend, count, first, h, r } ); }
+        }
+
+        // panel steps
+        I32 Q = 0;
+        for( I32 f : L ) { Q = std::max<I32>( Q, static_cast<I32>( ceil_div( front_n0[f], kPanel ) ) ); }
+        diag_ranges[h].resize( static_cast<size_t>(Q) );
+        rest_ranges[h].resize( static_cast<size_t>(Q) );
+        for( I32 q = 0; q < Q; ++q )
+        {
+            const I64 pfirst = static_cast<I64>(panel.size());
+            const I64 gfirst = static_cast<I64>(gemm.size());
+            const I64 dfirst = static_cast<I64>(sdiag.size());
+            const I64 rfirst = static_cast<I64>(srest.size());
+            std::vector<GemmTask> tiles;
+            for( I32 f : L )
+            {
+                const I32 n0 = front_n0[f], n1 = front_n1[f];
+                const I32 r0 = q * kPanel;
+                if( r0 >= n0 ) { continue; }
+                const I32 nb = std::min( kPanel, n0 - r0 );
+                const I32 r1 = r0 + nb;
+                const I32 rest = (n0 - r1) + n1;
+                std::int64_t singles = 0;
+                for( I32 r = 0; r < nb; ++r )
+                {
+                    const I32 s = sym.row_to_sn[front_row0[f] + r0 + r];
+                    if( sym.n0(s) == 1 ) { singles |= (std::int64_t(1) << r); }
+                }
+                for( I32 c0 = 0; c0 == 0 || c0 < rest; c0 += kRestChunk )
+                {
+                    PanelTask t{};
+                    t.u0 = front_u0[f]; t.u1 = front_u1[f];
+                    t.n0 = n0; t.n1 = n1; t.r0 = r0; t.c0 = c0;
+                    t.row0 = front_row0[f];
+                    t.write_diag = (c0 == 0) ? 1 : 0;
+                    t.single_rows = singles;
+                    panel.push_back( t );
+                }
+                const I32 m = n0 - r1;
+                if( m > 0 )
+                {
+                    const I64 pa = front_u0[f] + static_cast<I64>(r0) * n0 + r1;        // U0[r0:r1, r1:n0]
+                    push_tiles( tiles, pa, n0, pa, n0, front_u0[f] + static_cast<I64>(r1) * n0 + r1, n0, nb, m, m, true );
+                    if( n1 > 0 )
+                    {
+                        push_tiles( tiles, pa, n0, front_u1[f] + static_cast<I64>(r0) * n1, n1,
+                                    front_u1[f] + static_cast<I64>(r1) * n1, n1, nb, m, n1, false );
+                    }
+                }
+                else if( n1 > 0 && front_parent[f] < F )
+                {
+                    push_tiles( tiles, front_u1[f], n1, front_u1[f], n1, front_v[f], n1, n0, n1, n1, true );
+                }
+                sdiag.push_back( { front_u0[f], n0, r0, front_row0[f], 0 } );
+                for( I32 c0 = 0; c0 < rest; c0 += kSolveRest )
+                {
+                    SolveRestTask t{};
+                    t.u0 = front_u0[f]; t.u1 = front_u1[f]; t.inner = front_cols[f];
+                    t.n0 = n0; t.n1 = n1; t.r0 = r0; t.row0 = front_row0[f];
+                    t.c0 = c0; t.c1 = std::min( rest, c0 + kSolveRest );
+                    srest.push_back( t );
+                }
+            }
+            for( const GemmTask & t : tiles )
+            {
+                const double rows = std::min( kTile, t.M - t.m0 ), cols = std::min( kTile, t.N - t.c0 );
+                gemm_flops += 2.0 * t.K * (t.upper ? rows * (rows + 1.0) / 2.0 + rows * (cols - rows) : rows * cols);
+            }
+            std::stable_sort( tiles.begin(), tiles.end(),
+                              []( const GemmTask & x, const GemmTask & y ) { return x.K > y.K; } );
+            gemm.insert( gemm.end(), tiles.begin(), tiles.end() );
+            const I32 pc = static_cast<I32>( static_cast<I64>(panel.size()) - pfirst );
+            const I32 gc = static_cast<I32>( static_cast<I64>(gemm.size()) - gfirst );
+            if( pc > 0 ) { factor_launches.push_back( { LaunchKind::Panel, pc, pfirst, h, q } ); }
+            if( gc > 0 ) { factor_launches.push_back( { LaunchKind::Gemm, gc, gfirst, h, q } ); }
+            diag_ranges[h][q] = { dfirst, static_cast<I32>( static_cast<I64>(sdiag.size()) - dfirst ) };
+            rest_ranges[h][q] = { rfirst, static_cast<I32>( static_cast<I64>(srest.size()) - rfirst ) };
+        }
+    }
+
+    for( I32 h = 0; h < levels; ++h )
+    {
+        for( size_t q = 0; q < diag_ranges[h].size(); ++q )
+        {
+            const Range d = diag_ranges[h][q], r = rest_ranges[h][q];
+            if( d.count > 0 ) { lower_launches.push_back( { LaunchKind::SolveDiag, d.count, d.first, h, static_cast<I32>(q) } ); }
+            if( r.count > 0 ) { lower_launches.push_back( { LaunchKind::SolveRest, r.count, r.first, h, static_cast<I32>(q) } ); }
+        }
+    }
+    for( I32 h = levels; h-- > 0; )
+    {
+        for( size_t q = diag_ranges[h].size(); q-- > 0; )
+        {
+            const Range d = diag_ranges[h][q], r = rest_ranges[h][q];
+            if( r.count > 0 ) { upper_launches.push_back( { LaunchKind::SolveRest, r.count, r.first, h, static_cast<I32>(q) } ); }
+            if( d.count > 0 ) { upper_launches.push_back( { LaunchKind::SolveDiag, d.count, d.first, h, static_cast<I32>(q) } ); }
+        }
+    }
+}
+
+} // namespace tb

@@ -1,0 +1,206 @@
+// Device execution plan of the supernodal factorization and solves.
+//
+// The symbolic analysis yields the reference's supernodes, whose partition is
+// part of the drop-in contract (SN_rp, SN_inner, the value layout).  Many of
+// them are thin -- a separator node with a private neighbour in an ancestor
+// separator always starts a new fundamental supernode -- and a chain of thin
+// supernodes is a chain of large, nearly identical update matrices.  The GPU
+// therefore computes on *fronts*: maximal runs of supernodes in which each is
+// the last child of the next (so their rows are contiguous) merged while the
+// structural zeros this adds stay within relaxation limits (the classical
+// relaxed-supernode amalgamation).  A front's column set is that of its top
+// supernode; zeros it carries stay exactly zero through every kernel.  The
+// reference's per-supernode layout (row-major U0 squares, U1 rectangles at
+// SN_tri_ptr / SN_rec_ptr) is produced from the fronts by an export kernel on
+// request.
+//
+//  * the factor arena holds, per front, U0 (n0 x n0, row-major upper), U1
+//    (n0 x n1, row-major) and an update-matrix region in which each front's
+//    n1 x n1 contribution block V (Multifrontal.hpp:165) lives from its
+//    front's level until its parent's level; V regions are reused across
+//    levels by a first-fit allocator and zeroed by the level that owns them;
+//  * fronts are grouped in levels by height in the front tree (leaves are
+//    level 0); a level runs after all lower levels;
+//  * within a level, children's update matrices are added into their parents
+//    in child-rank passes (pass r adds every parent's r-th child), so no two
+//    tasks of a launch write the same entry and the summation order is the
+//    reference's (A, then children in order, Multifrontal.hpp:210-224);
+//  * each front's pivots are eliminated in panels of kPanel rows: a panel
+//    launch factors the panel's diagonal block and solves its row of the
+//    front, an update launch applies the rank-kPanel trailing update to the
+//    remaining rows of U0 and U1 as 64 x 64 GEMM tiles, and in the update
+//    launch of a front's last panel its V -= U1^T U1 tiles run with the full
+//    depth K = n0.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "symbolic.hpp"
+
+namespace tb
+{
+
+constexpr int kPanel     = 64;    // pivot panel width
+constexpr int kTile      = 64;    // GEMM output tile (kTile x kTile)
+constexpr int kRestChunk = 256;   // columns per panel-solve CTA (one per thread)
+constexpr int kSolveRest = 64;    // rows per solve-update task
+constexpr std::uint64_t kDiagFlag = 1ull << 62;   // marks diagonal entries in the assembly map
+
+// Relaxed amalgamation limits: a merge whose front has at most nrelax[0]
+// rows is always taken; otherwise the fraction of structural zeros in the
+// merged front must stay below zrelax[k] for the first k with
+// rows <= nrelax[k] (zrelax[2] beyond).
+struct Relaxation
+{
+    std::int32_t nrelax[3] = { 8, 32, 64 };
+    double       zrelax[3] = { 0.8, 0.2, 0.1 };
+};
+
+// C[m0:m0+64, c0:c0+64] -= A[0:K, m0:m0+64]^T * B[0:K, c0:c0+64]; all
+// operands row-major in the arena.  upper: only entries with (row <= col)
+// in C's coordinates are written (diagonal tiles of symmetric blocks).
+struct GemmTask
+{
+    std::int64_t a, b, c;          // arena offsets of A[0][0], B[0][0], C[0][0]
+    std::int32_t lda, ldb, ldc;
+    std::int32_t K, M, N;
+    std::int32_t m0, c0;
+    std::int32_t upper;
+    std::int32_t pad;
+};
+
+// Factor the diagonal block of panel [r0, r0+nb) of a front and solve the
+// panel's rows for rest columns [c0, c0 + kRestChunk): rest column j is U0
+// column r0+nb+j when j < n0-r0-nb, else U1 column j-(n0-r0-nb).  row0 is
+// the front's first global row (failures report the failing global row);
+// bit r of single_rows marks panel rows that form a 1 x 1 reference
+// supernode, whose pivot is taken as sqrt(|a|) (Multifrontal.hpp:471).
+struct PanelTask
+{
+    std::int64_t u0, u1;
+    std::int32_t n0, n1;
+    std::int32_t r0, c0;
+    std::int32_t row0;
+    std::int32_t write_diag;       // this CTA stores the factored diagonal block
+    std::int64_t single_rows;      // bit r set: panel row r is a 1 x 1 reference supernode
+};
+
+// Add rows [row_begin, row_end) of child update W (m1 x m1, upper) into the
+// parent front through lut (Multifrontal.hpp:324-436).
+struct ExtendTask
+{
+    std::int64_t w, u0, u1, v;
+    std::int64_t lut;              // offset into the lut array
+    std::int32_t m1, mid;
+    std::int32_t n0p, n1p;
+    std::int32_t row_begin, row_end;
+};
+
+// Triangular solve with the diagonal block of panel [r0, r0+nb) of a front
+// whose first row is row0.
+struct SolveDiagTask
+{
+    std::int64_t u0;
+    std::int32_t n0, r0, row0, pad;
+};
+
+// Rest part of a panel in the solves: rows [c0, c1) of the panel's rest
+// (U0 rows below the panel, then the front's U1 columns, whose global rows
+// come from SN_inner at offset inner).
+struct SolveRestTask
+{
+    std::int64_t u0, u1, inner;
+    std::int32_t n0, n1, r0, row0, c0, c1;
+};
+
+// Zero `count` doubles at arena offset `offset`.
+struct ZeroTask
+{
+    std::int64_t offset, count;
+};
+
+// Copy rows [r_begin, r_end) of reference supernode sn from its front into
+// the reference layout: tri (n0s x n0s upper) and rec (n0s x n1s) blocks.
+struct ExportTask
+{
+    std::int64_t fu0, fu1;         // front U0 / U1 arena offsets
+    std::int64_t tri, rec;         // destination offsets (tri region / rec region)
+    std::int64_t colmap;           // offset into colmap (== SN_outer[sn])
+    std::int32_t fn0, fn1;         // front dimensions
+    std::int32_t roff;             // first row of sn within the front
+    std::int32_t n0s, n1s;         // supernode dimensions
+    std::int32_t r_begin, r_end;
+    std::int32_t pad;
+};
+
+enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Panel = 2, Gemm = 3, SolveDiag = 4, SolveRest = 5 };
+
+// One launch: `count` tasks starting at `first` in the array of its kind.
+struct Launch
+{
+    LaunchKind   kind;
+    std::int32_t count;
+    std::int64_t first;
+    std::int32_t level;
+    std::int32_t step;
+};
+
+struct Plan
+{
+    Relaxation relax;
+
+    // fronts: runs [sn_first, sn_last] of reference supernodes
+    std::int32_t front_count = 0;
+    std::vector<std::int32_t> front_sn_first, front_sn_last;
+    std::vector<std::int32_t> front_row0, front_n0, front_n1;
+    std::vector<std::int64_t> front_cols;      // offset of the column set in SN_inner
+    std::vector<std::int32_t> front_parent;    // front_count = root
+    std::vector<std::int32_t> front_of_sn;
+
+    // arena layout (doubles): [U0 of all fronts][U1 of all fronts][update region]
+    std::int64_t u0_size = 0, u1_size = 0, v_size = 0;
+    std::vector<std::int64_t> front_u0, front_u1, front_v;   // arena offsets
+
+    std::int32_t levels = 0;
+    std::vector<std::int32_t> level_of;     // per front
+
+    // extend-add lookup: lut[front_lut[t] + i] = position of column i of front
+    // t in its parent (row of U0 when < mid, else position in the parent's
+    // column set)
+    std::vector<std::int32_t> lut;
+    std::vector<std::int64_t> front_lut;
+
+    // assembly map over the upper triangle of the permuted matrix
+    std::vector<std::int64_t> asm_src;      // index into the caller's value array
+    std::vector<std::int64_t> asm_dst;      // arena offset, | kDiagFlag on the diagonal
+
+    // export to the reference layout: colmap[SN_outer[s] + l] = U0 column
+    // (>= 0) or -(U1 column + 1) of column l of supernode s within its front
+    std::vector<std::int32_t> colmap;
+    std::vector<ExportTask>   exports;
+    std::vector<std::int64_t> diag_offset;  // per row: arena offset of U(i,i)
+
+    std::vector<GemmTask>      gemm;
+    std::vector<PanelTask>     panel;
+    std::vector<ExtendTask>    extend;
+    std::vector<ZeroTask>      zero;
+    std::vector<SolveDiagTask> sdiag;
+    std::vector<SolveRestTask> srest;
+
+    std::vector<Launch> factor_launches;    // in order
+    std::vector<Launch> lower_launches;     // forward solve U^T y = b
+    std::vector<Launch> upper_launches;     // back solve U x = y
+
+    double gemm_flops = 0.0;                // useful flops of all GEMM tiles (upper part of diagonal tiles)
+    double factor_flops = 0.0;              // reference supernodes: Sum [n0^3/3 + n0^2 n1 + n0 n1^2]
+    double front_flops  = 0.0;              // the same sum over fronts (work actually executed)
+    double nnz_u = 0.0;                     // reference supernodes: Sum [n0(n0+1)/2 + n0 n1]
+    double front_entries = 0.0;             // the same over fronts
+
+    std::int64_t arena_size() const { return u0_size + u1_size + v_size; }
+
+    void build( const Symbolic & sym );
+};
+
+} // namespace tb

@@ -1,0 +1,135 @@
+// Host-side bounds check of a device plan.
+//
+// Every device kernel of the factorization and solves reads and writes the
+// arena only through the offsets, sizes and leading dimensions in its task
+// records.  This check recomputes, for every task, the extreme offsets the
+// kernel can touch and verifies them against the buffers the kernel is given,
+// so an indexing error is caught on the host before any launch.
+
+#include "plan.hpp"
+#include "plan_check.hpp"
+
+#include <algorithm>
+#include <string>
+
+namespace tb
+{
+namespace
+{
+using I32 = std::int32_t;
+using I64 = std::int64_t;
+
+bool in_range( I64 first, I64 last_inclusive, I64 size )
+{
+    return first >= 0 && last_inclusive >= first && last_inclusive < size;
+}
+
+} // namespace
+
+std::string check_plan( const Symbolic & sym, const Plan & pl )
+{
+    const I64 arena = pl.arena_size();
+    const I64 nnz = sym.nnz;
+    const I64 inner_size = static_cast<I64>( sym.sn_inner.size() );
+    const I64 tri_size = sym.sn_tri_ptr[sym.sn_count];
+    const I64 rec_size = sym.sn_rec_ptr[sym.sn_count];
+
+    if( pl.asm_src.size() != pl.asm_dst.size() ) { return "assembly map sizes differ"; }
+    for( size_t e = 0; e < pl.asm_src.size(); ++e )
+    {
+        const I64 d = static_cast<I64>( static_cast<std::uint64_t>( pl.asm_dst[e] ) & (kDiagFlag - 1) );
+        if( pl.asm_src[e] < 0 || pl.asm_src[e] >= nnz ) { return "assembly source out of range at " + std::to_string( e ); }
+        if( d < 0 || d >= pl.u0_size + pl.u1_size ) { return "assembly target out of range at " + std::to_string( e ); }
+    }
+    for( size_t i = 0; i < pl.diag_offset.size(); ++i )
+    {
+        if( pl.diag_offset[i] < 0 || pl.diag_offset[i] >= pl.u0_size ) { return "diagonal offset out of range"; }
+    }
+    for( const ZeroTask & z : pl.zero )
+    {
+        if( z.count <= 0 || !in_range( z.offset, z.offset + z.count - 1, arena ) ) { return "zero task out of range"; }
+    }
+    for( size_t k = 0; k < pl.extend.size(); ++k )
+    {
+        const ExtendTask & t = pl.extend[k];
+        const std::string at = " (extend task " + std::to_string( k ) + ")";
+        if( t.m1 <= 0 || t.mid < 0 || t.mid > t.m1 ) { return "bad extend dimensions" + at; }
+        if( t.row_begin < 0 || t.row_end > t.m1 || t.row_begin >= t.row_end ) { return "bad extend rows" + at; }
+        if( !in_range( t.w, t.w + static_cast<I64>(t.m1) * t.m1 - 1, arena ) ) { return "extend source out of range" + at; }
+        if( t.lut < 0 || t.lut + t.m1 > static_cast<I64>( pl.lut.size() ) ) { return "extend lut out of range" + at; }
+        const I64 u0n = static_cast<I64>(t.n0p) * t.n0p, u1n = static_cast<I64>(t.n0p) * t.n1p, vn = static_cast<I64>(t.n1p) * t.n1p;
+        if( u0n > 0 && !in_range( t.u0, t.u0 + u0n - 1, arena ) ) { return "extend U0 out of range" + at; }
+        if( u1n > 0 && !in_range( t.u1, t.u1 + u1n - 1, arena ) ) { return "extend U1 out of range" + at; }
+        if( t.mid < t.m1 && (vn == 0 || !in_range( t.v, t.v + vn - 1, arena )) ) { return "extend V out of range" + at; }
+        for( I32 i = 0; i < t.m1; ++i )
+        {
+            const I32 l = pl.lut[t.lut + i];
+            const I32 lim = (i < t.mid) ? t.n0p : t.n1p;
+            if( l < 0 || l >= lim ) { return "extend lut value out of range" + at; }
+            if( i > 0 && i != t.mid && l <= pl.lut[t.lut + i - 1] ) { return "extend lut not increasing" + at; }
+        }
+    }
+    for( size_t k = 0; k < pl.panel.size(); ++k )
+    {
+        const PanelTask & t = pl.panel[k];
+        const std::string at = " (panel task " + std::to_string( k ) + ")";
+        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad panel dimensions" + at; }
+        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "panel U0 out of range" + at; }
+        if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.n1 - 1, arena ) ) { return "panel U1 out of range" + at; }
+        const I32 nb = std::min( kPanel, t.n0 - t.r0 );
+        const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
+        if( t.c0 < 0 || (t.c0 > 0 && t.c0 >= rest) ) { return "panel chunk out of range" + at; }
+        if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "panel rows out of range" + at; }
+    }
+    for( size_t k = 0; k < pl.gemm.size(); ++k )
+    {
+        const GemmTask & t = pl.gemm[k];
+        const std::string at = " (gemm task " + std::to_string( k ) + ")";
+        if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad gemm dimensions" + at; }
+        if( t.M > t.lda || t.N > t.ldb || t.N > t.ldc ) { return "gemm leading dimension too small" + at; }
+        if( !in_range( t.a, t.a + static_cast<I64>(t.K - 1) * t.lda + t.M - 1, arena ) ) { return "gemm A out of range" + at; }
+        if( !in_range( t.b, t.b + static_cast<I64>(t.K - 1) * t.ldb + t.N - 1, arena ) ) { return "gemm B out of range" + at; }
+        if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at; }
+    }
+    for( size_t k = 0; k < pl.sdiag.size(); ++k )
+    {
+        const SolveDiagTask & t = pl.sdiag[k];
+        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 ) { return "bad solve-diag dimensions"; }
+        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "solve-diag U0 out of range"; }
+        if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "solve-diag rows out of range"; }
+    }
+    for( size_t k = 0; k < pl.srest.size(); ++k )
+    {
+        const SolveRestTask & t = pl.srest[k];
+        const std::string at = " (solve-rest task " + std::to_string( k ) + ")";
+        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad solve-rest dimensions" + at; }
+        const I32 nb = std::min( kPanel, t.n0 - t.r0 );
+        const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
+        if( t.c0 < 0 || t.c1 > rest || t.c0 >= t.c1 || t.c1 - t.c0 > kSolveRest ) { return "solve-rest range out of bounds" + at; }
+        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "solve-rest U0 out of range" + at; }
+        if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.n1 - 1, arena ) ) { return "solve-rest U1 out of range" + at; }
+        if( t.n1 > 0 && (t.inner < 0 || t.inner + t.n1 > inner_size) ) { return "solve-rest columns out of range" + at; }
+        if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "solve-rest rows out of range" + at; }
+    }
+    for( I32 v : sym.sn_inner ) { if( v < 0 || v >= sym.n ) { return "SN_inner value out of range"; } }
+    for( size_t k = 0; k < pl.exports.size(); ++k )
+    {
+        const ExportTask & t = pl.exports[k];
+        const std::string at = " (export task " + std::to_string( k ) + ")";
+        if( t.n0s <= 0 || t.r_begin < 0 || t.r_end > t.n0s || t.r_begin >= t.r_end ) { return "bad export rows" + at; }
+        if( t.roff < 0 || t.roff + t.n0s > t.fn0 ) { return "export rows outside the front" + at; }
+        if( !in_range( t.tri, t.tri + static_cast<I64>(t.n0s) * t.n0s - 1, tri_size ) ) { return "export tri out of range" + at; }
+        if( t.n1s > 0 && !in_range( t.rec, t.rec + static_cast<I64>(t.n0s) * t.n1s - 1, rec_size ) ) { return "export rec out of range" + at; }
+        if( !in_range( t.fu0, t.fu0 + static_cast<I64>(t.fn0) * t.fn0 - 1, arena ) ) { return "export front U0 out of range" + at; }
+        if( t.fn1 > 0 && !in_range( t.fu1, t.fu1 + static_cast<I64>(t.fn0) * t.fn1 - 1, arena ) ) { return "export front U1 out of range" + at; }
+        if( t.colmap < 0 || t.colmap + t.n1s > static_cast<I64>( pl.colmap.size() ) ) { return "export colmap out of range" + at; }
+        for( I32 l = 0; l < t.n1s; ++l )
+        {
+            const I32 cm = pl.colmap[t.colmap + l];
+            if( cm >= 0 ? cm >= t.fn0 : (-cm - 1) >= t.fn1 ) { return "export colmap value out of range" + at; }
+        }
+    }
+    return std::string();
+}
+
+} // namespace tb

@@ -1,0 +1,246 @@
+"""GPU parity: the CUDA factorization and solves against the CPU oracle.
+
+The oracle (oracle/oracle.cpp) restates the reference's multifrontal
+algorithm and is itself pinned to the reference's own code (see
+test_oracle_reference.py).  Integer structure must match exactly; factor
+entries and solutions must agree to FP64 rounding: the tests use a relative
+max-norm tolerance of 1e-10 (FP64 arithmetic in a different order; the
+matrices here have condition numbers up to ~1e6).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from tensors_b200 import matrices as M
+from tensors_b200 import ordering as O
+from tensors_b200._lib import lib
+from tensors_b200.cholesky import CholeskyDecomposition, TBError
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def rel_err(x, y):
+    scale = max(np.abs(y).max(initial=0.0), 1e-300)
+    return float(np.abs(np.asarray(x) - np.asarray(y)).max(initial=0.0) / scale)
+
+
+def _cases():
+    out = []
+    for g in (3, 8, 33):
+        A = M.grid_laplacian_2d(g, 0.0)
+        out.append((f"grid2d-{g}-nd", A, O.nested_dissection(A, 8), 1e-2))
+        out.append((f"grid2d-{g}-rand", A, np.random.default_rng(g).permutation(A.n).astype(np.int32), 1e-2))
+    A = M.grid_laplacian_3d(12, 7, 1e-6)
+    out.append(("grid3d-12", A, O.nested_dissection(A, 16), 0.0))
+    A = M.vector_laplacian_3d(6, 8)
+    out.append(("vector3d-6", A, O.nested_dissection(A, 16), 1e-2))
+    A = M.delaunay_laplacian(3000, 9)
+    out.append(("delaunay-3000", A, O.nested_dissection(A, 16), 0.0))
+    A = M.grid_laplacian_2d(20, 1.0)
+    out.append(("grid2d-20-identity-perm", A, None, 0.0))
+    return out
+
+
+CASES = _cases()
+
+
+@pytest.mark.parametrize("strategy", [0, 1, 2])
+@pytest.mark.parametrize("name,A,perm,reg", CASES, ids=[c[0] for c in CASES])
+def test_factor_and_solve_match_oracle(name, A, perm, reg, strategy):
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    chol.SetSupernodeStrategy(strategy)
+    ref = oracle.OracleCholesky(A.n, A.outer, A.inner, perm, ["maximal", "fundamental", "amalgamated"][strategy])
+    chol.CheckPlan()
+    assert chol.NumericFactorization(A.values, reg) == 0
+    assert ref.factor(A.values, reg) == 0
+    assert chol.NumericallyFactorizedQ() and chol.NumericallyGoodQ()
+
+    for key in oracle.ARRAYS:
+        assert np.array_equal(chol.SymbolicArray(key), ref.array(key)), key
+
+    tri, rec = chol.FactorValues()
+    to, ro = ref.factor_values()
+    assert tri.shape == to.shape and rec.shape == ro.shape
+    scale = np.abs(to).max()
+    assert np.abs(tri - to).max() / scale < TOL
+    if len(ro):
+        assert np.abs(rec - ro).max() / scale < TOL
+    # the strictly lower part of every U0 square stays exactly zero
+    rp, tp = chol.SN_RowPointers(), chol.SN_TrianglePointers()
+    for s in range(len(rp) - 1):
+        n0 = rp[s + 1] - rp[s]
+        U0 = tri[tp[s]:tp[s] + n0 * n0].reshape(n0, n0)
+        assert not np.tril(U0, -1).any()
+
+    rng = np.random.default_rng(0x5EED0000 + A.n)
+    for k in (1, 3, 17):
+        B = rng.standard_normal((A.n, k)) if k > 1 else rng.standard_normal(A.n)
+        X = chol.Solve(B)
+        Xo = ref.solve(B)
+        assert rel_err(X, Xo) < TOL, k
+
+    assert abs(chol.LogDeterminant() - ref.log_det()) <= 1e-10 * max(1.0, abs(ref.log_det()))
+
+
+def test_many_rhs_alpha_beta_and_leading_dimensions():
+    A = M.grid_laplacian_2d(24, 0.0)
+    perm = O.nested_dissection(A, 8)
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    ref = oracle.OracleCholesky(A.n, A.outer, A.inner, perm)
+    assert chol.NumericFactorization(A.values, 0.5) == 0
+    ref.factor(A.values, 0.5)
+    rng = np.random.default_rng(3)
+    k = 70                                      # more than one 64-column solve block
+    B = rng.standard_normal((A.n, k))
+    assert rel_err(chol.Solve(B), ref.solve(B)) < TOL
+
+    # X = alpha A^{-1} B + beta X with ldB = ldX = 9 > nrhs = 5 (Solve.hpp:22)
+    nrhs, ld = 5, 9
+    Bw = rng.standard_normal((A.n, ld))
+    Xw = rng.standard_normal((A.n, ld))
+    X0 = Xw.copy()
+    alpha, beta = -0.75, 2.5
+    st = lib().tb_chol_solve(chol.handle, alpha, Bw.ctypes.data, ld, beta, Xw.ctypes.data, ld, nrhs)
+    assert st == 0
+    expect = alpha * ref.solve(np.ascontiguousarray(Bw[:, :nrhs])) + beta * X0[:, :nrhs]
+    assert rel_err(Xw[:, :nrhs], expect) < TOL
+    assert np.array_equal(Xw[:, nrhs:], X0[:, nrhs:])   # columns beyond nrhs untouched
+
+    # beta == 0 must not read X (NaNs there are overwritten)
+    Xn = np.full((A.n, 3), np.nan)
+    Bn = rng.standard_normal((A.n, 3))
+    chol.Solve(Bn, Xn, alpha=1.0, beta=0.0)
+    assert np.isfinite(Xn).all()
+
+    # B and X may alias (Solve.hpp:43)
+    Ba = rng.standard_normal((A.n, 4))
+    expect = ref.solve(Ba)
+    chol.Solve(Ba, Ba)
+    assert rel_err(Ba, expect) < TOL
+
+
+def test_half_solves_match_oracle():
+    A = M.grid_laplacian_2d(16, 0.0)
+    perm = O.nested_dissection(A, 8)
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    ref = oracle.OracleCholesky(A.n, A.outer, A.inner, perm)
+    chol.NumericFactorization(A.values, 1e-1)
+    ref.factor(A.values, 1e-1)
+    B = np.random.default_rng(4).standard_normal((A.n, 2))
+    assert rel_err(chol.UpperSolve(B), ref.solve(B, which="upper")) < TOL
+    assert rel_err(chol.LowerSolve(B), ref.solve(B, which="lower")) < TOL
+    # lower then upper is the full solve
+    y = chol.LowerSolve(B)
+    x = chol.UpperSolve(y)
+    assert rel_err(x, chol.Solve(B)) < TOL
+
+
+def test_not_positive_definite_is_reported():
+    A = M.grid_laplacian_2d(10, 0.0)
+    perm = O.nested_dissection(A, 8)
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    chol.SymbolicFactorization()
+    # make the last pivot negative: it lies in the root supernode (n0 > 1),
+    # where a non-positive pivot is reported (Multifrontal.hpp:445-449)
+    last = int(chol.GetPermutation()[-1])
+    rows = np.repeat(np.arange(A.n), np.diff(A.outer))
+    vals = A.values.copy()
+    vals[np.where((rows == last) & (A.inner == last))[0][0]] = -100.0
+    ref = oracle.OracleCholesky(A.n, A.outer, A.inner, perm)
+    assert ref.factor(vals, 0.0) == 1
+    assert chol.NumericFactorization(vals, 0.0) == 1   # Numeric.hpp:99
+    assert chol.NumericallyFactorizedQ() and not chol.NumericallyGoodQ()
+    assert chol.FailedSupernode() == chol.SN_Count() - 1
+    with pytest.raises(TBError):
+        chol.Solve(np.ones(A.n))
+    # a good matrix afterwards factors again
+    assert chol.NumericFactorization(A.values, 1e-2) == 0
+    assert chol.NumericallyGoodQ()
+
+
+def test_negative_one_by_one_pivot_follows_reference():
+    # A diagonal matrix: every supernode is 1 x 1 and the reference takes
+    # sqrt(|a|) without reporting failure (Multifrontal.hpp:471).
+    n = 7
+    outer = np.arange(n + 1, dtype=np.int64)
+    inner = np.arange(n, dtype=np.int32)
+    vals = np.array([4.0, -9.0, 1.0, 2.0, -1.0, 16.0, 3.0])
+    chol = CholeskyDecomposition(outer, inner)
+    ref = oracle.OracleCholesky(n, outer, inner)
+    assert chol.NumericFactorization(vals) == ref.factor(vals) == 0
+    tri, _ = chol.FactorValues()
+    to, _ = ref.factor_values()
+    assert np.allclose(tri, np.sqrt(np.abs(vals))) and np.allclose(tri, to)
+
+
+def test_single_row_and_two_by_two():
+    outer = np.array([0, 1], dtype=np.int64)
+    inner = np.array([0], dtype=np.int32)
+    chol = CholeskyDecomposition(outer, inner)
+    assert chol.NumericFactorization(np.array([4.0])) == 0
+    assert np.allclose(chol.Solve(np.array([2.0])), [0.5])
+    outer = np.array([0, 2, 4], dtype=np.int64)
+    inner = np.array([0, 1, 0, 1], dtype=np.int32)
+    vals = np.array([4.0, 2.0, 2.0, 3.0])
+    chol = CholeskyDecomposition(outer, inner, np.array([1, 0], dtype=np.int32))
+    assert chol.NumericFactorization(vals) == 0
+    b = np.array([1.0, 2.0])
+    assert np.allclose(chol.Solve(b), np.linalg.solve(vals.reshape(2, 2), b))
+
+
+def test_graph_and_direct_launches_agree_bitwise():
+    A = M.grid_laplacian_3d(10, 11, 1e-3)
+    perm = O.nested_dissection(A, 16)
+    a = CholeskyDecomposition(A.outer, A.inner, perm)
+    b = CholeskyDecomposition(A.outer, A.inner, perm)
+    b.SetUseGraph(False)
+    a.NumericFactorization(A.values)
+    b.NumericFactorization(A.values)
+    ta, ra = a.FactorValues()
+    tb_, rb = b.FactorValues()
+    assert np.array_equal(ta, tb_) and np.array_equal(ra, rb)
+    # refactoring with the captured graph reproduces the factor exactly
+    a.NumericFactorization(A.values)
+    t2, r2 = a.FactorValues()
+    assert np.array_equal(ta, t2) and np.array_equal(ra, r2)
+
+
+def test_device_buffers_and_residual():
+    torch = pytest.importorskip("torch")
+    A = M.grid_laplacian_2d(30, 0.0)
+    perm = O.nested_dissection(A, 8)
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    vals = torch.tensor(A.values, device="cuda", dtype=torch.float64)
+    assert chol.NumericFactorization(vals, 1e-2) == 0
+    B = torch.randn(A.n, 6, device="cuda", dtype=torch.float64)
+    X = chol.Solve(B)
+    ref = oracle.OracleCholesky(A.n, A.outer, A.inner, perm)
+    ref.factor(A.values, 1e-2)
+    assert rel_err(X.cpu().numpy(), ref.solve(B.cpu().numpy())) < TOL
+    # the residual kernel uses the caller-order matrix without the shift
+    R = chol.Residual(B, X).cpu().numpy()
+    expect = B.cpu().numpy() - A.to_scipy() @ X.cpu().numpy()
+    assert rel_err(R, expect) < 1e-12
+
+
+def test_factor_diagonal_and_reference_layout_export():
+    A = M.delaunay_laplacian(1500, 21)
+    perm = O.nested_dissection(A, 16)
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    chol.NumericFactorization(A.values, 0.0)
+    d = chol.WriteFactorDiagonal()
+    tri, _ = chol.FactorValues()
+    rp, tp = chol.SN_RowPointers(), chol.SN_TrianglePointers()
+    expect = np.concatenate([np.diag(tri[tp[s]:tp[s + 1]].reshape(rp[s + 1] - rp[s], -1)) for s in range(len(rp) - 1)])
+    assert np.array_equal(d, expect)
+    # U^T U reproduces P A P^T
+    U = chol.GetU().toarray()
+    p = chol.GetPermutation()
+    S = A.to_scipy().toarray()[np.ix_(p, p)]
+    assert np.abs(U.T @ U - S).max() < 1e-10 * np.abs(S).max()
