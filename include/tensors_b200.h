@@ -169,7 +169,8 @@ int tb_chol_set_stream( tb_chol * h, void * stream );
 int tb_chol_set_graph( tb_chol * h, int32_t enabled );
 /* Per-kernel timing: when enabled, factorizations run as direct launches
  * bracketed by CUDA events and tb_chol_kernel_profile reports, per launch
- * kind (0 zero, 1 extend-add, 2 panel, 3 GEMM tiles, 7 clear + assembly),
+ * kind (0 zero, 1 extend-add, 2 panel trsm, 3 GEMM tiles, 6 panel potrf,
+ * 7 clear + assembly),
  * the milliseconds and launches of the last factorization and the
  * algorithmic flops of the GEMM tiles (8 entries each). */
 int tb_chol_set_profiling( tb_chol * h, int32_t enabled );

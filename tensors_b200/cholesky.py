@@ -330,7 +330,7 @@ class CholeskyDecomposition:
         ln = np.zeros(8, dtype=np.int64)
         fl = np.zeros(8)
         _check(lib().tb_chol_kernel_profile(self._h, ms.ctypes.data, ln.ctypes.data, fl.ctypes.data))
-        names = {0: "zero", 1: "extend", 2: "panel", 3: "gemm", 7: "assemble"}
+        names = {0: "zero", 1: "extend", 2: "trsm", 3: "gemm", 6: "potrf", 7: "assemble"}
         return {names[k]: {"ms": float(ms[k]), "launches": int(ln[k]), "flops": float(fl[k])} for k in names}
 
     def LaunchCounts(self):

@@ -117,7 +117,7 @@ struct tb_chol
     DeviceArray<tb::ExportTask>     exports;
     DeviceArray<double>             exported;    // reference-layout factor (tri then rec)
     DeviceArray<tb::GemmTask>       gemm;
-    DeviceArray<tb::PanelTask>      panel;
+    DeviceArray<tb::PanelTask>      potrf, panel;
     DeviceArray<tb::ExtendTask>     extend;
     DeviceArray<tb::SolveDiagTask>  sdiag;
     DeviceArray<tb::SolveRestTask>  srest;
@@ -230,6 +230,7 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->p.upload( s.p, st_ ) );
     TB_TRY( h->p_inv.upload( s.p_inv, st_ ) );
     TB_TRY( h->gemm.upload( pl.gemm, st_ ) );
+    TB_TRY( h->potrf.upload( pl.potrf, st_ ) );
     TB_TRY( h->panel.upload( pl.panel, st_ ) );
     TB_TRY( h->extend.upload( pl.extend, st_ ) );
     TB_TRY( h->sdiag.upload( pl.sdiag, st_ ) );
@@ -279,7 +280,8 @@ std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * k
         {
             case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
             case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
-            case tb::LaunchKind::Panel:  tb::launch_panel( h->panel.ptr + L.first, L.count, A, h->status.ptr, st ); break;
+            case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, st ); break;
+            case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
             case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
             default: break;
         }
@@ -762,7 +764,7 @@ int tb_chol_device_bytes( tb_chol * h, std::int64_t * out )
     std::int64_t b = 0;
     b += h->arena.size * 8 + h->asm_src.size * 8 + h->asm_dst.size * 8 + h->diag_off.size * 8;
     b += (h->lut.size + h->sn_inner.size + h->p.size + h->p_inv.size + h->a_inner.size) * 4;
-    b += h->gemm.size * (std::int64_t)sizeof(tb::GemmTask) + h->panel.size * (std::int64_t)sizeof(tb::PanelTask);
+    b += h->gemm.size * (std::int64_t)sizeof(tb::GemmTask) + (h->panel.size + h->potrf.size) * (std::int64_t)sizeof(tb::PanelTask);
     b += h->extend.size * (std::int64_t)sizeof(tb::ExtendTask) + h->sdiag.size * (std::int64_t)sizeof(tb::SolveDiagTask);
     b += h->srest.size * (std::int64_t)sizeof(tb::SolveRestTask) + h->a_outer.size * 8;
     b += h->zero.size * (std::int64_t)sizeof(tb::ZeroTask) + h->exports.size * (std::int64_t)sizeof(tb::ExportTask);

@@ -116,33 +116,25 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
 }
 
 // ------------------------------------------------------------------ panel
-// Cholesky of the panel's nb x nb diagonal block in shared memory (every CTA
-// of the panel repeats it; the write_diag CTA stores it), then each thread
-// solves one rest column D^T x = u with the column held in registers
-// (potrf + trsm of FactorizeSupernode, Multifrontal.hpp:438-475).  A row
-// that forms a 1 x 1 reference supernode takes sqrt(|a|) as the reference
-// does (:471) and never reports failure.
-__global__ __launch_bounds__(kPanelThreads, 1) void panel_kernel( const PanelTask * __restrict__ tasks,
+// Cholesky of a panel's nb x nb diagonal block, in shared memory and then
+// in place (LAPACK potrf of FactorizeSupernode, Multifrontal.hpp:438-449).
+// A row that forms a 1 x 1 reference supernode takes sqrt(|a|) as the
+// reference does (:471) and never reports failure.
+__global__ __launch_bounds__(kPanelThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
                                                                double * __restrict__ arena, int * __restrict__ status )
 {
     const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    const int r1 = t.r0 + nb;
-    const int m = t.n0 - r1;
-    const int rest = m + t.n1;
     __shared__ double D[kPanel][kPanel + 1];
-    __shared__ double inv_d[kPanel];
+    __shared__ double inv_d;
     __shared__ int fail;
 
     double * U0 = arena + t.u0;
-    double * U1 = arena + t.u1;
-    for( int idx = tid; idx < kPanel * kPanel; idx += kPanelThreads )
+    for( int idx = tid; idx < nb * nb; idx += kPanelThreads )
     {
-        const int r = idx / kPanel, c = idx % kPanel;
-        double v = (r == c) ? 1.0 : 0.0;
-        if( r < nb && c < nb && c >= r ) { v = U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c]; }
-        D[r][c] = v;
+        const int r = idx / nb, c = idx % nb;
+        D[r][c] = (c >= r) ? U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] : 0.0;
     }
     if( tid == 0 ) { fail = -1; }
     __syncthreads();
@@ -156,10 +148,10 @@ __global__ __launch_bounds__(kPanelThreads, 1) void panel_kernel( const PanelTas
             else if( !(d > 0.0) && fail < 0 ) { fail = j; }
             d = sqrt( d );
             D[j][j] = d;
-            inv_d[j] = 1.0 / d;
+            inv_d = 1.0 / d;
         }
         __syncthreads();
-        for( int c = j + 1 + tid; c < nb; c += kPanelThreads ) { D[j][c] *= inv_d[j]; }
+        for( int c = j + 1 + tid; c < nb; c += kPanelThreads ) { D[j][c] *= inv_d; }
         __syncthreads();
         const int w = nb - j - 1;
         for( int idx = tid; idx < w * w; idx += kPanelThreads )
@@ -169,22 +161,45 @@ __global__ __launch_bounds__(kPanelThreads, 1) void panel_kernel( const PanelTas
         }
         __syncthreads();
     }
-    for( int r = nb + tid; r < kPanel; r += kPanelThreads ) { inv_d[r] = 1.0; }
-    __syncthreads();
-
-    if( t.write_diag )
+    for( int idx = tid; idx < nb * nb; idx += kPanelThreads )
     {
-        for( int idx = tid; idx < nb * nb; idx += kPanelThreads )
-        {
-            const int r = idx / nb, c = idx % nb;
-            if( c >= r ) { U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] = D[r][c]; }
-        }
-        if( tid == 0 && fail >= 0 )
-        {
-            atomicOr( status, 1 );
-            atomicMin( status + 1, t.row0 + t.r0 + fail );
-        }
+        const int r = idx / nb, c = idx % nb;
+        if( c >= r ) { U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] = D[r][c]; }
     }
+    if( tid == 0 && fail >= 0 )
+    {
+        atomicOr( status, 1 );
+        atomicMin( status + 1, t.row0 + t.r0 + fail );
+    }
+}
+
+// Solve D^T x = u for one rest column per thread against the factored
+// diagonal block (trsm of FactorizeSupernode, Multifrontal.hpp:452-466), the
+// column held in registers.
+__global__ __launch_bounds__(kPanelThreads, 1) void trsm_kernel( const PanelTask * __restrict__ tasks,
+                                                                 double * __restrict__ arena )
+{
+    const PanelTask t = tasks[blockIdx.x];
+    const int tid = threadIdx.x;
+    const int nb = min( kPanel, t.n0 - t.r0 );
+    const int r1 = t.r0 + nb;
+    const int m = t.n0 - r1;
+    const int rest = m + t.n1;
+    __shared__ double D[kPanel][kPanel + 1];
+    __shared__ double inv_d[kPanel];
+
+    double * U0 = arena + t.u0;
+    double * U1 = arena + t.u1;
+    for( int idx = tid; idx < kPanel * kPanel; idx += kPanelThreads )
+    {
+        const int r = idx / kPanel, c = idx % kPanel;
+        double v = (r == c) ? 1.0 : 0.0;
+        if( r < nb && c < nb && c >= r ) { v = U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c]; }
+        D[r][c] = v;
+    }
+    __syncthreads();
+    for( int r = tid; r < kPanel; r += kPanelThreads ) { inv_d[r] = 1.0 / D[r][r]; }
+    __syncthreads();
 
     const int col = t.c0 + tid;
     if( col < rest )
@@ -534,9 +549,14 @@ void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lu
     if( count > 0 ) { extend_kernel<<<count, 256, 0, st>>>( tasks, lut, arena ); }
 }
 
-void launch_panel( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st )
+void launch_potrf( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st )
 {
-    if( count > 0 ) { panel_kernel<<<count, kPanelThreads, 0, st>>>( tasks, arena, status ); }
+    if( count > 0 ) { potrf_kernel<<<count, kPanelThreads, 0, st>>>( tasks, arena, status ); }
+}
+
+void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st )
+{
+    if( count > 0 ) { trsm_kernel<<<count, kPanelThreads, 0, st>>>( tasks, arena ); }
 }
 
 void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st )

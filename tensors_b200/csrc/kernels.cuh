@@ -17,7 +17,8 @@ void launch_zero( const ZeroTask * tasks, int count, double * arena, cudaStream_
 void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const double * arena,
                     double * tri, double * rec, cudaStream_t st );
 void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, double * arena, cudaStream_t st );
-void launch_panel( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st );
+void launch_potrf( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st );
+void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st );
 void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st );
 
 void launch_solve_diag( const SolveDiagTask * tasks, int count, bool upper, const double * arena,

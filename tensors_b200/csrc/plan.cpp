@@ -327,7 +327,7 @@ void Plan::build( const Symbolic & sym )
     }
 
     // -------------------------------------------------- launch sequences
-    gemm.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
+    gemm.clear(); potrf.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
     gemm_flops = 0.0;
     factor_launches.clear(); lower_launches.clear(); upper_launches.clear();
 
@@ -395,6 +395,7 @@ void Plan::build( const Symbolic & sym )
         rest_ranges[h].resize( static_cast<size_t>(Q) );
         for( I32 q = 0; q < Q; ++q )
         {
+            const I64 ofirst = static_cast<I64>(potrf.size());
             const I64 pfirst = static_cast<I64>(panel.size());
             const I64 gfirst = static_cast<I64>(gemm.size());
             const I64 dfirst = static_cast<I64>(sdiag.size());
@@ -414,14 +415,15 @@ void Plan::build( const Symbolic & sym )
                     const I32 s = sym.row_to_sn[front_row0[f] + r0 + r];
                     if( sym.n0(s) == 1 ) { singles |= (std::int64_t(1) << r); }
                 }
-                for( I32 c0 = 0; c0 == 0 || c0 < rest; c0 += kRestChunk )
+                PanelTask t{};
+                t.u0 = front_u0[f]; t.u1 = front_u1[f];
+                t.n0 = n0; t.n1 = n1; t.r0 = r0; t.c0 = 0;
+                t.row0 = front_row0[f];
+                t.single_rows = singles;
+                potrf.push_back( t );
+                for( I32 c0 = 0; c0 < rest; c0 += kRestChunk )
                 {
-                    PanelTask t{};
-                    t.u0 = front_u0[f]; t.u1 = front_u1[f];
-                    t.n0 = n0; t.n1 = n1; t.r0 = r0; t.c0 = c0;
-                    t.row0 = front_row0[f];
-                    t.write_diag = (c0 == 0) ? 1 : 0;
-                    t.single_rows = singles;
+                    t.c0 = c0;
                     panel.push_back( t );
                 }
                 const I32 m = n0 - r1;
@@ -457,9 +459,11 @@ void Plan::build( const Symbolic & sym )
             std::stable_sort( tiles.begin(), tiles.end(),
                               []( const GemmTask & x, const GemmTask & y ) { return x.K > y.K; } );
             gemm.insert( gemm.end(), tiles.begin(), tiles.end() );
+            const I32 oc = static_cast<I32>( static_cast<I64>(potrf.size()) - ofirst );
             const I32 pc = static_cast<I32>( static_cast<I64>(panel.size()) - pfirst );
             const I32 gc = static_cast<I32>( static_cast<I64>(gemm.size()) - gfirst );
-            if( pc > 0 ) { factor_launches.push_back( { LaunchKind::Panel, pc, pfirst, h, q } ); }
+            if( oc > 0 ) { factor_launches.push_back( { LaunchKind::Potrf, oc, ofirst, h, q } ); }
+            if( pc > 0 ) { factor_launches.push_back( { LaunchKind::Trsm, pc, pfirst, h, q } ); }
             if( gc > 0 ) { factor_launches.push_back( { LaunchKind::Gemm, gc, gfirst, h, q } ); }
             diag_ranges[h][q] = { dfirst, static_cast<I32>( static_cast<I64>(sdiag.size()) - dfirst ) };
             rest_ranges[h][q] = { rfirst, static_cast<I32>( static_cast<I64>(srest.size()) - rfirst ) };

@@ -25,12 +25,13 @@
 //    in child-rank passes (pass r adds every parent's r-th child), so no two
 //    tasks of a launch write the same entry and the summation order is the
 //    reference's (A, then children in order, Multifrontal.hpp:210-224);
-//  * each front's pivots are eliminated in panels of kPanel rows: a panel
-//    launch factors the panel's diagonal block and solves its row of the
-//    front, an update launch applies the rank-kPanel trailing update to the
-//    remaining rows of U0 and U1 as 64 x 64 GEMM tiles, and in the update
-//    launch of a front's last panel its V -= U1^T U1 tiles run with the full
-//    depth K = n0.
+//  * each front's pivots are eliminated in panels of kPanel rows: a potrf
+//    launch factors the panel's diagonal block in place (one CTA per front),
+//    a trsm launch solves the panel's row of the front against it (one CTA
+//    per kRestChunk columns), an update launch applies the rank-kPanel
+//    trailing update to the remaining rows of U0 and U1 as 64 x 64 GEMM
+//    tiles, and in the update launch of a front's last panel its
+//    V -= U1^T U1 tiles run with the full depth K = n0.
 #pragma once
 
 #include <cstdint>
@@ -70,8 +71,9 @@ struct GemmTask
     std::int32_t pad;
 };
 
-// Factor the diagonal block of panel [r0, r0+nb) of a front and solve the
-// panel's rows for rest columns [c0, c0 + kRestChunk): rest column j is U0
+// Panel [r0, r0+nb) of a front.  As a potrf task: factor the diagonal block
+// in place.  As a trsm task: solve the panel's rows for rest columns
+// [c0, c0 + kRestChunk) against the factored block: rest column j is U0
 // column r0+nb+j when j < n0-r0-nb, else U1 column j-(n0-r0-nb).  row0 is
 // the front's first global row (failures report the failing global row);
 // bit r of single_rows marks panel rows that form a 1 x 1 reference
@@ -82,7 +84,7 @@ struct PanelTask
     std::int32_t n0, n1;
     std::int32_t r0, c0;
     std::int32_t row0;
-    std::int32_t write_diag;       // this CTA stores the factored diagonal block
+    std::int32_t pad;
     std::int64_t single_rows;      // bit r set: panel row r is a 1 x 1 reference supernode
 };
 
@@ -134,7 +136,7 @@ struct ExportTask
     std::int32_t pad;
 };
 
-enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Panel = 2, Gemm = 3, SolveDiag = 4, SolveRest = 5 };
+enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, SolveDiag = 4, SolveRest = 5, Potrf = 6 };
 
 // One launch: `count` tasks starting at `first` in the array of its kind.
 struct Launch
@@ -182,7 +184,8 @@ struct Plan
     std::vector<std::int64_t> diag_offset;  // per row: arena offset of U(i,i)
 
     std::vector<GemmTask>      gemm;
-    std::vector<PanelTask>     panel;
+    std::vector<PanelTask>     potrf;          // one per (front, panel)
+    std::vector<PanelTask>     panel;          // trsm chunks
     std::vector<ExtendTask>    extend;
     std::vector<ZeroTask>      zero;
     std::vector<SolveDiagTask> sdiag;

@@ -69,17 +69,21 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             if( i > 0 && i != t.mid && l <= pl.lut[t.lut + i - 1] ) { return "extend lut not increasing" + at; }
         }
     }
-    for( size_t k = 0; k < pl.panel.size(); ++k )
+    for( int which = 0; which < 2; ++which )
     {
-        const PanelTask & t = pl.panel[k];
-        const std::string at = " (panel task " + std::to_string( k ) + ")";
-        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad panel dimensions" + at; }
-        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "panel U0 out of range" + at; }
-        if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.n1 - 1, arena ) ) { return "panel U1 out of range" + at; }
-        const I32 nb = std::min( kPanel, t.n0 - t.r0 );
-        const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
-        if( t.c0 < 0 || (t.c0 > 0 && t.c0 >= rest) ) { return "panel chunk out of range" + at; }
-        if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "panel rows out of range" + at; }
+        const std::vector<PanelTask> & list = which == 0 ? pl.potrf : pl.panel;
+        for( size_t k = 0; k < list.size(); ++k )
+        {
+            const PanelTask & t = list[k];
+            const std::string at = std::string( which == 0 ? " (potrf task " : " (trsm task " ) + std::to_string( k ) + ")";
+            if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad panel dimensions" + at; }
+            if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "panel U0 out of range" + at; }
+            if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.n1 - 1, arena ) ) { return "panel U1 out of range" + at; }
+            const I32 nb = std::min( kPanel, t.n0 - t.r0 );
+            const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
+            if( which == 1 && (t.c0 < 0 || t.c0 >= rest) ) { return "panel chunk out of range" + at; }
+            if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "panel rows out of range" + at; }
+        }
     }
     for( size_t k = 0; k < pl.gemm.size(); ++k )
     {
