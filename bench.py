@@ -48,7 +48,8 @@ L2_FLUSH_BYTES = 256 << 20
 CPU_SAMPLE_GRID = 48
 
 
-def build_problem(grid: int = GRID):
+def build_problem(grid: int | None = None):
+    grid = GRID if grid is None else grid
     from tensors_b200 import matrices, ordering
 
     A = matrices.grid_laplacian_3d(grid, SEED, SHIFT)
@@ -205,6 +206,31 @@ def run_reference(args):
     return 0
 
 
+def run_for_profiler(args):
+    """The plain workload for ncu: (warmup + steps) x (factor + solve), direct launches."""
+    import torch
+    from tensors_b200 import build as tb_build
+    from tensors_b200.cholesky import CholeskyDecomposition
+
+    tb_build.build()
+    A, perm, B_host = build_problem(args.grid)
+    chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    chol.SymbolicFactorization()
+    chol.SetUseGraph(False)
+    vals = torch.tensor(A.values, device="cuda")
+    B = torch.tensor(B_host, device="cuda")
+    X = torch.empty_like(B)
+    for _ in range(args.warmup + args.steps):
+        assert chol.NumericFactorization(vals, 0.0) == 0
+        chol.Solve(B, X)
+    torch.cuda.synchronize()
+    R = chol.Residual(B, X)
+    torch.cuda.synchronize()
+    print(json.dumps({"grid": args.grid, "relres": float(torch.linalg.norm(R) / torch.linalg.norm(B)),
+                      "launches": chol.LaunchCounts(), "plan": chol.PlanStats()}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -212,9 +238,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=GRID, help="grid edge (profiling runs on smaller cases)")
+    ap.add_argument("--ncu", action="store_true",
+                    help="profiling run for ncu: warmup + steps factor+solve as direct launches, no timing, "
+                         "no baselines")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.ncu:
+        return run_for_profiler(args)
 
     import torch
     import torch.distributed as dist
