@@ -52,7 +52,15 @@ __global__ void zero_kernel( const ZeroTask * __restrict__ tasks, double * __res
 {
     const ZeroTask t = tasks[blockIdx.x];
     double * p = arena + t.offset;
-    for( std::int64_t i = threadIdx.x; i < t.count; i += blockDim.x ) { p[i] = 0.0; }
+    std::int64_t i = threadIdx.x;
+    // align to 16 bytes, then store double2
+    const int head = static_cast<int>( (reinterpret_cast<std::uintptr_t>( p ) >> 3) & 1 );
+    if( head && threadIdx.x == 0 && t.count > 0 ) { p[0] = 0.0; }
+    const std::int64_t body = (t.count - head) / 2;
+    double2 * q = reinterpret_cast<double2 *>( p + head );
+    for( ; i < body; i += blockDim.x ) { q[i] = make_double2( 0.0, 0.0 ); }
+    const std::int64_t tail = head + 2 * body;
+    if( threadIdx.x == 0 && tail < t.count ) { p[tail] = 0.0; }
 }
 
 // ---------------------------------------------------------------- export
@@ -67,8 +75,8 @@ __global__ void export_kernel( const ExportTask * __restrict__ tasks, const std:
     for( int r = t.r_begin; r < t.r_end; ++r )
     {
         const std::int64_t fr = t.roff + r;
-        const double * f0 = arena + t.fu0 + fr * t.fn0;
-        const double * f1 = arena + t.fu1 + fr * t.fn1;
+        const double * f0 = arena + t.fu0 + fr * t.fld0;
+        const double * f1 = arena + t.fu1 + fr * t.fld1;
         double * d0 = tri + t.tri + (std::int64_t)r * t.n0s;
         for( int c = threadIdx.x; c < t.n0s; c += blockDim.x ) { d0[c] = (c >= r) ? f0[t.roff + c] : 0.0; }
         double * d1 = rec + t.rec + (std::int64_t)r * t.n1s;
@@ -95,11 +103,11 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
     for( int i = t.row_begin + warp; i < t.row_end; i += 8 )
     {
         const std::int64_t li = lut[i];
-        const double * Wi = W + (std::int64_t)i * t.m1;
+        const double * Wi = W + (std::int64_t)i * t.ldw;
         if( i < t.mid )
         {
-            double * row0 = arena + t.u0 + li * t.n0p;
-            double * row1 = arena + t.u1 + li * t.n1p;
+            double * row0 = arena + t.u0 + li * t.ld0p;
+            double * row1 = arena + t.u1 + li * t.ld1p;
             for( int j = i + lane; j < t.m1; j += 32 )
             {
                 const int lj = lut[j];
@@ -109,7 +117,7 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
         }
         else
         {
-            double * rowv = arena + t.v + li * t.n1p;
+            double * rowv = arena + t.v + li * t.ldvp;
             for( int j = i + lane; j < t.m1; j += 32 ) { rowv[lut[j]] += Wi[j]; }
         }
     }
@@ -123,48 +131,79 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
 __global__ __launch_bounds__(kPanelThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
                                                                double * __restrict__ arena, int * __restrict__ status )
 {
+    // Thread (ty, tx) owns column tx, rows ty, ty+4, ..., ty+60 of the
+    // block in registers; row j is published through shared memory once it
+    // is final, and every thread updates its own entries (no division or
+    // shared-memory read-modify-write in the elimination loop).
+    constexpr int kRowsPerThread = kPanel * kPanel / kPanelThreads;   // 16
+    constexpr int kRowStride = kPanelThreads / kPanel;                // 4
     const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
+    const int tx = tid % kPanel, ty = tid / kPanel;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    __shared__ double D[kPanel][kPanel + 1];
-    __shared__ double inv_d;
+    __shared__ double row[kPanel];
+    __shared__ double piv;
     __shared__ int fail;
 
-    double * U0 = arena + t.u0;
-    for( int idx = tid; idx < nb * nb; idx += kPanelThreads )
+    double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
+    double a[kRowsPerThread];
+#pragma unroll
+    for( int k = 0; k < kRowsPerThread; ++k )
     {
-        const int r = idx / nb, c = idx % nb;
-        D[r][c] = (c >= r) ? U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] : 0.0;
+        const int r = ty + kRowStride * k;
+        a[k] = (r < nb && tx < nb && tx >= r) ? U0[(std::int64_t)r * t.ld0 + tx] : 0.0;
     }
     if( tid == 0 ) { fail = -1; }
     __syncthreads();
 
+#pragma unroll 1
     for( int j = 0; j < nb; ++j )
     {
-        if( tid == 0 )
+        const int kj = j / kRowStride;            // owner slot of row j
+        const bool owns_row = (ty == j % kRowStride);
+        if( owns_row && tx == j )
         {
-            double d = D[j][j];
-            if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
-            else if( !(d > 0.0) && fail < 0 ) { fail = j; }
-            d = sqrt( d );
-            D[j][j] = d;
-            inv_d = 1.0 / d;
+#pragma unroll
+            for( int k = 0; k < kRowsPerThread; ++k )
+            {
+                if( k == kj )
+                {
+                    double d = a[k];
+                    if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
+                    else if( !(d > 0.0) && fail < 0 ) { fail = j; }
+                    d = sqrt( d );
+                    a[k] = d;
+                    piv = d;
+                }
+            }
         }
         __syncthreads();
-        for( int c = j + 1 + tid; c < nb; c += kPanelThreads ) { D[j][c] *= inv_d; }
-        __syncthreads();
-        const int w = nb - j - 1;
-        for( int idx = tid; idx < w * w; idx += kPanelThreads )
+        if( owns_row && tx >= j )
         {
-            const int r = j + 1 + idx / w, c = j + 1 + idx % w;
-            if( c >= r ) { D[r][c] -= D[j][r] * D[j][c]; }
+#pragma unroll
+            for( int k = 0; k < kRowsPerThread; ++k )
+            {
+                if( k == kj )
+                {
+                    if( tx > j ) { a[k] /= piv; }
+                    row[tx] = a[k];
+                }
+            }
         }
         __syncthreads();
+        const double rc = (tx > j) ? row[tx] : 0.0;
+#pragma unroll
+        for( int k = 0; k < kRowsPerThread; ++k )
+        {
+            const int r = ty + kRowStride * k;
+            if( r > j && tx >= r ) { a[k] -= row[r] * rc; }
+        }
     }
-    for( int idx = tid; idx < nb * nb; idx += kPanelThreads )
+#pragma unroll
+    for( int k = 0; k < kRowsPerThread; ++k )
     {
-        const int r = idx / nb, c = idx % nb;
-        if( c >= r ) { U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] = D[r][c]; }
+        const int r = ty + kRowStride * k;
+        if( r < nb && tx < nb && tx >= r ) { U0[(std::int64_t)r * t.ld0 + tx] = a[k]; }
     }
     if( tid == 0 && fail >= 0 )
     {
@@ -194,7 +233,7 @@ __global__ __launch_bounds__(kPanelThreads, 1) void trsm_kernel( const PanelTask
     {
         const int r = idx / kPanel, c = idx % kPanel;
         double v = (r == c) ? 1.0 : 0.0;
-        if( r < nb && c < nb && c >= r ) { v = U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c]; }
+        if( r < nb && c < nb && c >= r ) { v = U0[(std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c]; }
         D[r][c] = v;
     }
     __syncthreads();
@@ -206,8 +245,8 @@ __global__ __launch_bounds__(kPanelThreads, 1) void trsm_kernel( const PanelTask
     {
         double * base;
         std::int64_t ld;
-        if( col < m ) { base = U0 + (std::int64_t)t.r0 * t.n0 + r1 + col; ld = t.n0; }
-        else          { base = U1 + (std::int64_t)t.r0 * t.n1 + (col - m); ld = t.n1; }
+        if( col < m ) { base = U0 + (std::int64_t)t.r0 * t.ld0 + r1 + col; ld = t.ld0; }
+        else          { base = U1 + (std::int64_t)t.r0 * t.ld1 + (col - m); ld = t.ld1; }
         double x[kPanel];
 #pragma unroll
         for( int r = 0; r < kPanel; ++r ) { x[r] = (r < nb) ? base[r * ld] : 0.0; }
@@ -226,14 +265,27 @@ __global__ __launch_bounds__(kPanelThreads, 1) void trsm_kernel( const PanelTask
 // ------------------------------------------------------------------- gemm
 // C[m0:m0+64, c0:c0+64] -= A[:, m0:]^T B[:, c0:] for row-major K x M / K x N
 // panels: 4 warps in a 2 x 2 arrangement, each a 32 x 32 block of 8 x 8
-// DMMA tiles; K staged through double-buffered shared memory 16 rows at a
-// time (register prefetch of the next chunk overlaps the MMAs).
+// DMMA tiles.  K is streamed through a kGemmStages-deep ring of shared-memory
+// stages filled by 16-byte cp.async copies (every operand row starts on a
+// 16-byte boundary: the plan pads leading dimensions to kLdAlign), so the
+// copies of the next chunks overlap the MMAs of the current one.
+constexpr int kGemmStages = 3;
+constexpr int kGemmStageDoubles = 2 * kGemmK * kGemmLd;          // A and B of one stage
+constexpr size_t kGemmSmemBytes = sizeof(double) * kGemmStages * kGemmStageDoubles;
+
+__device__ __forceinline__ void cp_async_16( double * smem_dst, const double * gmem_src, int src_bytes )
+{
+    const unsigned saddr = static_cast<unsigned>( __cvta_generic_to_shared( smem_dst ) );
+    asm volatile( "cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(saddr), "l"(gmem_src), "r"(src_bytes) );
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile( "cp.async.commit_group;\n" ::: "memory" ); }
+template<int N> __device__ __forceinline__ void cp_async_wait() { asm volatile( "cp.async.wait_group %0;\n" :: "n"(N) : "memory" ); }
+
 __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask * __restrict__ tasks,
                                                                 double * __restrict__ arena )
 {
+    extern __shared__ __align__(16) double gsm[];
     const GemmTask t = tasks[blockIdx.x];
-    __shared__ double As[2][kGemmK][kGemmLd];
-    __shared__ double Bs[2][kGemmK][kGemmLd];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -247,56 +299,60 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 #pragma unroll
         for( int j = 0; j < 4; ++j ) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
 
-    constexpr int kPer = kGemmK * kTile / kGemmThreads;   // 8 elements per thread per operand
-    double ra[kPer], rb[kPer];
-    auto load = [&]( int k0 )
+    // Each stage holds kGemmK rows of 64 doubles for A and for B = 512
+    // 16-byte chunks per operand; thread tid copies chunks tid + 128 * l.
+    constexpr int kChunks = kGemmK * kTile / 2 / kGemmThreads;       // 4 per operand
+    auto issue = [&]( int stage, int k0 )
     {
+        double * As = gsm + stage * kGemmStageDoubles;
+        double * Bs = As + kGemmK * kGemmLd;
 #pragma unroll
-        for( int l = 0; l < kPer; ++l )
+        for( int l = 0; l < kChunks; ++l )
         {
             const int idx = tid + kGemmThreads * l;
-            const int r = idx / kTile, c = idx % kTile;
+            const int r = idx / (kTile / 2), c = 2 * (idx % (kTile / 2));
             const int k = k0 + r;
-            ra[l] = (k < t.K && t.m0 + c < t.M) ? A[(std::int64_t)k * t.lda + t.m0 + c] : 0.0;
-            rb[l] = (k < t.K && t.c0 + c < t.N) ? B[(std::int64_t)k * t.ldb + t.c0 + c] : 0.0;
-        }
-    };
-    auto store = [&]( int buf )
-    {
-#pragma unroll
-        for( int l = 0; l < kPer; ++l )
-        {
-            const int idx = tid + kGemmThreads * l;
-            const int r = idx / kTile, c = idx % kTile;
-            As[buf][r][c] = ra[l];
-            Bs[buf][r][c] = rb[l];
+            const int am = t.M - (t.m0 + c), bn = t.N - (t.c0 + c);
+            const int abytes = (k < t.K) ? (am >= 2 ? 16 : (am == 1 ? 8 : 0)) : 0;
+            const int bbytes = (k < t.K) ? (bn >= 2 ? 16 : (bn == 1 ? 8 : 0)) : 0;
+            cp_async_16( As + r * kGemmLd + c, abytes ? A + (std::int64_t)k * t.lda + t.m0 + c : A, abytes );
+            cp_async_16( Bs + r * kGemmLd + c, bbytes ? B + (std::int64_t)k * t.ldb + t.c0 + c : B, bbytes );
         }
     };
 
     const int nk = (t.K + kGemmK - 1) / kGemmK;
-    load( 0 );
-    store( 0 );
-    __syncthreads();
+#pragma unroll
+    for( int s = 0; s < kGemmStages - 1; ++s )
+    {
+        if( s < nk ) { issue( s, s * kGemmK ); }
+        cp_async_commit();
+    }
     for( int kc = 0; kc < nk; ++kc )
     {
-        const int buf = kc & 1;
-        if( kc + 1 < nk ) { load( (kc + 1) * kGemmK ); }
+        cp_async_wait<kGemmStages - 2>();
+        __syncthreads();
+        {
+            const int nxt = kc + kGemmStages - 1;
+            if( nxt < nk ) { issue( nxt % kGemmStages, nxt * kGemmK ); }
+            cp_async_commit();
+        }
+        const double * As = gsm + (kc % kGemmStages) * kGemmStageDoubles;
+        const double * Bs = As + kGemmK * kGemmLd;
 #pragma unroll
         for( int kk = 0; kk < kGemmK; kk += 4 )
         {
             double af[4], bf[4];
 #pragma unroll
-            for( int i = 0; i < 4; ++i ) { af[i] = As[buf][kk + (lane & 3)][wm * 32 + i * 8 + (lane >> 2)]; }
+            for( int i = 0; i < 4; ++i ) { af[i] = As[(kk + (lane & 3)) * kGemmLd + wm * 32 + i * 8 + (lane >> 2)]; }
 #pragma unroll
-            for( int j = 0; j < 4; ++j ) { bf[j] = Bs[buf][kk + (lane & 3)][wn * 32 + j * 8 + (lane >> 2)]; }
+            for( int j = 0; j < 4; ++j ) { bf[j] = Bs[(kk + (lane & 3)) * kGemmLd + wn * 32 + j * 8 + (lane >> 2)]; }
 #pragma unroll
             for( int i = 0; i < 4; ++i )
 #pragma unroll
                 for( int j = 0; j < 4; ++j ) { dmma_8x8x4( acc[i][j], af[i], bf[j] ); }
         }
-        if( kc + 1 < nk ) { store( buf ^ 1 ); }
-        __syncthreads();
     }
+    cp_async_wait<0>();
 
     double * C = arena + t.c;
 #pragma unroll
@@ -304,17 +360,24 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
     {
         const int row = t.m0 + wm * 32 + i * 8 + (lane >> 2);
         if( row >= t.M ) { continue; }
+        double * Crow = C + (std::int64_t)row * t.ldc;
 #pragma unroll
         for( int j = 0; j < 4; ++j )
         {
-#pragma unroll
-            for( int e = 0; e < 2; ++e )
+            const int col = t.c0 + wn * 32 + j * 8 + (lane & 3) * 2;
+            const bool ok0 = col < t.N && (!t.upper || row <= col);
+            const bool ok1 = col + 1 < t.N && (!t.upper || row <= col + 1);
+            if( ok0 && ok1 )
             {
-                const int col = t.c0 + wn * 32 + j * 8 + (lane & 3) * 2 + e;
-                if( col < t.N && (!t.upper || row <= col) )
-                {
-                    C[(std::int64_t)row * t.ldc + col] -= acc[i][j][e];
-                }
+                double2 v = *reinterpret_cast<const double2 *>( Crow + col );
+                v.x -= acc[i][j][0];
+                v.y -= acc[i][j][1];
+                *reinterpret_cast<double2 *>( Crow + col ) = v;
+            }
+            else
+            {
+                if( ok0 ) { Crow[col] -= acc[i][j][0]; }
+                if( ok1 ) { Crow[col + 1] -= acc[i][j][1]; }
             }
         }
     }
@@ -334,17 +397,20 @@ __global__ __launch_bounds__(kSolveThreads) void solve_diag_kernel( const SolveD
     const SolveDiagTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    const double * U0 = arena + t.u0;
-    for( int idx = tid; idx < nb * nb; idx += kSolveThreads )
+    // thread -> (row group g, column c); groups cover rows g, g+G, g+2G, ...
+    const int c = tid % k;
+    const int g = tid / k;
+    const int G = kSolveThreads / k;
+    const double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
+    for( int r = tid / kPanel; r < nb; r += kSolveThreads / kPanel )
     {
-        const int r = idx / nb, c = idx % nb;
-        D[r][c] = (c >= r) ? U0[(std::int64_t)(t.r0 + r) * t.n0 + t.r0 + c] : 0.0;
+        const int cc = tid % kPanel;
+        if( cc < nb ) { D[r][cc] = (cc >= r) ? U0[(std::int64_t)r * t.ld0 + cc] : 0.0; }
     }
     const std::int64_t row_base = (std::int64_t)t.row0 + t.r0;
-    for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+    if( g < G )
     {
-        const int r = idx / k, c = idx % k;
-        Xs[r * k + c] = X[(row_base + r) * ldx + c];
+        for( int r = g; r < nb; r += G ) { Xs[r * k + c] = X[(row_base + r) * ldx + c]; }
     }
     __syncthreads();
     if( !upper )
@@ -353,11 +419,10 @@ __global__ __launch_bounds__(kSolveThreads) void solve_diag_kernel( const SolveD
         {
             if( tid < k ) { Xs[r * k + tid] /= D[r][r]; }
             __syncthreads();
-            const int w = nb - r - 1;
-            for( int idx = tid; idx < w * k; idx += kSolveThreads )
+            if( g < G )
             {
-                const int r2 = r + 1 + idx / k, c = idx % k;
-                Xs[r2 * k + c] -= D[r][r2] * Xs[r * k + c];
+                const double xr = Xs[r * k + c];
+                for( int r2 = r + 1 + g; r2 < nb; r2 += G ) { Xs[r2 * k + c] -= D[r][r2] * xr; }
             }
             __syncthreads();
         }
@@ -368,18 +433,17 @@ __global__ __launch_bounds__(kSolveThreads) void solve_diag_kernel( const SolveD
         {
             if( tid < k ) { Xs[r * k + tid] /= D[r][r]; }
             __syncthreads();
-            for( int idx = tid; idx < r * k; idx += kSolveThreads )
+            if( g < G )
             {
-                const int r2 = idx / k, c = idx % k;
-                Xs[r2 * k + c] -= D[r2][r] * Xs[r * k + c];
+                const double xr = Xs[r * k + c];
+                for( int r2 = g; r2 < r; r2 += G ) { Xs[r2 * k + c] -= D[r2][r] * xr; }
             }
             __syncthreads();
         }
     }
-    for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+    if( g < G )
     {
-        const int r = idx / k, c = idx % k;
-        X[(row_base + r) * ldx + c] = Xs[r * k + c];
+        for( int r = g; r < nb; r += G ) { X[(row_base + r) * ldx + c] = Xs[r * k + c]; }
     }
 }
 
@@ -397,58 +461,68 @@ __global__ __launch_bounds__(kSolveThreads) void solve_rest_kernel( const SolveR
     extern __shared__ double smem[];
     double (*P)[kSolveRest + 1] = reinterpret_cast<double (*)[kSolveRest + 1]>( smem );   // [kPanel][kSolveRest+1]
     double * Xs = smem + kPanel * (kSolveRest + 1);
+    __shared__ std::int64_t trow[kSolveRest];
     const SolveRestTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
     const int r1 = t.r0 + nb;
     const int m = t.n0 - r1;
     const int cw = t.c1 - t.c0;
+    const int c = tid % k;
+    const int g = tid / k;
+    const int G = kSolveThreads / k;
     const double * U0 = arena + t.u0;
     const double * U1 = arena + t.u1;
-    for( int idx = tid; idx < nb * cw; idx += kSolveThreads )
     {
-        const int i = idx / cw, jj = idx % cw;
+        const int jj = tid % kSolveRest;
         const int j = t.c0 + jj;
-        P[i][jj] = (j < m) ? U0[(std::int64_t)(t.r0 + i) * t.n0 + r1 + j]
-                           : U1[(std::int64_t)(t.r0 + i) * t.n1 + (j - m)];
+        if( jj < cw )
+        {
+            const double * src = (j < m) ? U0 + (std::int64_t)t.r0 * t.ld0 + r1 + j
+                                         : U1 + (std::int64_t)t.r0 * t.ld1 + (j - m);
+            const std::int64_t ld = (j < m) ? t.ld0 : t.ld1;
+            for( int i = tid / kSolveRest; i < nb; i += kSolveThreads / kSolveRest ) { P[i][jj] = src[i * ld]; }
+            if( tid < kSolveRest )
+            {
+                trow[jj] = (j < m) ? (std::int64_t)t.row0 + r1 + j : (std::int64_t)sn_inner[t.inner + (j - m)];
+            }
+        }
     }
     const std::int64_t panel_row = (std::int64_t)t.row0 + t.r0;
-    auto target_row = [&]( int j ) -> std::int64_t
-    {
-        return (j < m) ? (std::int64_t)t.row0 + r1 + j : (std::int64_t)sn_inner[t.inner + (j - m)];
-    };
     if( !upper )
     {
-        for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+        if( g < G )
         {
-            const int i = idx / k, c = idx % k;
-            Xs[i * k + c] = X[(panel_row + i) * ldx + c];
+            for( int i = g; i < nb; i += G ) { Xs[i * k + c] = X[(panel_row + i) * ldx + c]; }
         }
         __syncthreads();
-        for( int idx = tid; idx < cw * k; idx += kSolveThreads )
+        if( g < G )
         {
-            const int jj = idx / k, c = idx % k;
-            double acc = 0.0;
-            for( int i = 0; i < nb; ++i ) { acc += P[i][jj] * Xs[i * k + c]; }
-            const int j = t.c0 + jj;
-            double * dst = X + target_row( j ) * ldx + c;
-            if( j < m ) { *dst -= acc; } else { atomicAdd( dst, -acc ); }
+            for( int jj = g; jj < cw; jj += G )
+            {
+                double acc = 0.0;
+                for( int i = 0; i < nb; ++i ) { acc += P[i][jj] * Xs[i * k + c]; }
+                double * dst = X + trow[jj] * ldx + c;
+                if( t.c0 + jj < m ) { *dst -= acc; } else { atomicAdd( dst, -acc ); }
+            }
         }
     }
     else
     {
-        for( int idx = tid; idx < cw * k; idx += kSolveThreads )
+        __syncthreads();
+        if( g < G )
         {
-            const int jj = idx / k, c = idx % k;
-            Xs[jj * k + c] = X[target_row( t.c0 + jj ) * ldx + c];
+            for( int jj = g; jj < cw; jj += G ) { Xs[jj * k + c] = X[trow[jj] * ldx + c]; }
         }
         __syncthreads();
-        for( int idx = tid; idx < nb * k; idx += kSolveThreads )
+        if( g < G )
         {
-            const int i = idx / k, c = idx % k;
-            double acc = 0.0;
-            for( int jj = 0; jj < cw; ++jj ) { acc += P[i][jj] * Xs[jj * k + c]; }
-            atomicAdd( X + (panel_row + i) * ldx + c, -acc );
+            for( int i = g; i < nb; i += G )
+            {
+                double acc = 0.0;
+                for( int jj = 0; jj < cw; ++jj ) { acc += P[i][jj] * Xs[jj * k + c]; }
+                atomicAdd( X + (panel_row + i) * ldx + c, -acc );
+            }
         }
     }
 }
@@ -561,7 +635,7 @@ void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream
 
 void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st )
 {
-    if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, 0, st>>>( tasks, arena ); }
+    if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, kGemmSmemBytes, st>>>( tasks, arena ); }
 }
 
 void launch_solve_diag( const SolveDiagTask * tasks, int count, bool upper, const double * arena,
@@ -600,6 +674,11 @@ void launch_residual( int n, const std::int64_t * outer, const std::int32_t * in
 
 cudaError_t configure_kernels()
 {
+    {
+        const cudaError_t g = cudaFuncSetAttribute( gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)kGemmSmemBytes );
+        if( g != cudaSuccess ) { return g; }
+    }
     cudaError_t e = cudaFuncSetAttribute( solve_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)( sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kMaxRhs) ) );
     if( e != cudaSuccess ) { return e; }

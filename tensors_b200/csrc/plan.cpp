@@ -15,6 +15,7 @@ using I64 = std::int64_t;
 
 constexpr I64 kExtendEntries = 8192;   // target entries of W per extend-add task
 constexpr I64 kExportEntries = 16384;  // target entries per export task
+constexpr I64 kZeroChunk = 1 << 16;     // doubles per zeroing task
 
 void push_tiles( std::vector<GemmTask> & out, I64 a, I32 lda, I64 b, I32 ldb, I64 c, I32 ldc,
                  I32 K, I32 M, I32 N, bool symmetric )
@@ -204,10 +205,17 @@ void Plan::build( const Symbolic & sym )
     // ---------------------------------------------------------- arena layout
     front_u0.resize( static_cast<size_t>(F) );
     front_u1.resize( static_cast<size_t>(F) );
+    front_ld0.resize( static_cast<size_t>(F) );
+    front_ld1.resize( static_cast<size_t>(F) );
     front_v.assign( static_cast<size_t>(F), 0 );
     u0_size = u1_size = 0;
-    for( I32 f = 0; f < F; ++f ) { front_u0[f] = u0_size; u0_size += static_cast<I64>(front_n0[f]) * front_n0[f]; }
-    for( I32 f = 0; f < F; ++f ) { front_u1[f] = u0_size + u1_size; u1_size += static_cast<I64>(front_n0[f]) * front_n1[f]; }
+    for( I32 f = 0; f < F; ++f )
+    {
+        front_ld0[f] = static_cast<I32>( ceil_div( front_n0[f], kLdAlign ) * kLdAlign );
+        front_ld1[f] = static_cast<I32>( ceil_div( front_n1[f], kLdAlign ) * kLdAlign );
+    }
+    for( I32 f = 0; f < F; ++f ) { front_u0[f] = u0_size; u0_size += static_cast<I64>(front_n0[f]) * front_ld0[f]; }
+    for( I32 f = 0; f < F; ++f ) { front_u1[f] = u0_size + u1_size; u1_size += static_cast<I64>(front_n0[f]) * front_ld1[f]; }
     // update matrices: live from the front's level until its parent's level
     std::vector<std::vector<I32>> release_at( static_cast<size_t>(levels) + 1 );
     {
@@ -217,12 +225,12 @@ void Plan::build( const Symbolic & sym )
         {
             for( I32 f : by_level[h] )
             {
-                const I64 sz = static_cast<I64>(front_n1[f]) * front_n1[f];
+                const I64 sz = static_cast<I64>(front_n1[f]) * front_ld1[f];
                 voff[f] = va.allocate( sz );
                 const I32 p = front_parent[f];
                 release_at[p < F ? level_of[p] : h].push_back( f );
             }
-            for( I32 f : release_at[h] ) { va.release( voff[f], static_cast<I64>(front_n1[f]) * front_n1[f] ); }
+            for( I32 f : release_at[h] ) { va.release( voff[f], static_cast<I64>(front_n1[f]) * front_ld1[f] ); }
         }
         v_size = va.capacity();
         for( I32 f = 0; f < F; ++f ) { front_v[f] = u0_size + u1_size + voff[f]; }
@@ -275,12 +283,12 @@ void Plan::build( const Symbolic & sym )
                 I64 dst;
                 if( j < re )
                 {
-                    dst = front_u0[f] + static_cast<I64>(front_n0[f]) * (i - rb) + (j - rb);
+                    dst = front_u0[f] + static_cast<I64>(front_ld0[f]) * (i - rb) + (j - rb);
                 }
                 else
                 {
                     while( cols[l] < j ) { ++l; }
-                    dst = front_u1[f] + static_cast<I64>(front_n1[f]) * (i - rb) + l;
+                    dst = front_u1[f] + static_cast<I64>(front_ld1[f]) * (i - rb) + l;
                 }
                 asm_src.push_back( sym.value_perm[k] );
                 asm_dst.push_back( static_cast<I64>( static_cast<std::uint64_t>(dst) | (j == i ? kDiagFlag : 0ull) ) );
@@ -298,7 +306,7 @@ void Plan::build( const Symbolic & sym )
         {
             const I32 rb = front_row0[f], re = rb + front_n0[f];
             for( I32 j = 0; j < front_n1[f]; ++j ) { pos[sym.sn_inner[front_cols[f] + j]] = j; }
-            for( I32 r = rb; r < re; ++r ) { diag_offset[r] = front_u0[f] + static_cast<I64>(front_n0[f] + 1) * (r - rb); }
+            for( I32 r = rb; r < re; ++r ) { diag_offset[r] = front_u0[f] + static_cast<I64>(front_ld0[f] + 1) * (r - rb); }
             for( I32 s = front_sn_first[f]; s <= front_sn_last[f]; ++s )
             {
                 const I64 cb = sym.sn_outer[s];
@@ -317,6 +325,7 @@ void Plan::build( const Symbolic & sym )
                     e.tri = sym.sn_tri_ptr[s]; e.rec = sym.sn_rec_ptr[s];
                     e.colmap = cb;
                     e.fn0 = front_n0[f]; e.fn1 = front_n1[f];
+                    e.fld0 = front_ld0[f]; e.fld1 = front_ld1[f];
                     e.roff = sym.sn_rp[s] - rb;
                     e.n0s = n0s; e.n1s = n1s;
                     e.r_begin = r; e.r_end = std::min( n0s, r + rows_per_task );
@@ -343,8 +352,8 @@ void Plan::build( const Symbolic & sym )
             const I64 first = static_cast<I64>(zero.size());
             for( I32 f : L )
             {
-                const I64 sz = static_cast<I64>(front_n1[f]) * front_n1[f];
-                if( sz > 0 ) { zero.push_back( { front_v[f], sz } ); }
+                const I64 sz = static_cast<I64>(front_n1[f]) * front_ld1[f];
+                for( I64 o = 0; o < sz; o += kZeroChunk ) { zero.push_back( { front_v[f] + o, std::min( kZeroChunk, sz - o ) } ); }
             }
             const I32 count = static_cast<I32>( static_cast<I64>(zero.size()) - first );
             if( count > 0 ) { factor_launches.push_back( { LaunchKind::Zero, count, first, h, 0 } ); }
@@ -379,6 +388,8 @@ void Plan::build( const Symbolic & sym )
                     e.lut = front_lut[t];
                     e.m1 = m1; e.mid = mid[t];
                     e.n0p = front_n0[p]; e.n1p = front_n1[p];
+                    e.ldw = front_ld1[t];
+                    e.ld0p = front_ld0[p]; e.ld1p = front_ld1[p]; e.ldvp = front_ld1[p];
                     e.row_begin = row; e.row_end = end;
                     extend.push_back( e );
                     row = end;
@@ -415,9 +426,11 @@ void Plan::build( const Symbolic & sym )
                     const I32 s = sym.row_to_sn[front_row0[f] + r0 + r];
                     if( sym.n0(s) == 1 ) { singles |= (std::int64_t(1) << r); }
                 }
+                const I32 ld0 = front_ld0[f], ld1 = front_ld1[f];
                 PanelTask t{};
                 t.u0 = front_u0[f]; t.u1 = front_u1[f];
                 t.n0 = n0; t.n1 = n1; t.r0 = r0; t.c0 = 0;
+                t.ld0 = ld0; t.ld1 = ld1;
                 t.row0 = front_row0[f];
                 t.single_rows = singles;
                 potrf.push_back( t );
@@ -429,25 +442,26 @@ void Plan::build( const Symbolic & sym )
                 const I32 m = n0 - r1;
                 if( m > 0 )
                 {
-                    const I64 pa = front_u0[f] + static_cast<I64>(r0) * n0 + r1;        // U0[r0:r1, r1:n0]
-                    push_tiles( tiles, pa, n0, pa, n0, front_u0[f] + static_cast<I64>(r1) * n0 + r1, n0, nb, m, m, true );
+                    const I64 pa = front_u0[f] + static_cast<I64>(r0) * ld0 + r1;        // U0[r0:r1, r1:n0]
+                    push_tiles( tiles, pa, ld0, pa, ld0, front_u0[f] + static_cast<I64>(r1) * ld0 + r1, ld0, nb, m, m, true );
                     if( n1 > 0 )
                     {
-                        push_tiles( tiles, pa, n0, front_u1[f] + static_cast<I64>(r0) * n1, n1,
-                                    front_u1[f] + static_cast<I64>(r1) * n1, n1, nb, m, n1, false );
+                        push_tiles( tiles, pa, ld0, front_u1[f] + static_cast<I64>(r0) * ld1, ld1,
+                                    front_u1[f] + static_cast<I64>(r1) * ld1, ld1, nb, m, n1, false );
                     }
                 }
                 else if( n1 > 0 && front_parent[f] < F )
                 {
-                    push_tiles( tiles, front_u1[f], n1, front_u1[f], n1, front_v[f], n1, n0, n1, n1, true );
+                    push_tiles( tiles, front_u1[f], ld1, front_u1[f], ld1, front_v[f], ld1, n0, n1, n1, true );
                 }
-                sdiag.push_back( { front_u0[f], n0, r0, front_row0[f], 0 } );
+                sdiag.push_back( { front_u0[f], n0, r0, front_row0[f], ld0 } );
                 for( I32 c0 = 0; c0 < rest; c0 += kSolveRest )
                 {
                     SolveRestTask t{};
                     t.u0 = front_u0[f]; t.u1 = front_u1[f]; t.inner = front_cols[f];
                     t.n0 = n0; t.n1 = n1; t.r0 = r0; t.row0 = front_row0[f];
                     t.c0 = c0; t.c1 = std::min( rest, c0 + kSolveRest );
+                    t.ld0 = ld0; t.ld1 = ld1;
                     srest.push_back( t );
                 }
             }

@@ -15,7 +15,8 @@
 // request.
 //
 //  * the factor arena holds, per front, U0 (n0 x n0, row-major upper), U1
-//    (n0 x n1, row-major) and an update-matrix region in which each front's
+//    (n0 x n1, row-major), rows padded to kLdAlign entries (32-byte aligned
+//    rows for vector and bulk copies), and an update-matrix region in which each front's
 //    n1 x n1 contribution block V (Multifrontal.hpp:165) lives from its
 //    front's level until its parent's level; V regions are reused across
 //    levels by a first-fit allocator and zeroed by the level that owns them;
@@ -46,6 +47,7 @@ constexpr int kPanel     = 64;    // pivot panel width
 constexpr int kTile      = 64;    // GEMM output tile (kTile x kTile)
 constexpr int kRestChunk = 256;   // columns per panel-solve CTA (one per thread)
 constexpr int kSolveRest = 64;    // rows per solve-update task
+constexpr int kLdAlign   = 4;     // row padding of every front block (entries)
 constexpr std::uint64_t kDiagFlag = 1ull << 62;   // marks diagonal entries in the assembly map
 
 // Relaxed amalgamation limits: a merge whose front has at most nrelax[0]
@@ -82,6 +84,7 @@ struct PanelTask
 {
     std::int64_t u0, u1;
     std::int32_t n0, n1;
+    std::int32_t ld0, ld1;         // leading dimensions of U0 / U1
     std::int32_t r0, c0;
     std::int32_t row0;
     std::int32_t pad;
@@ -95,7 +98,9 @@ struct ExtendTask
     std::int64_t w, u0, u1, v;
     std::int64_t lut;              // offset into the lut array
     std::int32_t m1, mid;
-    std::int32_t n0p, n1p;
+    std::int32_t n0p, n1p;         // parent dimensions
+    std::int32_t ldw;              // leading dimension of the child's W
+    std::int32_t ld0p, ld1p, ldvp; // leading dimensions of the parent's U0 / U1 / V
     std::int32_t row_begin, row_end;
 };
 
@@ -104,7 +109,7 @@ struct ExtendTask
 struct SolveDiagTask
 {
     std::int64_t u0;
-    std::int32_t n0, r0, row0, pad;
+    std::int32_t n0, r0, row0, ld0;
 };
 
 // Rest part of a panel in the solves: rows [c0, c1) of the panel's rest
@@ -114,6 +119,7 @@ struct SolveRestTask
 {
     std::int64_t u0, u1, inner;
     std::int32_t n0, n1, r0, row0, c0, c1;
+    std::int32_t ld0, ld1;
 };
 
 // Zero `count` doubles at arena offset `offset`.
@@ -130,6 +136,7 @@ struct ExportTask
     std::int64_t tri, rec;         // destination offsets (tri region / rec region)
     std::int64_t colmap;           // offset into colmap (== SN_outer[sn])
     std::int32_t fn0, fn1;         // front dimensions
+    std::int32_t fld0, fld1;       // front leading dimensions
     std::int32_t roff;             // first row of sn within the front
     std::int32_t n0s, n1s;         // supernode dimensions
     std::int32_t r_begin, r_end;
@@ -160,9 +167,12 @@ struct Plan
     std::vector<std::int32_t> front_parent;    // front_count = root
     std::vector<std::int32_t> front_of_sn;
 
-    // arena layout (doubles): [U0 of all fronts][U1 of all fronts][update region]
+    // arena layout (doubles): [U0 of all fronts][U1 of all fronts][update region];
+    // rows are padded to a multiple of kLdAlign entries so every row of every
+    // block starts on a 32-byte boundary
     std::int64_t u0_size = 0, u1_size = 0, v_size = 0;
     std::vector<std::int64_t> front_u0, front_u1, front_v;   // arena offsets
+    std::vector<std::int32_t> front_ld0, front_ld1;          // U0 / U1 leading dimensions (V uses ld1)
 
     std::int32_t levels = 0;
     std::vector<std::int32_t> level_of;     // per front

@@ -55,9 +55,10 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         const std::string at = " (extend task " + std::to_string( k ) + ")";
         if( t.m1 <= 0 || t.mid < 0 || t.mid > t.m1 ) { return "bad extend dimensions" + at; }
         if( t.row_begin < 0 || t.row_end > t.m1 || t.row_begin >= t.row_end ) { return "bad extend rows" + at; }
-        if( !in_range( t.w, t.w + static_cast<I64>(t.m1) * t.m1 - 1, arena ) ) { return "extend source out of range" + at; }
+        if( t.ldw < t.m1 || t.ld0p < t.n0p || t.ld1p < t.n1p || t.ldvp < t.n1p ) { return "extend leading dimension too small" + at; }
+        if( !in_range( t.w, t.w + static_cast<I64>(t.m1) * t.ldw - 1, arena ) ) { return "extend source out of range" + at; }
         if( t.lut < 0 || t.lut + t.m1 > static_cast<I64>( pl.lut.size() ) ) { return "extend lut out of range" + at; }
-        const I64 u0n = static_cast<I64>(t.n0p) * t.n0p, u1n = static_cast<I64>(t.n0p) * t.n1p, vn = static_cast<I64>(t.n1p) * t.n1p;
+        const I64 u0n = static_cast<I64>(t.n0p) * t.ld0p, u1n = static_cast<I64>(t.n0p) * t.ld1p, vn = static_cast<I64>(t.n1p) * t.ldvp;
         if( u0n > 0 && !in_range( t.u0, t.u0 + u0n - 1, arena ) ) { return "extend U0 out of range" + at; }
         if( u1n > 0 && !in_range( t.u1, t.u1 + u1n - 1, arena ) ) { return "extend U1 out of range" + at; }
         if( t.mid < t.m1 && (vn == 0 || !in_range( t.v, t.v + vn - 1, arena )) ) { return "extend V out of range" + at; }
@@ -77,8 +78,9 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             const PanelTask & t = list[k];
             const std::string at = std::string( which == 0 ? " (potrf task " : " (trsm task " ) + std::to_string( k ) + ")";
             if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad panel dimensions" + at; }
-            if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "panel U0 out of range" + at; }
-            if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.n1 - 1, arena ) ) { return "panel U1 out of range" + at; }
+            if( t.ld0 < t.n0 || t.ld1 < t.n1 ) { return "panel leading dimension too small" + at; }
+            if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "panel U0 out of range" + at; }
+            if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.ld1 - 1, arena ) ) { return "panel U1 out of range" + at; }
             const I32 nb = std::min( kPanel, t.n0 - t.r0 );
             const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
             if( which == 1 && (t.c0 < 0 || t.c0 >= rest) ) { return "panel chunk out of range" + at; }
@@ -91,6 +93,7 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         const std::string at = " (gemm task " + std::to_string( k ) + ")";
         if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad gemm dimensions" + at; }
         if( t.M > t.lda || t.N > t.ldb || t.N > t.ldc ) { return "gemm leading dimension too small" + at; }
+        if( (t.a | t.b | t.c) % 2 != 0 || (t.lda | t.ldb | t.ldc) % 2 != 0 ) { return "gemm operand not 16-byte aligned" + at; }
         if( !in_range( t.a, t.a + static_cast<I64>(t.K - 1) * t.lda + t.M - 1, arena ) ) { return "gemm A out of range" + at; }
         if( !in_range( t.b, t.b + static_cast<I64>(t.K - 1) * t.ldb + t.N - 1, arena ) ) { return "gemm B out of range" + at; }
         if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at; }
@@ -98,8 +101,8 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
     for( size_t k = 0; k < pl.sdiag.size(); ++k )
     {
         const SolveDiagTask & t = pl.sdiag[k];
-        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 ) { return "bad solve-diag dimensions"; }
-        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "solve-diag U0 out of range"; }
+        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.ld0 < t.n0 ) { return "bad solve-diag dimensions"; }
+        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "solve-diag U0 out of range"; }
         if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "solve-diag rows out of range"; }
     }
     for( size_t k = 0; k < pl.srest.size(); ++k )
@@ -110,8 +113,9 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         const I32 nb = std::min( kPanel, t.n0 - t.r0 );
         const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
         if( t.c0 < 0 || t.c1 > rest || t.c0 >= t.c1 || t.c1 - t.c0 > kSolveRest ) { return "solve-rest range out of bounds" + at; }
-        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.n0 - 1, arena ) ) { return "solve-rest U0 out of range" + at; }
-        if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.n1 - 1, arena ) ) { return "solve-rest U1 out of range" + at; }
+        if( t.ld0 < t.n0 || t.ld1 < t.n1 ) { return "solve-rest leading dimension too small" + at; }
+        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "solve-rest U0 out of range" + at; }
+        if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.ld1 - 1, arena ) ) { return "solve-rest U1 out of range" + at; }
         if( t.n1 > 0 && (t.inner < 0 || t.inner + t.n1 > inner_size) ) { return "solve-rest columns out of range" + at; }
         if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "solve-rest rows out of range" + at; }
     }
@@ -124,8 +128,9 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         if( t.roff < 0 || t.roff + t.n0s > t.fn0 ) { return "export rows outside the front" + at; }
         if( !in_range( t.tri, t.tri + static_cast<I64>(t.n0s) * t.n0s - 1, tri_size ) ) { return "export tri out of range" + at; }
         if( t.n1s > 0 && !in_range( t.rec, t.rec + static_cast<I64>(t.n0s) * t.n1s - 1, rec_size ) ) { return "export rec out of range" + at; }
-        if( !in_range( t.fu0, t.fu0 + static_cast<I64>(t.fn0) * t.fn0 - 1, arena ) ) { return "export front U0 out of range" + at; }
-        if( t.fn1 > 0 && !in_range( t.fu1, t.fu1 + static_cast<I64>(t.fn0) * t.fn1 - 1, arena ) ) { return "export front U1 out of range" + at; }
+        if( t.fld0 < t.fn0 || t.fld1 < t.fn1 ) { return "export leading dimension too small" + at; }
+        if( !in_range( t.fu0, t.fu0 + static_cast<I64>(t.fn0) * t.fld0 - 1, arena ) ) { return "export front U0 out of range" + at; }
+        if( t.fn1 > 0 && !in_range( t.fu1, t.fu1 + static_cast<I64>(t.fn0) * t.fld1 - 1, arena ) ) { return "export front U1 out of range" + at; }
         if( t.colmap < 0 || t.colmap + t.n1s > static_cast<I64>( pl.colmap.size() ) ) { return "export colmap out of range" + at; }
         for( I32 l = 0; l < t.n1s; ++l )
         {
