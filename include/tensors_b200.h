@@ -175,6 +175,10 @@ int tb_chol_set_graph( tb_chol * h, int32_t enabled );
  * algorithmic flops of the GEMM tiles (8 entries each). */
 int tb_chol_set_profiling( tb_chol * h, int32_t enabled );
 int tb_chol_kernel_profile( tb_chol * h, double * ms, int64_t * launches, double * flops );
+/* Per launch of the last profiled factorization (at most cap entries):
+ * info[4i..4i+3] = kind, level, panel step (or child rank), task count and
+ * ms[i] its duration; entry 0 is the clear + assembly.  Returns the count. */
+int tb_chol_launch_profile( tb_chol * h, int64_t * info, double * ms, int32_t cap );
 /* Number of kernel launches the last numeric factorization / solve issued. */
 int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * solve_launches );
 

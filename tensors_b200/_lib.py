@@ -57,6 +57,7 @@ SIGNATURES = {
     "tb_chol_launch_counts": (ctypes.c_int, [_vp, _pi64, _pi64]),
     "tb_chol_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_kernel_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "tb_chol_launch_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
 }
 
 _LIB = None

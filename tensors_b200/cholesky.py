@@ -333,6 +333,16 @@ class CholeskyDecomposition:
         names = {0: "zero", 1: "extend", 2: "trsm", 3: "gemm", 6: "potrf", 7: "assemble"}
         return {names[k]: {"ms": float(ms[k]), "launches": int(ln[k]), "flops": float(fl[k])} for k in names}
 
+    def LaunchProfile(self):
+        """Per launch of the last profiled factorization: (kind, level, step, tasks, ms)."""
+        cap = 1 << 16
+        info = np.zeros(4 * cap, dtype=np.int64)
+        ms = np.zeros(cap)
+        m = _check(lib().tb_chol_launch_profile(self._h, info.ctypes.data, ms.ctypes.data, cap))
+        names = {0: "zero", 1: "extend", 2: "trsm", 3: "gemm", 6: "potrf", 7: "assemble"}
+        return [(names.get(int(info[4 * i]), "?"), int(info[4 * i + 1]), int(info[4 * i + 2]), int(info[4 * i + 3]),
+                 float(ms[i])) for i in range(m)]
+
     def LaunchCounts(self):
         a, b = ctypes.c_int64(), ctypes.c_int64()
         _check(lib().tb_chol_launch_counts(self._h, ctypes.byref(a), ctypes.byref(b)))

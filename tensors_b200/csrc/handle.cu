@@ -137,6 +137,7 @@ struct tb_chol
     double kind_ms[8] = {};
     std::int64_t kind_launches[8] = {};
     std::vector<cudaEvent_t> events;
+    std::vector<float> launch_ms;          // per factor launch of the last profiled run (0 = clear + assembly)
 
     bool factorized = false;
     bool good = false;
@@ -312,12 +313,14 @@ int run_factor( tb_chol * h, double reg )
         TB_CUDA( cudaGetLastError() );
         TB_CUDA( cudaStreamSynchronize( st ) );
         for( int k = 0; k < 8; ++k ) { h->kind_ms[k] = 0.0; h->kind_launches[k] = 0; }
+        h->launch_ms.assign( kinds.size(), 0.0f );
         for( std::size_t i = 0; i < kinds.size(); ++i )
         {
             float ms = 0.0f;
             TB_CUDA( cudaEventElapsedTime( &ms, h->events[i], h->events[i + 1] ) );
             h->kind_ms[kinds[i]] += ms;
             h->kind_launches[kinds[i]] += 1;
+            h->launch_ms[i] = ms;
         }
     }
     else if( h->use_graph )
@@ -819,6 +822,29 @@ int tb_chol_kernel_profile( tb_chol * h, double * ms, std::int64_t * launches, d
     }
     if( flops && h->symbolic_done ) { flops[static_cast<int>( tb::LaunchKind::Gemm )] = h->plan.gemm_flops; }
     return TB_OK;
+}
+
+int tb_chol_launch_profile( tb_chol * h, std::int64_t * info, double * ms, std::int32_t cap )
+{
+    if( h == nullptr || cap < 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( h->launch_ms.size() ) );
+    for( std::int32_t i = 0; i < m; ++i )
+    {
+        if( i == 0 )
+        {
+            if( info ) { info[0] = 7; info[1] = -1; info[2] = -1; info[3] = 1; }
+        }
+        else if( info )
+        {
+            const tb::Launch & L = h->plan.factor_launches[static_cast<size_t>( i - 1 )];
+            info[4 * i + 0] = static_cast<std::int64_t>( L.kind );
+            info[4 * i + 1] = L.level;
+            info[4 * i + 2] = L.step;
+            info[4 * i + 3] = L.count;
+        }
+        if( ms ) { ms[i] = h->launch_ms[static_cast<size_t>( i )]; }
+    }
+    return m;
 }
 
 int tb_chol_launch_counts( tb_chol * h, std::int64_t * factor_launches, std::int64_t * solve_launches )
