@@ -128,95 +128,82 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
 // in place (LAPACK potrf of FactorizeSupernode, Multifrontal.hpp:438-449).
 // A row that forms a 1 x 1 reference supernode takes sqrt(|a|) as the
 // reference does (:471) and never reports failure.
-__global__ __launch_bounds__(kPanelThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
+constexpr int kPotrfThreads = kPanel;       // one thread per column of the block
+constexpr int kTrsmThreads  = 256;          // 4 threads per rest column
+constexpr int kTrsmCols     = kTrsmThreads / 4;
+
+__global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
                                                                double * __restrict__ arena, int * __restrict__ status )
 {
-    // Thread (ty, tx) owns column tx, rows ty, ty+4, ..., ty+60 of the
-    // block in registers; row j is published through shared memory once it
-    // is final, and every thread updates its own entries (no division or
-    // shared-memory read-modify-write in the elimination loop).
-    constexpr int kRowsPerThread = kPanel * kPanel / kPanelThreads;   // 16
-    constexpr int kRowStride = kPanelThreads / kPanel;                // 4
+    // Thread c holds column c of the block in registers; the elimination
+    // loop is fully unrolled so every register index is static.  Per pivot:
+    // its owner takes the square root and reciprocal, the row is scaled and
+    // published through shared memory, and each thread updates its column.
     const PanelTask t = tasks[blockIdx.x];
-    const int tid = threadIdx.x;
-    const int tx = tid % kPanel, ty = tid / kPanel;
+    const int tx = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
     __shared__ double row[kPanel];
-    __shared__ double piv;
+    __shared__ double inv_piv;
     __shared__ int fail;
 
     double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    double a[kRowsPerThread];
+    double a[kPanel];
 #pragma unroll
-    for( int k = 0; k < kRowsPerThread; ++k )
-    {
-        const int r = ty + kRowStride * k;
-        a[k] = (r < nb && tx < nb && tx >= r) ? U0[(std::int64_t)r * t.ld0 + tx] : 0.0;
-    }
-    if( tid == 0 ) { fail = -1; }
-    __syncthreads();
+    for( int r = 0; r < kPanel; ++r ) { a[r] = (r < nb && tx < nb && r <= tx) ? U0[(std::int64_t)r * t.ld0 + tx] : 0.0; }
+    if( tx == 0 ) { fail = -1; }
 
-#pragma unroll 1
-    for( int j = 0; j < nb; ++j )
-    {
-        const int kj = j / kRowStride;            // owner slot of row j
-        const bool owns_row = (ty == j % kRowStride);
-        if( owns_row && tx == j )
-        {
 #pragma unroll
-            for( int k = 0; k < kRowsPerThread; ++k )
+    for( int j = 0; j < kPanel; ++j )
+    {
+        if( j < nb )
+        {
+            if( tx == j )
             {
-                if( k == kj )
+                double d = a[j];
+                if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
+                else if( !(d > 0.0) && fail < 0 ) { fail = j; }
+                d = sqrt( d );
+                a[j] = d;
+                inv_piv = 1.0 / d;
+            }
+            __syncthreads();
+            double u = 0.0;
+            if( tx > j )
+            {
+                u = a[j] * inv_piv;
+                a[j] = u;
+                row[tx] = u;
+            }
+            __syncthreads();
+            if( tx > j )
+            {
+#pragma unroll
+                for( int r = j + 1; r < kPanel; ++r )
                 {
-                    double d = a[k];
-                    if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
-                    else if( !(d > 0.0) && fail < 0 ) { fail = j; }
-                    d = sqrt( d );
-                    a[k] = d;
-                    piv = d;
+                    if( r <= tx ) { a[r] -= row[r] * u; }
                 }
             }
         }
-        __syncthreads();
-        if( owns_row && tx >= j )
-        {
-#pragma unroll
-            for( int k = 0; k < kRowsPerThread; ++k )
-            {
-                if( k == kj )
-                {
-                    if( tx > j ) { a[k] /= piv; }
-                    row[tx] = a[k];
-                }
-            }
-        }
-        __syncthreads();
-        const double rc = (tx > j) ? row[tx] : 0.0;
-#pragma unroll
-        for( int k = 0; k < kRowsPerThread; ++k )
-        {
-            const int r = ty + kRowStride * k;
-            if( r > j && tx >= r ) { a[k] -= row[r] * rc; }
-        }
     }
 #pragma unroll
-    for( int k = 0; k < kRowsPerThread; ++k )
+    for( int r = 0; r < kPanel; ++r )
     {
-        const int r = ty + kRowStride * k;
-        if( r < nb && tx < nb && tx >= r ) { U0[(std::int64_t)r * t.ld0 + tx] = a[k]; }
+        if( r < nb && tx < nb && r <= tx ) { U0[(std::int64_t)r * t.ld0 + tx] = a[r]; }
     }
-    if( tid == 0 && fail >= 0 )
+    if( tx == 0 && fail >= 0 )
     {
         atomicOr( status, 1 );
         atomicMin( status + 1, t.row0 + t.r0 + fail );
     }
 }
 
-// Solve D^T x = u for one rest column per thread against the factored
-// diagonal block (trsm of FactorizeSupernode, Multifrontal.hpp:452-466), the
-// column held in registers.
-__global__ __launch_bounds__(kPanelThreads, 1) void trsm_kernel( const PanelTask * __restrict__ tasks,
-                                                                 double * __restrict__ arena )
+// Solve D^T x = u against the factored diagonal block for the rest columns
+// [c0, c0 + kRestChunk) (trsm of FactorizeSupernode, Multifrontal.hpp:
+// 452-466).  Four threads share a column: thread q of the quad holds rows
+// q, q+4, ..., q+60 in registers; each solved entry is broadcast to the quad
+// by a shuffle.
+__global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
+                                                             double * __restrict__ arena )
 {
     const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
@@ -229,7 +216,7 @@ __global__ __launch_bounds__(kPanelThreads, 1) void trsm_kernel( const PanelTask
 
     double * U0 = arena + t.u0;
     double * U1 = arena + t.u1;
-    for( int idx = tid; idx < kPanel * kPanel; idx += kPanelThreads )
+    for( int idx = tid; idx < kPanel * kPanel; idx += kTrsmThreads )
     {
         const int r = idx / kPanel, c = idx % kPanel;
         double v = (r == c) ? 1.0 : 0.0;
@@ -237,28 +224,50 @@ __global__ __launch_bounds__(kPanelThreads, 1) void trsm_kernel( const PanelTask
         D[r][c] = v;
     }
     __syncthreads();
-    for( int r = tid; r < kPanel; r += kPanelThreads ) { inv_d[r] = 1.0 / D[r][r]; }
+    for( int r = tid; r < kPanel; r += kTrsmThreads ) { inv_d[r] = 1.0 / D[r][r]; }
     __syncthreads();
 
-    const int col = t.c0 + tid;
-    if( col < rest )
+    const int q = tid & 3;
+    const int quad_base = (tid & 31) & ~3;
+    for( int cb = 0; cb < kRestChunk; cb += kTrsmCols )
     {
-        double * base;
-        std::int64_t ld;
-        if( col < m ) { base = U0 + (std::int64_t)t.r0 * t.ld0 + r1 + col; ld = t.ld0; }
-        else          { base = U1 + (std::int64_t)t.r0 * t.ld1 + (col - m); ld = t.ld1; }
-        double x[kPanel];
+        const int col = t.c0 + cb + (tid >> 2);
+        const bool active = col < rest && (t.c0 + cb + (tid >> 2)) < t.c0 + kRestChunk;
+        double * base = nullptr;
+        std::int64_t ld = 0;
+        if( active )
+        {
+            if( col < m ) { base = U0 + (std::int64_t)t.r0 * t.ld0 + r1 + col; ld = t.ld0; }
+            else          { base = U1 + (std::int64_t)t.r0 * t.ld1 + (col - m); ld = t.ld1; }
+        }
+        double x[kPanel / 4];
 #pragma unroll
-        for( int r = 0; r < kPanel; ++r ) { x[r] = (r < nb) ? base[r * ld] : 0.0; }
+        for( int i = 0; i < kPanel / 4; ++i )
+        {
+            const int r = 4 * i + q;
+            x[i] = (active && r < nb) ? base[r * ld] : 0.0;
+        }
 #pragma unroll
         for( int r = 0; r < kPanel; ++r )
         {
-            x[r] *= inv_d[r];
+            const int owner = r & 3, slot = r >> 2;
+            if( q == owner ) { x[slot] *= inv_d[r]; }
+            const double xr = __shfl_sync( 0xffffffffu, x[slot], quad_base + owner );
 #pragma unroll
-            for( int r2 = 0; r2 < kPanel; ++r2 ) { if( r2 > r ) { x[r2] -= D[r][r2] * x[r]; } }
+            for( int i = 0; i < kPanel / 4; ++i )
+            {
+                if( 4 * i + q > r ) { x[i] -= D[r][4 * i + q] * xr; }
+            }
         }
+        if( active )
+        {
 #pragma unroll
-        for( int r = 0; r < kPanel; ++r ) { if( r < nb ) { base[r * ld] = x[r]; } }
+            for( int i = 0; i < kPanel / 4; ++i )
+            {
+                const int r = 4 * i + q;
+                if( r < nb ) { base[r * ld] = x[i]; }
+            }
+        }
     }
 }
 
@@ -625,12 +634,12 @@ void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lu
 
 void launch_potrf( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st )
 {
-    if( count > 0 ) { potrf_kernel<<<count, kPanelThreads, 0, st>>>( tasks, arena, status ); }
+    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, 0, st>>>( tasks, arena, status ); }
 }
 
 void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st )
 {
-    if( count > 0 ) { trsm_kernel<<<count, kPanelThreads, 0, st>>>( tasks, arena ); }
+    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, 0, st>>>( tasks, arena ); }
 }
 
 void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st )
