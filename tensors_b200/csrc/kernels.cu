@@ -128,69 +128,64 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
 // in place (LAPACK potrf of FactorizeSupernode, Multifrontal.hpp:438-449).
 // A row that forms a 1 x 1 reference supernode takes sqrt(|a|) as the
 // reference does (:471) and never reports failure.
-constexpr int kPotrfThreads = kPanel;       // one thread per column of the block
-constexpr int kTrsmThreads  = 256;          // 4 threads per rest column
+constexpr int kPotrfThreads = 256;         // four threads per column of the block
+constexpr int kTrsmThreads  = 256;         // four threads per rest column
 constexpr int kTrsmCols     = kTrsmThreads / 4;
+constexpr size_t kTrsmSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * (kTrsmCols + 1));
+
+// The elimination loops below stay rolled: fully unrolled versions of these
+// 64-step recurrences do not fit the instruction cache and run slower.
 
 __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
                                                                double * __restrict__ arena, int * __restrict__ status )
 {
-    // Thread c holds column c of the block in registers; the elimination
-    // loop is fully unrolled so every register index is static.  Per pivot:
-    // its owner takes the square root and reciprocal, the row is scaled and
-    // published through shared memory, and each thread updates its column.
+    // Right-looking Cholesky of the block in shared memory.  Thread
+    // (c = tid / 4, q = tid % 4) updates column c, rows q, q+4, ... of the
+    // trailing part; per pivot one thread takes the square root and
+    // reciprocal and one thread per column scales the pivot row.
     const PanelTask t = tasks[blockIdx.x];
-    const int tx = threadIdx.x;
+    const int tid = threadIdx.x;
+    const int c = tid >> 2, q = tid & 3;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    __shared__ double row[kPanel];
+    __shared__ double D[kPanel][kPanel + 1];
     __shared__ double inv_piv;
     __shared__ int fail;
 
     double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    double a[kPanel];
-#pragma unroll
-    for( int r = 0; r < kPanel; ++r ) { a[r] = (r < nb && tx < nb && r <= tx) ? U0[(std::int64_t)r * t.ld0 + tx] : 0.0; }
-    if( tx == 0 ) { fail = -1; }
-
-#pragma unroll
-    for( int j = 0; j < kPanel; ++j )
+    for( int r = q; r < nb; r += 4 )
     {
-        if( j < nb )
+        if( c < nb ) { D[r][c] = (r <= c) ? U0[(std::int64_t)r * t.ld0 + c] : 0.0; }
+    }
+    if( tid == 0 ) { fail = -1; }
+    __syncthreads();
+
+    for( int j = 0; j < nb; ++j )
+    {
+        if( tid == 0 )
         {
-            if( tx == j )
-            {
-                double d = a[j];
-                if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
-                else if( !(d > 0.0) && fail < 0 ) { fail = j; }
-                d = sqrt( d );
-                a[j] = d;
-                inv_piv = 1.0 / d;
-            }
-            __syncthreads();
-            double u = 0.0;
-            if( tx > j )
-            {
-                u = a[j] * inv_piv;
-                a[j] = u;
-                row[tx] = u;
-            }
-            __syncthreads();
-            if( tx > j )
-            {
-#pragma unroll
-                for( int r = j + 1; r < kPanel; ++r )
-                {
-                    if( r <= tx ) { a[r] -= row[r] * u; }
-                }
-            }
+            double d = D[j][j];
+            if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
+            else if( !(d > 0.0) && fail < 0 ) { fail = j; }
+            d = sqrt( d );
+            D[j][j] = d;
+            inv_piv = 1.0 / d;
+        }
+        __syncthreads();
+        if( q == 0 && c > j && c < nb ) { D[j][c] *= inv_piv; }
+        __syncthreads();
+        if( c > j && c < nb )
+        {
+            const double u = D[j][c];
+            int r = j + 1 + ((q - (j + 1)) & 3);
+            for( ; r <= c; r += 4 ) { D[r][c] -= D[j][r] * u; }
         }
     }
-#pragma unroll
-    for( int r = 0; r < kPanel; ++r )
+    __syncthreads();
+    for( int r = q; r < nb; r += 4 )
     {
-        if( r < nb && tx < nb && r <= tx ) { U0[(std::int64_t)r * t.ld0 + tx] = a[r]; }
+        if( c < nb && r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = D[r][c]; }
     }
-    if( tx == 0 && fail >= 0 )
+    if( tid == 0 && fail >= 0 )
     {
         atomicOr( status, 1 );
         atomicMin( status + 1, t.row0 + t.r0 + fail );
@@ -199,73 +194,71 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
 
 // Solve D^T x = u against the factored diagonal block for the rest columns
 // [c0, c0 + kRestChunk) (trsm of FactorizeSupernode, Multifrontal.hpp:
-// 452-466).  Four threads share a column: thread q of the quad holds rows
-// q, q+4, ..., q+60 in registers; each solved entry is broadcast to the quad
-// by a shuffle.
+// 452-466), kTrsmCols columns at a time staged in shared memory.  The four
+// threads of a quad (one warp-local group per column) handle rows q, q+4,
+// ...; a quad only synchronises with its own warp.
 __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
                                                              double * __restrict__ arena )
 {
+    extern __shared__ double tsm[];
+    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( tsm );
+    double (*X)[kTrsmCols + 1] = reinterpret_cast<double (*)[kTrsmCols + 1]>( tsm + kPanel * (kPanel + 1) );
+    __shared__ double inv_d[kPanel];
     const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
     const int r1 = t.r0 + nb;
     const int m = t.n0 - r1;
     const int rest = m + t.n1;
-    __shared__ double D[kPanel][kPanel + 1];
-    __shared__ double inv_d[kPanel];
-
+    const double * U0c = arena + t.u0;
     double * U0 = arena + t.u0;
     double * U1 = arena + t.u1;
-    for( int idx = tid; idx < kPanel * kPanel; idx += kTrsmThreads )
+    for( int idx = tid; idx < nb * kPanel; idx += kTrsmThreads )
     {
-        const int r = idx / kPanel, c = idx % kPanel;
-        double v = (r == c) ? 1.0 : 0.0;
-        if( r < nb && c < nb && c >= r ) { v = U0[(std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c]; }
-        D[r][c] = v;
+        const int r = idx / kPanel, cc = idx % kPanel;
+        if( cc < nb ) { D[r][cc] = (cc >= r) ? U0c[(std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + cc] : 0.0; }
     }
     __syncthreads();
-    for( int r = tid; r < kPanel; r += kTrsmThreads ) { inv_d[r] = 1.0 / D[r][r]; }
-    __syncthreads();
+    for( int r = tid; r < nb; r += kTrsmThreads ) { inv_d[r] = 1.0 / D[r][r]; }
 
     const int q = tid & 3;
-    const int quad_base = (tid & 31) & ~3;
+    const int lc = tid >> 2;                   // local column
     for( int cb = 0; cb < kRestChunk; cb += kTrsmCols )
     {
-        const int col = t.c0 + cb + (tid >> 2);
-        const bool active = col < rest && (t.c0 + cb + (tid >> 2)) < t.c0 + kRestChunk;
-        double * base = nullptr;
-        std::int64_t ld = 0;
-        if( active )
+        const int first = t.c0 + cb;
+        if( first >= rest ) { break; }
+        __syncthreads();
+        // stage kTrsmCols columns (coalesced along each row)
+        for( int idx = tid; idx < nb * kTrsmCols; idx += kTrsmThreads )
         {
-            if( col < m ) { base = U0 + (std::int64_t)t.r0 * t.ld0 + r1 + col; ld = t.ld0; }
-            else          { base = U1 + (std::int64_t)t.r0 * t.ld1 + (col - m); ld = t.ld1; }
-        }
-        double x[kPanel / 4];
-#pragma unroll
-        for( int i = 0; i < kPanel / 4; ++i )
-        {
-            const int r = 4 * i + q;
-            x[i] = (active && r < nb) ? base[r * ld] : 0.0;
-        }
-#pragma unroll
-        for( int r = 0; r < kPanel; ++r )
-        {
-            const int owner = r & 3, slot = r >> 2;
-            if( q == owner ) { x[slot] *= inv_d[r]; }
-            const double xr = __shfl_sync( 0xffffffffu, x[slot], quad_base + owner );
-#pragma unroll
-            for( int i = 0; i < kPanel / 4; ++i )
+            const int r = idx / kTrsmCols, cc = idx % kTrsmCols;
+            const int col = first + cc;
+            double v = 0.0;
+            if( col < rest )
             {
-                if( 4 * i + q > r ) { x[i] -= D[r][4 * i + q] * xr; }
+                v = (col < m) ? U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col]
+                              : U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)];
             }
+            X[r][cc] = v;
         }
-        if( active )
+        __syncthreads();
+        for( int r = 0; r < nb; ++r )
         {
-#pragma unroll
-            for( int i = 0; i < kPanel / 4; ++i )
+            if( q == (r & 3) ) { X[r][lc] *= inv_d[r]; }
+            __syncwarp();
+            const double xr = X[r][lc];
+            for( int r2 = r + 1 + ((q - (r + 1)) & 3); r2 < nb; r2 += 4 ) { X[r2][lc] -= D[r][r2] * xr; }
+            __syncwarp();
+        }
+        __syncthreads();
+        for( int idx = tid; idx < nb * kTrsmCols; idx += kTrsmThreads )
+        {
+            const int r = idx / kTrsmCols, cc = idx % kTrsmCols;
+            const int col = first + cc;
+            if( col < rest )
             {
-                const int r = 4 * i + q;
-                if( r < nb ) { base[r * ld] = x[i]; }
+                if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = X[r][cc]; }
+                else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = X[r][cc]; }
             }
         }
     }
@@ -639,7 +632,7 @@ void launch_potrf( const PanelTask * tasks, int count, double * arena, int * sta
 
 void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st )
 {
-    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, 0, st>>>( tasks, arena ); }
+    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, kTrsmSmemBytes, st>>>( tasks, arena ); }
 }
 
 void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st )
@@ -683,6 +676,11 @@ void launch_residual( int n, const std::int64_t * outer, const std::int32_t * in
 
 cudaError_t configure_kernels()
 {
+    {
+        const cudaError_t g = cudaFuncSetAttribute( trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)kTrsmSmemBytes );
+        if( g != cudaSuccess ) { return g; }
+    }
     {
         const cudaError_t g = cudaFuncSetAttribute( gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                     (int)kGemmSmemBytes );
