@@ -179,8 +179,8 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
             int r = j + 1 + ((q - (j + 1)) & 3);
             for( ; r <= c; r += 4 ) { D[r][c] -= D[j][r] * u; }
         }
+        __syncthreads();
     }
-    __syncthreads();
     for( int r = q; r < nb; r += 4 )
     {
         if( c < nb && r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = D[r][c]; }
