@@ -128,62 +128,134 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
 // in place (LAPACK potrf of FactorizeSupernode, Multifrontal.hpp:438-449).
 // A row that forms a 1 x 1 reference supernode takes sqrt(|a|) as the
 // reference does (:471) and never reports failure.
-constexpr int kPotrfThreads = 256;         // four threads per column of the block
-constexpr int kTrsmThreads  = 256;         // four threads per rest column
-constexpr int kTrsmCols     = kTrsmThreads / 4;
-constexpr size_t kTrsmSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * (kTrsmCols + 1));
+// Panel kernels work on the 64 x 64 diagonal block in 8 x 8 sub-blocks:
+// sequential 8-step recurrences run in registers (unrolled 8 x 8), and every
+// update between sub-blocks is an 8 x 8 x 8 product on the FP64 tensor cores
+// (two DMMA m8n8k4).  The outer loops over sub-blocks stay rolled so the code
+// fits the instruction cache.
+constexpr int kPotrfThreads = 256;
+constexpr int kTrsmThreads  = 256;
+constexpr int kSub          = 8;                     // sub-block edge
+constexpr int kSubs         = kPanel / kSub;         // 8 sub-blocks per panel edge
+constexpr int kXld          = kRestChunk + 4;        // padded row of the staged rest columns
+constexpr size_t kTrsmSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kXld);
 
-// The elimination loops below stay rolled: fully unrolled versions of these
-// 64-step recurrences do not fit the instruction cache and run slower.
+// C(8x8) += A(8x8) * B(8x8) with A read through a(i, k), B through b(k, j)
+// and C through c(i, j) (warp-wide; fragment layouts of mma.m8n8k4.f64).
+template<typename FA, typename FB>
+__device__ __forceinline__ void dmma_8x8x8( double (&acc)[2], FA a, FB b )
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for( int s = 0; s < 2; ++s )
+    {
+        dmma_8x8x4( acc, a( lane >> 2, (lane & 3) + 4 * s ), b( (lane & 3) + 4 * s, lane >> 2 ) );
+    }
+}
 
 __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
                                                                double * __restrict__ arena, int * __restrict__ status )
 {
-    // Right-looking Cholesky of the block in shared memory.  Thread
-    // (c = tid / 4, q = tid % 4) updates column c, rows q, q+4, ... of the
-    // trailing part; per pivot one thread takes the square root and
-    // reciprocal and one thread per column scales the pivot row.
     const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
-    const int c = tid >> 2, q = tid & 3;
+    const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
     __shared__ double D[kPanel][kPanel + 1];
-    __shared__ double inv_piv;
     __shared__ int fail;
 
     double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    for( int r = q; r < nb; r += 4 )
+    for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
     {
-        if( c < nb ) { D[r][c] = (r <= c) ? U0[(std::int64_t)r * t.ld0 + c] : 0.0; }
+        const int r = idx / kPanel, c = idx % kPanel;
+        double v = (r == c) ? 1.0 : 0.0;                 // identity padding beyond nb
+        if( r < nb && c < nb && r <= c ) { v = U0[(std::int64_t)r * t.ld0 + c]; }
+        D[r][c] = v;
     }
     if( tid == 0 ) { fail = -1; }
     __syncthreads();
 
-    for( int j = 0; j < nb; ++j )
+    const int nsub = (nb + kSub - 1) / kSub;
+    for( int b = 0; b < nsub; ++b )
     {
-        if( tid == 0 )
+        const int o = b * kSub;
+        // (a) Cholesky of the 8 x 8 diagonal sub-block: lane c < 8 holds column c
+        if( warp == 0 )
         {
-            double d = D[j][j];
-            if( (t.single_rows >> j) & 1 ) { d = fabs( d ); }
-            else if( !(d > 0.0) && fail < 0 ) { fail = j; }
-            d = sqrt( d );
-            D[j][j] = d;
-            inv_piv = 1.0 / d;
+            double a[kSub];
+#pragma unroll
+            for( int r = 0; r < kSub; ++r ) { a[r] = (lane < kSub && r <= lane) ? D[o + r][o + lane] : 0.0; }
+#pragma unroll
+            for( int r = 0; r < kSub; ++r )
+            {
+                double d = __shfl_sync( 0xffffffffu, a[r], r );
+                if( lane == 0 )
+                {
+                    if( (t.single_rows >> (o + r)) & 1 ) { }
+                    else if( o + r < nb && !(d > 0.0) && fail < 0 ) { fail = o + r; }
+                }
+                if( (t.single_rows >> (o + r)) & 1 ) { d = fabs( d ); }
+                const double piv = sqrt( d );
+                const double inv = 1.0 / piv;
+                if( lane == r ) { a[r] = piv; }
+                if( lane > r ) { a[r] *= inv; }                     // U(r, lane)
+#pragma unroll
+                for( int r2 = r + 1; r2 < kSub; ++r2 )
+                {
+                    const double urr2 = __shfl_sync( 0xffffffffu, a[r], r2 );   // U(r, r2)
+                    if( lane >= r2 ) { a[r2] -= urr2 * a[r]; }
+                }
+            }
+            if( lane < kSub )
+            {
+#pragma unroll
+                for( int r = 0; r < kSub; ++r ) { if( r <= lane ) { D[o + r][o + lane] = a[r]; } }
+            }
         }
         __syncthreads();
-        if( q == 0 && c > j && c < nb ) { D[j][c] *= inv_piv; }
-        __syncthreads();
-        if( c > j && c < nb )
+        // (b) rows o..o+7 of the columns right of the sub-block: U_b,c = L_bb^{-1} A_b,c
         {
-            const double u = D[j][c];
-            int r = j + 1 + ((q - (j + 1)) & 3);
-            for( ; r <= c; r += 4 ) { D[r][c] -= D[j][r] * u; }
+            const int col = o + kSub + tid;
+            if( col < kPanel )
+            {
+                double x[kSub];
+#pragma unroll
+                for( int r = 0; r < kSub; ++r ) { x[r] = D[o + r][col]; }
+#pragma unroll
+                for( int r = 0; r < kSub; ++r )
+                {
+                    x[r] /= D[o + r][o + r];
+#pragma unroll
+                    for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= D[o + r][o + r2] * x[r]; }
+                }
+#pragma unroll
+                for( int r = 0; r < kSub; ++r ) { D[o + r][col] = x[r]; }
+            }
+        }
+        __syncthreads();
+        // (c) trailing sub-blocks (b2, b3), b < b2 <= b3: D -= U_b,b2^T U_b,b3
+        {
+            const int rem = kSubs - 1 - b;
+            const int tiles = rem * (rem + 1) / 2;
+            for( int tile = warp; tile < tiles; tile += kPotrfThreads / 32 )
+            {
+                int b2 = 0, acc_t = tile;
+                while( acc_t >= rem - b2 ) { acc_t -= rem - b2; ++b2; }
+                const int b3 = b2 + acc_t;
+                const int o2 = o + kSub + b2 * kSub, o3 = o + kSub + b3 * kSub;
+                double acc[2] = { 0.0, 0.0 };
+                dmma_8x8x8( acc, [&]( int i, int k ) { return D[o + k][o2 + i]; },
+                                 [&]( int k, int j ) { return D[o + k][o3 + j]; } );
+                const int i = lane >> 2, j = 2 * (lane & 3);
+                D[o2 + i][o3 + j]     -= acc[0];
+                D[o2 + i][o3 + j + 1] -= acc[1];
+            }
         }
         __syncthreads();
     }
-    for( int r = q; r < nb; r += 4 )
+    for( int idx = tid; idx < nb * nb; idx += kPotrfThreads )
     {
-        if( c < nb && r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = D[r][c]; }
+        const int r = idx / nb, c = idx % nb;
+        if( r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = D[r][c]; }
     }
     if( tid == 0 && fail >= 0 )
     {
@@ -194,72 +266,89 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
 
 // Solve D^T x = u against the factored diagonal block for the rest columns
 // [c0, c0 + kRestChunk) (trsm of FactorizeSupernode, Multifrontal.hpp:
-// 452-466), kTrsmCols columns at a time staged in shared memory.  The four
-// threads of a quad (one warp-local group per column) handle rows q, q+4,
-// ...; a quad only synchronises with its own warp.
+// 452-466): the columns are staged in shared memory; per 8-row sub-block,
+// one thread per column solves the 8 x 8 triangle in registers, then the
+// warps update the rows below with DMMA (warp w owns columns 8w..8w+7).
 __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
                                                              double * __restrict__ arena )
 {
     extern __shared__ double tsm[];
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( tsm );
-    double (*X)[kTrsmCols + 1] = reinterpret_cast<double (*)[kTrsmCols + 1]>( tsm + kPanel * (kPanel + 1) );
-    __shared__ double inv_d[kPanel];
+    double (*X)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm + kPanel * (kPanel + 1) );
     const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
     const int r1 = t.r0 + nb;
     const int m = t.n0 - r1;
     const int rest = m + t.n1;
-    const double * U0c = arena + t.u0;
+    const int cw = min( kRestChunk, rest - t.c0 );
     double * U0 = arena + t.u0;
     double * U1 = arena + t.u1;
-    for( int idx = tid; idx < nb * kPanel; idx += kTrsmThreads )
+    for( int idx = tid; idx < kPanel * kPanel; idx += kTrsmThreads )
     {
-        const int r = idx / kPanel, cc = idx % kPanel;
-        if( cc < nb ) { D[r][cc] = (cc >= r) ? U0c[(std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + cc] : 0.0; }
+        const int r = idx / kPanel, c = idx % kPanel;
+        double v = (r == c) ? 1.0 : 0.0;
+        if( r < nb && c < nb && r <= c ) { v = U0[(std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c]; }
+        D[r][c] = v;
+    }
+    for( int idx = tid; idx < kPanel * kRestChunk; idx += kTrsmThreads )
+    {
+        const int r = idx / kRestChunk, cc = idx % kRestChunk;
+        const int col = t.c0 + cc;
+        double v = 0.0;
+        if( r < nb && cc < cw )
+        {
+            v = (col < m) ? U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col]
+                          : U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)];
+        }
+        X[r][cc] = v;
     }
     __syncthreads();
-    for( int r = tid; r < nb; r += kTrsmThreads ) { inv_d[r] = 1.0 / D[r][r]; }
-
-    const int q = tid & 3;
-    const int lc = tid >> 2;                   // local column
-    for( int cb = 0; cb < kRestChunk; cb += kTrsmCols )
+    const int nsub = (nb + kSub - 1) / kSub;
+    for( int b = 0; b < nsub; ++b )
     {
-        const int first = t.c0 + cb;
-        if( first >= rest ) { break; }
-        __syncthreads();
-        // stage kTrsmCols columns (coalesced along each row)
-        for( int idx = tid; idx < nb * kTrsmCols; idx += kTrsmThreads )
+        const int o = b * kSub;
+        if( tid < kRestChunk )
         {
-            const int r = idx / kTrsmCols, cc = idx % kTrsmCols;
-            const int col = first + cc;
-            double v = 0.0;
-            if( col < rest )
+            double x[kSub];
+#pragma unroll
+            for( int r = 0; r < kSub; ++r ) { x[r] = X[o + r][tid]; }
+#pragma unroll
+            for( int r = 0; r < kSub; ++r )
             {
-                v = (col < m) ? U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col]
-                              : U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)];
+                x[r] /= D[o + r][o + r];
+#pragma unroll
+                for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= D[o + r][o + r2] * x[r]; }
             }
-            X[r][cc] = v;
+#pragma unroll
+            for( int r = 0; r < kSub; ++r ) { X[o + r][tid] = x[r]; }
         }
         __syncthreads();
-        for( int r = 0; r < nb; ++r )
+        for( int b2 = b + 1; b2 < nsub; ++b2 )
         {
-            if( q == (r & 3) ) { X[r][lc] *= inv_d[r]; }
-            __syncwarp();
-            const double xr = X[r][lc];
-            for( int r2 = r + 1 + ((q - (r + 1)) & 3); r2 < nb; r2 += 4 ) { X[r2][lc] -= D[r][r2] * xr; }
-            __syncwarp();
+            const int o2 = b2 * kSub;
+            for( int ct = warp; ct < kRestChunk / kSub; ct += kTrsmThreads / 32 )
+            {
+                const int cb = ct * kSub;
+                double acc[2] = { 0.0, 0.0 };
+                dmma_8x8x8( acc, [&]( int i, int k ) { return D[o + k][o2 + i]; },
+                                 [&]( int k, int j ) { return X[o + k][cb + j]; } );
+                const int i = lane >> 2, j = 2 * (lane & 3);
+                X[o2 + i][cb + j]     -= acc[0];
+                X[o2 + i][cb + j + 1] -= acc[1];
+            }
         }
         __syncthreads();
-        for( int idx = tid; idx < nb * kTrsmCols; idx += kTrsmThreads )
+    }
+    for( int idx = tid; idx < nb * kRestChunk; idx += kTrsmThreads )
+    {
+        const int r = idx / kRestChunk, cc = idx % kRestChunk;
+        const int col = t.c0 + cc;
+        if( cc < cw )
         {
-            const int r = idx / kTrsmCols, cc = idx % kTrsmCols;
-            const int col = first + cc;
-            if( col < rest )
-            {
-                if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = X[r][cc]; }
-                else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = X[r][cc]; }
-            }
+            if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = X[r][cc]; }
+            else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = X[r][cc]; }
         }
     }
 }

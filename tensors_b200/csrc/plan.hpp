@@ -45,7 +45,7 @@ namespace tb
 
 constexpr int kPanel     = 64;    // pivot panel width
 constexpr int kTile      = 64;    // GEMM output tile (kTile x kTile)
-constexpr int kRestChunk = 256;   // columns per panel-solve CTA (one per thread)
+constexpr int kRestChunk = 64;    // rest columns per panel-solve CTA
 constexpr int kSolveRest = 64;    // rows per solve-update task
 constexpr int kLdAlign   = 4;     // row padding of every front block (entries)
 constexpr std::uint64_t kDiagFlag = 1ull << 62;   // marks diagonal entries in the assembly map
