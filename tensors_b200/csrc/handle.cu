@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <map>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -131,6 +132,9 @@ struct tb_chol
 
     cudaGraphExec_t factor_graph = nullptr;
     bool use_graph = true;
+    // captured solve sweeps on the work buffer, keyed by (which, nrhs)
+    std::map<std::pair<int,int>, cudaGraphExec_t> solve_graphs;
+    double * solve_graph_work = nullptr;
 
     // optional per-kernel timing of direct (non-graph) factorizations
     bool profiling = false;
@@ -144,10 +148,19 @@ struct tb_chol
     std::int32_t failed_sn = -1;
     std::int64_t factor_launch_count = 0;
     std::int64_t solve_launch_count = 0;
+    std::int64_t solve_sweep_launches = 0;
+
+    void drop_solve_graphs()
+    {
+        for( auto & kv : solve_graphs ) { cudaGraphExecDestroy( kv.second ); }
+        solve_graphs.clear();
+        solve_graph_work = nullptr;
+    }
 
     ~tb_chol()
     {
         for( cudaEvent_t e : events ) { cudaEventDestroy( e ); }
+        drop_solve_graphs();
         if( factor_graph ) { cudaGraphExecDestroy( factor_graph ); }
         if( own_stream && stream ) { cudaStreamDestroy( stream ); }
     }
@@ -159,6 +172,7 @@ struct tb_chol
         factorized = false;
         good = false;
         if( factor_graph ) { cudaGraphExecDestroy( factor_graph ); factor_graph = nullptr; }
+        drop_solve_graphs();
     }
 };
 
@@ -248,6 +262,7 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->diag_vals.reserve( s.n ) );
     TB_CUDA( cudaStreamSynchronize( st_ ) );
     if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    h->drop_solve_graphs();
     h->device_ready = true;
     return TB_OK;
 }
@@ -366,20 +381,13 @@ int require_factor( tb_chol * h )
     return TB_OK;
 }
 
-// which: 0 lower only, 1 upper only, 2 both.  d_B (ldB) -> d_X (ldX), device.
-int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
-                      double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+// Issues the forward (which != 1) and back (which != 0) sweeps on the
+// permuted work block W (n x k, leading dimension k); capturable.
+std::int64_t issue_sweeps( tb_chol * h, int which, double * W, std::int32_t k )
 {
     const tb::Plan & pl = h->plan;
     cudaStream_t st = h->stream;
-    const std::int32_t n = h->n;
-    const std::int32_t k = std::max( 1, nrhs );
-    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
-    TB_TRY( h->work.reserve( static_cast<std::int64_t>(n) * k ) );
-    double * W = h->work.ptr;
     std::int64_t launches = 0;
-    tb::launch_gather_rows( d_B, ldB, h->p.ptr, W, k, n, k, st );            // ReadRightHandSide
-    ++launches;
     for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
     {
         const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
@@ -402,6 +410,47 @@ int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, 
                 ++launches;
             }
         }
+    }
+    return launches;
+}
+
+// which: 0 lower only, 1 upper only, 2 both.  d_B (ldB) -> d_X (ldX), device.
+// The gather (ReadRightHandSide) and scatter (WriteSolution) run as direct
+// launches; the sweeps are captured once per (which, nrhs) into a CUDA graph
+// over the handle's work buffer.
+int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
+                      double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+{
+    cudaStream_t st = h->stream;
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    TB_TRY( h->work.reserve( static_cast<std::int64_t>(n) * k ) );
+    double * W = h->work.ptr;
+    if( h->solve_graph_work != W ) { h->drop_solve_graphs(); h->solve_graph_work = W; }
+    std::int64_t launches = 0;
+    tb::launch_gather_rows( d_B, ldB, h->p.ptr, W, k, n, k, st );            // ReadRightHandSide
+    ++launches;
+    if( h->use_graph && !h->profiling )
+    {
+        cudaGraphExec_t & g = h->solve_graphs[{ which, k }];
+        if( g == nullptr )
+        {
+            cudaGraph_t graph = nullptr;
+            TB_CUDA( cudaStreamBeginCapture( st, cudaStreamCaptureModeThreadLocal ) );
+            h->solve_sweep_launches = issue_sweeps( h, which, W, k );
+            const cudaError_t ce = cudaStreamEndCapture( st, &graph );
+            if( ce != cudaSuccess ) { h->solve_graphs.erase( { which, k } ); return fail( TB_ERR_CUDA, std::string( "graph capture: " ) + cudaGetErrorString( ce ) ); }
+            const cudaError_t ie = cudaGraphInstantiate( &g, graph, 0 );
+            cudaGraphDestroy( graph );
+            if( ie != cudaSuccess ) { h->solve_graphs.erase( { which, k } ); return fail( TB_ERR_CUDA, std::string( "graph instantiate: " ) + cudaGetErrorString( ie ) ); }
+        }
+        TB_CUDA( cudaGraphLaunch( g, st ) );
+        launches += h->solve_sweep_launches;
+    }
+    else
+    {
+        launches += issue_sweeps( h, which, W, k );
     }
     tb::launch_scatter_rows( W, k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );   // WriteSolution
     ++launches;
@@ -783,6 +832,7 @@ int tb_chol_set_stream( tb_chol * h, void * stream )
     TB_CUDA( cudaSetDevice( h->device ) );
     if( h->stream ) { TB_CUDA( cudaStreamSynchronize( h->stream ) ); }
     if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    h->drop_solve_graphs();
     if( h->own_stream && h->stream ) { cudaStreamDestroy( h->stream ); }
     if( stream == nullptr )
     {

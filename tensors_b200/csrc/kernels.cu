@@ -161,6 +161,7 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
     const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
     __shared__ double D[kPanel][kPanel + 1];
+    __shared__ double inv_d[kPanel];
     __shared__ int fail;
 
     double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
@@ -194,9 +195,11 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
                     else if( o + r < nb && !(d > 0.0) && fail < 0 ) { fail = o + r; }
                 }
                 if( (t.single_rows >> (o + r)) & 1 ) { d = fabs( d ); }
-                const double piv = sqrt( d );
-                const double inv = 1.0 / piv;
-                if( lane == r ) { a[r] = piv; }
+                // reciprocal square root and one product instead of sqrt and a
+                // division: both are long dependent sequences on the FP64 pipe
+                const double inv = rsqrt( d );
+                const double piv = d * inv;
+                if( lane == r ) { a[r] = piv; inv_d[o + r] = inv; }
                 if( lane > r ) { a[r] *= inv; }                     // U(r, lane)
 #pragma unroll
                 for( int r2 = r + 1; r2 < kSub; ++r2 )
@@ -223,7 +226,7 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
 #pragma unroll
                 for( int r = 0; r < kSub; ++r )
                 {
-                    x[r] /= D[o + r][o + r];
+                    x[r] *= inv_d[o + r];
 #pragma unroll
                     for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= D[o + r][o + r2] * x[r]; }
                 }
@@ -275,6 +278,7 @@ __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * _
     extern __shared__ double tsm[];
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( tsm );
     double (*X)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm + kPanel * (kPanel + 1) );
+    __shared__ double inv_d[kPanel];
     const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -305,6 +309,8 @@ __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * _
         X[r][cc] = v;
     }
     __syncthreads();
+    if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
+    __syncthreads();
     const int nsub = (nb + kSub - 1) / kSub;
     for( int b = 0; b < nsub; ++b )
     {
@@ -317,7 +323,7 @@ __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * _
 #pragma unroll
             for( int r = 0; r < kSub; ++r )
             {
-                x[r] /= D[o + r][o + r];
+                x[r] *= inv_d[o + r];
 #pragma unroll
                 for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= D[o + r][o + r2] * x[r]; }
             }
