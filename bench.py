@@ -196,7 +196,8 @@ def run_reference(args):
         "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded)",
-        "config": config_dict({"relres": r["relres"], "cpu_threads": threads}),
+        "config": config_dict({"cpu_sample": f"{CPU_SAMPLE_GRID}^3 grid of the same generator, GFLOP/s from its own flops",
+                               "sample_relres": r["relres"], "cpu_threads": threads}),
         "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "reference",
                          "sample": f"same generator on a {CPU_SAMPLE_GRID}^3 grid (n={CPU_SAMPLE_GRID**3}), "
                                    "one factor+solve per step"},

@@ -152,7 +152,8 @@ int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
  * doubles, out[2] levels, out[3] factorization launches, out[4] GEMM tile
  * tasks, out[5] panel tasks, out[6] extend-add tasks, out[7] forward-solve
  * launches, out[8] back-solve launches, out[9] supernodes, out[10] fronts
- * (runs of supernodes merged for computation).  Returns the
+ * (runs of supernodes merged for computation), out[11] flops of the front
+ * factorization (explicit zeros of merged fronts included).  Returns the
  * number of entries written (at most cap). */
 int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
 /* Host-side bounds check of every device task of the plan (also run before

@@ -1,0 +1,207 @@
+// tensors_b200::Sparse::CholeskyDecomposition -- header-only C++ mirror of
+// Tensors::Sparse::CholeskyDecomposition<double,int32_t,int64_t>
+// (src/Sparse/CholeskyDecomposition.hpp) over the C-ABI of tensors_b200.h.
+//
+// Member names, argument order and argument meaning follow the reference so
+// that code written against it compiles after swapping the include and the
+// namespace.  Differences:
+//  - errors throw tensors_b200::Sparse::Error (the reference prints with
+//    eprint and continues); NumericFactorization still returns 1 for a
+//    non-positive pivot, like the reference (Numeric.hpp:99);
+//  - LowerSolve solves with U^T as documented (the reference's LowerSolve
+//    runs the upper solve, Solve.hpp:290-307);
+//  - the template arguments of the reference's Solve (NRHS, parQ, op) are not
+//    needed: the right-hand-side count is a run-time argument and every solve
+//    runs on the GPU.
+// Link with tensors_b200/_tensors_b200*.so (the library built by
+// tensors_b200/build.py).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../tensors_b200.h"
+
+namespace tensors_b200 {
+namespace Sparse {
+
+class Error : public std::runtime_error
+{
+public:
+    Error( int status, const std::string & what ) : std::runtime_error( what ), status_( status ) {}
+    int Status() const noexcept { return status_; }
+private:
+    int status_;
+};
+
+inline int Check( int status )
+{
+    if( status < 0 ) { throw Error( status, tb_last_error() ); }
+    return status;
+}
+
+enum class SupernodeStrategy_T : int32_t
+{
+    Maximal = TB_SN_MAXIMAL, Fundamental = TB_SN_FUNDAMENTAL, Amalgamated = TB_SN_AMALGAMATED
+};
+
+enum class FactorizationMethod_T : int32_t
+{
+    Multifrontal = TB_MULTIFRONTAL, LeftLooking = TB_LEFT_LOOKING
+};
+
+class CholeskyDecomposition
+{
+public:
+    using Scal = double;
+    using Int  = int32_t;
+    using LInt = int64_t;
+
+    // Fill-reducing permutation p of size n (Inverse::False), ctor
+    // CholeskyDecomposition.hpp:336-346.  thread_count is used by the host
+    // symbolic phase.
+    CholeskyDecomposition( const LInt * A_outer, const Int * A_inner, const Int * p,
+                           Int n, Int thread_count )
+    {
+        Check( tb_chol_create( &h_, n, A_outer, A_inner, p, thread_count ) );
+    }
+
+    // Matrix already permuted, ctor CholeskyDecomposition.hpp:350-371.
+    CholeskyDecomposition( const LInt * A_outer, const Int * A_inner, Int n, Int thread_count )
+    {
+        Check( tb_chol_create( &h_, n, A_outer, A_inner, nullptr, thread_count ) );
+    }
+
+    ~CholeskyDecomposition() { if( h_ != nullptr ) { tb_chol_destroy( h_ ); } }
+
+    CholeskyDecomposition( const CholeskyDecomposition & ) = delete;
+    CholeskyDecomposition & operator=( const CholeskyDecomposition & ) = delete;
+    CholeskyDecomposition( CholeskyDecomposition && o ) noexcept : h_( std::exchange( o.h_, nullptr ) ) {}
+    CholeskyDecomposition & operator=( CholeskyDecomposition && o ) noexcept
+    {
+        if( this != &o )
+        {
+            if( h_ != nullptr ) { tb_chol_destroy( h_ ); }
+            h_ = std::exchange( o.h_, nullptr );
+        }
+        return *this;
+    }
+
+    // Setters, CholeskyDecomposition/InputOutput.hpp:369-409.
+    void SetSupernodeStrategy( SupernodeStrategy_T s )
+    {
+        Check( tb_chol_set_supernode_strategy( h_, static_cast<int32_t>( s ) ) );
+    }
+    void SetAmalgamationThreshold( Int t ) { Check( tb_chol_set_amalgamation_threshold( h_, t ) ); }
+    void SetFactorizationMethod( FactorizationMethod_T m )
+    {
+        Check( tb_chol_set_factorization_method( h_, static_cast<int32_t>( m ) ) );
+    }
+
+    // CholeskyDecomposition/Symbolic.hpp:3-66.
+    void SymbolicFactorization() { Check( tb_chol_symbolic( h_ ) ); }
+
+    // CholeskyDecomposition/Numeric.hpp:3-24: values in the caller's CSR
+    // order, reg added to the diagonal.  0 = success, 1 = not positive definite.
+    int NumericFactorization( const Scal * A_val, Scal reg = 0 )
+    {
+        return Check( tb_chol_numeric( h_, A_val, reg ) );
+    }
+    // Same with A_val in device memory of the handle's GPU.
+    int NumericFactorization_Device( const Scal * d_A_val, Scal reg = 0 )
+    {
+        return Check( tb_chol_numeric_device( h_, d_A_val, reg ) );
+    }
+
+    // X_out = alpha * A^{-1} B + beta * X_out, row-major n x nrhs
+    // (Solve.hpp:22-80); host pointers.
+    void Solve( Scal alpha, const Scal * B, Int ldB, Scal beta, Scal * X_out, Int ldX, Int nrhs = 1 )
+    {
+        Check( tb_chol_solve( h_, alpha, B, ldB, beta, X_out, ldX, nrhs ) );
+    }
+    // X_out = A^{-1} B, Solve.hpp:87-99.
+    void Solve( const Scal * B, Scal * X_out, Int nrhs = 1 )
+    {
+        Solve( 1.0, B, nrhs, 0.0, X_out, nrhs, nrhs );
+    }
+    // Same on device buffers of the handle's GPU and stream.
+    void Solve_Device( Scal alpha, const Scal * d_B, Int ldB, Scal beta, Scal * d_X, Int ldX, Int nrhs = 1 )
+    {
+        Check( tb_chol_solve_device( h_, alpha, d_B, ldB, beta, d_X, ldX, nrhs ) );
+    }
+
+    // X_out = alpha * P^T U^{-1} P B + beta * X_out (Solve.hpp:182-245).
+    void UpperSolve( Scal alpha, const Scal * B, Int ldB, Scal beta, Scal * X_out, Int ldX, Int nrhs = 1 )
+    {
+        Check( tb_chol_upper_solve( h_, alpha, B, ldB, beta, X_out, ldX, nrhs ) );
+    }
+    // X_out = alpha * P^T U^{-T} P B + beta * X_out (Solve.hpp:251-310, documented meaning).
+    void LowerSolve( Scal alpha, const Scal * B, Int ldB, Scal beta, Scal * X_out, Int ldX, Int nrhs = 1 )
+    {
+        Check( tb_chol_lower_solve( h_, alpha, B, ldB, beta, X_out, ldX, nrhs ) );
+    }
+
+    // Queries, CholeskyDecomposition/InputOutput.hpp:85-367 and Numeric.hpp:183-215.
+    Int RowCount() const { Int v = 0; Check( tb_chol_row_count( h_, &v ) ); return v; }
+    Int ColCount() const { return RowCount(); }
+    LInt NonzeroCount() const { LInt v = 0; Check( tb_chol_nonzero_count( h_, &v ) ); return v; }
+    Int SN_Count() const { Int v = 0; Check( tb_chol_sn_count( h_, &v ) ); return v; }
+
+    bool NumericallyFactorizedQ() const { int32_t f = 0, g = 0; Check( tb_chol_factorized( h_, &f, &g ) ); return f != 0; }
+    bool NumericallyGoodQ() const { int32_t f = 0, g = 0; Check( tb_chol_factorized( h_, &f, &g ) ); return g != 0; }
+    Int FailedSupernode() const { Int v = -1; Check( tb_chol_failed_supernode( h_, &v ) ); return v; }
+
+    LInt RequiredTriangularSize() const { LInt t = 0, r = 0; Check( tb_chol_factor_sizes( h_, &t, &r ) ); return t; }
+    LInt RequiredRectangularSize() const { LInt t = 0, r = 0; Check( tb_chol_factor_sizes( h_, &t, &r ) ); return r; }
+
+    std::vector<Int>  SN_RowPointers() const       { return Array<Int>( TB_ARRAY_SN_RP ); }
+    std::vector<LInt> SN_Outer() const             { return Array<LInt>( TB_ARRAY_SN_OUTER ); }
+    std::vector<Int>  SN_Inner() const             { return Array<Int>( TB_ARRAY_SN_INNER ); }
+    std::vector<Int>  RowToSN() const              { return Array<Int>( TB_ARRAY_ROW_TO_SN ); }
+    std::vector<LInt> SN_TrianglePointers() const  { return Array<LInt>( TB_ARRAY_SN_TRI_PTR ); }
+    std::vector<LInt> SN_RectanglePointers() const { return Array<LInt>( TB_ARRAY_SN_REC_PTR ); }
+    std::vector<Int>  Permutation() const          { return Array<Int>( TB_ARRAY_PERM ); }
+    std::vector<Int>  InversePermutation() const   { return Array<Int>( TB_ARRAY_PERM_INV ); }
+    std::vector<LInt> ValuePermutation() const     { return Array<LInt>( TB_ARRAY_VALUE_PERM ); }
+    std::vector<Int>  AssemblyTreeParents() const  { return Array<Int>( TB_ARRAY_ATREE_PARENTS ); }
+    std::vector<Int>  EliminationTreeParents() const { return Array<Int>( TB_ARRAY_ETREE_PARENTS ); }
+
+    // SN_TriangleValues / SN_RectangleValues (InputOutput.hpp:322-352),
+    // copied back from the device in the reference's layout.
+    std::pair<std::vector<Scal>, std::vector<Scal>> FactorValues() const
+    {
+        std::pair<std::vector<Scal>, std::vector<Scal>> out;
+        out.first.resize( static_cast<size_t>( RequiredTriangularSize() ) );
+        out.second.resize( static_cast<size_t>( RequiredRectangularSize() ) );
+        Check( tb_chol_factor_values( h_, out.first.data(), out.second.data() ) );
+        return out;
+    }
+
+    // LogDeterminant (InputOutput.hpp:294-297), WriteFactorDiagonal (:238-257).
+    Scal LogDeterminant() const { Scal v = 0; Check( tb_chol_log_det( h_, &v ) ); return v; }
+    void WriteFactorDiagonal( Scal * diag ) const { Check( tb_chol_factor_diagonal( h_, diag ) ); }
+
+    // Stream of the handle (a cudaStream_t).
+    void SetStream( void * stream ) { Check( tb_chol_set_stream( h_, stream ) ); }
+
+    tb_chol * Handle() const noexcept { return h_; }
+
+private:
+    template<typename T>
+    std::vector<T> Array( int32_t which ) const
+    {
+        int64_t size = 0;
+        Check( tb_chol_array_size( h_, which, &size ) );
+        std::vector<int64_t> tmp( static_cast<size_t>( size ) );
+        Check( tb_chol_array_copy( h_, which, tmp.data() ) );
+        return std::vector<T>( tmp.begin(), tmp.end() );
+    }
+
+    tb_chol * h_ = nullptr;
+};
+
+} // namespace Sparse
+} // namespace tensors_b200

@@ -309,7 +309,7 @@ class CholeskyDecomposition:
         out = np.zeros(16, dtype=np.int64)
         m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 16))
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
-                "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts"]
+                "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

@@ -795,7 +795,8 @@ int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
         pl.arena_size(), pl.v_size, pl.levels, static_cast<std::int64_t>( pl.factor_launches.size() ) + 2,
         static_cast<std::int64_t>( pl.gemm.size() ), static_cast<std::int64_t>( pl.panel.size() ),
         static_cast<std::int64_t>( pl.extend.size() ), static_cast<std::int64_t>( pl.lower_launches.size() ),
-        static_cast<std::int64_t>( pl.upper_launches.size() ), h->sym.sn_count, pl.front_count };
+        static_cast<std::int64_t>( pl.upper_launches.size() ), h->sym.sn_count, pl.front_count,
+        static_cast<std::int64_t>( pl.front_flops ) };
     const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
     for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
     return m;

@@ -1,0 +1,66 @@
+// Exercises the C++ mirror class (include/tensors_b200/CholeskyDecomposition.hpp)
+// the way a user of the reference's Sparse::CholeskyDecomposition would:
+// 2D 5-point Laplacian on a g x g grid (+ shift), reversed ordering as the
+// fill-reducing permutation, symbolic phase, and with "numeric" as second
+// argument a factorization and a 3-RHS solve whose relative residual is
+// printed.  Output: "sn_count <S>" [ "status <0|1>" "relres <r>" ].
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "tensors_b200/CholeskyDecomposition.hpp"
+
+using tensors_b200::Sparse::CholeskyDecomposition;
+
+int main( int argc, char ** argv )
+{
+    const int g = argc > 1 ? std::atoi( argv[1] ) : 20;
+    const bool numeric = argc > 2 && std::string( argv[2] ) == "numeric";
+    const int n = g * g;
+    std::vector<int64_t> outer( 1, 0 );
+    std::vector<int32_t> inner;
+    std::vector<double> val;
+    for( int i = 0; i < g; ++i )
+    {
+        for( int j = 0; j < g; ++j )
+        {
+            const int r = i * g + j;
+            auto add = [&]( int c, double v ) { inner.push_back( c ); val.push_back( v ); };
+            if( i > 0 )     { add( r - g, -1.0 ); }
+            if( j > 0 )     { add( r - 1, -1.0 ); }
+            add( r, 4.0 + 1e-2 );
+            if( j + 1 < g ) { add( r + 1, -1.0 ); }
+            if( i + 1 < g ) { add( r + g, -1.0 ); }
+            outer.push_back( static_cast<int64_t>( inner.size() ) );
+        }
+    }
+    std::vector<int32_t> p( n );
+    for( int i = 0; i < n; ++i ) { p[i] = n - 1 - i; }
+
+    CholeskyDecomposition S( outer.data(), inner.data(), p.data(), n, 1 );
+    S.SymbolicFactorization();
+    std::printf( "sn_count %d\n", S.SN_Count() );
+    if( !numeric ) { return 0; }
+
+    const int status = S.NumericFactorization( val.data(), 0.0 );
+    std::printf( "status %d\n", status );
+    const int nrhs = 3;
+    std::vector<double> B( static_cast<size_t>( n ) * nrhs ), X( B.size() );
+    for( size_t k = 0; k < B.size(); ++k ) { B[k] = std::sin( 0.37 * static_cast<double>( k ) ); }
+    S.Solve( B.data(), X.data(), nrhs );
+    double rn = 0.0, bn = 0.0;
+    for( int r = 0; r < n; ++r )
+    {
+        for( int k = 0; k < nrhs; ++k )
+        {
+            double ax = 0.0;
+            for( int64_t l = outer[r]; l < outer[r + 1]; ++l ) { ax += val[l] * X[inner[l] * nrhs + k]; }
+            const double d = B[r * nrhs + k] - ax;
+            rn += d * d;
+            bn += B[r * nrhs + k] * B[r * nrhs + k];
+        }
+    }
+    std::printf( "relres %.3e\n", std::sqrt( rn / bn ) );
+    return 0;
+}
