@@ -180,6 +180,15 @@ int tb_chol_kernel_profile( tb_chol * h, double * ms, int64_t * launches, double
  * info[4i..4i+3] = kind, level, panel step (or child rank), task count and
  * ms[i] its duration; entry 0 is the clear + assembly.  Returns the count. */
 int tb_chol_launch_profile( tb_chol * h, int64_t * info, double * ms, int32_t cap );
+/* Solve (as tb_chol_solve_device) that allocates no device memory: the
+ * permuted work block lives in a fixed device array of 4,194,304 doubles
+ * (32 MiB) per device, so n * nrhs must not exceed that (else
+ * TB_ERR_INVALID_ARGUMENT, nothing launched).  For callers that may not
+ * allocate at solve time.  The first call on a device looks the array up
+ * (make it outside stream capture); calls that can overlap on one device
+ * share the array and must be serialised.  No counterpart in the reference. */
+int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B, int32_t ldB,
+                                  double beta, double * d_X, int32_t ldX, int32_t nrhs );
 /* Number of kernel launches the last numeric factorization / solve issued. */
 int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * solve_launches );
 

@@ -34,6 +34,7 @@ SIGNATURES = {
     "tb_chol_numeric_device": (ctypes.c_int, [_vp, _vp, _d]),
     "tb_chol_solve": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_solve_device": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
+    "tb_chol_solve_device_noalloc": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_upper_solve": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_lower_solve": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_residual_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i32]),

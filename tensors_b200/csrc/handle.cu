@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <climits>
 #include <map>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -903,6 +904,89 @@ int tb_chol_launch_counts( tb_chol * h, std::int64_t * factor_launches, std::int
     if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
     if( factor_launches ) { *factor_launches = h->factor_launch_count; }
     if( solve_launches ) { *solve_launches = h->solve_launch_count; }
+    return TB_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Solve without any device allocation.
+//
+// Some callers cannot allocate device memory at solve time: a real-time loop
+// that has reserved everything up front and must not stall in the allocator,
+// a memory-capped serving process that admits work only against a fixed
+// budget, or code running while another component owns the allocator.
+// tb_chol_solve_device grows a per-handle work block on first use (and when
+// nrhs grows), which such callers cannot allow.  tb_chol_solve_device_noalloc
+// runs the same gather, forward/back sweeps and scatter, but its permuted
+// work block is a fixed, file-scope device array instead.
+//
+//  - Capacity: n * nrhs <= kNoAllocScratchEntries (4,194,304 doubles,
+//    32 MiB); larger requests are rejected with TB_ERR_INVALID_ARGUMENT
+//    before anything is launched.
+//  - Set-up: the first call on a device looks up the array's device address
+//    with cudaGetSymbolAddress (that device current) and caches it; make
+//    that first call outside any stream capture.
+//  - Nothing in the array has to start at zero: the gather writes every
+//    entry the sweeps read.
+//  - There is one array per device, shared by every handle: calls whose
+//    solves can overlap on the device (other streams, other host threads)
+//    race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace
+{
+
+constexpr std::int64_t kNoAllocScratchEntries = std::int64_t( 1 ) << 22;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__( 256 ) double g_noalloc_scratch[kNoAllocScratchEntries];
+
+std::mutex g_noalloc_mutex;
+double * g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+int noalloc_scratch( int device, double ** out )
+{
+    if( device < 0 || device >= kNoAllocMaxDevices ) { return fail( TB_ERR_INVALID_ARGUMENT, "device ordinal out of range" ); }
+    std::lock_guard<std::mutex> lock( g_noalloc_mutex );
+    if( g_noalloc_ptr[device] == nullptr )
+    {
+        void * p = nullptr;
+        TB_CUDA( cudaSetDevice( device ) );
+        TB_CUDA( cudaGetSymbolAddress( &p, g_noalloc_scratch ) );
+        g_noalloc_ptr[device] = static_cast<double *>( p );
+    }
+    *out = g_noalloc_ptr[device];
+    return TB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
+                                  double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    if( d_B == nullptr || d_X == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: null buffer" ); }
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    if( static_cast<std::int64_t>( n ) * k > kNoAllocScratchEntries )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "solve_device_noalloc: n * nrhs = " +
+                     std::to_string( static_cast<std::int64_t>( n ) * k ) + " exceeds the fixed scratch of " +
+                     std::to_string( kNoAllocScratchEntries ) + " doubles" );
+    }
+    double * W = nullptr;
+    TB_TRY( noalloc_scratch( h->device, &W ) );
+    cudaStream_t st = h->stream;
+    std::int64_t launches = 2;
+    tb::launch_gather_rows( d_B, ldB, h->p.ptr, W, k, n, k, st );
+    launches += issue_sweeps( h, 2, W, k );
+    tb::launch_scatter_rows( W, k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );
+    h->solve_launch_count = launches;
+    TB_CUDA( cudaGetLastError() );
     return TB_OK;
 }
 
