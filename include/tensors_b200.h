@@ -170,8 +170,8 @@ int tb_chol_set_stream( tb_chol * h, void * stream );
 int tb_chol_set_graph( tb_chol * h, int32_t enabled );
 /* Per-kernel timing: when enabled, factorizations run as direct launches
  * bracketed by CUDA events and tb_chol_kernel_profile reports, per launch
- * kind (0 zero, 1 extend-add, 2 panel trsm, 3 GEMM tiles, 6 panel potrf,
- * 7 clear + assembly),
+ * kind (0 zero, 1 extend-add, 2 panel trsm, 3 GEMM tiles, 4 inversion of
+ * the diagonal blocks for the solves, 6 panel potrf, 7 clear + assembly),
  * the milliseconds and launches of the last factorization and the
  * algorithmic flops of the GEMM tiles (8 entries each). */
 int tb_chol_set_profiling( tb_chol * h, int32_t enabled );
@@ -180,15 +180,19 @@ int tb_chol_kernel_profile( tb_chol * h, double * ms, int64_t * launches, double
  * info[4i..4i+3] = kind, level, panel step (or child rank), task count and
  * ms[i] its duration; entry 0 is the clear + assembly.  Returns the count. */
 int tb_chol_launch_profile( tb_chol * h, int64_t * info, double * ms, int32_t cap );
-/* Solve (as tb_chol_solve_device) that allocates no device memory: the
- * permuted work block lives in a fixed device array of 4,194,304 doubles
- * (32 MiB) per device, so n * nrhs must not exceed that (else
+/* Solve (as tb_chol_solve_device) that allocates no device memory: its two
+ * permuted work blocks live in a fixed device array of 2 x 4,194,304 doubles
+ * (64 MiB) per device, so n * nrhs must not exceed 4,194,304 (else
  * TB_ERR_INVALID_ARGUMENT, nothing launched).  For callers that may not
  * allocate at solve time.  The first call on a device looks the array up
  * (make it outside stream capture); calls that can overlap on one device
  * share the array and must be serialised.  No counterpart in the reference. */
 int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B, int32_t ldB,
                                   double beta, double * d_X, int32_t ldX, int32_t nrhs );
+/* Per launch of the last solve run with profiling enabled (at most cap
+ * entries): info[4i..4i+3] = sweep (0 forward, 1 back), level, panel step,
+ * task count and ms[i] its duration.  Returns the count. */
+int tb_chol_solve_profile( tb_chol * h, int64_t * info, double * ms, int32_t cap );
 /* Number of kernel launches the last numeric factorization / solve issued. */
 int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * solve_launches );
 

@@ -55,6 +55,7 @@ SIGNATURES = {
     "tb_chol_check_plan": (ctypes.c_int, [_vp]),
     "tb_chol_set_stream": (ctypes.c_int, [_vp, _vp]),
     "tb_chol_set_graph": (ctypes.c_int, [_vp, _i32]),
+    "tb_chol_solve_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
     "tb_chol_launch_counts": (ctypes.c_int, [_vp, _pi64, _pi64]),
     "tb_chol_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_kernel_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp]),

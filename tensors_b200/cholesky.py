@@ -330,7 +330,7 @@ class CholeskyDecomposition:
         ln = np.zeros(8, dtype=np.int64)
         fl = np.zeros(8)
         _check(lib().tb_chol_kernel_profile(self._h, ms.ctypes.data, ln.ctypes.data, fl.ctypes.data))
-        names = {0: "zero", 1: "extend", 2: "trsm", 3: "gemm", 6: "potrf", 7: "assemble"}
+        names = {0: "zero", 1: "extend", 2: "trsm", 3: "gemm", 4: "invert", 6: "potrf", 7: "assemble"}
         return {names[k]: {"ms": float(ms[k]), "launches": int(ln[k]), "flops": float(fl[k])} for k in names}
 
     def LaunchProfile(self):
@@ -339,9 +339,18 @@ class CholeskyDecomposition:
         info = np.zeros(4 * cap, dtype=np.int64)
         ms = np.zeros(cap)
         m = _check(lib().tb_chol_launch_profile(self._h, info.ctypes.data, ms.ctypes.data, cap))
-        names = {0: "zero", 1: "extend", 2: "trsm", 3: "gemm", 6: "potrf", 7: "assemble"}
+        names = {0: "zero", 1: "extend", 2: "trsm", 3: "gemm", 4: "invert", 6: "potrf", 7: "assemble"}
         return [(names.get(int(info[4 * i]), "?"), int(info[4 * i + 1]), int(info[4 * i + 2]), int(info[4 * i + 3]),
                  float(ms[i])) for i in range(m)]
+
+    def SolveProfile(self):
+        """Per launch of the last profiled solve: (sweep, level, step, tasks, ms), sweep 0 forward / 1 back."""
+        cap = 1 << 16
+        info = np.zeros(4 * cap, dtype=np.int64)
+        ms = np.zeros(cap)
+        m = _check(lib().tb_chol_solve_profile(self._h, info.ctypes.data, ms.ctypes.data, cap))
+        return [(int(info[4 * i]), int(info[4 * i + 1]), int(info[4 * i + 2]), int(info[4 * i + 3]), float(ms[i]))
+                for i in range(m)]
 
     def LaunchCounts(self):
         a, b = ctypes.c_int64(), ctypes.c_int64()

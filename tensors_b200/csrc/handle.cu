@@ -128,14 +128,16 @@ struct tb_chol
     DeviceArray<double>             values;      // caller-order values of the last factorization
     DeviceArray<double>             reg;
     DeviceArray<int>                status;
-    DeviceArray<double>             work, in, out, diag_vals;
+    DeviceArray<double>             work, work2, in, out, diag_vals;
+    DeviceArray<double>             tinv;        // inverse diagonal block of every panel (64 x 64 each)
     PinnedBuffer                    pin_in, pin_out, pin_small;
 
     cudaGraphExec_t factor_graph = nullptr;
     bool use_graph = true;
-    // captured solve sweeps on the work buffer, keyed by (which, nrhs)
+    // captured solve sweeps on the work buffers, keyed by (which, nrhs)
     std::map<std::pair<int,int>, cudaGraphExec_t> solve_graphs;
     double * solve_graph_work = nullptr;
+    double * solve_graph_work2 = nullptr;
 
     // optional per-kernel timing of direct (non-graph) factorizations
     bool profiling = false;
@@ -143,6 +145,9 @@ struct tb_chol
     std::int64_t kind_launches[8] = {};
     std::vector<cudaEvent_t> events;
     std::vector<float> launch_ms;          // per factor launch of the last profiled run (0 = clear + assembly)
+    std::vector<cudaEvent_t> solve_events;
+    std::vector<std::int64_t> solve_info;  // per solve launch of the last profiled solve: upper, level, step, tasks
+    std::vector<float> solve_ms;
 
     bool factorized = false;
     bool good = false;
@@ -156,11 +161,13 @@ struct tb_chol
         for( auto & kv : solve_graphs ) { cudaGraphExecDestroy( kv.second ); }
         solve_graphs.clear();
         solve_graph_work = nullptr;
+        solve_graph_work2 = nullptr;
     }
 
     ~tb_chol()
     {
         for( cudaEvent_t e : events ) { cudaEventDestroy( e ); }
+        for( cudaEvent_t e : solve_events ) { cudaEventDestroy( e ); }
         drop_solve_graphs();
         if( factor_graph ) { cudaGraphExecDestroy( factor_graph ); }
         if( own_stream && stream ) { cudaStreamDestroy( stream ); }
@@ -261,6 +268,7 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->status.reserve( 2 ) );
     TB_TRY( h->diag_off.upload( pl.diag_offset, st_ ) );
     TB_TRY( h->diag_vals.reserve( s.n ) );
+    TB_TRY( h->tinv.reserve( static_cast<std::int64_t>( pl.sdiag.size() ) * tb::kPanel * tb::kPanel ) );
     TB_CUDA( cudaStreamSynchronize( st_ ) );
     if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
     h->drop_solve_graphs();
@@ -300,6 +308,7 @@ std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * k
             case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, st ); break;
             case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
             case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
+            case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
             default: break;
         }
         mark( static_cast<int>( L.kind ) );
@@ -382,32 +391,54 @@ int require_factor( tb_chol * h )
     return TB_OK;
 }
 
-// Issues the forward (which != 1) and back (which != 0) sweeps on the
-// permuted work block W (n x k, leading dimension k); capturable.
-std::int64_t issue_sweeps( tb_chol * h, int which, double * W, std::int32_t k )
+// Issues the forward (which != 1) and back (which != 0) sweeps over two
+// permuted n x k blocks (leading dimension k); capturable.  The right-hand
+// side is expected in W for which 0 and 2 and in Y for which 1; the result
+// is left in sweep_result( which, W, Y ).  The back sweep accumulates into W,
+// which it clears first.
+// With `timed`, every launch is bracketed by the handle's solve events and
+// described in solve_info (the events must exist).
+std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::int32_t k, bool timed = false )
 {
     const tb::Plan & pl = h->plan;
     cudaStream_t st = h->stream;
     std::int64_t launches = 0;
-    for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
+    std::size_t ev = 0;
+    auto begin = [&]() { if( timed ) { cudaEventRecord( h->solve_events[ev++], st ); } };
+    auto end = [&]( const tb::Launch & L, int upper )
     {
-        const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
-        double * Wc = W + c0;
-        if( which != 1 )
+        if( !timed ) { return; }
+        cudaEventRecord( h->solve_events[ev++], st );
+        h->solve_info.insert( h->solve_info.end(), { upper, L.level, L.step, L.count } );
+    };
+    if( timed ) { h->solve_info.clear(); }
+    if( which != 1 )
+    {
+        for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
+            const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
             for( const tb::Launch & L : pl.lower_launches )
             {
-                if( L.kind == tb::LaunchKind::SolveDiag ) { tb::launch_solve_diag( h->sdiag.ptr + L.first, L.count, false, h->arena.ptr, Wc, k, kc, st ); }
-                else { tb::launch_solve_rest( h->srest.ptr + L.first, L.count, false, h->arena.ptr, h->sn_inner.ptr, Wc, k, kc, st ); }
+                begin();
+                tb::launch_solve_step( h->srest.ptr + L.first, L.count, false, h->arena.ptr, h->tinv.ptr, h->sn_inner.ptr,
+                                       W + c0, Y + c0, k, kc, st );
+                end( L, 0 );
                 ++launches;
             }
         }
-        if( which != 0 )
+    }
+    if( which != 0 )
+    {
+        cudaMemsetAsync( W, 0, sizeof(double) * static_cast<size_t>( h->n ) * k, st );
+        for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
+            const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
             for( const tb::Launch & L : pl.upper_launches )
             {
-                if( L.kind == tb::LaunchKind::SolveDiag ) { tb::launch_solve_diag( h->sdiag.ptr + L.first, L.count, true, h->arena.ptr, Wc, k, kc, st ); }
-                else { tb::launch_solve_rest( h->srest.ptr + L.first, L.count, true, h->arena.ptr, h->sn_inner.ptr, Wc, k, kc, st ); }
+                begin();
+                tb::launch_solve_step( h->srest.ptr + L.first, L.count, true, h->arena.ptr, h->tinv.ptr, h->sn_inner.ptr,
+                                       Y + c0, W + c0, k, kc, st );
+                end( L, 1 );
                 ++launches;
             }
         }
@@ -415,10 +446,13 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, std::int32_t k )
     return launches;
 }
 
+double * sweep_input( int which, double * W, double * Y ) { return which == 1 ? Y : W; }
+double * sweep_result( int which, double * W, double * Y ) { return which == 0 ? Y : W; }
+
 // which: 0 lower only, 1 upper only, 2 both.  d_B (ldB) -> d_X (ldX), device.
 // The gather (ReadRightHandSide) and scatter (WriteSolution) run as direct
 // launches; the sweeps are captured once per (which, nrhs) into a CUDA graph
-// over the handle's work buffer.
+// over the handle's work buffers.
 int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
                       double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
 {
@@ -427,10 +461,17 @@ int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, 
     const std::int32_t k = std::max( 1, nrhs );
     if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
     TB_TRY( h->work.reserve( static_cast<std::int64_t>(n) * k ) );
+    TB_TRY( h->work2.reserve( static_cast<std::int64_t>(n) * k ) );
     double * W = h->work.ptr;
-    if( h->solve_graph_work != W ) { h->drop_solve_graphs(); h->solve_graph_work = W; }
+    double * Y = h->work2.ptr;
+    if( h->solve_graph_work != W || h->solve_graph_work2 != Y )
+    {
+        h->drop_solve_graphs();
+        h->solve_graph_work = W;
+        h->solve_graph_work2 = Y;
+    }
     std::int64_t launches = 0;
-    tb::launch_gather_rows( d_B, ldB, h->p.ptr, W, k, n, k, st );            // ReadRightHandSide
+    tb::launch_gather_rows( d_B, ldB, h->p.ptr, sweep_input( which, W, Y ), k, n, k, st );   // ReadRightHandSide
     ++launches;
     if( h->use_graph && !h->profiling )
     {
@@ -439,7 +480,7 @@ int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, 
         {
             cudaGraph_t graph = nullptr;
             TB_CUDA( cudaStreamBeginCapture( st, cudaStreamCaptureModeThreadLocal ) );
-            h->solve_sweep_launches = issue_sweeps( h, which, W, k );
+            h->solve_sweep_launches = issue_sweeps( h, which, W, Y, k );
             const cudaError_t ce = cudaStreamEndCapture( st, &graph );
             if( ce != cudaSuccess ) { h->solve_graphs.erase( { which, k } ); return fail( TB_ERR_CUDA, std::string( "graph capture: " ) + cudaGetErrorString( ce ) ); }
             const cudaError_t ie = cudaGraphInstantiate( &g, graph, 0 );
@@ -449,11 +490,31 @@ int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, 
         TB_CUDA( cudaGraphLaunch( g, st ) );
         launches += h->solve_sweep_launches;
     }
+    else if( h->profiling )
+    {
+        const std::int32_t chunks = (k + tb::kSolveMaxRhs - 1) / tb::kSolveMaxRhs;
+        const std::size_t need = 2 * static_cast<std::size_t>( chunks ) * (h->plan.lower_launches.size() + h->plan.upper_launches.size());
+        while( h->solve_events.size() < need )
+        {
+            cudaEvent_t e;
+            TB_CUDA( cudaEventCreate( &e ) );
+            h->solve_events.push_back( e );
+        }
+        launches += issue_sweeps( h, which, W, Y, k, true );
+        TB_CUDA( cudaStreamSynchronize( st ) );
+        h->solve_ms.clear();
+        for( std::size_t i = 0; i < h->solve_info.size() / 4; ++i )
+        {
+            float ms = 0.0f;
+            TB_CUDA( cudaEventElapsedTime( &ms, h->solve_events[2 * i], h->solve_events[2 * i + 1] ) );
+            h->solve_ms.push_back( ms );
+        }
+    }
     else
     {
-        launches += issue_sweeps( h, which, W, k );
+        launches += issue_sweeps( h, which, W, Y, k );
     }
-    tb::launch_scatter_rows( W, k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );   // WriteSolution
+    tb::launch_scatter_rows( sweep_result( which, W, Y ), k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );   // WriteSolution
     ++launches;
     h->solve_launch_count = launches;
     TB_CUDA( cudaGetLastError() );
@@ -823,7 +884,7 @@ int tb_chol_device_bytes( tb_chol * h, std::int64_t * out )
     b += h->srest.size * (std::int64_t)sizeof(tb::SolveRestTask) + h->a_outer.size * 8;
     b += h->zero.size * (std::int64_t)sizeof(tb::ZeroTask) + h->exports.size * (std::int64_t)sizeof(tb::ExportTask);
     b += h->colmap.size * 4 + h->exported.size * 8;
-    b += (h->values.size + h->work.size + h->in.size + h->out.size + h->diag_vals.size) * 8;
+    b += (h->values.size + h->work.size + h->work2.size + h->in.size + h->out.size + h->diag_vals.size + h->tinv.size) * 8;
     *out = b;
     return TB_OK;
 }
@@ -899,6 +960,18 @@ int tb_chol_launch_profile( tb_chol * h, std::int64_t * info, double * ms, std::
     return m;
 }
 
+int tb_chol_solve_profile( tb_chol * h, std::int64_t * info, double * ms, std::int32_t cap )
+{
+    if( h == nullptr || cap < 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
+    const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( h->solve_ms.size() ) );
+    for( std::int32_t i = 0; i < m; ++i )
+    {
+        if( info ) { for( int j = 0; j < 4; ++j ) { info[4 * i + j] = h->solve_info[static_cast<size_t>( 4 * i + j )]; } }
+        if( ms ) { ms[i] = h->solve_ms[static_cast<size_t>( i )]; }
+    }
+    return m;
+}
+
 int tb_chol_launch_counts( tb_chol * h, std::int64_t * factor_launches, std::int64_t * solve_launches )
 {
     if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
@@ -919,16 +992,17 @@ int tb_chol_launch_counts( tb_chol * h, std::int64_t * factor_launches, std::int
 // tb_chol_solve_device grows a per-handle work block on first use (and when
 // nrhs grows), which such callers cannot allow.  tb_chol_solve_device_noalloc
 // runs the same gather, forward/back sweeps and scatter, but its permuted
-// work block is a fixed, file-scope device array instead.
+// two work blocks are one fixed, file-scope device array instead.
 //
-//  - Capacity: n * nrhs <= kNoAllocScratchEntries (4,194,304 doubles,
-//    32 MiB); larger requests are rejected with TB_ERR_INVALID_ARGUMENT
-//    before anything is launched.
+//  - Capacity: n * nrhs <= kNoAllocScratchEntries (4,194,304 doubles per
+//    block, 64 MiB for both); larger requests are rejected with
+//    TB_ERR_INVALID_ARGUMENT before anything is launched.
 //  - Set-up: the first call on a device looks up the array's device address
 //    with cudaGetSymbolAddress (that device current) and caches it; make
 //    that first call outside any stream capture.
 //  - Nothing in the array has to start at zero: the gather writes every
-//    entry the sweeps read.
+//    entry the forward sweep reads, and the back sweep clears the block it
+//    accumulates into.
 //  - There is one array per device, shared by every handle: calls whose
 //    solves can overlap on the device (other streams, other host threads)
 //    race on it and must be serialised by the caller.
@@ -939,7 +1013,7 @@ namespace
 constexpr std::int64_t kNoAllocScratchEntries = std::int64_t( 1 ) << 22;
 constexpr int kNoAllocMaxDevices = 64;
 
-static __device__ __align__( 256 ) double g_noalloc_scratch[kNoAllocScratchEntries];
+static __device__ __align__( 256 ) double g_noalloc_scratch[2 * kNoAllocScratchEntries];
 
 std::mutex g_noalloc_mutex;
 double * g_noalloc_ptr[kNoAllocMaxDevices] = {};
@@ -976,14 +1050,15 @@ int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B,
     {
         return fail( TB_ERR_INVALID_ARGUMENT, "solve_device_noalloc: n * nrhs = " +
                      std::to_string( static_cast<std::int64_t>( n ) * k ) + " exceeds the fixed scratch of " +
-                     std::to_string( kNoAllocScratchEntries ) + " doubles" );
+                     std::to_string( kNoAllocScratchEntries ) + " doubles per block" );
     }
     double * W = nullptr;
     TB_TRY( noalloc_scratch( h->device, &W ) );
+    double * Y = W + kNoAllocScratchEntries;
     cudaStream_t st = h->stream;
     std::int64_t launches = 2;
     tb::launch_gather_rows( d_B, ldB, h->p.ptr, W, k, n, k, st );
-    launches += issue_sweeps( h, 2, W, k );
+    launches += issue_sweeps( h, 2, W, Y, k );
     tb::launch_scatter_rows( W, k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );
     h->solve_launch_count = launches;
     TB_CUDA( cudaGetLastError() );

@@ -21,13 +21,31 @@ constexpr int kGemmK        = 16;
 constexpr int kGemmLd       = kTile + 4;   // padded smem row (2 wavefronts per fragment load)
 constexpr int kPanelThreads = kRestChunk;
 constexpr int kSolveThreads = 256;
-constexpr int kMaxRhs       = kSolveMaxRhs;   // columns per solve launch
 
 __device__ __forceinline__ void dmma_8x8x4( double (&d)[2], double a, double b )
 {
     asm volatile( "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                   : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b) );
 }
+
+__device__ __forceinline__ void cp_async_16( double * smem_dst, const double * gmem_src, int src_bytes )
+{
+    const unsigned saddr = static_cast<unsigned>( __cvta_generic_to_shared( smem_dst ) );
+    asm volatile( "cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(saddr), "l"(gmem_src), "r"(src_bytes) );
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile( "cp.async.commit_group;\n" ::: "memory" ); }
+template<int N> __device__ __forceinline__ void cp_async_wait() { asm volatile( "cp.async.wait_group %0;\n" :: "n"(N) : "memory" ); }
+
+// 8-byte asynchronous copy global -> shared, zero-filled when !valid (the
+// source address is then not read, but must still be a mapped address).
+// Tile loads are issued this way so that all of a thread's copies are in
+// flight at once instead of one load-then-store round trip per element.
+__device__ __forceinline__ void cp_async_8( double * smem_dst, const double * gmem_src, bool valid )
+{
+    const unsigned saddr = static_cast<unsigned>( __cvta_generic_to_shared( smem_dst ) );
+    asm volatile( "cp.async.ca.shared.global [%0], [%1], 8, %2;\n" :: "r"(saddr), "l"(gmem_src), "r"(valid ? 8 : 0) );
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile( "cp.async.wait_all;\n" ::: "memory" ); }
 
 // ---------------------------------------------------------------- assembly
 // arena[dst] = values[src] (+ reg on the diagonal): ReadNonzeroValues
@@ -165,14 +183,19 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
     __shared__ int fail;
 
     double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
+#pragma unroll 4
     for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
     {
         const int r = idx / kPanel, c = idx % kPanel;
-        double v = (r == c) ? 1.0 : 0.0;                 // identity padding beyond nb
-        if( r < nb && c < nb && r <= c ) { v = U0[(std::int64_t)r * t.ld0 + c]; }
-        D[r][c] = v;
+        if( r >= nb && r == c ) { D[r][c] = 1.0; }      // identity padding beyond nb
+        else
+        {
+            const bool valid = r < nb && c < nb && r <= c;
+            cp_async_8( &D[r][c], valid ? U0 + (std::int64_t)r * t.ld0 + c : U0, valid );
+        }
     }
     if( tid == 0 ) { fail = -1; }
+    cp_async_wait_all();
     __syncthreads();
 
     const int nsub = (nb + kSub - 1) / kSub;
@@ -289,25 +312,33 @@ __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * _
     const int cw = min( kRestChunk, rest - t.c0 );
     double * U0 = arena + t.u0;
     double * U1 = arena + t.u1;
+#pragma unroll 4
     for( int idx = tid; idx < kPanel * kPanel; idx += kTrsmThreads )
     {
         const int r = idx / kPanel, c = idx % kPanel;
-        double v = (r == c) ? 1.0 : 0.0;
-        if( r < nb && c < nb && r <= c ) { v = U0[(std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c]; }
-        D[r][c] = v;
+        if( r >= nb && r == c ) { D[r][c] = 1.0; }
+        else
+        {
+            const bool valid = r < nb && c < nb && r <= c;
+            const double * src = U0 + (std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c;
+            cp_async_8( &D[r][c], valid ? src : U0, valid );
+        }
     }
+#pragma unroll 4
     for( int idx = tid; idx < kPanel * kRestChunk; idx += kTrsmThreads )
     {
         const int r = idx / kRestChunk, cc = idx % kRestChunk;
         const int col = t.c0 + cc;
-        double v = 0.0;
-        if( r < nb && cc < cw )
+        const bool valid = r < nb && cc < cw;
+        const double * src = U0;
+        if( valid )
         {
-            v = (col < m) ? U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col]
-                          : U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)];
+            src = (col < m) ? U0 + (std::int64_t)(t.r0 + r) * t.ld0 + r1 + col
+                            : U1 + (std::int64_t)(t.r0 + r) * t.ld1 + (col - m);
         }
-        X[r][cc] = v;
+        cp_async_8( &X[r][cc], src, valid );
     }
+    cp_async_wait_all();
     __syncthreads();
     if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
     __syncthreads();
@@ -370,13 +401,6 @@ constexpr int kGemmStages = 3;
 constexpr int kGemmStageDoubles = 2 * kGemmK * kGemmLd;          // A and B of one stage
 constexpr size_t kGemmSmemBytes = sizeof(double) * kGemmStages * kGemmStageDoubles;
 
-__device__ __forceinline__ void cp_async_16( double * smem_dst, const double * gmem_src, int src_bytes )
-{
-    const unsigned saddr = static_cast<unsigned>( __cvta_generic_to_shared( smem_dst ) );
-    asm volatile( "cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(saddr), "l"(gmem_src), "r"(src_bytes) );
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile( "cp.async.commit_group;\n" ::: "memory" ); }
-template<int N> __device__ __forceinline__ void cp_async_wait() { asm volatile( "cp.async.wait_group %0;\n" :: "n"(N) : "memory" ); }
 
 __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask * __restrict__ tasks,
                                                                 double * __restrict__ arena )
@@ -481,144 +505,253 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 }
 
 // ------------------------------------------------------------------ solves
-// Triangular solve with a panel's diagonal block for the panel's rows of X
-// (k <= 64 columns): D^T x = b forward (LowerSolver.hpp:183-197) or
-// D x = b backward (UpperSolver.hpp:190-200).
-__global__ __launch_bounds__(kSolveThreads) void solve_diag_kernel( const SolveDiagTask * __restrict__ tasks, int upper,
-                                                                    const double * __restrict__ arena,
-                                                                    double * __restrict__ X, int ldx, int k )
+// The supernodal solves (LowerSolver.hpp:143-305, UpperSolver.hpp:127-255)
+// run as one launch per (level, panel step) and sweep.  The triangular solves
+// with the 64 x 64 diagonal blocks become products with their inverses,
+// computed once after the factorization, so every CTA of a step can form the
+// panel's solution itself and no CTA waits for another.
+
+constexpr int kTld = kPanel + 4;   // padded shared-memory row of 64-wide blocks (conflict-free DMMA fragments)
+constexpr size_t kInvSmemBytes = sizeof(double) * 2 * kPanel * (kPanel + 1);
+
+// T = D^{-1} for the upper-triangular diagonal block D of one panel (nb x nb,
+// identity beyond nb): thread j back-substitutes D t = e_j for column j of T,
+// rows 63 down to 0, with four independent partial sums per row.
+__global__ __launch_bounds__(kPanel) void invert_diag_kernel( const SolveDiagTask * __restrict__ tasks,
+                                                               const double * __restrict__ arena,
+                                                               double * __restrict__ tinv )
 {
-    extern __shared__ double smem[];
-    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem );
-    double * Xs = smem + kPanel * (kPanel + 1);        // [kPanel][k]
+    extern __shared__ double ism[];
+    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( ism );
+    double (*T)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( ism + kPanel * (kPanel + 1) );
+    __shared__ double inv_d[kPanel];
     const SolveDiagTask t = tasks[blockIdx.x];
-    const int tid = threadIdx.x;
+    const int j = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    // thread -> (row group g, column c); groups cover rows g, g+G, g+2G, ...
-    const int c = tid % k;
-    const int g = tid / k;
-    const int G = kSolveThreads / k;
     const double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    for( int r = tid / kPanel; r < nb; r += kSolveThreads / kPanel )
+#pragma unroll 8
+    for( int r = 0; r < kPanel; ++r )
     {
-        const int cc = tid % kPanel;
-        if( cc < nb ) { D[r][cc] = (cc >= r) ? U0[(std::int64_t)r * t.ld0 + cc] : 0.0; }
+        if( r >= nb && r == j ) { D[r][j] = 1.0; }
+        else
+        {
+            const bool valid = r < nb && j < nb && j >= r;
+            cp_async_8( &D[r][j], valid ? U0 + (std::int64_t)r * t.ld0 + j : U0, valid );
+        }
     }
-    const std::int64_t row_base = (std::int64_t)t.row0 + t.r0;
-    if( g < G )
-    {
-        for( int r = g; r < nb; r += G ) { Xs[r * k + c] = X[(row_base + r) * ldx + c]; }
-    }
+    cp_async_wait_all();
     __syncthreads();
-    if( !upper )
+    inv_d[j] = 1.0 / D[j][j];
+    __syncthreads();
+    for( int i = kPanel - 1; i >= 0; --i )
     {
-        for( int r = 0; r < nb; ++r )
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int k = i + 1;
+        for( ; k + 3 < kPanel; k += 4 )
         {
-            if( tid < k ) { Xs[r * k + tid] /= D[r][r]; }
-            __syncthreads();
-            if( g < G )
-            {
-                const double xr = Xs[r * k + c];
-                for( int r2 = r + 1 + g; r2 < nb; r2 += G ) { Xs[r2 * k + c] -= D[r][r2] * xr; }
-            }
-            __syncthreads();
+            s0 += D[i][k]     * T[k][j];
+            s1 += D[i][k + 1] * T[k + 1][j];
+            s2 += D[i][k + 2] * T[k + 2][j];
+            s3 += D[i][k + 3] * T[k + 3][j];
         }
+        for( ; k < kPanel; ++k ) { s0 += D[i][k] * T[k][j]; }
+        T[i][j] = ((i == j ? 1.0 : 0.0) - ((s0 + s1) + (s2 + s3))) * inv_d[i];
     }
-    else
+    double * out = tinv + (std::int64_t)blockIdx.x * (kPanel * kPanel);
+    for( int r = 0; r < kPanel; ++r ) { out[r * kPanel + j] = T[r][j]; }
+}
+
+// acc[ct] (8 x 8 tile ct of this warp's 8 output rows) += sum over the K
+// blocks [kb0, kb1) of A(i, kk) * B(kk, ct * 8 + j).
+template<typename FA, typename FB>
+__device__ __forceinline__ void warp_rows_product( double (&acc)[kSolveMaxRhs / 8][2], int nct, int kb0, int kb1, FA a, FB b )
+{
+    for( int kb = kb0; kb < kb1; ++kb )
     {
-        for( int r = nb - 1; r >= 0; --r )
+#pragma unroll
+        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
         {
-            if( tid < k ) { Xs[r * k + tid] /= D[r][r]; }
-            __syncthreads();
-            if( g < G )
+            if( ct < nct )
             {
-                const double xr = Xs[r * k + c];
-                for( int r2 = g; r2 < r; r2 += G ) { Xs[r2 * k + c] -= D[r2][r] * xr; }
+                dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return a( i, kb * 8 + kk ); },
+                                     [&]( int kk, int j ) { return b( kb * 8 + kk, ct * 8 + j ); } );
             }
-            __syncthreads();
         }
-    }
-    if( g < G )
-    {
-        for( int r = g; r < nb; r += G ) { X[(row_base + r) * ldx + c] = Xs[r * k + c]; }
     }
 }
 
-// The rest of a panel in the solves.  Forward: X[rest] -= P^T X_panel, with
-// rows of the supernode itself updated in place and ancestor rows (through
-// SN_inner) by atomic adds, since other supernodes of the level may target
-// them (LowerSolver.hpp:199-231).  Backward: X_panel -= P X[rest] gathered
-// from final rows (UpperSolver.hpp:151-188), reduced over rest chunks by
-// atomic adds.
-__global__ __launch_bounds__(kSolveThreads) void solve_rest_kernel( const SolveRestTask * __restrict__ tasks, int upper,
+// One solve step.  Forward (U^T y = b): every task forms x_q = T_q^T y_q for
+// the panel's rows of `in`; the owner task writes x_q to `out`, each rest
+// task subtracts P^T x_q from its 64 rest rows of `in` (rows of the front in
+// place, ancestor rows by atomic adds: other fronts of the level may target
+// them).  Backward (U x = y): `out` starts at zero on the panel's rows; the
+// owner adds T_q y_q (y_q from `in`), each rest task subtracts T_q (P x_r)
+// with x_r its rest rows of `out`, already final.  Warp w owns rows
+// 8w..8w+7 of every 64 x kp product; kp = k rounded up to a power of two >= 8.
+__global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveRestTask * __restrict__ tasks, int upper,
                                                                     const double * __restrict__ arena,
+                                                                    const double * __restrict__ tinv,
                                                                     const std::int32_t * __restrict__ sn_inner,
-                                                                    double * __restrict__ X, int ldx, int k )
+                                                                    double * in, double * out, int ld, int k, int lkp )
 {
-    extern __shared__ double smem[];
-    double (*P)[kSolveRest + 1] = reinterpret_cast<double (*)[kSolveRest + 1]>( smem );   // [kPanel][kSolveRest+1]
-    double * Xs = smem + kPanel * (kSolveRest + 1);
+    extern __shared__ double ssm[];
+    double (*sT)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm );
+    double (*sP)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm + kPanel * kTld );
+    double * sV = ssm + 2 * kPanel * kTld;
     __shared__ std::int64_t trow[kSolveRest];
     const SolveRestTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int kp = 1 << lkp;
+    const int ldv = kp + 4;
+    const int nct = kp >> 3;
     const int nb = min( kPanel, t.n0 - t.r0 );
     const int r1 = t.r0 + nb;
     const int m = t.n0 - r1;
-    const int cw = t.c1 - t.c0;
-    const int c = tid % k;
-    const int g = tid / k;
-    const int G = kSolveThreads / k;
-    const double * U0 = arena + t.u0;
-    const double * U1 = arena + t.u1;
+    const bool owner = t.c0 < 0;
+    const int cw = owner ? 0 : t.c1 - t.c0;
+    const std::int64_t prow = (std::int64_t)t.row0 + t.r0;
+
     {
-        const int jj = tid % kSolveRest;
-        const int j = t.c0 + jj;
-        if( jj < cw )
+        const double * Tg = tinv + (std::int64_t)t.panel * (kPanel * kPanel);
+#pragma unroll
+        for( int u = 0; u < kPanel * kPanel / (2 * kSolveThreads); ++u )
         {
-            const double * src = (j < m) ? U0 + (std::int64_t)t.r0 * t.ld0 + r1 + j
-                                         : U1 + (std::int64_t)t.r0 * t.ld1 + (j - m);
-            const std::int64_t ld = (j < m) ? t.ld0 : t.ld1;
-            for( int i = tid / kSolveRest; i < nb; i += kSolveThreads / kSolveRest ) { P[i][jj] = src[i * ld]; }
-            if( tid < kSolveRest )
-            {
-                trow[jj] = (j < m) ? (std::int64_t)t.row0 + r1 + j : (std::int64_t)sn_inner[t.inner + (j - m)];
-            }
+            const int idx = 2 * (tid + u * kSolveThreads);
+            cp_async_16( &sT[idx >> 6][idx & 63], Tg + idx, 16 );
         }
     }
-    const std::int64_t panel_row = (std::int64_t)t.row0 + t.r0;
+    if( !owner )
+    {
+        const double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
+        const double * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
+#pragma unroll 4
+        for( int idx = tid; idx < kPanel * kPanel; idx += kSolveThreads )
+        {
+            const int i = idx >> 6, jj = idx & 63;
+            const int col = t.c0 + jj;
+            const bool valid = i < nb && jj < cw;
+            const double * src = U0;
+            if( valid ) { src = (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col : U1 + (std::int64_t)i * t.ld1 + (col - m); }
+            cp_async_8( &sP[i][jj], src, valid );
+        }
+    }
+    if( tid < kSolveRest )
+    {
+        const int col = t.c0 + tid;
+        trow[tid] = (tid < cw) ? ((col < m) ? (std::int64_t)t.row0 + r1 + col
+                                            : (std::int64_t)sn_inner[t.inner + (col - m)]) : -1;
+    }
+    __syncthreads();
+    // V: the panel's rows of `in` (forward, and the backward owner) or the
+    // rest rows of `out` (backward rest tasks)
+    const bool rest_rows = upper && !owner;
+#pragma unroll 4
+    for( int idx = tid; idx < (kPanel << lkp); idx += kSolveThreads )
+    {
+        const int i = idx >> lkp, c = idx & (kp - 1);
+        const double * src = in;
+        bool valid = false;
+        if( c < k )
+        {
+            if( rest_rows ) { valid = i < cw; if( valid ) { src = out + trow[i] * ld + c; } }
+            else { valid = i < nb; if( valid ) { src = in + (prow + i) * ld + c; } }
+        }
+        cp_async_8( &sV[i * ldv + c], src, valid );
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    const int fi = lane >> 2, fj = 2 * (lane & 3);     // accumulator fragment: row fi, columns fj, fj + 1
+    double acc[kSolveMaxRhs / 8][2];
+    auto clear = [&]() {
+#pragma unroll
+        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+    };
+    auto store_v = [&]() {       // sV rows of this warp <- acc (after a barrier)
+#pragma unroll
+        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+        {
+            if( ct < nct )
+            {
+                sV[(warp * 8 + fi) * ldv + ct * 8 + fj]     = acc[ct][0];
+                sV[(warp * 8 + fi) * ldv + ct * 8 + fj + 1] = acc[ct][1];
+            }
+        }
+    };
+    const int o = warp * 8;
     if( !upper )
     {
-        if( g < G )
-        {
-            for( int i = g; i < nb; i += G ) { Xs[i * k + c] = X[(panel_row + i) * ldx + c]; }
-        }
+        // x_q = T^T y_q (T^T is lower triangular: K blocks 0..warp)
+        clear();
+        warp_rows_product( acc, nct, 0, warp + 1, [&]( int i, int kk ) { return sT[kk][o + i]; },
+                                                  [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
         __syncthreads();
-        if( g < G )
+        store_v();
+        __syncthreads();
+        if( owner )
         {
-            for( int jj = g; jj < cw; jj += G )
+            for( int idx = tid; idx < (kPanel << lkp); idx += kSolveThreads )
             {
-                double acc = 0.0;
-                for( int i = 0; i < nb; ++i ) { acc += P[i][jj] * Xs[i * k + c]; }
-                double * dst = X + trow[jj] * ldx + c;
-                if( t.c0 + jj < m ) { *dst -= acc; } else { atomicAdd( dst, -acc ); }
+                const int i = idx >> lkp, c = idx & (kp - 1);
+                if( i < nb && c < k ) { out[(prow + i) * ld + c] = sV[i * ldv + c]; }
+            }
+            return;
+        }
+        // rest rows: y_r -= P^T x_q
+        clear();
+        warp_rows_product( acc, nct, 0, (nb + 7) >> 3, [&]( int i, int kk ) { return sP[kk][o + i]; },
+                                                       [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
+        const int jj = o + fi;
+        if( jj < cw )
+        {
+            double * dst = in + trow[jj] * ld;
+            const bool own_row = t.c0 + jj < m;
+#pragma unroll
+            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+            {
+#pragma unroll
+                for( int e = 0; e < 2; ++e )
+                {
+                    const int c = ct * 8 + fj + e;
+                    if( ct < nct && c < k )
+                    {
+                        if( own_row ) { dst[c] -= acc[ct][e]; } else { atomicAdd( dst + c, -acc[ct][e] ); }
+                    }
+                }
             }
         }
     }
     else
     {
-        __syncthreads();
-        if( g < G )
+        if( !owner )
         {
-            for( int jj = g; jj < cw; jj += G ) { Xs[jj * k + c] = X[trow[jj] * ldx + c]; }
+            // partial = P x_r
+            clear();
+            warp_rows_product( acc, nct, 0, (cw + 7) >> 3, [&]( int i, int kk ) { return sP[o + i][kk]; },
+                                                           [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
+            __syncthreads();
+            store_v();
+            __syncthreads();
         }
-        __syncthreads();
-        if( g < G )
+        // z = T partial (T upper triangular: K blocks warp..7)
+        clear();
+        warp_rows_product( acc, nct, warp, kPanel / 8, [&]( int i, int kk ) { return sT[o + i][kk]; },
+                                                       [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
+        const int i = o + fi;
+        if( i < nb )
         {
-            for( int i = g; i < nb; i += G )
+            double * dst = out + (prow + i) * ld;
+            const double sign = owner ? 1.0 : -1.0;
+#pragma unroll
+            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
             {
-                double acc = 0.0;
-                for( int jj = 0; jj < cw; ++jj ) { acc += P[i][jj] * Xs[jj * k + c]; }
-                atomicAdd( X + (panel_row + i) * ldx + c, -acc );
+#pragma unroll
+                for( int e = 0; e < 2; ++e )
+                {
+                    const int c = ct * 8 + fj + e;
+                    if( ct < nct && c < k ) { atomicAdd( dst + c, sign * acc[ct][e] ); }
+                }
             }
         }
     }
@@ -735,20 +868,30 @@ void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_
     if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, kGemmSmemBytes, st>>>( tasks, arena ); }
 }
 
-void launch_solve_diag( const SolveDiagTask * tasks, int count, bool upper, const double * arena,
-                        double * X, int ldx, int k, cudaStream_t st )
+void launch_invert_diag( const SolveDiagTask * tasks, int count, const double * arena, double * tinv, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
-    const size_t smem = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kMaxRhs);
-    solve_diag_kernel<<<count, kSolveThreads, smem, st>>>( tasks, upper ? 1 : 0, arena, X, ldx, k );
+    invert_diag_kernel<<<count, kPanel, kInvSmemBytes, st>>>( tasks, arena, tinv );
 }
 
-void launch_solve_rest( const SolveRestTask * tasks, int count, bool upper, const double * arena,
-                        const std::int32_t * sn_inner, double * X, int ldx, int k, cudaStream_t st )
+static int solve_lkp( int k )
+{
+    int l = 3;
+    while( (1 << l) < k ) { ++l; }
+    return l;
+}
+
+static size_t solve_smem_bytes( int k )
+{
+    return sizeof(double) * (2 * kPanel * kTld + kPanel * ((1 << solve_lkp( k )) + 4));
+}
+
+void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const double * arena, const double * tinv,
+                        const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
-    const size_t smem = sizeof(double) * (kPanel * (kSolveRest + 1) + kSolveRest * kMaxRhs);
-    solve_rest_kernel<<<count, kSolveThreads, smem, st>>>( tasks, upper ? 1 : 0, arena, sn_inner, X, ldx, k );
+    solve_step_kernel<<<count, kSolveThreads, solve_smem_bytes( k ), st>>>( tasks, upper ? 1 : 0, arena, tinv, sn_inner,
+                                                                           in, out, ld, k, solve_lkp( k ) );
 }
 
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
@@ -781,11 +924,13 @@ cudaError_t configure_kernels()
                                                     (int)kGemmSmemBytes );
         if( g != cudaSuccess ) { return g; }
     }
-    cudaError_t e = cudaFuncSetAttribute( solve_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)( sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kMaxRhs) ) );
-    if( e != cudaSuccess ) { return e; }
-    return cudaFuncSetAttribute( solve_rest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)( sizeof(double) * (kPanel * (kSolveRest + 1) + kSolveRest * kMaxRhs) ) );
+    {
+        const cudaError_t g = cudaFuncSetAttribute( invert_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)kInvSmemBytes );
+        if( g != cudaSuccess ) { return g; }
+    }
+    return cudaFuncSetAttribute( solve_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)solve_smem_bytes( kSolveMaxRhs ) );
 }
 
 void launch_gather_diag( const std::int64_t * offsets, const double * arena, double * out, int n, cudaStream_t st )

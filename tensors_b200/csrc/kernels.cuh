@@ -9,6 +9,8 @@
 namespace tb
 {
 
+constexpr int kSolveMaxRhs = 64;   // right-hand sides per solve launch
+
 // status[0]: bit 0 set when a pivot was not positive; status[1]: smallest
 // failing (permuted) row index (initialised to INT_MAX).
 void launch_assemble( const double * values, const std::int64_t * src, const std::int64_t * dst,
@@ -21,10 +23,12 @@ void launch_potrf( const PanelTask * tasks, int count, double * arena, int * sta
 void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st );
 void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st );
 
-void launch_solve_diag( const SolveDiagTask * tasks, int count, bool upper, const double * arena,
-                        double * X, int ldx, int k, cudaStream_t st );
-void launch_solve_rest( const SolveRestTask * tasks, int count, bool upper, const double * arena,
-                        const std::int32_t * sn_inner, double * X, int ldx, int k, cudaStream_t st );
+// Inverse of every panel's diagonal block into tinv (count x 64 x 64).
+void launch_invert_diag( const SolveDiagTask * tasks, int count, const double * arena, double * tinv, cudaStream_t st );
+// One forward (upper = false) or backward solve step over `count` tasks;
+// in / out row-major with leading dimension ld, k <= kSolveMaxRhs columns.
+void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const double * arena, const double * tinv,
+                        const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st );
 
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
                          int n, int k, cudaStream_t st );
@@ -38,7 +42,5 @@ void launch_gather_diag( const std::int64_t * offsets, const double * arena, dou
 // Raises the dynamic shared-memory limits of the solve kernels on the
 // current device; call once per device before the first launch.
 cudaError_t configure_kernels();
-
-constexpr int kSolveMaxRhs = 64;   // right-hand sides per solve launch
 
 } // namespace tb

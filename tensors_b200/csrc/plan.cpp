@@ -341,7 +341,7 @@ void Plan::build( const Symbolic & sym )
     factor_launches.clear(); lower_launches.clear(); upper_launches.clear();
 
     struct Range { I64 first; I32 count; };
-    std::vector<std::vector<Range>> diag_ranges( static_cast<size_t>(levels) ), rest_ranges( static_cast<size_t>(levels) );
+    std::vector<std::vector<Range>> rest_ranges( static_cast<size_t>(levels) );
 
     for( I32 h = 0; h < levels; ++h )
     {
@@ -402,14 +402,12 @@ void Plan::build( const Symbolic & sym )
         // panel steps
         I32 Q = 0;
         for( I32 f : L ) { Q = std::max<I32>( Q, static_cast<I32>( ceil_div( front_n0[f], kPanel ) ) ); }
-        diag_ranges[h].resize( static_cast<size_t>(Q) );
         rest_ranges[h].resize( static_cast<size_t>(Q) );
         for( I32 q = 0; q < Q; ++q )
         {
             const I64 ofirst = static_cast<I64>(potrf.size());
             const I64 pfirst = static_cast<I64>(panel.size());
             const I64 gfirst = static_cast<I64>(gemm.size());
-            const I64 dfirst = static_cast<I64>(sdiag.size());
             const I64 rfirst = static_cast<I64>(srest.size());
             std::vector<GemmTask> tiles;
             for( I32 f : L )
@@ -454,16 +452,21 @@ void Plan::build( const Symbolic & sym )
                 {
                     push_tiles( tiles, front_u1[f], ld1, front_u1[f], ld1, front_v[f], ld1, n0, n1, n1, true );
                 }
-                sdiag.push_back( { front_u0[f], n0, r0, front_row0[f], ld0 } );
-                for( I32 c0 = 0; c0 < rest; c0 += kSolveRest )
                 {
                     SolveRestTask t{};
                     t.u0 = front_u0[f]; t.u1 = front_u1[f]; t.inner = front_cols[f];
                     t.n0 = n0; t.n1 = n1; t.r0 = r0; t.row0 = front_row0[f];
-                    t.c0 = c0; t.c1 = std::min( rest, c0 + kSolveRest );
                     t.ld0 = ld0; t.ld1 = ld1;
+                    t.panel = static_cast<I32>( sdiag.size() );
+                    t.c0 = -1; t.c1 = 0;
                     srest.push_back( t );
+                    for( I32 c0 = 0; c0 < rest; c0 += kSolveRest )
+                    {
+                        t.c0 = c0; t.c1 = std::min( rest, c0 + kSolveRest );
+                        srest.push_back( t );
+                    }
                 }
+                sdiag.push_back( { front_u0[f], n0, r0, front_row0[f], ld0 } );
             }
             for( const GemmTask & t : tiles )
             {
@@ -479,27 +482,28 @@ void Plan::build( const Symbolic & sym )
             if( oc > 0 ) { factor_launches.push_back( { LaunchKind::Potrf, oc, ofirst, h, q } ); }
             if( pc > 0 ) { factor_launches.push_back( { LaunchKind::Trsm, pc, pfirst, h, q } ); }
             if( gc > 0 ) { factor_launches.push_back( { LaunchKind::Gemm, gc, gfirst, h, q } ); }
-            diag_ranges[h][q] = { dfirst, static_cast<I32>( static_cast<I64>(sdiag.size()) - dfirst ) };
             rest_ranges[h][q] = { rfirst, static_cast<I32>( static_cast<I64>(srest.size()) - rfirst ) };
         }
     }
 
+    if( !sdiag.empty() )
+    {
+        factor_launches.push_back( { LaunchKind::Invert, static_cast<I32>( sdiag.size() ), 0, levels, 0 } );
+    }
     for( I32 h = 0; h < levels; ++h )
     {
-        for( size_t q = 0; q < diag_ranges[h].size(); ++q )
+        for( size_t q = 0; q < rest_ranges[h].size(); ++q )
         {
-            const Range d = diag_ranges[h][q], r = rest_ranges[h][q];
-            if( d.count > 0 ) { lower_launches.push_back( { LaunchKind::SolveDiag, d.count, d.first, h, static_cast<I32>(q) } ); }
-            if( r.count > 0 ) { lower_launches.push_back( { LaunchKind::SolveRest, r.count, r.first, h, static_cast<I32>(q) } ); }
+            const Range r = rest_ranges[h][q];
+            if( r.count > 0 ) { lower_launches.push_back( { LaunchKind::Solve, r.count, r.first, h, static_cast<I32>(q) } ); }
         }
     }
     for( I32 h = levels; h-- > 0; )
     {
-        for( size_t q = diag_ranges[h].size(); q-- > 0; )
+        for( size_t q = rest_ranges[h].size(); q-- > 0; )
         {
-            const Range d = diag_ranges[h][q], r = rest_ranges[h][q];
-            if( r.count > 0 ) { upper_launches.push_back( { LaunchKind::SolveRest, r.count, r.first, h, static_cast<I32>(q) } ); }
-            if( d.count > 0 ) { upper_launches.push_back( { LaunchKind::SolveDiag, d.count, d.first, h, static_cast<I32>(q) } ); }
+            const Range r = rest_ranges[h][q];
+            if( r.count > 0 ) { upper_launches.push_back( { LaunchKind::Solve, r.count, r.first, h, static_cast<I32>(q) } ); }
         }
     }
 }

@@ -104,22 +104,26 @@ struct ExtendTask
     std::int32_t row_begin, row_end;
 };
 
-// Triangular solve with the diagonal block of panel [r0, r0+nb) of a front
-// whose first row is row0.
+// Diagonal block of panel [r0, r0+nb) of a front whose first row is row0.
+// Its inverse (kPanel x kPanel, row-major, identity-padded beyond nb) is
+// block k of the inverse-diagonal buffer, k = the task's index.
 struct SolveDiagTask
 {
     std::int64_t u0;
     std::int32_t n0, r0, row0, ld0;
 };
 
-// Rest part of a panel in the solves: rows [c0, c1) of the panel's rest
-// (U0 rows below the panel, then the front's U1 columns, whose global rows
-// come from SN_inner at offset inner).
+// One CTA of a solve step for panel [r0, r0+nb) of a front.  c0 < 0: the
+// panel's owner task (applies the inverse diagonal block to the panel's own
+// rows).  Otherwise rows [c0, c1) of the panel's rest: U0 rows below the
+// panel, then the front's U1 columns, whose global rows come from SN_inner
+// at offset inner.  panel = index of the panel's SolveDiagTask.
 struct SolveRestTask
 {
     std::int64_t u0, u1, inner;
     std::int32_t n0, n1, r0, row0, c0, c1;
     std::int32_t ld0, ld1;
+    std::int32_t panel, pad;
 };
 
 // Zero `count` doubles at arena offset `offset`.
@@ -143,7 +147,7 @@ struct ExportTask
     std::int32_t pad;
 };
 
-enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, SolveDiag = 4, SolveRest = 5, Potrf = 6 };
+enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, Invert = 4, Solve = 5, Potrf = 6 };
 
 // One launch: `count` tasks starting at `first` in the array of its kind.
 struct Launch
@@ -198,10 +202,10 @@ struct Plan
     std::vector<PanelTask>     panel;          // trsm chunks
     std::vector<ExtendTask>    extend;
     std::vector<ZeroTask>      zero;
-    std::vector<SolveDiagTask> sdiag;
-    std::vector<SolveRestTask> srest;
+    std::vector<SolveDiagTask> sdiag;          // one per (front, panel); also the inverse-block list
+    std::vector<SolveRestTask> srest;          // solve-step tasks, owner first per panel
 
-    std::vector<Launch> factor_launches;    // in order
+    std::vector<Launch> factor_launches;    // in order; the last one inverts the diagonal blocks
     std::vector<Launch> lower_launches;     // forward solve U^T y = b
     std::vector<Launch> upper_launches;     // back solve U x = y
 

@@ -112,7 +112,14 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad solve-rest dimensions" + at; }
         const I32 nb = std::min( kPanel, t.n0 - t.r0 );
         const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
-        if( t.c0 < 0 || t.c1 > rest || t.c0 >= t.c1 || t.c1 - t.c0 > kSolveRest ) { return "solve-rest range out of bounds" + at; }
+        const bool owner = t.c0 < 0;
+        if( owner ? (t.c0 != -1 || t.c1 != 0)
+                  : (t.c1 > rest || t.c0 >= t.c1 || t.c1 - t.c0 > kSolveRest) ) { return "solve-rest range out of bounds" + at; }
+        if( t.panel < 0 || static_cast<size_t>( t.panel ) >= pl.sdiag.size() ) { return "solve-rest panel out of range" + at; }
+        {
+            const SolveDiagTask & d = pl.sdiag[static_cast<size_t>( t.panel )];
+            if( d.u0 != t.u0 || d.r0 != t.r0 || d.n0 != t.n0 || d.row0 != t.row0 ) { return "solve-rest panel mismatch" + at; }
+        }
         if( t.ld0 < t.n0 || t.ld1 < t.n1 ) { return "solve-rest leading dimension too small" + at; }
         if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "solve-rest U0 out of range" + at; }
         if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.ld1 - 1, arena ) ) { return "solve-rest U1 out of range" + at; }
@@ -138,6 +145,29 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             if( cm >= 0 ? cm >= t.fn0 : (-cm - 1) >= t.fn1 ) { return "export colmap value out of range" + at; }
         }
     }
+    auto size_of = [&]( LaunchKind kind ) -> I64
+    {
+        switch( kind )
+        {
+            case LaunchKind::Zero:   return static_cast<I64>( pl.zero.size() );
+            case LaunchKind::Extend: return static_cast<I64>( pl.extend.size() );
+            case LaunchKind::Trsm:   return static_cast<I64>( pl.panel.size() );
+            case LaunchKind::Gemm:   return static_cast<I64>( pl.gemm.size() );
+            case LaunchKind::Invert: return static_cast<I64>( pl.sdiag.size() );
+            case LaunchKind::Solve:  return static_cast<I64>( pl.srest.size() );
+            case LaunchKind::Potrf:  return static_cast<I64>( pl.potrf.size() );
+        }
+        return -1;
+    };
+    for( const std::vector<Launch> * list : { &pl.factor_launches, &pl.lower_launches, &pl.upper_launches } )
+    {
+        for( const Launch & L : *list )
+        {
+            if( L.count <= 0 || L.first < 0 || L.first + L.count > size_of( L.kind ) ) { return "launch task range out of bounds"; }
+        }
+    }
+    for( const Launch & L : pl.lower_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the forward solve"; } }
+    for( const Launch & L : pl.upper_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the back solve"; } }
     return std::string();
 }
 

@@ -1,4 +1,5 @@
-"""Per-level breakdown of one factorization (direct launches timed by events).
+"""Per-level breakdown of one factorization and one 16-RHS solve (direct
+launches timed by events).
 
     python -m tensors_b200.profile_levels [--grid 64]
 
@@ -35,12 +36,29 @@ def main():
     for kind, level, step, tasks, ms in prof:
         per[level][kind] += ms
         cnt[level][kind] += 1
-    kinds = ["assemble", "zero", "extend", "potrf", "trsm", "gemm"]
+    kinds = ["assemble", "zero", "extend", "potrf", "trsm", "gemm", "invert"]
     print("level " + " ".join(f"{k:>14s}" for k in kinds) + "        total")
     for level in sorted(per):
         row = per[level]
         print(f"{level:5d} " + " ".join(f"{row[k]:8.3f}ms/{cnt[level][k]:4d}" for k in kinds) + f" {sum(row.values()):10.3f}")
-    print(json.dumps(prof))
+    B = torch.randn(A.n, 16, dtype=torch.float64, device="cuda")
+    X = torch.empty_like(B)
+    for _ in range(3):
+        chol.Solve(B, X)
+    torch.cuda.synchronize()
+    sprof = chol.SolveProfile()
+    sper = collections.defaultdict(lambda: [0.0, 0, 0.0, 0, 0])
+    for sweep, level, step, tasks, ms in sprof:
+        e = sper[level]
+        e[2 * sweep] += ms
+        e[2 * sweep + 1] += 1
+        e[4] = max(e[4], tasks)
+    print("level  forward ms/launches   back ms/launches  max tasks")
+    for level in sorted(sper):
+        f, fc, b, bc, mt = sper[level]
+        print(f"{level:5d} {f:10.3f}/{fc:4d}      {b:10.3f}/{bc:4d}   {mt:8d}")
+    print(f"solve total {sum(x[4] for x in sprof):.3f} ms over {len(sprof)} launches")
+    print(json.dumps({"factor": prof, "solve": sprof}))
 
 
 if __name__ == "__main__":
