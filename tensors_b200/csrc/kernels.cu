@@ -581,13 +581,16 @@ __device__ __forceinline__ void warp_rows_product( double (&acc)[kSolveMaxRhs / 
 }
 
 // One solve step.  Forward (U^T y = b): every task forms x_q = T_q^T y_q for
-// the panel's rows of `in`; the owner task writes x_q to `out`, each rest
-// task subtracts P^T x_q from its 64 rest rows of `in` (rows of the front in
-// place, ancestor rows by atomic adds: other fronts of the level may target
-// them).  Backward (U x = y): `out` starts at zero on the panel's rows; the
-// owner adds T_q y_q (y_q from `in`), each rest task subtracts T_q (P x_r)
-// with x_r its rest rows of `out`, already final.  Warp w owns rows
-// 8w..8w+7 of every 64 x kp product; kp = k rounded up to a power of two >= 8.
+// the panel's rows of `in`; the owner writes x_q to `out`, and a task with
+// rest rows subtracts P^T x_q from its (up to) 64 rest rows of `in` (rows of
+// the front in place, ancestor rows by atomic adds: other fronts of the level
+// may target them).  Backward (U x = y): `out` starts at zero on the panel's
+// rows; a task adds T_q (y_q - P x_r) (owner) or -T_q P x_r, with x_r its rest
+// rows of `out`, already final.  The owner is the task with c0 <= 0: the
+// first rest chunk, or a rest-less task for a front's last panel without
+// rest.  Warp w owns rows 8w..8w+7 of every 64 x kp product, kp = k rounded
+// up to a power of two >= 8, and skips row and K blocks beyond the panel's
+// nb rows and the task's cw rest rows.
 __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveRestTask * __restrict__ tasks, int upper,
                                                                     const double * __restrict__ arena,
                                                                     const double * __restrict__ tinv,
@@ -595,21 +598,24 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
                                                                     double * in, double * out, int ld, int k, int lkp )
 {
     extern __shared__ double ssm[];
+    const int kp = 1 << lkp;
+    const int ldv = kp + 4;
     double (*sT)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm );
     double (*sP)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm + kPanel * kTld );
-    double * sV = ssm + 2 * kPanel * kTld;
+    double * sX = ssm + 2 * kPanel * kTld;          // [64][ldv]: x_q (forward) / x_r (backward)
+    double * sY = sX + kPanel * ldv;                // [64][ldv]: y_q
     __shared__ std::int64_t trow[kSolveRest];
     const SolveRestTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int kp = 1 << lkp;
-    const int ldv = kp + 4;
     const int nct = kp >> 3;
     const int nb = min( kPanel, t.n0 - t.r0 );
+    const int nbb = (nb + 7) >> 3;
     const int r1 = t.r0 + nb;
     const int m = t.n0 - r1;
-    const bool owner = t.c0 < 0;
-    const int cw = owner ? 0 : t.c1 - t.c0;
+    const bool owner = t.c0 <= 0;
+    const bool has_rest = t.c0 >= 0;
+    const int cw = has_rest ? t.c1 - t.c0 : 0;
     const std::int64_t prow = (std::int64_t)t.row0 + t.r0;
 
     {
@@ -621,7 +627,7 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
             cp_async_16( &sT[idx >> 6][idx & 63], Tg + idx, 16 );
         }
     }
-    if( !owner )
+    if( has_rest )
     {
         const double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
         const double * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
@@ -636,6 +642,15 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
             cp_async_8( &sP[i][jj], src, valid );
         }
     }
+    // y_q: the panel's rows of `in` (forward: every task; backward: the owner)
+    const bool need_y = !upper || owner;
+#pragma unroll 4
+    for( int idx = tid; idx < (kPanel << lkp); idx += kSolveThreads )
+    {
+        const int i = idx >> lkp, c = idx & (kp - 1);
+        const bool valid = need_y && i < nb && c < k;
+        cp_async_8( &sY[i * ldv + c], valid ? in + (prow + i) * ld + c : in, valid );
+    }
     if( tid < kSolveRest )
     {
         const int col = t.c0 + tid;
@@ -643,65 +658,57 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
                                             : (std::int64_t)sn_inner[t.inner + (col - m)]) : -1;
     }
     __syncthreads();
-    // V: the panel's rows of `in` (forward, and the backward owner) or the
-    // rest rows of `out` (backward rest tasks)
-    const bool rest_rows = upper && !owner;
-#pragma unroll 4
-    for( int idx = tid; idx < (kPanel << lkp); idx += kSolveThreads )
+    if( upper )
     {
-        const int i = idx >> lkp, c = idx & (kp - 1);
-        const double * src = in;
-        bool valid = false;
-        if( c < k )
+        // x_r: the rest rows of `out`, final
+#pragma unroll 4
+        for( int idx = tid; idx < (kPanel << lkp); idx += kSolveThreads )
         {
-            if( rest_rows ) { valid = i < cw; if( valid ) { src = out + trow[i] * ld + c; } }
-            else { valid = i < nb; if( valid ) { src = in + (prow + i) * ld + c; } }
+            const int i = idx >> lkp, c = idx & (kp - 1);
+            const bool valid = i < cw && c < k;
+            cp_async_8( &sX[i * ldv + c], valid ? out + trow[i] * ld + c : out, valid );
         }
-        cp_async_8( &sV[i * ldv + c], src, valid );
     }
     cp_async_wait_all();
     __syncthreads();
 
     const int fi = lane >> 2, fj = 2 * (lane & 3);     // accumulator fragment: row fi, columns fj, fj + 1
-    double acc[kSolveMaxRhs / 8][2];
-    auto clear = [&]() {
-#pragma unroll
-        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
-    };
-    auto store_v = [&]() {       // sV rows of this warp <- acc (after a barrier)
-#pragma unroll
-        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
-        {
-            if( ct < nct )
-            {
-                sV[(warp * 8 + fi) * ldv + ct * 8 + fj]     = acc[ct][0];
-                sV[(warp * 8 + fi) * ldv + ct * 8 + fj + 1] = acc[ct][1];
-            }
-        }
-    };
     const int o = warp * 8;
+    double acc[kSolveMaxRhs / 8][2];
+#pragma unroll
+    for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
     if( !upper )
     {
-        // x_q = T^T y_q (T^T is lower triangular: K blocks 0..warp)
-        clear();
-        warp_rows_product( acc, nct, 0, warp + 1, [&]( int i, int kk ) { return sT[kk][o + i]; },
-                                                  [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
-        __syncthreads();
-        store_v();
+        // x_q = T^T y_q (T^T lower triangular: K blocks 0..warp)
+        if( o < nb )
+        {
+            warp_rows_product( acc, nct, 0, warp + 1, [&]( int i, int kk ) { return sT[kk][o + i]; },
+                                                      [&]( int kk, int c ) { return sY[kk * ldv + c]; } );
+#pragma unroll
+            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+            {
+                if( ct < nct )
+                {
+                    sX[(o + fi) * ldv + ct * 8 + fj]     = acc[ct][0];
+                    sX[(o + fi) * ldv + ct * 8 + fj + 1] = acc[ct][1];
+                }
+            }
+        }
         __syncthreads();
         if( owner )
         {
             for( int idx = tid; idx < (kPanel << lkp); idx += kSolveThreads )
             {
                 const int i = idx >> lkp, c = idx & (kp - 1);
-                if( i < nb && c < k ) { out[(prow + i) * ld + c] = sV[i * ldv + c]; }
+                if( i < nb && c < k ) { out[(prow + i) * ld + c] = sX[i * ldv + c]; }
             }
-            return;
         }
+        if( !has_rest || o >= cw ) { return; }
         // rest rows: y_r -= P^T x_q
-        clear();
-        warp_rows_product( acc, nct, 0, (nb + 7) >> 3, [&]( int i, int kk ) { return sP[kk][o + i]; },
-                                                       [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
+#pragma unroll
+        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+        warp_rows_product( acc, nct, 0, nbb, [&]( int i, int kk ) { return sP[kk][o + i]; },
+                                             [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
         const int jj = o + fi;
         if( jj < cw )
         {
@@ -724,25 +731,36 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
     }
     else
     {
-        if( !owner )
+        // sY rows of this warp <- (owner ? y_q : 0) - P x_r
+        if( has_rest && o < nb )
         {
-            // partial = P x_r
-            clear();
             warp_rows_product( acc, nct, 0, (cw + 7) >> 3, [&]( int i, int kk ) { return sP[o + i][kk]; },
-                                                           [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
-            __syncthreads();
-            store_v();
-            __syncthreads();
+                                                           [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
+#pragma unroll
+            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+            {
+                if( ct < nct )
+                {
+#pragma unroll
+                    for( int e = 0; e < 2; ++e )
+                    {
+                        double & v = sY[(o + fi) * ldv + ct * 8 + fj + e];
+                        v = (owner ? v : 0.0) - acc[ct][e];
+                    }
+                }
+            }
         }
-        // z = T partial (T upper triangular: K blocks warp..7)
-        clear();
-        warp_rows_product( acc, nct, warp, kPanel / 8, [&]( int i, int kk ) { return sT[o + i][kk]; },
-                                                       [&]( int kk, int c ) { return sV[kk * ldv + c]; } );
+        __syncthreads();
+        if( o >= nb ) { return; }
+        // z = T (.) (T upper triangular: K blocks warp..nbb-1)
+#pragma unroll
+        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+        warp_rows_product( acc, nct, warp, nbb, [&]( int i, int kk ) { return sT[o + i][kk]; },
+                                                [&]( int kk, int c ) { return sY[kk * ldv + c]; } );
         const int i = o + fi;
         if( i < nb )
         {
             double * dst = out + (prow + i) * ld;
-            const double sign = owner ? 1.0 : -1.0;
 #pragma unroll
             for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
             {
@@ -750,7 +768,7 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
                 for( int e = 0; e < 2; ++e )
                 {
                     const int c = ct * 8 + fj + e;
-                    if( ct < nct && c < k ) { atomicAdd( dst + c, sign * acc[ct][e] ); }
+                    if( ct < nct && c < k ) { atomicAdd( dst + c, acc[ct][e] ); }
                 }
             }
         }
@@ -883,7 +901,7 @@ static int solve_lkp( int k )
 
 static size_t solve_smem_bytes( int k )
 {
-    return sizeof(double) * (2 * kPanel * kTld + kPanel * ((1 << solve_lkp( k )) + 4));
+    return sizeof(double) * (2 * kPanel * kTld + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
 }
 
 void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const double * arena, const double * tinv,

@@ -458,8 +458,11 @@ void Plan::build( const Symbolic & sym )
                     t.n0 = n0; t.n1 = n1; t.r0 = r0; t.row0 = front_row0[f];
                     t.ld0 = ld0; t.ld1 = ld1;
                     t.panel = static_cast<I32>( sdiag.size() );
-                    t.c0 = -1; t.c1 = 0;
-                    srest.push_back( t );
+                    if( rest == 0 )
+                    {
+                        t.c0 = -1; t.c1 = 0;            // owner without rest rows
+                        srest.push_back( t );
+                    }
                     for( I32 c0 = 0; c0 < rest; c0 += kSolveRest )
                     {
                         t.c0 = c0; t.c1 = std::min( rest, c0 + kSolveRest );

@@ -113,11 +113,12 @@ struct SolveDiagTask
     std::int32_t n0, r0, row0, ld0;
 };
 
-// One CTA of a solve step for panel [r0, r0+nb) of a front.  c0 < 0: the
-// panel's owner task (applies the inverse diagonal block to the panel's own
-// rows).  Otherwise rows [c0, c1) of the panel's rest: U0 rows below the
-// panel, then the front's U1 columns, whose global rows come from SN_inner
-// at offset inner.  panel = index of the panel's SolveDiagTask.
+// One CTA of a solve step for panel [r0, r0+nb) of a front: rows [c0, c1)
+// of the panel's rest (U0 rows below the panel, then the front's U1 columns,
+// whose global rows come from SN_inner at offset inner), or c0 = -1, c1 = 0
+// for a panel without rest rows.  The task with c0 <= 0 also applies the
+// inverse diagonal block to the panel's own rows.  panel = index of the
+// panel's SolveDiagTask.
 struct SolveRestTask
 {
     std::int64_t u0, u1, inner;

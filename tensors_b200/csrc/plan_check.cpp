@@ -113,7 +113,7 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         const I32 nb = std::min( kPanel, t.n0 - t.r0 );
         const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
         const bool owner = t.c0 < 0;
-        if( owner ? (t.c0 != -1 || t.c1 != 0)
+        if( owner ? (t.c0 != -1 || t.c1 != 0 || rest != 0)
                   : (t.c1 > rest || t.c0 >= t.c1 || t.c1 - t.c0 > kSolveRest) ) { return "solve-rest range out of bounds" + at; }
         if( t.panel < 0 || static_cast<size_t>( t.panel ) >= pl.sdiag.size() ) { return "solve-rest panel out of range" + at; }
         {

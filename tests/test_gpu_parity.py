@@ -51,6 +51,8 @@ def _cases():
     out.append(("delaunay-3000", A, O.nested_dissection(A, 16), 0.0, 1e-6))
     A = M.grid_laplacian_2d(20, 1.0)
     out.append(("grid2d-20-identity-perm", A, None, 0.0, TOL))
+    A = M.grid_laplacian_2d(64, 0.0)                  # the reference's CPU case: 64^2 grid, shift 1e-2
+    out.append(("c1-grid2d-64", A, O.nested_dissection(A), 1e-2, TOL))
     return out
 
 
