@@ -153,7 +153,9 @@ int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
  * tasks, out[5] panel tasks, out[6] extend-add tasks, out[7] forward-solve
  * launches, out[8] back-solve launches, out[9] supernodes, out[10] fronts
  * (runs of supernodes merged for computation), out[11] flops of the front
- * factorization (explicit zeros of merged fronts included).  Returns the
+ * factorization (explicit zeros of merged fronts included), out[12] simulated
+ * microseconds of the scheduled task graph (0 before the first numeric
+ * factorization on a device), out[13] tasks of the graph.  Returns the
  * number of entries written (at most cap). */
 int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
 /* Host-side bounds check of every device task of the plan (also run before
@@ -168,6 +170,25 @@ int tb_chol_set_stream( tb_chol * h, void * stream );
 /* Capture the numeric factorization into a CUDA graph on first use (default
  * on); off runs the same kernels as individual launches. */
 int tb_chol_set_graph( tb_chol * h, int32_t enabled );
+/* Schedule of the numeric factorization.  TB_SCHEDULE_LEVELS (default): one
+ * launch per task kind, level and panel step (also used while profiling).
+ * TB_SCHEDULE_TASK_GRAPH: the levels below the first level with 8
+ * or more panel steps run as level launches; the levels from there up run as
+ * one persistent launch whose CTAs take the tasks (extend-adds, panel potrf /
+ * trsm, GEMM tiles, inverse diagonal blocks) from a dependency-ordered list,
+ * so the next panel of a front and independent fronts overlap.
+ * TB_SCHEDULE_TASK_GRAPH_ALL: every level in the persistent launch (changing
+ * to or from it redoes the symbolic phase).  All compute the same factor,
+ * bit for bit. */
+enum tb_schedule { TB_SCHEDULE_LEVELS = 0, TB_SCHEDULE_TASK_GRAPH = 1, TB_SCHEDULE_TASK_GRAPH_ALL = 2 };
+int tb_chol_set_schedule( tb_chol * h, int32_t schedule );
+/* Execution trace of the persistent factorization launch: when enabled,
+ * each task records when it was taken, when its inputs were ready, when it
+ * was done (%globaltimer ns) and which CTA ran it.  tb_chol_trace writes 6
+ * entries per task in list order (kind, index, taken, ready, done, CTA;
+ * cap >= 6 x tasks) for the last factorization and returns the task count. */
+int tb_chol_set_trace( tb_chol * h, int32_t enabled );
+int tb_chol_trace( tb_chol * h, int64_t * out, int64_t cap );
 /* Per-kernel timing: when enabled, factorizations run as direct launches
  * bracketed by CUDA events and tb_chol_kernel_profile reports, per launch
  * kind (0 zero, 1 extend-add, 2 panel trsm, 3 GEMM tiles, 4 inversion of

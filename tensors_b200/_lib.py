@@ -57,6 +57,9 @@ SIGNATURES = {
     "tb_chol_set_graph": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_solve_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
     "tb_chol_launch_counts": (ctypes.c_int, [_vp, _pi64, _pi64]),
+    "tb_chol_set_schedule": (ctypes.c_int, [_vp, _i32]),
+    "tb_chol_set_trace": (ctypes.c_int, [_vp, _i32]),
+    "tb_chol_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64]),
     "tb_chol_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_kernel_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "tb_chol_launch_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),

@@ -121,6 +121,23 @@ class CholeskyDecomposition:
     def SetUseGraph(self, enabled: bool) -> None:
         _check(lib().tb_chol_set_graph(self._h, 1 if enabled else 0))
 
+    def SetSchedule(self, schedule) -> None:
+        """'levels' (default: one launch per kind, level and step), 'task_graph' (level launches, then one
+        persistent launch for the levels with long panel chains) or 'task_graph_all' (every level in the
+        persistent launch)."""
+        code = {"levels": 0, "task_graph": 1, "task_graph_all": 2}[schedule] if isinstance(schedule, str) else int(schedule)
+        _check(lib().tb_chol_set_schedule(self._h, code))
+
+    def SetTrace(self, enabled: bool) -> None:
+        _check(lib().tb_chol_set_trace(self._h, 1 if enabled else 0))
+
+    def Trace(self) -> np.ndarray:
+        """Trace of the last persistent factorization: rows (kind, index, taken_ns, ready_ns, done_ns, cta)."""
+        cap = 6 * self.PlanStats()["graph_tasks"]
+        out = np.zeros(cap, dtype=np.int64)
+        m = _check(lib().tb_chol_trace(self._h, out.ctypes.data, cap))
+        return out[: 6 * m].reshape(m, 6)
+
     def SetStream(self, stream) -> None:
         """Run on a torch.cuda.Stream (or raw handle); None = an owned stream."""
         ptr = None if stream is None else int(getattr(stream, "cuda_stream", stream))
@@ -309,7 +326,7 @@ class CholeskyDecomposition:
         out = np.zeros(16, dtype=np.int64)
         m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 16))
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
-                "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops"]
+                "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

@@ -5,6 +5,7 @@
 #include "kernels.cuh"
 #include "plan.hpp"
 #include "plan_check.hpp"
+#include "schedule.hpp"
 #include "symbolic.hpp"
 
 #include <cuda_runtime.h>
@@ -23,6 +24,8 @@ namespace
 
 thread_local std::string g_error = "no error";
 int g_device = 0;
+// Bound on one dependency wait of the persistent factorization kernel.
+constexpr unsigned long long kDagTimeoutNs = 2000000000ull;
 
 int fail( int code, const std::string & msg )
 {
@@ -130,6 +133,13 @@ struct tb_chol
     DeviceArray<int>                status;
     DeviceArray<double>             work, work2, in, out, diag_vals;
     DeviceArray<double>             tinv;        // inverse diagonal block of every panel (64 x 64 each)
+    DeviceArray<tb::DagTask>        dag;         // the factorization as one dependency-ordered task list
+    DeviceArray<int>                dag_state;   // task-graph counters, then the ticket and the error word
+    int dag_grid = 0;                            // CTAs of the persistent factorization launch
+    bool use_dag = false;                        // persistent task-graph launch (else one launch per step)
+    int schedule = TB_SCHEDULE_LEVELS;
+    bool trace = false;                          // record the persistent launch's execution trace
+    DeviceArray<unsigned long long> trace_buf;
     PinnedBuffer                    pin_in, pin_out, pin_small;
 
     cudaGraphExec_t factor_graph = nullptr;
@@ -211,6 +221,7 @@ int ensure_symbolic( tb_chol * h )
                           : "invalid CSR pattern";
         return fail( st, std::string( "SymbolicFactorization: " ) + what );
     }
+    h->plan.dag_min_steps = h->schedule == TB_SCHEDULE_TASK_GRAPH_ALL ? 0 : tb::kDagMinSteps;
     h->plan.build( h->sym );
     h->symbolic_done = true;
     h->device_ready = false;
@@ -237,6 +248,16 @@ int ensure_device( tb_chol * h )
         h->kernels_configured = true;
     }
     if( h->device_ready ) { return TB_OK; }
+    {
+        // the persistent launch's CTA count, and the task order for it
+        int sms = 0;
+        TB_CUDA( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, h->device ) );
+        const int per_sm = tb::factor_dag_blocks_per_sm();
+        if( per_sm <= 0 ) { return fail( TB_ERR_CUDA, "persistent factorization kernel cannot be resident" ); }
+        h->dag_grid = static_cast<int>( std::min<std::int64_t>( static_cast<std::int64_t>( per_sm ) * sms,
+                                                                static_cast<std::int64_t>( h->plan.dag.size() ) ) );
+        tb::schedule_task_graph( h->plan, h->dag_grid );
+    }
     {
         const std::string msg = tb::check_plan( h->sym, h->plan );
         if( !msg.empty() ) { return fail( TB_ERR_INVALID_ARGUMENT, "plan check: " + msg ); }
@@ -269,6 +290,8 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->diag_off.upload( pl.diag_offset, st_ ) );
     TB_TRY( h->diag_vals.reserve( s.n ) );
     TB_TRY( h->tinv.reserve( static_cast<std::int64_t>( pl.sdiag.size() ) * tb::kPanel * tb::kPanel ) );
+    TB_TRY( h->dag.upload( pl.dag, st_ ) );
+    TB_TRY( h->dag_state.reserve( static_cast<std::int64_t>( pl.dag_counters ) + 2 ) );
     TB_CUDA( cudaStreamSynchronize( st_ ) );
     if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
     h->drop_solve_graphs();
@@ -299,6 +322,36 @@ std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * k
                          static_cast<std::int64_t>( pl.asm_src.size() ), h->reg.ptr, A, st );
     mark( 7 );
     launches += 2;
+    if( h->use_dag && !timed )
+    {
+        for( const tb::Launch & L : pl.pre_dag_launches )
+        {
+            switch( L.kind )
+            {
+                case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
+                case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
+                case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, st ); break;
+                case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
+                case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
+                case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
+                default: break;
+            }
+            ++launches;
+        }
+        const int nc = pl.dag_counters;
+        cudaMemsetAsync( h->dag_state.ptr, 0, sizeof(int) * (static_cast<size_t>( nc ) + 2), st );
+        tb::DagArgs a{};
+        a.tasks = h->dag.ptr; a.ntasks = static_cast<int>( pl.dag.size() );
+        a.counters = h->dag_state.ptr; a.next = h->dag_state.ptr + nc; a.error = h->dag_state.ptr + nc + 1;
+        a.arena = A; a.status = h->status.ptr;
+        a.zero = h->zero.ptr; a.extend = h->extend.ptr; a.lut = h->lut.ptr;
+        a.potrf = h->potrf.ptr; a.panel = h->panel.ptr; a.gemm = h->gemm.ptr;
+        a.sdiag = h->sdiag.ptr; a.tinv = h->tinv.ptr;
+        a.timeout_ns = kDagTimeoutNs;
+        a.trace = h->trace ? h->trace_buf.ptr : nullptr;
+        tb::launch_factor_dag( a, h->dag_grid, st );
+        return launches + (pl.dag.empty() ? 0 : 1);
+    }
     for( const tb::Launch & L : pl.factor_launches )
     {
         switch( L.kind )
@@ -369,8 +422,20 @@ int run_factor( tb_chol * h, double reg )
         TB_CUDA( cudaGetLastError() );
     }
     int * ps = reinterpret_cast<int*>( pr + 1 );
+    ps[2] = 0;
     TB_CUDA( cudaMemcpyAsync( ps, h->status.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, st ) );
+    if( h->use_dag && !h->profiling )
+    {
+        TB_CUDA( cudaMemcpyAsync( ps + 2, h->dag_state.ptr + h->plan.dag_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st ) );
+    }
     TB_CUDA( cudaStreamSynchronize( st ) );
+    if( ps[2] != 0 )
+    {
+        h->factorized = false;
+        h->good = false;
+        return fail( TB_ERR_TIMEOUT, "NumericFactorization: persistent launch stopped, the wait of task "
+                     + std::to_string( ps[2] - 1 ) + " ran out of time" );
+    }
     h->factorized = true;                       // marked in any case, Numeric.hpp:94-95
     h->good = (ps[0] == 0);
     h->failed_sn = h->good ? -1 : h->sym.row_to_sn[std::min( std::max( ps[1], 0 ), h->n - 1 )];
@@ -858,7 +923,8 @@ int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
         static_cast<std::int64_t>( pl.gemm.size() ), static_cast<std::int64_t>( pl.panel.size() ),
         static_cast<std::int64_t>( pl.extend.size() ), static_cast<std::int64_t>( pl.lower_launches.size() ),
         static_cast<std::int64_t>( pl.upper_launches.size() ), h->sym.sn_count, pl.front_count,
-        static_cast<std::int64_t>( pl.front_flops ) };
+        static_cast<std::int64_t>( pl.front_flops ), static_cast<std::int64_t>( pl.dag_makespan_us ),
+        static_cast<std::int64_t>( pl.dag.size() ) };
     const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
     for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
     return m;
@@ -915,6 +981,54 @@ int tb_chol_set_graph( tb_chol * h, std::int32_t enabled )
     if( h == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null handle" ); }
     h->use_graph = (enabled != 0);
     return TB_OK;
+}
+
+int tb_chol_set_schedule( tb_chol * h, std::int32_t schedule )
+{
+    TB_TRY( check_handle( h ) );
+    if( schedule != TB_SCHEDULE_LEVELS && schedule != TB_SCHEDULE_TASK_GRAPH && schedule != TB_SCHEDULE_TASK_GRAPH_ALL )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "unknown schedule" );
+    }
+    if( schedule == h->schedule ) { return TB_OK; }
+    const bool split_changes = (schedule == TB_SCHEDULE_TASK_GRAPH_ALL) != (h->schedule == TB_SCHEDULE_TASK_GRAPH_ALL);
+    h->schedule = schedule;
+    h->use_dag = schedule != TB_SCHEDULE_LEVELS;
+    if( split_changes ) { h->invalidate_symbolic(); }
+    if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    return TB_OK;
+}
+
+int tb_chol_set_trace( tb_chol * h, std::int32_t enabled )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( ensure_device( h ) );
+    if( enabled ) { TB_TRY( h->trace_buf.reserve( 4 * static_cast<std::int64_t>( h->plan.dag.size() ) ) ); }
+    if( (enabled != 0) != h->trace )
+    {
+        h->trace = enabled != 0;
+        if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    }
+    return TB_OK;
+}
+
+int tb_chol_trace( tb_chol * h, std::int64_t * out, std::int64_t cap )
+{
+    TB_TRY( check_handle( h ) );
+    if( !h->trace || h->trace_buf.ptr == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "trace not enabled" ); }
+    const std::int64_t n = static_cast<std::int64_t>( h->plan.dag.size() );
+    if( out == nullptr || cap < 6 * n ) { return fail( TB_ERR_INVALID_ARGUMENT, "trace buffer too small" ); }
+    std::vector<unsigned long long> raw( static_cast<size_t>( 4 * n ) );
+    TB_CUDA( cudaMemcpyAsync( raw.data(), h->trace_buf.ptr, sizeof(unsigned long long) * raw.size(), cudaMemcpyDeviceToHost, h->stream ) );
+    TB_CUDA( cudaStreamSynchronize( h->stream ) );
+    for( std::int64_t k = 0; k < n; ++k )
+    {
+        const tb::DagTask & t = h->plan.dag[static_cast<size_t>( k )];
+        out[6 * k + 0] = t.kind;
+        out[6 * k + 1] = t.index;
+        for( int j = 0; j < 4; ++j ) { out[6 * k + 2 + j] = static_cast<std::int64_t>( raw[static_cast<size_t>( 4 * k + j )] ); }
+    }
+    return static_cast<int>( std::min<std::int64_t>( n, INT_MAX ) );
 }
 
 int tb_chol_set_profiling( tb_chol * h, std::int32_t enabled )

@@ -16,7 +16,7 @@ namespace tb
 namespace
 {
 
-constexpr int kGemmThreads  = 128;
+constexpr int kGemmThreads  = 256;
 constexpr int kGemmK        = 16;
 constexpr int kGemmLd       = kTile + 4;   // padded smem row (2 wavefronts per fragment load)
 constexpr int kPanelThreads = kRestChunk;
@@ -66,9 +66,8 @@ __global__ void assemble_kernel( const double * __restrict__ values, const std::
 }
 
 // ------------------------------------------------------------------ zeroing
-__global__ void zero_kernel( const ZeroTask * __restrict__ tasks, double * __restrict__ arena )
+__device__ __forceinline__ void zero_body( const ZeroTask & t, double * __restrict__ arena )
 {
-    const ZeroTask t = tasks[blockIdx.x];
     double * p = arena + t.offset;
     std::int64_t i = threadIdx.x;
     // align to 16 bytes, then store double2
@@ -79,6 +78,11 @@ __global__ void zero_kernel( const ZeroTask * __restrict__ tasks, double * __res
     for( ; i < body; i += blockDim.x ) { q[i] = make_double2( 0.0, 0.0 ); }
     const std::int64_t tail = head + 2 * body;
     if( threadIdx.x == 0 && tail < t.count ) { p[tail] = 0.0; }
+}
+
+__global__ void zero_kernel( const ZeroTask * __restrict__ tasks, double * __restrict__ arena )
+{
+    zero_body( tasks[blockIdx.x], arena );
 }
 
 // ---------------------------------------------------------------- export
@@ -109,36 +113,54 @@ __global__ void export_kernel( const ExportTask * __restrict__ tasks, const std:
 // ------------------------------------------------------------- extend-add
 // One warp per row of the child's update W; lanes walk the row's upper part
 // (coalesced reads of W, lut-indexed adds into the parent front).
-__global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restrict__ tasks,
-                                                      const std::int32_t * __restrict__ lut_all,
-                                                      double * __restrict__ arena )
+__device__ __forceinline__ void extend_body( const ExtendTask & t, const std::int32_t * __restrict__ lut_all,
+                                             double * __restrict__ arena )
 {
-    const ExtendTask t = tasks[blockIdx.x];
     const std::int32_t * lut = lut_all + t.lut;
     const double * W = arena + t.w;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    constexpr int kU = 4;     // entries per lane in flight: the lut entries, W values and targets of a
+                              // group are loaded before any target is written (lut is injective within
+                              // a row, so the targets of a group are distinct)
     for( int i = t.row_begin + warp; i < t.row_end; i += 8 )
     {
         const std::int64_t li = lut[i];
         const double * Wi = W + (std::int64_t)i * t.ldw;
-        if( i < t.mid )
+        double * row0 = arena + t.u0 + li * t.ld0p;
+        double * row1 = arena + t.u1 + li * t.ld1p;
+        double * rowv = arena + t.v + li * t.ldvp;
+        const bool upper_part = i < t.mid;
+        for( int j0 = i + lane; j0 < t.m1; j0 += 32 * kU )
         {
-            double * row0 = arena + t.u0 + li * t.ld0p;
-            double * row1 = arena + t.u1 + li * t.ld1p;
-            for( int j = i + lane; j < t.m1; j += 32 )
+            double v[kU], old[kU];
+            double * dst[kU];
+#pragma unroll
+            for( int u = 0; u < kU; ++u )
             {
-                const int lj = lut[j];
-                const double v = Wi[j];
-                if( j < t.mid ) { row0[lj] += v; } else { row1[lj] += v; }
+                const int j = j0 + 32 * u;
+                dst[u] = nullptr;
+                v[u] = 0.0;
+                if( j < t.m1 )
+                {
+                    const int lj = lut[j];
+                    v[u] = Wi[j];
+                    dst[u] = upper_part ? ((j < t.mid) ? row0 + lj : row1 + lj) : rowv + lj;
+                }
             }
-        }
-        else
-        {
-            double * rowv = arena + t.v + li * t.ldvp;
-            for( int j = i + lane; j < t.m1; j += 32 ) { rowv[lut[j]] += Wi[j]; }
+#pragma unroll
+            for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : 0.0; }
+#pragma unroll
+            for( int u = 0; u < kU; ++u ) { if( dst[u] ) { *dst[u] = old[u] + v[u]; } }
         }
     }
+}
+
+__global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restrict__ tasks,
+                                                      const std::int32_t * __restrict__ lut_all,
+                                                      double * __restrict__ arena )
+{
+    extend_body( tasks[blockIdx.x], lut_all, arena );
 }
 
 // ------------------------------------------------------------------ panel
@@ -156,7 +178,7 @@ constexpr int kTrsmThreads  = 256;
 constexpr int kSub          = 8;                     // sub-block edge
 constexpr int kSubs         = kPanel / kSub;         // 8 sub-blocks per panel edge
 constexpr int kXld          = kRestChunk + 4;        // padded row of the staged rest columns
-constexpr size_t kTrsmSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kXld);
+constexpr size_t kTrsmSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kXld + kPanel);
 
 // C(8x8) += A(8x8) * B(8x8) with A read through a(i, k), B through b(k, j)
 // and C through c(i, j) (warp-wide; fragment layouts of mma.m8n8k4.f64).
@@ -171,16 +193,17 @@ __device__ __forceinline__ void dmma_8x8x8( double (&acc)[2], FA a, FB b )
     }
 }
 
-__global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
-                                                               double * __restrict__ arena, int * __restrict__ status )
+constexpr size_t kPotrfSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel + 1);
+
+__device__ __forceinline__ void potrf_body( const PanelTask & t, double * __restrict__ arena, int * __restrict__ status,
+                                            double * smem )
 {
-    const PanelTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    __shared__ double D[kPanel][kPanel + 1];
-    __shared__ double inv_d[kPanel];
-    __shared__ int fail;
+    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem );
+    double * inv_d = smem + kPanel * (kPanel + 1);
+    int & fail = *reinterpret_cast<int *>( inv_d + kPanel );
 
     double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
 #pragma unroll 4
@@ -290,19 +313,23 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
     }
 }
 
+__global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
+                                                               double * __restrict__ arena, int * __restrict__ status )
+{
+    extern __shared__ __align__(16) double psm[];
+    potrf_body( tasks[blockIdx.x], arena, status, psm );
+}
+
 // Solve D^T x = u against the factored diagonal block for the rest columns
 // [c0, c0 + kRestChunk) (trsm of FactorizeSupernode, Multifrontal.hpp:
 // 452-466): the columns are staged in shared memory; per 8-row sub-block,
 // one thread per column solves the 8 x 8 triangle in registers, then the
 // warps update the rows below with DMMA (warp w owns columns 8w..8w+7).
-__global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
-                                                             double * __restrict__ arena )
+__device__ __forceinline__ void trsm_body( const PanelTask & t, double * __restrict__ arena, double * tsm )
 {
-    extern __shared__ double tsm[];
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( tsm );
     double (*X)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm + kPanel * (kPanel + 1) );
-    __shared__ double inv_d[kPanel];
-    const PanelTask t = tasks[blockIdx.x];
+    double * inv_d = tsm + kPanel * (kPanel + 1) + kPanel * kXld;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
@@ -390,9 +417,16 @@ __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * _
     }
 }
 
+__global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
+                                                             double * __restrict__ arena )
+{
+    extern __shared__ __align__(16) double tsm[];
+    trsm_body( tasks[blockIdx.x], arena, tsm );
+}
+
 // ------------------------------------------------------------------- gemm
 // C[m0:m0+64, c0:c0+64] -= A[:, m0:]^T B[:, c0:] for row-major K x M / K x N
-// panels: 4 warps in a 2 x 2 arrangement, each a 32 x 32 block of 8 x 8
+// panels: 8 warps in a 2 x 4 arrangement, each a 32 x 16 block of 8 x 8
 // DMMA tiles.  K is streamed through a kGemmStages-deep ring of shared-memory
 // stages filled by 16-byte cp.async copies (every operand row starts on a
 // 16-byte boundary: the plan pads leading dimensions to kLdAlign), so the
@@ -401,28 +435,24 @@ constexpr int kGemmStages = 3;
 constexpr int kGemmStageDoubles = 2 * kGemmK * kGemmLd;          // A and B of one stage
 constexpr size_t kGemmSmemBytes = sizeof(double) * kGemmStages * kGemmStageDoubles;
 
-
-__global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask * __restrict__ tasks,
-                                                                double * __restrict__ arena )
+__device__ __forceinline__ void gemm_body( const GemmTask & t, double * __restrict__ arena, double * gsm )
 {
-    extern __shared__ __align__(16) double gsm[];
-    const GemmTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const int wm = warp >> 1, wn = warp & 1;
+    const int wm = warp & 1, wn = warp >> 1;
     const double * A = arena + t.a;
     const double * B = arena + t.b;
 
-    double acc[4][4][2];
+    double acc[4][2][2];
 #pragma unroll
     for( int i = 0; i < 4; ++i )
 #pragma unroll
-        for( int j = 0; j < 4; ++j ) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
+        for( int j = 0; j < 2; ++j ) { acc[i][j][0] = 0.0; acc[i][j][1] = 0.0; }
 
     // Each stage holds kGemmK rows of 64 doubles for A and for B = 512
-    // 16-byte chunks per operand; thread tid copies chunks tid + 128 * l.
-    constexpr int kChunks = kGemmK * kTile / 2 / kGemmThreads;       // 4 per operand
+    // 16-byte chunks per operand; thread tid copies chunks tid + 256 * l.
+    constexpr int kChunks = kGemmK * kTile / 2 / kGemmThreads;       // 2 per operand
     auto issue = [&]( int stage, int k0 )
     {
         double * As = gsm + stage * kGemmStageDoubles;
@@ -462,18 +492,20 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 #pragma unroll
         for( int kk = 0; kk < kGemmK; kk += 4 )
         {
-            double af[4], bf[4];
+            double af[4], bf[2];
 #pragma unroll
             for( int i = 0; i < 4; ++i ) { af[i] = As[(kk + (lane & 3)) * kGemmLd + wm * 32 + i * 8 + (lane >> 2)]; }
 #pragma unroll
-            for( int j = 0; j < 4; ++j ) { bf[j] = Bs[(kk + (lane & 3)) * kGemmLd + wn * 32 + j * 8 + (lane >> 2)]; }
+            for( int j = 0; j < 2; ++j ) { bf[j] = Bs[(kk + (lane & 3)) * kGemmLd + wn * 16 + j * 8 + (lane >> 2)]; }
 #pragma unroll
             for( int i = 0; i < 4; ++i )
 #pragma unroll
-                for( int j = 0; j < 4; ++j ) { dmma_8x8x4( acc[i][j], af[i], bf[j] ); }
+                for( int j = 0; j < 2; ++j ) { dmma_8x8x4( acc[i][j], af[i], bf[j] ); }
         }
     }
     cp_async_wait<0>();
+    // the ring is reused by the next task of a persistent CTA
+    __syncthreads();
 
     double * C = arena + t.c;
 #pragma unroll
@@ -483,9 +515,9 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
         if( row >= t.M ) { continue; }
         double * Crow = C + (std::int64_t)row * t.ldc;
 #pragma unroll
-        for( int j = 0; j < 4; ++j )
+        for( int j = 0; j < 2; ++j )
         {
-            const int col = t.c0 + wn * 32 + j * 8 + (lane & 3) * 2;
+            const int col = t.c0 + wn * 16 + j * 8 + (lane & 3) * 2;
             const bool ok0 = col < t.N && (!t.upper || row <= col);
             const bool ok1 = col + 1 < t.N && (!t.upper || row <= col + 1);
             if( ok0 && ok1 )
@@ -504,6 +536,13 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
     }
 }
 
+__global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask * __restrict__ tasks,
+                                                                double * __restrict__ arena )
+{
+    extern __shared__ __align__(16) double gsm[];
+    gemm_body( tasks[blockIdx.x], arena, gsm );
+}
+
 // ------------------------------------------------------------------ solves
 // The supernodal solves (LowerSolver.hpp:143-305, UpperSolver.hpp:127-255)
 // run as one launch per (level, panel step) and sweep.  The triangular solves
@@ -512,53 +551,67 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 // panel's solution itself and no CTA waits for another.
 
 constexpr int kTld = kPanel + 4;   // padded shared-memory row of 64-wide blocks (conflict-free DMMA fragments)
-constexpr size_t kInvSmemBytes = sizeof(double) * 2 * kPanel * (kPanel + 1);
+constexpr size_t kInvSmemBytes = sizeof(double) * (2 * kPanel * (kPanel + 1) + kPanel);
 
 // T = D^{-1} for the upper-triangular diagonal block D of one panel (nb x nb,
-// identity beyond nb): thread j back-substitutes D t = e_j for column j of T,
-// rows 63 down to 0, with four independent partial sums per row.
-__global__ __launch_bounds__(kPanel) void invert_diag_kernel( const SolveDiagTask * __restrict__ tasks,
-                                                               const double * __restrict__ arena,
-                                                               double * __restrict__ tinv )
+// identity beyond nb): thread j < 64 back-substitutes D t = e_j for column j
+// of T, rows 63 down to 0, with four independent partial sums per row; all
+// threads stage D and write T.
+constexpr int kInvThreads = 256;
+
+__device__ __forceinline__ void invert_body( const SolveDiagTask & t, const double * __restrict__ arena,
+                                             double * __restrict__ out, double * ism )
 {
-    extern __shared__ double ism[];
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( ism );
     double (*T)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( ism + kPanel * (kPanel + 1) );
-    __shared__ double inv_d[kPanel];
-    const SolveDiagTask t = tasks[blockIdx.x];
-    const int j = threadIdx.x;
+    double * inv_d = ism + 2 * kPanel * (kPanel + 1);
+    const int tid = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
     const double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-#pragma unroll 8
-    for( int r = 0; r < kPanel; ++r )
+#pragma unroll 4
+    for( int idx = tid; idx < kPanel * kPanel; idx += kInvThreads )
     {
-        if( r >= nb && r == j ) { D[r][j] = 1.0; }
+        const int r = idx >> 6, c = idx & 63;
+        if( r >= nb && r == c ) { D[r][c] = 1.0; }
         else
         {
-            const bool valid = r < nb && j < nb && j >= r;
-            cp_async_8( &D[r][j], valid ? U0 + (std::int64_t)r * t.ld0 + j : U0, valid );
+            const bool valid = r < nb && c < nb && c >= r;
+            cp_async_8( &D[r][c], valid ? U0 + (std::int64_t)r * t.ld0 + c : U0, valid );
         }
     }
     cp_async_wait_all();
     __syncthreads();
-    inv_d[j] = 1.0 / D[j][j];
+    if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
     __syncthreads();
-    for( int i = kPanel - 1; i >= 0; --i )
+    if( tid < kPanel )
     {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int k = i + 1;
-        for( ; k + 3 < kPanel; k += 4 )
+        const int j = tid;
+        for( int i = kPanel - 1; i >= 0; --i )
         {
-            s0 += D[i][k]     * T[k][j];
-            s1 += D[i][k + 1] * T[k + 1][j];
-            s2 += D[i][k + 2] * T[k + 2][j];
-            s3 += D[i][k + 3] * T[k + 3][j];
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            int k = i + 1;
+            for( ; k + 3 < kPanel; k += 4 )
+            {
+                s0 += D[i][k]     * T[k][j];
+                s1 += D[i][k + 1] * T[k + 1][j];
+                s2 += D[i][k + 2] * T[k + 2][j];
+                s3 += D[i][k + 3] * T[k + 3][j];
+            }
+            for( ; k < kPanel; ++k ) { s0 += D[i][k] * T[k][j]; }
+            T[i][j] = ((i == j ? 1.0 : 0.0) - ((s0 + s1) + (s2 + s3))) * inv_d[i];
         }
-        for( ; k < kPanel; ++k ) { s0 += D[i][k] * T[k][j]; }
-        T[i][j] = ((i == j ? 1.0 : 0.0) - ((s0 + s1) + (s2 + s3))) * inv_d[i];
     }
-    double * out = tinv + (std::int64_t)blockIdx.x * (kPanel * kPanel);
-    for( int r = 0; r < kPanel; ++r ) { out[r * kPanel + j] = T[r][j]; }
+    __syncthreads();
+    for( int idx = tid; idx < kPanel * kPanel; idx += kInvThreads ) { out[idx] = T[idx >> 6][idx & 63]; }
+    __syncthreads();
+}
+
+__global__ __launch_bounds__(kInvThreads) void invert_diag_kernel( const SolveDiagTask * __restrict__ tasks,
+                                                                   const double * __restrict__ arena,
+                                                                   double * __restrict__ tinv )
+{
+    extern __shared__ __align__(16) double ism[];
+    invert_body( tasks[blockIdx.x], arena, tinv + (std::int64_t)blockIdx.x * (kPanel * kPanel), ism );
 }
 
 // acc[ct] (8 x 8 tile ct of this warp's 8 output rows) += sum over the K
@@ -775,6 +828,117 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
     }
 }
 
+// ------------------------------------------------- persistent factorization
+// The whole numeric factorization as one launch: each CTA repeatedly takes
+// the next task of the plan's dependency-ordered list (an atomic ticket),
+// waits until the task's counters reach their targets, runs the task body
+// and increments its counters.  Tasks are taken in list order and every wait
+// is satisfied by tasks earlier in the list, so the earliest unfinished task
+// can always proceed; waits are nevertheless bounded in time, and a wait that
+// runs out records the task in `error` and makes every CTA stop.
+//
+// Counter protocol: every thread fences its own writes of the task, the CTA
+// synchronises, and thread 0 increments the counters (release); a waiting
+// thread 0 reads counters with ld.acquire.gpu and the CTA synchronises
+// before any thread touches the task's data.
+constexpr int kDagThreads = 256;
+constexpr size_t kDagSmemBytes = kTrsmSmemBytes > kInvSmemBytes
+    ? (kTrsmSmemBytes > kGemmSmemBytes ? kTrsmSmemBytes : kGemmSmemBytes)
+    : (kInvSmemBytes > kGemmSmemBytes ? kInvSmemBytes : kGemmSmemBytes);
+static_assert( kDagSmemBytes >= kPotrfSmemBytes, "persistent kernel shared memory too small" );
+
+__device__ __forceinline__ int ld_acquire( const int * p )
+{
+    int v;
+    asm volatile( "ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory" );
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile( "mov.u64 %0, %%globaltimer;\n" : "=l"(t) );
+    return t;
+}
+
+// Thread 0 only: 1 when all waits of the task are met, 0 on timeout or when
+// another CTA has reported an error.
+__device__ int dag_wait( const DagTask & t, const DagArgs & a, int idx )
+{
+    const unsigned long long start = global_ns();
+    for( int i = 0; i < kDagWaits; ++i )
+    {
+        if( t.wait[i] < 0 ) { continue; }
+        const int * c = a.counters + t.wait[i];
+        unsigned spins = 0;
+        while( ld_acquire( c ) < t.target[i] )
+        {
+            ++spins;
+            if( (spins & 31u) == 0 )
+            {
+                if( *reinterpret_cast<volatile int *>( a.error ) != 0 ) { return 0; }
+                if( global_ns() - start > a.timeout_ns || spins > kDagMaxSpins )
+                {
+                    atomicCAS( a.error, 0, idx + 1 );
+                    return 0;
+                }
+            }
+            __nanosleep( 100 );
+        }
+    }
+    return 1;
+}
+
+__global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagArgs a )
+{
+    extern __shared__ __align__(16) double dsm[];
+    __shared__ int s_idx, s_ok;
+    const int tid = threadIdx.x;
+    for( ;; )
+    {
+        if( tid == 0 )
+        {
+            int idx = a.ntasks, ok = 0;
+            if( *reinterpret_cast<volatile int *>( a.error ) == 0 ) { idx = atomicAdd( a.next, 1 ); }
+            if( idx < a.ntasks )
+            {
+                const unsigned long long taken = a.trace ? global_ns() : 0ull;
+                ok = dag_wait( a.tasks[idx], a, idx );
+                if( a.trace )
+                {
+                    a.trace[4 * (std::int64_t)idx]     = taken;
+                    a.trace[4 * (std::int64_t)idx + 1] = global_ns();
+                    a.trace[4 * (std::int64_t)idx + 3] = blockIdx.x;
+                }
+            }
+            s_idx = idx;
+            s_ok = ok;
+        }
+        __syncthreads();
+        const int idx = s_idx;
+        if( idx >= a.ntasks || !s_ok ) { break; }
+        const DagTask t = a.tasks[idx];
+        switch( static_cast<LaunchKind>( t.kind ) )
+        {
+            case LaunchKind::Zero:   zero_body( a.zero[t.index], a.arena ); break;
+            case LaunchKind::Extend: extend_body( a.extend[t.index], a.lut, a.arena ); break;
+            case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], a.arena, a.status, dsm ); break;
+            case LaunchKind::Trsm:   trsm_body( a.panel[t.index], a.arena, dsm ); break;
+            case LaunchKind::Gemm:   gemm_body( a.gemm[t.index], a.arena, dsm ); break;
+            case LaunchKind::Invert: invert_body( a.sdiag[t.index], a.arena, a.tinv + (std::int64_t)t.index * (kPanel * kPanel), dsm ); break;
+            default: break;
+        }
+        __threadfence();
+        __syncthreads();
+        if( tid == 0 )
+        {
+            if( a.trace ) { a.trace[4 * (std::int64_t)idx + 2] = global_ns(); }
+            if( t.signal[0] >= 0 ) { atomicAdd( a.counters + t.signal[0], 1 ); }
+            if( t.signal[1] >= 0 ) { atomicAdd( a.counters + t.signal[1], 1 ); }
+        }
+    }
+}
+
 // ------------------------------------------------------ permutations, SpMV
 __global__ void gather_rows_kernel( const double * __restrict__ B, int ldB, const std::int32_t * __restrict__ p,
                                     double * __restrict__ W, int ldw, int n, int k )
@@ -873,7 +1037,7 @@ void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lu
 
 void launch_potrf( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st )
 {
-    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, 0, st>>>( tasks, arena, status ); }
+    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, kPotrfSmemBytes, st>>>( tasks, arena, status ); }
 }
 
 void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st )
@@ -886,10 +1050,25 @@ void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_
     if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, kGemmSmemBytes, st>>>( tasks, arena ); }
 }
 
+void launch_factor_dag( const DagArgs & args, int grid, cudaStream_t st )
+{
+    if( args.ntasks > 0 && grid > 0 ) { factor_dag_kernel<<<grid, kDagThreads, kDagSmemBytes, st>>>( args ); }
+}
+
+int factor_dag_blocks_per_sm()
+{
+    int blocks = 0;
+    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &blocks, factor_dag_kernel, kDagThreads, kDagSmemBytes ) != cudaSuccess )
+    {
+        return 0;
+    }
+    return blocks;
+}
+
 void launch_invert_diag( const SolveDiagTask * tasks, int count, const double * arena, double * tinv, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
-    invert_diag_kernel<<<count, kPanel, kInvSmemBytes, st>>>( tasks, arena, tinv );
+    invert_diag_kernel<<<count, kInvThreads, kInvSmemBytes, st>>>( tasks, arena, tinv );
 }
 
 static int solve_lkp( int k )
@@ -940,6 +1119,11 @@ cudaError_t configure_kernels()
     {
         const cudaError_t g = cudaFuncSetAttribute( gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                     (int)kGemmSmemBytes );
+        if( g != cudaSuccess ) { return g; }
+    }
+    {
+        const cudaError_t g = cudaFuncSetAttribute( factor_dag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)kDagSmemBytes );
         if( g != cudaSuccess ) { return g; }
     }
     {

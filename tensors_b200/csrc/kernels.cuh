@@ -23,6 +23,38 @@ void launch_potrf( const PanelTask * tasks, int count, double * arena, int * sta
 void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st );
 void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st );
 
+// The numeric factorization as one persistent launch over the plan's task
+// graph (Plan::dag).  counters (dag_counters ints), next and error must be
+// zero before the launch; afterwards error != 0 names the task (index + 1)
+// whose wait ran out of time.
+struct DagArgs
+{
+    const DagTask * tasks;
+    int ntasks;
+    int * counters;
+    int * next;
+    int * error;
+    double * arena;
+    int * status;
+    const ZeroTask * zero;
+    const ExtendTask * extend;
+    const std::int32_t * lut;
+    const PanelTask * potrf;
+    const PanelTask * panel;
+    const GemmTask * gemm;
+    const SolveDiagTask * sdiag;
+    double * tinv;
+    unsigned long long timeout_ns;
+    // optional execution trace, 4 entries per task in list order: time the
+    // task was taken, its inputs were ready and it was done (%globaltimer
+    // ns), and the CTA (block index) that ran it; nullptr: no trace
+    unsigned long long * trace;
+};
+constexpr unsigned kDagMaxSpins = 1u << 26;    // bound on polls of one wait, besides the time limit
+void launch_factor_dag( const DagArgs & args, int grid, cudaStream_t st );
+// Resident CTAs per SM of the persistent kernel (0 on error).
+int factor_dag_blocks_per_sm();
+
 // Inverse of every panel's diagonal block into tinv (count x 64 x 64).
 void launch_invert_diag( const SolveDiagTask * tasks, int count, const double * arena, double * tinv, cudaStream_t st );
 // One forward (upper = false) or backward solve step over `count` tasks;

@@ -1,6 +1,8 @@
 // Device execution plan; see plan.hpp.
 
 #include "plan.hpp"
+
+#include <stdexcept>
 #include "common.hpp"
 
 #include <algorithm>
@@ -339,27 +341,77 @@ void Plan::build( const Symbolic & sym )
     gemm.clear(); potrf.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
     gemm_flops = 0.0;
     factor_launches.clear(); lower_launches.clear(); upper_launches.clear();
+    dag.clear();
 
     struct Range { I64 first; I32 count; };
     std::vector<std::vector<Range>> rest_ranges( static_cast<size_t>(levels) );
 
+    // Dependency counters of the task graph (see DagTask): per level the
+    // finished extend-add tasks, per front the extend-adds received and
+    // the zeroing chunks done, per panel the potrf, trsm chunks, GEMM tiles
+    // of the panel's row block that feed the next panel, and all GEMM tiles.
+    // Panel indices follow the potrf / sdiag arrays, so they are only known
+    // while the arrays are built; counters are laid out once the panel count
+    // is known, so their ids are assigned in a second pass (CounterRef).
+    enum CounterKind : I32 { kExtLevel = 0, kExtIn, kZeroDone, kPotrfDone, kTrsmDone, kNextDone, kGemmDone };
+    struct CounterRef { I32 kind = -1, idx = 0; };
+    struct PendingTask { I32 kind, index, level; CounterRef signal[2]; CounterRef wait[kDagWaits]; I32 target[kDagWaits]; };
+    I32 cur_level = 0;
+    std::vector<PendingTask> pending;
+    auto make = [&]( LaunchKind k, I64 index ) {
+        PendingTask t{};
+        t.kind = static_cast<I32>( k ); t.index = static_cast<I32>( index ); t.level = cur_level;
+        for( int i = 0; i < kDagWaits; ++i ) { t.target[i] = 0; }
+        return t;
+    };
+    auto add_wait = [&]( PendingTask & t, I32 kind, I32 idx, I32 target ) {
+        if( target <= 0 ) { return; }
+        for( int i = 0; i < kDagWaits; ++i )
+        {
+            if( t.wait[i].kind < 0 ) { t.wait[i] = { kind, idx }; t.target[i] = target; return; }
+        }
+        throw std::logic_error( "task with too many dependencies" );
+    };
+
+    std::vector<I32> ext_into( static_cast<size_t>(F), 0 );        // extend tasks into each front (so far)
+    std::vector<I32> zero_of( static_cast<size_t>(F), 0 );         // zeroing chunks of each front's V
+    std::vector<I32> last_panel( static_cast<size_t>(F), -1 );     // panel index of the front's latest panel
+    std::vector<I32> panel_tiles, panel_next, panel_trsm;          // per panel: GEMM tiles, next-row tiles, trsm chunks
+    // Update-matrix regions are reused across levels: a level's zeroing
+    // waits until every extend-add of the earlier levels has read its child's
+    // region.  Each level's extend-adds wait for all those of the previous
+    // level that has any, so the count of that one level covers all before.
+    I32 prev_ext_level = -1, prev_ext_count = 0;
+
+    std::vector<I32> panel_level, level_steps( static_cast<size_t>(levels), 0 );
     for( I32 h = 0; h < levels; ++h )
     {
         const auto & L = by_level[h];
+        cur_level = h;
 
-        // zero this level's update matrices before children add into them
+        // zero this level's update matrices before children add into them;
+        // the regions may have been used by fronts consumed at earlier levels
         {
             const I64 first = static_cast<I64>(zero.size());
             for( I32 f : L )
             {
                 const I64 sz = static_cast<I64>(front_n1[f]) * front_ld1[f];
-                for( I64 o = 0; o < sz; o += kZeroChunk ) { zero.push_back( { front_v[f] + o, std::min( kZeroChunk, sz - o ) } ); }
+                for( I64 o = 0; o < sz; o += kZeroChunk )
+                {
+                    PendingTask t = make( LaunchKind::Zero, static_cast<I64>(zero.size()) );
+                    if( prev_ext_level >= 0 ) { add_wait( t, kExtLevel, prev_ext_level, prev_ext_count ); }
+                    t.signal[0] = { kZeroDone, f };
+                    pending.push_back( t );
+                    ++zero_of[f];
+                    zero.push_back( { front_v[f] + o, std::min( kZeroChunk, sz - o ) } );
+                }
             }
             const I32 count = static_cast<I32>( static_cast<I64>(zero.size()) - first );
             if( count > 0 ) { factor_launches.push_back( { LaunchKind::Zero, count, first, h, 0 } ); }
         }
 
-        // extend-add passes by child rank
+        // extend-add passes by child rank (one child per parent and pass, so
+        // no two tasks of a pass touch the same parent entries)
         I32 max_children = 0;
         for( I32 f : L ) { max_children = std::max( max_children, child_ptr[f+1] - child_ptr[f] ); }
         for( I32 r = 0; r < max_children; ++r )
@@ -372,6 +424,7 @@ void Plan::build( const Symbolic & sym )
                 const I32 t = child_idx[cb + r];
                 const I32 m1 = front_n1[t];
                 if( m1 == 0 ) { continue; }
+                const I32 before = ext_into[p];
                 I32 row = 0;
                 while( row < m1 )
                 {
@@ -391,6 +444,15 @@ void Plan::build( const Symbolic & sym )
                     e.ldw = front_ld1[t];
                     e.ld0p = front_ld0[p]; e.ld1p = front_ld1[p]; e.ldvp = front_ld1[p];
                     e.row_begin = row; e.row_end = end;
+                    PendingTask d = make( LaunchKind::Extend, static_cast<I64>(extend.size()) );
+                    add_wait( d, kGemmDone, last_panel[t], panel_tiles[static_cast<size_t>( last_panel[t] )] );
+                    add_wait( d, kZeroDone, p, zero_of[p] );
+                    add_wait( d, kExtIn, p, before );
+                    if( prev_ext_level >= 0 ) { add_wait( d, kExtLevel, prev_ext_level, prev_ext_count ); }
+                    d.signal[0] = { kExtIn, p };
+                    d.signal[1] = { kExtLevel, h };
+                    pending.push_back( d );
+                    ++ext_into[p];
                     extend.push_back( e );
                     row = end;
                 }
@@ -399,10 +461,15 @@ void Plan::build( const Symbolic & sym )
             if( count > 0 ) { factor_launches.push_back( { LaunchKind::Extend, count, first, h, r } ); }
         }
 
-        // panel steps
+        // panel steps; in the task graph a step's GEMM tiles that update the
+        // next panel's rows come first, then the next panel's potrf, trsm and
+        // inversion, then the rest of the step's tiles (one step of look-ahead)
         I32 Q = 0;
         for( I32 f : L ) { Q = std::max<I32>( Q, static_cast<I32>( ceil_div( front_n0[f], kPanel ) ) ); }
         rest_ranges[h].resize( static_cast<size_t>(Q) );
+        level_steps[static_cast<size_t>(h)] = Q;
+        std::vector<std::vector<PendingTask>> step_potrf( static_cast<size_t>(Q) ), step_trsm( static_cast<size_t>(Q) ),
+            step_inv( static_cast<size_t>(Q) ), next_tiles( static_cast<size_t>(Q) ), rest_tiles( static_cast<size_t>(Q) );
         for( I32 q = 0; q < Q; ++q )
         {
             const I64 ofirst = static_cast<I64>(potrf.size());
@@ -410,6 +477,8 @@ void Plan::build( const Symbolic & sym )
             const I64 gfirst = static_cast<I64>(gemm.size());
             const I64 rfirst = static_cast<I64>(srest.size());
             std::vector<GemmTask> tiles;
+            std::vector<I32> tile_panel, tile_prev;
+            std::vector<char> tile_next;
             for( I32 f : L )
             {
                 const I32 n0 = front_n0[f], n1 = front_n1[f];
@@ -418,6 +487,10 @@ void Plan::build( const Symbolic & sym )
                 const I32 nb = std::min( kPanel, n0 - r0 );
                 const I32 r1 = r0 + nb;
                 const I32 rest = (n0 - r1) + n1;
+                const I32 pi = static_cast<I32>( potrf.size() );
+                const I32 prev = last_panel[f];
+                last_panel[f] = pi;
+                panel_tiles.push_back( 0 ); panel_next.push_back( 0 ); panel_trsm.push_back( 0 ); panel_level.push_back( h );
                 std::int64_t singles = 0;
                 for( I32 r = 0; r < nb; ++r )
                 {
@@ -431,13 +504,28 @@ void Plan::build( const Symbolic & sym )
                 t.ld0 = ld0; t.ld1 = ld1;
                 t.row0 = front_row0[f];
                 t.single_rows = singles;
+                {
+                    PendingTask d = make( LaunchKind::Potrf, static_cast<I64>(potrf.size()) );
+                    // the first panel starts once the children's contributions are in and
+                    // the front's own update matrix is cleared (its last step writes it)
+                    if( q == 0 ) { add_wait( d, kExtIn, f, ext_into[f] ); add_wait( d, kZeroDone, f, zero_of[f] ); }
+                    else { add_wait( d, kNextDone, prev, panel_next[static_cast<size_t>(prev)] ); }
+                    d.signal[0] = { kPotrfDone, pi };
+                    step_potrf[q].push_back( d );
+                }
                 potrf.push_back( t );
                 for( I32 c0 = 0; c0 < rest; c0 += kRestChunk )
                 {
                     t.c0 = c0;
+                    PendingTask d = make( LaunchKind::Trsm, static_cast<I64>(panel.size()) );
+                    add_wait( d, kPotrfDone, pi, 1 );
+                    d.signal[0] = { kTrsmDone, pi };
+                    step_trsm[q].push_back( d );
+                    ++panel_trsm[static_cast<size_t>(pi)];
                     panel.push_back( t );
                 }
                 const I32 m = n0 - r1;
+                const size_t tfirst = tiles.size();
                 if( m > 0 )
                 {
                     const I64 pa = front_u0[f] + static_cast<I64>(r0) * ld0 + r1;        // U0[r0:r1, r1:n0]
@@ -447,10 +535,19 @@ void Plan::build( const Symbolic & sym )
                         push_tiles( tiles, pa, ld0, front_u1[f] + static_cast<I64>(r0) * ld1, ld1,
                                     front_u1[f] + static_cast<I64>(r1) * ld1, ld1, nb, m, n1, false );
                     }
+                    // tiles of rows [r1, r1 + 64) feed the next panel
+                    for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_next.push_back( tiles[i].m0 == 0 ? 1 : 0 ); }
                 }
                 else if( n1 > 0 && front_parent[f] < F )
                 {
                     push_tiles( tiles, front_u1[f], ld1, front_u1[f], ld1, front_v[f], ld1, n0, n1, n1, true );
+                    for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_next.push_back( 0 ); }
+                }
+                for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_panel.push_back( pi ); tile_prev.push_back( prev ); }
+                {
+                    PendingTask d = make( LaunchKind::Invert, static_cast<I64>(sdiag.size()) );
+                    add_wait( d, kPotrfDone, pi, 1 );
+                    step_inv[q].push_back( d );
                 }
                 {
                     SolveRestTask t{};
@@ -471,14 +568,31 @@ void Plan::build( const Symbolic & sym )
                 }
                 sdiag.push_back( { front_u0[f], n0, r0, front_row0[f], ld0 } );
             }
-            for( const GemmTask & t : tiles )
+            // tiles of the step: next-row tiles first, each group by K descending
+            std::vector<size_t> order( tiles.size() );
+            for( size_t i = 0; i < order.size(); ++i ) { order[i] = i; }
+            std::stable_sort( order.begin(), order.end(), [&]( size_t x, size_t y ) {
+                if( tile_next[x] != tile_next[y] ) { return tile_next[x] > tile_next[y]; }
+                return tiles[x].K > tiles[y].K;
+            } );
+            for( size_t i : order )
             {
+                const GemmTask & t = tiles[i];
                 const double rows = std::min( kTile, t.M - t.m0 ), cols = std::min( kTile, t.N - t.c0 );
                 gemm_flops += 2.0 * t.K * (t.upper ? rows * (rows + 1.0) / 2.0 + rows * (cols - rows) : rows * cols);
+                const I32 pi = tile_panel[i];
+                const I32 prev = tile_prev[i];
+                PendingTask d = make( LaunchKind::Gemm, static_cast<I64>(gemm.size()) );
+                add_wait( d, kTrsmDone, pi, panel_trsm[static_cast<size_t>(pi)] );
+                // the previous step's tiles of the front update the same C blocks
+                if( prev >= 0 ) { add_wait( d, kGemmDone, prev, panel_tiles[static_cast<size_t>(prev)] ); }
+                d.signal[0] = { kGemmDone, pi };
+                if( tile_next[i] ) { d.signal[1] = { kNextDone, pi }; ++panel_next[static_cast<size_t>(pi)]; }
+                (tile_next[i] ? next_tiles[q] : rest_tiles[q]).push_back( d );
+                gemm.push_back( t );
             }
-            std::stable_sort( tiles.begin(), tiles.end(),
-                              []( const GemmTask & x, const GemmTask & y ) { return x.K > y.K; } );
-            gemm.insert( gemm.end(), tiles.begin(), tiles.end() );
+            for( size_t i : order ) { ++panel_tiles[static_cast<size_t>( tile_panel[i] )]; }
+
             const I32 oc = static_cast<I32>( static_cast<I64>(potrf.size()) - ofirst );
             const I32 pc = static_cast<I32>( static_cast<I64>(panel.size()) - pfirst );
             const I32 gc = static_cast<I32>( static_cast<I64>(gemm.size()) - gfirst );
@@ -487,7 +601,72 @@ void Plan::build( const Symbolic & sym )
             if( gc > 0 ) { factor_launches.push_back( { LaunchKind::Gemm, gc, gfirst, h, q } ); }
             rest_ranges[h][q] = { rfirst, static_cast<I32>( static_cast<I64>(srest.size()) - rfirst ) };
         }
+        // task order of the level: P0 T0 I0, then per step q: the tiles that
+        // feed panel q+1, panel q+1's potrf / trsm / inversion, the other tiles
+        auto emit = [&]( const std::vector<PendingTask> & v ) { pending.insert( pending.end(), v.begin(), v.end() ); };
+        if( Q > 0 ) { emit( step_potrf[0] ); emit( step_trsm[0] ); emit( step_inv[0] ); }
+        for( I32 q = 0; q < Q; ++q )
+        {
+            emit( next_tiles[q] );
+            if( q + 1 < Q ) { emit( step_potrf[q+1] ); emit( step_trsm[q+1] ); emit( step_inv[q+1] ); }
+            emit( rest_tiles[q] );
+        }
+        {
+            I32 count = 0;
+            for( const PendingTask & t : pending ) { if( t.kind == static_cast<I32>( LaunchKind::Extend ) && t.signal[1].idx == h ) { ++count; } }
+            if( count > 0 ) { prev_ext_level = h; prev_ext_count = count; }
+        }
     }
+
+    // counter ids: [extend-adds per level][extend-in per front][zeroed per front]
+    // [potrf, trsm, next-row tiles, all tiles per panel]
+    {
+        const I32 NP = static_cast<I32>( potrf.size() );
+        const I32 Lv = levels;
+        const I32 base[7] = { 0, Lv, Lv + F, Lv + 2 * F, Lv + 2 * F + NP, Lv + 2 * F + 2 * NP, Lv + 2 * F + 3 * NP };
+        dag_counters = Lv + 2 * F + 4 * NP;
+        auto id = [&]( const CounterRef & r ) { return r.kind < 0 ? -1 : base[r.kind] + r.idx; };
+        // The levels below the first one whose fronts take kDagMinSteps or
+        // more panel steps run as level launches (many small independent
+        // fronts, where one launch per step keeps every SM full); the levels
+        // from there up, where long chains of panel steps follow each other,
+        // run as the task graph.  Waits on counters of the launched levels
+        // are met before the persistent launch starts and are dropped.
+        dag_split_level = levels;
+        for( I32 h = 0; h < levels; ++h ) { if( level_steps[static_cast<size_t>(h)] >= dag_min_steps ) { dag_split_level = h; break; } }
+        auto counter_level = [&]( const CounterRef & r ) -> I32 {
+            switch( r.kind )
+            {
+                case kExtLevel: return r.idx;
+                case kExtIn: case kZeroDone: return level_of[static_cast<size_t>( r.idx )];
+                default: return panel_level[static_cast<size_t>( r.idx )];
+            }
+        };
+        dag.reserve( pending.size() );
+        for( const PendingTask & t : pending )
+        {
+            if( t.level < dag_split_level ) { continue; }
+            DagTask d{};
+            d.kind = t.kind; d.index = t.index;
+            for( int i = 0; i < 2; ++i ) { d.signal[i] = id( t.signal[i] ); }
+            int w = 0;
+            for( int i = 0; i < kDagWaits; ++i ) { d.wait[i] = -1; d.target[i] = 0; }
+            for( int i = 0; i < kDagWaits; ++i )
+            {
+                if( t.wait[i].kind < 0 || counter_level( t.wait[i] ) < dag_split_level ) { continue; }
+                d.wait[w] = id( t.wait[i] ); d.target[w] = t.target[i]; ++w;
+            }
+            dag.push_back( d );
+        }
+        dag_first_panel = static_cast<I32>( std::find_if( panel_level.begin(), panel_level.end(),
+                                                          [&]( I32 l ) { return l >= dag_split_level; } ) - panel_level.begin() );
+    }
+
+    // the launches that precede the persistent launch: the levels below the
+    // split and the inversion of their panels' diagonal blocks
+    pre_dag_launches.clear();
+    for( const Launch & L : factor_launches ) { if( L.level < dag_split_level ) { pre_dag_launches.push_back( L ); } }
+    if( dag_first_panel > 0 ) { pre_dag_launches.push_back( { LaunchKind::Invert, dag_first_panel, 0, levels, 0 } ); }
 
     if( !sdiag.empty() )
     {

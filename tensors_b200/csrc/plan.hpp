@@ -148,6 +148,23 @@ struct ExportTask
     std::int32_t pad;
 };
 
+// One task of the factorization's task graph, executed by one CTA of the
+// persistent factorization kernel: `index` into the task array of `kind`.
+// Before it runs, counter wait[i] must have reached target[i] (unused
+// waits: -1); when it is done it increments the counters signal[0..1]
+// (-1: none).  The task list is in a topological order: every target is
+// reached by tasks earlier in the list, which the plan check verifies.
+constexpr int kDagWaits = 4;
+constexpr int kDagMinSteps = 8;      // levels from the first with this many panel steps run as the task graph
+
+struct DagTask
+{
+    std::int32_t kind, index;
+    std::int32_t signal[2];
+    std::int32_t wait[kDagWaits];
+    std::int32_t target[kDagWaits];
+};
+
 enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, Invert = 4, Solve = 5, Potrf = 6 };
 
 // One launch: `count` tasks starting at `first` in the array of its kind.
@@ -207,6 +224,13 @@ struct Plan
     std::vector<SolveRestTask> srest;          // solve-step tasks, owner first per panel
 
     std::vector<Launch> factor_launches;    // in order; the last one inverts the diagonal blocks
+    std::vector<DagTask> dag;               // the levels from dag_split_level up as one dependency-ordered task list
+    std::int32_t dag_counters = 0;
+    std::int32_t dag_min_steps = kDagMinSteps;   // set before build(): 0 puts every level in the task graph
+    std::int32_t dag_split_level = 0;       // first level in the task graph
+    std::int32_t dag_first_panel = 0;       // first panel (sdiag index) of that level
+    std::vector<Launch> pre_dag_launches;   // the levels below, as launches, then their inversions
+    double dag_makespan_us = 0.0;           // simulated duration of the scheduled list (schedule.cpp)
     std::vector<Launch> lower_launches;     // forward solve U^T y = b
     std::vector<Launch> upper_launches;     // back solve U x = y
 

@@ -159,12 +159,43 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         }
         return -1;
     };
-    for( const std::vector<Launch> * list : { &pl.factor_launches, &pl.lower_launches, &pl.upper_launches } )
+    for( const std::vector<Launch> * list : { &pl.factor_launches, &pl.pre_dag_launches, &pl.lower_launches, &pl.upper_launches } )
     {
         for( const Launch & L : *list )
         {
             if( L.count <= 0 || L.first < 0 || L.first + L.count > size_of( L.kind ) ) { return "launch task range out of bounds"; }
         }
+    }
+    // task graph: every task index in range, and every wait reached by
+    // signals of tasks earlier in the list (so a first-come first-served
+    // walk of the list never waits for a task that has not been taken)
+    {
+        std::vector<I64> cnt( static_cast<size_t>( std::max( 0, pl.dag_counters ) ), 0 );
+        I64 work = 0;
+        for( size_t k = 0; k < pl.dag.size(); ++k )
+        {
+            const DagTask & t = pl.dag[k];
+            const std::string at = " (graph task " + std::to_string( k ) + ")";
+            const LaunchKind kind = static_cast<LaunchKind>( t.kind );
+            if( kind == LaunchKind::Solve || t.index < 0 || t.index >= size_of( kind ) ) { return "task graph index out of range" + at; }
+            ++work;
+            for( int i = 0; i < kDagWaits; ++i )
+            {
+                if( t.wait[i] < 0 ) { continue; }
+                if( t.wait[i] >= pl.dag_counters ) { return "task graph counter out of range" + at; }
+                if( t.target[i] <= 0 || cnt[static_cast<size_t>( t.wait[i] )] < t.target[i] ) { return "task graph wait not reached by earlier tasks" + at; }
+            }
+            for( int i = 0; i < 2; ++i )
+            {
+                if( t.signal[i] < 0 ) { continue; }
+                if( t.signal[i] >= pl.dag_counters ) { return "task graph counter out of range" + at; }
+                ++cnt[static_cast<size_t>( t.signal[i] )];
+            }
+        }
+        I64 expect = 0, pre = 0;
+        for( const Launch & L : pl.factor_launches ) { expect += L.count; }
+        for( const Launch & L : pl.pre_dag_launches ) { pre += L.count; }
+        if( work + pre != expect ) { return "task graph and preceding launches do not cover the factorization tasks"; }
     }
     for( const Launch & L : pl.lower_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the forward solve"; } }
     for( const Launch & L : pl.upper_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the back solve"; } }

@@ -231,6 +231,29 @@ def test_single_row_and_two_by_two():
     assert np.allclose(chol.Solve(b), np.linalg.solve(vals.reshape(2, 2), b))
 
 
+@pytest.mark.parametrize("grid,leaf,schedule", [(10, 16, "task_graph_all"), (24, 64, "task_graph"),
+                                                (18, 8, "task_graph_all"), (28, 32, "task_graph")])
+def test_task_graph_and_level_schedules_agree_bitwise(grid, leaf, schedule):
+    # the persistent task-graph launch runs the same task bodies in a
+    # dependency order; every entry is produced by the same sequence of
+    # floating-point operations, so the factors are identical
+    A = M.grid_laplacian_3d(grid, 12, 1e-3)
+    perm = O.nested_dissection(A, leaf)
+    a = CholeskyDecomposition(A.outer, A.inner, perm)
+    b = CholeskyDecomposition(A.outer, A.inner, perm)
+    a.SetSchedule(schedule)
+    b.SetSchedule("levels")
+    for _ in range(2):
+        assert a.NumericFactorization(A.values) == 0
+        assert b.NumericFactorization(A.values) == 0
+        ta, ra = a.FactorValues()
+        tb_, rb = b.FactorValues()
+        assert np.array_equal(ta, tb_) and np.array_equal(ra, rb)
+    B = np.random.default_rng(grid).standard_normal((A.n, 3))
+    xa, xb = a.Solve(B), b.Solve(B)
+    assert rel_err(xa, xb) < 1e-12
+
+
 def test_graph_and_direct_launches_agree_bitwise():
     A = M.grid_laplacian_3d(10, 11, 1e-3)
     perm = O.nested_dissection(A, 16)
