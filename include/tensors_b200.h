@@ -170,6 +170,22 @@ int tb_chol_set_stream( tb_chol * h, void * stream );
 /* Capture the numeric factorization into a CUDA graph on first use (default
  * on); off runs the same kernels as individual launches. */
 int tb_chol_set_graph( tb_chol * h, int32_t enabled );
+/* Arithmetic of the factorization.  TB_PRECISION_FP64 (default): FP64 factor,
+ * FP64 arithmetic.  TB_PRECISION_MIXED: the factor is stored in FP32, the
+ * Schur-complement updates (the bulk of the flops) run as split-precision
+ * 3xTF32 tensor-core products with FP32 accumulation, the diagonal-block
+ * Cholesky and the triangular solves with the panels run in FP64 on FP32
+ * data, and tb_chol_solve / tb_chol_solve_device refine in FP64: conjugate
+ * gradients on (A + reg I) x = b with the FP64 matrix, preconditioned by the
+ * FP32 factor, until max_c |b_c - (A + reg I) x_c| / |b_c| <= tol.  Half
+ * solves are not refined.  Changing the precision discards the factor. */
+enum tb_precision { TB_PRECISION_FP64 = 0, TB_PRECISION_MIXED = 1 };
+int tb_chol_set_precision( tb_chol * h, int32_t precision );
+/* Refinement target and iteration cap of mixed-precision solves (defaults
+ * 1e-12, 30). */
+int tb_chol_set_refinement( tb_chol * h, double tol, int32_t max_iterations );
+/* Refinement steps and final relative residual of the last mixed solve. */
+int tb_chol_refinement_info( tb_chol * h, int32_t * iterations, double * relres );
 /* Schedule of the numeric factorization.  TB_SCHEDULE_LEVELS (default): one
  * launch per task kind, level and panel step (also used while profiling).
  * TB_SCHEDULE_TASK_GRAPH: the levels below the first level with 8

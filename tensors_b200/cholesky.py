@@ -121,6 +121,21 @@ class CholeskyDecomposition:
     def SetUseGraph(self, enabled: bool) -> None:
         _check(lib().tb_chol_set_graph(self._h, 1 if enabled else 0))
 
+    def SetPrecision(self, precision) -> None:
+        """'fp64' (default) or 'mixed' (FP32 factor with 3xTF32 updates, FP64 refinement in Solve)."""
+        code = {"fp64": 0, "mixed": 1}[precision] if isinstance(precision, str) else int(precision)
+        _check(lib().tb_chol_set_precision(self._h, code))
+
+    def SetRefinement(self, tol: float = 1e-12, max_iterations: int = 30) -> None:
+        _check(lib().tb_chol_set_refinement(self._h, float(tol), int(max_iterations)))
+
+    def RefinementInfo(self):
+        """(iterations, relative residual) of the last mixed-precision solve."""
+        it = ctypes.c_int32()
+        rr = ctypes.c_double()
+        _check(lib().tb_chol_refinement_info(self._h, ctypes.byref(it), ctypes.byref(rr)))
+        return it.value, rr.value
+
     def SetSchedule(self, schedule) -> None:
         """'levels' (default: one launch per kind, level and step), 'task_graph' (level launches, then one
         persistent launch for the levels with long panel chains) or 'task_graph_all' (every level in the

@@ -115,7 +115,7 @@ struct tb_chol
     tb::Plan plan;
 
     // device state
-    DeviceArray<double>             arena;
+    DeviceArray<double>             arena;       // factor storage: doubles, or floats in the mixed-precision mode
     DeviceArray<std::int64_t>       asm_src, asm_dst, diag_off;
     DeviceArray<std::int32_t>       lut, sn_inner, p, p_inv, colmap;
     DeviceArray<tb::ZeroTask>       zero;
@@ -138,6 +138,15 @@ struct tb_chol
     int dag_grid = 0;                            // CTAs of the persistent factorization launch
     bool use_dag = false;                        // persistent task-graph launch (else one launch per step)
     int schedule = TB_SCHEDULE_LEVELS;
+    int precision = TB_PRECISION_FP64;
+    double last_reg = 0.0;
+    // iterative refinement of the mixed-precision solves
+    double ir_tol = 1e-12;
+    std::int32_t ir_max = 30;
+    std::int32_t ir_iters = 0;
+    double ir_relres = 0.0;
+    DeviceArray<double> ir_x, ir_r, ir_norms;
+    PinnedBuffer pin_norms;
     bool trace = false;                          // record the persistent launch's execution trace
     DeviceArray<unsigned long long> trace_buf;
     PinnedBuffer                    pin_in, pin_out, pin_small;
@@ -266,7 +275,7 @@ int ensure_device( tb_chol * h )
     const tb::Symbolic & s = h->sym;
     const tb::Plan & pl = h->plan;
     cudaStream_t st_ = h->stream;
-    TB_TRY( h->arena.reserve( pl.arena_size() ) );
+    TB_TRY( h->arena.reserve( h->precision == TB_PRECISION_MIXED ? (pl.arena_size() + 1) / 2 : pl.arena_size() ) );
     TB_TRY( h->asm_src.upload( pl.asm_src, st_ ) );
     TB_TRY( h->asm_dst.upload( pl.asm_dst, st_ ) );
     TB_TRY( h->lut.upload( pl.lut, st_ ) );
@@ -299,13 +308,16 @@ int ensure_device( tb_chol * h )
     return TB_OK;
 }
 
+template<typename T> T * arena_as( tb_chol * h ) { return reinterpret_cast<T *>( h->arena.ptr ); }
+
 // Issues the numeric factorization on h->stream (capturable).  With
 // `timed`, every launch is bracketed by events (kind index in `kinds`).
-std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * kinds = nullptr )
+template<typename T>
+std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
 {
     const tb::Plan & pl = h->plan;
     cudaStream_t st = h->stream;
-    double * A = h->arena.ptr;
+    T * A = arena_as<T>( h );
     std::int64_t launches = 0;
     std::size_t ev = 0;
     auto mark = [&]( int kind )
@@ -316,7 +328,7 @@ std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * k
     };
     mark( -1 );
     // ClearFactors (Numeric.hpp:256-268); update matrices are zeroed per level
-    cudaMemsetAsync( A, 0, sizeof(double) * static_cast<size_t>( pl.u0_size + pl.u1_size ), st );
+    cudaMemsetAsync( A, 0, sizeof(T) * static_cast<size_t>( pl.u0_size + pl.u1_size ), st );
     tb::launch_init_status( h->status.ptr, st );
     tb::launch_assemble( h->values.ptr, h->asm_src.ptr, h->asm_dst.ptr,
                          static_cast<std::int64_t>( pl.asm_src.size() ), h->reg.ptr, A, st );
@@ -349,7 +361,7 @@ std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * k
         a.sdiag = h->sdiag.ptr; a.tinv = h->tinv.ptr;
         a.timeout_ns = kDagTimeoutNs;
         a.trace = h->trace ? h->trace_buf.ptr : nullptr;
-        tb::launch_factor_dag( a, h->dag_grid, st );
+        tb::launch_factor_dag<T>( a, h->dag_grid, st );
         return launches + (pl.dag.empty() ? 0 : 1);
     }
     for( const tb::Launch & L : pl.factor_launches )
@@ -370,12 +382,19 @@ std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * k
     return launches;
 }
 
+std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * kinds = nullptr )
+{
+    return h->precision == TB_PRECISION_MIXED ? issue_factor_t<float>( h, timed, kinds )
+                                              : issue_factor_t<double>( h, timed, kinds );
+}
+
 int run_factor( tb_chol * h, double reg )
 {
     cudaStream_t st = h->stream;
     TB_TRY( h->pin_small.reserve( 64 ) );
     double * pr = h->pin_small.as<double>();
     pr[0] = reg;
+    h->last_reg = reg;
     TB_CUDA( cudaMemcpyAsync( h->reg.ptr, pr, sizeof(double), cudaMemcpyHostToDevice, st ) );
     if( h->profiling )
     {
@@ -485,8 +504,16 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
             for( const tb::Launch & L : pl.lower_launches )
             {
                 begin();
-                tb::launch_solve_step( h->srest.ptr + L.first, L.count, false, h->arena.ptr, h->tinv.ptr, h->sn_inner.ptr,
-                                       W + c0, Y + c0, k, kc, st );
+                if( h->precision == TB_PRECISION_MIXED )
+                {
+                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, false, arena_as<float>( h ), h->tinv.ptr,
+                                           h->sn_inner.ptr, W + c0, Y + c0, k, kc, st );
+                }
+                else
+                {
+                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, false, arena_as<double>( h ), h->tinv.ptr,
+                                           h->sn_inner.ptr, W + c0, Y + c0, k, kc, st );
+                }
                 end( L, 0 );
                 ++launches;
             }
@@ -501,8 +528,16 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
             for( const tb::Launch & L : pl.upper_launches )
             {
                 begin();
-                tb::launch_solve_step( h->srest.ptr + L.first, L.count, true, h->arena.ptr, h->tinv.ptr, h->sn_inner.ptr,
-                                       Y + c0, W + c0, k, kc, st );
+                if( h->precision == TB_PRECISION_MIXED )
+                {
+                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, true, arena_as<float>( h ), h->tinv.ptr,
+                                           h->sn_inner.ptr, Y + c0, W + c0, k, kc, st );
+                }
+                else
+                {
+                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, true, arena_as<double>( h ), h->tinv.ptr,
+                                           h->sn_inner.ptr, Y + c0, W + c0, k, kc, st );
+                }
                 end( L, 1 );
                 ++launches;
             }
@@ -518,8 +553,8 @@ double * sweep_result( int which, double * W, double * Y ) { return which == 0 ?
 // The gather (ReadRightHandSide) and scatter (WriteSolution) run as direct
 // launches; the sweeps are captured once per (which, nrhs) into a CUDA graph
 // over the handle's work buffers.
-int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
-                      double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
+                    double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
 {
     cudaStream_t st = h->stream;
     const std::int32_t n = h->n;
@@ -586,6 +621,118 @@ int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, 
     return TB_OK;
 }
 
+// Mixed-precision solve: conjugate gradients in FP64 on (A + reg I) x = b
+// (the matrix of the last factorization), preconditioned by the FP32 factor
+// F ~ A + reg I, one independent recurrence per right-hand side, started
+// from x0 = F^{-1} b.  With an accurate factor this is iterative refinement
+// that converges in a few steps; unlike plain refinement it still converges
+// when cond(A) * eps_fp32 is not small.  Stops when
+// max_c |r_c| / |b_c| <= tol or after the iteration cap.  Per-column scalars
+// stay on the device; the residual norms are read back once per iteration.
+int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
+                       double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+{
+    cudaStream_t st = h->stream;
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    const std::int64_t nk = static_cast<std::int64_t>( n ) * k;
+    TB_TRY( h->ir_x.reserve( 4 * nk ) );               // x, r, z (and q), p
+    TB_TRY( h->ir_r.reserve( nk ) );
+    TB_TRY( h->ir_norms.reserve( 5 * k ) );            // |r|^2, |b|^2, rz, rz_new, pq
+    TB_TRY( h->pin_norms.reserve( sizeof(double) * 2 * static_cast<size_t>( k ) ) );
+    double * hn = h->pin_norms.as<double>();
+    double * X = h->ir_x.ptr;
+    double * P = X + nk;
+    double * Z = X + 2 * nk;
+    double * Q = X + 3 * nk;
+    double * R = h->ir_r.ptr;
+    double * rr = h->ir_norms.ptr;
+    double * bb = rr + k;
+    double * rz = rr + 2 * k;
+    double * rz_new = rr + 3 * k;
+    double * pq = rr + 4 * k;
+    const double shift = h->last_reg;
+    std::int64_t launches = 0;
+    auto apply = [&]( const double * x, const double * b, double * out ) {
+        tb::launch_apply_shifted( n, h->a_outer.ptr, h->a_inner.ptr, h->values.ptr, shift, x, k, b, b == d_B ? ldB : k, out, k, k, st );
+        ++launches;
+    };
+    auto dots = [&]( const double * x, int ldx, const double * y, int ldy, double * out ) -> int {
+        TB_CUDA( cudaMemsetAsync( out, 0, sizeof(double) * static_cast<size_t>( k ), st ) );
+        tb::launch_column_dots( x, ldx, y, ldy, n, k, out, st );
+        ++launches;
+        return TB_OK;
+    };
+    auto precondition = [&]( const double * in, double * out ) -> int {
+        TB_TRY( run_solve_core( h, 2, 1.0, in, k, 0.0, out, k, k ) );
+        launches += h->solve_launch_count;
+        return TB_OK;
+    };
+
+    TB_TRY( dots( d_B, ldB, d_B, ldB, bb ) );
+    TB_TRY( run_solve_core( h, 2, 1.0, d_B, ldB, 0.0, X, k, k ) );   // x0 = F^{-1} b
+    launches += h->solve_launch_count;
+    apply( X, d_B, R );                                             // r = b - A x
+    h->ir_iters = 0;
+    bool restart = true, verified = true;
+    for( std::int32_t it = 0;; ++it )
+    {
+        TB_TRY( dots( R, k, R, k, rr ) );
+        TB_CUDA( cudaMemcpyAsync( hn, rr, sizeof(double) * 2 * static_cast<size_t>( k ), cudaMemcpyDeviceToHost, st ) );
+        TB_CUDA( cudaStreamSynchronize( st ) );
+        double rel = 0.0;
+        for( std::int32_t c = 0; c < k; ++c )
+        {
+            const double bn = std::sqrt( hn[k + c] ), rn = std::sqrt( hn[c] );
+            rel = std::max( rel, bn > 0.0 ? rn / bn : rn );
+        }
+        h->ir_relres = rel;
+        if( it >= h->ir_max ) { break; }
+        if( rel <= h->ir_tol )
+        {
+            // the recurrence r -= a q drifts from b - A x in finite precision:
+            // accept only when the true residual meets the target as well
+            if( verified ) { break; }
+            apply( X, d_B, R );
+            verified = true;
+            restart = true;
+            continue;
+        }
+        verified = false;
+        TB_TRY( precondition( R, Z ) );                             // z = F^{-1} r
+        if( restart )
+        {
+            TB_TRY( dots( R, k, Z, k, rz ) );
+            TB_CUDA( cudaMemcpyAsync( P, Z, sizeof(double) * static_cast<size_t>( nk ), cudaMemcpyDeviceToDevice, st ) );
+            restart = false;
+        }
+        else
+        {
+            TB_TRY( dots( R, k, Z, k, rz_new ) );
+            tb::launch_cg_update_p( n, k, rz_new, rz, Z, P, st );   // p = z + (rz_new / rz) p
+            TB_CUDA( cudaMemcpyAsync( rz, rz_new, sizeof(double) * static_cast<size_t>( k ), cudaMemcpyDeviceToDevice, st ) );
+            ++launches;
+        }
+        apply( P, nullptr, Q );                                     // q = A p
+        TB_TRY( dots( P, k, Q, k, pq ) );
+        tb::launch_cg_update_xr( n, k, rz, pq, P, Q, X, R, st );    // x += a p, r -= a q
+        ++launches;
+        ++h->ir_iters;
+    }
+    tb::launch_combine( n, k, alpha, X, k, beta, d_X, ldX, st );
+    h->solve_launch_count = launches + 1;
+    TB_CUDA( cudaGetLastError() );
+    return TB_OK;
+}
+
+int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
+                      double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+{
+    if( h->precision == TB_PRECISION_MIXED && which == 2 ) { return run_solve_refined( h, alpha, d_B, ldB, beta, d_X, ldX, nrhs ); }
+    return run_solve_core( h, which, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
+}
+
 // Host-buffer solve through pinned staging buffers.
 int run_solve_host( tb_chol * h, int which, double alpha, const double * B, std::int32_t ldB,
                     double beta, double * X, std::int32_t ldX, std::int32_t nrhs )
@@ -622,7 +769,8 @@ int run_solve_host( tb_chol * h, int which, double alpha, const double * B, std:
 int fetch_diagonal( tb_chol * h, std::vector<double> & d )
 {
     TB_TRY( require_factor( h ) );
-    tb::launch_gather_diag( h->diag_off.ptr, h->arena.ptr, h->diag_vals.ptr, h->n, h->stream );
+    if( h->precision == TB_PRECISION_MIXED ) { tb::launch_gather_diag( h->diag_off.ptr, arena_as<float>( h ), h->diag_vals.ptr, h->n, h->stream ); }
+    else { tb::launch_gather_diag( h->diag_off.ptr, arena_as<double>( h ), h->diag_vals.ptr, h->n, h->stream ); }
     d.resize( static_cast<size_t>(h->n) );
     TB_CUDA( cudaMemcpyAsync( d.data(), h->diag_vals.ptr, sizeof(double) * d.size(), cudaMemcpyDeviceToHost, h->stream ) );
     TB_CUDA( cudaStreamSynchronize( h->stream ) );
@@ -872,8 +1020,16 @@ int tb_chol_factor_values( tb_chol * h, double * tri, double * rec )
     const std::int64_t ts = h->sym.sn_tri_ptr[h->sym.sn_count];
     const std::int64_t rs = h->sym.sn_rec_ptr[h->sym.sn_count];
     TB_TRY( h->exported.reserve( ts + rs ) );
-    tb::launch_export( h->exports.ptr, static_cast<int>( h->plan.exports.size() ), h->colmap.ptr, h->arena.ptr,
-                       h->exported.ptr, h->exported.ptr + ts, h->stream );
+    if( h->precision == TB_PRECISION_MIXED )
+    {
+        tb::launch_export( h->exports.ptr, static_cast<int>( h->plan.exports.size() ), h->colmap.ptr, arena_as<float>( h ),
+                           h->exported.ptr, h->exported.ptr + ts, h->stream );
+    }
+    else
+    {
+        tb::launch_export( h->exports.ptr, static_cast<int>( h->plan.exports.size() ), h->colmap.ptr, arena_as<double>( h ),
+                           h->exported.ptr, h->exported.ptr + ts, h->stream );
+    }
     TB_CUDA( cudaGetLastError() );
     if( tri && ts ) { TB_CUDA( cudaMemcpyAsync( tri, h->exported.ptr, sizeof(double) * ts, cudaMemcpyDeviceToHost, h->stream ) ); }
     if( rec && rs ) { TB_CUDA( cudaMemcpyAsync( rec, h->exported.ptr + ts, sizeof(double) * rs, cudaMemcpyDeviceToHost, h->stream ) ); }
@@ -996,6 +1152,37 @@ int tb_chol_set_schedule( tb_chol * h, std::int32_t schedule )
     h->use_dag = schedule != TB_SCHEDULE_LEVELS;
     if( split_changes ) { h->invalidate_symbolic(); }
     if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    return TB_OK;
+}
+
+int tb_chol_set_precision( tb_chol * h, std::int32_t precision )
+{
+    TB_TRY( check_handle( h ) );
+    if( precision != TB_PRECISION_FP64 && precision != TB_PRECISION_MIXED ) { return fail( TB_ERR_INVALID_ARGUMENT, "unknown precision" ); }
+    if( precision == h->precision ) { return TB_OK; }
+    h->precision = precision;
+    h->device_ready = false;        // storage of the other width; the next factorization re-creates the device plan
+    h->factorized = false;
+    h->good = false;
+    if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    h->drop_solve_graphs();
+    return TB_OK;
+}
+
+int tb_chol_set_refinement( tb_chol * h, double tol, std::int32_t max_iterations )
+{
+    TB_TRY( check_handle( h ) );
+    if( !(tol >= 0.0) || max_iterations < 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "refinement: tol >= 0 and max_iterations >= 0" ); }
+    h->ir_tol = tol;
+    h->ir_max = max_iterations;
+    return TB_OK;
+}
+
+int tb_chol_refinement_info( tb_chol * h, std::int32_t * iterations, double * relres )
+{
+    TB_TRY( check_handle( h ) );
+    if( iterations ) { *iterations = h->ir_iters; }
+    if( relres ) { *relres = h->ir_relres; }
     return TB_OK;
 }
 

@@ -28,7 +28,7 @@ __device__ __forceinline__ void dmma_8x8x4( double (&d)[2], double a, double b )
                   : "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b) );
 }
 
-__device__ __forceinline__ void cp_async_16( double * smem_dst, const double * gmem_src, int src_bytes )
+__device__ __forceinline__ void cp_async_16( void * smem_dst, const void * gmem_src, int src_bytes )
 {
     const unsigned saddr = static_cast<unsigned>( __cvta_generic_to_shared( smem_dst ) );
     asm volatile( "cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(saddr), "l"(gmem_src), "r"(src_bytes) );
@@ -47,12 +47,23 @@ __device__ __forceinline__ void cp_async_8( double * smem_dst, const double * gm
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile( "cp.async.wait_all;\n" ::: "memory" ); }
 
+// One element of a factor block into a double shared-memory cell: an
+// asynchronous copy for FP64 storage, a converting load for FP32 storage
+// (`base` is any mapped address of the block, used when !valid).
+template<typename T>
+__device__ __forceinline__ void stage_element( double * smem_dst, const T * base, const T * src, bool valid )
+{
+    if constexpr ( sizeof(T) == 8 ) { cp_async_8( smem_dst, valid ? src : base, valid ); }
+    else { *smem_dst = valid ? static_cast<double>( *src ) : 0.0; }
+}
+
 // ---------------------------------------------------------------- assembly
 // arena[dst] = values[src] (+ reg on the diagonal): ReadNonzeroValues
 // (Numeric.hpp:165-180) fused with FetchFromA (Multifrontal.hpp:249-321).
+template<typename T>
 __global__ void assemble_kernel( const double * __restrict__ values, const std::int64_t * __restrict__ src,
                                  const std::int64_t * __restrict__ dst, std::int64_t count,
-                                 const double * __restrict__ reg, double * __restrict__ arena )
+                                 const double * __restrict__ reg, T * __restrict__ arena )
 {
     const double r = *reg;
     for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < count;
@@ -61,14 +72,21 @@ __global__ void assemble_kernel( const double * __restrict__ values, const std::
         const std::uint64_t d = static_cast<std::uint64_t>( dst[e] );
         double v = values[src[e]];
         if( d & kDiagFlag ) { v += r; }
-        arena[d & (kDiagFlag - 1)] = v;
+        arena[d & (kDiagFlag - 1)] = static_cast<T>( v );
     }
 }
 
 // ------------------------------------------------------------------ zeroing
-__device__ __forceinline__ void zero_body( const ZeroTask & t, double * __restrict__ arena )
+template<typename T>
+__device__ __forceinline__ void zero_body( const ZeroTask & t, T * __restrict__ arena )
 {
-    double * p = arena + t.offset;
+    if constexpr ( sizeof(T) != 8 )
+    {
+        T * p = arena + t.offset;
+        for( std::int64_t i = threadIdx.x; i < t.count; i += blockDim.x ) { p[i] = T( 0 ); }
+        return;
+    }
+    double * p = reinterpret_cast<double *>( arena ) + t.offset;
     std::int64_t i = threadIdx.x;
     // align to 16 bytes, then store double2
     const int head = static_cast<int>( (reinterpret_cast<std::uintptr_t>( p ) >> 3) & 1 );
@@ -80,7 +98,8 @@ __device__ __forceinline__ void zero_body( const ZeroTask & t, double * __restri
     if( threadIdx.x == 0 && tail < t.count ) { p[tail] = 0.0; }
 }
 
-__global__ void zero_kernel( const ZeroTask * __restrict__ tasks, double * __restrict__ arena )
+template<typename T>
+__global__ void zero_kernel( const ZeroTask * __restrict__ tasks, T * __restrict__ arena )
 {
     zero_body( tasks[blockIdx.x], arena );
 }
@@ -89,23 +108,24 @@ __global__ void zero_kernel( const ZeroTask * __restrict__ tasks, double * __res
 // Reference layout from the fronts: U0 of supernode s is the diagonal block
 // of its front at row offset roff; column l of its U1 is front U0 column
 // colmap[l] (>= 0) or front U1 column -colmap[l]-1.
+template<typename T>
 __global__ void export_kernel( const ExportTask * __restrict__ tasks, const std::int32_t * __restrict__ colmap_all,
-                               const double * __restrict__ arena, double * __restrict__ tri, double * __restrict__ rec )
+                               const T * __restrict__ arena, double * __restrict__ tri, double * __restrict__ rec )
 {
     const ExportTask t = tasks[blockIdx.x];
     const std::int32_t * colmap = colmap_all + t.colmap;
     for( int r = t.r_begin; r < t.r_end; ++r )
     {
         const std::int64_t fr = t.roff + r;
-        const double * f0 = arena + t.fu0 + fr * t.fld0;
-        const double * f1 = arena + t.fu1 + fr * t.fld1;
+        const T * f0 = arena + t.fu0 + fr * t.fld0;
+        const T * f1 = arena + t.fu1 + fr * t.fld1;
         double * d0 = tri + t.tri + (std::int64_t)r * t.n0s;
-        for( int c = threadIdx.x; c < t.n0s; c += blockDim.x ) { d0[c] = (c >= r) ? f0[t.roff + c] : 0.0; }
+        for( int c = threadIdx.x; c < t.n0s; c += blockDim.x ) { d0[c] = (c >= r) ? static_cast<double>( f0[t.roff + c] ) : 0.0; }
         double * d1 = rec + t.rec + (std::int64_t)r * t.n1s;
         for( int l = threadIdx.x; l < t.n1s; l += blockDim.x )
         {
             const int cm = colmap[l];
-            d1[l] = (cm >= 0) ? f0[cm] : f1[-cm - 1];
+            d1[l] = static_cast<double>( (cm >= 0) ? f0[cm] : f1[-cm - 1] );
         }
     }
 }
@@ -113,11 +133,12 @@ __global__ void export_kernel( const ExportTask * __restrict__ tasks, const std:
 // ------------------------------------------------------------- extend-add
 // One warp per row of the child's update W; lanes walk the row's upper part
 // (coalesced reads of W, lut-indexed adds into the parent front).
+template<typename T>
 __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::int32_t * __restrict__ lut_all,
-                                             double * __restrict__ arena )
+                                             T * __restrict__ arena )
 {
     const std::int32_t * lut = lut_all + t.lut;
-    const double * W = arena + t.w;
+    const T * W = arena + t.w;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     constexpr int kU = 4;     // entries per lane in flight: the lut entries, W values and targets of a
@@ -126,21 +147,21 @@ __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::in
     for( int i = t.row_begin + warp; i < t.row_end; i += 8 )
     {
         const std::int64_t li = lut[i];
-        const double * Wi = W + (std::int64_t)i * t.ldw;
-        double * row0 = arena + t.u0 + li * t.ld0p;
-        double * row1 = arena + t.u1 + li * t.ld1p;
-        double * rowv = arena + t.v + li * t.ldvp;
+        const T * Wi = W + (std::int64_t)i * t.ldw;
+        T * row0 = arena + t.u0 + li * t.ld0p;
+        T * row1 = arena + t.u1 + li * t.ld1p;
+        T * rowv = arena + t.v + li * t.ldvp;
         const bool upper_part = i < t.mid;
         for( int j0 = i + lane; j0 < t.m1; j0 += 32 * kU )
         {
-            double v[kU], old[kU];
-            double * dst[kU];
+            T v[kU], old[kU];
+            T * dst[kU];
 #pragma unroll
             for( int u = 0; u < kU; ++u )
             {
                 const int j = j0 + 32 * u;
                 dst[u] = nullptr;
-                v[u] = 0.0;
+                v[u] = T( 0 );
                 if( j < t.m1 )
                 {
                     const int lj = lut[j];
@@ -149,16 +170,17 @@ __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::in
                 }
             }
 #pragma unroll
-            for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : 0.0; }
+            for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : T( 0 ); }
 #pragma unroll
             for( int u = 0; u < kU; ++u ) { if( dst[u] ) { *dst[u] = old[u] + v[u]; } }
         }
     }
 }
 
+template<typename T>
 __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restrict__ tasks,
                                                       const std::int32_t * __restrict__ lut_all,
-                                                      double * __restrict__ arena )
+                                                      T * __restrict__ arena )
 {
     extend_body( tasks[blockIdx.x], lut_all, arena );
 }
@@ -195,7 +217,8 @@ __device__ __forceinline__ void dmma_8x8x8( double (&acc)[2], FA a, FB b )
 
 constexpr size_t kPotrfSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel + 1);
 
-__device__ __forceinline__ void potrf_body( const PanelTask & t, double * __restrict__ arena, int * __restrict__ status,
+template<typename T>
+__device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict__ arena, int * __restrict__ status,
                                             double * smem )
 {
     const int tid = threadIdx.x;
@@ -205,7 +228,7 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, double * __rest
     double * inv_d = smem + kPanel * (kPanel + 1);
     int & fail = *reinterpret_cast<int *>( inv_d + kPanel );
 
-    double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
+    T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
 #pragma unroll 4
     for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
     {
@@ -214,7 +237,7 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, double * __rest
         else
         {
             const bool valid = r < nb && c < nb && r <= c;
-            cp_async_8( &D[r][c], valid ? U0 + (std::int64_t)r * t.ld0 + c : U0, valid );
+            stage_element( &D[r][c], U0, U0 + (std::int64_t)r * t.ld0 + c, valid );
         }
     }
     if( tid == 0 ) { fail = -1; }
@@ -304,7 +327,7 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, double * __rest
     for( int idx = tid; idx < nb * nb; idx += kPotrfThreads )
     {
         const int r = idx / nb, c = idx % nb;
-        if( r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = D[r][c]; }
+        if( r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = static_cast<T>( D[r][c] ); }
     }
     if( tid == 0 && fail >= 0 )
     {
@@ -313,8 +336,9 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, double * __rest
     }
 }
 
+template<typename T>
 __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
-                                                               double * __restrict__ arena, int * __restrict__ status )
+                                                               T * __restrict__ arena, int * __restrict__ status )
 {
     extern __shared__ __align__(16) double psm[];
     potrf_body( tasks[blockIdx.x], arena, status, psm );
@@ -325,7 +349,8 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
 // 452-466): the columns are staged in shared memory; per 8-row sub-block,
 // one thread per column solves the 8 x 8 triangle in registers, then the
 // warps update the rows below with DMMA (warp w owns columns 8w..8w+7).
-__device__ __forceinline__ void trsm_body( const PanelTask & t, double * __restrict__ arena, double * tsm )
+template<typename T>
+__device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__ arena, double * tsm )
 {
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( tsm );
     double (*X)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm + kPanel * (kPanel + 1) );
@@ -337,8 +362,8 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, double * __restr
     const int m = t.n0 - r1;
     const int rest = m + t.n1;
     const int cw = min( kRestChunk, rest - t.c0 );
-    double * U0 = arena + t.u0;
-    double * U1 = arena + t.u1;
+    T * U0 = arena + t.u0;
+    T * U1 = arena + t.u1;
 #pragma unroll 4
     for( int idx = tid; idx < kPanel * kPanel; idx += kTrsmThreads )
     {
@@ -347,8 +372,7 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, double * __restr
         else
         {
             const bool valid = r < nb && c < nb && r <= c;
-            const double * src = U0 + (std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c;
-            cp_async_8( &D[r][c], valid ? src : U0, valid );
+            stage_element( &D[r][c], U0, U0 + (std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c, valid );
         }
     }
 #pragma unroll 4
@@ -357,13 +381,13 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, double * __restr
         const int r = idx / kRestChunk, cc = idx % kRestChunk;
         const int col = t.c0 + cc;
         const bool valid = r < nb && cc < cw;
-        const double * src = U0;
+        const T * src = U0;
         if( valid )
         {
             src = (col < m) ? U0 + (std::int64_t)(t.r0 + r) * t.ld0 + r1 + col
                             : U1 + (std::int64_t)(t.r0 + r) * t.ld1 + (col - m);
         }
-        cp_async_8( &X[r][cc], src, valid );
+        stage_element( &X[r][cc], U0, src, valid );
     }
     cp_async_wait_all();
     __syncthreads();
@@ -411,14 +435,15 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, double * __restr
         const int col = t.c0 + cc;
         if( cc < cw )
         {
-            if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = X[r][cc]; }
-            else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = X[r][cc]; }
+            if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = static_cast<T>( X[r][cc] ); }
+            else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = static_cast<T>( X[r][cc] ); }
         }
     }
 }
 
+template<typename T>
 __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
-                                                             double * __restrict__ arena )
+                                                             T * __restrict__ arena )
 {
     extern __shared__ __align__(16) double tsm[];
     trsm_body( tasks[blockIdx.x], arena, tsm );
@@ -536,12 +561,168 @@ __device__ __forceinline__ void gemm_body( const GemmTask & t, double * __restri
     }
 }
 
+// FP32 storage: the same tile with split-precision 3xTF32 tensor-core
+// products (x = hi + lo with hi, lo TF32; a b ~ a_lo b_hi + a_hi b_lo +
+// a_hi b_hi, FP32 accumulation) on mma.sync m16n8k8: 8 warps in a 2 x 4
+// arrangement of 32 x 16 blocks, 32 k rows per stage, rows padded to 72
+// floats so the fragment loads are conflict-free.
+constexpr int kGemmKF = 32;
+constexpr int kGemmLdF = kTile + 8;
+constexpr int kGemmStageFloats = 2 * kGemmKF * kGemmLdF;
+constexpr size_t kGemmSmemBytesF = sizeof(float) * kGemmStages * kGemmStageFloats;
+
+__device__ __forceinline__ unsigned to_tf32( float x )
+{
+    unsigned r;
+    asm( "cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x) );
+    return r;
+}
+
+__device__ __forceinline__ void split_tf32( float x, unsigned & hi, unsigned & lo )
+{
+    hi = to_tf32( x );
+    lo = to_tf32( x - __uint_as_float( hi ) );
+}
+
+__device__ __forceinline__ void mma_tf32( float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2] )
+{
+    asm volatile( "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                  : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]) );
+}
+
+__device__ __forceinline__ void gemm_body( const GemmTask & t, float * __restrict__ arena, double * smem )
+{
+    float * gsm = reinterpret_cast<float *>( smem );
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;
+    const int g = lane >> 2, tq = lane & 3;
+    const float * A = arena + t.a;
+    const float * B = arena + t.b;
+
+    float acc[2][2][4];
+#pragma unroll
+    for( int i = 0; i < 2; ++i )
+#pragma unroll
+        for( int j = 0; j < 2; ++j )
+#pragma unroll
+            for( int e = 0; e < 4; ++e ) { acc[i][j][e] = 0.0f; }
+
+    constexpr int kChunks = kGemmKF * kTile / 4 / kGemmThreads;      // 2 per operand
+    auto issue = [&]( int stage, int k0 )
+    {
+        float * As = gsm + stage * kGemmStageFloats;
+        float * Bs = As + kGemmKF * kGemmLdF;
+#pragma unroll
+        for( int l = 0; l < kChunks; ++l )
+        {
+            const int idx = tid + kGemmThreads * l;
+            const int r = idx / (kTile / 4), c = 4 * (idx % (kTile / 4));
+            const int k = k0 + r;
+            const int am = min( max( t.M - (t.m0 + c), 0 ), 4 ), bn = min( max( t.N - (t.c0 + c), 0 ), 4 );
+            const int abytes = (k < t.K) ? 4 * am : 0;
+            const int bbytes = (k < t.K) ? 4 * bn : 0;
+            cp_async_16( As + r * kGemmLdF + c, abytes ? A + (std::int64_t)k * t.lda + t.m0 + c : A, abytes );
+            cp_async_16( Bs + r * kGemmLdF + c, bbytes ? B + (std::int64_t)k * t.ldb + t.c0 + c : B, bbytes );
+        }
+    };
+
+    const int nk = (t.K + kGemmKF - 1) / kGemmKF;
+#pragma unroll
+    for( int s = 0; s < kGemmStages - 1; ++s )
+    {
+        if( s < nk ) { issue( s, s * kGemmKF ); }
+        cp_async_commit();
+    }
+    for( int kc = 0; kc < nk; ++kc )
+    {
+        cp_async_wait<kGemmStages - 2>();
+        __syncthreads();
+        {
+            const int nxt = kc + kGemmStages - 1;
+            if( nxt < nk ) { issue( nxt % kGemmStages, nxt * kGemmKF ); }
+            cp_async_commit();
+        }
+        const float * As = gsm + (kc % kGemmStages) * kGemmStageFloats;
+        const float * Bs = As + kGemmKF * kGemmLdF;
+#pragma unroll
+        for( int kk = 0; kk < kGemmKF; kk += 8 )
+        {
+            unsigned ah[2][4], al[2][4], bh[2][2], bl[2][2];
+#pragma unroll
+            for( int mi = 0; mi < 2; ++mi )
+            {
+                const int m = wm * 32 + mi * 16 + g;
+                split_tf32( As[(kk + tq) * kGemmLdF + m],         ah[mi][0], al[mi][0] );
+                split_tf32( As[(kk + tq) * kGemmLdF + m + 8],     ah[mi][1], al[mi][1] );
+                split_tf32( As[(kk + tq + 4) * kGemmLdF + m],     ah[mi][2], al[mi][2] );
+                split_tf32( As[(kk + tq + 4) * kGemmLdF + m + 8], ah[mi][3], al[mi][3] );
+            }
+#pragma unroll
+            for( int nj = 0; nj < 2; ++nj )
+            {
+                const int n = wn * 16 + nj * 8 + g;
+                split_tf32( Bs[(kk + tq) * kGemmLdF + n],     bh[nj][0], bl[nj][0] );
+                split_tf32( Bs[(kk + tq + 4) * kGemmLdF + n], bh[nj][1], bl[nj][1] );
+            }
+#pragma unroll
+            for( int mi = 0; mi < 2; ++mi )
+#pragma unroll
+                for( int nj = 0; nj < 2; ++nj )
+                {
+                    mma_tf32( acc[mi][nj], al[mi], bh[nj] );
+                    mma_tf32( acc[mi][nj], ah[mi], bl[nj] );
+                    mma_tf32( acc[mi][nj], ah[mi], bh[nj] );
+                }
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+
+    float * C = arena + t.c;
+#pragma unroll
+    for( int mi = 0; mi < 2; ++mi )
+    {
+#pragma unroll
+        for( int h = 0; h < 2; ++h )
+        {
+            const int row = t.m0 + wm * 32 + mi * 16 + g + 8 * h;
+            if( row >= t.M ) { continue; }
+            float * Crow = C + (std::int64_t)row * t.ldc;
+#pragma unroll
+            for( int nj = 0; nj < 2; ++nj )
+            {
+                const int col = t.c0 + wn * 16 + nj * 8 + 2 * tq;
+                const bool ok0 = col < t.N && (!t.upper || row <= col);
+                const bool ok1 = col + 1 < t.N && (!t.upper || row <= col + 1);
+                const float v0 = acc[mi][nj][2 * h], v1 = acc[mi][nj][2 * h + 1];
+                if( ok0 && ok1 )
+                {
+                    float2 v = *reinterpret_cast<const float2 *>( Crow + col );
+                    v.x -= v0;
+                    v.y -= v1;
+                    *reinterpret_cast<float2 *>( Crow + col ) = v;
+                }
+                else
+                {
+                    if( ok0 ) { Crow[col] -= v0; }
+                    if( ok1 ) { Crow[col + 1] -= v1; }
+                }
+            }
+        }
+    }
+}
+
+template<typename T>
 __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask * __restrict__ tasks,
-                                                                double * __restrict__ arena )
+                                                                T * __restrict__ arena )
 {
     extern __shared__ __align__(16) double gsm[];
     gemm_body( tasks[blockIdx.x], arena, gsm );
 }
+
+template<typename T> constexpr size_t gemm_smem_bytes() { return sizeof(T) == 8 ? kGemmSmemBytes : kGemmSmemBytesF; }
 
 // ------------------------------------------------------------------ solves
 // The supernodal solves (LowerSolver.hpp:143-305, UpperSolver.hpp:127-255)
@@ -559,7 +740,8 @@ constexpr size_t kInvSmemBytes = sizeof(double) * (2 * kPanel * (kPanel + 1) + k
 // threads stage D and write T.
 constexpr int kInvThreads = 256;
 
-__device__ __forceinline__ void invert_body( const SolveDiagTask & t, const double * __restrict__ arena,
+template<typename S>
+__device__ __forceinline__ void invert_body( const SolveDiagTask & t, const S * __restrict__ arena,
                                              double * __restrict__ out, double * ism )
 {
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( ism );
@@ -567,7 +749,7 @@ __device__ __forceinline__ void invert_body( const SolveDiagTask & t, const doub
     double * inv_d = ism + 2 * kPanel * (kPanel + 1);
     const int tid = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    const double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
+    const S * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
 #pragma unroll 4
     for( int idx = tid; idx < kPanel * kPanel; idx += kInvThreads )
     {
@@ -576,7 +758,7 @@ __device__ __forceinline__ void invert_body( const SolveDiagTask & t, const doub
         else
         {
             const bool valid = r < nb && c < nb && c >= r;
-            cp_async_8( &D[r][c], valid ? U0 + (std::int64_t)r * t.ld0 + c : U0, valid );
+            stage_element( &D[r][c], U0, U0 + (std::int64_t)r * t.ld0 + c, valid );
         }
     }
     cp_async_wait_all();
@@ -606,8 +788,9 @@ __device__ __forceinline__ void invert_body( const SolveDiagTask & t, const doub
     __syncthreads();
 }
 
+template<typename T>
 __global__ __launch_bounds__(kInvThreads) void invert_diag_kernel( const SolveDiagTask * __restrict__ tasks,
-                                                                   const double * __restrict__ arena,
+                                                                   const T * __restrict__ arena,
                                                                    double * __restrict__ tinv )
 {
     extern __shared__ __align__(16) double ism[];
@@ -644,8 +827,9 @@ __device__ __forceinline__ void warp_rows_product( double (&acc)[kSolveMaxRhs / 
 // rest.  Warp w owns rows 8w..8w+7 of every 64 x kp product, kp = k rounded
 // up to a power of two >= 8, and skips row and K blocks beyond the panel's
 // nb rows and the task's cw rest rows.
+template<typename T>
 __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveRestTask * __restrict__ tasks, int upper,
-                                                                    const double * __restrict__ arena,
+                                                                    const T * __restrict__ arena,
                                                                     const double * __restrict__ tinv,
                                                                     const std::int32_t * __restrict__ sn_inner,
                                                                     double * in, double * out, int ld, int k, int lkp )
@@ -682,17 +866,17 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
     }
     if( has_rest )
     {
-        const double * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
-        const double * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
+        const T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
+        const T * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
 #pragma unroll 4
         for( int idx = tid; idx < kPanel * kPanel; idx += kSolveThreads )
         {
             const int i = idx >> 6, jj = idx & 63;
             const int col = t.c0 + jj;
             const bool valid = i < nb && jj < cw;
-            const double * src = U0;
+            const T * src = U0;
             if( valid ) { src = (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col : U1 + (std::int64_t)i * t.ld1 + (col - m); }
-            cp_async_8( &sP[i][jj], src, valid );
+            stage_element( &sP[i][jj], U0, src, valid );
         }
     }
     // y_q: the panel's rows of `in` (forward: every task; backward: the owner)
@@ -845,7 +1029,7 @@ constexpr int kDagThreads = 256;
 constexpr size_t kDagSmemBytes = kTrsmSmemBytes > kInvSmemBytes
     ? (kTrsmSmemBytes > kGemmSmemBytes ? kTrsmSmemBytes : kGemmSmemBytes)
     : (kInvSmemBytes > kGemmSmemBytes ? kInvSmemBytes : kGemmSmemBytes);
-static_assert( kDagSmemBytes >= kPotrfSmemBytes, "persistent kernel shared memory too small" );
+static_assert( kDagSmemBytes >= kPotrfSmemBytes && kDagSmemBytes >= kGemmSmemBytesF, "persistent kernel shared memory too small" );
 
 __device__ __forceinline__ int ld_acquire( const int * p )
 {
@@ -889,8 +1073,10 @@ __device__ int dag_wait( const DagTask & t, const DagArgs & a, int idx )
     return 1;
 }
 
+template<typename T>
 __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagArgs a )
 {
+    T * arena = static_cast<T *>( a.arena );
     extern __shared__ __align__(16) double dsm[];
     __shared__ int s_idx, s_ok;
     const int tid = threadIdx.x;
@@ -920,12 +1106,12 @@ __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagAr
         const DagTask t = a.tasks[idx];
         switch( static_cast<LaunchKind>( t.kind ) )
         {
-            case LaunchKind::Zero:   zero_body( a.zero[t.index], a.arena ); break;
-            case LaunchKind::Extend: extend_body( a.extend[t.index], a.lut, a.arena ); break;
-            case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], a.arena, a.status, dsm ); break;
-            case LaunchKind::Trsm:   trsm_body( a.panel[t.index], a.arena, dsm ); break;
-            case LaunchKind::Gemm:   gemm_body( a.gemm[t.index], a.arena, dsm ); break;
-            case LaunchKind::Invert: invert_body( a.sdiag[t.index], a.arena, a.tinv + (std::int64_t)t.index * (kPanel * kPanel), dsm ); break;
+            case LaunchKind::Zero:   zero_body( a.zero[t.index], arena ); break;
+            case LaunchKind::Extend: extend_body( a.extend[t.index], a.lut, arena ); break;
+            case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], arena, a.status, dsm ); break;
+            case LaunchKind::Trsm:   trsm_body( a.panel[t.index], arena, dsm ); break;
+            case LaunchKind::Gemm:   gemm_body( a.gemm[t.index], arena, dsm ); break;
+            case LaunchKind::Invert: invert_body( a.sdiag[t.index], arena, a.tinv + (std::int64_t)t.index * (kPanel * kPanel), dsm ); break;
             default: break;
         }
         __threadfence();
@@ -989,12 +1175,124 @@ __global__ void residual_kernel( int n, const std::int64_t * __restrict__ outer,
     }
 }
 
-__global__ void gather_diag_kernel( const std::int64_t * __restrict__ offsets, const double * __restrict__ arena,
+// R = B - (A + shift I) X (B != nullptr) or R = (A + shift I) X (B == nullptr)
+// for row-major blocks with leading dimensions: one warp per row, lanes over
+// the row's entries, 8 right-hand sides per pass over the row.
+__global__ void apply_shifted_kernel( int n, const std::int64_t * __restrict__ outer, const std::int32_t * __restrict__ inner,
+                                      const double * __restrict__ vals, double shift,
+                                      const double * __restrict__ X, int ldx, const double * __restrict__ B, int ldb,
+                                      double * __restrict__ R, int ldr, int k )
+{
+    const int lane = threadIdx.x & 31;
+    const std::int64_t warp = (blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x) >> 5;
+    const std::int64_t warps = ((std::int64_t)gridDim.x * blockDim.x) >> 5;
+    for( std::int64_t i = warp; i < n; i += warps )
+    {
+        for( int c0 = 0; c0 < k; c0 += 8 )
+        {
+            double s[8] = { 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0 };
+            for( std::int64_t e = outer[i] + lane; e < outer[i+1]; e += 32 )
+            {
+                const double v = vals[e];
+                const double * xr = X + (std::int64_t)inner[e] * ldx;
+#pragma unroll
+                for( int u = 0; u < 8; ++u ) { if( c0 + u < k ) { s[u] += v * xr[c0 + u]; } }
+            }
+#pragma unroll
+            for( int u = 0; u < 8; ++u )
+            {
+#pragma unroll
+                for( int o = 16; o > 0; o >>= 1 ) { s[u] += __shfl_xor_sync( 0xffffffffu, s[u], o ); }
+            }
+            if( lane < 8 && c0 + lane < k )
+            {
+                double v = 0.0;
+#pragma unroll
+                for( int u = 0; u < 8; ++u ) { if( u == lane ) { v = s[u]; } }
+                const int c = c0 + lane;
+                const double ax = v + shift * X[i * ldx + c];
+                R[i * ldr + c] = B ? B[i * ldb + c] - ax : ax;
+            }
+        }
+    }
+}
+
+// out[c] += sum_i X[i][c] Y[i][c] (out zeroed by the caller).
+__global__ void column_dots_kernel( const double * __restrict__ X, int ldx, const double * __restrict__ Y, int ldy,
+                                    int n, int k, double * __restrict__ out )
+{
+    for( int c = 0; c < k; ++c )
+    {
+        double s = 0.0;
+        for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
+        {
+            s += X[i * ldx + c] * Y[i * ldy + c];
+        }
+#pragma unroll
+        for( int o = 16; o > 0; o >>= 1 ) { s += __shfl_xor_sync( 0xffffffffu, s, o ); }
+        if( (threadIdx.x & 31) == 0 && s != 0.0 ) { atomicAdd( out + c, s ); }
+    }
+}
+
+// Conjugate-gradient updates with per-column scalars kept on the device:
+// alpha_c = rz[c] / pq[c];  x += alpha p;  r -= alpha q.
+__global__ void cg_update_xr_kernel( int n, int k, const double * __restrict__ rz, const double * __restrict__ pq,
+                                     const double * __restrict__ p, const double * __restrict__ q,
+                                     double * __restrict__ x, double * __restrict__ r )
+{
+    const std::int64_t total = (std::int64_t)n * k;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total; e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const int c = static_cast<int>( e % k );
+        const double a = pq[c] != 0.0 ? rz[c] / pq[c] : 0.0;
+        x[e] += a * p[e];
+        r[e] -= a * q[e];
+    }
+}
+
+// beta_c = rz_new[c] / rz_old[c];  p = z + beta p.
+__global__ void cg_update_p_kernel( int n, int k, const double * __restrict__ rz_new, const double * __restrict__ rz_old,
+                                    const double * __restrict__ z, double * __restrict__ p )
+{
+    const std::int64_t total = (std::int64_t)n * k;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total; e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const int c = static_cast<int>( e % k );
+        const double b = rz_old[c] != 0.0 ? rz_new[c] / rz_old[c] : 0.0;
+        p[e] = z[e] + b * p[e];
+    }
+}
+
+__global__ void axpy_kernel( std::int64_t n, double a, const double * __restrict__ x, double * __restrict__ y )
+{
+    for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        y[i] += a * x[i];
+    }
+}
+
+// Y = alpha X + beta Y (beta == 0: Y is not read).
+__global__ void combine_kernel( int n, int k, double alpha, const double * __restrict__ X, int ldx,
+                                double beta, double * __restrict__ Y, int ldy )
+{
+    const std::int64_t total = (std::int64_t)n * k;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total; e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const std::int64_t i = e / k;
+        const int c = static_cast<int>( e % k );
+        double y = alpha * X[i * ldx + c];
+        if( beta != 0.0 ) { y += beta * Y[i * ldy + c]; }
+        Y[i * ldy + c] = y;
+    }
+}
+
+template<typename T>
+__global__ void gather_diag_kernel( const std::int64_t * __restrict__ offsets, const T * __restrict__ arena,
                                     double * __restrict__ out, int n )
 {
     for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
     {
-        out[i] = arena[offsets[i]];
+        out[i] = static_cast<double>( arena[offsets[i]] );
     }
 }
 
@@ -1012,60 +1310,70 @@ int grid_for( std::int64_t work, int threads )
 
 } // namespace
 
+template<typename T>
 void launch_assemble( const double * values, const std::int64_t * src, const std::int64_t * dst,
-                      std::int64_t count, const double * reg, double * arena, cudaStream_t st )
+                      std::int64_t count, const double * reg, T * arena, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
     assemble_kernel<<<grid_for( count, 256 ), 256, 0, st>>>( values, src, dst, count, reg, arena );
 }
 
-void launch_zero( const ZeroTask * tasks, int count, double * arena, cudaStream_t st )
+template<typename T>
+void launch_zero( const ZeroTask * tasks, int count, T * arena, cudaStream_t st )
 {
     if( count > 0 ) { zero_kernel<<<count, 256, 0, st>>>( tasks, arena ); }
 }
 
-void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const double * arena,
+template<typename T>
+void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const T * arena,
                     double * tri, double * rec, cudaStream_t st )
 {
     if( count > 0 ) { export_kernel<<<count, 128, 0, st>>>( tasks, colmap, arena, tri, rec ); }
 }
 
-void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, double * arena, cudaStream_t st )
+template<typename T>
+void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, T * arena, cudaStream_t st )
 {
     if( count > 0 ) { extend_kernel<<<count, 256, 0, st>>>( tasks, lut, arena ); }
 }
 
-void launch_potrf( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st )
+template<typename T>
+void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, cudaStream_t st )
 {
     if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, kPotrfSmemBytes, st>>>( tasks, arena, status ); }
 }
 
-void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st )
+template<typename T>
+void launch_trsm( const PanelTask * tasks, int count, T * arena, cudaStream_t st )
 {
     if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, kTrsmSmemBytes, st>>>( tasks, arena ); }
 }
 
-void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st )
+template<typename T>
+void launch_gemm( const GemmTask * tasks, int count, T * arena, cudaStream_t st )
 {
-    if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, kGemmSmemBytes, st>>>( tasks, arena ); }
+    if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, gemm_smem_bytes<T>(), st>>>( tasks, arena ); }
 }
 
+template<typename T>
 void launch_factor_dag( const DagArgs & args, int grid, cudaStream_t st )
 {
-    if( args.ntasks > 0 && grid > 0 ) { factor_dag_kernel<<<grid, kDagThreads, kDagSmemBytes, st>>>( args ); }
+    if( args.ntasks > 0 && grid > 0 ) { factor_dag_kernel<T><<<grid, kDagThreads, kDagSmemBytes, st>>>( args ); }
 }
 
 int factor_dag_blocks_per_sm()
 {
-    int blocks = 0;
-    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &blocks, factor_dag_kernel, kDagThreads, kDagSmemBytes ) != cudaSuccess )
+    int b64 = 0, b32 = 0;
+    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b64, factor_dag_kernel<double>, kDagThreads, kDagSmemBytes ) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b32, factor_dag_kernel<float>, kDagThreads, kDagSmemBytes ) != cudaSuccess )
     {
         return 0;
     }
-    return blocks;
+    return b64 < b32 ? b64 : b32;
 }
 
-void launch_invert_diag( const SolveDiagTask * tasks, int count, const double * arena, double * tinv, cudaStream_t st )
+template<typename T>
+void launch_invert_diag( const SolveDiagTask * tasks, int count, const T * arena, double * tinv, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
     invert_diag_kernel<<<count, kInvThreads, kInvSmemBytes, st>>>( tasks, arena, tinv );
@@ -1083,13 +1391,39 @@ static size_t solve_smem_bytes( int k )
     return sizeof(double) * (2 * kPanel * kTld + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
 }
 
-void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const double * arena, const double * tinv,
+template<typename T>
+void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const T * arena, const double * tinv,
                         const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
     solve_step_kernel<<<count, kSolveThreads, solve_smem_bytes( k ), st>>>( tasks, upper ? 1 : 0, arena, tinv, sn_inner,
                                                                            in, out, ld, k, solve_lkp( k ) );
 }
+
+template<typename T>
+void launch_gather_diag( const std::int64_t * offsets, const T * arena, double * out, int n, cudaStream_t st )
+{
+    gather_diag_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( offsets, arena, out, n );
+}
+
+#define TB_INSTANTIATE( T )                                                                                          \
+    template void launch_assemble<T>( const double *, const std::int64_t *, const std::int64_t *, std::int64_t,      \
+                                      const double *, T *, cudaStream_t );                                         \
+    template void launch_zero<T>( const ZeroTask *, int, T *, cudaStream_t );                                        \
+    template void launch_export<T>( const ExportTask *, int, const std::int32_t *, const T *, double *, double *,    \
+                                    cudaStream_t );                                                                \
+    template void launch_extend<T>( const ExtendTask *, int, const std::int32_t *, T *, cudaStream_t );             \
+    template void launch_potrf<T>( const PanelTask *, int, T *, int *, cudaStream_t );                               \
+    template void launch_trsm<T>( const PanelTask *, int, T *, cudaStream_t );                                       \
+    template void launch_gemm<T>( const GemmTask *, int, T *, cudaStream_t );                                        \
+    template void launch_factor_dag<T>( const DagArgs &, int, cudaStream_t );                                        \
+    template void launch_invert_diag<T>( const SolveDiagTask *, int, const T *, double *, cudaStream_t );            \
+    template void launch_solve_step<T>( const SolveRestTask *, int, bool, const T *, const double *,                \
+                                        const std::int32_t *, double *, double *, int, int, cudaStream_t );         \
+    template void launch_gather_diag<T>( const std::int64_t *, const T *, double *, int, cudaStream_t );
+TB_INSTANTIATE( double )
+TB_INSTANTIATE( float )
+#undef TB_INSTANTIATE
 
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
                          int n, int k, cudaStream_t st )
@@ -1111,33 +1445,59 @@ void launch_residual( int n, const std::int64_t * outer, const std::int32_t * in
 
 cudaError_t configure_kernels()
 {
+    const struct { const void * fn; size_t bytes; } attrs[] = {
+        { reinterpret_cast<const void *>( trsm_kernel<double> ), kTrsmSmemBytes },
+        { reinterpret_cast<const void *>( trsm_kernel<float> ), kTrsmSmemBytes },
+        { reinterpret_cast<const void *>( gemm_tn_kernel<double> ), kGemmSmemBytes },
+        { reinterpret_cast<const void *>( gemm_tn_kernel<float> ), kGemmSmemBytesF },
+        { reinterpret_cast<const void *>( factor_dag_kernel<double> ), kDagSmemBytes },
+        { reinterpret_cast<const void *>( factor_dag_kernel<float> ), kDagSmemBytes },
+        { reinterpret_cast<const void *>( invert_diag_kernel<double> ), kInvSmemBytes },
+        { reinterpret_cast<const void *>( invert_diag_kernel<float> ), kInvSmemBytes },
+        { reinterpret_cast<const void *>( solve_step_kernel<double> ), solve_smem_bytes( kSolveMaxRhs ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float> ), solve_smem_bytes( kSolveMaxRhs ) },
+    };
+    for( const auto & a : attrs )
     {
-        const cudaError_t g = cudaFuncSetAttribute( trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)kTrsmSmemBytes );
-        if( g != cudaSuccess ) { return g; }
+        const cudaError_t e = cudaFuncSetAttribute( a.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a.bytes );
+        if( e != cudaSuccess ) { return e; }
     }
-    {
-        const cudaError_t g = cudaFuncSetAttribute( gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)kGemmSmemBytes );
-        if( g != cudaSuccess ) { return g; }
-    }
-    {
-        const cudaError_t g = cudaFuncSetAttribute( factor_dag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)kDagSmemBytes );
-        if( g != cudaSuccess ) { return g; }
-    }
-    {
-        const cudaError_t g = cudaFuncSetAttribute( invert_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)kInvSmemBytes );
-        if( g != cudaSuccess ) { return g; }
-    }
-    return cudaFuncSetAttribute( solve_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)solve_smem_bytes( kSolveMaxRhs ) );
+    return cudaSuccess;
 }
 
-void launch_gather_diag( const std::int64_t * offsets, const double * arena, double * out, int n, cudaStream_t st )
+void launch_apply_shifted( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
+                           double shift, const double * X, int ldx, const double * B, int ldb, double * R, int ldr,
+                           int k, cudaStream_t st )
 {
-    gather_diag_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( offsets, arena, out, n );
+    apply_shifted_kernel<<<grid_for( (std::int64_t)n * 32, 256 ), 256, 0, st>>>( n, outer, inner, vals, shift, X, ldx,
+                                                                                B, ldb, R, ldr, k );
+}
+
+void launch_column_dots( const double * X, int ldx, const double * Y, int ldy, int n, int k, double * out, cudaStream_t st )
+{
+    column_dots_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( X, ldx, Y, ldy, n, k, out );
+}
+
+void launch_cg_update_xr( int n, int k, const double * rz, const double * pq, const double * p, const double * q,
+                          double * x, double * r, cudaStream_t st )
+{
+    cg_update_xr_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( n, k, rz, pq, p, q, x, r );
+}
+
+void launch_cg_update_p( int n, int k, const double * rz_new, const double * rz_old, const double * z, double * p,
+                         cudaStream_t st )
+{
+    cg_update_p_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( n, k, rz_new, rz_old, z, p );
+}
+
+void launch_axpy( std::int64_t n, double a, const double * x, double * y, cudaStream_t st )
+{
+    axpy_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( n, a, x, y );
+}
+
+void launch_combine( int n, int k, double alpha, const double * X, int ldx, double beta, double * Y, int ldy, cudaStream_t st )
+{
+    combine_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( n, k, alpha, X, ldx, beta, Y, ldy );
 }
 
 void launch_init_status( int * status, cudaStream_t st )

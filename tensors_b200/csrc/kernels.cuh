@@ -13,15 +13,19 @@ constexpr int kSolveMaxRhs = 64;   // right-hand sides per solve launch
 
 // status[0]: bit 0 set when a pivot was not positive; status[1]: smallest
 // failing (permuted) row index (initialised to INT_MAX).
+// T: factor storage, double (FP64 path) or float (mixed precision: FP32
+// storage, 3xTF32 Schur updates, FP64 panel factorization and solves).
+template<typename T>
 void launch_assemble( const double * values, const std::int64_t * src, const std::int64_t * dst,
-                      std::int64_t count, const double * reg, double * arena, cudaStream_t st );
-void launch_zero( const ZeroTask * tasks, int count, double * arena, cudaStream_t st );
-void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const double * arena,
+                      std::int64_t count, const double * reg, T * arena, cudaStream_t st );
+template<typename T> void launch_zero( const ZeroTask * tasks, int count, T * arena, cudaStream_t st );
+template<typename T>
+void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const T * arena,
                     double * tri, double * rec, cudaStream_t st );
-void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, double * arena, cudaStream_t st );
-void launch_potrf( const PanelTask * tasks, int count, double * arena, int * status, cudaStream_t st );
-void launch_trsm( const PanelTask * tasks, int count, double * arena, cudaStream_t st );
-void launch_gemm( const GemmTask * tasks, int count, double * arena, cudaStream_t st );
+template<typename T> void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, T * arena, cudaStream_t st );
+template<typename T> void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, cudaStream_t st );
+template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, cudaStream_t st );
+template<typename T> void launch_gemm( const GemmTask * tasks, int count, T * arena, cudaStream_t st );
 
 // The numeric factorization as one persistent launch over the plan's task
 // graph (Plan::dag).  counters (dag_counters ints), next and error must be
@@ -34,7 +38,7 @@ struct DagArgs
     int * counters;
     int * next;
     int * error;
-    double * arena;
+    void * arena;                 // factor storage (double or float, the launch's type)
     int * status;
     const ZeroTask * zero;
     const ExtendTask * extend;
@@ -51,15 +55,17 @@ struct DagArgs
     unsigned long long * trace;
 };
 constexpr unsigned kDagMaxSpins = 1u << 26;    // bound on polls of one wait, besides the time limit
-void launch_factor_dag( const DagArgs & args, int grid, cudaStream_t st );
+template<typename T> void launch_factor_dag( const DagArgs & args, int grid, cudaStream_t st );
 // Resident CTAs per SM of the persistent kernel (0 on error).
 int factor_dag_blocks_per_sm();
 
 // Inverse of every panel's diagonal block into tinv (count x 64 x 64).
-void launch_invert_diag( const SolveDiagTask * tasks, int count, const double * arena, double * tinv, cudaStream_t st );
+template<typename T>
+void launch_invert_diag( const SolveDiagTask * tasks, int count, const T * arena, double * tinv, cudaStream_t st );
 // One forward (upper = false) or backward solve step over `count` tasks;
 // in / out row-major with leading dimension ld, k <= kSolveMaxRhs columns.
-void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const double * arena, const double * tinv,
+template<typename T>
+void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const T * arena, const double * tinv,
                         const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st );
 
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
@@ -69,7 +75,21 @@ void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv,
 void launch_residual( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
                       const double * X, const double * B, double * R, int k, cudaStream_t st );
 void launch_init_status( int * status, cudaStream_t st );
-void launch_gather_diag( const std::int64_t * offsets, const double * arena, double * out, int n, cudaStream_t st );
+// R = B - (A + shift I) X, or (A + shift I) X when B is null;
+// out[c] += X(:, c) . Y(:, c); the two CG updates with per-column scalars on
+// the device; y += a x; Y = alpha X + beta Y.
+void launch_apply_shifted( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
+                           double shift, const double * X, int ldx, const double * B, int ldb, double * R, int ldr,
+                           int k, cudaStream_t st );
+void launch_column_dots( const double * X, int ldx, const double * Y, int ldy, int n, int k, double * out, cudaStream_t st );
+void launch_cg_update_xr( int n, int k, const double * rz, const double * pq, const double * p, const double * q,
+                          double * x, double * r, cudaStream_t st );
+void launch_cg_update_p( int n, int k, const double * rz_new, const double * rz_old, const double * z, double * p,
+                         cudaStream_t st );
+void launch_axpy( std::int64_t n, double a, const double * x, double * y, cudaStream_t st );
+void launch_combine( int n, int k, double alpha, const double * X, int ldx, double beta, double * Y, int ldy, cudaStream_t st );
+template<typename T>
+void launch_gather_diag( const std::int64_t * offsets, const T * arena, double * out, int n, cudaStream_t st );
 
 // Raises the dynamic shared-memory limits of the solve kernels on the
 // current device; call once per device before the first launch.

@@ -93,7 +93,8 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         const std::string at = " (gemm task " + std::to_string( k ) + ")";
         if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad gemm dimensions" + at; }
         if( t.M > t.lda || t.N > t.ldb || t.N > t.ldc ) { return "gemm leading dimension too small" + at; }
-        if( (t.a | t.b | t.c) % 2 != 0 || (t.lda | t.ldb | t.ldc) % 2 != 0 ) { return "gemm operand not 16-byte aligned" + at; }
+        // 16-byte copies of FP64 (2 entries) and FP32 (4 entries) storage
+        if( (t.a | t.b | t.c) % 4 != 0 || (t.lda | t.ldb | t.ldc) % 4 != 0 ) { return "gemm operand not 16-byte aligned" + at; }
         if( !in_range( t.a, t.a + static_cast<I64>(t.K - 1) * t.lda + t.M - 1, arena ) ) { return "gemm A out of range" + at; }
         if( !in_range( t.b, t.b + static_cast<I64>(t.K - 1) * t.ldb + t.N - 1, arena ) ) { return "gemm B out of range" + at; }
         if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at; }
