@@ -233,6 +233,31 @@ int tb_chol_solve_profile( tb_chol * h, int64_t * info, double * ms, int32_t cap
 /* Number of kernel launches the last numeric factorization / solve issued. */
 int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * solve_launches );
 
+/* ------------------------------------------------------------------------
+ * Batches of independent systems (no counterpart in the reference, which
+ * factors one matrix per object).  The systems become the diagonal blocks of
+ * one matrix handled by a tb_chol (tb_batch_handle gives it, for setters such
+ * as the precision and for statistics); its schedule defaults to one
+ * persistent launch for the whole batch (TB_SCHEDULE_TASK_GRAPH_ALL).  Each
+ * system keeps its own pattern, permutation (NULL: identity) and values;
+ * right-hand sides and solutions are per system (host calls) or the systems'
+ * row-major n_s x nrhs blocks stacked in system order (device calls, row
+ * offsets from tb_batch_offsets). */
+typedef struct tb_batch tb_batch;
+int tb_batch_create( tb_batch ** out, int32_t count, const int32_t * n, const int64_t * const * outer,
+                     const int32_t * const * inner, const int32_t * const * perm, int32_t thread_count );
+int tb_batch_destroy( tb_batch * b );
+int tb_batch_handle( tb_batch * b, tb_chol ** out );
+int tb_batch_count( tb_batch * b, int32_t * out );
+/* count + 1 entries each: first row and first value of every system. */
+int tb_batch_offsets( tb_batch * b, int64_t * row_offsets, int64_t * value_offsets );
+int tb_batch_numeric( tb_batch * b, const double * const * values, double reg );
+int tb_batch_numeric_device( tb_batch * b, const double * d_values, double reg );
+/* First system whose factorization failed (-1: none). */
+int tb_batch_failed_system( tb_batch * b, int32_t * out );
+int tb_batch_solve( tb_batch * b, const double * const * B, double * const * X, int32_t nrhs );
+int tb_batch_solve_device( tb_batch * b, const double * d_B, double * d_X, int32_t nrhs );
+
 #ifdef __cplusplus
 }
 #endif

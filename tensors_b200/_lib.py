@@ -66,6 +66,16 @@ SIGNATURES = {
     "tb_chol_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_kernel_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "tb_chol_launch_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
+    "tb_batch_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, _vp, _vp, _vp, _vp, _i32]),
+    "tb_batch_destroy": (ctypes.c_int, [_vp]),
+    "tb_batch_handle": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "tb_batch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_batch_offsets": (ctypes.c_int, [_vp, _vp, _vp]),
+    "tb_batch_numeric": (ctypes.c_int, [_vp, _vp, _d]),
+    "tb_batch_numeric_device": (ctypes.c_int, [_vp, _vp, _d]),
+    "tb_batch_failed_system": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_batch_solve": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
+    "tb_batch_solve_device": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
 }
 
 _LIB = None

@@ -86,11 +86,22 @@ class CholeskyDecomposition:
         _check(lib().tb_chol_create(ctypes.byref(h), self._n, self._outer.ctypes.data, self._inner.ctypes.data,
                                     None if self._perm is None else self._perm.ctypes.data, int(thread_count)))
         self._h = h
+        self._owned = True
+
+    @classmethod
+    def _wrap(cls, h, n):
+        """A view of a handle owned elsewhere (a batch's combined handle)."""
+        obj = cls.__new__(cls)
+        obj._h = h
+        obj._n = int(n)
+        obj._outer = obj._inner = obj._perm = None
+        obj._owned = False
+        return obj
 
     def close(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
+        if getattr(self, "_h", None) is not None and self._h.value and getattr(self, "_owned", True):
             lib().tb_chol_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -241,7 +252,9 @@ class CholeskyDecomposition:
         return self._n
 
     def NonzeroCount(self) -> int:
-        return int(self._outer[-1])
+        v = ctypes.c_int64()
+        _check(lib().tb_chol_nonzero_count(self._h, ctypes.byref(v)))
+        return v.value
 
     def SN_Count(self) -> int:
         v = ctypes.c_int32()
@@ -415,3 +428,86 @@ class CholeskyDecomposition:
 
 def _is_cuda_tensor(x) -> bool:
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+class BatchedCholesky:
+    """Many independent SPD systems factored and solved together (tb_batch_*).
+
+    ``systems`` is a list of ``(outer, inner, perm)`` (perm may be None).  The
+    systems become the diagonal blocks of one matrix whose factorization runs
+    as a single persistent launch; ``handle`` gives the underlying
+    :class:`CholeskyDecomposition` for precision, refinement and statistics.
+    """
+
+    def __init__(self, systems, thread_count: int = 1):
+        self._keep = []
+        count = len(systems)
+        n = np.zeros(count, dtype=np.int32)
+        outer_p = (ctypes.c_void_p * count)()
+        inner_p = (ctypes.c_void_p * count)()
+        perm_p = (ctypes.c_void_p * count)()
+        for s, (outer, inner, perm) in enumerate(systems):
+            o = np.ascontiguousarray(outer, dtype=np.int64)
+            i = np.ascontiguousarray(inner, dtype=np.int32)
+            n[s] = len(o) - 1
+            outer_p[s] = o.ctypes.data
+            inner_p[s] = i.ctypes.data
+            self._keep += [o, i]
+            if perm is not None:
+                p = np.ascontiguousarray(perm, dtype=np.int32)
+                perm_p[s] = p.ctypes.data
+                self._keep.append(p)
+        self._b = ctypes.c_void_p()
+        _check(lib().tb_batch_create(ctypes.byref(self._b), count, n.ctypes.data, ctypes.addressof(outer_p),
+                                     ctypes.addressof(inner_p), ctypes.addressof(perm_p), int(thread_count)))
+        self._keep.clear()
+        self.count = count
+        self.sizes = n.astype(np.int64)
+        self.row_offsets = np.zeros(count + 1, dtype=np.int64)
+        self.value_offsets = np.zeros(count + 1, dtype=np.int64)
+        _check(lib().tb_batch_offsets(self._b, self.row_offsets.ctypes.data, self.value_offsets.ctypes.data))
+        h = ctypes.c_void_p()
+        _check(lib().tb_batch_handle(self._b, ctypes.byref(h)))
+        self.handle = CholeskyDecomposition._wrap(h, self.row_offsets[-1])
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().tb_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def NumericFactorization(self, values, reg: float = 0.0) -> int:
+        """values: list of per-system arrays, or one concatenated CUDA tensor / array."""
+        if isinstance(values, (list, tuple)):
+            vs = [np.ascontiguousarray(v, dtype=np.float64) for v in values]
+            ptrs = (ctypes.c_void_p * self.count)(*[v.ctypes.data for v in vs])
+            return _check(lib().tb_batch_numeric(self._b, ctypes.addressof(ptrs), float(reg)))
+        if _is_cuda_tensor(values):
+            return _check(lib().tb_batch_numeric_device(self._b, values.data_ptr(), float(reg)))
+        return self.handle.NumericFactorization(np.ascontiguousarray(values, dtype=np.float64), reg)
+
+    def FailedSystem(self) -> int:
+        v = ctypes.c_int32()
+        _check(lib().tb_batch_failed_system(self._b, ctypes.byref(v)))
+        return v.value
+
+    def Solve(self, B, X=None):
+        """B: list of per-system (n_s,) or (n_s, k) arrays -> list of solutions; or a stacked CUDA tensor."""
+        if _is_cuda_tensor(B):
+            k = 1 if B.dim() == 1 else B.shape[1]
+            if X is None:
+                X = B.new_empty(B.shape)
+            _check(lib().tb_batch_solve_device(self._b, B.data_ptr(), X.data_ptr(), int(k)))
+            return X
+        Bs = [np.ascontiguousarray(b, dtype=np.float64) for b in B]
+        k = 1 if Bs[0].ndim == 1 else Bs[0].shape[1]
+        Xs = [np.empty_like(b) for b in Bs]
+        bp = (ctypes.c_void_p * self.count)(*[b.ctypes.data for b in Bs])
+        xp = (ctypes.c_void_p * self.count)(*[x.ctypes.data for x in Xs])
+        _check(lib().tb_batch_solve(self._b, ctypes.addressof(bp), ctypes.addressof(xp), int(k)))
+        return Xs

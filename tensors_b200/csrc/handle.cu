@@ -33,6 +33,13 @@ int fail( int code, const std::string & msg )
     return code;
 }
 
+} // namespace
+
+void tb::set_last_error( const std::string & msg ) { g_error = msg; }
+
+namespace
+{
+
 #define TB_CUDA( call )                                                                              \
     do {                                                                                             \
         cudaError_t e_ = (call);                                                                     \
