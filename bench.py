@@ -232,6 +232,172 @@ def run_for_profiler(args):
     return 0
 
 
+# ------------------------------------------------------------ other configs
+C3_GRID, C3_SEED, C3_SHIFT, C3_NRHS = 48, 0x5EED0003, 1e-2, 8
+C4_COUNT, C4_SEED, C4_MIN, C4_MAX = 2000, 0x5EED0004, 500, 20000
+# The random Delaunay meshes carry near-flat hull triangles whose cotangent
+# weights reach ~1e6 while the lumped mass is ~1e-8: kappa ~1e12-1e14.  The
+# plain FP64 direct solve attains a relative residual of ~2e-8 on them, so the
+# batch's refinement target is 1e-7 (the 1e-10 target of C3 / C5 is out of
+# reach of any FP64 solver here).
+C4_TARGET = 1e-7
+TARGET_RELRES = 1e-10
+
+
+def _time_steps(torch, stream, fn, steps, warmup):
+    """(mean ms of fn() per step, mean ms of its first phase) with CUDA events on `stream`."""
+    for _ in range(warmup):
+        fn(None)
+    torch.cuda.synchronize()
+    tot, first = [], []
+    for _ in range(steps):
+        s, m, e = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        s.record(stream)
+        fn(m)
+        e.record(stream)
+        e.synchronize()
+        tot.append(s.elapsed_time(e))
+        first.append(s.elapsed_time(m))
+    return statistics.mean(tot), statistics.mean(first)
+
+
+def run_c3(args):
+    """Mixed precision vs FP64 on the 3-dof 27-point vector Laplacian (48^3 nodes, n = 331,776).
+
+    The stiffness sum_e [[B,-B],[-B,B]] with SPD edge blocks B = G G^T + 0.1 I is
+    singular (rigid translations are in its null space), so the matrix carries
+    a 1e-2 diagonal shift.  Both paths solve 8 RHS to the same 1e-10 relative
+    residual target; the FP64 path reaches ~1e-14 directly.
+    """
+    import torch
+    from tensors_b200 import build as tb_build
+    from tensors_b200 import matrices, ordering
+    from tensors_b200.cholesky import CholeskyDecomposition
+
+    tb_build.build()
+    dev = torch.device("cuda", 0)
+    A = matrices.vector_laplacian_3d(C3_GRID, C3_SEED, C3_SHIFT)
+    perm = ordering.nested_dissection(A)
+    B = torch.tensor(np.random.default_rng(C3_SEED + 1).standard_normal((A.n, C3_NRHS)), device=dev)
+    vals = torch.tensor(A.values, device=dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        c = CholeskyDecomposition(A.outer, A.inner, perm)
+        c.SetPrecision(prec)
+        c.SetRefinement(TARGET_RELRES, 30)
+        c.SetStream(stream)
+        c.SymbolicFactorization()
+        X = torch.empty_like(B)
+
+        def step(mid):
+            assert c.NumericFactorization(vals, 0.0) == 0
+            if mid is not None:
+                mid.record(stream)
+            c.Solve(B, X)
+
+        with ClockSampler(0) as clocks:
+            t, tf = _time_steps(torch, stream, step, args.steps, args.warmup)
+        R = c.Residual(B, X)
+        stream.synchronize()
+        rr = float((torch.linalg.norm(R, dim=0) / torch.linalg.norm(B, dim=0)).max())
+        F, nnz_u = c.FlopCount()
+        out[prec] = {"ms": t, "factor_ms": tf, "solve_ms": t - tf, "relres": rr,
+                     "refinement": c.RefinementInfo() if prec == "mixed" else None,
+                     "clocks": clocks.summary()}
+    flops = F + 4.0 * C3_NRHS * nnz_u
+    line = {
+        "metric": "factor+solve GFLOP/s to 1e-10 relative residual, mixed precision (FP32 factor, 3xTF32 updates, "
+                  "FP64 refinement) vs plain FP64, 48^3 3-dof 27-pt vector Laplacian, 8 RHS",
+        "value": flops / (out["mixed"]["ms"] * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": out["mixed"]["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"3-dof 27-point vector Laplacian {C3_GRID}^3 (n={A.n}), SPD 3x3 edge blocks "
+                               f"G G^T + 0.1 I, shift {C3_SHIFT:g}, nested dissection, {C3_NRHS} RHS",
+                   "factor_gflop": F / 1e9, "fp64": out["fp64"], "mixed": out["mixed"],
+                   "speedup_mixed_over_fp64": out["fp64"]["ms"] / out["mixed"]["ms"],
+                   "l2": "factor and matrix exceed L2"},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def _c4_system(args):
+    s, m = args
+    from tensors_b200 import matrices, ordering
+
+    A = matrices.delaunay_laplacian(int(m), C4_SEED + s, 1e-3)
+    return A.outer, A.inner, A.values, ordering.nested_dissection(A)
+
+
+def c4_systems(count=C4_COUNT):
+    """The batch: Delaunay meshes of m ~ U[500, 20000] uniform points, cotangent Laplacian + 1e-3 lumped mass."""
+    import multiprocessing as mp
+
+    ms = np.random.default_rng(C4_SEED).integers(C4_MIN, C4_MAX + 1, size=count)
+    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        return pool.map(_c4_system, list(enumerate(ms)), chunksize=8)
+
+
+def run_c4(args):
+    """2,000 independent Delaunay systems factored as one batch (one persistent launch), FP32 factor + FP64
+    refinement to 1e-10, 1 RHS each."""
+    systems = c4_systems(args.batch or C4_COUNT)       # process pool before any GPU call
+    import torch
+    from tensors_b200 import build as tb_build
+    from tensors_b200.cholesky import BatchedCholesky
+
+    tb_build.build()
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    b = BatchedCholesky([(o, i, p) for o, i, v, p in systems])
+    b.handle.SetPrecision("mixed")
+    b.handle.SetRefinement(C4_TARGET, 60)
+    b.handle.SetSchedule(args.schedule or "task_graph_all")
+    b.handle.SymbolicFactorization()
+    t_setup = time.perf_counter() - t0
+    vals = torch.tensor(np.concatenate([v for o, i, v, p in systems]), device=dev)
+    n = int(b.row_offsets[-1])
+    B = torch.tensor(np.random.default_rng(C4_SEED + 1).standard_normal(n), device=dev)
+    X = torch.empty_like(B)
+    stream = torch.cuda.Stream(dev)
+    b.handle.SetStream(stream)
+    torch.cuda.set_stream(stream)
+
+    def step(mid):
+        assert b.NumericFactorization(vals, 0.0) == 0
+        if mid is not None:
+            mid.record(stream)
+        b.Solve(B, X)
+
+    with ClockSampler(0) as clocks:
+        t, tf = _time_steps(torch, stream, step, args.steps, args.warmup)
+    stream.synchronize()
+    it, rr = b.handle.RefinementInfo()
+    R = b.handle.Residual(B, X)
+    stream.synchronize()
+    relres = float(torch.linalg.norm(R) / torch.linalg.norm(B))
+    F, nnz_u = b.handle.FlopCount()
+    flops = F + 4.0 * nnz_u
+    line = {
+        "metric": f"batched factor+solve GFLOP/s, {len(systems)} Delaunay systems, FP32 factor + FP64 refinement "
+                  f"to {C4_TARGET:g}",
+        "value": flops / (t * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{len(systems)} 2D Delaunay meshes, m ~ U[{C4_MIN}, {C4_MAX}] points, cotangent "
+                               "Laplacian + 1e-3 lumped mass, nested dissection each, 1 RHS each",
+                   "rows": n, "factor_gflop": F / 1e9, "factor_ms": tf, "solve_ms": t - tf,
+                   "systems_per_s": len(systems) / (t * 1e-3), "refinement": [it, rr], "relres": relres,
+                   "perturbed_pivots": b.handle.PerturbedPivots(),
+                   "schedule": args.schedule or "task_graph_all", "setup_s": t_setup,
+                   "plan": b.handle.PlanStats(), "clocks": clocks.summary()},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -240,6 +406,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=GRID, help="grid edge (profiling runs on smaller cases)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+                    help="c2 (default): the headline FP64 64^3 Laplacian; c3: mixed vs FP64 vector Laplacian; "
+                         "c4: batched Delaunay systems; c5: serving stream")
+    ap.add_argument("--batch", type=int, default=0, help="c4: number of systems (default 2000)")
+    ap.add_argument("--schedule", default=None, help="c4: factorization schedule of the batch")
     ap.add_argument("--ncu", action="store_true",
                     help="profiling run for ncu: warmup + steps factor+solve as direct launches, no timing, "
                          "no baselines")
@@ -248,6 +419,12 @@ def main():
         return run_reference(args)
     if args.ncu:
         return run_for_profiler(args)
+    if args.workload == "c3":
+        return run_c3(args)
+    if args.workload == "c4":
+        return run_c4(args)
+    if args.workload == "c5":
+        return run_c5(args)
 
     import torch
     import torch.distributed as dist

@@ -44,7 +44,8 @@ enum tb_status {
     TB_ERR_CUDA                = -6,
     TB_ERR_OUT_OF_MEMORY       = -7,
     TB_ERR_NO_DEVICE           = -8,
-    TB_ERR_TIMEOUT             = -9
+    TB_ERR_TIMEOUT             = -9,
+    TB_ERR_NOT_CONVERGED       = -10
 };
 
 /* Supernode strategies (CholeskyDecomposition.hpp:119-124). */
@@ -186,6 +187,14 @@ int tb_chol_set_precision( tb_chol * h, int32_t precision );
 int tb_chol_set_refinement( tb_chol * h, double tol, int32_t max_iterations );
 /* Refinement steps and final relative residual of the last mixed solve. */
 int tb_chol_refinement_info( tb_chol * h, int32_t * iterations, double * relres );
+/* Mixed precision only: pivots of the last factorization that came out at or
+ * below tau = 1e-5 x |assembled diagonal entry of the row| and were raised to
+ * tau instead of failing (static pivoting: for ill-conditioned matrices FP32
+ * rounding of the Schur complements can wipe out small pivots, and the FP64
+ * refinement corrects the perturbation).  In this mode a matrix that is not
+ * positive definite is reported by the solve, whose refinement then does not
+ * reach its target (TB_ERR_NOT_CONVERGED), not by the factorization. */
+int tb_chol_perturbed_pivots( tb_chol * h, int32_t * out );
 /* Schedule of the numeric factorization.  TB_SCHEDULE_LEVELS (default): one
  * launch per task kind, level and panel step (also used while profiling).
  * TB_SCHEDULE_TASK_GRAPH: the levels below the first level with 8

@@ -147,6 +147,12 @@ class CholeskyDecomposition:
         _check(lib().tb_chol_refinement_info(self._h, ctypes.byref(it), ctypes.byref(rr)))
         return it.value, rr.value
 
+    def PerturbedPivots(self) -> int:
+        """Mixed precision: pivots raised to their floor in the last factorization."""
+        v = ctypes.c_int32()
+        _check(lib().tb_chol_perturbed_pivots(self._h, ctypes.byref(v)))
+        return v.value
+
     def SetSchedule(self, schedule) -> None:
         """'levels' (default: one launch per kind, level and step), 'task_graph' (level launches, then one
         persistent launch for the levels with long panel chains) or 'task_graph_all' (every level in the

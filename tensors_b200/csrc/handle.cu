@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -26,6 +27,8 @@ thread_local std::string g_error = "no error";
 int g_device = 0;
 // Bound on one dependency wait of the persistent factorization kernel.
 constexpr unsigned long long kDagTimeoutNs = 2000000000ull;
+// Mixed precision: a pivot is raised to this fraction of its row's assembled diagonal entry.
+constexpr double kPivotFloorRel = 1e-5;
 
 int fail( int code, const std::string & msg )
 {
@@ -153,6 +156,8 @@ struct tb_chol
     std::int32_t ir_iters = 0;
     double ir_relres = 0.0;
     DeviceArray<double> ir_x, ir_r, ir_norms;
+    DeviceArray<double> pivot_floor;             // mixed precision: static-pivot floor per row
+    std::int32_t perturbed_pivots = 0;
     PinnedBuffer pin_norms;
     bool trace = false;                          // record the persistent launch's execution trace
     DeviceArray<unsigned long long> trace_buf;
@@ -302,9 +307,10 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->a_inner.upload( h->inner, st_ ) );
     TB_TRY( h->values.reserve( s.nnz ) );
     TB_TRY( h->reg.reserve( 1 ) );
-    TB_TRY( h->status.reserve( 2 ) );
+    TB_TRY( h->status.reserve( 3 ) );
     TB_TRY( h->diag_off.upload( pl.diag_offset, st_ ) );
     TB_TRY( h->diag_vals.reserve( s.n ) );
+    if( h->precision == TB_PRECISION_MIXED ) { TB_TRY( h->pivot_floor.reserve( s.n ) ); }
     TB_TRY( h->tinv.reserve( static_cast<std::int64_t>( pl.sdiag.size() ) * tb::kPanel * tb::kPanel ) );
     TB_TRY( h->dag.upload( pl.dag, st_ ) );
     TB_TRY( h->dag_state.reserve( static_cast<std::int64_t>( pl.dag_counters ) + 2 ) );
@@ -339,6 +345,13 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
     tb::launch_init_status( h->status.ptr, st );
     tb::launch_assemble( h->values.ptr, h->asm_src.ptr, h->asm_dst.ptr,
                          static_cast<std::int64_t>( pl.asm_src.size() ), h->reg.ptr, A, st );
+    const double * floor = nullptr;
+    if constexpr ( sizeof(T) == 4 )
+    {
+        tb::launch_pivot_floor( h->diag_off.ptr, A, kPivotFloorRel, h->pivot_floor.ptr, h->n, st );
+        floor = h->pivot_floor.ptr;
+        ++launches;
+    }
     mark( 7 );
     launches += 2;
     if( h->use_dag && !timed )
@@ -349,7 +362,7 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
             {
                 case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
                 case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
-                case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, st ); break;
+                case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, st ); break;
                 case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
                 case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
                 case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
@@ -362,7 +375,7 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         tb::DagArgs a{};
         a.tasks = h->dag.ptr; a.ntasks = static_cast<int>( pl.dag.size() );
         a.counters = h->dag_state.ptr; a.next = h->dag_state.ptr + nc; a.error = h->dag_state.ptr + nc + 1;
-        a.arena = A; a.status = h->status.ptr;
+        a.arena = A; a.status = h->status.ptr; a.pivot_floor = floor;
         a.zero = h->zero.ptr; a.extend = h->extend.ptr; a.lut = h->lut.ptr;
         a.potrf = h->potrf.ptr; a.panel = h->panel.ptr; a.gemm = h->gemm.ptr;
         a.sdiag = h->sdiag.ptr; a.tinv = h->tinv.ptr;
@@ -377,7 +390,7 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         {
             case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
             case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
-            case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, st ); break;
+            case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, st ); break;
             case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
             case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
             case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
@@ -448,19 +461,20 @@ int run_factor( tb_chol * h, double reg )
         TB_CUDA( cudaGetLastError() );
     }
     int * ps = reinterpret_cast<int*>( pr + 1 );
-    ps[2] = 0;
-    TB_CUDA( cudaMemcpyAsync( ps, h->status.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, st ) );
+    ps[3] = 0;
+    TB_CUDA( cudaMemcpyAsync( ps, h->status.ptr, 3 * sizeof(int), cudaMemcpyDeviceToHost, st ) );
     if( h->use_dag && !h->profiling )
     {
-        TB_CUDA( cudaMemcpyAsync( ps + 2, h->dag_state.ptr + h->plan.dag_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st ) );
+        TB_CUDA( cudaMemcpyAsync( ps + 3, h->dag_state.ptr + h->plan.dag_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, st ) );
     }
     TB_CUDA( cudaStreamSynchronize( st ) );
-    if( ps[2] != 0 )
+    h->perturbed_pivots = ps[2];
+    if( ps[3] != 0 )
     {
         h->factorized = false;
         h->good = false;
         return fail( TB_ERR_TIMEOUT, "NumericFactorization: persistent launch stopped, the wait of task "
-                     + std::to_string( ps[2] - 1 ) + " ran out of time" );
+                     + std::to_string( ps[3] - 1 ) + " ran out of time" );
     }
     h->factorized = true;                       // marked in any case, Numeric.hpp:94-95
     h->good = (ps[0] == 0);
@@ -730,6 +744,13 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
     tb::launch_combine( n, k, alpha, X, k, beta, d_X, ldX, st );
     h->solve_launch_count = launches + 1;
     TB_CUDA( cudaGetLastError() );
+    if( !(h->ir_relres <= h->ir_tol) )
+    {
+        char msg[160];
+        std::snprintf( msg, sizeof(msg), "Solve: refinement stopped at relative residual %.3e after %d steps (target %.3e)",
+                       h->ir_relres, static_cast<int>( h->ir_iters ), h->ir_tol );
+        return fail( TB_ERR_NOT_CONVERGED, msg );
+    }
     return TB_OK;
 }
 
@@ -1190,6 +1211,13 @@ int tb_chol_refinement_info( tb_chol * h, std::int32_t * iterations, double * re
     TB_TRY( check_handle( h ) );
     if( iterations ) { *iterations = h->ir_iters; }
     if( relres ) { *relres = h->ir_relres; }
+    return TB_OK;
+}
+
+int tb_chol_perturbed_pivots( tb_chol * h, std::int32_t * out )
+{
+    TB_TRY( check_handle( h ) );
+    if( out ) { *out = h->perturbed_pivots; }
     return TB_OK;
 }
 

@@ -219,7 +219,7 @@ constexpr size_t kPotrfSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPa
 
 template<typename T>
 __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict__ arena, int * __restrict__ status,
-                                            double * smem )
+                                            double * smem, const double * __restrict__ pivot_floor )
 {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -258,12 +258,24 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
             for( int r = 0; r < kSub; ++r )
             {
                 double d = __shfl_sync( 0xffffffffu, a[r], r );
+                const bool single = (t.single_rows >> (o + r)) & 1;
+                if( pivot_floor != nullptr && !single && o + r < nb )
+                {
+                    // mixed precision: a pivot lost to FP32 rounding is raised to
+                    // its floor (static pivoting); the FP64 refinement corrects it
+                    const double tau = pivot_floor[t.row0 + t.r0 + o + r];
+                    if( !(d > tau) )
+                    {
+                        if( lane == 0 ) { atomicAdd( status + 2, 1 ); }
+                        d = tau;
+                    }
+                }
                 if( lane == 0 )
                 {
-                    if( (t.single_rows >> (o + r)) & 1 ) { }
+                    if( single ) { }
                     else if( o + r < nb && !(d > 0.0) && fail < 0 ) { fail = o + r; }
                 }
-                if( (t.single_rows >> (o + r)) & 1 ) { d = fabs( d ); }
+                if( single ) { d = fabs( d ); }
                 // reciprocal square root and one product instead of sqrt and a
                 // division: both are long dependent sequences on the FP64 pipe
                 const double inv = rsqrt( d );
@@ -338,10 +350,11 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
 
 template<typename T>
 __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
-                                                               T * __restrict__ arena, int * __restrict__ status )
+                                                               T * __restrict__ arena, int * __restrict__ status,
+                                                               const double * __restrict__ pivot_floor )
 {
     extern __shared__ __align__(16) double psm[];
-    potrf_body( tasks[blockIdx.x], arena, status, psm );
+    potrf_body( tasks[blockIdx.x], arena, status, psm, pivot_floor );
 }
 
 // Solve D^T x = u against the factored diagonal block for the rest columns
@@ -1108,7 +1121,7 @@ __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagAr
         {
             case LaunchKind::Zero:   zero_body( a.zero[t.index], arena ); break;
             case LaunchKind::Extend: extend_body( a.extend[t.index], a.lut, arena ); break;
-            case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], arena, a.status, dsm ); break;
+            case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], arena, a.status, dsm, a.pivot_floor ); break;
             case LaunchKind::Trsm:   trsm_body( a.panel[t.index], arena, dsm ); break;
             case LaunchKind::Gemm:   gemm_body( a.gemm[t.index], arena, dsm ); break;
             case LaunchKind::Invert: invert_body( a.sdiag[t.index], arena, a.tinv + (std::int64_t)t.index * (kPanel * kPanel), dsm ); break;
@@ -1300,6 +1313,7 @@ __global__ void init_status_kernel( int * status )
 {
     status[0] = 0;
     status[1] = INT_MAX;
+    status[2] = 0;
 }
 
 int grid_for( std::int64_t work, int threads )
@@ -1338,9 +1352,24 @@ void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lu
 }
 
 template<typename T>
-void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, cudaStream_t st )
+void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, const double * pivot_floor, cudaStream_t st )
 {
-    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, kPotrfSmemBytes, st>>>( tasks, arena, status ); }
+    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, kPotrfSmemBytes, st>>>( tasks, arena, status, pivot_floor ); }
+}
+
+// floor[i] = rel * |diagonal entry of row i| after assembly (FP32 storage).
+__global__ void pivot_floor_kernel( const std::int64_t * __restrict__ offsets, const float * __restrict__ arena, double rel,
+                                    double * __restrict__ out, int n )
+{
+    for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        out[i] = rel * fabs( static_cast<double>( arena[offsets[i]] ) );
+    }
+}
+
+void launch_pivot_floor( const std::int64_t * offsets, const float * arena, double rel, double * out, int n, cudaStream_t st )
+{
+    pivot_floor_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( offsets, arena, rel, out, n );
 }
 
 template<typename T>
@@ -1413,7 +1442,7 @@ void launch_gather_diag( const std::int64_t * offsets, const T * arena, double *
     template void launch_export<T>( const ExportTask *, int, const std::int32_t *, const T *, double *, double *,    \
                                     cudaStream_t );                                                                \
     template void launch_extend<T>( const ExtendTask *, int, const std::int32_t *, T *, cudaStream_t );             \
-    template void launch_potrf<T>( const PanelTask *, int, T *, int *, cudaStream_t );                               \
+    template void launch_potrf<T>( const PanelTask *, int, T *, int *, const double *, cudaStream_t );               \
     template void launch_trsm<T>( const PanelTask *, int, T *, cudaStream_t );                                       \
     template void launch_gemm<T>( const GemmTask *, int, T *, cudaStream_t );                                        \
     template void launch_factor_dag<T>( const DagArgs &, int, cudaStream_t );                                        \

@@ -12,7 +12,8 @@ namespace tb
 constexpr int kSolveMaxRhs = 64;   // right-hand sides per solve launch
 
 // status[0]: bit 0 set when a pivot was not positive; status[1]: smallest
-// failing (permuted) row index (initialised to INT_MAX).
+// failing (permuted) row index (initialised to INT_MAX); status[2]: pivots
+// raised to their floor (mixed precision).
 // T: factor storage, double (FP64 path) or float (mixed precision: FP32
 // storage, 3xTF32 Schur updates, FP64 panel factorization and solves).
 template<typename T>
@@ -23,7 +24,11 @@ template<typename T>
 void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const T * arena,
                     double * tri, double * rec, cudaStream_t st );
 template<typename T> void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, T * arena, cudaStream_t st );
-template<typename T> void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, cudaStream_t st );
+// pivot_floor (mixed precision only, else null): per permuted row the value a
+// non-positive or lost pivot is raised to instead of failing; status[2] counts them.
+template<typename T> void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status,
+                                        const double * pivot_floor, cudaStream_t st );
+void launch_pivot_floor( const std::int64_t * offsets, const float * arena, double rel, double * out, int n, cudaStream_t st );
 template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, cudaStream_t st );
 template<typename T> void launch_gemm( const GemmTask * tasks, int count, T * arena, cudaStream_t st );
 
@@ -40,6 +45,7 @@ struct DagArgs
     int * error;
     void * arena;                 // factor storage (double or float, the launch's type)
     int * status;
+    const double * pivot_floor;   // see launch_potrf
     const ZeroTask * zero;
     const ExtendTask * extend;
     const std::int32_t * lut;
