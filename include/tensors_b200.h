@@ -267,6 +267,35 @@ int tb_batch_failed_system( tb_batch * b, int32_t * out );
 int tb_batch_solve( tb_batch * b, const double * const * B, double * const * X, int32_t nrhs );
 int tb_batch_solve_device( tb_batch * b, const double * d_B, double * d_X, int32_t nrhs );
 
+/* ------------------------------------------------------------------------
+ * Request serving (no counterpart in the reference).  A server owns `slots`
+ * worker threads on one GPU and a queue of requests over registered
+ * matrices (sparsity pattern + permutation; footprint_bytes = the caller's
+ * estimate of a handle's device memory, replaced by the measured size after
+ * its first factorization).  Continuous batching: a free slot takes the
+ * oldest queued request whose matrix is idle and whose footprint fits under
+ * the HBM cap (idle resident factors are evicted least recently used first),
+ * so requests arriving while others run start as soon as a slot and memory
+ * are free, and requests on different matrices overlap on the device (each
+ * matrix has its own stream).  A request factors (values != NULL, caller
+ * order, copied at submission), solves (B, X host row-major n x nrhs, used
+ * until tb_server_wait returns; refined to tol in the mixed mode), or both;
+ * a solve-only request uses the resident factor, refactoring from the last
+ * values if it was evicted.  precision: TB_PRECISION_MIXED or _FP64. */
+typedef struct tb_server tb_server;
+int tb_server_create( tb_server ** out, int device, int64_t hbm_cap_bytes, int32_t slots, int32_t precision );
+int tb_server_destroy( tb_server * s );
+int tb_server_add_matrix( tb_server * s, int32_t n, const int64_t * outer, const int32_t * inner, const int32_t * perm,
+                          int64_t footprint_bytes, int64_t * matrix_id );
+int tb_server_submit( tb_server * s, int64_t matrix_id, const double * values, double reg, const double * B, double * X,
+                      int32_t nrhs, double tol, int64_t * request_id );
+/* Blocks until the request is done; returns its status.  latency_ms: from
+ * submission to completion; run_ms: on a slot; refinement steps / residual. */
+int tb_server_wait( tb_server * s, int64_t request_id, int32_t * status, double * latency_ms, double * run_ms,
+                    int32_t * iterations, double * relres );
+int tb_server_stats( tb_server * s, int64_t * resident_bytes, int64_t * peak_resident_bytes, int64_t * evictions,
+                     int64_t * refactors );
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,12 @@ SIGNATURES = {
     "tb_batch_failed_system": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
     "tb_batch_solve": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
     "tb_batch_solve_device": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
+    "tb_server_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _i64, _i32, _i32]),
+    "tb_server_destroy": (ctypes.c_int, [_vp]),
+    "tb_server_add_matrix": (ctypes.c_int, [_vp, _i32, _vp, _vp, _vp, _i64, _pi64]),
+    "tb_server_submit": (ctypes.c_int, [_vp, _i64, _vp, _d, _vp, _vp, _i32, _d, _pi64]),
+    "tb_server_wait": (ctypes.c_int, [_vp, _i64, _pi32, _pd, _pd, _pi32, _pd]),
+    "tb_server_stats": (ctypes.c_int, [_vp, _pi64, _pi64, _pi64, _pi64]),
 }
 
 _LIB = None

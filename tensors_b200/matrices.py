@@ -21,6 +21,7 @@ fixes every value on every host.  The workloads:
 * :func:`delaunay_laplacian` -- cotangent Laplacian of the Delaunay
   triangulation of ``m`` uniform points in the unit square plus ``shift``
   times the lumped (one third of incident triangle areas) mass matrix.
+* :func:`mesh_laplacian` -- the same operator on a jittered-grid point set.
 """
 from __future__ import annotations
 
@@ -35,6 +36,7 @@ __all__ = [
     "grid_laplacian_3d",
     "vector_laplacian_3d",
     "delaunay_laplacian",
+    "mesh_laplacian",
     "csr_matvec",
 ]
 
@@ -174,6 +176,11 @@ def delaunay_laplacian(m: int, seed: int, shift: float = 1e-3) -> CSRMatrix:
     rng = np.random.Generator(np.random.PCG64(seed))
     pts = rng.random((m, 2))
     tri = Delaunay(pts).simplices.astype(np.int64)
+    return _cotangent_laplacian(pts, tri, shift, {"kind": "delaunay", "m": m, "seed": seed, "shift": shift})
+
+
+def _cotangent_laplacian(pts, tri, shift, meta) -> CSRMatrix:
+    m = len(pts)
     P = pts[tri]                                  # (t, 3, 2)
     rows, cols, vals = [], [], []
     for k in range(3):
@@ -196,8 +203,23 @@ def delaunay_laplacian(m: int, seed: int, shift: float = 1e-3) -> CSRMatrix:
     rows.append(np.arange(m))
     cols.append(np.arange(m))
     vals.append(shift * mass)
-    return from_coo(m, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals),
-                    coords=pts, meta={"kind": "delaunay", "m": m, "seed": seed, "shift": shift})
+    return from_coo(m, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals), coords=pts, meta=meta)
+
+
+def mesh_laplacian(m: int, seed: int, shift: float = 1e-3) -> CSRMatrix:
+    """Cotangent Laplacian + shift * lumped mass of a quality 2D mesh: the Delaunay
+    triangulation of about m points on a jittered grid (every point moved by up to
+    a quarter cell), which keeps the angles bounded away from 0 and pi -- unlike
+    uniform random points, whose hull slivers give cotangent weights of ~1e6."""
+    from scipy.spatial import Delaunay
+
+    rng = np.random.Generator(np.random.PCG64(seed))
+    g = max(2, int(round(np.sqrt(m))))
+    h = 1.0 / (g - 1)
+    yy, xx = np.meshgrid(np.arange(g) * h, np.arange(g) * h, indexing="ij")
+    pts = np.stack([xx.ravel(), yy.ravel()], 1) + rng.uniform(-0.25 * h, 0.25 * h, size=(g * g, 2))
+    tri = Delaunay(pts).simplices.astype(np.int64)
+    return _cotangent_laplacian(pts, tri, shift, {"kind": "mesh", "m": g * g, "seed": seed, "shift": shift})
 
 
 def csr_matvec(A: CSRMatrix, X: np.ndarray) -> np.ndarray:
