@@ -216,6 +216,7 @@ def run_for_profiler(args):
     tb_build.build()
     A, perm, B_host = build_problem(args.grid)
     chol = CholeskyDecomposition(A.outer, A.inner, perm)
+    chol.SetPrecision(args.precision)
     chol.SymbolicFactorization()
     chol.SetUseGraph(False)
     vals = torch.tensor(A.values, device="cuda")
@@ -227,7 +228,8 @@ def run_for_profiler(args):
     torch.cuda.synchronize()
     R = chol.Residual(B, X)
     torch.cuda.synchronize()
-    print(json.dumps({"grid": args.grid, "relres": float(torch.linalg.norm(R) / torch.linalg.norm(B)),
+    print(json.dumps({"grid": args.grid, "precision": args.precision,
+                      "relres": float(torch.linalg.norm(R) / torch.linalg.norm(B)),
                       "launches": chol.LaunchCounts(), "plan": chol.PlanStats()}))
     return 0
 
@@ -497,6 +499,21 @@ def run_c5(args):
     return 0
 
 
+def max_over_ranks(dist, value, device):
+    """The largest of the ranks' values, on every rank (one all-reduce)."""
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(flops_per_replica, t_ms, world):
+    """Whole-job GFLOP/s of `world` independent replicas, each doing
+    flops_per_replica per step, timed by the slowest rank's t_ms."""
+    return flops_per_replica / (t_ms * 1e-3) / 1e9 * world
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -511,6 +528,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="c4: number of systems (default 2000)")
     ap.add_argument("--requests", type=int, default=0, help="c5: number of requests (default 2000 of the 10000)")
     ap.add_argument("--schedule", default=None, help="c4: factorization schedule of the batch")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="--ncu runs: factor precision (mixed: FP32 factor with tensor-core GEMM tiles)")
     ap.add_argument("--ncu", action="store_true",
                     help="profiling run for ncu: warmup + steps factor+solve as direct launches, no timing, "
                          "no baselines")
@@ -593,9 +612,7 @@ def main():
             dist.barrier()
     t_ms = statistics.mean(times)
     if world > 1:
-        tt = torch.tensor([t_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_ms = float(tt.item())
+        t_ms = max_over_ranks(dist, t_ms, dev)
 
     # correctness of the timed result
     R = chol.Residual(B, X)
@@ -653,7 +670,7 @@ def main():
                              f"grid (OpenBLAS 1 thread per tree task, {threads} tree threads)",
                    "seconds": r["seconds"][0], "relres": r["relres"]}
 
-    value = flops / (t_ms * 1e-3) / 1e9 * world
+    value = replica_throughput(flops, t_ms, world)
     line = {
         "metric": "factor+solve GFLOP/s (FP64, 64^3 7-pt Laplacian, 16 RHS)",
         "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

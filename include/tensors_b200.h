@@ -156,8 +156,9 @@ int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
  * (runs of supernodes merged for computation), out[11] flops of the front
  * factorization (explicit zeros of merged fronts included), out[12] simulated
  * microseconds of the scheduled task graph (0 before the first numeric
- * factorization on a device), out[13] tasks of the graph.  Returns the
- * number of entries written (at most cap). */
+ * factorization on a device), out[13] tasks of the graph, out[14] tasks of
+ * the solve's task graph, out[15] its first level.  Returns the number of
+ * entries written (at most cap). */
 int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
 /* Host-side bounds check of every device task of the plan (also run before
  * the plan is first uploaded).  TB_OK or TB_ERR_INVALID_ARGUMENT with the
@@ -207,6 +208,17 @@ int tb_chol_perturbed_pivots( tb_chol * h, int32_t * out );
  * bit for bit. */
 enum tb_schedule { TB_SCHEDULE_LEVELS = 0, TB_SCHEDULE_TASK_GRAPH = 1, TB_SCHEDULE_TASK_GRAPH_ALL = 2 };
 int tb_chol_set_schedule( tb_chol * h, int32_t schedule );
+/* Schedule of the solve sweeps.  TB_SCHEDULE_LEVELS (default): one launch per
+ * level and panel step in each sweep.  TB_SCHEDULE_TASK_GRAPH: the levels
+ * below the first level with 4 or more panel steps as level launches, the
+ * levels from there up as one persistent launch per sweep whose CTAs take the
+ * solve tasks in dependency order (a panel's tasks start once every update of
+ * its rows is in).  TB_SCHEDULE_TASK_GRAPH_ALL: every level in the persistent
+ * launch.  The schedules agree to rounding (updates of shared rows are
+ * atomic additions in any order).  A wait of the persistent launch that runs
+ * out of time is reported (TB_ERR_TIMEOUT) by the next call that
+ * synchronizes with the solve. */
+int tb_chol_set_solve_schedule( tb_chol * h, int32_t schedule );
 /* Execution trace of the persistent factorization launch: when enabled,
  * each task records when it was taken, when its inputs were ready, when it
  * was done (%globaltimer ns) and which CTA ran it.  tb_chol_trace writes 6
@@ -214,6 +226,12 @@ int tb_chol_set_schedule( tb_chol * h, int32_t schedule );
  * cap >= 6 x tasks) for the last factorization and returns the task count. */
 int tb_chol_set_trace( tb_chol * h, int32_t enabled );
 int tb_chol_trace( tb_chol * h, int64_t * out, int64_t cap );
+/* Execution trace of the persistent solve launches of the last solve with
+ * the trace enabled (tb_chol_set_trace), first 64 right-hand sides: per task
+ * of the forward then the back sweep, 6 int64 (sweep 0/1, solve task index,
+ * taken_ns, ready_ns, done_ns, cta), in list order.  Returns the number of
+ * rows; cap must hold 12 x the graph's task count. */
+int tb_chol_solve_trace( tb_chol * h, int64_t * out, int64_t cap );
 /* Per-kernel timing: when enabled, factorizations run as direct launches
  * bracketed by CUDA events and tb_chol_kernel_profile reports, per launch
  * kind (0 zero, 1 extend-add, 2 panel trsm, 3 GEMM tiles, 4 inversion of

@@ -58,8 +58,10 @@ SIGNATURES = {
     "tb_chol_solve_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
     "tb_chol_launch_counts": (ctypes.c_int, [_vp, _pi64, _pi64]),
     "tb_chol_set_schedule": (ctypes.c_int, [_vp, _i32]),
+    "tb_chol_set_solve_schedule": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_set_trace": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64]),
+    "tb_chol_solve_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64]),
     "tb_chol_set_precision": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_set_refinement": (ctypes.c_int, [_vp, _d, _i32]),
     "tb_chol_refinement_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]),

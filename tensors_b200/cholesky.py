@@ -160,6 +160,20 @@ class CholeskyDecomposition:
         code = {"levels": 0, "task_graph": 1, "task_graph_all": 2}[schedule] if isinstance(schedule, str) else int(schedule)
         _check(lib().tb_chol_set_schedule(self._h, code))
 
+    def SetSolveSchedule(self, schedule) -> None:
+        """Solve sweeps: 'levels' (default: one launch per level and step), 'task_graph' (level launches, then
+        one persistent launch per sweep for the levels with 4 or more panel steps) or 'task_graph_all'."""
+        code = {"levels": 0, "task_graph": 1, "task_graph_all": 2}[schedule] if isinstance(schedule, str) else int(schedule)
+        _check(lib().tb_chol_set_solve_schedule(self._h, code))
+
+    def SolveTrace(self) -> np.ndarray:
+        """Trace of the persistent solve launches of the last solve: rows (sweep, task, taken_ns, ready_ns,
+        done_ns, cta), forward sweep then back sweep."""
+        cap = 12 * max(1, self.PlanStats().get("solve_graph_tasks", 0))
+        out = np.zeros(cap, dtype=np.int64)
+        m = _check(lib().tb_chol_solve_trace(self._h, out.ctypes.data, cap))
+        return out[: 6 * m].reshape(m, 6)
+
     def SetTrace(self, enabled: bool) -> None:
         _check(lib().tb_chol_set_trace(self._h, 1 if enabled else 0))
 
@@ -360,7 +374,8 @@ class CholeskyDecomposition:
         out = np.zeros(16, dtype=np.int64)
         m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 16))
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
-                "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks"]
+                "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks",
+                "solve_graph_tasks", "solve_split_level"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

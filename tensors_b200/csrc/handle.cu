@@ -145,6 +145,15 @@ struct tb_chol
     DeviceArray<double>             tinv;        // inverse diagonal block of every panel (64 x 64 each)
     DeviceArray<tb::DagTask>        dag;         // the factorization as one dependency-ordered task list
     DeviceArray<int>                dag_state;   // task-graph counters, then the ticket and the error word
+    // the solve's task graph (Plan::solve_*): orders, targets, expected counts,
+    // and per-panel counters followed by the ticket and the error word
+    DeviceArray<std::int32_t>       solve_fwd_order, solve_bwd_order, solve_targets, solve_fwd_expected, solve_panel_tasks;
+    DeviceArray<std::int64_t>       solve_target_ptr;
+    DeviceArray<int>                solve_state;
+    PinnedBuffer                    pin_solve_err;   // error word of the last sweeps (list position + 1)
+    std::map<int, int>              solve_grid;      // CTAs of the persistent solve launch per right-hand-side count
+    DeviceArray<unsigned long long> solve_trace_buf; // with `trace`: forward then back sweep of the first RHS chunk
+    int solve_schedule = TB_SCHEDULE_LEVELS;
     int dag_grid = 0;                            // CTAs of the persistent factorization launch
     bool use_dag = false;                        // persistent task-graph launch (else one launch per step)
     int schedule = TB_SCHEDULE_LEVELS;
@@ -244,6 +253,8 @@ int ensure_symbolic( tb_chol * h )
     }
     h->plan.dag_min_steps = h->schedule == TB_SCHEDULE_TASK_GRAPH_ALL ? 0 : tb::kDagMinSteps;
     h->plan.build( h->sym );
+    if( h->solve_schedule == TB_SCHEDULE_LEVELS ) { h->plan.build_solve_graph( h->sym, h->plan.levels ); }
+    else if( h->solve_schedule == TB_SCHEDULE_TASK_GRAPH_ALL ) { h->plan.build_solve_graph( h->sym, 0 ); }
     h->symbolic_done = true;
     h->device_ready = false;
     h->factorized = false;
@@ -314,6 +325,16 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->tinv.reserve( static_cast<std::int64_t>( pl.sdiag.size() ) * tb::kPanel * tb::kPanel ) );
     TB_TRY( h->dag.upload( pl.dag, st_ ) );
     TB_TRY( h->dag_state.reserve( static_cast<std::int64_t>( pl.dag_counters ) + 2 ) );
+    TB_TRY( h->solve_fwd_order.upload( pl.solve_fwd_order, st_ ) );
+    TB_TRY( h->solve_bwd_order.upload( pl.solve_bwd_order, st_ ) );
+    TB_TRY( h->solve_targets.upload( pl.solve_targets, st_ ) );
+    TB_TRY( h->solve_fwd_expected.upload( pl.solve_fwd_expected, st_ ) );
+    TB_TRY( h->solve_panel_tasks.upload( pl.solve_panel_tasks, st_ ) );
+    TB_TRY( h->solve_target_ptr.upload( pl.solve_target_ptr, st_ ) );
+    TB_TRY( h->solve_state.reserve( static_cast<std::int64_t>( pl.solve_panel_tasks.size() ) + 2 ) );
+    TB_TRY( h->pin_solve_err.reserve( 64 ) );
+    *h->pin_solve_err.as<int>() = 0;
+    h->solve_grid.clear();
     TB_CUDA( cudaStreamSynchronize( st_ ) );
     if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
     h->drop_solve_graphs();
@@ -364,7 +385,7 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
                 case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
                 case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, st ); break;
                 case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
-                case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
+                case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, st ); break;
                 case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
                 default: break;
             }
@@ -392,7 +413,7 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
             case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
             case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, st ); break;
             case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
-            case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, st ); break;
+            case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, st ); break;
             case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
             default: break;
         }
@@ -469,6 +490,12 @@ int run_factor( tb_chol * h, double reg )
     }
     TB_CUDA( cudaStreamSynchronize( st ) );
     h->perturbed_pivots = ps[2];
+    if( ps[0] & 2 )
+    {
+        h->factorized = false;
+        h->good = false;
+        return fail( TB_ERR_TIMEOUT, "NumericFactorization: a tensor-core completion wait ran out of time" );
+    }
     if( ps[3] != 0 )
     {
         h->factorized = false;
@@ -477,7 +504,7 @@ int run_factor( tb_chol * h, double reg )
                      + std::to_string( ps[3] - 1 ) + " ran out of time" );
     }
     h->factorized = true;                       // marked in any case, Numeric.hpp:94-95
-    h->good = (ps[0] == 0);
+    h->good = (ps[0] & 1) == 0;
     h->failed_sn = h->good ? -1 : h->sym.row_to_sn[std::min( std::max( ps[1], 0 ), h->n - 1 )];
     if( !h->good )
     {
@@ -510,34 +537,77 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
     std::int64_t launches = 0;
     std::size_t ev = 0;
     auto begin = [&]() { if( timed ) { cudaEventRecord( h->solve_events[ev++], st ); } };
-    auto end = [&]( const tb::Launch & L, int upper )
+    auto end = [&]( std::int32_t level, std::int32_t step, std::int32_t count, int upper )
     {
         if( !timed ) { return; }
         cudaEventRecord( h->solve_events[ev++], st );
-        h->solve_info.insert( h->solve_info.end(), { upper, L.level, L.step, L.count } );
+        h->solve_info.insert( h->solve_info.end(), { upper, level, step, count } );
     };
     if( timed ) { h->solve_info.clear(); }
+    const bool mixed = h->precision == TB_PRECISION_MIXED;
+    // the levels from solve_split_level up: one persistent launch per sweep
+    bool graph = !pl.solve_fwd_order.empty();
+    for( std::int32_t c0 = 0; c0 < k && graph; c0 += tb::kSolveMaxRhs )
+    {
+        const auto it = h->solve_grid.find( std::min( tb::kSolveMaxRhs, k - c0 ) );
+        graph = it != h->solve_grid.end() && it->second > 0;
+    }
+    const std::int32_t split = graph ? pl.solve_split_level : pl.levels;
+    const std::int32_t np = static_cast<std::int32_t>( pl.solve_panel_tasks.size() );
+    int * err = h->solve_state.ptr + np + 1;
+    if( graph ) { cudaMemsetAsync( err, 0, sizeof(int), st ); }
+    auto step = [&]( const tb::Launch & L, bool upper, double * in, double * out, std::int32_t kc )
+    {
+        begin();
+        if( mixed )
+        {
+            tb::launch_solve_step( h->srest.ptr + L.first, L.count, upper, arena_as<float>( h ), h->tinv.ptr,
+                                   h->sn_inner.ptr, in, out, k, kc, st );
+        }
+        else
+        {
+            tb::launch_solve_step( h->srest.ptr + L.first, L.count, upper, arena_as<double>( h ), h->tinv.ptr,
+                                   h->sn_inner.ptr, in, out, k, kc, st );
+        }
+        end( L.level, L.step, L.count, upper ? 1 : 0 );
+        ++launches;
+    };
+    auto persistent = [&]( bool upper, double * in, double * out, std::int32_t kc, std::int32_t c0 )
+    {
+        cudaMemsetAsync( h->solve_state.ptr, 0, sizeof(int) * (static_cast<size_t>( np ) + 1), st );
+        tb::SolveDagArgs a{};
+        a.tasks = h->srest.ptr;
+        a.order = upper ? h->solve_bwd_order.ptr : h->solve_fwd_order.ptr;
+        a.ntasks = static_cast<int>( pl.solve_fwd_order.size() );
+        a.upper = upper ? 1 : 0;
+        a.first_task = pl.solve_first_task;
+        a.first_panel = pl.solve_first_panel;
+        a.target_ptr = h->solve_target_ptr.ptr;
+        a.targets = h->solve_targets.ptr;
+        a.fwd_expected = h->solve_fwd_expected.ptr;
+        a.panel_tasks = h->solve_panel_tasks.ptr;
+        a.counters = h->solve_state.ptr;
+        a.next = h->solve_state.ptr + np;
+        a.error = err;
+        a.tinv = h->tinv.ptr;
+        a.sn_inner = h->sn_inner.ptr;
+        a.timeout_ns = kDagTimeoutNs;
+        a.trace = (h->trace && h->solve_trace_buf.ptr && c0 == 0)
+                ? h->solve_trace_buf.ptr + (upper ? 4 * static_cast<std::int64_t>( a.ntasks ) : 0) : nullptr;
+        const int grid = h->solve_grid.at( kc );
+        begin();
+        if( mixed ) { tb::launch_solve_dag( a, grid, arena_as<float>( h ), in, out, k, kc, st ); }
+        else        { tb::launch_solve_dag( a, grid, arena_as<double>( h ), in, out, k, kc, st ); }
+        end( split, -1, a.ntasks, upper ? 1 : 0 );
+        ++launches;
+    };
     if( which != 1 )
     {
         for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
             const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
-            for( const tb::Launch & L : pl.lower_launches )
-            {
-                begin();
-                if( h->precision == TB_PRECISION_MIXED )
-                {
-                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, false, arena_as<float>( h ), h->tinv.ptr,
-                                           h->sn_inner.ptr, W + c0, Y + c0, k, kc, st );
-                }
-                else
-                {
-                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, false, arena_as<double>( h ), h->tinv.ptr,
-                                           h->sn_inner.ptr, W + c0, Y + c0, k, kc, st );
-                }
-                end( L, 0 );
-                ++launches;
-            }
+            for( const tb::Launch & L : pl.lower_launches ) { if( L.level < split ) { step( L, false, W + c0, Y + c0, kc ); } }
+            if( graph ) { persistent( false, W + c0, Y + c0, kc, c0 ); }
         }
     }
     if( which != 0 )
@@ -546,25 +616,44 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
         for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
             const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
-            for( const tb::Launch & L : pl.upper_launches )
-            {
-                begin();
-                if( h->precision == TB_PRECISION_MIXED )
-                {
-                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, true, arena_as<float>( h ), h->tinv.ptr,
-                                           h->sn_inner.ptr, Y + c0, W + c0, k, kc, st );
-                }
-                else
-                {
-                    tb::launch_solve_step( h->srest.ptr + L.first, L.count, true, arena_as<double>( h ), h->tinv.ptr,
-                                           h->sn_inner.ptr, Y + c0, W + c0, k, kc, st );
-                }
-                end( L, 1 );
-                ++launches;
-            }
+            if( graph ) { persistent( true, Y + c0, W + c0, kc, c0 ); }
+            for( const tb::Launch & L : pl.upper_launches ) { if( L.level < split ) { step( L, true, Y + c0, W + c0, kc ); } }
         }
     }
+    if( graph ) { cudaMemcpyAsync( h->pin_solve_err.ptr, err, sizeof(int), cudaMemcpyDeviceToHost, st ); }
     return launches;
+}
+
+// CTAs of the persistent solve launch for every right-hand-side chunk width
+// of k (before the sweeps are issued or captured).
+int prepare_solve_grid( tb_chol * h, std::int32_t k )
+{
+    if( h->plan.solve_fwd_order.empty() ) { return TB_OK; }
+    int sms = 0;
+    TB_CUDA( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, h->device ) );
+    for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
+    {
+        const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
+        if( h->solve_grid.count( kc ) ) { continue; }
+        const int per_sm = tb::solve_dag_blocks_per_sm( kc );
+        if( per_sm <= 0 ) { return fail( TB_ERR_CUDA, "persistent solve kernel cannot be resident" ); }
+        h->solve_grid[kc] = static_cast<int>( std::min<std::int64_t>( static_cast<std::int64_t>( per_sm ) * sms,
+                                                                       static_cast<std::int64_t>( h->plan.solve_fwd_order.size() ) ) );
+    }
+    return TB_OK;
+}
+
+// After a synchronization: a wait of the persistent solve launch that ran out
+// of time (the result is then wrong).
+int check_solve_error( tb_chol * h )
+{
+    if( h->pin_solve_err.ptr == nullptr ) { return TB_OK; }
+    int & e = *h->pin_solve_err.as<int>();
+    if( e == 0 ) { return TB_OK; }
+    const int pos = e - 1;
+    e = 0;
+    return fail( TB_ERR_TIMEOUT, "Solve: persistent solve launch stopped, the wait of list position " + std::to_string( pos )
+                 + " ran out of time" );
 }
 
 double * sweep_input( int which, double * W, double * Y ) { return which == 1 ? Y : W; }
@@ -591,6 +680,7 @@ int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, st
         h->solve_graph_work = W;
         h->solve_graph_work2 = Y;
     }
+    TB_TRY( prepare_solve_grid( h, k ) );
     std::int64_t launches = 0;
     tb::launch_gather_rows( d_B, ldB, h->p.ptr, sweep_input( which, W, Y ), k, n, k, st );   // ReadRightHandSide
     ++launches;
@@ -702,6 +792,7 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
         TB_TRY( dots( R, k, R, k, rr ) );
         TB_CUDA( cudaMemcpyAsync( hn, rr, sizeof(double) * 2 * static_cast<size_t>( k ), cudaMemcpyDeviceToHost, st ) );
         TB_CUDA( cudaStreamSynchronize( st ) );
+        TB_TRY( check_solve_error( h ) );
         double rel = 0.0;
         for( std::int32_t c = 0; c < k; ++c )
         {
@@ -789,6 +880,7 @@ int run_solve_host( tb_chol * h, int which, double alpha, const double * B, std:
     TB_TRY( run_solve_device( h, which, alpha, h->in.ptr, k, beta, h->out.ptr, k, k ) );
     TB_CUDA( cudaMemcpyAsync( po, h->out.ptr, bytes, cudaMemcpyDeviceToHost, st ) );
     TB_CUDA( cudaStreamSynchronize( st ) );
+    TB_TRY( check_solve_error( h ) );
     if( ldX == k ) { std::memcpy( X, po, bytes ); }
     else { for( std::int64_t i = 0; i < n; ++i ) { std::memcpy( X + i * ldX, po + i * k, sizeof(double) * k ); } }
     return TB_OK;
@@ -1108,7 +1200,8 @@ int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
         static_cast<std::int64_t>( pl.extend.size() ), static_cast<std::int64_t>( pl.lower_launches.size() ),
         static_cast<std::int64_t>( pl.upper_launches.size() ), h->sym.sn_count, pl.front_count,
         static_cast<std::int64_t>( pl.front_flops ), static_cast<std::int64_t>( pl.dag_makespan_us ),
-        static_cast<std::int64_t>( pl.dag.size() ) };
+        static_cast<std::int64_t>( pl.dag.size() ), static_cast<std::int64_t>( pl.solve_fwd_order.size() ),
+        pl.solve_split_level };
     const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
     for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
     return m;
@@ -1183,6 +1276,40 @@ int tb_chol_set_schedule( tb_chol * h, std::int32_t schedule )
     return TB_OK;
 }
 
+int tb_chol_set_solve_schedule( tb_chol * h, std::int32_t schedule )
+{
+    TB_TRY( check_handle( h ) );
+    if( schedule != TB_SCHEDULE_LEVELS && schedule != TB_SCHEDULE_TASK_GRAPH && schedule != TB_SCHEDULE_TASK_GRAPH_ALL )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "unknown schedule" );
+    }
+    if( schedule == h->solve_schedule ) { return TB_OK; }
+    h->solve_schedule = schedule;
+    if( h->symbolic_done )
+    {
+        if( h->stream ) { TB_CUDA( cudaStreamSynchronize( h->stream ) ); }
+        tb::Plan & pl = h->plan;
+        if( schedule == TB_SCHEDULE_LEVELS ) { pl.build_solve_graph( h->sym, pl.levels ); }
+        else if( schedule == TB_SCHEDULE_TASK_GRAPH_ALL ) { pl.build_solve_graph( h->sym, 0 ); }
+        else { pl.build_solve_graph( h->sym, pl.solve_default_split ); }
+        if( h->device_ready )
+        {
+            cudaStream_t st_ = h->stream;
+            TB_TRY( h->solve_fwd_order.upload( pl.solve_fwd_order, st_ ) );
+            TB_TRY( h->solve_bwd_order.upload( pl.solve_bwd_order, st_ ) );
+            TB_TRY( h->solve_targets.upload( pl.solve_targets, st_ ) );
+            TB_TRY( h->solve_fwd_expected.upload( pl.solve_fwd_expected, st_ ) );
+            TB_TRY( h->solve_panel_tasks.upload( pl.solve_panel_tasks, st_ ) );
+            TB_TRY( h->solve_target_ptr.upload( pl.solve_target_ptr, st_ ) );
+            TB_TRY( h->solve_state.reserve( static_cast<std::int64_t>( pl.solve_panel_tasks.size() ) + 2 ) );
+            TB_CUDA( cudaStreamSynchronize( st_ ) );
+            h->solve_grid.clear();
+        }
+    }
+    h->drop_solve_graphs();
+    return TB_OK;
+}
+
 int tb_chol_set_precision( tb_chol * h, std::int32_t precision )
 {
     TB_TRY( check_handle( h ) );
@@ -1225,11 +1352,16 @@ int tb_chol_set_trace( tb_chol * h, std::int32_t enabled )
 {
     TB_TRY( check_handle( h ) );
     TB_TRY( ensure_device( h ) );
-    if( enabled ) { TB_TRY( h->trace_buf.reserve( 4 * static_cast<std::int64_t>( h->plan.dag.size() ) ) ); }
+    if( enabled )
+    {
+        TB_TRY( h->trace_buf.reserve( 4 * static_cast<std::int64_t>( h->plan.dag.size() ) ) );
+        TB_TRY( h->solve_trace_buf.reserve( 8 * static_cast<std::int64_t>( h->plan.srest.size() ) ) );
+    }
     if( (enabled != 0) != h->trace )
     {
         h->trace = enabled != 0;
         if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+        h->drop_solve_graphs();
     }
     return TB_OK;
 }
@@ -1251,6 +1383,30 @@ int tb_chol_trace( tb_chol * h, std::int64_t * out, std::int64_t cap )
         for( int j = 0; j < 4; ++j ) { out[6 * k + 2 + j] = static_cast<std::int64_t>( raw[static_cast<size_t>( 4 * k + j )] ); }
     }
     return static_cast<int>( std::min<std::int64_t>( n, INT_MAX ) );
+}
+
+int tb_chol_solve_trace( tb_chol * h, std::int64_t * out, std::int64_t cap )
+{
+    TB_TRY( check_handle( h ) );
+    if( !h->trace || h->solve_trace_buf.ptr == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "trace not enabled" ); }
+    const std::int64_t n = static_cast<std::int64_t>( h->plan.solve_fwd_order.size() );
+    if( out == nullptr || cap < 12 * n ) { return fail( TB_ERR_INVALID_ARGUMENT, "trace buffer too small" ); }
+    std::vector<unsigned long long> raw( static_cast<size_t>( 8 * n ) );
+    if( n > 0 )
+    {
+        TB_CUDA( cudaMemcpyAsync( raw.data(), h->solve_trace_buf.ptr, sizeof(unsigned long long) * raw.size(),
+                                  cudaMemcpyDeviceToHost, h->stream ) );
+        TB_CUDA( cudaStreamSynchronize( h->stream ) );
+    }
+    for( std::int64_t k = 0; k < 2 * n; ++k )
+    {
+        const int upper = k >= n ? 1 : 0;
+        const std::int64_t pos = k - upper * n;
+        out[6 * k + 0] = upper;
+        out[6 * k + 1] = upper ? h->plan.solve_bwd_order[static_cast<size_t>( pos )] : h->plan.solve_fwd_order[static_cast<size_t>( pos )];
+        for( int j = 0; j < 4; ++j ) { out[6 * k + 2 + j] = static_cast<std::int64_t>( raw[static_cast<size_t>( 4 * k + j )] ); }
+    }
+    return static_cast<int>( std::min<std::int64_t>( 2 * n, INT_MAX ) );
 }
 
 int tb_chol_set_profiling( tb_chol * h, std::int32_t enabled )
@@ -1390,6 +1546,7 @@ int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B,
     }
     double * W = nullptr;
     TB_TRY( noalloc_scratch( h->device, &W ) );
+    TB_TRY( prepare_solve_grid( h, k ) );
     double * Y = W + kNoAllocScratchEntries;
     cudaStream_t st = h->stream;
     std::int64_t launches = 2;

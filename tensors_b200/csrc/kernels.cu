@@ -47,14 +47,56 @@ __device__ __forceinline__ void cp_async_8( double * smem_dst, const double * gm
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile( "cp.async.wait_all;\n" ::: "memory" ); }
 
-// One element of a factor block into a double shared-memory cell: an
-// asynchronous copy for FP64 storage, a converting load for FP32 storage
-// (`base` is any mapped address of the block, used when !valid).
-template<typename T>
-__device__ __forceinline__ void stage_element( double * smem_dst, const T * base, const T * src, bool valid )
+__device__ __forceinline__ void cp_async_4( void * smem_dst, const void * gmem_src, bool valid )
 {
-    if constexpr ( sizeof(T) == 8 ) { cp_async_8( smem_dst, valid ? src : base, valid ); }
-    else { *smem_dst = valid ? static_cast<double>( *src ) : 0.0; }
+    const unsigned saddr = static_cast<unsigned>( __cvta_generic_to_shared( smem_dst ) );
+    asm volatile( "cp.async.ca.shared.global [%0], [%1], 4, %2;\n" :: "r"(saddr), "l"(gmem_src), "r"(valid ? 4 : 0) );
+}
+
+// Stages kIters elements per thread (element idx = threadIdx.x + u * kThreads)
+// of a factor block into double shared-memory cells with asynchronous copies,
+// so that all of a thread's copies are in flight together.  src( idx, fill )
+// returns the element's address, or nullptr with `fill` set to the value of a
+// cell outside the block; dst( idx ) is the cell.  FP32 storage: the float is
+// copied into the cell's first 4 bytes and widened in place by stage_finish,
+// which every thread calls for its own cells after cp_async_wait_all and
+// before the block is shared (__syncthreads).
+template<typename T, int kIters, int kThreads, typename Src, typename Dst>
+__device__ __forceinline__ void stage_block( const T * base, Src src, Dst dst )
+{
+#pragma unroll 4
+    for( int u = 0; u < kIters; ++u )
+    {
+        const int idx = threadIdx.x + u * kThreads;
+        double fill = 0.0;
+        const T * s = src( idx, fill );
+        if( s != nullptr || fill == 0.0 )
+        {
+            if constexpr ( sizeof(T) == 8 ) { cp_async_8( dst( idx ), s ? s : base, s != nullptr ); }
+            else { cp_async_4( dst( idx ), s ? s : base, s != nullptr ); }
+        }
+        else { *dst( idx ) = fill; }
+    }
+}
+
+template<typename T, int kIters, int kThreads, typename Src, typename Dst>
+__device__ __forceinline__ void stage_finish( Src src, Dst dst )
+{
+    if constexpr ( sizeof(T) == 4 )
+    {
+#pragma unroll 4
+        for( int u = 0; u < kIters; ++u )
+        {
+            const int idx = threadIdx.x + u * kThreads;
+            double fill = 0.0;
+            const T * s = src( idx, fill );
+            if( s != nullptr || fill == 0.0 )
+            {
+                double * d = dst( idx );
+                *d = static_cast<double>( *reinterpret_cast<const float *>( d ) );
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------- assembly
@@ -215,7 +257,7 @@ __device__ __forceinline__ void dmma_8x8x8( double (&acc)[2], FA a, FB b )
     }
 }
 
-constexpr size_t kPotrfSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel + 1);
+constexpr size_t kPotrfSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + 2 * kPanel + 1);
 
 template<typename T>
 __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict__ arena, int * __restrict__ status,
@@ -226,22 +268,22 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     const int nb = min( kPanel, t.n0 - t.r0 );
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem );
     double * inv_d = smem + kPanel * (kPanel + 1);
-    int & fail = *reinterpret_cast<int *>( inv_d + kPanel );
+    double * floor_s = inv_d + kPanel;                  // the panel's pivot floors (mixed precision)
+    int & fail = *reinterpret_cast<int *>( floor_s + kPanel );
 
     T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-#pragma unroll 4
-    for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
+    if( pivot_floor != nullptr && tid < nb ) { floor_s[tid] = pivot_floor[t.row0 + t.r0 + tid]; }
+    auto stage_src = [&]( int idx, double & fill ) -> const T *
     {
         const int r = idx / kPanel, c = idx % kPanel;
-        if( r >= nb && r == c ) { D[r][c] = 1.0; }      // identity padding beyond nb
-        else
-        {
-            const bool valid = r < nb && c < nb && r <= c;
-            stage_element( &D[r][c], U0, U0 + (std::int64_t)r * t.ld0 + c, valid );
-        }
-    }
+        fill = (r >= nb && r == c) ? 1.0 : 0.0;      // identity padding beyond nb
+        return (r < nb && c < nb && r <= c) ? U0 + (std::int64_t)r * t.ld0 + c : nullptr;
+    };
+    auto stage_dst = [&]( int idx ) { return &D[idx / kPanel][idx % kPanel]; };
+    stage_block<T, kPanel * kPanel / kPotrfThreads, kPotrfThreads>( U0, stage_src, stage_dst );
     if( tid == 0 ) { fail = -1; }
     cp_async_wait_all();
+    stage_finish<T, kPanel * kPanel / kPotrfThreads, kPotrfThreads>( stage_src, stage_dst );
     __syncthreads();
 
     const int nsub = (nb + kSub - 1) / kSub;
@@ -263,7 +305,7 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
                 {
                     // mixed precision: a pivot lost to FP32 rounding is raised to
                     // its floor (static pivoting); the FP64 refinement corrects it
-                    const double tau = pivot_floor[t.row0 + t.r0 + o + r];
+                    const double tau = floor_s[o + r];
                     if( !(d > tau) )
                     {
                         if( lane == 0 ) { atomicAdd( status + 2, 1 ); }
@@ -377,32 +419,30 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__
     const int cw = min( kRestChunk, rest - t.c0 );
     T * U0 = arena + t.u0;
     T * U1 = arena + t.u1;
-#pragma unroll 4
-    for( int idx = tid; idx < kPanel * kPanel; idx += kTrsmThreads )
+    // D (64 x 64) and the rest columns (64 x kRestChunk) as one block of
+    // 2 x 64 rows, so that with FP32 storage all loads are in flight together
+    static_assert( kRestChunk == kPanel, "trsm staging assumes square blocks" );
+    auto stage_src = [&]( int idx, double & fill ) -> const T *
     {
-        const int r = idx / kPanel, c = idx % kPanel;
-        if( r >= nb && r == c ) { D[r][c] = 1.0; }
-        else
+        const int r = (idx / kPanel) & (kPanel - 1), c = idx % kPanel;
+        if( idx < kPanel * kPanel )
         {
-            const bool valid = r < nb && c < nb && r <= c;
-            stage_element( &D[r][c], U0, U0 + (std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c, valid );
+            fill = (r >= nb && r == c) ? 1.0 : 0.0;
+            return (r < nb && c < nb && r <= c) ? U0 + (std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c : nullptr;
         }
-    }
-#pragma unroll 4
-    for( int idx = tid; idx < kPanel * kRestChunk; idx += kTrsmThreads )
+        const int col = t.c0 + c;
+        if( r >= nb || c >= cw ) { return nullptr; }
+        return (col < m) ? U0 + (std::int64_t)(t.r0 + r) * t.ld0 + r1 + col
+                         : U1 + (std::int64_t)(t.r0 + r) * t.ld1 + (col - m);
+    };
+    auto stage_dst = [&]( int idx ) -> double *
     {
-        const int r = idx / kRestChunk, cc = idx % kRestChunk;
-        const int col = t.c0 + cc;
-        const bool valid = r < nb && cc < cw;
-        const T * src = U0;
-        if( valid )
-        {
-            src = (col < m) ? U0 + (std::int64_t)(t.r0 + r) * t.ld0 + r1 + col
-                            : U1 + (std::int64_t)(t.r0 + r) * t.ld1 + (col - m);
-        }
-        stage_element( &X[r][cc], U0, src, valid );
-    }
+        const int r = (idx / kPanel) & (kPanel - 1), c = idx % kPanel;
+        return idx < kPanel * kPanel ? &D[r][c] : &X[r][c];
+    };
+    stage_block<T, 2 * kPanel * kPanel / kTrsmThreads, kTrsmThreads>( U0, stage_src, stage_dst );
     cp_async_wait_all();
+    stage_finish<T, 2 * kPanel * kPanel / kTrsmThreads, kTrsmThreads>( stage_src, stage_dst );
     __syncthreads();
     if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
     __syncthreads();
@@ -574,15 +614,31 @@ __device__ __forceinline__ void gemm_body( const GemmTask & t, double * __restri
     }
 }
 
-// FP32 storage: the same tile with split-precision 3xTF32 tensor-core
-// products (x = hi + lo with hi, lo TF32; a b ~ a_lo b_hi + a_hi b_lo +
-// a_hi b_hi, FP32 accumulation) on mma.sync m16n8k8: 8 warps in a 2 x 4
-// arrangement of 32 x 16 blocks, 32 k rows per stage, rows padded to 72
-// floats so the fragment loads are conflict-free.
-constexpr int kGemmKF = 32;
-constexpr int kGemmLdF = kTile + 8;
-constexpr int kGemmStageFloats = 2 * kGemmKF * kGemmLdF;
-constexpr size_t kGemmSmemBytesF = sizeof(float) * kGemmStages * kGemmStageFloats;
+// FP32 storage: the same tiles as split-precision 3xTF32 products on the
+// 5th-generation tensor cores (x = hi + lo with hi, lo TF32; a b ~ a_lo b_hi +
+// a_hi b_lo + a_hi b_hi, FP32 accumulation in tensor memory).  K is streamed
+// in chunks of 32 rows through two shared-memory stages; every chunk is read
+// from global memory into registers one chunk ahead (a warp reads 4 rows of
+// 8 consecutive floats), split, and stored in the canonical K-major
+// no-swizzle layout of tcgen05 operands: core matrices of 8 (m or n) rows x
+// 4 k (16 B per row, 128 B per core matrix), the 8 row groups 128 B apart
+// (stride byte offset) and the k groups of 4 1024 B apart (leading byte
+// offset).  One thread issues the 12 tcgen05.mma (M = N = 64, K = 8) of a
+// chunk and commits them to the stage's mbarrier; the stage is refilled once
+// that barrier has completed.  The 64 x 64 accumulator is read back with
+// tcgen05.ld, staged in shared memory and subtracted from C with coalesced
+// 16-byte accesses (the plan keeps C offsets and leading dimensions
+// multiples of 4 floats).
+constexpr int kTcK = 32;                               // k rows per chunk
+constexpr int kTcPart = kTcK * kTile * 4;              // one operand part (64 x 32 TF32): 8 KB
+constexpr int kTcStage = 4 * kTcPart;                  // A_hi, A_lo, B_hi, B_lo
+constexpr size_t kGemmSmemBytesF = 2 * kTcStage;       // 64 KB
+constexpr int kTcSld = kTile + 4;                      // staged result row (floats)
+constexpr int kTcCols = 64;                            // tensor-memory columns per CTA (FP32 accumulator 64 x 64)
+constexpr unsigned kTcMaxPolls = 1u << 24;             // bound on the polls of one mbarrier wait
+constexpr unsigned long long kTcTimeoutNs = 1000000000ull;
+constexpr int kStatusTcTimeout = 2;                    // status[0] bit: a tensor-core completion wait ran out
+static_assert( kGemmSmemBytesF >= sizeof(float) * kTile * kTcSld, "result staging does not fit" );
 
 __device__ __forceinline__ unsigned to_tf32( float x )
 {
@@ -591,151 +647,272 @@ __device__ __forceinline__ unsigned to_tf32( float x )
     return r;
 }
 
-__device__ __forceinline__ void split_tf32( float x, unsigned & hi, unsigned & lo )
+__device__ __forceinline__ std::uint32_t smem_u32( const void * p )
 {
-    hi = to_tf32( x );
-    lo = to_tf32( x - __uint_as_float( hi ) );
+    return static_cast<std::uint32_t>( __cvta_generic_to_shared( p ) );
 }
 
-__device__ __forceinline__ void mma_tf32( float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2] )
+__device__ __forceinline__ unsigned long long tc_now()
 {
-    asm volatile( "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                  : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]) );
+    unsigned long long t;
+    asm volatile( "mov.u64 %0, %%globaltimer;\n" : "=l"(t) );
+    return t;
 }
 
-__device__ __forceinline__ void gemm_body( const GemmTask & t, float * __restrict__ arena, double * smem )
+__device__ __forceinline__ int ld_acquire_i32( const int * p )
 {
-    float * gsm = reinterpret_cast<float *>( smem );
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-    const int wm = warp & 1, wn = warp >> 1;
-    const int g = lane >> 2, tq = lane & 3;
+    int v;
+    asm volatile( "ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory" );
+    return v;
+}
+
+// Waits until the mbarrier phase of the given parity has completed; false
+// when the wait ran out (polls or time).
+__device__ __forceinline__ bool tc_wait( std::uint32_t bar, std::uint32_t parity )
+{
+    const unsigned long long start = tc_now();
+    for( unsigned i = 0; i < kTcMaxPolls; ++i )
+    {
+        std::uint32_t done;
+        asm volatile( "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                      : "=r"(done) : "r"(bar), "r"(parity) : "memory" );
+        if( done ) { return true; }
+        if( (i & 1023u) == 1023u && tc_now() - start > kTcTimeoutNs ) { return false; }
+    }
+    return false;
+}
+
+// Per-CTA tensor-core state: the accumulator's tensor-memory address, the two
+// stage mbarriers and the number of commits made to each (the parity of the
+// next completion to wait for), carried across the tasks of a persistent CTA.
+struct TcState
+{
+    std::uint32_t tmem;
+    std::uint32_t bar;            // shared address of bar[0]; bar[1] = bar + 8
+    unsigned commits0, commits1;  // commits made to bar[0] / bar[1]
+    __device__ unsigned commits( int s ) const { return s ? commits1 : commits0; }
+};
+
+// All threads of the CTA; warp 0 allocates the accumulator columns.
+__device__ __forceinline__ TcState tc_setup( std::uint64_t * bars, std::uint32_t * s_tmem )
+{
+    if( threadIdx.x == 0 )
+    {
+        asm volatile( "mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(smem_u32( bars )) );
+        asm volatile( "mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(smem_u32( bars + 1 )) );
+        asm volatile( "fence.mbarrier_init.release.cluster;\n" ::: "memory" );
+    }
+    if( (threadIdx.x >> 5) == 0 )
+    {
+        asm volatile( "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" :: "r"(smem_u32( s_tmem )), "r"(kTcCols) );
+        asm volatile( "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" );
+    }
+    asm volatile( "tcgen05.fence::before_thread_sync;\n" ::: "memory" );
+    __syncthreads();
+    asm volatile( "tcgen05.fence::after_thread_sync;\n" ::: "memory" );
+    TcState tc;
+    tc.tmem = *s_tmem;
+    tc.bar = smem_u32( bars );
+    tc.commits0 = 0;
+    tc.commits1 = 0;
+    return tc;
+}
+
+// All threads of the CTA, after its last task: frees the accumulator columns.
+__device__ __forceinline__ void tc_teardown( const TcState & tc )
+{
+    asm volatile( "tcgen05.fence::before_thread_sync;\n" ::: "memory" );
+    __syncthreads();
+    if( (threadIdx.x >> 5) == 0 )
+    {
+        asm volatile( "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tc.tmem), "r"(kTcCols) );
+    }
+}
+
+// Shared-memory matrix descriptor of one K-major no-swizzle operand part:
+// start address, leading byte offset 1024 (next 4 k), stride byte offset 128
+// (next 8 rows), descriptor version 1 (sm_100), no swizzle.
+__device__ __forceinline__ std::uint64_t tc_desc( std::uint32_t addr )
+{
+    return static_cast<std::uint64_t>( (addr >> 4) & 0x3FFFu ) | (static_cast<std::uint64_t>( 1024 >> 4 ) << 16)
+         | (static_cast<std::uint64_t>( 128 >> 4 ) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::tf32: FP32 accumulator, TF32 A and B, both
+// K-major, N = 64 (bits 17-22: N / 8), M = 64 (bits 24-28: M / 16).
+constexpr std::uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((64u >> 4) << 24);
+
+__device__ __forceinline__ void gemm_body( const GemmTask & t, float * __restrict__ arena, double * smem, TcState & tc,
+                                           int * status )
+{
+    unsigned char * sm = reinterpret_cast<unsigned char *>( smem );
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // this thread's elements of every chunk: k = 4 i + kl (i = 0..7), row mn of A and of B
+    const int mn = 8 * warp + (lane & 7), kl = lane >> 3;
+    const bool a_ok = t.m0 + mn < t.M, b_ok = t.c0 + mn < t.N;
     const float * A = arena + t.a;
     const float * B = arena + t.b;
-
-    float acc[2][2][4];
-#pragma unroll
-    for( int i = 0; i < 2; ++i )
-#pragma unroll
-        for( int j = 0; j < 2; ++j )
-#pragma unroll
-            for( int e = 0; e < 4; ++e ) { acc[i][j][e] = 0.0f; }
-
-    constexpr int kChunks = kGemmKF * kTile / 4 / kGemmThreads;      // 2 per operand
-    auto issue = [&]( int stage, int k0 )
+    const std::int64_t acol = t.m0 + mn, bcol = t.c0 + mn;
+    const int soff = warp * 128 + (lane & 7) * 16 + kl * 4;   // K-major offset of (mn, kl) in a part
+    const int nk = (t.K + kTcK - 1) / kTcK;
+    float ra[8], rb[8];
+    auto load = [&]( int c )
     {
-        float * As = gsm + stage * kGemmStageFloats;
-        float * Bs = As + kGemmKF * kGemmLdF;
 #pragma unroll
-        for( int l = 0; l < kChunks; ++l )
+        for( int i = 0; i < 8; ++i )
         {
-            const int idx = tid + kGemmThreads * l;
-            const int r = idx / (kTile / 4), c = 4 * (idx % (kTile / 4));
-            const int k = k0 + r;
-            const int am = min( max( t.M - (t.m0 + c), 0 ), 4 ), bn = min( max( t.N - (t.c0 + c), 0 ), 4 );
-            const int abytes = (k < t.K) ? 4 * am : 0;
-            const int bbytes = (k < t.K) ? 4 * bn : 0;
-            cp_async_16( As + r * kGemmLdF + c, abytes ? A + (std::int64_t)k * t.lda + t.m0 + c : A, abytes );
-            cp_async_16( Bs + r * kGemmLdF + c, bbytes ? B + (std::int64_t)k * t.ldb + t.c0 + c : B, bbytes );
+            const int k = c * kTcK + 4 * i + kl;
+            ra[i] = (k < t.K && a_ok) ? A[(std::int64_t)k * t.lda + acol] : 0.0f;
+            rb[i] = (k < t.K && b_ok) ? B[(std::int64_t)k * t.ldb + bcol] : 0.0f;
         }
     };
-
-    const int nk = (t.K + kGemmKF - 1) / kGemmKF;
+    if( nk > 0 ) { load( 0 ); }
+    bool ok = true;
+    for( int c = 0; c < nk; ++c )
+    {
+        const int s = c & 1;
+        unsigned char * st = sm + s * kTcStage;
+        float ca[8], cb[8];
 #pragma unroll
-    for( int s = 0; s < kGemmStages - 1; ++s )
-    {
-        if( s < nk ) { issue( s, s * kGemmKF ); }
-        cp_async_commit();
+        for( int i = 0; i < 8; ++i ) { ca[i] = ra[i]; cb[i] = rb[i]; }
+        if( c + 1 < nk ) { load( c + 1 ); }
+        // the stage is free once the MMAs of its previous chunk have completed
+        const bool mine = (tc.commits( s ) == 0) || tc_wait( tc.bar + 8 * s, (tc.commits( s ) & 1u) ^ 1u );
+#pragma unroll
+        for( int i = 0; i < 8; ++i )
+        {
+            const unsigned ha = to_tf32( ca[i] ), hb = to_tf32( cb[i] );
+            const int o = i * 1024 + soff;
+            *reinterpret_cast<unsigned *>( st + o ) = ha;
+            *reinterpret_cast<unsigned *>( st + kTcPart + o ) = to_tf32( ca[i] - __uint_as_float( ha ) );
+            *reinterpret_cast<unsigned *>( st + 2 * kTcPart + o ) = hb;
+            *reinterpret_cast<unsigned *>( st + 3 * kTcPart + o ) = to_tf32( cb[i] - __uint_as_float( hb ) );
+        }
+        asm volatile( "fence.proxy.async.shared::cta;\n" ::: "memory" );
+        if( __syncthreads_or( mine ? 0 : 1 ) ) { ok = false; break; }
+        if( tid == 0 )
+        {
+            asm volatile( "tcgen05.fence::after_thread_sync;\n" ::: "memory" );
+            const std::uint32_t base = smem_u32( st );
+#pragma unroll
+            for( int ks = 0; ks < kTcK / 8; ++ks )
+            {
+                const std::uint32_t off = ks * 2048;
+                const std::uint64_t ahi = tc_desc( base + off ), alo = tc_desc( base + kTcPart + off );
+                const std::uint64_t bhi = tc_desc( base + 2 * kTcPart + off ), blo = tc_desc( base + 3 * kTcPart + off );
+                const std::uint64_t ad[3] = { alo, ahi, ahi }, bd[3] = { bhi, blo, bhi };
+#pragma unroll
+                for( int u = 0; u < 3; ++u )
+                {
+                    const std::uint32_t accumulate = (c > 0 || ks > 0 || u > 0) ? 1u : 0u;
+                    asm volatile( "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                  "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+                                  :: "r"(tc.tmem), "l"(ad[u]), "l"(bd[u]), "r"(kTcIdesc), "r"(accumulate) );
+                }
+            }
+            asm volatile( "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                          :: "r"(tc.bar + 8 * s) : "memory" );
+        }
+        if( s ) { ++tc.commits1; } else { ++tc.commits0; }
     }
-    for( int kc = 0; kc < nk; ++kc )
+    // every commit of both stages complete: the accumulator is final and the
+    // stages are free for the next task
+    bool fine = ok;
+#pragma unroll
+    for( int s = 0; s < 2; ++s )
     {
-        cp_async_wait<kGemmStages - 2>();
+        if( fine && tc.commits( s ) > 0 ) { fine = tc_wait( tc.bar + 8 * s, (tc.commits( s ) & 1u) ^ 1u ); }
+    }
+    if( __syncthreads_or( fine ? 0 : 1 ) )
+    {
+        if( tid == 0 )
+        {
+            atomicOr( status, kStatusTcTimeout );
+            // one more bounded wait for the MMAs in flight before the memory is reused
+            for( int s = 0; s < 2; ++s ) { if( tc.commits( s ) > 0 ) { tc_wait( tc.bar + 8 * s, (tc.commits( s ) & 1u) ^ 1u ); } }
+        }
         __syncthreads();
-        {
-            const int nxt = kc + kGemmStages - 1;
-            if( nxt < nk ) { issue( nxt % kGemmStages, nxt * kGemmKF ); }
-            cp_async_commit();
-        }
-        const float * As = gsm + (kc % kGemmStages) * kGemmStageFloats;
-        const float * Bs = As + kGemmKF * kGemmLdF;
-#pragma unroll
-        for( int kk = 0; kk < kGemmKF; kk += 8 )
-        {
-            unsigned ah[2][4], al[2][4], bh[2][2], bl[2][2];
-#pragma unroll
-            for( int mi = 0; mi < 2; ++mi )
-            {
-                const int m = wm * 32 + mi * 16 + g;
-                split_tf32( As[(kk + tq) * kGemmLdF + m],         ah[mi][0], al[mi][0] );
-                split_tf32( As[(kk + tq) * kGemmLdF + m + 8],     ah[mi][1], al[mi][1] );
-                split_tf32( As[(kk + tq + 4) * kGemmLdF + m],     ah[mi][2], al[mi][2] );
-                split_tf32( As[(kk + tq + 4) * kGemmLdF + m + 8], ah[mi][3], al[mi][3] );
-            }
-#pragma unroll
-            for( int nj = 0; nj < 2; ++nj )
-            {
-                const int n = wn * 16 + nj * 8 + g;
-                split_tf32( Bs[(kk + tq) * kGemmLdF + n],     bh[nj][0], bl[nj][0] );
-                split_tf32( Bs[(kk + tq + 4) * kGemmLdF + n], bh[nj][1], bl[nj][1] );
-            }
-#pragma unroll
-            for( int mi = 0; mi < 2; ++mi )
-#pragma unroll
-                for( int nj = 0; nj < 2; ++nj )
-                {
-                    mma_tf32( acc[mi][nj], al[mi], bh[nj] );
-                    mma_tf32( acc[mi][nj], ah[mi], bl[nj] );
-                    mma_tf32( acc[mi][nj], ah[mi], bh[nj] );
-                }
-        }
+        return;
     }
-    cp_async_wait<0>();
-    __syncthreads();
-
-    float * C = arena + t.c;
-#pragma unroll
-    for( int mi = 0; mi < 2; ++mi )
+    if( nk == 0 ) { return; }
+    asm volatile( "tcgen05.fence::after_thread_sync;\n" ::: "memory" );
+    float * S = reinterpret_cast<float *>( sm );
     {
-#pragma unroll
-        for( int h = 0; h < 2; ++h )
+        // warp w reads accumulator rows 16 (w % 4) .. +15 (tensor-memory lanes 32 (w % 4) .. +15 for
+        // M = 64), columns 32 (w / 4) .. +31
+        const int q = warp & 3, h = warp >> 2;
+        std::uint32_t v[32];
+        asm volatile( "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+                        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                      : "r"(tc.tmem + ((std::uint32_t)(32 * q) << 16) + 32 * h) );
+        asm volatile( "tcgen05.wait::ld.sync.aligned;\n" ::: "memory" );
+        asm volatile( "tcgen05.fence::before_thread_sync;\n" ::: "memory" );
+        if( lane < 16 )
         {
-            const int row = t.m0 + wm * 32 + mi * 16 + g + 8 * h;
-            if( row >= t.M ) { continue; }
-            float * Crow = C + (std::int64_t)row * t.ldc;
+            float4 * dst = reinterpret_cast<float4 *>( S + (16 * q + lane) * kTcSld + 32 * h );
 #pragma unroll
-            for( int nj = 0; nj < 2; ++nj )
+            for( int j = 0; j < 8; ++j )
             {
-                const int col = t.c0 + wn * 16 + nj * 8 + 2 * tq;
-                const bool ok0 = col < t.N && (!t.upper || row <= col);
-                const bool ok1 = col + 1 < t.N && (!t.upper || row <= col + 1);
-                const float v0 = acc[mi][nj][2 * h], v1 = acc[mi][nj][2 * h + 1];
-                if( ok0 && ok1 )
-                {
-                    float2 v = *reinterpret_cast<const float2 *>( Crow + col );
-                    v.x -= v0;
-                    v.y -= v1;
-                    *reinterpret_cast<float2 *>( Crow + col ) = v;
-                }
-                else
-                {
-                    if( ok0 ) { Crow[col] -= v0; }
-                    if( ok1 ) { Crow[col + 1] -= v1; }
-                }
+                dst[j] = make_float4( __uint_as_float( v[4 * j] ), __uint_as_float( v[4 * j + 1] ),
+                                      __uint_as_float( v[4 * j + 2] ), __uint_as_float( v[4 * j + 3] ) );
             }
         }
     }
+    __syncthreads();
+    float * C = arena + t.c;
+    const int cq = 4 * (tid & 15);
+    const int col = t.c0 + cq;
+#pragma unroll
+    for( int i = 0; i < 4; ++i )
+    {
+        const int r = (tid >> 4) + 16 * i;
+        const int row = t.m0 + r;
+        if( row >= t.M || col >= t.N ) { continue; }
+        const float4 d = *reinterpret_cast<const float4 *>( S + r * kTcSld + cq );
+        float * Cp = C + (std::int64_t)row * t.ldc + col;
+        if( col + 3 < t.N && (!t.upper || row <= col) )
+        {
+            float4 x = *reinterpret_cast<float4 *>( Cp );
+            x.x -= d.x; x.y -= d.y; x.z -= d.z; x.w -= d.w;
+            *reinterpret_cast<float4 *>( Cp ) = x;
+        }
+        else
+        {
+            const float dv[4] = { d.x, d.y, d.z, d.w };
+#pragma unroll
+            for( int j = 0; j < 4; ++j )
+            {
+                if( col + j < t.N && (!t.upper || row <= col + j) ) { Cp[j] -= dv[j]; }
+            }
+        }
+    }
+    // the staged result and the accumulator are reused by the next task
+    __syncthreads();
 }
 
-template<typename T>
+// One CTA per SM slot, looping over the launch's tiles with its tensor memory
+// held throughout.
+__global__ __launch_bounds__(kGemmThreads, 3) void gemm_tc_kernel( const GemmTask * __restrict__ tasks, int count,
+                                                                  float * __restrict__ arena, int * status )
+{
+    extern __shared__ __align__(16) double gsm[];
+    __shared__ std::uint64_t bars[2];
+    __shared__ std::uint32_t s_tmem;
+    TcState tc = tc_setup( bars, &s_tmem );
+    for( int i = blockIdx.x; i < count; i += gridDim.x ) { gemm_body( tasks[i], arena, gsm, tc, status ); }
+    tc_teardown( tc );
+}
+
 __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask * __restrict__ tasks,
-                                                                T * __restrict__ arena )
+                                                                double * __restrict__ arena )
 {
     extern __shared__ __align__(16) double gsm[];
     gemm_body( tasks[blockIdx.x], arena, gsm );
 }
-
-template<typename T> constexpr size_t gemm_smem_bytes() { return sizeof(T) == 8 ? kGemmSmemBytes : kGemmSmemBytesF; }
 
 // ------------------------------------------------------------------ solves
 // The supernodal solves (LowerSolver.hpp:143-305, UpperSolver.hpp:127-255)
@@ -763,18 +940,16 @@ __device__ __forceinline__ void invert_body( const SolveDiagTask & t, const S * 
     const int tid = threadIdx.x;
     const int nb = min( kPanel, t.n0 - t.r0 );
     const S * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-#pragma unroll 4
-    for( int idx = tid; idx < kPanel * kPanel; idx += kInvThreads )
+    auto stage_src = [&]( int idx, double & fill ) -> const S *
     {
         const int r = idx >> 6, c = idx & 63;
-        if( r >= nb && r == c ) { D[r][c] = 1.0; }
-        else
-        {
-            const bool valid = r < nb && c < nb && c >= r;
-            stage_element( &D[r][c], U0, U0 + (std::int64_t)r * t.ld0 + c, valid );
-        }
-    }
+        fill = (r >= nb && r == c) ? 1.0 : 0.0;
+        return (r < nb && c < nb && c >= r) ? U0 + (std::int64_t)r * t.ld0 + c : nullptr;
+    };
+    auto stage_dst = [&]( int idx ) { return &D[idx >> 6][idx & 63]; };
+    stage_block<S, kPanel * kPanel / kInvThreads, kInvThreads>( U0, stage_src, stage_dst );
     cp_async_wait_all();
+    stage_finish<S, kPanel * kPanel / kInvThreads, kInvThreads>( stage_src, stage_dst );
     __syncthreads();
     if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
     __syncthreads();
@@ -840,14 +1015,16 @@ __device__ __forceinline__ void warp_rows_product( double (&acc)[kSolveMaxRhs / 
 // rest.  Warp w owns rows 8w..8w+7 of every 64 x kp product, kp = k rounded
 // up to a power of two >= 8, and skips row and K blocks beyond the panel's
 // nb rows and the task's cw rest rows.
+//
+// atomic_own: rows of the task's own front are updated with atomics too (the
+// task-graph solve, where panels of one front can run concurrently).
 template<typename T>
-__global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveRestTask * __restrict__ tasks, int upper,
-                                                                    const T * __restrict__ arena,
-                                                                    const double * __restrict__ tinv,
-                                                                    const std::int32_t * __restrict__ sn_inner,
-                                                                    double * in, double * out, int ld, int k, int lkp )
+__device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int upper, const T * __restrict__ arena,
+                                                 const double * __restrict__ tinv,
+                                                 const std::int32_t * __restrict__ sn_inner,
+                                                 double * in, double * out, int ld, int k, int lkp, bool atomic_own,
+                                                 double * ssm )
 {
-    extern __shared__ double ssm[];
     const int kp = 1 << lkp;
     const int ldv = kp + 4;
     double (*sT)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm );
@@ -855,7 +1032,6 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
     double * sX = ssm + 2 * kPanel * kTld;          // [64][ldv]: x_q (forward) / x_r (backward)
     double * sY = sX + kPanel * ldv;                // [64][ldv]: y_q
     __shared__ std::int64_t trow[kSolveRest];
-    const SolveRestTask t = tasks[blockIdx.x];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int nct = kp >> 3;
@@ -869,27 +1045,15 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
     const std::int64_t prow = (std::int64_t)t.row0 + t.r0;
 
     {
+        // only the leading (nb rounded up to 8)^2 block of T is read below
         const double * Tg = tinv + (std::int64_t)t.panel * (kPanel * kPanel);
+        const int nbp = 8 * nbb;
 #pragma unroll
         for( int u = 0; u < kPanel * kPanel / (2 * kSolveThreads); ++u )
         {
             const int idx = 2 * (tid + u * kSolveThreads);
-            cp_async_16( &sT[idx >> 6][idx & 63], Tg + idx, 16 );
-        }
-    }
-    if( has_rest )
-    {
-        const T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
-        const T * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
-#pragma unroll 4
-        for( int idx = tid; idx < kPanel * kPanel; idx += kSolveThreads )
-        {
-            const int i = idx >> 6, jj = idx & 63;
-            const int col = t.c0 + jj;
-            const bool valid = i < nb && jj < cw;
-            const T * src = U0;
-            if( valid ) { src = (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col : U1 + (std::int64_t)i * t.ld1 + (col - m); }
-            stage_element( &sP[i][jj], U0, src, valid );
+            const bool used = (idx >> 6) < nbp && (idx & 63) < nbp;
+            cp_async_16( &sT[idx >> 6][idx & 63], used ? Tg + idx : Tg, used ? 16 : 0 );
         }
     }
     // y_q: the panel's rows of `in` (forward: every task; backward: the owner)
@@ -918,6 +1082,24 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
             const bool valid = i < cw && c < k;
             cp_async_8( &sX[i * ldv + c], valid ? out + trow[i] * ld + c : out, valid );
         }
+    }
+    // the panel's rest block last: with FP32 storage its converting loads then
+    // overlap the copies above
+    if( has_rest )
+    {
+        const T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
+        const T * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
+        auto stage_src = [&]( int idx, double & ) -> const T *
+        {
+            const int i = idx >> 6, jj = idx & 63;
+            const int col = t.c0 + jj;
+            if( i >= nb || jj >= cw ) { return nullptr; }
+            return (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col : U1 + (std::int64_t)i * t.ld1 + (col - m);
+        };
+        auto stage_dst = [&]( int idx ) { return &sP[idx >> 6][idx & 63]; };
+        stage_block<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( U0, stage_src, stage_dst );
+        cp_async_wait_all();
+        stage_finish<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( stage_src, stage_dst );
     }
     cp_async_wait_all();
     __syncthreads();
@@ -973,7 +1155,7 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
                     const int c = ct * 8 + fj + e;
                     if( ct < nct && c < k )
                     {
-                        if( own_row ) { dst[c] -= acc[ct][e]; } else { atomicAdd( dst + c, -acc[ct][e] ); }
+                        if( own_row && !atomic_own ) { dst[c] -= acc[ct][e]; } else { atomicAdd( dst + c, -acc[ct][e] ); }
                     }
                 }
             }
@@ -1020,6 +1202,91 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
                     const int c = ct * 8 + fj + e;
                     if( ct < nct && c < k ) { atomicAdd( dst + c, acc[ct][e] ); }
                 }
+            }
+        }
+    }
+}
+
+template<typename T>
+__global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveRestTask * __restrict__ tasks, int upper,
+                                                                    const T * __restrict__ arena,
+                                                                    const double * __restrict__ tinv,
+                                                                    const std::int32_t * __restrict__ sn_inner,
+                                                                    double * in, double * out, int ld, int k, int lkp )
+{
+    extern __shared__ double ssm[];
+    solve_step_body( tasks[blockIdx.x], upper, arena, tinv, sn_inner, in, out, ld, k, lkp, false, ssm );
+}
+
+// The solve's task graph (Plan::solve_*) as one persistent launch per sweep:
+// CTAs take tasks in list order, thread 0 waits (bounded) until the task's
+// inputs are final, the CTA runs the step body with atomic updates of every
+// row, and thread 0 signals after a fence.  Forward: wait for the panel's
+// expected contributions, signal every target panel.  Back: wait until every
+// target panel has all of its tasks done, signal the task's own panel.
+template<typename T>
+__global__ __launch_bounds__(kSolveThreads) void solve_dag_kernel( const SolveDagArgs a, const T * __restrict__ arena,
+                                                                   double * in, double * out, int ld, int k, int lkp )
+{
+    extern __shared__ double ssm[];
+    __shared__ int s_idx, s_ok;
+    const int tid = threadIdx.x;
+    for( ;; )
+    {
+        if( tid == 0 )
+        {
+            int idx = a.ntasks, ok = 0;
+            if( *reinterpret_cast<volatile int *>( a.error ) == 0 ) { idx = atomicAdd( a.next, 1 ); }
+            if( idx < a.ntasks )
+            {
+                const int ti = a.order[idx];
+                const int g = ti - a.first_task;
+                const unsigned long long start = tc_now();
+                if( a.trace ) { a.trace[4 * (std::int64_t)idx] = start; a.trace[4 * (std::int64_t)idx + 3] = blockIdx.x; }
+                ok = 1;
+                // forward: one wait (the task's panel); back: one per target panel
+                const int nw = a.upper ? static_cast<int>( a.target_ptr[g + 1] - a.target_ptr[g] ) : 1;
+                for( int w = 0; w < nw && ok; ++w )
+                {
+                    const int pnl = a.upper ? a.targets[a.target_ptr[g] + w] : a.tasks[ti].panel - a.first_panel;
+                    const int need = a.upper ? a.panel_tasks[pnl] : a.fwd_expected[pnl];
+                    unsigned spins = 0;
+                    while( ld_acquire_i32( a.counters + pnl ) < need )
+                    {
+                        ++spins;
+                        if( (spins & 31u) == 0 )
+                        {
+                            if( *reinterpret_cast<volatile int *>( a.error ) != 0 ) { ok = 0; break; }
+                            if( tc_now() - start > a.timeout_ns || spins > kDagMaxSpins )
+                            {
+                                atomicCAS( a.error, 0, idx + 1 );
+                                ok = 0;
+                                break;
+                            }
+                        }
+                        __nanosleep( 64 );
+                    }
+                }
+                if( a.trace ) { a.trace[4 * (std::int64_t)idx + 1] = tc_now(); }
+            }
+            s_idx = idx;
+            s_ok = ok;
+        }
+        __syncthreads();
+        const int idx = s_idx;
+        if( idx >= a.ntasks || !s_ok ) { break; }
+        const int ti = a.order[idx];
+        solve_step_body( a.tasks[ti], a.upper, arena, a.tinv, a.sn_inner, in, out, ld, k, lkp, true, ssm );
+        __threadfence();
+        __syncthreads();
+        if( tid == 0 )
+        {
+            if( a.trace ) { a.trace[4 * (std::int64_t)idx + 2] = tc_now(); }
+            const int g = ti - a.first_task;
+            if( a.upper ) { atomicAdd( a.counters + (a.tasks[ti].panel - a.first_panel), 1 ); }
+            else
+            {
+                for( std::int64_t e = a.target_ptr[g]; e < a.target_ptr[g + 1]; ++e ) { atomicAdd( a.counters + a.targets[e], 1 ); }
             }
         }
     }
@@ -1092,7 +1359,11 @@ __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagAr
     T * arena = static_cast<T *>( a.arena );
     extern __shared__ __align__(16) double dsm[];
     __shared__ int s_idx, s_ok;
+    __shared__ std::uint64_t tc_bars[2];
+    __shared__ std::uint32_t tc_tmem;
     const int tid = threadIdx.x;
+    TcState tc{};
+    if constexpr ( sizeof(T) == 4 ) { tc = tc_setup( tc_bars, &tc_tmem ); }
     for( ;; )
     {
         if( tid == 0 )
@@ -1123,7 +1394,10 @@ __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagAr
             case LaunchKind::Extend: extend_body( a.extend[t.index], a.lut, arena ); break;
             case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], arena, a.status, dsm, a.pivot_floor ); break;
             case LaunchKind::Trsm:   trsm_body( a.panel[t.index], arena, dsm ); break;
-            case LaunchKind::Gemm:   gemm_body( a.gemm[t.index], arena, dsm ); break;
+            case LaunchKind::Gemm:
+                if constexpr ( sizeof(T) == 4 ) { gemm_body( a.gemm[t.index], arena, dsm, tc, a.status ); }
+                else { gemm_body( a.gemm[t.index], arena, dsm ); }
+                break;
             case LaunchKind::Invert: invert_body( a.sdiag[t.index], arena, a.tinv + (std::int64_t)t.index * (kPanel * kPanel), dsm ); break;
             default: break;
         }
@@ -1136,6 +1410,7 @@ __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagAr
             if( t.signal[1] >= 0 ) { atomicAdd( a.counters + t.signal[1], 1 ); }
         }
     }
+    if constexpr ( sizeof(T) == 4 ) { tc_teardown( tc ); }
 }
 
 // ------------------------------------------------------ permutations, SpMV
@@ -1379,9 +1654,22 @@ void launch_trsm( const PanelTask * tasks, int count, T * arena, cudaStream_t st
 }
 
 template<typename T>
-void launch_gemm( const GemmTask * tasks, int count, T * arena, cudaStream_t st )
+void launch_gemm( const GemmTask * tasks, int count, T * arena, int * status, cudaStream_t st )
 {
-    if( count > 0 ) { gemm_tn_kernel<<<count, kGemmThreads, gemm_smem_bytes<T>(), st>>>( tasks, arena ); }
+    if( count <= 0 ) { return; }
+    if constexpr ( sizeof(T) == 8 )
+    {
+        (void)status;
+        gemm_tn_kernel<<<count, kGemmThreads, kGemmSmemBytes, st>>>( tasks, arena );
+    }
+    else
+    {
+        int dev = 0, sms = 0;
+        cudaGetDevice( &dev );
+        cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
+        const int grid = std::min( count, 3 * std::max( sms, 1 ) );
+        gemm_tc_kernel<<<grid, kGemmThreads, kGemmSmemBytesF, st>>>( tasks, count, arena, status );
+    }
 }
 
 template<typename T>
@@ -1421,6 +1709,31 @@ static size_t solve_smem_bytes( int k )
 }
 
 template<typename T>
+void launch_solve_dag( const SolveDagArgs & args, int grid, const T * arena, double * in, double * out, int ld, int k,
+                       cudaStream_t st )
+{
+    if( args.ntasks > 0 && grid > 0 )
+    {
+        solve_dag_kernel<T><<<grid, kSolveThreads, solve_smem_bytes( k ), st>>>( args, arena, in, out, ld, k, solve_lkp( k ) );
+    }
+}
+
+int solve_dag_blocks_per_sm( int k )
+{
+    int n = 0;
+    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &n, solve_dag_kernel<double>, kSolveThreads, solve_smem_bytes( k ) ) != cudaSuccess )
+    {
+        return 0;
+    }
+    int m = 0;
+    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &m, solve_dag_kernel<float>, kSolveThreads, solve_smem_bytes( k ) ) != cudaSuccess )
+    {
+        return 0;
+    }
+    return std::min( n, m );
+}
+
+template<typename T>
 void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const T * arena, const double * tinv,
                         const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st )
 {
@@ -1444,7 +1757,8 @@ void launch_gather_diag( const std::int64_t * offsets, const T * arena, double *
     template void launch_extend<T>( const ExtendTask *, int, const std::int32_t *, T *, cudaStream_t );             \
     template void launch_potrf<T>( const PanelTask *, int, T *, int *, const double *, cudaStream_t );               \
     template void launch_trsm<T>( const PanelTask *, int, T *, cudaStream_t );                                       \
-    template void launch_gemm<T>( const GemmTask *, int, T *, cudaStream_t );                                        \
+    template void launch_gemm<T>( const GemmTask *, int, T *, int *, cudaStream_t );                                 \
+    template void launch_solve_dag<T>( const SolveDagArgs &, int, const T *, double *, double *, int, int, cudaStream_t );                                        \
     template void launch_factor_dag<T>( const DagArgs &, int, cudaStream_t );                                        \
     template void launch_invert_diag<T>( const SolveDiagTask *, int, const T *, double *, cudaStream_t );            \
     template void launch_solve_step<T>( const SolveRestTask *, int, bool, const T *, const double *,                \
@@ -1477,14 +1791,16 @@ cudaError_t configure_kernels()
     const struct { const void * fn; size_t bytes; } attrs[] = {
         { reinterpret_cast<const void *>( trsm_kernel<double> ), kTrsmSmemBytes },
         { reinterpret_cast<const void *>( trsm_kernel<float> ), kTrsmSmemBytes },
-        { reinterpret_cast<const void *>( gemm_tn_kernel<double> ), kGemmSmemBytes },
-        { reinterpret_cast<const void *>( gemm_tn_kernel<float> ), kGemmSmemBytesF },
+        { reinterpret_cast<const void *>( gemm_tn_kernel ), kGemmSmemBytes },
+        { reinterpret_cast<const void *>( gemm_tc_kernel ), kGemmSmemBytesF },
         { reinterpret_cast<const void *>( factor_dag_kernel<double> ), kDagSmemBytes },
         { reinterpret_cast<const void *>( factor_dag_kernel<float> ), kDagSmemBytes },
         { reinterpret_cast<const void *>( invert_diag_kernel<double> ), kInvSmemBytes },
         { reinterpret_cast<const void *>( invert_diag_kernel<float> ), kInvSmemBytes },
         { reinterpret_cast<const void *>( solve_step_kernel<double> ), solve_smem_bytes( kSolveMaxRhs ) },
         { reinterpret_cast<const void *>( solve_step_kernel<float> ), solve_smem_bytes( kSolveMaxRhs ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double> ), solve_smem_bytes( kSolveMaxRhs ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float> ), solve_smem_bytes( kSolveMaxRhs ) },
     };
     for( const auto & a : attrs )
     {

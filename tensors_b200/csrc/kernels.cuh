@@ -30,7 +30,9 @@ template<typename T> void launch_potrf( const PanelTask * tasks, int count, T * 
                                         const double * pivot_floor, cudaStream_t st );
 void launch_pivot_floor( const std::int64_t * offsets, const float * arena, double rel, double * out, int n, cudaStream_t st );
 template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, cudaStream_t st );
-template<typename T> void launch_gemm( const GemmTask * tasks, int count, T * arena, cudaStream_t st );
+// status[0] gets kStatusTcTimeout (2) when a tensor-core completion wait of
+// the FP32 path ran out (its tile is then not updated).
+template<typename T> void launch_gemm( const GemmTask * tasks, int count, T * arena, int * status, cudaStream_t st );
 
 // The numeric factorization as one persistent launch over the plan's task
 // graph (Plan::dag).  counters (dag_counters ints), next and error must be
@@ -73,6 +75,37 @@ void launch_invert_diag( const SolveDiagTask * tasks, int count, const T * arena
 template<typename T>
 void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, const T * arena, const double * tinv,
                         const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st );
+
+// The levels of the solve task graph as one persistent launch per sweep
+// (Plan::solve_*): counters (one per graph panel), next and error zero
+// before the launch; afterwards error != 0 names the list position (+ 1)
+// whose wait ran out of time.
+struct SolveDagArgs
+{
+    const SolveRestTask * tasks;          // all srest tasks
+    const std::int32_t * order;           // srest indices in the sweep's order
+    int ntasks;
+    int upper;
+    std::int64_t first_task;
+    int first_panel;
+    const std::int64_t * target_ptr;
+    const std::int32_t * targets;
+    const std::int32_t * fwd_expected;
+    const std::int32_t * panel_tasks;
+    int * counters;
+    int * next;
+    int * error;
+    const double * tinv;
+    const std::int32_t * sn_inner;
+    unsigned long long timeout_ns;
+    // optional execution trace, 4 entries per list position (as DagArgs::trace); nullptr: none
+    unsigned long long * trace;
+};
+template<typename T>
+void launch_solve_dag( const SolveDagArgs & args, int grid, const T * arena, double * in, double * out, int ld, int k,
+                       cudaStream_t st );
+// Resident CTAs per SM of the persistent solve kernel for k right-hand sides (0 on error).
+int solve_dag_blocks_per_sm( int k );
 
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
                          int n, int k, cudaStream_t st );

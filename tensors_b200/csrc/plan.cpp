@@ -688,6 +688,89 @@ void Plan::build( const Symbolic & sym )
             if( r.count > 0 ) { upper_launches.push_back( { LaunchKind::Solve, r.count, r.first, h, static_cast<I32>(q) } ); }
         }
     }
+    I32 solve_split = levels;
+    for( I32 h = 0; h < levels; ++h ) { if( level_steps[static_cast<size_t>(h)] >= kSolveDagMinSteps ) { solve_split = h; break; } }
+    solve_default_split = solve_split;
+    build_solve_graph( sym, solve_split );
+}
+
+void Plan::build_solve_graph( const Symbolic & sym, I32 split )
+{
+    solve_split_level = std::min( std::max( split, 0 ), levels );
+    solve_fwd_order.clear(); solve_bwd_order.clear(); solve_target_ptr.clear(); solve_targets.clear();
+    solve_fwd_expected.clear(); solve_panel_tasks.clear();
+    solve_first_task = static_cast<I64>( srest.size() );
+    for( const Launch & L : lower_launches )
+    {
+        if( L.level >= solve_split_level ) { solve_first_task = std::min( solve_first_task, L.first ); }
+    }
+    solve_first_panel = solve_first_task < static_cast<I64>( srest.size() ) ? srest[static_cast<size_t>( solve_first_task )].panel
+                                                                            : static_cast<I32>( sdiag.size() );
+    const I64 nt = static_cast<I64>( srest.size() ) - solve_first_task;
+    const I32 np = static_cast<I32>( sdiag.size() ) - solve_first_panel;
+    solve_target_ptr.assign( static_cast<size_t>( nt ) + 1, 0 );
+    solve_fwd_expected.assign( static_cast<size_t>( np ), 0 );
+    solve_panel_tasks.assign( static_cast<size_t>( np ), 0 );
+    if( nt == 0 ) { return; }
+
+    // panel id of (front, panel step)
+    auto front_of_row = [&]( I32 row ) { return front_of_sn[static_cast<size_t>( sym.row_to_sn[static_cast<size_t>( row )] )]; };
+    std::vector<std::vector<I32>> panel_of( static_cast<size_t>( front_count ) );
+    for( I32 p = solve_first_panel; p < static_cast<I32>( sdiag.size() ); ++p )
+    {
+        const SolveDiagTask & d = sdiag[static_cast<size_t>(p)];
+        std::vector<I32> & v = panel_of[static_cast<size_t>( front_of_row( d.row0 ) )];
+        const size_t q = static_cast<size_t>( d.r0 / kPanel );
+        if( v.size() <= q ) { v.resize( q + 1, -1 ); }
+        v[q] = p;
+    }
+    auto panel_of_row = [&]( I32 f, I32 local ) -> I32 {
+        const std::vector<I32> & v = panel_of[static_cast<size_t>(f)];
+        const size_t q = static_cast<size_t>( local / kPanel );
+        return q < v.size() ? v[q] : -1;
+    };
+    std::vector<I32> tg;
+    for( I64 i = 0; i < nt; ++i )
+    {
+        const SolveRestTask & t = srest[static_cast<size_t>( solve_first_task + i )];
+        ++solve_panel_tasks[static_cast<size_t>( t.panel - solve_first_panel )];
+        tg.clear();
+        if( t.c0 >= 0 )
+        {
+            const I32 f = front_of_row( t.row0 );
+            const I32 nb = std::min( kPanel, t.n0 - t.r0 );
+            const I32 r1 = t.r0 + nb, m = t.n0 - r1;
+            for( I32 col = t.c0; col < t.c1; ++col )
+            {
+                I32 p = -1;
+                if( col < m ) { p = panel_of_row( f, r1 + col ); }
+                else
+                {
+                    const I32 g = sym.sn_inner[static_cast<size_t>( t.inner + (col - m) )];
+                    const I32 fa = front_of_row( g );
+                    p = panel_of_row( fa, g - front_row0[static_cast<size_t>(fa)] );
+                }
+                if( p >= solve_first_panel && (tg.empty() || tg.back() != p) ) { tg.push_back( p ); }
+            }
+            std::sort( tg.begin(), tg.end() );
+            tg.erase( std::unique( tg.begin(), tg.end() ), tg.end() );
+        }
+        for( I32 p : tg )
+        {
+            solve_targets.push_back( p - solve_first_panel );
+            ++solve_fwd_expected[static_cast<size_t>( p - solve_first_panel )];
+        }
+        solve_target_ptr[static_cast<size_t>( i ) + 1] = static_cast<I64>( solve_targets.size() );
+        solve_fwd_order.push_back( static_cast<I32>( solve_first_task + i ) );
+    }
+    // back sweep: panels in reverse order, each panel's tasks in list order
+    for( I64 e = static_cast<I64>( srest.size() ); e > solve_first_task; )
+    {
+        I64 b = e - 1;
+        while( b > solve_first_task && srest[static_cast<size_t>( b - 1 )].panel == srest[static_cast<size_t>( e - 1 )].panel ) { --b; }
+        for( I64 j = b; j < e; ++j ) { solve_bwd_order.push_back( static_cast<I32>( j ) ); }
+        e = b;
+    }
 }
 
 } // namespace tb

@@ -156,6 +156,7 @@ struct ExportTask
 // reached by tasks earlier in the list, which the plan check verifies.
 constexpr int kDagWaits = 4;
 constexpr int kDagMinSteps = 8;      // levels from the first with this many panel steps run as the task graph
+constexpr int kSolveDagMinSteps = 4; // the same for the solves
 
 struct DagTask
 {
@@ -234,6 +235,25 @@ struct Plan
     std::vector<Launch> lower_launches;     // forward solve U^T y = b
     std::vector<Launch> upper_launches;     // back solve U x = y
 
+    // Solve task graph: the levels from solve_split_level up run as one
+    // persistent launch per sweep, the levels below as the launches above.
+    // A graph task is an srest task; its targets are the panels its rest
+    // rows belong to (panel ids relative to solve_first_panel).  Forward:
+    // a panel's tasks start once the solve_fwd_expected[p] graph tasks that
+    // target it have applied their updates; each task signals its targets.
+    // Back: a task starts once every target panel has all of its
+    // solve_panel_tasks tasks done; each task signals its own panel.
+    std::int32_t solve_split_level = 0;
+    std::int32_t solve_default_split = 0;         // first level with kSolveDagMinSteps or more panel steps
+    std::int32_t solve_first_panel = 0;
+    std::int64_t solve_first_task = 0;
+    std::vector<std::int32_t> solve_fwd_order;    // srest indices of the graph in forward order
+    std::vector<std::int32_t> solve_bwd_order;    // the same in back-sweep order
+    std::vector<std::int64_t> solve_target_ptr;   // per graph task (srest index - solve_first_task), + 1
+    std::vector<std::int32_t> solve_targets;
+    std::vector<std::int32_t> solve_fwd_expected; // per graph panel
+    std::vector<std::int32_t> solve_panel_tasks;  // per graph panel
+
     double gemm_flops = 0.0;                // useful flops of all GEMM tiles (upper part of diagonal tiles)
     double factor_flops = 0.0;              // reference supernodes: Sum [n0^3/3 + n0^2 n1 + n0 n1^2]
     double front_flops  = 0.0;              // the same sum over fronts (work actually executed)
@@ -243,6 +263,8 @@ struct Plan
     std::int64_t arena_size() const { return u0_size + u1_size + v_size; }
 
     void build( const Symbolic & sym );
+    // Fills the solve task graph for the levels from `split` up (levels: none).
+    void build_solve_graph( const Symbolic & sym, std::int32_t split );
 };
 
 } // namespace tb

@@ -200,6 +200,66 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
     }
     for( const Launch & L : pl.lower_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the forward solve"; } }
     for( const Launch & L : pl.upper_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the back solve"; } }
+    {
+        // solve task graph: sizes, ranges, and deadlock freedom: in the forward
+        // list every task that updates a panel's rows comes before the panel's
+        // first task; in the back list every task of a target panel comes
+        // before the task that reads it
+        const I64 nt = static_cast<I64>( pl.srest.size() ) - pl.solve_first_task;
+        const I64 np = static_cast<I64>( pl.sdiag.size() ) - pl.solve_first_panel;
+        if( static_cast<I64>( pl.solve_fwd_order.size() ) != (pl.solve_fwd_order.empty() ? 0 : nt)
+            || pl.solve_bwd_order.size() != pl.solve_fwd_order.size() )
+        {
+            return "solve graph order sizes";
+        }
+        if( !pl.solve_fwd_order.empty() )
+        {
+            if( static_cast<I64>( pl.solve_target_ptr.size() ) != nt + 1 || static_cast<I64>( pl.solve_fwd_expected.size() ) != np
+                || static_cast<I64>( pl.solve_panel_tasks.size() ) != np )
+            {
+                return "solve graph array sizes";
+            }
+            auto check_order = [&]( const std::vector<I32> & order, bool upper ) -> std::string
+            {
+                std::vector<I64> done( static_cast<size_t>( np ), 0 );       // forward: updates in; back: tasks done
+                std::vector<char> seen( static_cast<size_t>( nt ), 0 );
+                for( size_t pos = 0; pos < order.size(); ++pos )
+                {
+                    const I64 g = static_cast<I64>( order[pos] ) - pl.solve_first_task;
+                    if( g < 0 || g >= nt || seen[static_cast<size_t>(g)] ) { return "solve graph order is not a permutation"; }
+                    seen[static_cast<size_t>(g)] = 1;
+                    const I64 p = pl.srest[static_cast<size_t>( order[pos] )].panel - pl.solve_first_panel;
+                    if( p < 0 || p >= np ) { return "solve graph panel out of range"; }
+                    for( I64 e = pl.solve_target_ptr[static_cast<size_t>(g)]; e < pl.solve_target_ptr[static_cast<size_t>(g) + 1]; ++e )
+                    {
+                        const I32 q = pl.solve_targets[static_cast<size_t>(e)];
+                        if( q < 0 || q >= np ) { return "solve graph target out of range"; }
+                        if( upper && done[static_cast<size_t>(q)] != pl.solve_panel_tasks[static_cast<size_t>(q)] )
+                        {
+                            return "back-solve task at list position " + std::to_string( pos ) + " reads an unfinished panel";
+                        }
+                    }
+                    if( !upper && done[static_cast<size_t>(p)] != pl.solve_fwd_expected[static_cast<size_t>(p)] )
+                    {
+                        return "forward-solve task at list position " + std::to_string( pos ) + " starts before its updates";
+                    }
+                    if( upper ) { ++done[static_cast<size_t>(p)]; }
+                    else
+                    {
+                        for( I64 e = pl.solve_target_ptr[static_cast<size_t>(g)]; e < pl.solve_target_ptr[static_cast<size_t>(g) + 1]; ++e )
+                        {
+                            ++done[static_cast<size_t>( pl.solve_targets[static_cast<size_t>(e)] )];
+                        }
+                    }
+                }
+                return std::string();
+            };
+            std::string m = check_order( pl.solve_fwd_order, false );
+            if( !m.empty() ) { return m; }
+            m = check_order( pl.solve_bwd_order, true );
+            if( !m.empty() ) { return m; }
+        }
+    }
     return std::string();
 }
 

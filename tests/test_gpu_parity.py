@@ -254,6 +254,58 @@ def test_task_graph_and_level_schedules_agree_bitwise(grid, leaf, schedule):
     assert rel_err(xa, xb) < 1e-12
 
 
+@pytest.mark.parametrize("grid,leaf,nrhs", [(24, 64, 1), (28, 32, 16), (16, 8, 70)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_solve_task_graph_matches_level_launches(grid, leaf, nrhs, precision):
+    # the persistent solve runs the same step bodies in dependency order; rows
+    # shared between tasks are updated by atomic additions in another order, so
+    # the sweeps agree to rounding, and every schedule solves the system
+    A = M.grid_laplacian_3d(grid, 14, 1e-3)
+    perm = O.nested_dissection(A, leaf)
+    c = CholeskyDecomposition(A.outer, A.inner, perm)
+    c.SetPrecision(precision)
+    c.SetRefinement(1e-12, 30)
+    assert c.NumericFactorization(A.values) == 0
+    B = np.random.default_rng(grid + nrhs).standard_normal((A.n, nrhs))
+    out = {}
+    for sched in ("levels", "task_graph", "task_graph_all", "levels"):
+        c.SetSolveSchedule(sched)
+        out[sched] = (c.Solve(B), c.UpperSolve(B), c.LowerSolve(B))
+    ref = out["levels"]
+    S = A.to_scipy()
+    for sched in ("task_graph", "task_graph_all"):
+        # the refined mixed solve iterates from slightly different preconditioner
+        # outputs, so its result agrees to the refinement target instead
+        tols = (1e-12 if precision == "fp64" else 1e-8, 1e-12, 1e-12)
+        for got, want, tol in zip(out[sched], ref, tols):
+            assert rel_err(got, want) < tol, sched
+        X = out[sched][0]
+        R = B - S @ X
+        assert np.max(np.linalg.norm(R, axis=0) / np.linalg.norm(B, axis=0)) < 1e-10
+
+
+def test_solve_task_graph_without_device_allocation():
+    torch = pytest.importorskip("torch")
+    A = M.grid_laplacian_3d(20, 15, 1e-3)
+    perm = O.nested_dissection(A, 32)
+    c = CholeskyDecomposition(A.outer, A.inner, perm)
+    assert c.NumericFactorization(A.values) == 0
+    from tensors_b200 import _lib
+
+    lib = _lib.lib()
+    k = 4
+    B = torch.tensor(np.random.default_rng(3).standard_normal((A.n, k)), device="cuda")
+    c.SetSolveSchedule("levels")
+    X_lv = torch.zeros_like(B)
+    assert lib.tb_chol_solve_device(c.handle, 1.0, B.data_ptr(), k, 0.0, X_lv.data_ptr(), k, k) == 0
+    torch.cuda.synchronize()
+    c.SetSolveSchedule("task_graph")
+    X = torch.full_like(B, float("nan"))
+    assert lib.tb_chol_solve_device_noalloc(c.handle, 1.0, B.data_ptr(), k, 0.0, X.data_ptr(), k, k) == 0
+    torch.cuda.synchronize()
+    assert rel_err(X.cpu().numpy(), X_lv.cpu().numpy()) < 1e-12
+
+
 def test_graph_and_direct_launches_agree_bitwise():
     A = M.grid_laplacian_3d(10, 11, 1e-3)
     perm = O.nested_dissection(A, 16)
