@@ -19,7 +19,6 @@ namespace
 constexpr int kGemmThreads  = 256;
 constexpr int kGemmK        = 16;
 constexpr int kGemmLd       = kTile + 4;   // padded smem row (2 wavefronts per fragment load)
-constexpr int kPanelThreads = kRestChunk;
 constexpr int kSolveThreads = 256;
 
 __device__ __forceinline__ void dmma_8x8x4( double (&d)[2], double a, double b )
@@ -921,7 +920,6 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 // computed once after the factorization, so every CTA of a step can form the
 // panel's solution itself and no CTA waits for another.
 
-constexpr int kTld = kPanel + 4;   // padded shared-memory row of 64-wide blocks (conflict-free DMMA fragments)
 constexpr size_t kInvSmemBytes = sizeof(double) * (2 * kPanel * (kPanel + 1) + kPanel);
 
 // T = D^{-1} for the upper-triangular diagonal block D of one panel (nb x nb,
@@ -985,21 +983,20 @@ __global__ __launch_bounds__(kInvThreads) void invert_diag_kernel( const SolveDi
     invert_body( tasks[blockIdx.x], arena, tinv + (std::int64_t)blockIdx.x * (kPanel * kPanel), ism );
 }
 
-// acc[ct] (8 x 8 tile ct of this warp's 8 output rows) += sum over the K
-// blocks [kb0, kb1) of A(i, kk) * B(kk, ct * 8 + j).
-template<typename FA, typename FB>
-__device__ __forceinline__ void warp_rows_product( double (&acc)[kSolveMaxRhs / 8][2], int nct, int kb0, int kb1, FA a, FB b )
+constexpr int kTld = kPanel + 4;   // padded shared-memory row of 64-wide blocks (conflict-free DMMA fragments)
+
+// acc[ct] (8 x 8 tile ct of this warp's 8 output rows, NCT tiles) += sum over
+// the K blocks [kb0, kb1) of A(i, kk) * B(kk, ct * 8 + j).
+template<int NCT, typename FA, typename FB>
+__device__ __forceinline__ void warp_rows_product( double (&acc)[NCT][2], int kb0, int kb1, FA a, FB b )
 {
     for( int kb = kb0; kb < kb1; ++kb )
     {
 #pragma unroll
-        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+        for( int ct = 0; ct < NCT; ++ct )
         {
-            if( ct < nct )
-            {
-                dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return a( i, kb * 8 + kk ); },
-                                     [&]( int kk, int j ) { return b( kb * 8 + kk, ct * 8 + j ); } );
-            }
+            dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return a( i, kb * 8 + kk ); },
+                                 [&]( int kk, int j ) { return b( kb * 8 + kk, ct * 8 + j ); } );
         }
     }
 }
@@ -1012,21 +1009,25 @@ __device__ __forceinline__ void warp_rows_product( double (&acc)[kSolveMaxRhs / 
 // rows; a task adds T_q (y_q - P x_r) (owner) or -T_q P x_r, with x_r its rest
 // rows of `out`, already final.  The owner is the task with c0 <= 0: the
 // first rest chunk, or a rest-less task for a front's last panel without
-// rest.  Warp w owns rows 8w..8w+7 of every 64 x kp product, kp = k rounded
-// up to a power of two >= 8, and skips row and K blocks beyond the panel's
-// nb rows and the task's cw rest rows.
+// rest.  Warp w owns rows 8w..8w+7 of every 64 x KP product (KP = k rounded
+// up to a power of two >= 8) as 8 x 8 DMMA tiles and skips row and K blocks
+// beyond the panel's nb rows and the task's cw rest rows; only the used
+// block of T is copied.  The body is instantiated per KP: with the tile
+// counts known at compile time the tile loops unroll and the accumulators
+// take only the registers they need (a task ran 11.6 us with KP a run-time
+// value and 7 us with it fixed, 64^3 Laplacian with 16 RHS).
 //
 // atomic_own: rows of the task's own front are updated with atomics too (the
 // task-graph solve, where panels of one front can run concurrently).
-template<typename T>
+template<typename T, int KP>
 __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int upper, const T * __restrict__ arena,
                                                  const double * __restrict__ tinv,
                                                  const std::int32_t * __restrict__ sn_inner,
-                                                 double * in, double * out, int ld, int k, int lkp, bool atomic_own,
-                                                 double * ssm )
+                                                 double * in, double * out, int ld, int k, bool atomic_own, double * ssm )
 {
-    const int kp = 1 << lkp;
-    const int ldv = kp + 4;
+    constexpr int kp = KP;
+    constexpr int lkp = KP == 8 ? 3 : KP == 16 ? 4 : KP == 32 ? 5 : 6;
+    constexpr int ldv = kp + 4;
     double (*sT)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm );
     double (*sP)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm + kPanel * kTld );
     double * sX = ssm + 2 * kPanel * kTld;          // [64][ldv]: x_q (forward) / x_r (backward)
@@ -1034,7 +1035,7 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
     __shared__ std::int64_t trow[kSolveRest];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int nct = kp >> 3;
+    constexpr int nct = kp >> 3;
     const int nb = min( kPanel, t.n0 - t.r0 );
     const int nbb = (nb + 7) >> 3;
     const int r1 = t.r0 + nb;
@@ -1106,24 +1107,21 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
 
     const int fi = lane >> 2, fj = 2 * (lane & 3);     // accumulator fragment: row fi, columns fj, fj + 1
     const int o = warp * 8;
-    double acc[kSolveMaxRhs / 8][2];
+    double acc[nct][2];
 #pragma unroll
-    for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+    for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
     if( !upper )
     {
         // x_q = T^T y_q (T^T lower triangular: K blocks 0..warp)
         if( o < nb )
         {
-            warp_rows_product( acc, nct, 0, warp + 1, [&]( int i, int kk ) { return sT[kk][o + i]; },
+            warp_rows_product<nct>( acc, 0, warp + 1, [&]( int i, int kk ) { return sT[kk][o + i]; },
                                                       [&]( int kk, int c ) { return sY[kk * ldv + c]; } );
 #pragma unroll
-            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+            for( int ct = 0; ct < nct; ++ct )
             {
-                if( ct < nct )
-                {
-                    sX[(o + fi) * ldv + ct * 8 + fj]     = acc[ct][0];
-                    sX[(o + fi) * ldv + ct * 8 + fj + 1] = acc[ct][1];
-                }
+                sX[(o + fi) * ldv + ct * 8 + fj]     = acc[ct][0];
+                sX[(o + fi) * ldv + ct * 8 + fj + 1] = acc[ct][1];
             }
         }
         __syncthreads();
@@ -1138,8 +1136,8 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         if( !has_rest || o >= cw ) { return; }
         // rest rows: y_r -= P^T x_q
 #pragma unroll
-        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
-        warp_rows_product( acc, nct, 0, nbb, [&]( int i, int kk ) { return sP[kk][o + i]; },
+        for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+        warp_rows_product<nct>( acc, 0, nbb, [&]( int i, int kk ) { return sP[kk][o + i]; },
                                              [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
         const int jj = o + fi;
         if( jj < cw )
@@ -1147,13 +1145,13 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
             double * dst = in + trow[jj] * ld;
             const bool own_row = t.c0 + jj < m;
 #pragma unroll
-            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+            for( int ct = 0; ct < nct; ++ct )
             {
 #pragma unroll
                 for( int e = 0; e < 2; ++e )
                 {
                     const int c = ct * 8 + fj + e;
-                    if( ct < nct && c < k )
+                    if( c < k )
                     {
                         if( own_row && !atomic_own ) { dst[c] -= acc[ct][e]; } else { atomicAdd( dst + c, -acc[ct][e] ); }
                     }
@@ -1166,19 +1164,16 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         // sY rows of this warp <- (owner ? y_q : 0) - P x_r
         if( has_rest && o < nb )
         {
-            warp_rows_product( acc, nct, 0, (cw + 7) >> 3, [&]( int i, int kk ) { return sP[o + i][kk]; },
+            warp_rows_product<nct>( acc, 0, (cw + 7) >> 3, [&]( int i, int kk ) { return sP[o + i][kk]; },
                                                            [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
 #pragma unroll
-            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+            for( int ct = 0; ct < nct; ++ct )
             {
-                if( ct < nct )
-                {
 #pragma unroll
-                    for( int e = 0; e < 2; ++e )
-                    {
-                        double & v = sY[(o + fi) * ldv + ct * 8 + fj + e];
-                        v = (owner ? v : 0.0) - acc[ct][e];
-                    }
+                for( int e = 0; e < 2; ++e )
+                {
+                    double & v = sY[(o + fi) * ldv + ct * 8 + fj + e];
+                    v = (owner ? v : 0.0) - acc[ct][e];
                 }
             }
         }
@@ -1186,36 +1181,37 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         if( o >= nb ) { return; }
         // z = T (.) (T upper triangular: K blocks warp..nbb-1)
 #pragma unroll
-        for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
-        warp_rows_product( acc, nct, warp, nbb, [&]( int i, int kk ) { return sT[o + i][kk]; },
+        for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+        warp_rows_product<nct>( acc, warp, nbb, [&]( int i, int kk ) { return sT[o + i][kk]; },
                                                 [&]( int kk, int c ) { return sY[kk * ldv + c]; } );
         const int i = o + fi;
         if( i < nb )
         {
             double * dst = out + (prow + i) * ld;
 #pragma unroll
-            for( int ct = 0; ct < kSolveMaxRhs / 8; ++ct )
+            for( int ct = 0; ct < nct; ++ct )
             {
 #pragma unroll
                 for( int e = 0; e < 2; ++e )
                 {
                     const int c = ct * 8 + fj + e;
-                    if( ct < nct && c < k ) { atomicAdd( dst + c, acc[ct][e] ); }
+                    if( c < k ) { atomicAdd( dst + c, acc[ct][e] ); }
                 }
             }
         }
     }
 }
 
-template<typename T>
+// One kernel per right-hand-side width KP, so that each gets the registers it needs.
+template<typename T, int KP>
 __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveRestTask * __restrict__ tasks, int upper,
                                                                     const T * __restrict__ arena,
                                                                     const double * __restrict__ tinv,
                                                                     const std::int32_t * __restrict__ sn_inner,
-                                                                    double * in, double * out, int ld, int k, int lkp )
+                                                                    double * in, double * out, int ld, int k )
 {
-    extern __shared__ double ssm[];
-    solve_step_body( tasks[blockIdx.x], upper, arena, tinv, sn_inner, in, out, ld, k, lkp, false, ssm );
+    extern __shared__ __align__(16) double ssm[];
+    solve_step_body<T, KP>( tasks[blockIdx.x], upper, arena, tinv, sn_inner, in, out, ld, k, false, ssm );
 }
 
 // The solve's task graph (Plan::solve_*) as one persistent launch per sweep:
@@ -1224,11 +1220,11 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
 // row, and thread 0 signals after a fence.  Forward: wait for the panel's
 // expected contributions, signal every target panel.  Back: wait until every
 // target panel has all of its tasks done, signal the task's own panel.
-template<typename T>
+template<typename T, int KP>
 __global__ __launch_bounds__(kSolveThreads) void solve_dag_kernel( const SolveDagArgs a, const T * __restrict__ arena,
-                                                                   double * in, double * out, int ld, int k, int lkp )
+                                                                   double * in, double * out, int ld, int k )
 {
-    extern __shared__ double ssm[];
+    extern __shared__ __align__(16) double ssm[];
     __shared__ int s_idx, s_ok;
     const int tid = threadIdx.x;
     for( ;; )
@@ -1276,7 +1272,7 @@ __global__ __launch_bounds__(kSolveThreads) void solve_dag_kernel( const SolveDa
         const int idx = s_idx;
         if( idx >= a.ntasks || !s_ok ) { break; }
         const int ti = a.order[idx];
-        solve_step_body( a.tasks[ti], a.upper, arena, a.tinv, a.sn_inner, in, out, ld, k, lkp, true, ssm );
+        solve_step_body<T, KP>( a.tasks[ti], a.upper, arena, a.tinv, a.sn_inner, in, out, ld, k, true, ssm );
         __threadfence();
         __syncthreads();
         if( tid == 0 )
@@ -1712,25 +1708,36 @@ template<typename T>
 void launch_solve_dag( const SolveDagArgs & args, int grid, const T * arena, double * in, double * out, int ld, int k,
                        cudaStream_t st )
 {
-    if( args.ntasks > 0 && grid > 0 )
+    if( args.ntasks <= 0 || grid <= 0 ) { return; }
+    const size_t sm = solve_smem_bytes( k );
+    switch( solve_lkp( k ) )
     {
-        solve_dag_kernel<T><<<grid, kSolveThreads, solve_smem_bytes( k ), st>>>( args, arena, in, out, ld, k, solve_lkp( k ) );
+        case 3:  solve_dag_kernel<T, 8><<<grid, kSolveThreads, sm, st>>>( args, arena, in, out, ld, k ); break;
+        case 4:  solve_dag_kernel<T, 16><<<grid, kSolveThreads, sm, st>>>( args, arena, in, out, ld, k ); break;
+        case 5:  solve_dag_kernel<T, 32><<<grid, kSolveThreads, sm, st>>>( args, arena, in, out, ld, k ); break;
+        default: solve_dag_kernel<T, 64><<<grid, kSolveThreads, sm, st>>>( args, arena, in, out, ld, k ); break;
     }
+}
+
+template<typename T>
+int solve_dag_occupancy( int k )
+{
+    const size_t sm = solve_smem_bytes( k );
+    int n = 0;
+    cudaError_t e = cudaSuccess;
+    switch( solve_lkp( k ) )
+    {
+        case 3:  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &n, solve_dag_kernel<T, 8>, kSolveThreads, sm ); break;
+        case 4:  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &n, solve_dag_kernel<T, 16>, kSolveThreads, sm ); break;
+        case 5:  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &n, solve_dag_kernel<T, 32>, kSolveThreads, sm ); break;
+        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &n, solve_dag_kernel<T, 64>, kSolveThreads, sm ); break;
+    }
+    return e == cudaSuccess ? n : 0;
 }
 
 int solve_dag_blocks_per_sm( int k )
 {
-    int n = 0;
-    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &n, solve_dag_kernel<double>, kSolveThreads, solve_smem_bytes( k ) ) != cudaSuccess )
-    {
-        return 0;
-    }
-    int m = 0;
-    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &m, solve_dag_kernel<float>, kSolveThreads, solve_smem_bytes( k ) ) != cudaSuccess )
-    {
-        return 0;
-    }
-    return std::min( n, m );
+    return std::min( solve_dag_occupancy<double>( k ), solve_dag_occupancy<float>( k ) );
 }
 
 template<typename T>
@@ -1738,8 +1745,15 @@ void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, cons
                         const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
-    solve_step_kernel<<<count, kSolveThreads, solve_smem_bytes( k ), st>>>( tasks, upper ? 1 : 0, arena, tinv, sn_inner,
-                                                                           in, out, ld, k, solve_lkp( k ) );
+    const size_t sm = solve_smem_bytes( k );
+    const int u = upper ? 1 : 0;
+    switch( solve_lkp( k ) )
+    {
+        case 3:  solve_step_kernel<T, 8><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+        case 4:  solve_step_kernel<T, 16><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+        case 5:  solve_step_kernel<T, 32><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+        default: solve_step_kernel<T, 64><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+    }
 }
 
 template<typename T>
@@ -1797,10 +1811,22 @@ cudaError_t configure_kernels()
         { reinterpret_cast<const void *>( factor_dag_kernel<float> ), kDagSmemBytes },
         { reinterpret_cast<const void *>( invert_diag_kernel<double> ), kInvSmemBytes },
         { reinterpret_cast<const void *>( invert_diag_kernel<float> ), kInvSmemBytes },
-        { reinterpret_cast<const void *>( solve_step_kernel<double> ), solve_smem_bytes( kSolveMaxRhs ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<float> ), solve_smem_bytes( kSolveMaxRhs ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<double> ), solve_smem_bytes( kSolveMaxRhs ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<float> ), solve_smem_bytes( kSolveMaxRhs ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 8> ), solve_smem_bytes( 8 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 16> ), solve_smem_bytes( 16 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 32> ), solve_smem_bytes( 32 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 64> ), solve_smem_bytes( 64 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 8> ), solve_smem_bytes( 8 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 16> ), solve_smem_bytes( 16 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 32> ), solve_smem_bytes( 32 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 64> ), solve_smem_bytes( 64 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 8> ), solve_smem_bytes( 8 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 16> ), solve_smem_bytes( 16 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 32> ), solve_smem_bytes( 32 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 64> ), solve_smem_bytes( 64 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 8> ), solve_smem_bytes( 8 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 16> ), solve_smem_bytes( 16 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 32> ), solve_smem_bytes( 32 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 64> ), solve_smem_bytes( 64 ) },
     };
     for( const auto & a : attrs )
     {
