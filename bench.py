@@ -356,7 +356,7 @@ def run_c4(args):
     b = BatchedCholesky([(o, i, p) for o, i, v, p in systems])
     b.handle.SetPrecision("mixed")
     b.handle.SetRefinement(C4_TARGET, 60)
-    b.handle.SetSchedule(args.schedule or "task_graph_all")
+    b.handle.SetSchedule(args.schedule or "levels")
     b.handle.SymbolicFactorization()
     t_setup = time.perf_counter() - t0
     vals = torch.tensor(np.concatenate([v for o, i, v, p in systems]), device=dev)
@@ -393,7 +393,7 @@ def run_c4(args):
                    "rows": n, "factor_gflop": F / 1e9, "factor_ms": tf, "solve_ms": t - tf,
                    "systems_per_s": len(systems) / (t * 1e-3), "refinement": [it, rr], "relres": relres,
                    "perturbed_pivots": b.handle.PerturbedPivots(),
-                   "schedule": args.schedule or "task_graph_all", "setup_s": t_setup,
+                   "schedule": args.schedule or "levels", "setup_s": t_setup,
                    "plan": b.handle.PlanStats(), "clocks": clocks.summary()},
     }
     print(json.dumps(line))

@@ -157,8 +157,9 @@ int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
  * factorization (explicit zeros of merged fronts included), out[12] simulated
  * microseconds of the scheduled task graph (0 before the first numeric
  * factorization on a device), out[13] tasks of the graph, out[14] tasks of
- * the solve's task graph, out[15] its first level.  Returns the number of
- * entries written (at most cap). */
+ * the solve's task graph, out[15] its first level, out[16] CTAs of the
+ * persistent factorization launch (0 before the device plan exists).
+ * Returns the number of entries written (at most cap). */
 int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
 /* Host-side bounds check of every device task of the plan (also run before
  * the plan is first uploaded).  TB_OK or TB_ERR_INVALID_ARGUMENT with the
@@ -264,8 +265,9 @@ int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * sol
  * Batches of independent systems (no counterpart in the reference, which
  * factors one matrix per object).  The systems become the diagonal blocks of
  * one matrix handled by a tb_chol (tb_batch_handle gives it, for setters such
- * as the precision and for statistics); its schedule defaults to one
- * persistent launch for the whole batch (TB_SCHEDULE_TASK_GRAPH_ALL).  Each
+ * as the precision and for statistics); its schedule defaults to level
+ * launches over the merged task lists (TB_SCHEDULE_LEVELS; one persistent
+ * launch for the whole batch is TB_SCHEDULE_TASK_GRAPH_ALL).  Each
  * system keeps its own pattern, permutation (NULL: identity) and values;
  * right-hand sides and solutions are per system (host calls) or the systems'
  * row-major n_s x nrhs blocks stacked in system order (device calls, row

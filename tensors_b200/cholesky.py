@@ -371,11 +371,11 @@ class CholeskyDecomposition:
         return f.value, z.value
 
     def PlanStats(self) -> dict:
-        out = np.zeros(16, dtype=np.int64)
-        m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 16))
+        out = np.zeros(24, dtype=np.int64)
+        m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 24))
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
                 "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks",
-                "solve_graph_tasks", "solve_split_level"]
+                "solve_graph_tasks", "solve_split_level", "graph_ctas"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

@@ -1674,15 +1674,17 @@ void launch_factor_dag( const DagArgs & args, int grid, cudaStream_t st )
     if( args.ntasks > 0 && grid > 0 ) { factor_dag_kernel<T><<<grid, kDagThreads, kDagSmemBytes, st>>>( args ); }
 }
 
+// The occupancy query answers 1 for the FP32 instance, which allocates tensor
+// memory, although 3 such CTAs (64 KB of shared memory and 64 TMEM columns
+// each) were measured co-resident on one SM; both instances have the same
+// shared memory and launch bounds, so the FP64 instance's answer is used for
+// both.  Correctness does not depend on residency: tasks are taken by running
+// CTAs in a topological order.
 int factor_dag_blocks_per_sm()
 {
-    int b64 = 0, b32 = 0;
-    if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b64, factor_dag_kernel<double>, kDagThreads, kDagSmemBytes ) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b32, factor_dag_kernel<float>, kDagThreads, kDagSmemBytes ) != cudaSuccess )
-    {
-        return 0;
-    }
-    return b64 < b32 ? b64 : b32;
+    int b = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor( &b, factor_dag_kernel<double>, kDagThreads, kDagSmemBytes );
+    return e == cudaSuccess ? b : 0;
 }
 
 template<typename T>
