@@ -105,6 +105,10 @@ struct tb_chol
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // second stream of the level schedule: the GEMM tiles of a panel step that
+    // do not touch the next panel run there, overlapping the next potrf / trsm
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_trsm = nullptr, ev_rest = nullptr;
 
     // input pattern (copied, CholeskyDecomposition.hpp:313-371)
     std::int32_t n = 0;
@@ -211,6 +215,9 @@ struct tb_chol
         drop_solve_graphs();
         if( factor_graph ) { cudaGraphExecDestroy( factor_graph ); }
         if( own_stream && stream ) { cudaStreamDestroy( stream ); }
+        if( side ) { cudaStreamDestroy( side ); }
+        if( ev_trsm ) { cudaEventDestroy( ev_trsm ); }
+        if( ev_rest ) { cudaEventDestroy( ev_rest ); }
     }
 
     void invalidate_symbolic()
@@ -273,6 +280,12 @@ int ensure_device( tb_chol * h )
     {
         TB_CUDA( cudaStreamCreateWithFlags( &h->stream, cudaStreamNonBlocking ) );
         h->own_stream = true;
+    }
+    if( h->side == nullptr )
+    {
+        TB_CUDA( cudaStreamCreateWithFlags( &h->side, cudaStreamNonBlocking ) );
+        TB_CUDA( cudaEventCreateWithFlags( &h->ev_trsm, cudaEventDisableTiming ) );
+        TB_CUDA( cudaEventCreateWithFlags( &h->ev_rest, cudaEventDisableTiming ) );
     }
     if( !h->kernels_configured )
     {
@@ -405,21 +418,58 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         tb::launch_factor_dag<T>( a, h->dag_grid, st );
         return launches + (pl.dag.empty() ? 0 : 1);
     }
+    // One panel of look-ahead over two streams (the profiled path keeps one,
+    // so that every launch is timed alone).  Main stream: potrf(q), trsm(q),
+    // the tiles of step q that update panel q+1's rows (part 0).  Side
+    // stream: the other tiles of step q (part 1), after trsm(q); they run
+    // while potrf(q+1) and trsm(q+1) do.  Part 0 of step q waits for part 1
+    // of step q-1 (both update panel q+1's rows), which also orders
+    // potrf(q+1) after every update of its block; each C tile keeps the order
+    // of its updates, so the factor is the same bit for bit.
+    // Levels join the side stream at their boundaries (the next extend-adds
+    // read the update matrices the part-1 tiles write).
+    const bool overlap = !timed && h->side != nullptr;
+    bool side_busy = false;
+    std::int32_t level = -1;
+    auto join = [&]()
+    {
+        if( !side_busy ) { return; }
+        cudaEventRecord( h->ev_rest, h->side );
+        cudaStreamWaitEvent( st, h->ev_rest, 0 );
+        side_busy = false;
+    };
     for( const tb::Launch & L : pl.factor_launches )
     {
+        cudaStream_t s = st;
+        if( overlap )
+        {
+            if( L.level != level ) { join(); level = L.level; }
+            if( L.kind == tb::LaunchKind::Gemm )
+            {
+                if( L.part == 0 ) { join(); }
+                else
+                {
+                    cudaStreamWaitEvent( h->side, h->ev_trsm, 0 );
+                    s = h->side;
+                    side_busy = true;
+                }
+            }
+        }
         switch( L.kind )
         {
-            case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
-            case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
-            case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, st ); break;
-            case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
-            case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, st ); break;
-            case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
+            case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, s ); break;
+            case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, s ); break;
+            case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, s ); break;
+            case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, s ); break;
+            case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, s ); break;
+            case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, s ); break;
             default: break;
         }
+        if( overlap && L.kind == tb::LaunchKind::Trsm ) { cudaEventRecord( h->ev_trsm, st ); }
         mark( static_cast<int>( L.kind ) );
         ++launches;
     }
+    if( overlap ) { join(); }
     return launches;
 }
 

@@ -598,7 +598,13 @@ void Plan::build( const Symbolic & sym )
             const I32 gc = static_cast<I32>( static_cast<I64>(gemm.size()) - gfirst );
             if( oc > 0 ) { factor_launches.push_back( { LaunchKind::Potrf, oc, ofirst, h, q } ); }
             if( pc > 0 ) { factor_launches.push_back( { LaunchKind::Trsm, pc, pfirst, h, q } ); }
-            if( gc > 0 ) { factor_launches.push_back( { LaunchKind::Gemm, gc, gfirst, h, q } ); }
+            {
+                // the step's tiles are in the order of `order`: the next panel's rows first
+                I32 gn = 0;
+                for( size_t i : order ) { gn += tile_next[i] ? 1 : 0; }
+                if( gn > 0 ) { factor_launches.push_back( { LaunchKind::Gemm, gn, gfirst, h, q, 0 } ); }
+                if( gc > gn ) { factor_launches.push_back( { LaunchKind::Gemm, gc - gn, gfirst + gn, h, q, 1 } ); }
+            }
             rest_ranges[h][q] = { rfirst, static_cast<I32>( static_cast<I64>(srest.size()) - rfirst ) };
         }
         // task order of the level: P0 T0 I0, then per step q: the tiles that

@@ -169,6 +169,9 @@ struct DagTask
 enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, Invert = 4, Solve = 5, Potrf = 6 };
 
 // One launch: `count` tasks starting at `first` in the array of its kind.
+// A panel step's GEMM tiles come as two launches: part 0 updates the next
+// panel's rows (the next potrf / trsm wait for it), part 1 the rest of the
+// trailing matrix and the update matrices (it may overlap the next panel).
 struct Launch
 {
     LaunchKind   kind;
@@ -176,6 +179,7 @@ struct Launch
     std::int64_t first;
     std::int32_t level;
     std::int32_t step;
+    std::int32_t part = 0;
 };
 
 struct Plan
