@@ -528,12 +528,24 @@ void Plan::build( const Symbolic & sym )
                 const size_t tfirst = tiles.size();
                 if( m > 0 )
                 {
-                    const I64 pa = front_u0[f] + static_cast<I64>(r0) * ld0 + r1;        // U0[r0:r1, r1:n0]
-                    push_tiles( tiles, pa, ld0, pa, ld0, front_u0[f] + static_cast<I64>(r1) * ld0 + r1, ld0, nb, m, m, true );
+                    // Trailing updates are deferred over kDeferSteps panel steps: the
+                    // next panel's rows [r1, r1 + 64) get every pending panel at once,
+                    // and the whole trailing matrix is updated at every kDeferSteps-th
+                    // step, with the rows of the panels since the last such update
+                    // (contiguous in U0 / U1, K up to 64 kDeferSteps).  Each C entry is
+                    // read and written kDeferSteps times less often and the tiles are
+                    // that much deeper; the next panel still sees every update before
+                    // its potrf, and every contribution is applied exactly once.
+                    const I32 j = q % kDeferSteps;
+                    const I32 k0 = r0 - j * kPanel;
+                    const I32 K = r1 - k0;
+                    const I32 rows = (j + 1 < kDeferSteps) ? std::min( kPanel, m ) : m;
+                    const I64 pa = front_u0[f] + static_cast<I64>(k0) * ld0 + r1;        // U0[k0:r1, r1:n0]
+                    push_tiles( tiles, pa, ld0, pa, ld0, front_u0[f] + static_cast<I64>(r1) * ld0 + r1, ld0, K, rows, m, true );
                     if( n1 > 0 )
                     {
-                        push_tiles( tiles, pa, ld0, front_u1[f] + static_cast<I64>(r0) * ld1, ld1,
-                                    front_u1[f] + static_cast<I64>(r1) * ld1, ld1, nb, m, n1, false );
+                        push_tiles( tiles, pa, ld0, front_u1[f] + static_cast<I64>(k0) * ld1, ld1,
+                                    front_u1[f] + static_cast<I64>(r1) * ld1, ld1, K, rows, n1, false );
                     }
                     // tiles of rows [r1, r1 + 64) feed the next panel
                     for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_next.push_back( tiles[i].m0 == 0 ? 1 : 0 ); }

@@ -157,6 +157,7 @@ struct ExportTask
 constexpr int kDagWaits = 4;
 constexpr int kDagMinSteps = 8;      // levels from the first with this many panel steps run as the task graph
 constexpr int kSolveDagMinSteps = 4; // the same for the solves
+constexpr int kDeferSteps = 3;       // panel steps over which a front's trailing update is deferred
 
 struct DagTask
 {
