@@ -396,10 +396,9 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
             {
                 case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
                 case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
-                case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, st ); break;
-                case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, st ); break;
+                case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, h->tinv.ptr, st ); break;
+                case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
                 case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, st ); break;
-                case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
                 default: break;
             }
             ++launches;
@@ -459,10 +458,9 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         {
             case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, s ); break;
             case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, s ); break;
-            case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, s ); break;
-            case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, s ); break;
+            case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, h->tinv.ptr, s ); break;
+            case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, s ); break;
             case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, s ); break;
-            case tb::LaunchKind::Invert: tb::launch_invert_diag( h->sdiag.ptr + L.first, L.count, A, h->tinv.ptr, s ); break;
             default: break;
         }
         if( overlap && L.kind == tb::LaunchKind::Trsm ) { cudaEventRecord( h->ev_trsm, st ); }

@@ -241,7 +241,7 @@ constexpr int kTrsmThreads  = 256;
 constexpr int kSub          = 8;                     // sub-block edge
 constexpr int kSubs         = kPanel / kSub;         // 8 sub-blocks per panel edge
 constexpr int kXld          = kRestChunk + 4;        // padded row of the staged rest columns
-constexpr size_t kTrsmSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + kPanel * kXld + kPanel);
+constexpr size_t kTrsmSmemBytes = sizeof(double) * (2 * kPanel * kXld);
 
 // C(8x8) += A(8x8) * B(8x8) with A read through a(i, k), B through b(k, j)
 // and C through c(i, j) (warp-wide; fragment layouts of mma.m8n8k4.f64).
@@ -256,17 +256,24 @@ __device__ __forceinline__ void dmma_8x8x8( double (&acc)[2], FA a, FB b )
     }
 }
 
-constexpr size_t kPotrfSmemBytes = sizeof(double) * (kPanel * (kPanel + 1) + 2 * kPanel + 1);
+constexpr size_t kPotrfSmemBytes = sizeof(double) * (2 * kPanel * (kPanel + 1) + 2 * kPanel + 1);
 
+// Cholesky of one panel's 64 x 64 diagonal block D (identity beyond nb), in
+// shared memory by 8 x 8 sub-blocks, written back in place; then the inverse
+// T = D^{-1} (upper triangular, zero below the diagonal) into tinv block
+// t.panel, which the panel's trsm and the solves use.  With FP32 storage the
+// block is rounded to FP32 before the inversion, so that T inverts the stored
+// factor.
 template<typename T>
 __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict__ arena, int * __restrict__ status,
-                                            double * smem, const double * __restrict__ pivot_floor )
+                                            double * smem, const double * __restrict__ pivot_floor, double * __restrict__ tinv )
 {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
     double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem );
-    double * inv_d = smem + kPanel * (kPanel + 1);
+    double (*Ti)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem + kPanel * (kPanel + 1) );
+    double * inv_d = smem + 2 * kPanel * (kPanel + 1);
     double * floor_s = inv_d + kPanel;                  // the panel's pivot floors (mixed precision)
     int & fail = *reinterpret_cast<int *>( floor_s + kPanel );
 
@@ -387,118 +394,160 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
         atomicOr( status, 1 );
         atomicMin( status + 1, t.row0 + t.r0 + fail );
     }
+
+    // T = D^{-1} by 8 x 8 blocks: (a) the 8 diagonal blocks, one thread per
+    // column; (b) the blocks at distance d = 1..7 from the diagonal, one warp
+    // per block: T_ij = -T_ii sum_{k=i+1..j} D_ik T_kj (T_kj at smaller
+    // distances, so each distance is one round).
+    if constexpr ( sizeof(T) == 4 )
+    {
+        for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
+        {
+            double & v = D[idx / kPanel][idx % kPanel];
+            v = static_cast<double>( static_cast<float>( v ) );
+        }
+        __syncthreads();
+    }
+    if( tid < kPanel )
+    {
+        const int o = (tid >> 3) * kSub, j = tid & (kSub - 1);
+        double col[kSub];
+#pragma unroll
+        for( int i = kSub - 1; i >= 0; --i )
+        {
+            double s = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+            for( int k = i + 1; k < kSub; ++k ) { if( k <= j ) { s -= D[o + i][o + k] * col[k]; } }
+            col[i] = (i <= j) ? s / D[o + i][o + i] : 0.0;
+        }
+#pragma unroll
+        for( int i = 0; i < kSub; ++i ) { Ti[o + i][o + j] = col[i]; }
+    }
+    __syncthreads();
+    for( int d = 1; d < kSubs; ++d )
+    {
+        if( warp < kSubs - d )
+        {
+            const int ib = warp, jb = warp + d;
+            double acc[2] = { 0.0, 0.0 };
+            for( int kb = ib + 1; kb <= jb; ++kb )
+            {
+                dmma_8x8x8( acc, [&]( int i, int k ) { return D[kSub * ib + i][kSub * kb + k]; },
+                                 [&]( int k, int j ) { return Ti[kSub * kb + k][kSub * jb + j]; } );
+            }
+            // the sum goes through the warp's strictly lower block (7, warp) of
+            // Ti, which nothing else reads, into the B operand layout
+            double (*S)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( &Ti[kPanel - kSub][kSub * warp] );
+            const int ri = lane >> 2, cj = 2 * (lane & 3);
+            S[ri][cj] = acc[0];
+            S[ri][cj + 1] = acc[1];
+            __syncwarp();
+            double acc2[2] = { 0.0, 0.0 };
+            dmma_8x8x8( acc2, [&]( int i, int k ) { return Ti[kSub * ib + i][kSub * ib + k]; },
+                              [&]( int k, int j ) { return S[k][j]; } );
+            Ti[kSub * ib + ri][kSub * jb + cj]     = -acc2[0];
+            Ti[kSub * ib + ri][kSub * jb + cj + 1] = -acc2[1];
+        }
+        __syncthreads();
+    }
+    double * out = tinv + (std::int64_t)t.panel * (kPanel * kPanel);
+    for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
+    {
+        const int r = idx / kPanel, c = idx % kPanel;
+        out[idx] = (r <= c) ? Ti[r][c] : 0.0;
+    }
 }
 
 template<typename T>
 __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
                                                                T * __restrict__ arena, int * __restrict__ status,
-                                                               const double * __restrict__ pivot_floor )
+                                                               const double * __restrict__ pivot_floor,
+                                                               double * __restrict__ tinv )
 {
     extern __shared__ __align__(16) double psm[];
-    potrf_body( tasks[blockIdx.x], arena, status, psm, pivot_floor );
+    potrf_body( tasks[blockIdx.x], arena, status, psm, pivot_floor, tinv );
 }
 
-// Solve D^T x = u against the factored diagonal block for the rest columns
-// [c0, c0 + kRestChunk) (trsm of FactorizeSupernode, Multifrontal.hpp:
-// 452-466): the columns are staged in shared memory; per 8-row sub-block,
-// one thread per column solves the 8 x 8 triangle in registers, then the
-// warps update the rows below with DMMA (warp w owns columns 8w..8w+7).
+// X = D^{-T} U for the rest columns [c0, c0 + kRestChunk) of a panel (trsm of
+// FactorizeSupernode, Multifrontal.hpp:452-466) as the product X = T^T U with
+// the inverse T = D^{-1} that the panel's potrf left in tinv: X row block rb
+// takes the K blocks 0..rb.  Warp w computes the output tiles (rb, ct) with
+// rb = (w + ct) mod 8, one of every block row, so every warp does the same
+// 36 8 x 8 x 8 DMMA steps (when nb = 64); no step waits on another.
 template<typename T>
-__device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__ arena, double * tsm )
+__device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__ arena, const double * __restrict__ tinv,
+                                           double * tsm )
 {
-    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( tsm );
-    double (*X)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm + kPanel * (kPanel + 1) );
-    double * inv_d = tsm + kPanel * (kPanel + 1) + kPanel * kXld;
+    double (*Ti)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm );
+    double (*X)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm + kPanel * kXld );
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
+    const int nbb = (nb + kSub - 1) / kSub;
     const int r1 = t.r0 + nb;
     const int m = t.n0 - r1;
     const int rest = m + t.n1;
     const int cw = min( kRestChunk, rest - t.c0 );
     T * U0 = arena + t.u0;
     T * U1 = arena + t.u1;
-    // D (64 x 64) and the rest columns (64 x kRestChunk) as one block of
-    // 2 x 64 rows, so that with FP32 storage all loads are in flight together
-    static_assert( kRestChunk == kPanel, "trsm staging assumes square blocks" );
-    auto stage_src = [&]( int idx, double & fill ) -> const T *
+    static_assert( kRestChunk == kPanel, "trsm assumes square blocks" );
     {
-        const int r = (idx / kPanel) & (kPanel - 1), c = idx % kPanel;
-        if( idx < kPanel * kPanel )
+        // only the leading (nb rounded up to 8)^2 block of T is read
+        const double * Tg = tinv + (std::int64_t)t.panel * (kPanel * kPanel);
+        const int nbp = kSub * nbb;
+#pragma unroll
+        for( int u = 0; u < kPanel * kPanel / (2 * kTrsmThreads); ++u )
         {
-            fill = (r >= nb && r == c) ? 1.0 : 0.0;
-            return (r < nb && c < nb && r <= c) ? U0 + (std::int64_t)(t.r0 + r) * t.ld0 + t.r0 + c : nullptr;
+            const int idx = 2 * (tid + u * kTrsmThreads);
+            const bool used = (idx >> 6) < nbp && (idx & 63) < nbp;
+            cp_async_16( &Ti[idx >> 6][idx & 63], used ? Tg + idx : Tg, used ? 16 : 0 );
         }
+    }
+    auto stage_src = [&]( int idx, double & ) -> const T *
+    {
+        const int r = idx / kPanel, c = idx % kPanel;
         const int col = t.c0 + c;
         if( r >= nb || c >= cw ) { return nullptr; }
         return (col < m) ? U0 + (std::int64_t)(t.r0 + r) * t.ld0 + r1 + col
                          : U1 + (std::int64_t)(t.r0 + r) * t.ld1 + (col - m);
     };
-    auto stage_dst = [&]( int idx ) -> double *
-    {
-        const int r = (idx / kPanel) & (kPanel - 1), c = idx % kPanel;
-        return idx < kPanel * kPanel ? &D[r][c] : &X[r][c];
-    };
-    stage_block<T, 2 * kPanel * kPanel / kTrsmThreads, kTrsmThreads>( U0, stage_src, stage_dst );
+    auto stage_dst = [&]( int idx ) { return &X[idx / kPanel][idx % kPanel]; };
+    stage_block<T, kPanel * kRestChunk / kTrsmThreads, kTrsmThreads>( U0, stage_src, stage_dst );
     cp_async_wait_all();
-    stage_finish<T, 2 * kPanel * kPanel / kTrsmThreads, kTrsmThreads>( stage_src, stage_dst );
+    stage_finish<T, kPanel * kRestChunk / kTrsmThreads, kTrsmThreads>( stage_src, stage_dst );
     __syncthreads();
-    if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
-    __syncthreads();
-    const int nsub = (nb + kSub - 1) / kSub;
-    for( int b = 0; b < nsub; ++b )
+    const int nct = (cw + kSub - 1) / kSub;
+    for( int ct = 0; ct < kRestChunk / kSub; ++ct )
     {
-        const int o = b * kSub;
-        if( tid < kRestChunk )
+        const int rb = (warp + ct) & (kSubs - 1);
+        if( rb >= nbb || ct >= nct ) { continue; }
+        double acc[2] = { 0.0, 0.0 };
+        for( int kb = 0; kb <= rb; ++kb )
         {
-            double x[kSub];
-#pragma unroll
-            for( int r = 0; r < kSub; ++r ) { x[r] = X[o + r][tid]; }
-#pragma unroll
-            for( int r = 0; r < kSub; ++r )
-            {
-                x[r] *= inv_d[o + r];
-#pragma unroll
-                for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= D[o + r][o + r2] * x[r]; }
-            }
-#pragma unroll
-            for( int r = 0; r < kSub; ++r ) { X[o + r][tid] = x[r]; }
+            dmma_8x8x8( acc, [&]( int i, int k ) { return Ti[kSub * kb + k][kSub * rb + i]; },
+                             [&]( int k, int j ) { return X[kSub * kb + k][kSub * ct + j]; } );
         }
-        __syncthreads();
-        for( int b2 = b + 1; b2 < nsub; ++b2 )
+        const int r = kSub * rb + (lane >> 2);
+#pragma unroll
+        for( int e = 0; e < 2; ++e )
         {
-            const int o2 = b2 * kSub;
-            for( int ct = warp; ct < kRestChunk / kSub; ct += kTrsmThreads / 32 )
+            const int cc = kSub * ct + 2 * (lane & 3) + e;
+            if( r < nb && cc < cw )
             {
-                const int cb = ct * kSub;
-                double acc[2] = { 0.0, 0.0 };
-                dmma_8x8x8( acc, [&]( int i, int k ) { return D[o + k][o2 + i]; },
-                                 [&]( int k, int j ) { return X[o + k][cb + j]; } );
-                const int i = lane >> 2, j = 2 * (lane & 3);
-                X[o2 + i][cb + j]     -= acc[0];
-                X[o2 + i][cb + j + 1] -= acc[1];
+                const int col = t.c0 + cc;
+                if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = static_cast<T>( acc[e] ); }
+                else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = static_cast<T>( acc[e] ); }
             }
-        }
-        __syncthreads();
-    }
-    for( int idx = tid; idx < nb * kRestChunk; idx += kTrsmThreads )
-    {
-        const int r = idx / kRestChunk, cc = idx % kRestChunk;
-        const int col = t.c0 + cc;
-        if( cc < cw )
-        {
-            if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = static_cast<T>( X[r][cc] ); }
-            else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = static_cast<T>( X[r][cc] ); }
         }
     }
 }
 
 template<typename T>
 __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
-                                                             T * __restrict__ arena )
+                                                             T * __restrict__ arena, const double * __restrict__ tinv )
 {
     extern __shared__ __align__(16) double tsm[];
-    trsm_body( tasks[blockIdx.x], arena, tsm );
+    trsm_body( tasks[blockIdx.x], arena, tinv, tsm );
 }
 
 // ------------------------------------------------------------------- gemm
@@ -916,72 +965,9 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 // ------------------------------------------------------------------ solves
 // The supernodal solves (LowerSolver.hpp:143-305, UpperSolver.hpp:127-255)
 // run as one launch per (level, panel step) and sweep.  The triangular solves
-// with the 64 x 64 diagonal blocks become products with their inverses,
-// computed once after the factorization, so every CTA of a step can form the
-// panel's solution itself and no CTA waits for another.
-
-constexpr size_t kInvSmemBytes = sizeof(double) * (2 * kPanel * (kPanel + 1) + kPanel);
-
-// T = D^{-1} for the upper-triangular diagonal block D of one panel (nb x nb,
-// identity beyond nb): thread j < 64 back-substitutes D t = e_j for column j
-// of T, rows 63 down to 0, with four independent partial sums per row; all
-// threads stage D and write T.
-constexpr int kInvThreads = 256;
-
-template<typename S>
-__device__ __forceinline__ void invert_body( const SolveDiagTask & t, const S * __restrict__ arena,
-                                             double * __restrict__ out, double * ism )
-{
-    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( ism );
-    double (*T)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( ism + kPanel * (kPanel + 1) );
-    double * inv_d = ism + 2 * kPanel * (kPanel + 1);
-    const int tid = threadIdx.x;
-    const int nb = min( kPanel, t.n0 - t.r0 );
-    const S * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    auto stage_src = [&]( int idx, double & fill ) -> const S *
-    {
-        const int r = idx >> 6, c = idx & 63;
-        fill = (r >= nb && r == c) ? 1.0 : 0.0;
-        return (r < nb && c < nb && c >= r) ? U0 + (std::int64_t)r * t.ld0 + c : nullptr;
-    };
-    auto stage_dst = [&]( int idx ) { return &D[idx >> 6][idx & 63]; };
-    stage_block<S, kPanel * kPanel / kInvThreads, kInvThreads>( U0, stage_src, stage_dst );
-    cp_async_wait_all();
-    stage_finish<S, kPanel * kPanel / kInvThreads, kInvThreads>( stage_src, stage_dst );
-    __syncthreads();
-    if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
-    __syncthreads();
-    if( tid < kPanel )
-    {
-        const int j = tid;
-        for( int i = kPanel - 1; i >= 0; --i )
-        {
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-            int k = i + 1;
-            for( ; k + 3 < kPanel; k += 4 )
-            {
-                s0 += D[i][k]     * T[k][j];
-                s1 += D[i][k + 1] * T[k + 1][j];
-                s2 += D[i][k + 2] * T[k + 2][j];
-                s3 += D[i][k + 3] * T[k + 3][j];
-            }
-            for( ; k < kPanel; ++k ) { s0 += D[i][k] * T[k][j]; }
-            T[i][j] = ((i == j ? 1.0 : 0.0) - ((s0 + s1) + (s2 + s3))) * inv_d[i];
-        }
-    }
-    __syncthreads();
-    for( int idx = tid; idx < kPanel * kPanel; idx += kInvThreads ) { out[idx] = T[idx >> 6][idx & 63]; }
-    __syncthreads();
-}
-
-template<typename T>
-__global__ __launch_bounds__(kInvThreads) void invert_diag_kernel( const SolveDiagTask * __restrict__ tasks,
-                                                                   const T * __restrict__ arena,
-                                                                   double * __restrict__ tinv )
-{
-    extern __shared__ __align__(16) double ism[];
-    invert_body( tasks[blockIdx.x], arena, tinv + (std::int64_t)blockIdx.x * (kPanel * kPanel), ism );
-}
+// with the 64 x 64 diagonal blocks become products with their inverses
+// (computed by the panel potrf), so every CTA of a step can form the panel's
+// solution itself and no CTA waits for another.
 
 constexpr int kTld = kPanel + 4;   // padded shared-memory row of 64-wide blocks (conflict-free DMMA fragments)
 
@@ -1302,9 +1288,7 @@ __global__ __launch_bounds__(kSolveThreads) void solve_dag_kernel( const SolveDa
 // thread 0 reads counters with ld.acquire.gpu and the CTA synchronises
 // before any thread touches the task's data.
 constexpr int kDagThreads = 256;
-constexpr size_t kDagSmemBytes = kTrsmSmemBytes > kInvSmemBytes
-    ? (kTrsmSmemBytes > kGemmSmemBytes ? kTrsmSmemBytes : kGemmSmemBytes)
-    : (kInvSmemBytes > kGemmSmemBytes ? kInvSmemBytes : kGemmSmemBytes);
+constexpr size_t kDagSmemBytes = kTrsmSmemBytes > kGemmSmemBytes ? kTrsmSmemBytes : kGemmSmemBytes;
 static_assert( kDagSmemBytes >= kPotrfSmemBytes && kDagSmemBytes >= kGemmSmemBytesF, "persistent kernel shared memory too small" );
 
 __device__ __forceinline__ int ld_acquire( const int * p )
@@ -1388,13 +1372,12 @@ __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagAr
         {
             case LaunchKind::Zero:   zero_body( a.zero[t.index], arena ); break;
             case LaunchKind::Extend: extend_body( a.extend[t.index], a.lut, arena ); break;
-            case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], arena, a.status, dsm, a.pivot_floor ); break;
-            case LaunchKind::Trsm:   trsm_body( a.panel[t.index], arena, dsm ); break;
+            case LaunchKind::Potrf:  potrf_body( a.potrf[t.index], arena, a.status, dsm, a.pivot_floor, a.tinv ); break;
+            case LaunchKind::Trsm:   trsm_body( a.panel[t.index], arena, a.tinv, dsm ); break;
             case LaunchKind::Gemm:
                 if constexpr ( sizeof(T) == 4 ) { gemm_body( a.gemm[t.index], arena, dsm, tc, a.status ); }
                 else { gemm_body( a.gemm[t.index], arena, dsm ); }
                 break;
-            case LaunchKind::Invert: invert_body( a.sdiag[t.index], arena, a.tinv + (std::int64_t)t.index * (kPanel * kPanel), dsm ); break;
             default: break;
         }
         __threadfence();
@@ -1623,9 +1606,10 @@ void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lu
 }
 
 template<typename T>
-void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, const double * pivot_floor, cudaStream_t st )
+void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, const double * pivot_floor, double * tinv,
+                   cudaStream_t st )
 {
-    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, kPotrfSmemBytes, st>>>( tasks, arena, status, pivot_floor ); }
+    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, kPotrfSmemBytes, st>>>( tasks, arena, status, pivot_floor, tinv ); }
 }
 
 // floor[i] = rel * |diagonal entry of row i| after assembly (FP32 storage).
@@ -1644,9 +1628,9 @@ void launch_pivot_floor( const std::int64_t * offsets, const float * arena, doub
 }
 
 template<typename T>
-void launch_trsm( const PanelTask * tasks, int count, T * arena, cudaStream_t st )
+void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st )
 {
-    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, kTrsmSmemBytes, st>>>( tasks, arena ); }
+    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, kTrsmSmemBytes, st>>>( tasks, arena, tinv ); }
 }
 
 template<typename T>
@@ -1687,12 +1671,6 @@ int factor_dag_blocks_per_sm()
     return e == cudaSuccess ? b : 0;
 }
 
-template<typename T>
-void launch_invert_diag( const SolveDiagTask * tasks, int count, const T * arena, double * tinv, cudaStream_t st )
-{
-    if( count <= 0 ) { return; }
-    invert_diag_kernel<<<count, kInvThreads, kInvSmemBytes, st>>>( tasks, arena, tinv );
-}
 
 static int solve_lkp( int k )
 {
@@ -1771,12 +1749,11 @@ void launch_gather_diag( const std::int64_t * offsets, const T * arena, double *
     template void launch_export<T>( const ExportTask *, int, const std::int32_t *, const T *, double *, double *,    \
                                     cudaStream_t );                                                                \
     template void launch_extend<T>( const ExtendTask *, int, const std::int32_t *, T *, cudaStream_t );             \
-    template void launch_potrf<T>( const PanelTask *, int, T *, int *, const double *, cudaStream_t );               \
-    template void launch_trsm<T>( const PanelTask *, int, T *, cudaStream_t );                                       \
+    template void launch_potrf<T>( const PanelTask *, int, T *, int *, const double *, double *, cudaStream_t );     \
+    template void launch_trsm<T>( const PanelTask *, int, T *, const double *, cudaStream_t );                       \
     template void launch_gemm<T>( const GemmTask *, int, T *, int *, cudaStream_t );                                 \
     template void launch_solve_dag<T>( const SolveDagArgs &, int, const T *, double *, double *, int, int, cudaStream_t );                                        \
     template void launch_factor_dag<T>( const DagArgs &, int, cudaStream_t );                                        \
-    template void launch_invert_diag<T>( const SolveDiagTask *, int, const T *, double *, cudaStream_t );            \
     template void launch_solve_step<T>( const SolveRestTask *, int, bool, const T *, const double *,                \
                                         const std::int32_t *, double *, double *, int, int, cudaStream_t );         \
     template void launch_gather_diag<T>( const std::int64_t *, const T *, double *, int, cudaStream_t );
@@ -1805,14 +1782,14 @@ void launch_residual( int n, const std::int64_t * outer, const std::int32_t * in
 cudaError_t configure_kernels()
 {
     const struct { const void * fn; size_t bytes; } attrs[] = {
+        { reinterpret_cast<const void *>( potrf_kernel<double> ), kPotrfSmemBytes },
+        { reinterpret_cast<const void *>( potrf_kernel<float> ), kPotrfSmemBytes },
         { reinterpret_cast<const void *>( trsm_kernel<double> ), kTrsmSmemBytes },
         { reinterpret_cast<const void *>( trsm_kernel<float> ), kTrsmSmemBytes },
         { reinterpret_cast<const void *>( gemm_tn_kernel ), kGemmSmemBytes },
         { reinterpret_cast<const void *>( gemm_tc_kernel ), kGemmSmemBytesF },
         { reinterpret_cast<const void *>( factor_dag_kernel<double> ), kDagSmemBytes },
         { reinterpret_cast<const void *>( factor_dag_kernel<float> ), kDagSmemBytes },
-        { reinterpret_cast<const void *>( invert_diag_kernel<double> ), kInvSmemBytes },
-        { reinterpret_cast<const void *>( invert_diag_kernel<float> ), kInvSmemBytes },
         { reinterpret_cast<const void *>( solve_step_kernel<double, 8> ), solve_smem_bytes( 8 ) },
         { reinterpret_cast<const void *>( solve_step_kernel<double, 16> ), solve_smem_bytes( 16 ) },
         { reinterpret_cast<const void *>( solve_step_kernel<double, 32> ), solve_smem_bytes( 32 ) },

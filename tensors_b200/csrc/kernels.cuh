@@ -26,10 +26,12 @@ void launch_export( const ExportTask * tasks, int count, const std::int32_t * co
 template<typename T> void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, T * arena, cudaStream_t st );
 // pivot_floor (mixed precision only, else null): per permuted row the value a
 // non-positive or lost pivot is raised to instead of failing; status[2] counts them.
+// tinv: per panel (PanelTask::panel) the 64 x 64 inverse of its diagonal block, written here.
 template<typename T> void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status,
-                                        const double * pivot_floor, cudaStream_t st );
+                                        const double * pivot_floor, double * tinv, cudaStream_t st );
 void launch_pivot_floor( const std::int64_t * offsets, const float * arena, double rel, double * out, int n, cudaStream_t st );
-template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, cudaStream_t st );
+// Uses the inverse diagonal blocks the panels' potrf wrote to tinv.
+template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st );
 // status[0] gets kStatusTcTimeout (2) when a tensor-core completion wait of
 // the FP32 path ran out (its tile is then not updated).
 template<typename T> void launch_gemm( const GemmTask * tasks, int count, T * arena, int * status, cudaStream_t st );
@@ -67,9 +69,6 @@ template<typename T> void launch_factor_dag( const DagArgs & args, int grid, cud
 // Resident CTAs per SM of the persistent kernel (0 on error).
 int factor_dag_blocks_per_sm();
 
-// Inverse of every panel's diagonal block into tinv (count x 64 x 64).
-template<typename T>
-void launch_invert_diag( const SolveDiagTask * tasks, int count, const T * arena, double * tinv, cudaStream_t st );
 // One forward (upper = false) or backward solve step over `count` tasks;
 // in / out row-major with leading dimension ld, k <= kSolveMaxRhs columns.
 template<typename T>

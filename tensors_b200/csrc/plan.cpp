@@ -462,14 +462,15 @@ void Plan::build( const Symbolic & sym )
         }
 
         // panel steps; in the task graph a step's GEMM tiles that update the
-        // next panel's rows come first, then the next panel's potrf, trsm and
-        // inversion, then the rest of the step's tiles (one step of look-ahead)
+        // next panel's rows come first, then the next panel's potrf (which also
+        // inverts its diagonal block) and trsm, then the rest of the step's
+        // tiles (one step of look-ahead)
         I32 Q = 0;
         for( I32 f : L ) { Q = std::max<I32>( Q, static_cast<I32>( ceil_div( front_n0[f], kPanel ) ) ); }
         rest_ranges[h].resize( static_cast<size_t>(Q) );
         level_steps[static_cast<size_t>(h)] = Q;
         std::vector<std::vector<PendingTask>> step_potrf( static_cast<size_t>(Q) ), step_trsm( static_cast<size_t>(Q) ),
-            step_inv( static_cast<size_t>(Q) ), next_tiles( static_cast<size_t>(Q) ), rest_tiles( static_cast<size_t>(Q) );
+            next_tiles( static_cast<size_t>(Q) ), rest_tiles( static_cast<size_t>(Q) );
         for( I32 q = 0; q < Q; ++q )
         {
             const I64 ofirst = static_cast<I64>(potrf.size());
@@ -504,6 +505,7 @@ void Plan::build( const Symbolic & sym )
                 t.ld0 = ld0; t.ld1 = ld1;
                 t.row0 = front_row0[f];
                 t.single_rows = singles;
+                t.panel = pi;                   // == sdiag.size(): one potrf task and one SolveDiagTask per panel
                 {
                     PendingTask d = make( LaunchKind::Potrf, static_cast<I64>(potrf.size()) );
                     // the first panel starts once the children's contributions are in and
@@ -556,11 +558,6 @@ void Plan::build( const Symbolic & sym )
                     for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_next.push_back( 0 ); }
                 }
                 for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_panel.push_back( pi ); tile_prev.push_back( prev ); }
-                {
-                    PendingTask d = make( LaunchKind::Invert, static_cast<I64>(sdiag.size()) );
-                    add_wait( d, kPotrfDone, pi, 1 );
-                    step_inv[q].push_back( d );
-                }
                 {
                     SolveRestTask t{};
                     t.u0 = front_u0[f]; t.u1 = front_u1[f]; t.inner = front_cols[f];
@@ -619,14 +616,14 @@ void Plan::build( const Symbolic & sym )
             }
             rest_ranges[h][q] = { rfirst, static_cast<I32>( static_cast<I64>(srest.size()) - rfirst ) };
         }
-        // task order of the level: P0 T0 I0, then per step q: the tiles that
-        // feed panel q+1, panel q+1's potrf / trsm / inversion, the other tiles
+        // task order of the level: P0 T0, then per step q: the tiles that feed
+        // panel q+1, panel q+1's potrf and trsm, the other tiles
         auto emit = [&]( const std::vector<PendingTask> & v ) { pending.insert( pending.end(), v.begin(), v.end() ); };
-        if( Q > 0 ) { emit( step_potrf[0] ); emit( step_trsm[0] ); emit( step_inv[0] ); }
+        if( Q > 0 ) { emit( step_potrf[0] ); emit( step_trsm[0] ); }
         for( I32 q = 0; q < Q; ++q )
         {
             emit( next_tiles[q] );
-            if( q + 1 < Q ) { emit( step_potrf[q+1] ); emit( step_trsm[q+1] ); emit( step_inv[q+1] ); }
+            if( q + 1 < Q ) { emit( step_potrf[q+1] ); emit( step_trsm[q+1] ); }
             emit( rest_tiles[q] );
         }
         {
@@ -680,16 +677,9 @@ void Plan::build( const Symbolic & sym )
                                                           [&]( I32 l ) { return l >= dag_split_level; } ) - panel_level.begin() );
     }
 
-    // the launches that precede the persistent launch: the levels below the
-    // split and the inversion of their panels' diagonal blocks
+    // the launches that precede the persistent launch: the levels below the split
     pre_dag_launches.clear();
     for( const Launch & L : factor_launches ) { if( L.level < dag_split_level ) { pre_dag_launches.push_back( L ); } }
-    if( dag_first_panel > 0 ) { pre_dag_launches.push_back( { LaunchKind::Invert, dag_first_panel, 0, levels, 0 } ); }
-
-    if( !sdiag.empty() )
-    {
-        factor_launches.push_back( { LaunchKind::Invert, static_cast<I32>( sdiag.size() ), 0, levels, 0 } );
-    }
     for( I32 h = 0; h < levels; ++h )
     {
         for( size_t q = 0; q < rest_ranges[h].size(); ++q )

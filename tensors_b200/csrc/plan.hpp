@@ -87,7 +87,7 @@ struct PanelTask
     std::int32_t ld0, ld1;         // leading dimensions of U0 / U1
     std::int32_t r0, c0;
     std::int32_t row0;
-    std::int32_t pad;
+    std::int32_t panel;            // index of the panel (its potrf task, SolveDiagTask and inverse block)
     std::int64_t single_rows;      // bit r set: panel row r is a 1 x 1 reference supernode
 };
 

@@ -85,6 +85,13 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
             if( which == 1 && (t.c0 < 0 || t.c0 >= rest) ) { return "panel chunk out of range" + at; }
             if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "panel rows out of range" + at; }
+            // the inverse diagonal block: one per panel, written by the panel's potrf task
+            if( t.panel < 0 || t.panel >= static_cast<I32>( pl.sdiag.size() ) ) { return "panel index out of range" + at; }
+            if( which == 0 && t.panel != static_cast<I32>( k ) ) { return "potrf task is not its panel's" + at; }
+            if( which == 1 && (pl.potrf[static_cast<size_t>( t.panel )].r0 != t.r0 || pl.potrf[static_cast<size_t>( t.panel )].u0 != t.u0) )
+            {
+                return "trsm task names another panel" + at;
+            }
         }
     }
     for( size_t k = 0; k < pl.gemm.size(); ++k )
