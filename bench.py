@@ -343,8 +343,9 @@ def c4_systems(count=C4_COUNT):
 
 
 def run_c4(args):
-    """2,000 independent Delaunay systems factored as one batch (one persistent launch), FP32 factor + FP64
-    refinement to 1e-10, 1 RHS each."""
+    """2,000 independent Delaunay systems factored as one batch (level launches over the merged task lists),
+    FP32 factor + FP64 refinement to C4_TARGET, 1 RHS each.  When the refinement breaks down on a system
+    whose conditioning is beyond FP32, the handle falls back to an FP64 factor (reported in the line)."""
     systems = c4_systems(args.batch or C4_COUNT)       # process pool before any GPU call
     import torch
     from tensors_b200 import build as tb_build
@@ -393,6 +394,7 @@ def run_c4(args):
                    "rows": n, "factor_gflop": F / 1e9, "factor_ms": tf, "solve_ms": t - tf,
                    "systems_per_s": len(systems) / (t * 1e-3), "refinement": [it, rr], "relres": relres,
                    "perturbed_pivots": b.handle.PerturbedPivots(),
+                   "precision_in_use": list(b.handle.PrecisionInUse()),
                    "schedule": args.schedule or "levels", "setup_s": t_setup,
                    "plan": b.handle.PlanStats(), "clocks": clocks.summary()},
     }

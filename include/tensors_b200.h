@@ -189,6 +189,16 @@ int tb_chol_set_precision( tb_chol * h, int32_t precision );
 int tb_chol_set_refinement( tb_chol * h, double tol, int32_t max_iterations );
 /* Refinement steps and final relative residual of the last mixed solve. */
 int tb_chol_refinement_info( tb_chol * h, int32_t * iterations, double * relres );
+/* When the refinement of a mixed solve breaks down (its residual becomes
+ * non-finite, grows a million-fold, or misses the target within the cap:
+ * FP32 is too coarse for the matrix, kappa far beyond 1 / eps_fp32), the
+ * solve refactors the same matrix in FP64 from the values the handle holds
+ * on the device and runs the same refinement with the FP64 factor as the
+ * preconditioner; the handle then stays in FP64 (its solves still refined to
+ * the target) until tb_chol_set_precision is called again.  This reports the precision in use
+ * (TB_PRECISION_FP64 after such a fallback) and whether the fallback
+ * happened (no counterpart in the reference, which has no mixed precision). */
+int tb_chol_precision_in_use( tb_chol * h, int32_t * precision, int32_t * fell_back );
 /* Mixed precision only: pivots of the last factorization that came out at or
  * below tau = 1e-5 x |assembled diagonal entry of the row| and were raised to
  * tau instead of failing (static pivoting: for ill-conditioned matrices FP32

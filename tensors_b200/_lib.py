@@ -66,6 +66,7 @@ SIGNATURES = {
     "tb_chol_set_refinement": (ctypes.c_int, [_vp, _d, _i32]),
     "tb_chol_refinement_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]),
     "tb_chol_perturbed_pivots": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32)]),
+    "tb_chol_precision_in_use": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "tb_chol_set_profiling": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_kernel_profile": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "tb_chol_launch_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),

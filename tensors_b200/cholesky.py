@@ -140,6 +140,13 @@ class CholeskyDecomposition:
     def SetRefinement(self, tol: float = 1e-12, max_iterations: int = 30) -> None:
         _check(lib().tb_chol_set_refinement(self._h, float(tol), int(max_iterations)))
 
+    def PrecisionInUse(self):
+        """('fp64' | 'mixed', fell_back): the precision of the current factor; fell_back is True when a mixed
+        solve's refinement broke down and the handle refactored in FP64."""
+        p, f = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().tb_chol_precision_in_use(self._h, ctypes.byref(p), ctypes.byref(f)))
+        return ("mixed" if p.value == 1 else "fp64"), bool(f.value)
+
     def RefinementInfo(self):
         """(iterations, relative residual) of the last mixed-precision solve."""
         it = ctypes.c_int32()

@@ -171,6 +171,7 @@ struct tb_chol
     DeviceArray<double> ir_x, ir_r, ir_norms;
     DeviceArray<double> pivot_floor;             // mixed precision: static-pivot floor per row
     std::int32_t perturbed_pivots = 0;
+    bool fell_back = false;                      // a mixed solve's refinement failed: refactored in FP64
     PinnedBuffer pin_norms;
     bool trace = false;                          // record the persistent launch's execution trace
     DeviceArray<unsigned long long> trace_buf;
@@ -334,7 +335,7 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->status.reserve( 3 ) );
     TB_TRY( h->diag_off.upload( pl.diag_offset, st_ ) );
     TB_TRY( h->diag_vals.reserve( s.n ) );
-    if( h->precision == TB_PRECISION_MIXED ) { TB_TRY( h->pivot_floor.reserve( s.n ) ); }
+    if( h->precision == TB_PRECISION_MIXED ) { TB_TRY( h->pivot_floor.reserve( static_cast<std::int64_t>( s.n ) + 1 ) ); }
     TB_TRY( h->tinv.reserve( static_cast<std::int64_t>( pl.sdiag.size() ) * tb::kPanel * tb::kPanel ) );
     TB_TRY( h->dag.upload( pl.dag, st_ ) );
     TB_TRY( h->dag_state.reserve( static_cast<std::int64_t>( pl.dag_counters ) + 2 ) );
@@ -789,6 +790,32 @@ int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, st
 // max_c |r_c| / |b_c| <= tol or after the iteration cap.  Per-column scalars
 // stay on the device; the residual norms are read back once per iteration.
 int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
+                       double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs );
+
+// The refinement of a mixed solve failed (FP32 rounding is too coarse for
+// the matrix: kappa far above 1 / eps_fp32): refactor the same matrix in FP64
+// from the values the handle holds on the device and run the same conjugate
+// gradients with the FP64 factor as the preconditioner.  The handle stays in
+// FP64 until the precision is set again (tb_chol_precision_in_use tells).
+int solve_fp64_fallback( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
+                         double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
+{
+    h->precision = TB_PRECISION_FP64;
+    h->fell_back = true;
+    h->device_ready = false;
+    if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    h->drop_solve_graphs();
+    TB_TRY( ensure_device( h ) );
+    const int fs = run_factor( h, h->last_reg );
+    if( fs != TB_OK )
+    {
+        return fail( fs < 0 ? fs : TB_ERR_NOT_CONVERGED, "Solve: mixed-precision refinement failed and the FP64 "
+                     "refactorization did not succeed: " + g_error );
+    }
+    return run_solve_refined( h, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
+}
+
+int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
                        double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
 {
     cudaStream_t st = h->stream;
@@ -834,7 +861,8 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
     launches += h->solve_launch_count;
     apply( X, d_B, R );                                             // r = b - A x
     h->ir_iters = 0;
-    bool restart = true, verified = true;
+    bool restart = true, verified = true, broke_down = false;
+    double rel0 = 0.0;
     for( std::int32_t it = 0;; ++it )
     {
         TB_TRY( dots( R, k, R, k, rr ) );
@@ -845,9 +873,14 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
         for( std::int32_t c = 0; c < k; ++c )
         {
             const double bn = std::sqrt( hn[k + c] ), rn = std::sqrt( hn[c] );
-            rel = std::max( rel, bn > 0.0 ? rn / bn : rn );
+            const double v = bn > 0.0 ? rn / bn : rn;
+            if( !(v <= rel) ) { rel = v; }              // a NaN residual propagates (std::max would drop it)
         }
         h->ir_relres = rel;
+        if( it == 0 ) { rel0 = rel; }
+        // breakdown: a non-finite residual, or one grown far beyond the first
+        // (the FP32 factor is no preconditioner for this matrix)
+        if( !std::isfinite( rel ) || rel > 1e6 * rel0 ) { broke_down = true; break; }
         if( it >= h->ir_max ) { break; }
         if( rel <= h->ir_tol )
         {
@@ -880,6 +913,14 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
         ++launches;
         ++h->ir_iters;
     }
+    if( (broke_down || !(h->ir_relres <= h->ir_tol)) && h->precision == TB_PRECISION_MIXED )
+    {
+        return solve_fp64_fallback( h, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
+    }
+    if( broke_down )
+    {
+        return fail( TB_ERR_NOT_CONVERGED, "Solve: refinement broke down (non-finite or diverging residual)" );
+    }
     tb::launch_combine( n, k, alpha, X, k, beta, d_X, ldX, st );
     h->solve_launch_count = launches + 1;
     TB_CUDA( cudaGetLastError() );
@@ -896,7 +937,11 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
 int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
                       double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
 {
-    if( h->precision == TB_PRECISION_MIXED && which == 2 ) { return run_solve_refined( h, alpha, d_B, ldB, beta, d_X, ldX, nrhs ); }
+    // refined: mixed precision, and a handle that fell back to FP64 from it (its target still holds)
+    if( (h->precision == TB_PRECISION_MIXED || h->fell_back) && which == 2 )
+    {
+        return run_solve_refined( h, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
+    }
     return run_solve_core( h, which, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
 }
 
@@ -1362,6 +1407,7 @@ int tb_chol_set_precision( tb_chol * h, std::int32_t precision )
 {
     TB_TRY( check_handle( h ) );
     if( precision != TB_PRECISION_FP64 && precision != TB_PRECISION_MIXED ) { return fail( TB_ERR_INVALID_ARGUMENT, "unknown precision" ); }
+    h->fell_back = false;
     if( precision == h->precision ) { return TB_OK; }
     h->precision = precision;
     h->device_ready = false;        // storage of the other width; the next factorization re-creates the device plan
@@ -1386,6 +1432,14 @@ int tb_chol_refinement_info( tb_chol * h, std::int32_t * iterations, double * re
     TB_TRY( check_handle( h ) );
     if( iterations ) { *iterations = h->ir_iters; }
     if( relres ) { *relres = h->ir_relres; }
+    return TB_OK;
+}
+
+int tb_chol_precision_in_use( tb_chol * h, std::int32_t * precision, std::int32_t * fell_back )
+{
+    TB_TRY( check_handle( h ) );
+    if( precision ) { *precision = h->precision; }
+    if( fell_back ) { *fell_back = h->fell_back ? 1 : 0; }
     return TB_OK;
 }
 

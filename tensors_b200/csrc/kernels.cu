@@ -278,7 +278,8 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     int & fail = *reinterpret_cast<int *>( floor_s + kPanel );
 
     T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    if( pivot_floor != nullptr && tid < nb ) { floor_s[tid] = pivot_floor[t.row0 + t.r0 + tid]; }
+    if( pivot_floor != nullptr && tid < nb ) { floor_s[tid] = pivot_floor[1 + t.row0 + t.r0 + tid]; }
+    const double beta2 = pivot_floor != nullptr ? pivot_floor[0] : 0.0;
     auto stage_src = [&]( int idx, double & fill ) -> const T *
     {
         const int r = idx / kPanel, c = idx % kPanel;
@@ -307,15 +308,38 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
             {
                 double d = __shfl_sync( 0xffffffffu, a[r], r );
                 const bool single = (t.single_rows >> (o + r)) & 1;
-                if( pivot_floor != nullptr && !single && o + r < nb )
+                if( single ) { d = fabs( d ); }                     // 1 x 1 reference supernodes: sqrt(|a|)
+                if( pivot_floor != nullptr && o + r < nb )
                 {
-                    // mixed precision: a pivot lost to FP32 rounding is raised to
-                    // its floor (static pivoting); the FP64 refinement corrects it
+                    // mixed precision: a pivot lost to FP32 rounding (for a 1 x 1
+                    // supernode too: |a| can cancel to 0) is raised to its floor
+                    // (static pivoting); the FP64 refinement corrects it.  The
+                    // raised pivot also bounds the row's entries in the block by
+                    // beta = sqrt(max |a_ii|), the growth bound of the modified
+                    // Cholesky of Gill, Murray and Wright: a small pivot under a
+                    // large row would otherwise make the next pivots of the block
+                    // hugely negative, floored in turn, until FP32 overflows.
                     const double tau = floor_s[o + r];
                     if( !(d > tau) )
                     {
+                        // the row's largest entry: this sub-block's columns (registers),
+                        // the rest of the block (shared memory) and the row's rest
+                        // columns in U0 and U1, which the trsm divides by the pivot
+                        double m = (lane > r && lane < kSub) ? fabs( a[r] ) : 0.0;
+                        for( int c = o + kSub + lane; c < kPanel; c += 32 ) { m = fmax( m, fabs( D[o + r][c] ) ); }
+                        const std::int64_t grow = t.r0 + o + r;
+                        for( int c = t.r0 + nb + lane; c < t.n0; c += 32 )
+                        {
+                            m = fmax( m, fabs( static_cast<double>( arena[t.u0 + grow * t.ld0 + c] ) ) );
+                        }
+                        for( int c = lane; c < t.n1; c += 32 )
+                        {
+                            m = fmax( m, fabs( static_cast<double>( arena[t.u1 + grow * t.ld1 + c] ) ) );
+                        }
+#pragma unroll
+                        for( int s2 = 16; s2 > 0; s2 >>= 1 ) { m = fmax( m, __shfl_xor_sync( 0xffffffffu, m, s2 ) ); }
                         if( lane == 0 ) { atomicAdd( status + 2, 1 ); }
-                        d = tau;
+                        d = fmax( tau, beta2 > 0.0 ? m * m / beta2 : 0.0 );
                     }
                 }
                 if( lane == 0 )
@@ -323,7 +347,6 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
                     if( single ) { }
                     else if( o + r < nb && !(d > 0.0) && fail < 0 ) { fail = o + r; }
                 }
-                if( single ) { d = fabs( d ); }
                 // reciprocal square root and one product instead of sqrt and a
                 // division: both are long dependent sequences on the FP64 pipe
                 const double inv = rsqrt( d );
@@ -1613,17 +1636,31 @@ void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, 
 }
 
 // floor[i] = rel * |diagonal entry of row i| after assembly (FP32 storage).
+// out[1 + i] = rel * |a_ii|; out[0] = max_i |a_ii| (cleared by the caller),
+// by an integer maximum over the bit patterns of non-negative doubles.
 __global__ void pivot_floor_kernel( const std::int64_t * __restrict__ offsets, const float * __restrict__ arena, double rel,
                                     double * __restrict__ out, int n )
 {
+    unsigned long long mx = 0ull;
     for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
     {
-        out[i] = rel * fabs( static_cast<double>( arena[offsets[i]] ) );
+        const double a = fabs( static_cast<double>( arena[offsets[i]] ) );
+        out[1 + i] = rel * a;
+        const unsigned long long bits = static_cast<unsigned long long>( __double_as_longlong( a ) );
+        mx = bits > mx ? bits : mx;
     }
+#pragma unroll
+    for( int o = 16; o > 0; o >>= 1 )
+    {
+        const unsigned long long v = __shfl_xor_sync( 0xffffffffu, mx, o );
+        mx = v > mx ? v : mx;
+    }
+    if( (threadIdx.x & 31) == 0 && mx != 0ull ) { atomicMax( reinterpret_cast<unsigned long long *>( out ), mx ); }
 }
 
 void launch_pivot_floor( const std::int64_t * offsets, const float * arena, double rel, double * out, int n, cudaStream_t st )
 {
+    cudaMemsetAsync( out, 0, sizeof(double), st );
     pivot_floor_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( offsets, arena, rel, out, n );
 }
 

@@ -24,11 +24,13 @@ template<typename T>
 void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const T * arena,
                     double * tri, double * rec, cudaStream_t st );
 template<typename T> void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, T * arena, cudaStream_t st );
-// pivot_floor (mixed precision only, else null): per permuted row the value a
-// non-positive or lost pivot is raised to instead of failing; status[2] counts them.
+// pivot_floor (mixed precision only, else null): element 0 the largest |a_ii|,
+// element 1 + i the value a non-positive or lost pivot of permuted row i is
+// raised to instead of failing; status[2] counts them.
 // tinv: per panel (PanelTask::panel) the 64 x 64 inverse of its diagonal block, written here.
 template<typename T> void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status,
                                         const double * pivot_floor, double * tinv, cudaStream_t st );
+// out (n + 1 doubles): the pivot floors in the layout of launch_potrf's pivot_floor.
 void launch_pivot_floor( const std::int64_t * offsets, const float * arena, double rel, double * out, int n, cudaStream_t st );
 // Uses the inverse diagonal blocks the panels' potrf wrote to tinv.
 template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st );

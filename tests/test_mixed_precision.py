@@ -121,3 +121,39 @@ def test_mixed_task_graph_matches_levels_bitwise(schedule):
     ta, ra = a.FactorValues()
     tb_, rb = b.FactorValues()
     assert np.array_equal(ta, tb_) and np.array_equal(ra, rb)
+
+
+def test_mixed_factor_stays_finite_when_pivots_are_raised():
+    # A Delaunay system of the batched workload (cotangent Laplacian of 13,580
+    # random points + 1e-3 lumped mass, kappa ~1e10) on which FP32 rounding
+    # wipes out several pivots.  Raised pivots must not let the rows below them
+    # grow until FP32 overflows (which left NaN in the factor before the growth
+    # bound); the refined solve then reaches what FP64 reaches.
+    seed = 0x5EED0004
+    m = np.random.default_rng(seed).integers(500, 20001, size=25)[24]
+    A = M.delaunay_laplacian(int(m), seed + 24, 1e-3)
+    perm = O.nested_dissection(A)
+    B = np.random.default_rng(7).standard_normal((A.n, 2))
+    ref = CholeskyDecomposition(A.outer, A.inner, perm)
+    assert ref.NumericFactorization(A.values, 0.0) == 0
+    target = max(1e-10, 4.0 * relres(A, ref.Solve(B), B, 0.0))
+
+    mix = CholeskyDecomposition(A.outer, A.inner, perm)
+    mix.SetPrecision("mixed")
+    mix.SetRefinement(target, 100)
+    assert mix.NumericFactorization(A.values, 0.0) == 0
+    tri, rec = mix.FactorValues()
+    assert np.isfinite(tri).all() and np.isfinite(rec).all(), mix.PerturbedPivots()
+    X = mix.Solve(B)
+    it, rr = mix.RefinementInfo()
+    assert np.isfinite(X).all() and rr <= target, (it, rr, target, mix.PerturbedPivots())
+    assert relres(A, X, B, 0.0) <= 2 * target
+    # whether the FP32 factor sufficed or the solve fell back to an FP64 factor,
+    # the handle says which, and a new precision setting clears the fallback
+    used, fell_back = mix.PrecisionInUse()
+    assert (used, fell_back) in (("mixed", False), ("fp64", True))
+    if fell_back:
+        tri, rec = mix.FactorValues()
+        assert np.isfinite(tri).all() and np.isfinite(rec).all()
+    mix.SetPrecision("mixed")
+    assert mix.PrecisionInUse() == ("mixed", False)
