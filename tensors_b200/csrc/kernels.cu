@@ -118,25 +118,16 @@ __global__ void assemble_kernel( const double * __restrict__ values, const std::
 }
 
 // ------------------------------------------------------------------ zeroing
+// One warp per row of the task's rows, lanes over its columns [r, n).
 template<typename T>
 __device__ __forceinline__ void zero_body( const ZeroTask & t, T * __restrict__ arena )
 {
-    if constexpr ( sizeof(T) != 8 )
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for( int r = t.row_begin + static_cast<int>( threadIdx.x >> 5 ); r < t.row_end; r += warps )
     {
-        T * p = arena + t.offset;
-        for( std::int64_t i = threadIdx.x; i < t.count; i += blockDim.x ) { p[i] = T( 0 ); }
-        return;
+        T * row = arena + t.offset + static_cast<std::int64_t>( r ) * t.ld;
+        for( int c = r + lane; c < t.n; c += 32 ) { row[c] = T( 0 ); }
     }
-    double * p = reinterpret_cast<double *>( arena ) + t.offset;
-    std::int64_t i = threadIdx.x;
-    // align to 16 bytes, then store double2
-    const int head = static_cast<int>( (reinterpret_cast<std::uintptr_t>( p ) >> 3) & 1 );
-    if( head && threadIdx.x == 0 && t.count > 0 ) { p[0] = 0.0; }
-    const std::int64_t body = (t.count - head) / 2;
-    double2 * q = reinterpret_cast<double2 *>( p + head );
-    for( ; i < body; i += blockDim.x ) { q[i] = make_double2( 0.0, 0.0 ); }
-    const std::int64_t tail = head + 2 * body;
-    if( threadIdx.x == 0 && tail < t.count ) { p[tail] = 0.0; }
 }
 
 template<typename T>

@@ -395,15 +395,23 @@ void Plan::build( const Symbolic & sym )
             const I64 first = static_cast<I64>(zero.size());
             for( I32 f : L )
             {
-                const I64 sz = static_cast<I64>(front_n1[f]) * front_ld1[f];
-                for( I64 o = 0; o < sz; o += kZeroChunk )
+                // the upper triangle only, in groups of rows of about kZeroChunk entries
+                const I32 nv = front_n1[f];
+                for( I32 r = 0; r < nv; )
                 {
+                    I32 e = r;
+                    I64 cnt = 0;
+                    while( e < nv && cnt < kZeroChunk ) { cnt += nv - e; ++e; }
                     PendingTask t = make( LaunchKind::Zero, static_cast<I64>(zero.size()) );
                     if( prev_ext_level >= 0 ) { add_wait( t, kExtLevel, prev_ext_level, prev_ext_count ); }
                     t.signal[0] = { kZeroDone, f };
                     pending.push_back( t );
                     ++zero_of[f];
-                    zero.push_back( { front_v[f] + o, std::min( kZeroChunk, sz - o ) } );
+                    ZeroTask z{};
+                    z.offset = front_v[f]; z.count = cnt;
+                    z.n = nv; z.ld = front_ld1[f]; z.row_begin = r; z.row_end = e;
+                    zero.push_back( z );
+                    r = e;
                 }
             }
             const I32 count = static_cast<I32>( static_cast<I64>(zero.size()) - first );

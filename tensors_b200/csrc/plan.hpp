@@ -127,10 +127,13 @@ struct SolveRestTask
     std::int32_t panel, pad;
 };
 
-// Zero `count` doubles at arena offset `offset`.
+// Zero rows [row_begin, row_end) of the upper triangle of the n x n update
+// matrix at arena offset `offset` (leading dimension ld): columns [r, n) of
+// row r, `count` entries in all.  The strictly lower triangle is never read.
 struct ZeroTask
 {
     std::int64_t offset, count;
+    std::int32_t n, ld, row_begin, row_end;
 };
 
 // Copy rows [r_begin, r_end) of reference supernode sn from its front into

@@ -47,7 +47,11 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
     }
     for( const ZeroTask & z : pl.zero )
     {
-        if( z.count <= 0 || !in_range( z.offset, z.offset + z.count - 1, arena ) ) { return "zero task out of range"; }
+        if( z.count <= 0 || z.row_begin < 0 || z.row_begin >= z.row_end || z.row_end > z.n || z.n > z.ld )
+        {
+            return "bad zero task";
+        }
+        if( !in_range( z.offset, z.offset + static_cast<I64>( z.row_end - 1 ) * z.ld + z.n - 1, arena ) ) { return "zero task out of range"; }
     }
     for( size_t k = 0; k < pl.extend.size(); ++k )
     {
