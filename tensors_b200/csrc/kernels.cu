@@ -422,6 +422,9 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
         }
         __syncthreads();
     }
+    // reciprocal pivots of the (possibly rounded) block, one division per thread
+    if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
+    __syncthreads();
     if( tid < kPanel )
     {
         const int o = (tid >> 3) * kSub, j = tid & (kSub - 1);
@@ -432,7 +435,7 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
             double s = (i == j) ? 1.0 : 0.0;
 #pragma unroll
             for( int k = i + 1; k < kSub; ++k ) { if( k <= j ) { s -= D[o + i][o + k] * col[k]; } }
-            col[i] = (i <= j) ? s / D[o + i][o + i] : 0.0;
+            col[i] = (i <= j) ? s * inv_d[o + i] : 0.0;
         }
 #pragma unroll
         for( int i = 0; i < kSub; ++i ) { Ti[o + i][o + j] = col[i]; }
