@@ -10,6 +10,7 @@
 #include "plan_check.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <string>
 
 namespace tb
@@ -96,6 +97,29 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             {
                 return "trsm task names another panel" + at;
             }
+        }
+    }
+    {
+        // every panel's contribution to every trailing entry is applied exactly
+        // once, however the updates are grouped (deferral over panel steps):
+        // the tiles' flops equal, front by front summed, 2 nb per upper entry of
+        // each panel's trailing block and U1 rows, plus the update matrix V
+        double expect = 0.0;
+        const I32 F = pl.front_count;
+        for( I32 f = 0; f < F; ++f )
+        {
+            const double n0 = pl.front_n0[static_cast<size_t>(f)], n1 = pl.front_n1[static_cast<size_t>(f)];
+            for( I32 r0 = 0; r0 < pl.front_n0[static_cast<size_t>(f)]; r0 += kPanel )
+            {
+                const double nb = std::min<double>( kPanel, n0 - r0 ), m = n0 - r0 - nb;
+                expect += 2.0 * nb * (m * (m + 1.0) / 2.0 + m * n1);
+            }
+            if( n1 > 0 && pl.front_parent[static_cast<size_t>(f)] < F ) { expect += 2.0 * n0 * n1 * (n1 + 1.0) / 2.0; }
+        }
+        if( std::abs( expect - pl.gemm_flops ) > 1e-12 * std::max( 1.0, expect ) )
+        {
+            return "GEMM tiles do not apply every panel update exactly once (flops " + std::to_string( pl.gemm_flops )
+                   + ", expected " + std::to_string( expect ) + ")";
         }
     }
     for( size_t k = 0; k < pl.gemm.size(); ++k )
