@@ -230,6 +230,16 @@ int tb_chol_set_schedule( tb_chol * h, int32_t schedule );
  * out of time is reported (TB_ERR_TIMEOUT) by the next call that
  * synchronizes with the solve. */
 int tb_chol_set_solve_schedule( tb_chol * h, int32_t schedule );
+/* Autotuner (no counterpart in the reference): after a numeric
+ * factorization, times the factorization of the same values under
+ * TB_SCHEDULE_LEVELS and TB_SCHEDULE_TASK_GRAPH and one solve with nrhs
+ * right-hand sides under both solve schedules (best of two runs each, after
+ * one that captures the graphs), and keeps the fastest of each.  The factor
+ * is the same bit for bit under both factor schedules, so it stays valid.
+ * choice (2 entries, may be NULL): the factor and the solve schedule chosen;
+ * times_ms (4 entries, may be NULL): factor levels, factor task graph, solve
+ * levels, solve task graph. */
+int tb_chol_autotune( tb_chol * h, int32_t nrhs, int32_t * choice, double * times_ms );
 /* Execution trace of the persistent factorization launch: when enabled,
  * each task records when it was taken, when its inputs were ready, when it
  * was done (%globaltimer ns) and which CTA ran it.  tb_chol_trace writes 6

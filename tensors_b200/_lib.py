@@ -59,6 +59,7 @@ SIGNATURES = {
     "tb_chol_launch_counts": (ctypes.c_int, [_vp, _pi64, _pi64]),
     "tb_chol_set_schedule": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_set_solve_schedule": (ctypes.c_int, [_vp, _i32]),
+    "tb_chol_autotune": (ctypes.c_int, [_vp, _i32, _vp, _vp]),
     "tb_chol_set_trace": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64]),
     "tb_chol_solve_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64]),

@@ -181,6 +181,17 @@ class CholeskyDecomposition:
         m = _check(lib().tb_chol_solve_trace(self._h, out.ctypes.data, cap))
         return out[: 6 * m].reshape(m, 6)
 
+    def Autotune(self, nrhs: int = 1) -> dict:
+        """Time both factor schedules (on the last factorization's values) and both solve schedules (nrhs
+        right-hand sides), keep the fastest of each; returns the choice and the times in ms."""
+        choice = np.zeros(2, dtype=np.int32)
+        times = np.zeros(4)
+        _check(lib().tb_chol_autotune(self._h, int(nrhs), choice.ctypes.data, times.ctypes.data))
+        names = {0: "levels", 1: "task_graph", 2: "task_graph_all"}
+        return {"factor": names[int(choice[0])], "solve": names[int(choice[1])],
+                "times_ms": {"factor_levels": times[0], "factor_task_graph": times[1],
+                             "solve_levels": times[2], "solve_task_graph": times[3]}}
+
     def SetTrace(self, enabled: bool) -> None:
         _check(lib().tb_chol_set_trace(self._h, 1 if enabled else 0))
 

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <cmath>
@@ -1400,6 +1401,69 @@ int tb_chol_set_solve_schedule( tb_chol * h, std::int32_t schedule )
         }
     }
     h->drop_solve_graphs();
+    return TB_OK;
+}
+
+int tb_chol_autotune( tb_chol * h, std::int32_t nrhs, std::int32_t * choice, double * times_ms )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    cudaStream_t st = h->stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TB_CUDA( cudaEventCreate( &e0 ) );
+    TB_CUDA( cudaEventCreate( &e1 ) );
+    auto elapsed = [&]() -> double {
+        float ms = 0.0f;
+        cudaEventSynchronize( e1 );
+        cudaEventElapsedTime( &ms, e0, e1 );
+        return ms;
+    };
+    const double inf = std::numeric_limits<double>::infinity();
+    const std::int32_t sched[2] = { TB_SCHEDULE_LEVELS, TB_SCHEDULE_TASK_GRAPH };
+    double t[4] = { inf, inf, inf, inf };
+    int status = TB_OK;
+    // factorization: the same values and shift as the last one; the factor is
+    // the same bit for bit under both schedules, so the handle's stays valid
+    for( int s = 0; s < 2 && status == TB_OK; ++s )
+    {
+        status = tb_chol_set_schedule( h, sched[s] );
+        for( int rep = 0; rep < 3 && status == TB_OK; ++rep )       // the first run captures the graph
+        {
+            cudaEventRecord( e0, st );
+            status = run_factor( h, h->last_reg );
+            cudaEventRecord( e1, st );
+            if( rep > 0 ) { t[s] = std::min( t[s], elapsed() ); }
+        }
+    }
+    const std::int32_t k = std::max( 1, nrhs );
+    if( status == TB_OK )
+    {
+        status = tb_chol_set_schedule( h, t[1] < t[0] ? sched[1] : sched[0] );
+    }
+    if( status == TB_OK )
+    {
+        // one solve's sweeps on zero right-hand sides (the work does not depend on the values)
+        const std::int64_t nk = static_cast<std::int64_t>( h->n ) * k;
+        status = h->ir_x.reserve( 2 * nk );
+        if( status == TB_OK ) { cudaMemsetAsync( h->ir_x.ptr, 0, sizeof(double) * static_cast<size_t>( nk ), st ); }
+        for( int s = 0; s < 2 && status == TB_OK; ++s )
+        {
+            status = tb_chol_set_solve_schedule( h, sched[s] );
+            for( int rep = 0; rep < 3 && status == TB_OK; ++rep )
+            {
+                cudaEventRecord( e0, st );
+                status = run_solve_core( h, 2, 1.0, h->ir_x.ptr, k, 0.0, h->ir_x.ptr + nk, k, k );
+                cudaEventRecord( e1, st );
+                if( rep > 0 && status == TB_OK ) { t[2 + s] = std::min( t[2 + s], elapsed() ); }
+            }
+        }
+        if( status == TB_OK ) { status = tb_chol_set_solve_schedule( h, t[3] < t[2] ? sched[1] : sched[0] ); }
+    }
+    cudaEventDestroy( e0 );
+    cudaEventDestroy( e1 );
+    if( status != TB_OK ) { return status; }
+    if( choice ) { choice[0] = t[1] < t[0] ? sched[1] : sched[0]; choice[1] = t[3] < t[2] ? sched[1] : sched[0]; }
+    if( times_ms ) { for( int i = 0; i < 4; ++i ) { times_ms[i] = t[i]; } }
     return TB_OK;
 }
 

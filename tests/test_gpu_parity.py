@@ -306,6 +306,26 @@ def test_solve_task_graph_without_device_allocation():
     assert rel_err(X.cpu().numpy(), X_lv.cpu().numpy()) < 1e-12
 
 
+def test_autotune_keeps_the_factor_and_the_solution():
+    A = M.grid_laplacian_3d(20, 16, 1e-3)
+    perm = O.nested_dissection(A, 32)
+    c = CholeskyDecomposition(A.outer, A.inner, perm)
+    assert c.NumericFactorization(A.values) == 0
+    tri0, rec0 = c.FactorValues()
+    B = np.random.default_rng(16).standard_normal((A.n, 4))
+    X0 = c.Solve(B)
+    r = c.Autotune(4)
+    assert r["factor"] in ("levels", "task_graph") and r["solve"] in ("levels", "task_graph")
+    assert all(np.isfinite(v) and v > 0 for v in r["times_ms"].values()), r
+    # the chosen factor schedule is kept: refactoring gives the same factor, bit for bit
+    tri, rec = c.FactorValues()
+    assert np.array_equal(tri, tri0) and np.array_equal(rec, rec0)
+    assert c.NumericFactorization(A.values) == 0
+    tri, rec = c.FactorValues()
+    assert np.array_equal(tri, tri0) and np.array_equal(rec, rec0)
+    assert rel_err(c.Solve(B), X0) < 1e-12
+
+
 def test_graph_and_direct_launches_agree_bitwise():
     A = M.grid_laplacian_3d(10, 11, 1e-3)
     perm = O.nested_dissection(A, 16)
