@@ -117,3 +117,23 @@ def test_relaxed_fronts_cover_supernodes_and_reduce_levels():
     assert st["fronts"] < st["supernodes"]
     assert st["levels"] < 40
     c.CheckPlan()
+
+
+@pytest.mark.parametrize("grid,leaf", [(12, 8), (20, 32), (16, 64)])
+def test_solve_task_graph_plan_is_deadlock_free(grid, leaf):
+    # host side of the persistent solve: for every solve schedule the plan
+    # check verifies the task lists (every update of a panel comes before the
+    # panel's first forward task; every task of a target panel before the back
+    # task that reads it) and the flop invariant of the deferred updates
+    A = M.grid_laplacian_3d(grid, 17, 1e-3)
+    c = CholeskyDecomposition(A.outer, A.inner, O.nested_dissection(A, leaf))
+    c.SymbolicFactorization()
+    c.CheckPlan()
+    assert c.PlanStats()["solve_graph_tasks"] == 0            # level launches by default
+    tasks = {}
+    for sched in ("task_graph_all", "task_graph", "levels"):
+        c.SetSolveSchedule(sched)
+        c.CheckPlan()
+        tasks[sched] = c.PlanStats()["solve_graph_tasks"]
+    assert tasks["levels"] == 0
+    assert tasks["task_graph_all"] > 0 and tasks["task_graph_all"] >= tasks["task_graph"]
