@@ -7,6 +7,8 @@
 
 #include <algorithm>
 #include <map>
+#include <set>
+#include <utility>
 
 namespace tb
 {
@@ -37,24 +39,24 @@ void push_tiles( std::vector<GemmTask> & out, I64 a, I32 lda, I64 b, I32 ldb, I6
     }
 }
 
-// First-fit allocator over [0, capacity) with coalescing free list; grows
-// the capacity when nothing fits.
+// Best-fit allocator over [0, capacity) with a coalescing free list; grows
+// the capacity when nothing fits.  Free blocks are indexed both by address
+// (for coalescing) and by (size, address) (for the O(log n) best-fit lookup),
+// so a merged plan over thousands of small fronts stays linear-logarithmic.
 class RegionAllocator
 {
 public:
     I64 allocate( I64 size )
     {
         if( size <= 0 ) { return 0; }
-        for( auto it = free_.begin(); it != free_.end(); ++it )
+        auto fit = by_size_.lower_bound( { size, I64(-1) } );
+        if( fit != by_size_.end() )
         {
-            if( it->second >= size )
-            {
-                const I64 off = it->first;
-                const I64 rest = it->second - size;
-                free_.erase( it );
-                if( rest > 0 ) { free_[off + size] = rest; }
-                return off;
-            }
+            const I64 off = fit->second;
+            const I64 rest = fit->first - size;
+            erase_block( off );
+            if( rest > 0 ) { insert_block( off + size, rest ); }
+            return off;
         }
         // extend: reuse a free block that ends at the top
         if( !free_.empty() )
@@ -63,7 +65,7 @@ public:
             if( last->first + last->second == top_ )
             {
                 const I64 off = last->first;
-                free_.erase( last );
+                erase_block( off );
                 top_ = off + size;
                 return off;
             }
@@ -75,28 +77,42 @@ public:
     void release( I64 off, I64 size )
     {
         if( size <= 0 ) { return; }
-        auto it = free_.emplace( off, size ).first;
-        if( it != free_.begin() )
+        auto next = free_.lower_bound( off );
+        if( next != free_.begin() )
         {
-            auto prev = std::prev( it );
-            if( prev->first + prev->second == it->first )
+            auto prev = std::prev( next );
+            if( prev->first + prev->second == off )
             {
-                prev->second += it->second;
-                free_.erase( it );
-                it = prev;
+                off = prev->first;
+                size += prev->second;
+                erase_block( off );
             }
         }
-        auto next = std::next( it );
-        if( next != free_.end() && it->first + it->second == next->first )
+        next = free_.lower_bound( off + size );
+        if( next != free_.end() && next->first == off + size )
         {
-            it->second += next->second;
-            free_.erase( next );
+            size += next->second;
+            erase_block( next->first );
         }
+        insert_block( off, size );
     }
     I64 capacity() const { return top_; }
 
 private:
-    std::map<I64,I64> free_;
+    void insert_block( I64 off, I64 size )
+    {
+        free_.emplace( off, size );
+        by_size_.emplace( size, off );
+    }
+    void erase_block( I64 off )
+    {
+        auto it = free_.find( off );
+        by_size_.erase( { it->second, off } );
+        free_.erase( it );
+    }
+
+    std::map<I64,I64> free_;              // address -> size
+    std::set<std::pair<I64,I64>> by_size_; // (size, address)
     I64 top_ = 0;
 };
 
