@@ -19,7 +19,7 @@
 //    rows for vector and bulk copies), and an update-matrix region in which each front's
 //    n1 x n1 contribution block V (Multifrontal.hpp:165) lives from its
 //    front's level until its parent's level; V regions are reused across
-//    levels by a first-fit allocator and zeroed by the level that owns them;
+//    levels by a best-fit allocator and zeroed by the level that owns them;
 //  * fronts are grouped in levels by height in the front tree (leaves are
 //    level 0); a level runs after all lower levels;
 //  * within a level, children's update matrices are added into their parents

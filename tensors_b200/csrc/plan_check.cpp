@@ -11,7 +11,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <string>
+#include <vector>
 
 namespace tb
 {
@@ -120,6 +122,47 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         {
             return "GEMM tiles do not apply every panel update exactly once (flops " + std::to_string( pl.gemm_flops )
                    + ", expected " + std::to_string( expect ) + ")";
+        }
+    }
+    {
+        // update matrices: each lies in the update region, and two whose
+        // lifetimes (the front's level to its parent's level, both inclusive)
+        // intersect never share an entry
+        const I32 F = pl.front_count;
+        std::vector<std::vector<I32>> born( static_cast<size_t>( pl.levels ) ), dies( static_cast<size_t>( pl.levels ) );
+        for( I32 f = 0; f < F; ++f )
+        {
+            const size_t fs = static_cast<size_t>( f );
+            const I64 size = static_cast<I64>( pl.front_n1[fs] ) * pl.front_ld1[fs];
+            if( size == 0 ) { continue; }
+            if( pl.front_v[fs] < pl.u0_size + pl.u1_size || !in_range( pl.front_v[fs], pl.front_v[fs] + size - 1, arena ) )
+            {
+                return "update matrix outside the update region (front " + std::to_string( f ) + ")";
+            }
+            const I32 p = pl.front_parent[fs];
+            const I32 last = p < F ? pl.level_of[static_cast<size_t>( p )] : pl.level_of[fs];
+            if( pl.level_of[fs] < 0 || last < pl.level_of[fs] || last >= pl.levels ) { return "update matrix lifetime invalid (front " + std::to_string( f ) + ")"; }
+            born[static_cast<size_t>( pl.level_of[fs] )].push_back( f );
+            dies[static_cast<size_t>( last )].push_back( f );
+        }
+        std::map<I64,I32> live;   // offset -> front
+        for( I32 h = 0; h < pl.levels; ++h )
+        {
+            for( I32 f : born[static_cast<size_t>( h )] )
+            {
+                const I64 off = pl.front_v[static_cast<size_t>( f )];
+                const I64 end = off + static_cast<I64>( pl.front_n1[static_cast<size_t>( f )] ) * pl.front_ld1[static_cast<size_t>( f )];
+                auto next = live.lower_bound( off );
+                bool clash = next != live.end() && next->first < end;
+                if( next != live.begin() )
+                {
+                    const I32 g = std::prev( next )->second;
+                    clash = clash || pl.front_v[static_cast<size_t>( g )] + static_cast<I64>( pl.front_n1[static_cast<size_t>( g )] ) * pl.front_ld1[static_cast<size_t>( g )] > off;
+                }
+                if( clash ) { return "live update matrices overlap (front " + std::to_string( f ) + ", level " + std::to_string( h ) + ")"; }
+                live.emplace( off, f );
+            }
+            for( I32 f : dies[static_cast<size_t>( h )] ) { live.erase( pl.front_v[static_cast<size_t>( f )] ); }
         }
     }
     for( size_t k = 0; k < pl.gemm.size(); ++k )
