@@ -45,7 +45,9 @@ enum tb_status {
     TB_ERR_OUT_OF_MEMORY       = -7,
     TB_ERR_NO_DEVICE           = -8,
     TB_ERR_TIMEOUT             = -9,
-    TB_ERR_NOT_CONVERGED       = -10
+    TB_ERR_NOT_CONVERGED       = -10,
+    TB_ERR_IO                  = -11,
+    TB_ERR_FORMAT              = -12
 };
 
 /* Supernode strategies (CholeskyDecomposition.hpp:119-124). */
@@ -335,6 +337,32 @@ int tb_server_wait( tb_server * s, int64_t request_id, int32_t * status, double 
                     int32_t * iterations, double * relres );
 int tb_server_stats( tb_server * s, int64_t * resident_bytes, int64_t * peak_resident_bytes, int64_t * evictions,
                      int64_t * refactors );
+
+/* ------------------------------------------------------------------------
+ * MatrixMarket files (host only, no device needed).
+ *
+ * tb_matrix_market_read replaces MatrixCSR::LoadFromMatrixMarket
+ * (src/Sparse/MatrixCSR/MatrixMarket.hpp:3-202) with the triple assembly it
+ * calls (MatrixCSR::FromTriples, src/Sparse/MatrixCSR/FromTriples.hpp:4-209,
+ * compressed and symmetrized): a coordinate file with field real, integer
+ * or pattern (entries 1) and symmetry general or symmetric (the stored
+ * triangle is mirrored, the diagonal kept once) becomes CSR with sorted
+ * columns and repeated (i, j) entries summed in file order.  The arrays are
+ * allocated by the library (rows + 1 int64 row pointers, nnz int32 columns,
+ * nnz doubles) and released with tb_matrix_market_free.  thread_count <= 0:
+ * all host threads.  TB_ERR_IO: unreadable file; TB_ERR_FORMAT: not a
+ * supported MatrixMarket file (complex, skew-symmetric, hermitian and array
+ * files included, as in the reference), an index outside the stated size,
+ * or an entry count other than the size line's.
+ *
+ * tb_matrix_market_write replaces MatrixCSR::WriteToMatrixMarket
+ * (MatrixMarket.hpp:205-306): "real general", one "%d %d %.17E" line per
+ * stored entry in CSR order (a written file reads back bit-exact). */
+int tb_matrix_market_read( const char * path, int32_t thread_count, int32_t * rows, int32_t * cols,
+                           int64_t ** outer, int32_t ** inner, double ** values );
+int tb_matrix_market_free( void * p );
+int tb_matrix_market_write( const char * path, int32_t rows, int32_t cols, const int64_t * outer,
+                            const int32_t * inner, const double * values );
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,11 @@ def _load_ref():
     lib.tb_ref_log_det.restype = _d
     lib.tb_ref_set_quiet.argtypes = [_i]
     lib.tb_ref_set_blas_threads.argtypes = [_i]
+    lib.tb_ref_mm_load.restype = _vp
+    lib.tb_ref_mm_load.argtypes = [ctypes.c_char_p, _i]
+    lib.tb_ref_mm_sizes.argtypes = [_vp, _vp, _vp, _vp]
+    lib.tb_ref_mm_copy.argtypes = [_vp, _vp, _vp, _vp]
+    lib.tb_ref_mm_free.argtypes = [_vp]
     lib.tb_ref_set_quiet(1)
     return lib
 
@@ -245,3 +250,65 @@ class RefCholesky(_Base):
         X = np.zeros_like(B) if X is None else X
         self.lib.tb_ref_lower_solve(self.h, alpha, B.ctypes.data, k, beta, X.ctypes.data, k, k)
         return X
+
+
+# ---------------------------------------------------------------- MatrixMarket
+
+def ref_mm_read(path, threads: int = 1):
+    """The reference's Sparse::MatrixCSR::LoadFromMatrixMarket (MatrixCSR/MatrixMarket.hpp:3-202):
+    (rows, cols, outer, inner, values); a file it rejects gives a 0 x 0 matrix."""
+    lib = ref_lib()
+    h = lib.tb_ref_mm_load(os.fsencode(path), int(threads))
+    try:
+        rows, cols, nnz = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        lib.tb_ref_mm_sizes(h, ctypes.byref(rows), ctypes.byref(cols), ctypes.byref(nnz))
+        m = max(rows.value, 0)
+        outer = np.zeros(m + 1, dtype=np.int64)
+        inner = np.zeros(max(nnz.value, 1), dtype=np.int32)
+        values = np.zeros(max(nnz.value, 1), dtype=np.float64)
+        lib.tb_ref_mm_copy(h, _ptr(outer), _ptr(inner), _ptr(values))
+    finally:
+        lib.tb_ref_mm_free(h)
+    return rows.value, cols.value, outer, inner[:nnz.value], values[:nnz.value]
+
+
+def mm_read_port(path):
+    """Pure-Python restatement of the same reader for small files: banner and comment
+    handling of MatrixMarket.hpp:19-138, triples of :146-174, and FromTriples
+    (MatrixCSR/FromTriples.hpp:96-190): off-diagonal entries of a symmetric file
+    mirrored, each row's entries in file order, stably sorted by column, repeated
+    columns summed in that order.  Returns None for a file the reference rejects."""
+    with open(path) as f:
+        head = f.readline().split()
+        words = [w.lower() for w in head]
+        if len(words) < 5 or words[0] != "%%matrixmarket" or words[1] != "matrix" or words[2] != "coordinate":
+            return None
+        field, symmetry = words[3], words[4]
+        if field == "complex" or symmetry not in ("general", "symmetric"):
+            return None
+        line = f.readline()
+        while line and line.startswith("%"):
+            line = f.readline()
+        m, n, nnz = (int(t) for t in line.split()[:3])
+        tokens = f.read().split()
+    per = 2 if field == "pattern" else 3
+    rows = [[] for _ in range(m)]
+    for k in range(nnz):
+        i = int(tokens[per * k]) - 1
+        j = int(tokens[per * k + 1]) - 1
+        a = 1.0 if per == 2 else float(tokens[per * k + 2])
+        rows[i].append((j, a))
+        if symmetry == "symmetric" and i != j:
+            rows[j].append((i, a))
+    outer, inner, values = [0], [], []
+    for r in rows:
+        r = sorted(r, key=lambda e: e[0])          # stable
+        for j, a in r:
+            if inner and len(inner) > outer[-1] and inner[-1] == j:
+                values[-1] += a
+            else:
+                inner.append(j)
+                values.append(a)
+        outer.append(len(inner))
+    return (m, n, np.asarray(outer, dtype=np.int64), np.asarray(inner, dtype=np.int32),
+            np.asarray(values, dtype=np.float64))

@@ -47,8 +47,10 @@ namespace Tensors
 #include "src/LAPACK_Wrappers.hpp"
 
 #include "src/Sorting/TwoArraySort.hpp"
+#include "src/Sorting/ThreeArraySort.hpp"
 #include "src/Aggregator.hpp"
 #include "src/PairAggregator.hpp"
+#include "src/TripleAggregator.hpp"
 #include "src/AssemblyCounters.hpp"
 #include "src/Sparse/Permutation.hpp"
 namespace Tensors {
@@ -59,10 +61,8 @@ namespace Tensors {
 #include "src/Sparse/PatternCSR.hpp"
 #include "src/Sparse/BinaryMatrixCSR.hpp"
 
-namespace Tensors { namespace Sparse {
-    // GetU() names this type in its declaration; it is never instantiated here.
-    template<typename Scal_, IntQ Int_, IntQ LInt_, Parallel_T parQ_> class MatrixCSR;
-} }
+// MatrixCSR carries the MatrixMarket reader and writer (MatrixCSR/MatrixMarket.hpp).
+#include "src/Sparse/MatrixCSR.hpp"
 
 #include "Sparse.hpp"
 
@@ -76,6 +76,7 @@ namespace
     using Int  = std::int32_t;
     using LInt = std::int64_t;
     using Chol = Sparse::CholeskyDecomposition<double, Int, LInt, Parallel>;
+    using Mat  = Sparse::MatrixCSR<double, Int, LInt, Parallel>;
 
     struct RefHandle
     {
@@ -236,5 +237,33 @@ void tb_ref_lower_solve( void * p, double alpha, const double * B, int ldB,
 double tb_ref_log_det( void * p ) { return static_cast<RefHandle*>(p)->chol->LogDeterminant(); }
 
 void tb_ref_factor_diagonal( void * p, double * diag ) { static_cast<RefHandle*>(p)->chol->WriteFactorDiagonal( diag ); }
+
+// MatrixMarket files through Sparse::MatrixCSR::LoadFromMatrixMarket
+// (MatrixCSR/MatrixMarket.hpp:3-202).  A file the reference rejects leaves the
+// matrix empty (0 x 0).  Its WriteToMatrixMarket is not bound: its merge step
+// (MatrixMarket.hpp:296-305) appends thread_strings[2 * thread + 2] for
+// thread 1, one past its four slices, and never writes slices 1 and 3.
+void * tb_ref_mm_load( const char * path, int threads )
+{
+    auto * A = new Mat();
+    A->LoadFromMatrixMarket( std::filesystem::path( path ), Int( threads < 1 ? 1 : threads ) );
+    return A;
+}
+
+void tb_ref_mm_sizes( void * p, std::int32_t * rows, std::int32_t * cols, std::int64_t * nnz )
+{
+    auto & A = *static_cast<Mat*>(p);
+    *rows = A.RowCount(); *cols = A.ColCount(); *nnz = A.NonzeroCount();
+}
+
+void tb_ref_mm_copy( void * p, std::int64_t * outer, std::int32_t * inner, double * values )
+{
+    auto & A = *static_cast<Mat*>(p);
+    if( A.RowCount() <= 0 ) { return; }
+    for( Int i = 0; i <= A.RowCount(); ++i ) { outer[i] = A.Outer()[i]; }
+    for( LInt k = 0; k < A.NonzeroCount(); ++k ) { inner[k] = A.Inner()[k]; values[k] = A.Values()[k]; }
+}
+
+void tb_ref_mm_free( void * p ) { delete static_cast<Mat*>(p); }
 
 } // extern "C"

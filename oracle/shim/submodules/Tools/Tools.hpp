@@ -72,10 +72,11 @@ namespace Tools
     template<typename T> concept IntQ       = std::integral<T>;
     template<typename T> concept SignedIntQ = std::integral<T> && std::is_signed_v<T>;
     template<typename A, typename B> constexpr bool SameQ = std::is_same_v<A,B>;
+    template<typename T> constexpr bool ArithmeticQ = std::is_arithmetic_v<T>;
 
     enum Parallel_T : bool { Sequential = false, Parallel = true };
 
-    enum class Op     : int { Id = 0, Trans = 1, ConjTrans = 2, Conj = 3 };
+    enum class Op     : int { Id = 0, Trans = 1, ConjTrans = 2, Conj = 3, Re = 4, ReTrans = 5, Im = 6, ImTrans = 7 };
     enum class Layout : int { RowMajor = 0, ColMajor = 1 };
     enum class UpLo   : int { Upper = 0, Lower = 1 };
     enum class Side   : int { Left = 0, Right = 1 };
@@ -115,7 +116,27 @@ namespace Tools
 
         // How a coefficient in a linear combination is to be treated.
         enum class Flag : int { Zero = 0, Plus = 1, Minus = -1, Generic = 2 };
+
+        // An entry under an operation (MatrixCSR's transpose and real/imaginary parts).
+        template<::Tools::Op op, typename T> constexpr T Op( const T & x )
+        {
+            if constexpr ( op == ::Tools::Op::Conj || op == ::Tools::Op::ConjTrans )
+            {
+                if constexpr ( ComplexQ<T> ) { return std::conj(x); } else { return x; }
+            }
+            else if constexpr ( op == ::Tools::Op::Re || op == ::Tools::Op::ReTrans )
+            {
+                if constexpr ( ComplexQ<T> ) { return T(std::real(x)); } else { return x; }
+            }
+            else if constexpr ( op == ::Tools::Op::Im || op == ::Tools::Op::ImTrans )
+            {
+                if constexpr ( ComplexQ<T> ) { return T(std::imag(x)); } else { return T(0); }
+            }
+            else { return x; }
+        }
     }
+    using Complex32 = std::complex<float>;
+    using Complex64 = std::complex<double>;
 
     template<typename T> inline T Max( const T a, const T b ) { return a < b ? b : a; }
     template<typename T> inline T Min( const T a, const T b ) { return a < b ? a : b; }
@@ -198,6 +219,7 @@ namespace Tools
 
 #define TOOLS_DUMP(x)
 #define TOOLS_LOGDUMP(x)
+#define TOOLS_DDUMP(x)
 #define TOOLS_PDUMP(x)
 #define TOOLS_PTIMER(timer, tag)
 #define TOOLS_PTIC(tag)

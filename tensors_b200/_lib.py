@@ -87,6 +87,10 @@ SIGNATURES = {
     "tb_server_submit": (ctypes.c_int, [_vp, _i64, _vp, _d, _vp, _vp, _i32, _d, _pi64]),
     "tb_server_wait": (ctypes.c_int, [_vp, _i64, _pi32, _pd, _pd, _pi32, _pd]),
     "tb_server_stats": (ctypes.c_int, [_vp, _pi64, _pi64, _pi64, _pi64]),
+    "tb_matrix_market_read": (ctypes.c_int, [ctypes.c_char_p, _i32, _pi32, _pi32, ctypes.POINTER(_pi64),
+                                             ctypes.POINTER(_pi32), ctypes.POINTER(_pd)]),
+    "tb_matrix_market_free": (ctypes.c_int, [_vp]),
+    "tb_matrix_market_write": (ctypes.c_int, [ctypes.c_char_p, _i32, _i32, _vp, _vp, _vp]),
 }
 
 _LIB = None

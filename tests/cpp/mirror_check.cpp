@@ -4,17 +4,32 @@
 // fill-reducing permutation, symbolic phase, and with "numeric" as second
 // argument a factorization and a 3-RHS solve whose relative residual is
 // printed.  Output: "sn_count <S>" [ "status <0|1>" "relres <r>" ].
+// "mm <in> <out>": MatrixCSR::LoadFromMatrixMarket of <in>, a Cholesky
+// symbolic phase on its pattern, WriteToMatrixMarket to <out>; prints
+// "rows <m> nnz <k> sn_count <S>".
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
 
 #include "tensors_b200/CholeskyDecomposition.hpp"
+#include "tensors_b200/MatrixCSR.hpp"
 
 using tensors_b200::Sparse::CholeskyDecomposition;
+using tensors_b200::Sparse::MatrixCSR;
 
 int main( int argc, char ** argv )
 {
+    if( argc > 3 && std::string( argv[1] ) == "mm" )
+    {
+        MatrixCSR A;
+        A.LoadFromMatrixMarket( argv[2], 4 );
+        CholeskyDecomposition S( A.Outer().data(), A.Inner().data(), A.RowCount(), 1 );
+        S.SymbolicFactorization();
+        A.WriteToMatrixMarket( argv[3] );
+        std::printf( "rows %d nnz %lld sn_count %d\n", A.RowCount(), static_cast<long long>( A.NonzeroCount() ), S.SN_Count() );
+        return 0;
+    }
     const int g = argc > 1 ? std::atoi( argv[1] ) : 20;
     const bool numeric = argc > 2 && std::string( argv[2] ) == "numeric";
     const int n = g * g;

@@ -55,3 +55,20 @@ def test_cpp_mirror_factor_and_solve(mirror_exe):
     vals = dict(line.split() for line in out.strip().splitlines())
     assert int(vals["status"]) == 0
     assert float(vals["relres"]) < 1e-13
+
+
+def test_cpp_mirror_matrix_market(mirror_exe, tmp_path):
+    from tensors_b200 import matrices as M
+    from tensors_b200.matrix_market import read_matrix_market, write_matrix_market
+
+    A = M.grid_laplacian_2d(13, 0.5)
+    src, dst = tmp_path / "a.mtx", tmp_path / "b.mtx"
+    write_matrix_market(src, A)
+    out = subprocess.run([mirror_exe, "mm", str(src), str(dst)], check=True, capture_output=True, text=True).stdout.split()
+    assert int(out[1]) == A.n and int(out[3]) == A.nnz
+    c = CholeskyDecomposition(A.outer, A.inner)
+    c.SymbolicFactorization()
+    assert int(out[5]) == c.SN_Count()
+    assert dst.read_text() == src.read_text()
+    m, n, outer, inner, values = read_matrix_market(dst)
+    assert np.array_equal(outer, A.outer) and np.array_equal(inner, A.inner) and np.array_equal(values, A.values)
