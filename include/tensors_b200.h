@@ -280,6 +280,24 @@ int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B,
  * entries): info[4i..4i+3] = sweep (0 forward, 1 back), level, panel step,
  * task count and ms[i] its duration.  Returns the count. */
 int tb_chol_solve_profile( tb_chol * h, int64_t * info, double * ms, int32_t cap );
+/* Conjugate gradients preconditioned by the factor: the reference's
+ * ConjugateGradient::operator() (ConjugateGradient.hpp:109-356) with the
+ * operator X -> (A' + reg I) X and the preconditioner P = the handle's factor
+ * (any precision).  A' has the handle's pattern and the given values (caller
+ * CSR order; NULL: the values of the last factorization), so a factor can
+ * precondition a nearby matrix.  X = alpha x + beta X, with x the iterate,
+ * started from 0 or, with use_initial_guess, from X.  Stops when every column
+ * meets |r.P r| <= rel_tol^2 |b.P b| (the reference's CheckResiduals,
+ * :470-480) or after max_iter steps; iterations and, when non-NULL,
+ * relres[nrhs] = sqrt(|r.P r| / |b.P b|) report the end state.
+ * TB_ERR_NOT_CONVERGED (X still written) when a column misses the tolerance.
+ * _device: device pointers on the handle's stream. */
+int tb_chol_cg( tb_chol * h, const double * values, double reg, double alpha, const double * B, int32_t ldB,
+                double beta, double * X, int32_t ldX, int32_t nrhs, double rel_tol, int32_t max_iter,
+                int32_t use_initial_guess, int32_t * iterations, double * relres );
+int tb_chol_cg_device( tb_chol * h, const double * values, double reg, double alpha, const double * B, int32_t ldB,
+                       double beta, double * X, int32_t ldX, int32_t nrhs, double rel_tol, int32_t max_iter,
+                       int32_t use_initial_guess, int32_t * iterations, double * relres );
 /* Number of kernel launches the last numeric factorization / solve issued. */
 int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * solve_launches );
 

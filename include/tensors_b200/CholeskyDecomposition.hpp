@@ -144,6 +144,25 @@ public:
         Check( tb_chol_lower_solve( h_, alpha, B, ldB, beta, X_out, ldX, nrhs ) );
     }
 
+    // Conjugate gradients on (A' + reg I) X = B preconditioned by this factor,
+    // the reference's ConjugateGradient::operator() (ConjugateGradient.hpp:109)
+    // with P = this factor's solve: X_out = alpha x + beta X_out.  A_val: A' in
+    // the caller's CSR order (nullptr: the factored values).  Returns whether
+    // every column met the relative tolerance; IterationCount() tells the steps.
+    bool ConjugateGradient( const Scal * A_val, Scal reg, Scal alpha, const Scal * B, Int ldB, Scal beta,
+                            Scal * X_out, Int ldX, Int nrhs, Scal relative_tolerance, Int max_iter,
+                            bool use_initial_guess = false )
+    {
+        relres_.assign( static_cast<size_t>( nrhs < 1 ? 1 : nrhs ), 0.0 );
+        const int st = tb_chol_cg( h_, A_val, reg, alpha, B, ldB, beta, X_out, ldX, nrhs, relative_tolerance, max_iter,
+                                   use_initial_guess ? 1 : 0, &cg_iter_, relres_.data() );
+        if( st == TB_ERR_NOT_CONVERGED ) { return false; }
+        Check( st );
+        return true;
+    }
+    Int IterationCount() const { return cg_iter_; }
+    const std::vector<Scal> & RelativeResiduals() const { return relres_; }
+
     // Queries, CholeskyDecomposition/InputOutput.hpp:85-367 and Numeric.hpp:183-215.
     Int RowCount() const { Int v = 0; Check( tb_chol_row_count( h_, &v ) ); return v; }
     Int ColCount() const { return RowCount(); }
@@ -201,6 +220,8 @@ private:
     }
 
     tb_chol * h_ = nullptr;
+    Int cg_iter_ = 0;
+    std::vector<Scal> relres_;
 };
 
 } // namespace Sparse

@@ -57,6 +57,8 @@ SIGNATURES = {
     "tb_chol_set_graph": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_solve_profile": (ctypes.c_int, [_vp, _vp, _vp, _i32]),
     "tb_chol_launch_counts": (ctypes.c_int, [_vp, _pi64, _pi64]),
+    "tb_chol_cg": (ctypes.c_int, [_vp, _vp, _d, _d, _vp, _i32, _d, _vp, _i32, _i32, _d, _i32, _i32, _pi32, _vp]),
+    "tb_chol_cg_device": (ctypes.c_int, [_vp, _vp, _d, _d, _vp, _i32, _d, _vp, _i32, _i32, _d, _i32, _i32, _pi32, _vp]),
     "tb_chol_set_schedule": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_set_solve_schedule": (ctypes.c_int, [_vp, _i32]),
     "tb_chol_autotune": (ctypes.c_int, [_vp, _i32, _vp, _vp]),

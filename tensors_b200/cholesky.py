@@ -271,6 +271,57 @@ class CholeskyDecomposition:
         _check(lib().tb_chol_residual_device(self._h, B.data_ptr(), X.data_ptr(), R.data_ptr(), k))
         return R
 
+    def ConjugateGradient(self, B, X=None, values=None, reg: float = 0.0, alpha: float = 1.0, beta: float = 0.0,
+                          relative_tolerance: float = 1e-10, max_iter: int = 100, use_initial_guess: bool = False):
+        """Conjugate gradients on (A' + reg I) X = B preconditioned by this factor, as the reference's
+        ``ConjugateGradient::operator()`` (ConjugateGradient.hpp:109-356) with P = the factor's solve.
+
+        ``values``: A' in the caller's CSR order (None: the values of the last factorization).
+        X = alpha x + beta X; with ``use_initial_guess`` the iteration starts from X.  Returns
+        ``(X, succeeded)``; ``IterationCount()`` and ``RelativeResiduals()`` report the end state
+        (per column sqrt(|r.P r| / |b.P b|)).  Host arrays or CUDA tensors (all of one kind)."""
+        cuda = _is_cuda_tensor(B)
+        k = 1 if B.ndim == 1 else B.shape[1]
+        rel = np.zeros(k, dtype=np.float64)
+        iters = ctypes.c_int32()
+        if cuda:
+            import torch
+
+            B = B.contiguous()
+            if X is None:
+                X = torch.zeros_like(B)
+                beta = 0.0
+            v = 0 if values is None else values.contiguous().data_ptr()
+            st = lib().tb_chol_cg_device(self._h, v, float(reg), float(alpha), B.data_ptr(), k, float(beta),
+                                         X.data_ptr(), k, k, float(relative_tolerance), int(max_iter),
+                                         int(bool(use_initial_guess)), ctypes.byref(iters), rel.ctypes.data)
+        else:
+            B = _f64(B)
+            if X is None:
+                X = np.zeros_like(B)
+                beta = 0.0
+            elif not (X.flags.c_contiguous and X.dtype == np.float64 and X.shape == B.shape):
+                raise TBError(-1, "ConjugateGradient: X must be a C-contiguous float64 array shaped like B")
+            v = None if values is None else _f64(values)
+            if v is not None and v.shape != (self.NonzeroCount(),):
+                raise TBError(-1, "ConjugateGradient: wrong number of values")
+            st = lib().tb_chol_cg(self._h, None if v is None else v.ctypes.data, float(reg), float(alpha), B.ctypes.data,
+                                  k, float(beta), X.ctypes.data, k, k, float(relative_tolerance), int(max_iter),
+                                  int(bool(use_initial_guess)), ctypes.byref(iters), rel.ctypes.data)
+        self._cg_iterations, self._cg_relres = iters.value, rel
+        if st == -10:
+            return X, False
+        _check(st)
+        return X, True
+
+    def IterationCount(self) -> int:
+        """Steps of the last ConjugateGradient call (ConjugateGradient.hpp:442)."""
+        return getattr(self, "_cg_iterations", 0)
+
+    def RelativeResiduals(self) -> np.ndarray:
+        """Per column sqrt(|r.P r| / |b.P b|) after the last ConjugateGradient call (ConjugateGradient.hpp:459)."""
+        return getattr(self, "_cg_relres", np.zeros(0))
+
     # ------------------------------------------------------------- getters
     def _array(self, name: str) -> np.ndarray:
         size = ctypes.c_int64()

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <climits>
 #include <limits>
 #include <map>
@@ -170,6 +171,7 @@ struct tb_chol
     std::int32_t ir_iters = 0;
     double ir_relres = 0.0;
     DeviceArray<double> ir_x, ir_r, ir_norms;
+    DeviceArray<double> cg_buf, cg_scal, cg_host;   // tb_chol_cg: vectors, per-column scalars, host-call copies
     DeviceArray<double> pivot_floor;             // mixed precision: static-pivot floor per row
     std::int32_t perturbed_pivots = 0;
     bool fell_back = false;                      // a mixed solve's refinement failed: refactored in FP64
@@ -1165,6 +1167,172 @@ int tb_chol_residual_device( tb_chol * h, const double * d_B, const double * d_X
     tb::launch_residual( h->n, h->a_outer.ptr, h->a_inner.ptr, h->values.ptr, d_X, d_B, d_R, std::max( 1, nrhs ), h->stream );
     TB_CUDA( cudaGetLastError() );
     return TB_OK;
+}
+
+// Preconditioned conjugate gradients with the factor as the preconditioner,
+// step for step the reference's ConjugateGradient::operator()
+// (ConjugateGradient.hpp:109-356): r = b (- A x0), z = P r, p = z,
+// rho = r.z; then u = A p, alpha = rho / p.u, x += alpha p, r -= alpha u,
+// z = P r, beta = rho_new / rho, p = z + beta p, until |rho_c| <= tol^2 |b_c.P b_c|
+// for every column (CheckResiduals, :470-480) or max_iter steps; then
+// X = alpha_out x + beta_out X.  One recurrence per column, scalars on the device.
+int tb_chol_cg_device( tb_chol * h, const double * d_values, double reg, double alpha, const double * d_B, std::int32_t ldB,
+                       double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs, double rel_tol, std::int32_t max_iter,
+                       std::int32_t use_initial_guess, std::int32_t * iterations, double * relres )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( d_B == nullptr || d_X == nullptr || ldB < k || ldX < k || max_iter < 0 || !(rel_tol >= 0.0) )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "ConjugateGradient: bad argument" );
+    }
+    cudaStream_t st = h->stream;
+    const std::int64_t nk = static_cast<std::int64_t>( n ) * k;
+    TB_TRY( h->cg_buf.reserve( 5 * nk ) );             // x, r, z, p, u
+    TB_TRY( h->cg_scal.reserve( 4 * k ) );             // b.Pb, rho, rho_old, p.u
+    TB_TRY( h->pin_norms.reserve( sizeof(double) * 2 * static_cast<size_t>( k ) ) );
+    double * x = h->cg_buf.ptr;
+    double * r = x + nk;
+    double * z = x + 2 * nk;
+    double * p = x + 3 * nk;
+    double * u = x + 4 * nk;
+    double * bsq = h->cg_scal.ptr;
+    double * rho = bsq + k;
+    double * rho_old = bsq + 2 * k;
+    double * pu = bsq + 3 * k;
+    double * hn = h->pin_norms.as<double>();
+    const double * vals = d_values != nullptr ? d_values : h->values.ptr;
+    auto dots = [&]( const double * a, const double * b, double * out ) -> int {
+        TB_CUDA( cudaMemsetAsync( out, 0, sizeof(double) * static_cast<size_t>( k ), st ) );
+        tb::launch_column_dots( a, k, b, k, n, k, out, st );
+        return TB_OK;
+    };
+    auto precondition = [&]( const double * in, double * out ) -> int {
+        return run_solve_core( h, 2, 1.0, in, k, 0.0, out, k, k );
+    };
+    // host copy of rho and b.Pb; true when every column meets its tolerance
+    std::vector<double> tol2( static_cast<size_t>( k ) );
+    auto converged = [&]( bool * done ) -> int {
+        TB_CUDA( cudaMemcpyAsync( hn, bsq, sizeof(double) * 2 * static_cast<size_t>( k ), cudaMemcpyDeviceToHost, st ) );
+        TB_CUDA( cudaStreamSynchronize( st ) );
+        TB_TRY( check_solve_error( h ) );
+        *done = true;
+        for( std::int32_t c = 0; c < k; ++c ) { *done = *done && std::abs( hn[k + c] ) <= tol2[static_cast<size_t>( c )]; }
+        return TB_OK;
+    };
+    std::int32_t iter = 0;
+    bool done = false;
+    if( alpha != 0.0 )
+    {
+        tb::launch_combine( n, k, 1.0, d_B, ldB, 0.0, r, k, st );              // r = b
+        TB_TRY( precondition( r, z ) );                                          // z = P b
+        TB_TRY( dots( r, z, bsq ) );
+        TB_CUDA( cudaMemcpyAsync( hn, bsq, sizeof(double) * static_cast<size_t>( k ), cudaMemcpyDeviceToHost, st ) );
+        TB_CUDA( cudaStreamSynchronize( st ) );
+        TB_TRY( check_solve_error( h ) );
+        double bmax = 0.0;
+        for( std::int32_t c = 0; c < k; ++c )
+        {
+            if( std::isnan( hn[c] ) ) { return fail( TB_ERR_INVALID_ARGUMENT, "ConjugateGradient: right-hand side contains NaNs" ); }
+            tol2[static_cast<size_t>( c )] = std::abs( hn[c] ) * rel_tol * rel_tol;
+            bmax = std::max( bmax, std::abs( hn[c] ) );
+        }
+        if( bmax > 0.0 )
+        {
+            if( use_initial_guess )
+            {
+                tb::launch_combine( n, k, 1.0, d_X, ldX, 0.0, x, k, st );      // x = x0
+                tb::launch_apply_shifted( n, h->a_outer.ptr, h->a_inner.ptr, vals, reg, x, k, r, k, u, k, k, st );   // b - A x0
+                std::swap( r, u );                                               // r = b - A x0 (u is scratch)
+                TB_TRY( precondition( r, z ) );
+            }
+            else
+            {
+                TB_CUDA( cudaMemsetAsync( x, 0, sizeof(double) * static_cast<size_t>( nk ), st ) );
+            }
+            TB_CUDA( cudaMemcpyAsync( p, z, sizeof(double) * static_cast<size_t>( nk ), cudaMemcpyDeviceToDevice, st ) );
+            TB_TRY( dots( r, z, rho ) );
+            TB_TRY( converged( &done ) );
+            while( !done && iter < max_iter )
+            {
+                tb::launch_apply_shifted( n, h->a_outer.ptr, h->a_inner.ptr, vals, reg, p, k, nullptr, k, u, k, k, st );   // u = A p
+                TB_TRY( dots( p, u, pu ) );
+                tb::launch_cg_update_xr( n, k, rho, pu, p, u, x, r, st );       // x += alpha p, r -= alpha u
+                TB_TRY( precondition( r, z ) );                                  // z = P r
+                TB_CUDA( cudaMemcpyAsync( rho_old, rho, sizeof(double) * static_cast<size_t>( k ), cudaMemcpyDeviceToDevice, st ) );
+                TB_TRY( dots( r, z, rho ) );
+                tb::launch_cg_update_p( n, k, rho, rho_old, z, p, st );         // p = z + beta p
+                TB_TRY( converged( &done ) );
+                ++iter;
+            }
+            tb::launch_combine( n, k, alpha, x, k, beta, d_X, ldX, st );         // X = alpha x + beta X
+        }
+        else
+        {
+            done = true;                                                         // b = 0: X = beta X
+            tb::launch_combine( n, k, beta, d_X, ldX, 0.0, d_X, ldX, st );
+        }
+    }
+    else
+    {
+        done = true;                                                             // alpha = 0: X = beta X
+        tb::launch_combine( n, k, beta, d_X, ldX, 0.0, d_X, ldX, st );
+    }
+    TB_CUDA( cudaGetLastError() );
+    TB_CUDA( cudaStreamSynchronize( st ) );
+    if( iterations != nullptr ) { *iterations = iter; }
+    if( relres != nullptr )
+    {
+        for( std::int32_t c = 0; c < k; ++c )
+        {
+            const double b2 = std::abs( hn[c] );
+            relres[c] = alpha == 0.0 || b2 <= 0.0 ? 0.0 : std::sqrt( std::abs( hn[k + c] ) / b2 );
+        }
+    }
+    if( !done )
+    {
+        return fail( TB_ERR_NOT_CONVERGED, "ConjugateGradient: not converged after " + std::to_string( iter ) + " iterations" );
+    }
+    return TB_OK;
+}
+
+// Host-buffer form of tb_chol_cg_device: values (caller order, NULL = those
+// of the last factorization), B and X are copied through device scratch.
+int tb_chol_cg( tb_chol * h, const double * values, double reg, double alpha, const double * B, std::int32_t ldB,
+                double beta, double * X, std::int32_t ldX, std::int32_t nrhs, double rel_tol, std::int32_t max_iter,
+                std::int32_t use_initial_guess, std::int32_t * iterations, double * relres )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    const std::int32_t k = std::max( 1, nrhs );
+    if( B == nullptr || X == nullptr || ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "ConjugateGradient: bad argument" ); }
+    const std::int64_t nnz = h->outer[h->n];
+    const std::int64_t nk = static_cast<std::int64_t>( h->n ) * k;
+    cudaStream_t st = h->stream;
+    TB_TRY( h->cg_host.reserve( (values != nullptr ? nnz : 0) + 2 * nk ) );
+    double * dB = h->cg_host.ptr;
+    double * dX = dB + nk;
+    double * dv = values != nullptr ? dX + nk : nullptr;
+    TB_CUDA( cudaMemcpy2DAsync( dB, sizeof(double) * k, B, sizeof(double) * ldB, sizeof(double) * k, h->n, cudaMemcpyHostToDevice, st ) );
+    if( use_initial_guess || beta != 0.0 )
+    {
+        TB_CUDA( cudaMemcpy2DAsync( dX, sizeof(double) * k, X, sizeof(double) * ldX, sizeof(double) * k, h->n, cudaMemcpyHostToDevice, st ) );
+    }
+    else
+    {
+        TB_CUDA( cudaMemsetAsync( dX, 0, sizeof(double) * static_cast<size_t>( nk ), st ) );
+    }
+    if( dv != nullptr ) { TB_CUDA( cudaMemcpyAsync( dv, values, sizeof(double) * static_cast<size_t>( nnz ), cudaMemcpyHostToDevice, st ) ); }
+    const int status = tb_chol_cg_device( h, dv, reg, alpha, dB, k, beta, dX, k, nrhs, rel_tol, max_iter, use_initial_guess,
+                                          iterations, relres );
+    if( status < 0 && status != TB_ERR_NOT_CONVERGED ) { return status; }
+    const std::string msg = g_error;
+    TB_CUDA( cudaMemcpy2DAsync( X, sizeof(double) * ldX, dX, sizeof(double) * k, sizeof(double) * k, h->n, cudaMemcpyDeviceToHost, st ) );
+    TB_CUDA( cudaStreamSynchronize( st ) );
+    if( status != TB_OK ) { g_error = msg; }
+    return status;
 }
 
 int tb_chol_sn_count( tb_chol * h, std::int32_t * out )

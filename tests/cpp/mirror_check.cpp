@@ -77,5 +77,13 @@ int main( int argc, char ** argv )
         }
     }
     std::printf( "relres %.3e\n", std::sqrt( rn / bn ) );
+    // conjugate gradients on the unshifted matrix, preconditioned by the shifted factor
+    std::vector<double> val2( val );
+    for( int r = 0; r < n; ++r )
+    {
+        for( int64_t l = outer[r]; l < outer[r + 1]; ++l ) { if( inner[l] == r ) { val2[l] -= 5e-3; } }
+    }
+    const bool ok = S.ConjugateGradient( val2.data(), 0.0, 1.0, B.data(), nrhs, 0.0, X.data(), nrhs, nrhs, 1e-12, 200 );
+    std::printf( "cg_ok %d\ncg_iter %d\n", ok ? 1 : 0, S.IterationCount() );
     return 0;
 }

@@ -55,6 +55,7 @@ def test_cpp_mirror_factor_and_solve(mirror_exe):
     vals = dict(line.split() for line in out.strip().splitlines())
     assert int(vals["status"]) == 0
     assert float(vals["relres"]) < 1e-13
+    assert int(vals["cg_ok"]) == 1 and 1 <= int(vals["cg_iter"]) <= 200
 
 
 def test_cpp_mirror_matrix_market(mirror_exe, tmp_path):
