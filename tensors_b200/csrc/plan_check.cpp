@@ -56,25 +56,29 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         }
         if( !in_range( z.offset, z.offset + static_cast<I64>( z.row_end - 1 ) * z.ld + z.n - 1, arena ) ) { return "zero task out of range"; }
     }
+    std::vector<I32> lut_seen( pl.lut.size() + 1, 0 );
     for( size_t k = 0; k < pl.extend.size(); ++k )
     {
         const ExtendTask & t = pl.extend[k];
-        const std::string at = " (extend task " + std::to_string( k ) + ")";
-        if( t.m1 <= 0 || t.mid < 0 || t.mid > t.m1 ) { return "bad extend dimensions" + at; }
-        if( t.row_begin < 0 || t.row_end > t.m1 || t.row_begin >= t.row_end ) { return "bad extend rows" + at; }
-        if( t.ldw < t.m1 || t.ld0p < t.n0p || t.ld1p < t.n1p || t.ldvp < t.n1p ) { return "extend leading dimension too small" + at; }
-        if( !in_range( t.w, t.w + static_cast<I64>(t.m1) * t.ldw - 1, arena ) ) { return "extend source out of range" + at; }
-        if( t.lut < 0 || t.lut + t.m1 > static_cast<I64>( pl.lut.size() ) ) { return "extend lut out of range" + at; }
+        auto at = [&]() { return " (extend task " + std::to_string( k ) + ")"; };   // built only on failure
+        if( t.m1 <= 0 || t.mid < 0 || t.mid > t.m1 ) { return "bad extend dimensions" + at(); }
+        if( t.row_begin < 0 || t.row_end > t.m1 || t.row_begin >= t.row_end ) { return "bad extend rows" + at(); }
+        if( t.ldw < t.m1 || t.ld0p < t.n0p || t.ld1p < t.n1p || t.ldvp < t.n1p ) { return "extend leading dimension too small" + at(); }
+        if( !in_range( t.w, t.w + static_cast<I64>(t.m1) * t.ldw - 1, arena ) ) { return "extend source out of range" + at(); }
+        if( t.lut < 0 || t.lut + t.m1 > static_cast<I64>( pl.lut.size() ) ) { return "extend lut out of range" + at(); }
         const I64 u0n = static_cast<I64>(t.n0p) * t.ld0p, u1n = static_cast<I64>(t.n0p) * t.ld1p, vn = static_cast<I64>(t.n1p) * t.ldvp;
-        if( u0n > 0 && !in_range( t.u0, t.u0 + u0n - 1, arena ) ) { return "extend U0 out of range" + at; }
-        if( u1n > 0 && !in_range( t.u1, t.u1 + u1n - 1, arena ) ) { return "extend U1 out of range" + at; }
-        if( t.mid < t.m1 && (vn == 0 || !in_range( t.v, t.v + vn - 1, arena )) ) { return "extend V out of range" + at; }
+        if( u0n > 0 && !in_range( t.u0, t.u0 + u0n - 1, arena ) ) { return "extend U0 out of range" + at(); }
+        if( u1n > 0 && !in_range( t.u1, t.u1 + u1n - 1, arena ) ) { return "extend U1 out of range" + at(); }
+        if( t.mid < t.m1 && (vn == 0 || !in_range( t.v, t.v + vn - 1, arena )) ) { return "extend V out of range" + at(); }
+        // the row groups of one child share its lookup table: check it once
+        if( lut_seen[static_cast<size_t>( t.lut )] == t.m1 + 1 ) { continue; }
+        lut_seen[static_cast<size_t>( t.lut )] = t.m1 + 1;
         for( I32 i = 0; i < t.m1; ++i )
         {
             const I32 l = pl.lut[t.lut + i];
             const I32 lim = (i < t.mid) ? t.n0p : t.n1p;
-            if( l < 0 || l >= lim ) { return "extend lut value out of range" + at; }
-            if( i > 0 && i != t.mid && l <= pl.lut[t.lut + i - 1] ) { return "extend lut not increasing" + at; }
+            if( l < 0 || l >= lim ) { return "extend lut value out of range" + at(); }
+            if( i > 0 && i != t.mid && l <= pl.lut[t.lut + i - 1] ) { return "extend lut not increasing" + at(); }
         }
     }
     for( int which = 0; which < 2; ++which )
@@ -83,21 +87,21 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         for( size_t k = 0; k < list.size(); ++k )
         {
             const PanelTask & t = list[k];
-            const std::string at = std::string( which == 0 ? " (potrf task " : " (trsm task " ) + std::to_string( k ) + ")";
-            if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad panel dimensions" + at; }
-            if( t.ld0 < t.n0 || t.ld1 < t.n1 ) { return "panel leading dimension too small" + at; }
-            if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "panel U0 out of range" + at; }
-            if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.ld1 - 1, arena ) ) { return "panel U1 out of range" + at; }
+            auto at = [&]() { return std::string( which == 0 ? " (potrf task " : " (trsm task " ) + std::to_string( k ) + ")"; };   // built only on failure
+            if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad panel dimensions" + at(); }
+            if( t.ld0 < t.n0 || t.ld1 < t.n1 ) { return "panel leading dimension too small" + at(); }
+            if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "panel U0 out of range" + at(); }
+            if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.ld1 - 1, arena ) ) { return "panel U1 out of range" + at(); }
             const I32 nb = std::min( kPanel, t.n0 - t.r0 );
             const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
-            if( which == 1 && (t.c0 < 0 || t.c0 >= rest) ) { return "panel chunk out of range" + at; }
-            if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "panel rows out of range" + at; }
+            if( which == 1 && (t.c0 < 0 || t.c0 >= rest) ) { return "panel chunk out of range" + at(); }
+            if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "panel rows out of range" + at(); }
             // the inverse diagonal block: one per panel, written by the panel's potrf task
-            if( t.panel < 0 || t.panel >= static_cast<I32>( pl.sdiag.size() ) ) { return "panel index out of range" + at; }
-            if( which == 0 && t.panel != static_cast<I32>( k ) ) { return "potrf task is not its panel's" + at; }
+            if( t.panel < 0 || t.panel >= static_cast<I32>( pl.sdiag.size() ) ) { return "panel index out of range" + at(); }
+            if( which == 0 && t.panel != static_cast<I32>( k ) ) { return "potrf task is not its panel's" + at(); }
             if( which == 1 && (pl.potrf[static_cast<size_t>( t.panel )].r0 != t.r0 || pl.potrf[static_cast<size_t>( t.panel )].u0 != t.u0) )
             {
-                return "trsm task names another panel" + at;
+                return "trsm task names another panel" + at();
             }
         }
     }
@@ -168,14 +172,14 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
     for( size_t k = 0; k < pl.gemm.size(); ++k )
     {
         const GemmTask & t = pl.gemm[k];
-        const std::string at = " (gemm task " + std::to_string( k ) + ")";
-        if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad gemm dimensions" + at; }
-        if( t.M > t.lda || t.N > t.ldb || t.N > t.ldc ) { return "gemm leading dimension too small" + at; }
+        auto at = [&]() { return " (gemm task " + std::to_string( k ) + ")"; };   // built only on failure
+        if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad gemm dimensions" + at(); }
+        if( t.M > t.lda || t.N > t.ldb || t.N > t.ldc ) { return "gemm leading dimension too small" + at(); }
         // 16-byte copies of FP64 (2 entries) and FP32 (4 entries) storage
-        if( (t.a | t.b | t.c) % 4 != 0 || (t.lda | t.ldb | t.ldc) % 4 != 0 ) { return "gemm operand not 16-byte aligned" + at; }
-        if( !in_range( t.a, t.a + static_cast<I64>(t.K - 1) * t.lda + t.M - 1, arena ) ) { return "gemm A out of range" + at; }
-        if( !in_range( t.b, t.b + static_cast<I64>(t.K - 1) * t.ldb + t.N - 1, arena ) ) { return "gemm B out of range" + at; }
-        if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at; }
+        if( (t.a | t.b | t.c) % 4 != 0 || (t.lda | t.ldb | t.ldc) % 4 != 0 ) { return "gemm operand not 16-byte aligned" + at(); }
+        if( !in_range( t.a, t.a + static_cast<I64>(t.K - 1) * t.lda + t.M - 1, arena ) ) { return "gemm A out of range" + at(); }
+        if( !in_range( t.b, t.b + static_cast<I64>(t.K - 1) * t.ldb + t.N - 1, arena ) ) { return "gemm B out of range" + at(); }
+        if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at(); }
     }
     for( size_t k = 0; k < pl.sdiag.size(); ++k )
     {
@@ -187,41 +191,41 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
     for( size_t k = 0; k < pl.srest.size(); ++k )
     {
         const SolveRestTask & t = pl.srest[k];
-        const std::string at = " (solve-rest task " + std::to_string( k ) + ")";
-        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad solve-rest dimensions" + at; }
+        auto at = [&]() { return " (solve-rest task " + std::to_string( k ) + ")"; };   // built only on failure
+        if( t.n0 <= 0 || t.r0 < 0 || t.r0 >= t.n0 || t.n1 < 0 ) { return "bad solve-rest dimensions" + at(); }
         const I32 nb = std::min( kPanel, t.n0 - t.r0 );
         const I32 rest = (t.n0 - t.r0 - nb) + t.n1;
         const bool owner = t.c0 < 0;
         if( owner ? (t.c0 != -1 || t.c1 != 0 || rest != 0)
-                  : (t.c1 > rest || t.c0 >= t.c1 || t.c1 - t.c0 > kSolveRest) ) { return "solve-rest range out of bounds" + at; }
-        if( t.panel < 0 || static_cast<size_t>( t.panel ) >= pl.sdiag.size() ) { return "solve-rest panel out of range" + at; }
+                  : (t.c1 > rest || t.c0 >= t.c1 || t.c1 - t.c0 > kSolveRest) ) { return "solve-rest range out of bounds" + at(); }
+        if( t.panel < 0 || static_cast<size_t>( t.panel ) >= pl.sdiag.size() ) { return "solve-rest panel out of range" + at(); }
         {
             const SolveDiagTask & d = pl.sdiag[static_cast<size_t>( t.panel )];
-            if( d.u0 != t.u0 || d.r0 != t.r0 || d.n0 != t.n0 || d.row0 != t.row0 ) { return "solve-rest panel mismatch" + at; }
+            if( d.u0 != t.u0 || d.r0 != t.r0 || d.n0 != t.n0 || d.row0 != t.row0 ) { return "solve-rest panel mismatch" + at(); }
         }
-        if( t.ld0 < t.n0 || t.ld1 < t.n1 ) { return "solve-rest leading dimension too small" + at; }
-        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "solve-rest U0 out of range" + at; }
-        if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.ld1 - 1, arena ) ) { return "solve-rest U1 out of range" + at; }
-        if( t.n1 > 0 && (t.inner < 0 || t.inner + t.n1 > inner_size) ) { return "solve-rest columns out of range" + at; }
-        if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "solve-rest rows out of range" + at; }
+        if( t.ld0 < t.n0 || t.ld1 < t.n1 ) { return "solve-rest leading dimension too small" + at(); }
+        if( !in_range( t.u0, t.u0 + static_cast<I64>(t.n0) * t.ld0 - 1, arena ) ) { return "solve-rest U0 out of range" + at(); }
+        if( t.n1 > 0 && !in_range( t.u1, t.u1 + static_cast<I64>(t.n0) * t.ld1 - 1, arena ) ) { return "solve-rest U1 out of range" + at(); }
+        if( t.n1 > 0 && (t.inner < 0 || t.inner + t.n1 > inner_size) ) { return "solve-rest columns out of range" + at(); }
+        if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "solve-rest rows out of range" + at(); }
     }
     for( I32 v : sym.sn_inner ) { if( v < 0 || v >= sym.n ) { return "SN_inner value out of range"; } }
     for( size_t k = 0; k < pl.exports.size(); ++k )
     {
         const ExportTask & t = pl.exports[k];
-        const std::string at = " (export task " + std::to_string( k ) + ")";
-        if( t.n0s <= 0 || t.r_begin < 0 || t.r_end > t.n0s || t.r_begin >= t.r_end ) { return "bad export rows" + at; }
-        if( t.roff < 0 || t.roff + t.n0s > t.fn0 ) { return "export rows outside the front" + at; }
-        if( !in_range( t.tri, t.tri + static_cast<I64>(t.n0s) * t.n0s - 1, tri_size ) ) { return "export tri out of range" + at; }
-        if( t.n1s > 0 && !in_range( t.rec, t.rec + static_cast<I64>(t.n0s) * t.n1s - 1, rec_size ) ) { return "export rec out of range" + at; }
-        if( t.fld0 < t.fn0 || t.fld1 < t.fn1 ) { return "export leading dimension too small" + at; }
-        if( !in_range( t.fu0, t.fu0 + static_cast<I64>(t.fn0) * t.fld0 - 1, arena ) ) { return "export front U0 out of range" + at; }
-        if( t.fn1 > 0 && !in_range( t.fu1, t.fu1 + static_cast<I64>(t.fn0) * t.fld1 - 1, arena ) ) { return "export front U1 out of range" + at; }
-        if( t.colmap < 0 || t.colmap + t.n1s > static_cast<I64>( pl.colmap.size() ) ) { return "export colmap out of range" + at; }
+        auto at = [&]() { return " (export task " + std::to_string( k ) + ")"; };   // built only on failure
+        if( t.n0s <= 0 || t.r_begin < 0 || t.r_end > t.n0s || t.r_begin >= t.r_end ) { return "bad export rows" + at(); }
+        if( t.roff < 0 || t.roff + t.n0s > t.fn0 ) { return "export rows outside the front" + at(); }
+        if( !in_range( t.tri, t.tri + static_cast<I64>(t.n0s) * t.n0s - 1, tri_size ) ) { return "export tri out of range" + at(); }
+        if( t.n1s > 0 && !in_range( t.rec, t.rec + static_cast<I64>(t.n0s) * t.n1s - 1, rec_size ) ) { return "export rec out of range" + at(); }
+        if( t.fld0 < t.fn0 || t.fld1 < t.fn1 ) { return "export leading dimension too small" + at(); }
+        if( !in_range( t.fu0, t.fu0 + static_cast<I64>(t.fn0) * t.fld0 - 1, arena ) ) { return "export front U0 out of range" + at(); }
+        if( t.fn1 > 0 && !in_range( t.fu1, t.fu1 + static_cast<I64>(t.fn0) * t.fld1 - 1, arena ) ) { return "export front U1 out of range" + at(); }
+        if( t.colmap < 0 || t.colmap + t.n1s > static_cast<I64>( pl.colmap.size() ) ) { return "export colmap out of range" + at(); }
         for( I32 l = 0; l < t.n1s; ++l )
         {
             const I32 cm = pl.colmap[t.colmap + l];
-            if( cm >= 0 ? cm >= t.fn0 : (-cm - 1) >= t.fn1 ) { return "export colmap value out of range" + at; }
+            if( cm >= 0 ? cm >= t.fn0 : (-cm - 1) >= t.fn1 ) { return "export colmap value out of range" + at(); }
         }
     }
     auto size_of = [&]( LaunchKind kind ) -> I64
@@ -254,20 +258,20 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         for( size_t k = 0; k < pl.dag.size(); ++k )
         {
             const DagTask & t = pl.dag[k];
-            const std::string at = " (graph task " + std::to_string( k ) + ")";
+            auto at = [&]() { return " (graph task " + std::to_string( k ) + ")"; };   // built only on failure
             const LaunchKind kind = static_cast<LaunchKind>( t.kind );
-            if( kind == LaunchKind::Solve || t.index < 0 || t.index >= size_of( kind ) ) { return "task graph index out of range" + at; }
+            if( kind == LaunchKind::Solve || t.index < 0 || t.index >= size_of( kind ) ) { return "task graph index out of range" + at(); }
             ++work;
             for( int i = 0; i < kDagWaits; ++i )
             {
                 if( t.wait[i] < 0 ) { continue; }
-                if( t.wait[i] >= pl.dag_counters ) { return "task graph counter out of range" + at; }
-                if( t.target[i] <= 0 || cnt[static_cast<size_t>( t.wait[i] )] < t.target[i] ) { return "task graph wait not reached by earlier tasks" + at; }
+                if( t.wait[i] >= pl.dag_counters ) { return "task graph counter out of range" + at(); }
+                if( t.target[i] <= 0 || cnt[static_cast<size_t>( t.wait[i] )] < t.target[i] ) { return "task graph wait not reached by earlier tasks" + at(); }
             }
             for( int i = 0; i < 2; ++i )
             {
                 if( t.signal[i] < 0 ) { continue; }
-                if( t.signal[i] >= pl.dag_counters ) { return "task graph counter out of range" + at; }
+                if( t.signal[i] >= pl.dag_counters ) { return "task graph counter out of range" + at(); }
                 ++cnt[static_cast<size_t>( t.signal[i] )];
             }
         }
