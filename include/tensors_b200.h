@@ -160,8 +160,9 @@ int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
  * microseconds of the scheduled task graph (0 before the first numeric
  * factorization on a device), out[13] tasks of the graph, out[14] tasks of
  * the solve's task graph, out[15] its first level, out[16] CTAs of the
- * persistent factorization launch (0 before the device plan exists).
- * Returns the number of entries written (at most cap). */
+ * persistent factorization launch (0 before the device plan exists),
+ * out[17] / out[18] host microseconds of the last symbolic analysis / plan
+ * build.  Returns the number of entries written (at most cap). */
 int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
 /* Host-side bounds check of every device task of the plan (also run before
  * the plan is first uploaded).  TB_OK or TB_ERR_INVALID_ARGUMENT with the
@@ -355,6 +356,20 @@ int tb_server_wait( tb_server * s, int64_t request_id, int32_t * status, double 
                     int32_t * iterations, double * relres );
 int tb_server_stats( tb_server * s, int64_t * resident_bytes, int64_t * peak_resident_bytes, int64_t * evictions,
                      int64_t * refactors );
+
+/* ------------------------------------------------------------------------
+ * Fill-reducing ordering from the pattern alone (host only, no device
+ * needed), for the constructor's permutation argument where the reference
+ * calls METIS or AMD (src/Sparse/Metis.hpp:81,
+ * src/Sparse/ApproximateMinimumDegree.hpp:58): George's automatic nested
+ * dissection on the node graph (dofs_per_node consecutive rows form a node
+ * and stay together): components split apart, rooted level structures from
+ * pseudo-peripheral nodes, median-level separators ordered last, subgraphs
+ * of at most leaf_size rows emitted in breadth-first order.  perm[i] is the
+ * original row placed at position i (Inverse::False, as the constructor
+ * takes it).  The pattern is symmetrized; a diagonal is not required. */
+int tb_nested_dissection( int32_t n, const int64_t * outer, const int32_t * inner, int32_t dofs_per_node,
+                          int32_t leaf_size, int32_t * perm );
 
 /* ------------------------------------------------------------------------
  * MatrixMarket files (host only, no device needed).

@@ -444,7 +444,7 @@ class CholeskyDecomposition:
         m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 24))
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
                 "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks",
-                "solve_graph_tasks", "solve_split_level", "graph_ctas"]
+                "solve_graph_tasks", "solve_split_level", "graph_ctas", "analyze_us", "plan_us"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

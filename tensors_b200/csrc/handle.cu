@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <utility>
 #include <climits>
 #include <limits>
@@ -125,6 +126,7 @@ struct tb_chol
     std::int32_t method = TB_MULTIFRONTAL;
 
     bool symbolic_done = false;
+    std::int64_t analyze_us = 0, plan_us = 0;   // host time of the last symbolic analysis and plan build
     bool device_ready = false;
     bool kernels_configured = false;
     tb::Symbolic sym;
@@ -254,7 +256,9 @@ int ensure_symbolic( tb_chol * h )
     in.perm = h->has_perm ? h->perm.data() : nullptr;
     in.strategy = h->strategy;
     in.amalgamation_threshold = h->amalgamation_threshold;
+    const auto t0 = std::chrono::steady_clock::now();
     const int st = h->sym.analyze( in );
+    const auto t1 = std::chrono::steady_clock::now();
     if( st != TB_OK )
     {
         const char * what = st == TB_ERR_INVALID_PERMUTATION ? "input is not a permutation"
@@ -266,6 +270,9 @@ int ensure_symbolic( tb_chol * h )
     h->plan.build( h->sym );
     if( h->solve_schedule == TB_SCHEDULE_LEVELS ) { h->plan.build_solve_graph( h->sym, h->plan.levels ); }
     else if( h->solve_schedule == TB_SCHEDULE_TASK_GRAPH_ALL ) { h->plan.build_solve_graph( h->sym, 0 ); }
+    const auto t2 = std::chrono::steady_clock::now();
+    h->analyze_us = std::chrono::duration_cast<std::chrono::microseconds>( t1 - t0 ).count();
+    h->plan_us = std::chrono::duration_cast<std::chrono::microseconds>( t2 - t1 ).count();
     h->symbolic_done = true;
     h->device_ready = false;
     h->factorized = false;
@@ -1463,7 +1470,7 @@ int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
         static_cast<std::int64_t>( pl.upper_launches.size() ), h->sym.sn_count, pl.front_count,
         static_cast<std::int64_t>( pl.front_flops ), static_cast<std::int64_t>( pl.dag_makespan_us ),
         static_cast<std::int64_t>( pl.dag.size() ), static_cast<std::int64_t>( pl.solve_fwd_order.size() ),
-        pl.solve_split_level, h->dag_grid };
+        pl.solve_split_level, h->dag_grid, h->analyze_us, h->plan_us };
     const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
     for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
     return m;

@@ -404,6 +404,7 @@ void Plan::build( const Symbolic & sym )
     {
         const auto & L = by_level[h];
         cur_level = h;
+        const size_t extend_before = extend.size();   // this level's extend-adds signal its counter
 
         // zero this level's update matrices before children add into them;
         // the regions may have been used by fronts consumed at earlier levels
@@ -651,8 +652,7 @@ void Plan::build( const Symbolic & sym )
             emit( rest_tiles[q] );
         }
         {
-            I32 count = 0;
-            for( const PendingTask & t : pending ) { if( t.kind == static_cast<I32>( LaunchKind::Extend ) && t.signal[1].idx == h ) { ++count; } }
+            const I32 count = static_cast<I32>( extend.size() - extend_before );
             if( count > 0 ) { prev_ext_level = h; prev_ext_count = count; }
         }
     }

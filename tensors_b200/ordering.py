@@ -19,7 +19,7 @@ import numpy as np
 
 from .matrices import CSRMatrix
 
-__all__ = ["nested_dissection", "identity_ordering", "is_permutation"]
+__all__ = ["nested_dissection", "graph_nested_dissection", "identity_ordering", "is_permutation"]
 
 
 def is_permutation(p: np.ndarray, n: int) -> bool:
@@ -52,10 +52,27 @@ def _node_graph(A: CSRMatrix):
     return G.indptr.astype(np.int64), G.indices.astype(np.int64), nodes
 
 
+def graph_nested_dissection(A: CSRMatrix, leaf_size: int = 64) -> np.ndarray:
+    """Nested dissection from the pattern alone (native ``tb_nested_dissection``): George's
+    automatic nested dissection with rooted level structures from pseudo-peripheral nodes.
+    Needs no coordinates, so it orders any matrix (one read from a file, say); the dofs of a
+    node (``A.dofs_per_node`` consecutive rows) stay together."""
+    from ._lib import lib
+    from .cholesky import _check
+
+    outer = np.ascontiguousarray(A.outer, dtype=np.int64)
+    inner = np.ascontiguousarray(A.inner, dtype=np.int32)
+    perm = np.zeros(A.n, dtype=np.int32)
+    _check(lib().tb_nested_dissection(int(A.n), outer.ctypes.data, inner.ctypes.data, int(A.dofs_per_node),
+                                      int(leaf_size), perm.ctypes.data))
+    return perm
+
+
 def nested_dissection(A: CSRMatrix, leaf_size: int = 64) -> np.ndarray:
-    """Geometric nested dissection of ``A`` using ``A.coords`` (see module doc)."""
+    """Geometric nested dissection of ``A`` using ``A.coords`` (see module doc); a matrix without
+    coordinates is ordered by :func:`graph_nested_dissection`."""
     if A.coords is None:
-        raise ValueError("nested_dissection needs node coordinates (CSRMatrix.coords)")
+        return graph_nested_dissection(A, leaf_size)
     indptr, indices, nodes = _node_graph(A)
     coords = np.asarray(A.coords, dtype=np.float64)
     if coords.shape[0] != nodes:
