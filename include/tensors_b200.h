@@ -367,9 +367,11 @@ int tb_server_stats( tb_server * s, int64_t * resident_bytes, int64_t * peak_res
  * pseudo-peripheral nodes, median-level separators ordered last, subgraphs
  * of at most leaf_size rows emitted in breadth-first order.  perm[i] is the
  * original row placed at position i (Inverse::False, as the constructor
- * takes it).  The pattern is symmetrized; a diagonal is not required. */
+ * takes it).  The pattern is symmetrized; a diagonal is not required.  The
+ * sides of the top splits are ordered on up to thread_count threads (<= 0:
+ * all host threads); the result does not depend on the thread count. */
 int tb_nested_dissection( int32_t n, const int64_t * outer, const int32_t * inner, int32_t dofs_per_node,
-                          int32_t leaf_size, int32_t * perm );
+                          int32_t leaf_size, int32_t thread_count, int32_t * perm );
 
 /* ------------------------------------------------------------------------
  * MatrixMarket files (host only, no device needed).

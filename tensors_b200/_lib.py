@@ -92,7 +92,7 @@ SIGNATURES = {
     "tb_matrix_market_read": (ctypes.c_int, [ctypes.c_char_p, _i32, _pi32, _pi32, ctypes.POINTER(_pi64),
                                              ctypes.POINTER(_pi32), ctypes.POINTER(_pd)]),
     "tb_matrix_market_free": (ctypes.c_int, [_vp]),
-    "tb_nested_dissection": (ctypes.c_int, [_i32, _vp, _vp, _i32, _i32, _vp]),
+    "tb_nested_dissection": (ctypes.c_int, [_i32, _vp, _vp, _i32, _i32, _i32, _vp]),
     "tb_matrix_market_write": (ctypes.c_int, [ctypes.c_char_p, _i32, _i32, _vp, _vp, _vp]),
 }
 

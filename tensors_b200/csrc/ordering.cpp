@@ -22,6 +22,9 @@
 #include "common.hpp"
 
 #include <algorithm>
+#include <atomic>
+#include <future>
+#include <thread>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -105,56 +108,119 @@ class Dissection
 {
 public:
     Dissection( const Graph & g, I32 leaf ) : g_( g ), leaf_( std::max( 1, leaf ) ),
-        owner_( static_cast<size_t>( g.n ), -1 ), level_( static_cast<size_t>( g.n ), -1 ), slot_( static_cast<size_t>( g.n ), -1 ),
-        key1_( static_cast<size_t>( g.n ), 0 ), key2_( static_cast<size_t>( g.n ), 0 ) {}
-
-    std::vector<I32> run()
+        owner_( static_cast<size_t>( g.n ) ), level_( static_cast<size_t>( g.n ), -1 ), slot_( static_cast<size_t>( g.n ), -1 ),
+        key1_( static_cast<size_t>( g.n ), 0 ), key2_( static_cast<size_t>( g.n ), 0 )
     {
-        std::vector<I32> order;
-        order.reserve( static_cast<size_t>( g_.n ) );
-        struct Item { std::vector<I32> nodes; bool emit; };
-        std::vector<Item> stack;
+        for( auto & o : owner_ ) { o.store( -1, std::memory_order_relaxed ); }
+    }
+
+    // The whole graph: the top levels of the dissection tree on up to
+    // `threads` threads (the two sides of a split are independent), the rest
+    // depth-first on each thread.  The order does not depend on the threads.
+    std::vector<I32> run( int threads )
+    {
         std::vector<I32> all( static_cast<size_t>( g_.n ) );
         for( I32 v = 0; v < g_.n; ++v ) { all[static_cast<size_t>( v )] = v; }
-        stack.push_back( { std::move( all ), false } );
+        int depth = 0;
+        while( (1 << depth) < threads ) { ++depth; }
+        return order_parallel( std::move( all ), depth );
+    }
+
+private:
+    // One dissection step on a node set: emit it whole (small or not
+    // separable), its components, or (left, right, separator).
+    struct Step { int kind = 0; std::vector<std::vector<I32>> parts; };
+
+    Step step( std::vector<I32> nodes )
+    {
+        const I32 id = stamp_.fetch_add( 1 ) + 1;
+        for( I32 v : nodes ) { set_owner( v, id ); }
+        // components, each in breadth-first order from its first node
+        std::vector<std::vector<I32>> comps;
+        for( I32 v : nodes )
+        {
+            if( owner( v ) != id ) { continue; }     // already reached
+            comps.push_back( bfs( v, id, -id - 1 ) );
+        }
+        Step st;
+        if( comps.size() > 1 ) { st.kind = 1; st.parts = std::move( comps ); return st; }
+        std::vector<I32> & S = comps[0];            // connected; owner now -id - 1
+        std::vector<I32> left, sep, right;
+        if( static_cast<I32>( S.size() ) <= leaf_ || !split( S, -id - 1, left, sep, right ) )
+        {
+            st.parts.push_back( std::move( S ) );
+            return st;
+        }
+        st.kind = 2;
+        st.parts.push_back( std::move( left ) );
+        st.parts.push_back( std::move( right ) );
+        st.parts.push_back( std::move( sep ) );
+        return st;
+    }
+
+    // Depth-first with an explicit stack: components in turn, and per split
+    // the left side, the right side, then the separator.
+    std::vector<I32> run_serial( std::vector<I32> nodes )
+    {
+        std::vector<I32> order;
+        order.reserve( nodes.size() );
+        struct Item { std::vector<I32> nodes; bool emit; };
+        std::vector<Item> stack;
+        stack.push_back( { std::move( nodes ), false } );
         while( !stack.empty() )
         {
             Item it = std::move( stack.back() );
             stack.pop_back();
             if( it.emit ) { order.insert( order.end(), it.nodes.begin(), it.nodes.end() ); continue; }
-            const I32 id = ++stamp_;
-            for( I32 v : it.nodes ) { owner_[static_cast<size_t>( v )] = id; }
-            // components, each in breadth-first order from its first node
-            std::vector<std::vector<I32>> comps;
-            for( I32 v : it.nodes )
+            Step st = step( std::move( it.nodes ) );
+            if( st.kind == 0 ) { order.insert( order.end(), st.parts[0].begin(), st.parts[0].end() ); continue; }
+            if( st.kind == 1 )
             {
-                if( owner_[static_cast<size_t>( v )] != id ) { continue; }     // already reached
-                comps.push_back( bfs( v, id, -id - 1 ) );
-            }
-            if( comps.size() > 1 )
-            {
-                for( size_t c = comps.size(); c-- > 0; ) { stack.push_back( { std::move( comps[c] ), false } ); }
+                for( size_t c = st.parts.size(); c-- > 0; ) { stack.push_back( { std::move( st.parts[c] ), false } ); }
                 continue;
             }
-            std::vector<I32> & S = comps[0];            // connected; owner_ now -id - 1
-            const I32 sid = -id - 1;
-            if( static_cast<I32>( S.size() ) <= leaf_ ) { order.insert( order.end(), S.begin(), S.end() ); continue; }
-            std::vector<I32> left, sep, right;
-            if( !split( S, sid, left, sep, right ) ) { order.insert( order.end(), S.begin(), S.end() ); continue; }
-            stack.push_back( { std::move( sep ), true } );
-            stack.push_back( { std::move( right ), false } );
-            stack.push_back( { std::move( left ), false } );
+            stack.push_back( { std::move( st.parts[2] ), true } );
+            stack.push_back( { std::move( st.parts[1] ), false } );
+            stack.push_back( { std::move( st.parts[0] ), false } );
         }
         return order;
     }
 
-private:
+    // The same order, with the sides of the top `depth` splits on two threads.
+    std::vector<I32> order_parallel( std::vector<I32> nodes, int depth )
+    {
+        if( depth <= 0 || nodes.size() < kParallelMin ) { return run_serial( std::move( nodes ) ); }
+        Step st = step( std::move( nodes ) );
+        if( st.kind == 0 ) { return std::move( st.parts[0] ); }
+        std::vector<I32> order;
+        if( st.kind == 1 )
+        {
+            for( auto & c : st.parts )
+            {
+                std::vector<I32> o = order_parallel( std::move( c ), depth );
+                order.insert( order.end(), o.begin(), o.end() );
+            }
+            return order;
+        }
+        auto left = std::async( std::launch::async, [this, &st, depth] { return order_parallel( std::move( st.parts[0] ), depth - 1 ); } );
+        std::vector<I32> right = order_parallel( std::move( st.parts[1] ), depth - 1 );
+        order = left.get();
+        order.insert( order.end(), right.begin(), right.end() );
+        order.insert( order.end(), st.parts[2].begin(), st.parts[2].end() );
+        return order;
+    }
+
+    // Set membership labels: read across sets by concurrent searches (a
+    // neighbour may belong to another thread's set), so accessed atomically.
+    I32 owner( I32 v ) const { return owner_[static_cast<size_t>( v )].load( std::memory_order_relaxed ); }
+    void set_owner( I32 v, I32 x ) { owner_[static_cast<size_t>( v )].store( x, std::memory_order_relaxed ); }
+
     // Breadth-first search over nodes with owner_ == from, relabelling them
     // to `to` and recording their levels; returns the nodes in visit order.
     std::vector<I32> bfs( I32 root, I32 from, I32 to )
     {
         std::vector<I32> q{ root };
-        owner_[static_cast<size_t>( root )] = to;
+        set_owner( root, to );
         level_[static_cast<size_t>( root )] = 0;
         for( size_t h = 0; h < q.size(); ++h )
         {
@@ -162,8 +228,8 @@ private:
             for( I64 k = g_.ptr[static_cast<size_t>( u )]; k < g_.ptr[static_cast<size_t>( u ) + 1]; ++k )
             {
                 const I32 v = g_.adj[static_cast<size_t>( k )];
-                if( owner_[static_cast<size_t>( v )] != from ) { continue; }
-                owner_[static_cast<size_t>( v )] = to;
+                if( owner( v ) != from ) { continue; }
+                set_owner( v, to );
                 level_[static_cast<size_t>( v )] = level_[static_cast<size_t>( u )] + 1;
                 q.push_back( v );
             }
@@ -175,9 +241,9 @@ private:
     // owner marks are restored to sid afterwards.  Returns the depth.
     I32 levels_from( const std::vector<I32> & S, I32 sid, I32 root, std::vector<I32> & visit )
     {
-        const I32 tmp = --tmp_stamp_;
+        const I32 tmp = tmp_stamp_.fetch_sub( 1 ) - 1;
         visit = bfs( root, sid, tmp );
-        for( I32 v : S ) { owner_[static_cast<size_t>( v )] = sid; }
+        for( I32 v : S ) { set_owner( v, sid ); }
         return level_[static_cast<size_t>( visit.back() )];
     }
 
@@ -230,7 +296,7 @@ private:
         }
         if( best.which < 0 || best.cover.empty() ) { return false; }
         const std::vector<I32> & key = best.which == 0 ? key1_ : key2_;
-        const I32 tag = --tmp_stamp_;
+        const I32 tag = tmp_stamp_.fetch_sub( 1 ) - 1;
         for( I32 v : best.cover ) { level_[static_cast<size_t>( v )] = tag; }    // level_ is free again: mark the cover
         for( I32 v : visit )                        // breadth-first order from the root
         {
@@ -266,7 +332,7 @@ private:
             for( I64 e = g_.ptr[static_cast<size_t>( v )]; e < g_.ptr[static_cast<size_t>( v ) + 1]; ++e )
             {
                 const I32 w = g_.adj[static_cast<size_t>( e )];
-                if( owner_[static_cast<size_t>( w )] != sid ) { continue; }
+                if( owner( w ) != sid ) { continue; }
                 if( from_left ? key[static_cast<size_t>( w )] > c : key[static_cast<size_t>( w )] <= c ) { return true; }
             }
             return false;
@@ -291,7 +357,7 @@ private:
             for( I64 e = g_.ptr[static_cast<size_t>( u )]; e < g_.ptr[static_cast<size_t>( u ) + 1]; ++e )
             {
                 const I32 w = g_.adj[static_cast<size_t>( e )];
-                if( owner_[static_cast<size_t>( w )] == sid && key[static_cast<size_t>( w )] > c ) { nbr[i].push_back( slot_[static_cast<size_t>( w )] ); }
+                if( owner( w ) == sid && key[static_cast<size_t>( w )] > c ) { nbr[i].push_back( slot_[static_cast<size_t>( w )] ); }
             }
         }
         std::vector<I32> match_a( na, -1 ), match_b( nb, -1 ), seen( nb, -1 );
@@ -351,15 +417,17 @@ private:
 
     const Graph & g_;
     I32 leaf_;
-    std::vector<I32> owner_, level_, slot_, key1_, key2_;
-    I32 stamp_ = 0;
-    I32 tmp_stamp_ = -(1 << 30);
+    static constexpr size_t kParallelMin = 20000;   // smaller sets are not worth a thread
+    std::vector<std::atomic<I32>> owner_;
+    std::vector<I32> level_, slot_, key1_, key2_;
+    std::atomic<I32> stamp_{ 0 };
+    std::atomic<I32> tmp_stamp_{ -(1 << 30) };
 };
 
 } // namespace
 
 extern "C" int tb_nested_dissection( int32_t n, const int64_t * outer, const int32_t * inner, int32_t dofs_per_node,
-                                     int32_t leaf_size, int32_t * perm )
+                                     int32_t leaf_size, int32_t thread_count, int32_t * perm )
 {
     if( n < 0 || (n > 0 && (outer == nullptr || inner == nullptr || perm == nullptr)) || dofs_per_node < 1 )
     {
@@ -377,7 +445,9 @@ extern "C" int tb_nested_dissection( int32_t n, const int64_t * outer, const int
         if( inner[k] < 0 || inner[k] >= n ) { return fail( TB_ERR_INVALID_PATTERN, "tb_nested_dissection: column index out of range" ); }
     }
     const Graph g = node_graph( n, outer, inner, dofs_per_node );
-    const std::vector<I32> order = Dissection( g, std::max( 1, leaf_size / dofs_per_node ) ).run();
+    int threads = thread_count;
+    if( threads <= 0 ) { const unsigned h = std::thread::hardware_concurrency(); threads = h == 0 ? 1 : static_cast<int>( std::min( h, 64u ) ); }
+    const std::vector<I32> order = Dissection( g, std::max( 1, leaf_size / dofs_per_node ) ).run( threads );
     I64 i = 0;
     for( I32 u : order )
     {

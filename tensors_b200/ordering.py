@@ -52,11 +52,12 @@ def _node_graph(A: CSRMatrix):
     return G.indptr.astype(np.int64), G.indices.astype(np.int64), nodes
 
 
-def graph_nested_dissection(A: CSRMatrix, leaf_size: int = 64) -> np.ndarray:
+def graph_nested_dissection(A: CSRMatrix, leaf_size: int = 64, thread_count: int = 0) -> np.ndarray:
     """Nested dissection from the pattern alone (native ``tb_nested_dissection``): George's
     automatic nested dissection with rooted level structures from pseudo-peripheral nodes.
     Needs no coordinates, so it orders any matrix (one read from a file, say); the dofs of a
-    node (``A.dofs_per_node`` consecutive rows) stay together."""
+    node (``A.dofs_per_node`` consecutive rows) stay together.  ``thread_count`` <= 0: all host
+    threads; the order is the same for every thread count."""
     from ._lib import lib
     from .cholesky import _check
 
@@ -64,7 +65,7 @@ def graph_nested_dissection(A: CSRMatrix, leaf_size: int = 64) -> np.ndarray:
     inner = np.ascontiguousarray(A.inner, dtype=np.int32)
     perm = np.zeros(A.n, dtype=np.int32)
     _check(lib().tb_nested_dissection(int(A.n), outer.ctypes.data, inner.ctypes.data, int(A.dofs_per_node),
-                                      int(leaf_size), perm.ctypes.data))
+                                      int(leaf_size), int(thread_count), perm.ctypes.data))
     return perm
 
 

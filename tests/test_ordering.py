@@ -45,6 +45,7 @@ def test_graph_nested_dissection_is_a_permutation():
         p = O.graph_nested_dissection(A)
         assert O.is_permutation(p, A.n)
         assert np.array_equal(p, O.graph_nested_dissection(A))          # deterministic
+        assert np.array_equal(p, O.graph_nested_dissection(A, thread_count=1))   # and the same on one thread
         if A.dofs_per_node > 1:
             assert np.array_equal(p.reshape(-1, 3), (p[::3] // 3)[:, None] * 3 + np.arange(3))
 
