@@ -48,12 +48,17 @@ L2_FLUSH_BYTES = 256 << 20
 CPU_SAMPLE_GRID = 48
 
 
+# C2's nested dissection: "geometric" (grid planes from the node coordinates, the default) or
+# "graph" (from the pattern alone; on this grid about half the factor flops, see --ordering).
+ORDERING = "geometric"
+
+
 def build_problem(grid: int | None = None):
     grid = GRID if grid is None else grid
     from tensors_b200 import matrices, ordering
 
     A = matrices.grid_laplacian_3d(grid, SEED, SHIFT)
-    perm = ordering.nested_dissection(A)
+    perm = ordering.graph_nested_dissection(A) if ORDERING == "graph" else ordering.nested_dissection(A)
     B = np.random.default_rng(SEED + 1).standard_normal((A.n, NRHS))
     return A, perm, B
 
@@ -63,7 +68,7 @@ def config_dict(extra=None):
         "workload": f"3D 7-point Laplacian {GRID}^3 (n={GRID**3}), lognormal(0,1) edge conductivities, "
                     f"shift {SHIFT:g}, nested dissection, {NRHS} RHS N(0,1), FP64 factor+solve",
         "grid": GRID, "n": GRID ** 3, "nrhs": NRHS, "seed": SEED,
-        "supernode_strategy": "Maximal",
+        "supernode_strategy": "Maximal", "ordering": f"{ORDERING} nested dissection",
         "l2": "256 MiB buffer written between timed steps (inputs and factor also exceed L2)",
     }
     if extra:
@@ -545,7 +550,12 @@ def main():
     ap.add_argument("--ncu", action="store_true",
                     help="profiling run for ncu: warmup + steps factor+solve as direct launches, no timing, "
                          "no baselines")
+    ap.add_argument("--ordering", default="geometric", choices=["geometric", "graph"],
+                    help="c2: nested dissection from node coordinates (default) or from the pattern alone "
+                         "(fewer factor flops on this grid; GFLOP/s is then computed from its own flops)")
     args = ap.parse_args()
+    global ORDERING
+    ORDERING = args.ordering
     if args.impl == "reference":
         return run_reference(args)
     if args.ncu:
