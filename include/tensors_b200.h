@@ -145,6 +145,13 @@ int tb_chol_factor_sizes( tb_chol * h, int64_t * tri_size, int64_t * rec_size );
 /* Copy the factor back in the reference's layout: SN_TriangleValues and
  * SN_RectangleValues (InputOutput.hpp:339-352), row-major U0 / U1 blocks. */
 int tb_chol_factor_values( tb_chol * h, double * tri, double * rec );
+/* U as a CSR matrix in the permuted ordering, as the reference's GetU
+ * (InputOutput.hpp:116-217): row i of supernode s holds the triangle's
+ * columns i .. end of s, then the supernode's column set; rows sorted.
+ * tb_chol_u_nonzero_count (host-only, after the symbolic phase) sizes
+ * inner / values; outer has n + 1 entries. */
+int tb_chol_u_nonzero_count( tb_chol * h, int64_t * out );
+int tb_chol_get_u( tb_chol * h, int64_t * outer, int32_t * inner, double * values );
 /* LogDeterminant (InputOutput.hpp:294-297) and WriteFactorDiagonal (:238-257). */
 int tb_chol_log_det( tb_chol * h, double * out );
 int tb_chol_factor_diagonal( tb_chol * h, double * diag );

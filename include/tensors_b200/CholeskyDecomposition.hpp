@@ -24,24 +24,11 @@
 #include <vector>
 
 #include "../tensors_b200.h"
+#include "Error.hpp"
+#include "MatrixCSR.hpp"
 
 namespace tensors_b200 {
 namespace Sparse {
-
-class Error : public std::runtime_error
-{
-public:
-    Error( int status, const std::string & what ) : std::runtime_error( what ), status_( status ) {}
-    int Status() const noexcept { return status_; }
-private:
-    int status_;
-};
-
-inline int Check( int status )
-{
-    if( status < 0 ) { throw Error( status, tb_last_error() ); }
-    return status;
-}
 
 enum class SupernodeStrategy_T : int32_t
 {
@@ -197,6 +184,19 @@ public:
         out.second.resize( static_cast<size_t>( RequiredRectangularSize() ) );
         Check( tb_chol_factor_values( h_, out.first.data(), out.second.data() ) );
         return out;
+    }
+
+    // GetU (InputOutput.hpp:116-217): U in the permuted ordering as CSR.
+    MatrixCSR GetU() const
+    {
+        LInt nnz = 0;
+        Check( tb_chol_u_nonzero_count( h_, &nnz ) );
+        const Int n = RowCount();
+        std::vector<LInt> outer( static_cast<size_t>( n ) + 1 );
+        std::vector<Int> inner( static_cast<size_t>( nnz ) );
+        std::vector<Scal> values( static_cast<size_t>( nnz ) );
+        Check( tb_chol_get_u( h_, outer.data(), inner.data(), values.data() ) );
+        return MatrixCSR( outer.data(), inner.data(), values.data(), n, n, 1 );
     }
 
     // LogDeterminant (InputOutput.hpp:294-297), WriteFactorDiagonal (:238-257).

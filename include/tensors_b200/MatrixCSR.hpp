@@ -15,7 +15,8 @@
 #include <filesystem>
 #include <vector>
 
-#include "CholeskyDecomposition.hpp"
+#include "../tensors_b200.h"
+#include "Error.hpp"
 
 namespace tensors_b200 {
 namespace Sparse {

@@ -48,6 +48,8 @@ SIGNATURES = {
     "tb_chol_factor_sizes": (ctypes.c_int, [_vp, _pi64, _pi64]),
     "tb_chol_factor_values": (ctypes.c_int, [_vp, _vp, _vp]),
     "tb_chol_log_det": (ctypes.c_int, [_vp, _pd]),
+    "tb_chol_u_nonzero_count": (ctypes.c_int, [_vp, _pi64]),
+    "tb_chol_get_u": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "tb_chol_factor_diagonal": (ctypes.c_int, [_vp, _vp]),
     "tb_chol_flop_count": (ctypes.c_int, [_vp, _pd, _pd]),
     "tb_chol_device_bytes": (ctypes.c_int, [_vp, _pi64]),

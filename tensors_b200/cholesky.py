@@ -492,6 +492,11 @@ class CholeskyDecomposition:
         _check(lib().tb_chol_launch_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def UNonzeroCount(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().tb_chol_u_nonzero_count(self._h, ctypes.byref(v)))
+        return v.value
+
     def GetU(self):
         """U as a scipy CSR matrix in the permuted ordering (InputOutput.hpp:116-217)."""
         import scipy.sparse as sp
@@ -514,6 +519,12 @@ class CholeskyDecomposition:
                 rr = np.repeat(np.arange(n0), n1)
                 rows.append(i0 + rr); cols.append(np.tile(si[so[s]: so[s + 1]], n0)); vals.append(U1.ravel())
         return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(self._n, self._n))
+
+    def UNonzeroCount(self) -> int:
+        """Nonzeros of U (tb_chol_u_nonzero_count; host-only after the symbolic phase)."""
+        v = ctypes.c_int64()
+        _check(lib().tb_chol_u_nonzero_count(self._h, ctypes.byref(v)))
+        return v.value
 
 
 def _is_cuda_tensor(x) -> bool:

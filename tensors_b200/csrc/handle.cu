@@ -1426,6 +1426,56 @@ int tb_chol_factor_values( tb_chol * h, double * tri, double * rec )
     return TB_OK;
 }
 
+// Nonzeros of U (InputOutput.hpp:124-137): per supernode row i, the
+// triangle's columns i .. i_end - 1 and the supernode's n1 columns.
+int tb_chol_u_nonzero_count( tb_chol * h, std::int64_t * out )
+{
+    TB_TRY( check_handle( h ) );
+    if( out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    TB_TRY( ensure_symbolic( h ) );
+    const tb::Symbolic & s = h->sym;
+    std::int64_t nnz = 0;
+    for( std::int32_t k = 0; k < s.sn_count; ++k )
+    {
+        const std::int64_t n0 = s.sn_rp[k + 1] - s.sn_rp[k], n1 = s.sn_outer[k + 1] - s.sn_outer[k];
+        nnz += n0 * (n0 + 1) / 2 + n0 * n1;
+    }
+    *out = nnz;
+    return TB_OK;
+}
+
+// U as CSR in the permuted ordering, rows sorted, as the reference's GetU
+// (InputOutput.hpp:116-217) lays it out: row i of supernode s holds U0's row
+// from the diagonal on (columns i .. i_end - 1), then U1's row (columns
+// SN_inner[SN_outer[s] ..]).
+int tb_chol_get_u( tb_chol * h, std::int64_t * outer, std::int32_t * inner, double * values )
+{
+    TB_TRY( check_handle( h ) );
+    if( outer == nullptr || inner == nullptr || values == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    const tb::Symbolic & s = h->sym;
+    if( !h->factorized ) { return fail( TB_ERR_NOT_FACTORIZED, "GetU requested before NumericFactorization" ); }
+    std::vector<double> tri( static_cast<size_t>( s.sn_tri_ptr[s.sn_count] ) ), rec( static_cast<size_t>( s.sn_rec_ptr[s.sn_count] ) );
+    TB_TRY( tb_chol_factor_values( h, tri.data(), rec.data() ) );
+    outer[0] = 0;
+    for( std::int32_t k = 0; k < s.sn_count; ++k )
+    {
+        const std::int32_t i0 = s.sn_rp[k], i1 = s.sn_rp[k + 1];
+        const std::int32_t n0 = i1 - i0;
+        const std::int64_t l0 = s.sn_outer[k];
+        const std::int32_t n1 = static_cast<std::int32_t>( s.sn_outer[k + 1] - l0 );
+        const double * U0 = tri.data() + s.sn_tri_ptr[k];
+        const double * U1 = rec.data() + s.sn_rec_ptr[k];
+        for( std::int32_t r = 0; r < n0; ++r )
+        {
+            std::int64_t e = outer[i0 + r];
+            for( std::int32_t c = r; c < n0; ++c, ++e ) { inner[e] = i0 + c; values[e] = U0[static_cast<std::int64_t>( r ) * n0 + c]; }
+            for( std::int32_t c = 0; c < n1; ++c, ++e ) { inner[e] = s.sn_inner[static_cast<size_t>( l0 + c )]; values[e] = U1[static_cast<std::int64_t>( r ) * n1 + c]; }
+            outer[i0 + r + 1] = e;
+        }
+    }
+    return TB_OK;
+}
+
 int tb_chol_log_det( tb_chol * h, double * out )
 {
     TB_TRY( check_handle( h ) );

@@ -376,3 +376,17 @@ def test_factor_diagonal_and_reference_layout_export():
     p = chol.GetPermutation()
     S = A.to_scipy().toarray()[np.ix_(p, p)]
     assert np.abs(U.T @ U - S).max() < 1e-10 * np.abs(S).max()
+
+
+def test_get_u_through_the_c_abi_matches_the_python_assembly():
+    A = M.delaunay_laplacian(1200, 23)
+    chol = CholeskyDecomposition(A.outer, A.inner, O.nested_dissection(A, 16))
+    assert chol.NumericFactorization(A.values, 0.0) == 0
+    nnz = chol.UNonzeroCount()
+    outer = np.zeros(A.n + 1, dtype=np.int64)
+    inner = np.zeros(nnz, dtype=np.int32)
+    values = np.zeros(nnz)
+    assert lib().tb_chol_get_u(chol._h, outer.ctypes.data, inner.ctypes.data, values.ctypes.data) == 0
+    U = chol.GetU()
+    U.sort_indices()
+    assert np.array_equal(outer, U.indptr) and np.array_equal(inner, U.indices) and np.array_equal(values, U.data)

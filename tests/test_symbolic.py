@@ -137,3 +137,13 @@ def test_solve_task_graph_plan_is_deadlock_free(grid, leaf):
         tasks[sched] = c.PlanStats()["solve_graph_tasks"]
     assert tasks["levels"] == 0
     assert tasks["task_graph_all"] > 0 and tasks["task_graph_all"] >= tasks["task_graph"]
+
+
+def test_u_nonzero_count_matches_the_flop_count_structure():
+    for A in (M.grid_laplacian_2d(30, 1.0), M.delaunay_laplacian(2500, 5)):
+        c = CholeskyDecomposition(A.outer, A.inner, O.nested_dissection(A, 16))
+        c.SymbolicFactorization()
+        rp, so = c.SymbolicArray("SN_rp"), c.SymbolicArray("SN_outer")
+        n0, n1 = np.diff(rp), np.diff(so)
+        assert c.UNonzeroCount() == int(np.sum(n0 * (n0 + 1) // 2 + n0 * n1))
+        assert c.UNonzeroCount() == int(c.FlopCount()[1])
