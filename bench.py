@@ -251,11 +251,15 @@ C4_TARGET = 1e-7
 TARGET_RELRES = 1e-10
 
 
-def _time_steps(torch, stream, fn, steps, warmup):
-    """(mean ms of fn() per step, mean ms of its first phase) with CUDA events on `stream`."""
+def _time_steps(torch, stream, fn, steps, warmup, barrier=None):
+    """(mean ms of fn() per step, mean ms of its first phase) with CUDA events on `stream`;
+    `barrier` (several ranks) lines the ranks up after the warm-up."""
     for _ in range(warmup):
         fn(None)
     torch.cuda.synchronize()
+    if barrier is not None:
+        barrier()
+        torch.cuda.synchronize()
     tot, first = [], []
     for _ in range(steps):
         s, m, e = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -338,13 +342,32 @@ def _c4_system(args):
     return A.outer, A.inner, A.values, ordering.nested_dissection(A)
 
 
-def c4_systems(count=C4_COUNT):
-    """The batch: Delaunay meshes of m ~ U[500, 20000] uniform points, cotangent Laplacian + 1e-3 lumped mass."""
+def c4_sizes(count=C4_COUNT):
+    """Point counts m ~ U[500, 20000] of the batch's meshes (system s has seed C4_SEED + s)."""
+    return np.random.default_rng(C4_SEED).integers(C4_MIN, C4_MAX + 1, size=count)
+
+
+def c4_systems(count=C4_COUNT, which=None):
+    """The batch (or the systems `which` of it): Delaunay meshes of m ~ U[500, 20000] uniform points,
+    cotangent Laplacian + 1e-3 lumped mass."""
     import multiprocessing as mp
 
-    ms = np.random.default_rng(C4_SEED).integers(C4_MIN, C4_MAX + 1, size=count)
+    ms = c4_sizes(count)
+    jobs = [(s, ms[s]) for s in (range(count) if which is None else which)]
     with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
-        return pool.map(_c4_system, list(enumerate(ms)), chunksize=8)
+        return pool.map(_c4_system, jobs, chunksize=8)
+
+
+def shard_by_work(work, world):
+    """Independent systems over `world` GPUs with no exchange: largest estimated work first, each to
+    the least-loaded rank (ties: lowest index, lowest rank).  Returns each rank's sorted indices."""
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for s in sorted(range(len(work)), key=lambda i: (-float(work[i]), i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(s)
+        load[r] += float(work[s])
+    return [sorted(p) for p in parts]
 
 
 def run_c4(args):
@@ -352,13 +375,27 @@ def run_c4(args):
     FP32 factor + FP64 refinement to max(C4_TARGET, 2 x the residual a plain FP64 solve attains on the
     batch), 1 RHS each.  When the refinement breaks down on a system
     whose conditioning is beyond FP32, the handle falls back to an FP64 factor (reported in the line)."""
-    systems = c4_systems(args.batch or C4_COUNT)       # process pool before any GPU call
+    count = args.batch or C4_COUNT
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    # several GPUs: the systems shard by estimated factor work (~m^1.5 for a 2D mesh under nested
+    # dissection), no collective on the data path
+    mine = shard_by_work(c4_sizes(count).astype(np.float64) ** 1.5, world)[rank] if world > 1 else None
+    systems = c4_systems(count, mine)                  # process pool before any GPU call
     import torch
     from tensors_b200 import build as tb_build
     from tensors_b200.cholesky import BatchedCholesky
 
     tb_build.build()
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(dev)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
     t0 = time.perf_counter()
     b = BatchedCholesky([(o, i, p) for o, i, v, p in systems])
     b.handle.SetSchedule(args.schedule or "levels")
@@ -388,8 +425,9 @@ def run_c4(args):
             mid.record(stream)
         b.Solve(B, X)
 
-    with ClockSampler(0) as clocks:
-        t, tf = _time_steps(torch, stream, step, args.steps, args.warmup)
+    with ClockSampler(local) as clocks:
+        t, tf = _time_steps(torch, stream, step, args.steps, args.warmup,
+                            barrier=dist.barrier if dist is not None else None)
     stream.synchronize()
     it, rr = b.handle.RefinementInfo()
     R = b.handle.Residual(B, X)
@@ -397,16 +435,29 @@ def run_c4(args):
     relres = float(torch.linalg.norm(R) / torch.linalg.norm(B))
     F, nnz_u = b.handle.FlopCount()
     flops = F + 4.0 * nnz_u
+    n_systems = len(systems)
+    if dist is not None:
+        # the job: every rank's work over the slowest rank's time
+        t, tf = max_over_ranks(dist, t, dev), max_over_ranks(dist, tf, dev)
+        relres, target = max_over_ranks(dist, relres, dev), max_over_ranks(dist, target, dev)
+        tot = torch.tensor([flops, F, float(n_systems), float(n)], dtype=torch.float64, device=dev)
+        dist.all_reduce(tot)
+        flops, F, n_systems, n = float(tot[0]), float(tot[1]), int(tot[2]), int(tot[3])
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return 0
     line = {
-        "metric": f"batched factor+solve GFLOP/s, {len(systems)} Delaunay systems, FP32 factor + FP64 refinement "
+        "metric": f"batched factor+solve GFLOP/s, {n_systems} Delaunay systems, FP32 factor + FP64 refinement "
                   f"to max({C4_TARGET:g}, 2 x the FP64 direct residual)",
-        "value": flops / (t * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "value": flops / (t * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"{len(systems)} 2D Delaunay meshes, m ~ U[{C4_MIN}, {C4_MAX}] points, cotangent "
+        "config": {"workload": f"{n_systems} 2D Delaunay meshes, m ~ U[{C4_MIN}, {C4_MAX}] points, cotangent "
                                "Laplacian + 1e-3 lumped mass, nested dissection each, 1 RHS each",
+                   "parallelism": f"{world} GPU(s), systems sharded by estimated factor work, no collective",
                    "rows": n, "factor_gflop": F / 1e9, "factor_ms": tf, "solve_ms": t - tf,
-                   "systems_per_s": len(systems) / (t * 1e-3), "refinement": [it, rr], "relres": relres,
+                   "systems_per_s": n_systems / (t * 1e-3), "refinement": [it, rr], "relres": relres,
                    "target": target, "fp64_direct_relres": attainable,
                    "perturbed_pivots": b.handle.PerturbedPivots(),
                    "precision_in_use": list(b.handle.PrecisionInUse()),

@@ -1,7 +1,8 @@
 """The multi-GPU bench path without GPUs: N independent replicas, timed by the
 slowest rank (max over ranks), whole-job throughput = N x one replica's work
 over that time; the reference arm runs on rank 0 only.  Two gloo ranks on
-CPU stand in for two GPUs."""
+CPU stand in for two GPUs.  The batch workload's partition of systems over
+ranks is checked directly."""
 from __future__ import annotations
 
 import json
@@ -10,6 +11,7 @@ import socket
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -68,3 +70,21 @@ def test_replica_throughput_is_linear_in_ranks():
     assert bench.replica_throughput(1e9, 1000.0, 1) == pytest.approx(1.0)
     assert bench.replica_throughput(1e9, 1000.0, 8) == pytest.approx(8.0)
     json.dumps({"v": bench.replica_throughput(3e9, 7.0, 4)})
+
+
+def test_batch_shards_cover_every_system_once_and_balance_the_work():
+    rng = np.random.default_rng(0)
+    work = rng.integers(1, 1000, 137).astype(float)
+    for world in (1, 2, 3, 8):
+        parts = bench.shard_by_work(work, world)
+        assert len(parts) == world
+        assert sorted(i for p in parts for i in p) == list(range(len(work)))
+        assert all(p == sorted(p) for p in parts)
+        loads = [work[p].sum() for p in parts]
+        assert max(loads) - min(loads) <= work.max()           # greedy largest-first bound
+        assert parts == bench.shard_by_work(work, world)        # deterministic
+    # the C4 batch over 2-8 GPUs: within 1% of an even split
+    w = bench.c4_sizes(2000).astype(float) ** 1.5
+    for world in (2, 4, 8):
+        loads = [w[p].sum() for p in bench.shard_by_work(w, world)]
+        assert max(loads) / (w.sum() / world) < 1.01
