@@ -390,3 +390,18 @@ def test_get_u_through_the_c_abi_matches_the_python_assembly():
     U = chol.GetU()
     U.sort_indices()
     assert np.array_equal(outer, U.indptr) and np.array_equal(inner, U.indices) and np.array_equal(values, U.data)
+
+
+def test_left_looking_setting_gives_the_multifrontal_factor_bitwise():
+    from tensors_b200.cholesky import FactorizationMethod
+
+    A = M.delaunay_laplacian(1500, 4)
+    perm = O.nested_dissection(A, 16)
+    vals = []
+    for method in (FactorizationMethod.Multifrontal, FactorizationMethod.LeftLooking):
+        c = CholeskyDecomposition(A.outer, A.inner, perm)
+        c.SetFactorizationMethod(method)
+        assert c.NumericFactorization(A.values, 1e-3) == 0
+        vals.append(c.FactorValues())
+    for a, b in zip(*vals):
+        assert np.array_equal(a, b)

@@ -96,3 +96,33 @@ def test_reference_lower_solve_runs_the_upper_solve():
     r.factor(A.values, 0.1)
     B = np.random.default_rng(3).standard_normal((A.n, 2))
     assert np.abs(r.lower_solve(B) - o.solve(B, which="upper")).max() <= 1e-12 * np.abs(B).max() * 100
+
+
+@pytest.mark.parametrize("name,A,perm", [c[:3] for c in CASES[:4]], ids=[c[0] for c in CASES[:4]])
+def test_reference_left_looking_computes_the_multifrontal_factor(name, A, perm):
+    """The reference's two numeric methods (CholeskyDecomposition.hpp:126-130, LeftLooking.hpp:171) give
+    the same factor to rounding; this library runs one factorization for both settings."""
+    out = []
+    for method in ("multifrontal", "left_looking"):
+        r = oracle.RefCholesky(A.n, A.outer, A.inner, perm, method=method)
+        assert r.factor(A.values, 1e-3) == 0
+        out.append(r.factor_values())
+    for a, b in zip(*out):
+        assert a.shape == b.shape
+        if a.size:
+            assert np.abs(a - b).max() <= 1e-12 * max(1.0, np.abs(a).max())
+
+
+def test_factorization_method_setter_keeps_the_symbolic_structure():
+    from tensors_b200.cholesky import CholeskyDecomposition, FactorizationMethod
+
+    A = M.delaunay_laplacian(1500, 4)
+    perm = O.nested_dissection(A, 16)
+    arrays = []
+    for method in (FactorizationMethod.Multifrontal, FactorizationMethod.LeftLooking):
+        c = CholeskyDecomposition(A.outer, A.inner, perm)
+        c.SetFactorizationMethod(method)
+        c.SymbolicFactorization()
+        arrays.append([c.SymbolicArray(k) for k in ("SN_rp", "SN_outer", "SN_inner", "value_perm")])
+    for a, b in zip(*arrays):
+        assert np.array_equal(a, b)
