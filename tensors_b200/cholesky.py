@@ -289,8 +289,9 @@ class CholeskyDecomposition:
 
             B = B.contiguous()
             if X is None:
-                X = torch.zeros_like(B)
+                X = torch.zeros_like(B)           # the initial guess, if one is asked for: 0
                 beta = 0.0
+                torch.cuda.current_stream().synchronize()   # the handle's stream is not ordered after torch's
             v = 0 if values is None else values.contiguous().data_ptr()
             st = lib().tb_chol_cg_device(self._h, v, float(reg), float(alpha), B.data_ptr(), k, float(beta),
                                          X.data_ptr(), k, k, float(relative_tolerance), int(max_iter),
