@@ -1,6 +1,7 @@
 // Device execution plan; see plan.hpp.
 
 #include "plan.hpp"
+#include "parallel.hpp"
 
 #include <stdexcept>
 #include "common.hpp"
@@ -282,36 +283,39 @@ void Plan::build( const Symbolic & sym )
     }
 
     // ------------------------------------------------------- assembly map
-    asm_src.clear();
-    asm_dst.clear();
     {
-        I64 upper_count = 0;
-        for( I32 i = 0; i < n; ++i ) { upper_count += sym.outer[i+1] - sym.diag[i]; }
-        asm_src.reserve( static_cast<size_t>(upper_count) );
-        asm_dst.reserve( static_cast<size_t>(upper_count) );
-        for( I32 i = 0; i < n; ++i )
+        // row i's upper entries occupy [first[i], first[i + 1]): rows fill in parallel
+        std::vector<I64> first( static_cast<size_t>(n) + 1, 0 );
+        for( I32 i = 0; i < n; ++i ) { first[static_cast<size_t>(i) + 1] = first[static_cast<size_t>(i)] + (sym.outer[i+1] - sym.diag[i]); }
+        asm_src.assign( static_cast<size_t>( first[static_cast<size_t>(n)] ), 0 );
+        asm_dst.assign( static_cast<size_t>( first[static_cast<size_t>(n)] ), 0 );
+        parallel_rows( n, [&]( I64 b, I64 e )
         {
-            const I32 f = front_of_sn[ sym.row_to_sn[i] ];
-            const I32 rb = front_row0[f], re = rb + front_n0[f];
-            const I32 * cols = sym.sn_inner.data() + front_cols[f];
-            I32 l = 0;
-            for( I64 k = sym.diag[i]; k < sym.outer[i+1]; ++k )
+            for( I32 i = static_cast<I32>( b ); i < static_cast<I32>( e ); ++i )
             {
-                const I32 j = sym.inner[k];
-                I64 dst;
-                if( j < re )
+                const I32 f = front_of_sn[ sym.row_to_sn[i] ];
+                const I32 rb = front_row0[f], re = rb + front_n0[f];
+                const I32 * cols = sym.sn_inner.data() + front_cols[f];
+                I32 l = 0;
+                I64 out = first[static_cast<size_t>(i)];
+                for( I64 k = sym.diag[i]; k < sym.outer[i+1]; ++k, ++out )
                 {
-                    dst = front_u0[f] + static_cast<I64>(front_ld0[f]) * (i - rb) + (j - rb);
+                    const I32 j = sym.inner[k];
+                    I64 dst;
+                    if( j < re )
+                    {
+                        dst = front_u0[f] + static_cast<I64>(front_ld0[f]) * (i - rb) + (j - rb);
+                    }
+                    else
+                    {
+                        while( cols[l] < j ) { ++l; }
+                        dst = front_u1[f] + static_cast<I64>(front_ld1[f]) * (i - rb) + l;
+                    }
+                    asm_src[static_cast<size_t>(out)] = sym.value_perm[k];
+                    asm_dst[static_cast<size_t>(out)] = static_cast<I64>( static_cast<std::uint64_t>(dst) | (j == i ? kDiagFlag : 0ull) );
                 }
-                else
-                {
-                    while( cols[l] < j ) { ++l; }
-                    dst = front_u1[f] + static_cast<I64>(front_ld1[f]) * (i - rb) + l;
-                }
-                asm_src.push_back( sym.value_perm[k] );
-                asm_dst.push_back( static_cast<I64>( static_cast<std::uint64_t>(dst) | (j == i ? kDiagFlag : 0ull) ) );
             }
-        }
+        } );
     }
 
     // ------------------------------------------ export to reference layout

@@ -6,6 +6,7 @@
 // supernode sweep parameterised by the merge rule.
 
 #include "symbolic.hpp"
+#include "parallel.hpp"
 #include "common.hpp"
 
 #include <algorithm>
@@ -19,22 +20,6 @@ namespace
 
 using I32 = std::int32_t;
 using I64 = std::int64_t;
-
-// Runs body(begin, end) over [0, count) split across the host's cores.
-template<typename Body>
-void parallel_rows( I64 count, Body && body )
-{
-    const unsigned hw = std::max( 1u, std::thread::hardware_concurrency() );
-    const I64 threads = std::min<I64>( hw, std::max<I64>( 1, count / 65536 ) );
-    if( threads <= 1 ) { body( I64(0), count ); return; }
-    std::vector<std::thread> pool;
-    for( I64 t = 0; t < threads; ++t )
-    {
-        const I64 b = count * t / threads, e = count * (t + 1) / threads;
-        pool.emplace_back( [&body, b, e]() { body( b, e ); } );
-    }
-    for( auto & th : pool ) { th.join(); }
-}
 
 // Sorted union of two strictly increasing runs (UniteSortedBuffers.hpp:6).
 void sorted_union( const std::vector<I32> & a, const I32 * b, I64 nb, std::vector<I32> & out )
