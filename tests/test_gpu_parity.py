@@ -45,6 +45,7 @@ def _cases():
     out.append(("grid3d-12", A, O.nested_dissection(A, 16), 0.0, 1e-8))
     A = M.grid_laplacian_3d(18, 5, 1e-2)              # fronts with several panels and > 256 rest columns
     out.append(("grid3d-18", A, O.nested_dissection(A, 64), 0.0, TOL))
+    out.append(("grid3d-18-graph", A, O.graph_nested_dissection(A, 64), 0.0, TOL))   # ordering from the pattern
     A = M.vector_laplacian_3d(6, 8)
     out.append(("vector3d-6", A, O.nested_dissection(A, 16), 1e-2, TOL))
     A = M.delaunay_laplacian(3000, 9)                 # shift 1e-3 * lumped mass: kappa ~ 1e9

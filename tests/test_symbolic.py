@@ -32,6 +32,12 @@ def _cases():
     A = M.delaunay_laplacian(2500, 5)
     out.append(("delaunay-2500", A, O.nested_dissection(A, 16)))
     out.append(("delaunay-2500-rand", A, np.random.default_rng(9).permutation(A.n).astype(np.int32)))
+    # the ordering from the pattern alone (other front shapes than the geometric one)
+    out.append(("delaunay-2500-graph", A, O.graph_nested_dissection(A, 16)))
+    A = M.grid_laplacian_3d(14, 3)
+    out.append(("grid3d-14-graph", A, O.graph_nested_dissection(A, 32)))
+    A = M.vector_laplacian_3d(5, 4)
+    out.append(("vector3d-5-graph", A, O.graph_nested_dissection(A, 8)))
     return out
 
 
