@@ -101,3 +101,14 @@ def test_matrix_without_coordinates_is_ordered_from_its_pattern():
     p = O.nested_dissection(bare)
     assert np.array_equal(p, O.graph_nested_dissection(A))
     assert _flops(A, p) < 0.05 * _flops(A, O.identity_ordering(A.n))
+
+
+def test_best_nested_dissection_takes_the_one_with_fewer_flops():
+    grid = M.grid_laplacian_3d(16, 2)                  # the pattern's ordering wins here
+    vec = M.vector_laplacian_3d(10, 3)                 # the geometric one wins here
+    for A in (grid, vec):
+        best = O.best_nested_dissection(A)
+        f = [_flops(A, O.nested_dissection(A)), _flops(A, O.graph_nested_dissection(A))]
+        assert _flops(A, best) == min(f)
+    assert np.array_equal(O.best_nested_dissection(grid), O.graph_nested_dissection(grid))
+    assert np.array_equal(O.best_nested_dissection(vec), O.nested_dissection(vec))
