@@ -54,7 +54,7 @@ _ARRAYS = {
 
 def _check(status: int) -> int:
     if status < 0:
-        raise TBError(status, lib().tb_last_error().decode())
+        raise TBError(status, lib().tb_last_error().decode("utf-8", errors="replace"))
     return status
 
 

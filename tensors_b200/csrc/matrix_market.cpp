@@ -74,6 +74,14 @@ const char * skip_blanks( const char * p, const char * end )
     return p;
 }
 
+// Text of the file quoted in an error message: printable ASCII only.
+std::string quoted( const char * b, const char * e )
+{
+    std::string s( b, static_cast<size_t>( std::min<std::ptrdiff_t>( e - b, 80 ) ) );
+    for( char & c : s ) { if( static_cast<unsigned char>( c ) < 32 || static_cast<unsigned char>( c ) > 126 ) { c = '?'; } }
+    return s;
+}
+
 std::string lower( std::string s )
 {
     for( char & c : s ) { c = static_cast<char>( std::tolower( static_cast<unsigned char>( c ) ) ); }
@@ -123,7 +131,7 @@ void parse_entries( const char * begin, const char * end, bool pattern, I32 rows
             if( q != nullptr && !pattern ) { q = parse_real( q, eol, a ); }
             if( q == nullptr )
             {
-                c.error = "malformed entry line \"" + std::string( p, static_cast<size_t>( std::min<I64>( eol - p, 80 ) ) ) + "\"";
+                c.error = "malformed entry line \"" + quoted( p, eol ) + "\"";
                 return;
             }
             if( i < 1 || i > rows || j < 1 || j > cols )
@@ -136,7 +144,7 @@ void parse_entries( const char * begin, const char * end, bool pattern, I32 rows
             c.j.push_back( static_cast<I32>( j - 1 ) );
             c.a.push_back( a );
         }
-        p = eol + 1;
+        p = eol < end ? eol + 1 : end;
     }
 }
 
@@ -188,18 +196,18 @@ extern "C" int tb_matrix_market_read( const char * path, int32_t thread_count, i
     if( words[1] != "matrix" ) { return fail( TB_ERR_FORMAT, "tb_matrix_market_read: second word of the banner is not \"matrix\"" ); }
     if( words[2] != "coordinate" )
     {
-        return fail( TB_ERR_FORMAT, "tb_matrix_market_read: \"" + words[2] + "\" storage is not supported (coordinate only)" );
+        return fail( TB_ERR_FORMAT, "tb_matrix_market_read: \"" + quoted( words[2].data(), words[2].data() + words[2].size() ) + "\" storage is not supported (coordinate only)" );
     }
     const std::string & field = words[3];
     if( field != "real" && field != "integer" && field != "pattern" && field != "double" )
     {
-        return fail( TB_ERR_FORMAT, "tb_matrix_market_read: field \"" + field + "\" is not supported for real matrices" );
+        return fail( TB_ERR_FORMAT, "tb_matrix_market_read: field \"" + quoted( field.data(), field.data() + field.size() ) + "\" is not supported for real matrices" );
     }
     const bool pattern = field == "pattern";
     const std::string & symmetry = words[4];
     if( symmetry != "general" && symmetry != "symmetric" )
     {
-        return fail( TB_ERR_FORMAT, "tb_matrix_market_read: symmetry \"" + symmetry + "\" is not supported" );
+        return fail( TB_ERR_FORMAT, "tb_matrix_market_read: symmetry \"" + quoted( symmetry.data(), symmetry.data() + symmetry.size() ) + "\" is not supported" );
     }
     const bool symmetric = symmetry == "symmetric";
 

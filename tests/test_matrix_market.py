@@ -252,3 +252,16 @@ def test_factor_and_solve_a_matrix_read_from_a_file(tmp_path):
     X = c.Solve(rhs)
     R = rhs - M.csr_matvec(A, X)
     assert np.linalg.norm(R) <= 1e-12 * np.linalg.norm(rhs)
+
+
+def test_binary_garbage_in_a_file_gives_a_status_not_a_decoding_error(tmp_path):
+    # bytes that are not UTF-8 inside a malformed line and inside the banner
+    p = tmp_path / "bin.mtx"
+    p.write_bytes(b"%%MatrixMarket matrix coordinate real general\n2 2 1\n1 \xee\xff 1.0\n")
+    with pytest.raises(TBError) as e:
+        read_matrix_market(p)
+    assert e.value.status == TB_ERR_FORMAT and "?" in str(e.value)
+    p.write_bytes(b"%%MatrixMarket matrix coordinate r\xe9al general\n1 1 1\n1 1 1.0\n")
+    with pytest.raises(TBError) as e:
+        read_matrix_market(p)
+    assert e.value.status == TB_ERR_FORMAT
