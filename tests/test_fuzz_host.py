@@ -1,5 +1,6 @@
 """Seeded fuzzing of the host boundary (no GPU): corrupted patterns and
-permutations through the constructor, symbolic analysis, plan and plan check;
+permutations through the constructor (single systems and batches), symbolic
+analysis, plan and plan check;
 mutated MatrixMarket files through the reader; adversarial graphs through the
 pattern-only nested dissection.  Every input either works or fails with a
 status (TBError); nothing crashes, and what is accepted is consistent."""
@@ -92,3 +93,31 @@ def test_adversarial_graphs_are_ordered():
         p = O.graph_nested_dissection(G, 64)
         assert O.is_permutation(p, G.n)
         assert np.array_equal(p, O.graph_nested_dissection(G, 64, thread_count=1))
+
+
+def test_corrupted_systems_in_a_batch():
+    from tensors_b200.cholesky import BatchedCholesky
+
+    rng = np.random.default_rng(6)
+    mats = [M.grid_laplacian_2d(int(g), 1.0) for g in (3, 5, 7, 4)]
+    rejected = 0
+    for _ in range(200):
+        systems = []
+        for A in mats:
+            outer, inner, perm = A.outer.copy(), A.inner.copy(), O.nested_dissection(A, 8).copy()
+            if rng.random() < 0.3:
+                kind = rng.integers(0, 3)
+                if kind == 0:
+                    inner[rng.integers(0, len(inner))] = rng.integers(-3, A.n + 3)
+                elif kind == 1:
+                    perm[rng.integers(0, len(perm))] = rng.integers(-2, A.n + 2)
+                else:
+                    outer[rng.integers(1, len(outer))] += rng.integers(-2, 3)
+            systems.append((outer, inner, perm))
+        try:
+            b = BatchedCholesky(systems)
+            b.handle.SymbolicFactorization()
+            b.handle.CheckPlan()
+        except TBError:
+            rejected += 1
+    assert 0 < rejected < 200
