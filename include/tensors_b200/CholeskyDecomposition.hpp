@@ -172,6 +172,18 @@ public:
     std::vector<Int>  Permutation() const          { return Array<Int>( TB_ARRAY_PERM ); }
     std::vector<Int>  InversePermutation() const   { return Array<Int>( TB_ARRAY_PERM_INV ); }
     std::vector<LInt> ValuePermutation() const     { return Array<LInt>( TB_ARRAY_VALUE_PERM ); }
+
+    // GetPermutation / GetValuePermutation (InputOutput.hpp:304-312) under the
+    // reference's names: the permutation after postordering as an object with
+    // the accessors its callers use, and A's value permutation.
+    struct Permutation_T
+    {
+        std::vector<Int> p, p_inv;
+        const std::vector<Int> & GetPermutation() const { return p; }
+        const std::vector<Int> & GetInversePermutation() const { return p_inv; }
+    };
+    Permutation_T GetPermutation() const { return Permutation_T{ Permutation(), InversePermutation() }; }
+    std::vector<LInt> GetValuePermutation() const { return ValuePermutation(); }
     std::vector<Int>  AssemblyTreeParents() const  { return Array<Int>( TB_ARRAY_ATREE_PARENTS ); }
     std::vector<Int>  EliminationTreeParents() const { return Array<Int>( TB_ARRAY_ETREE_PARENTS ); }
 

@@ -56,6 +56,10 @@ int main( int argc, char ** argv )
     CholeskyDecomposition S( outer.data(), inner.data(), p.data(), n, 1 );
     S.SymbolicFactorization();
     std::printf( "sn_count %d\n", S.SN_Count() );
+    // the reference's accessor shapes: S.GetPermutation().GetPermutation() and its inverse
+    const auto P = S.GetPermutation();
+    for( int i = 0; i < n; ++i ) { if( P.GetInversePermutation()[P.GetPermutation()[i]] != i ) { return 2; } }
+    if( static_cast<int64_t>( S.GetValuePermutation().size() ) != S.NonzeroCount() ) { return 3; }
     if( !numeric ) { return 0; }
 
     const int status = S.NumericFactorization( val.data(), 0.0 );
