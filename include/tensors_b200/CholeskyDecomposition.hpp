@@ -52,12 +52,14 @@ public:
     // symbolic phase.
     CholeskyDecomposition( const LInt * A_outer, const Int * A_inner, const Int * p,
                            Int n, Int thread_count )
+    : threads_( thread_count )
     {
         Check( tb_chol_create( &h_, n, A_outer, A_inner, p, thread_count ) );
     }
 
     // Matrix already permuted, ctor CholeskyDecomposition.hpp:350-371.
     CholeskyDecomposition( const LInt * A_outer, const Int * A_inner, Int n, Int thread_count )
+    : threads_( thread_count )
     {
         Check( tb_chol_create( &h_, n, A_outer, A_inner, nullptr, thread_count ) );
     }
@@ -66,13 +68,17 @@ public:
 
     CholeskyDecomposition( const CholeskyDecomposition & ) = delete;
     CholeskyDecomposition & operator=( const CholeskyDecomposition & ) = delete;
-    CholeskyDecomposition( CholeskyDecomposition && o ) noexcept : h_( std::exchange( o.h_, nullptr ) ) {}
+    CholeskyDecomposition( CholeskyDecomposition && o ) noexcept
+    :   h_( std::exchange( o.h_, nullptr ) ), strategy_( o.strategy_ ), threshold_( o.threshold_ ), method_( o.method_ ),
+        threads_( o.threads_ ), cg_iter_( o.cg_iter_ ), relres_( std::move( o.relres_ ) ) {}
     CholeskyDecomposition & operator=( CholeskyDecomposition && o ) noexcept
     {
         if( this != &o )
         {
             if( h_ != nullptr ) { tb_chol_destroy( h_ ); }
             h_ = std::exchange( o.h_, nullptr );
+            strategy_ = o.strategy_; threshold_ = o.threshold_; method_ = o.method_; threads_ = o.threads_;
+            cg_iter_ = o.cg_iter_; relres_ = std::move( o.relres_ );
         }
         return *this;
     }
@@ -81,12 +87,19 @@ public:
     void SetSupernodeStrategy( SupernodeStrategy_T s )
     {
         Check( tb_chol_set_supernode_strategy( h_, static_cast<int32_t>( s ) ) );
+        strategy_ = s;
     }
-    void SetAmalgamationThreshold( Int t ) { Check( tb_chol_set_amalgamation_threshold( h_, t ) ); }
+    void SetAmalgamationThreshold( Int t ) { Check( tb_chol_set_amalgamation_threshold( h_, t ) ); threshold_ = t; }
     void SetFactorizationMethod( FactorizationMethod_T m )
     {
         Check( tb_chol_set_factorization_method( h_, static_cast<int32_t>( m ) ) );
+        method_ = m;
     }
+    // The settings' getters (InputOutput.hpp) and the thread count given to the constructor.
+    SupernodeStrategy_T GetSupernodeStrategy() const { return strategy_; }
+    Int AmalgamationThreshold() const { return threshold_; }
+    FactorizationMethod_T GetFactorizationMethod() const { return method_; }
+    Int ThreadCount() const { return threads_; }
 
     // CholeskyDecomposition/Symbolic.hpp:3-66.
     void SymbolicFactorization() { Check( tb_chol_symbolic( h_ ) ); }
@@ -213,6 +226,8 @@ public:
 
     // LogDeterminant (InputOutput.hpp:294-297), WriteFactorDiagonal (:238-257).
     Scal LogDeterminant() const { Scal v = 0; Check( tb_chol_log_det( h_, &v ) ); return v; }
+    // log det U = half of log det A (InputOutput.hpp:259-292).
+    Scal FactorLogDeterminant() const { return 0.5 * LogDeterminant(); }
     void WriteFactorDiagonal( Scal * diag ) const { Check( tb_chol_factor_diagonal( h_, diag ) ); }
 
     // Stream of the handle (a cudaStream_t).
@@ -232,6 +247,10 @@ private:
     }
 
     tb_chol * h_ = nullptr;
+    SupernodeStrategy_T strategy_ = SupernodeStrategy_T::Maximal;     // the reference's defaults
+    Int threshold_ = 4;
+    FactorizationMethod_T method_ = FactorizationMethod_T::Multifrontal;
+    Int threads_ = 1;
     Int cg_iter_ = 0;
     std::vector<Scal> relres_;
 };

@@ -60,6 +60,13 @@ int main( int argc, char ** argv )
     const auto P = S.GetPermutation();
     for( int i = 0; i < n; ++i ) { if( P.GetInversePermutation()[P.GetPermutation()[i]] != i ) { return 2; } }
     if( static_cast<int64_t>( S.GetValuePermutation().size() ) != S.NonzeroCount() ) { return 3; }
+    // settings read back with the reference's getters, and across a move
+    S.SetAmalgamationThreshold( 4 );
+    CholeskyDecomposition T( std::move( S ) );
+    if( T.AmalgamationThreshold() != 4 || T.ThreadCount() != 1
+        || T.GetSupernodeStrategy() != tensors_b200::Sparse::SupernodeStrategy_T::Maximal
+        || T.GetFactorizationMethod() != tensors_b200::Sparse::FactorizationMethod_T::Multifrontal ) { return 4; }
+    S = std::move( T );
     if( !numeric ) { return 0; }
 
     const int status = S.NumericFactorization( val.data(), 0.0 );
