@@ -79,6 +79,7 @@ class CholeskyDecomposition:
         self._outer = np.ascontiguousarray(outer, dtype=np.int64)
         self._inner = np.ascontiguousarray(inner, dtype=np.int32)
         self._n = int(n) if n is not None else len(self._outer) - 1
+        self._threads = int(thread_count)
         self._perm = None if perm is None else np.ascontiguousarray(perm, dtype=np.int32)
         if self._perm is not None and self._perm.shape != (self._n,):
             raise TBError(-1, "permutation has the wrong length")
@@ -122,12 +123,28 @@ class CholeskyDecomposition:
     # ---------------------------------------------------------------- setup
     def SetSupernodeStrategy(self, strategy) -> None:
         _check(lib().tb_chol_set_supernode_strategy(self._h, int(strategy)))
+        self._strategy = SupernodeStrategy(int(strategy))
 
     def SetAmalgamationThreshold(self, threshold: int) -> None:
         _check(lib().tb_chol_set_amalgamation_threshold(self._h, int(threshold)))
+        self._threshold = int(threshold)
 
     def SetFactorizationMethod(self, method) -> None:
         _check(lib().tb_chol_set_factorization_method(self._h, int(method)))
+        self._method = FactorizationMethod(int(method))
+
+    # the settings' getters (InputOutput.hpp), the reference's defaults until set
+    def GetSupernodeStrategy(self) -> SupernodeStrategy:
+        return getattr(self, "_strategy", SupernodeStrategy.Maximal)
+
+    def AmalgamationThreshold(self) -> int:
+        return getattr(self, "_threshold", 4)
+
+    def GetFactorizationMethod(self) -> FactorizationMethod:
+        return getattr(self, "_method", FactorizationMethod.Multifrontal)
+
+    def ThreadCount(self) -> int:
+        return self._threads
 
     def SetUseGraph(self, enabled: bool) -> None:
         _check(lib().tb_chol_set_graph(self._h, 1 if enabled else 0))

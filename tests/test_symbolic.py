@@ -153,3 +153,17 @@ def test_u_nonzero_count_matches_the_flop_count_structure():
         n0, n1 = np.diff(rp), np.diff(so)
         assert c.UNonzeroCount() == int(np.sum(n0 * (n0 + 1) // 2 + n0 * n1))
         assert c.UNonzeroCount() == int(c.FlopCount()[1])
+
+
+def test_settings_getters_follow_the_setters():
+    from tensors_b200.cholesky import FactorizationMethod, SupernodeStrategy
+
+    A = M.grid_laplacian_2d(8, 1.0)
+    c = CholeskyDecomposition(A.outer, A.inner, thread_count=2)
+    assert (c.GetSupernodeStrategy(), c.AmalgamationThreshold(), c.GetFactorizationMethod(), c.ThreadCount()) == \
+        (SupernodeStrategy.Maximal, 4, FactorizationMethod.Multifrontal, 2)
+    c.SetSupernodeStrategy(SupernodeStrategy.Amalgamated)
+    c.SetAmalgamationThreshold(7)
+    c.SetFactorizationMethod(FactorizationMethod.LeftLooking)
+    assert (c.GetSupernodeStrategy(), c.AmalgamationThreshold(), c.GetFactorizationMethod()) == \
+        (SupernodeStrategy.Amalgamated, 7, FactorizationMethod.LeftLooking)
