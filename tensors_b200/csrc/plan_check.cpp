@@ -8,8 +8,10 @@
 
 #include "plan.hpp"
 #include "plan_check.hpp"
+#include "parallel.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <string>
@@ -27,6 +29,27 @@ bool in_range( I64 first, I64 last_inclusive, I64 size )
     return first >= 0 && last_inclusive >= first && last_inclusive < size;
 }
 
+// The lowest index in [0, count) for which bad(i) holds, or -1; the range is
+// split over the host threads (the message is then rebuilt for that index, so
+// the report does not depend on the threads).
+template<typename Bad>
+I64 first_bad( I64 count, Bad && bad )
+{
+    std::atomic<I64> first{ count };
+    parallel_rows( count, [&]( I64 b, I64 e )
+    {
+        for( I64 i = b; i < e && i < first.load( std::memory_order_relaxed ); ++i )
+        {
+            if( !bad( i ) ) { continue; }
+            I64 cur = first.load();
+            while( i < cur && !first.compare_exchange_weak( cur, i ) ) {}
+            break;
+        }
+    } );
+    const I64 f = first.load();
+    return f < count ? f : -1;
+}
+
 } // namespace
 
 std::string check_plan( const Symbolic & sym, const Plan & pl )
@@ -38,11 +61,17 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
     const I64 rec_size = sym.sn_rec_ptr[sym.sn_count];
 
     if( pl.asm_src.size() != pl.asm_dst.size() ) { return "assembly map sizes differ"; }
-    for( size_t e = 0; e < pl.asm_src.size(); ++e )
     {
-        const I64 d = static_cast<I64>( static_cast<std::uint64_t>( pl.asm_dst[e] ) & (kDiagFlag - 1) );
-        if( pl.asm_src[e] < 0 || pl.asm_src[e] >= nnz ) { return "assembly source out of range at " + std::to_string( e ); }
-        if( d < 0 || d >= pl.u0_size + pl.u1_size ) { return "assembly target out of range at " + std::to_string( e ); }
+        auto entry = [&]( I64 e ) -> std::string
+        {
+            const I64 d = static_cast<I64>( static_cast<std::uint64_t>( pl.asm_dst[static_cast<size_t>( e )] ) & (kDiagFlag - 1) );
+            const I64 src = pl.asm_src[static_cast<size_t>( e )];
+            if( src < 0 || src >= nnz ) { return "assembly source out of range at " + std::to_string( e ); }
+            if( d < 0 || d >= pl.u0_size + pl.u1_size ) { return "assembly target out of range at " + std::to_string( e ); }
+            return std::string();
+        };
+        const I64 bad = first_bad( static_cast<I64>( pl.asm_src.size() ), [&]( I64 e ) { return !entry( e ).empty(); } );
+        if( bad >= 0 ) { return entry( bad ); }
     }
     for( size_t i = 0; i < pl.diag_offset.size(); ++i )
     {
@@ -169,17 +198,22 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             for( I32 f : dies[static_cast<size_t>( h )] ) { live.erase( pl.front_v[static_cast<size_t>( f )] ); }
         }
     }
-    for( size_t k = 0; k < pl.gemm.size(); ++k )
     {
-        const GemmTask & t = pl.gemm[k];
-        auto at = [&]() { return " (gemm task " + std::to_string( k ) + ")"; };   // built only on failure
-        if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad gemm dimensions" + at(); }
-        if( t.M > t.lda || t.N > t.ldb || t.N > t.ldc ) { return "gemm leading dimension too small" + at(); }
-        // 16-byte copies of FP64 (2 entries) and FP32 (4 entries) storage
-        if( (t.a | t.b | t.c) % 4 != 0 || (t.lda | t.ldb | t.ldc) % 4 != 0 ) { return "gemm operand not 16-byte aligned" + at(); }
-        if( !in_range( t.a, t.a + static_cast<I64>(t.K - 1) * t.lda + t.M - 1, arena ) ) { return "gemm A out of range" + at(); }
-        if( !in_range( t.b, t.b + static_cast<I64>(t.K - 1) * t.ldb + t.N - 1, arena ) ) { return "gemm B out of range" + at(); }
-        if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at(); }
+        auto task = [&]( I64 k ) -> std::string
+        {
+            const GemmTask & t = pl.gemm[static_cast<size_t>( k )];
+            auto at = [&]() { return " (gemm task " + std::to_string( k ) + ")"; };   // built only on failure
+            if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad gemm dimensions" + at(); }
+            if( t.M > t.lda || t.N > t.ldb || t.N > t.ldc ) { return "gemm leading dimension too small" + at(); }
+            // 16-byte copies of FP64 (2 entries) and FP32 (4 entries) storage
+            if( (t.a | t.b | t.c) % 4 != 0 || (t.lda | t.ldb | t.ldc) % 4 != 0 ) { return "gemm operand not 16-byte aligned" + at(); }
+            if( !in_range( t.a, t.a + static_cast<I64>(t.K - 1) * t.lda + t.M - 1, arena ) ) { return "gemm A out of range" + at(); }
+            if( !in_range( t.b, t.b + static_cast<I64>(t.K - 1) * t.ldb + t.N - 1, arena ) ) { return "gemm B out of range" + at(); }
+            if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at(); }
+            return std::string();
+        };
+        const I64 bad = first_bad( static_cast<I64>( pl.gemm.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
+        if( bad >= 0 ) { return task( bad ); }
     }
     for( size_t k = 0; k < pl.sdiag.size(); ++k )
     {
