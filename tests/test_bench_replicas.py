@@ -88,3 +88,12 @@ def test_batch_shards_cover_every_system_once_and_balance_the_work():
     for world in (2, 4, 8):
         loads = [w[p].sum() for p in bench.shard_by_work(w, world)]
         assert max(loads) / (w.sum() / world) < 1.01
+
+
+def test_a_rank_generates_exactly_its_share_of_the_batch():
+    # systems are seeded by their index in the whole batch, so a rank's subset equals the full batch's rows
+    full = bench.c4_systems(4)
+    part = bench.c4_systems(4, [1, 3])
+    for got, want in zip(part, [full[1], full[3]]):
+        for a, b in zip(got, want):
+            assert np.array_equal(a, b)
