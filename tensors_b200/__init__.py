@@ -7,4 +7,6 @@ reached through the C-ABI declared in ``include/tensors_b200.h``.
 """
 from . import matrices, ordering  # noqa: F401
 
-__all__ = ["matrices", "ordering"]
+# the library-backed modules (cholesky, serving, matrix_market) load the shared
+# object on first use: ``from tensors_b200.cholesky import CholeskyDecomposition``
+__all__ = ["matrices", "ordering", "cholesky", "serving", "matrix_market"]
