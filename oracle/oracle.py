@@ -37,7 +37,10 @@ _i64 = ctypes.c_int64
 
 
 def build(with_reference: bool = True) -> None:
-    """Compile the restatement (and the reference, when its checkout exists)."""
+    """Compile the restatement (and the reference, when its checkout exists).
+
+    The checkout's location is the Makefile's REFERENCE_DIR (override it in
+    the environment); without a checkout the reference target is skipped."""
     targets = ["oracle"] + (["ref"] if with_reference else [])
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
