@@ -3,22 +3,32 @@
 
 Workload (one step): NumericFactorization + Solve with 16 right-hand sides of
 the 7-point Laplacian of a 64^3 grid (n = 262,144) with per-edge
-conductivities exp(N(0,1)) and a 1e-6 diagonal shift, nested-dissection
-ordering, plain FP64.  Inputs are seeded synthetic data (no dataset exists for
-this path).  Symbolic analysis is done once before timing, as in the
-reference's driver (Example_SparseCholesky/main.cpp:135 vs :147).
+conductivities exp(N(0,1)) and a 1e-6 diagonal shift, plain FP64, under the
+nested dissection with fewer factor flops (on this grid the one from the
+pattern alone: about half the flops of the geometric one).  Inputs are seeded
+synthetic data (no dataset exists for this path).  Symbolic analysis is done
+once before timing, as in the reference's driver
+(Example_SparseCholesky/main.cpp:135 vs :147).
 
 The metric is factor+solve throughput in GFLOP/s, counting the reference's
 algorithmic flops once: factor Sum_s [n0^3/3 + n0^2 n1 + n0 n1^2] over the
 reference's supernodes plus solve 4 k nnz(U); ms_per_step is the factor+solve
 time.  Every run checks the relative residual ||B - A X|| / ||B|| on the
-device.
+device; the CPU-baseline leg also runs the reference's own code on the same
+system and reports the forward difference of the two solutions.
+
+The default line also carries the mixed-precision comparison on the 3-dof
+27-point vector Laplacian of a 48^3 grid (FP32 factor with 3xTF32 tensor-core
+updates + FP64 refinement vs plain FP64, both to 1e-10): `config.mixed_vs_fp64`.
 
 Multi-GPU (torchrun): the workload is replicated -- each rank factors and
 solves its own system (weak scaling, no collective on the data path).
 
 `--impl reference` times the reference's own CPU implementation (compiled
-from its headers into oracle/_ref) on the host cores for the same metric.
+from its headers into oracle/_ref) on all host cores for the same metric on
+the same system: each step is one full factor + solve.  It takes the
+permutation from tests/golden/bench/c2_grid64_graph_nd.npz, so that process loads
+only the reference's library.
 """
 from __future__ import annotations
 
@@ -41,24 +51,38 @@ SEED = 0x5EED0002
 SHIFT = 1e-6
 NRHS = 16
 L2_FLUSH_BYTES = 256 << 20
-# The reference's CPU code needs about a minute per full 64^3 factor+solve on
-# 8 cores, so its timed runs use a bounded sample of the same workload: the
-# same generator and ordering on a 48^3 grid (same stencil, weights, shift,
-# RHS count); GFLOP/s is computed with the sample's own flop count.
-CPU_SAMPLE_GRID = 48
+# The permutation of the 64^3 system under the pattern-only nested dissection,
+# written by tests/golden/bench/make_bench_inputs.py (checked against the library by
+# tests/test_bench_inputs.py): the reference arm reads it instead of running
+# this library's ordering.
+PERM_FIXTURE = os.path.join(ROOT, "tests", "golden", "bench", "c2_grid64_graph_nd.npz")
+
+# The system's nested dissection: "graph" (from the pattern alone, the default:
+# the fewer-flop ordering on this grid) or "geometric" (grid planes from the
+# node coordinates, twice the factor flops here).
+ORDERING = "graph"
+METRIC = "factor+solve GFLOP/s (FP64, 64^3 7-pt Laplacian, 16 RHS)"
 
 
-# C2's nested dissection: "geometric" (grid planes from the node coordinates, the default) or
-# "graph" (from the pattern alone; on this grid about half the factor flops, see --ordering).
-ORDERING = "geometric"
+def c2_permutation(A, name, product=True):
+    """Fill-reducing order of the benchmark matrix.  product=False (reference arm): the geometric
+    order is pure numpy and the pattern-only order of the 64^3 system comes from the fixture."""
+    from tensors_b200 import ordering
+
+    if name == "geometric":
+        return ordering.nested_dissection(A)
+    if not product and A.n == 64 ** 3 and os.path.exists(PERM_FIXTURE):
+        z = np.load(PERM_FIXTURE)
+        return np.cumsum(z["delta"].astype(np.int64)).astype(np.int32)
+    return ordering.graph_nested_dissection(A)
 
 
-def build_problem(grid: int | None = None):
+def build_problem(grid: int | None = None, ordering_name: str | None = None, product: bool = True):
     grid = GRID if grid is None else grid
-    from tensors_b200 import matrices, ordering
+    from tensors_b200 import matrices
 
     A = matrices.grid_laplacian_3d(grid, SEED, SHIFT)
-    perm = ordering.graph_nested_dissection(A) if ORDERING == "graph" else ordering.nested_dissection(A)
+    perm = c2_permutation(A, ORDERING if ordering_name is None else ordering_name, product)
     B = np.random.default_rng(SEED + 1).standard_normal((A.n, NRHS))
     return A, perm, B
 
@@ -68,7 +92,9 @@ def config_dict(extra=None):
         "workload": f"3D 7-point Laplacian {GRID}^3 (n={GRID**3}), lognormal(0,1) edge conductivities, "
                     f"shift {SHIFT:g}, nested dissection, {NRHS} RHS N(0,1), FP64 factor+solve",
         "grid": GRID, "n": GRID ** 3, "nrhs": NRHS, "seed": SEED,
-        "supernode_strategy": "Maximal", "ordering": f"{ORDERING} nested dissection",
+        "supernode_strategy": "Maximal",
+        "ordering": ("nested dissection from the pattern alone (fewer factor flops than the geometric one)"
+                     if ORDERING == "graph" else "geometric nested dissection"),
         "l2": "256 MiB buffer written between timed steps (inputs and factor also exceed L2)",
     }
     if extra:
@@ -150,8 +176,10 @@ def measure_dgemm_tflops(torch, dev):
     return best
 
 
-def cpu_reference_run(A, perm, B, threads, steps=1, warmup=0, sample=None):
-    """Times the reference's own CPU factor+solve (oracle/_ref) on this host."""
+def reference_run(A, perm, B, threads, steps=1, warmup=0):
+    """Times the reference's own CPU factor+solve (oracle/_ref) on this host: `threads` tree threads, one
+    BLAS thread each (the reference parallelises over the assembly tree).  Its flops come from its own
+    supernodes, so this needs nothing from this library."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
@@ -159,7 +187,14 @@ def cpu_reference_run(A, perm, B, threads, steps=1, warmup=0, sample=None):
         return None
     ref = oracle.RefCholesky(A.n, A.outer, A.inner, perm, "maximal", threads=threads, blas_threads=1)
     ref.symbolic()
+    n0 = np.diff(ref.array("SN_rp")).astype(np.float64)
+    n1 = np.diff(ref.array("SN_outer")).astype(np.float64)
+    factor_flops = float((n0 ** 3 / 3.0 + n0 ** 2 * n1 + n0 * n1 ** 2).sum())
+    nnz_u = float((n0 * (n0 + 1.0) / 2.0 + n0 * n1).sum())
+    k = 1 if B.ndim == 1 else B.shape[1]
     times = []
+    X = None
+    st = 0
     for i in range(warmup + steps):
         t0 = time.perf_counter()
         st = ref.factor(A.values, 0.0)
@@ -168,44 +203,33 @@ def cpu_reference_run(A, perm, B, threads, steps=1, warmup=0, sample=None):
         if i >= warmup:
             times.append(dt)
     res = np.linalg.norm(B - A.to_scipy() @ X) / np.linalg.norm(B)
-    return {"seconds": times, "status": st, "relres": float(res)}
-
-
-def reference_flops(A, perm):
-    """Reference-supernode factor flops and nnz(U) (host-only symbolic)."""
-    from tensors_b200.cholesky import CholeskyDecomposition
-
-    c = CholeskyDecomposition(A.outer, A.inner, perm)
-    c.SymbolicFactorization()
-    f, nnz_u = c.FlopCount()
-    return f, nnz_u
+    return {"seconds": times, "status": st, "relres": float(res), "X": X,
+            "factor_flops": factor_flops, "nnz_u": nnz_u, "flops": factor_flops + 4.0 * k * nnz_u}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU code on the benchmark's system, every host thread."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    A, perm, B = build_problem(CPU_SAMPLE_GRID)
-    f, nnz_u = reference_flops(A, perm)
-    flops = f + 4.0 * NRHS * nnz_u
+    A, perm, B = build_problem(args.grid, product=False)
     threads = os.cpu_count() or 1
-    r = cpu_reference_run(A, perm, B, threads, steps=args.steps, warmup=args.warmup)
+    r = reference_run(A, perm, B, threads, steps=args.steps, warmup=args.warmup)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtb_ref.so not built (needs the reference checkout)"}))
         return 0
     t = statistics.mean(r["seconds"])
-    v = flops / t / 1e9
+    v = r["flops"] / t / 1e9
+    sample = f"one full factor + solve of the benchmark system per step ({threads} tree threads, 1 BLAS thread each)"
     line = {
         "impl": "reference",
-        "metric": "factor+solve GFLOP/s (FP64, 64^3 7-pt Laplacian, 16 RHS)",
+        "metric": METRIC,
         "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded)",
-        "config": config_dict({"cpu_sample": f"{CPU_SAMPLE_GRID}^3 grid of the same generator, GFLOP/s from its own flops",
-                               "sample_relres": r["relres"], "cpu_threads": threads}),
-        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "reference",
-                         "sample": f"same generator on a {CPU_SAMPLE_GRID}^3 grid (n={CPU_SAMPLE_GRID**3}), "
-                                   "one factor+solve per step"},
+        "config": config_dict({"relres": r["relres"], "cpu_threads": threads, "factor_gflop": r["factor_flops"] / 1e9,
+                               "seconds": r["seconds"]}),
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -272,28 +296,31 @@ def _time_steps(torch, stream, fn, steps, warmup, barrier=None):
     return statistics.mean(tot), statistics.mean(first)
 
 
-def run_c3(args):
-    """Mixed precision vs FP64 on the 3-dof 27-point vector Laplacian (48^3 nodes, n = 331,776).
+def c3_compare(torch, dev, steps, warmup):
+    """Mixed precision vs FP64 on the 3-dof 27-point vector Laplacian (48^3 nodes, n = 331,776), 8 RHS.
 
     The stiffness sum_e [[B,-B],[-B,B]] with SPD edge blocks B = G G^T + 0.1 I is
     singular (rigid translations are in its null space), so the matrix carries
-    a 1e-2 diagonal shift.  Both paths solve 8 RHS to the same 1e-10 relative
-    residual target; the FP64 path reaches ~1e-14 directly.
+    a 1e-2 diagonal shift.  Both paths solve to the same 1e-10 relative
+    residual target; the FP64 path reaches ~1e-14 directly.  Returns per
+    precision the step, factor and solve times, the relative residual and the
+    refinement, plus the speed-up and the forward difference of the mixed
+    solution from the FP64 one.
     """
-    import torch
     from tensors_b200 import build as tb_build
     from tensors_b200 import matrices, ordering
     from tensors_b200.cholesky import CholeskyDecomposition
 
     tb_build.build()
-    dev = torch.device("cuda", 0)
     A = matrices.vector_laplacian_3d(C3_GRID, C3_SEED, C3_SHIFT)
     perm = ordering.nested_dissection(A)
     B = torch.tensor(np.random.default_rng(C3_SEED + 1).standard_normal((A.n, C3_NRHS)), device=dev)
     vals = torch.tensor(A.values, device=dev)
     stream = torch.cuda.Stream(dev)
+    prev = torch.cuda.current_stream(dev)
     torch.cuda.set_stream(stream)
-    out = {}
+    out, sols = {}, {}
+    F = nnz_u = 0.0
     for prec in ("fp64", "mixed"):
         c = CholeskyDecomposition(A.outer, A.inner, perm)
         c.SetPrecision(prec)
@@ -308,27 +335,42 @@ def run_c3(args):
                 mid.record(stream)
             c.Solve(B, X)
 
-        with ClockSampler(0) as clocks:
-            t, tf = _time_steps(torch, stream, step, args.steps, args.warmup)
+        with ClockSampler(dev.index or 0) as clocks:
+            t, tf = _time_steps(torch, stream, step, steps, warmup)
         R = c.Residual(B, X)
         stream.synchronize()
         rr = float((torch.linalg.norm(R, dim=0) / torch.linalg.norm(B, dim=0)).max())
         F, nnz_u = c.FlopCount()
         out[prec] = {"ms": t, "factor_ms": tf, "solve_ms": t - tf, "relres": rr,
                      "refinement": c.RefinementInfo() if prec == "mixed" else None,
-                     "clocks": clocks.summary()}
+                     "precision_in_use": list(c.PrecisionInUse()), "clocks": clocks.summary()}
+        sols[prec] = X
+        del c
+    torch.cuda.set_stream(prev)
     flops = F + 4.0 * C3_NRHS * nnz_u
+    return {"workload": f"3-dof 27-point vector Laplacian {C3_GRID}^3 (n={A.n}), SPD 3x3 edge blocks "
+                        f"G G^T + 0.1 I, shift {C3_SHIFT:g}, geometric nested dissection, {C3_NRHS} RHS, "
+                        f"target relres {TARGET_RELRES:g}",
+            "factor_gflop": F / 1e9, "flops": flops, "fp64": out["fp64"], "mixed": out["mixed"],
+            "speedup_mixed_over_fp64": out["fp64"]["ms"] / out["mixed"]["ms"],
+            "forward_diff_mixed_vs_fp64": float(torch.linalg.norm(sols["mixed"] - sols["fp64"])
+                                                / torch.linalg.norm(sols["fp64"])),
+            "l2": "factor and matrix exceed L2"}
+
+
+def run_c3(args):
+    """The mixed-precision vs FP64 comparison (c3_compare) as its own line: GFLOP/s of the mixed path."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    r = c3_compare(torch, dev, args.steps, args.warmup)
     line = {
         "metric": "factor+solve GFLOP/s to 1e-10 relative residual, mixed precision (FP32 factor, 3xTF32 updates, "
                   "FP64 refinement) vs plain FP64, 48^3 3-dof 27-pt vector Laplacian, 8 RHS",
-        "value": flops / (out["mixed"]["ms"] * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": out["mixed"]["ms"], "higher_is_better": True, "scaling": "weak",
+        "value": r["flops"] / (r["mixed"]["ms"] * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["mixed"]["ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"3-dof 27-point vector Laplacian {C3_GRID}^3 (n={A.n}), SPD 3x3 edge blocks "
-                               f"G G^T + 0.1 I, shift {C3_SHIFT:g}, nested dissection, {C3_NRHS} RHS",
-                   "factor_gflop": F / 1e9, "fp64": out["fp64"], "mixed": out["mixed"],
-                   "speedup_mixed_over_fp64": out["fp64"]["ms"] / out["mixed"]["ms"],
-                   "l2": "factor and matrix exceed L2"},
+        "config": r,
     }
     print(json.dumps(line))
     return 0
@@ -635,9 +677,12 @@ def main():
     ap.add_argument("--ncu", action="store_true",
                     help="profiling run for ncu: warmup + steps factor+solve as direct launches, no timing, "
                          "no baselines")
-    ap.add_argument("--ordering", default="geometric", choices=["geometric", "graph"],
-                    help="c2: nested dissection from node coordinates (default) or from the pattern alone "
-                         "(fewer factor flops on this grid; GFLOP/s is then computed from its own flops)")
+    ap.add_argument("--ordering", default="graph", choices=["geometric", "graph"],
+                    help="c2: nested dissection from the pattern alone (default: fewer factor flops on this grid) "
+                         "or from the node coordinates (GFLOP/s is computed from each ordering's own flops)")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="c2: skip the mixed-precision vs FP64 comparison on the 48^3 vector Laplacian")
+    ap.add_argument("--c3-steps", type=int, default=5, help="timed steps of each precision in that comparison")
     args = ap.parse_args()
     global ORDERING
     ORDERING = args.ordering
@@ -748,6 +793,12 @@ def main():
         prof = chol.KernelProfile()
     chol.SetProfiling(False)
     dgemm_peak = measure_dgemm_tflops(torch, dev)
+    plan_stats = chol.PlanStats()
+    F_geo = None
+    if ORDERING != "geometric" and rank == 0:
+        cg = CholeskyDecomposition(A.outer, A.inner, c2_permutation(A, "geometric"))
+        F_geo = cg.FlopCount()[0]
+        del cg
 
     if world > 1:
         dist.destroy_process_group()
@@ -765,21 +816,37 @@ def main():
             traffic = None
 
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
+        # the reference's own code on the same system (same ordering, values and RHS), all host threads
         threads = os.cpu_count() or 1
-        As, ps, Bs = build_problem(CPU_SAMPLE_GRID)
-        fs, zs = reference_flops(As, ps)
-        r = cpu_reference_run(As, ps, Bs, threads, steps=1, warmup=0)
+        r = reference_run(A, perm, B_host, threads, steps=1, warmup=0)
         if r is not None:
-            cpu = {"value": (fs + 4.0 * NRHS * zs) / r["seconds"][0] / 1e9, "unit": "GFLOP/s", "cores": threads,
+            Xg = X.cpu().numpy()
+            cpu = {"value": r["flops"] / r["seconds"][0] / 1e9, "unit": "GFLOP/s", "cores": threads,
                    "kind": "reference",
-                   "sample": f"reference's own code, one factor+solve of the same generator on a {CPU_SAMPLE_GRID}^3 "
-                             f"grid (OpenBLAS 1 thread per tree task, {threads} tree threads)",
-                   "seconds": r["seconds"][0], "relres": r["relres"]}
+                   "sample": f"the reference's own code, one factor+solve of the benchmark system "
+                             f"({threads} tree threads, 1 BLAS thread each)",
+                   "seconds": r["seconds"][0], "relres": r["relres"],
+                   "forward_diff_vs_gpu": float(np.linalg.norm(Xg - r["X"]) / np.linalg.norm(r["X"]))}
+            del r
+            if ORDERING != "geometric":
+                # the same reference run under the geometric dissection (twice the flops on this grid)
+                Ag, pg, Bg = build_problem(args.grid, "geometric")
+                rg = reference_run(Ag, pg, Bg, threads, steps=1, warmup=0)
+                cpu["geometric_ordering"] = {"value": rg["flops"] / rg["seconds"][0] / 1e9, "unit": "GFLOP/s",
+                                             "seconds": rg["seconds"][0], "factor_gflop": rg["factor_flops"] / 1e9,
+                                             "relres": rg["relres"]}
+                del rg
+
+    mixed = None
+    if not args.no_mixed and world == 1:
+        del chol
+        torch.cuda.empty_cache()
+        mixed = c3_compare(torch, dev, args.c3_steps, args.warmup)
 
     value = replica_throughput(flops, t_ms, world)
     line = {
-        "metric": "factor+solve GFLOP/s (FP64, 64^3 7-pt Laplacian, 16 RHS)",
+        "metric": METRIC,
         "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded)",
@@ -788,8 +855,10 @@ def main():
             "relres": relres, "symbolic_s": t_symbolic,
             "factor_ms": statistics.mean(factor_times), "solve_ms": t_ms - statistics.mean(factor_times),
             "factor_gflop": F / 1e9, "solve_gflop": 4.0 * NRHS * nnz_u / 1e9,
-            "plan": chol.PlanStats(),
+            "plan": plan_stats,
             "kernel_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "flops_geometric_ordering_gflop": F_geo / 1e9 if F_geo else None,
+            "mixed_vs_fp64": mixed,
         }),
         "e2e": {"value": flops / e2e_s / 1e9 * world, "unit": "GFLOP/s",
                 "h2d_bytes_per_step": int(A.values.nbytes + B_host.nbytes),
