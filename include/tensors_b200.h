@@ -77,7 +77,12 @@ enum tb_array {
     TB_ARRAY_ATREE_CHILD_IDX = 14 /* AssemblyTree().ChildIndices()            */
 };
 
+/* Scalar types of values, right-hand sides and solutions at the boundary
+ * (the reference's ExtScal and B_T / X_T template arguments). */
+enum tb_dtype { TB_F64 = 0, TB_F32 = 1 };
+
 typedef struct tb_chol tb_chol;
+typedef struct tb_factor tb_factor;
 
 /* Message of the last failing call on this thread (never NULL). */
 const char * tb_last_error( void );
@@ -109,6 +114,11 @@ int tb_chol_symbolic( tb_chol * h );
  * Numeric.hpp:95) or an error. */
 int tb_chol_numeric( tb_chol * h, const double * values, double reg );
 int tb_chol_numeric_device( tb_chol * h, const double * d_values, double reg );
+/* NumericFactorization<ExtScal>(cptr<ExtScal> A_val, ExtScal reg),
+ * Numeric.hpp:3-8: values of type dtype (TB_F64 or TB_F32), converted to
+ * FP64 on copy (ReadNonzeroValues casts, Numeric.hpp:165-180). */
+int tb_chol_numeric_ex( tb_chol * h, const void * values, int32_t dtype, double reg );
+int tb_chol_numeric_device_ex( tb_chol * h, const void * d_values, int32_t dtype, double reg );
 
 /* Solve: X = alpha * A^{-1} B + beta * X (Solve.hpp:22-80).  B and X are
  * row-major n x nrhs with leading dimensions ldB, ldX >= nrhs; they may
@@ -117,6 +127,31 @@ int tb_chol_solve( tb_chol * h, double alpha, const double * B, int32_t ldB,
                    double beta, double * X, int32_t ldX, int32_t nrhs );
 int tb_chol_solve_device( tb_chol * h, double alpha, const double * d_B, int32_t ldB,
                           double beta, double * d_X, int32_t ldX, int32_t nrhs );
+/* Solve<NRHS,parQ,op,a_T,B_T,b_T,X_T> (Solve.hpp:20-27): B of type b_dtype
+ * and X of type x_dtype (TB_F64 or TB_F32), each cast on copy; the solve
+ * itself runs as tb_chol_solve / tb_chol_solve_device. */
+int tb_chol_solve_ex( tb_chol * h, double alpha, const void * B, int32_t ldB, int32_t b_dtype,
+                      double beta, void * X, int32_t ldX, int32_t x_dtype, int32_t nrhs );
+int tb_chol_solve_device_ex( tb_chol * h, double alpha, const void * d_B, int32_t ldB, int32_t b_dtype,
+                             double beta, void * d_X, int32_t ldX, int32_t x_dtype, int32_t nrhs );
+
+/* NumericalFactorization_T (CholeskyDecomposition.hpp:132-201): a numeric
+ * factor held apart from any handle (device memory: the factor storage, the
+ * inverse diagonal blocks and the values it was computed from).  A new one is
+ * empty (not factorized).  tb_factor_state: NumericallyFactorizedQ,
+ * NumericallyGoodQ, AllocatedByteCount and the precision of the stored factor
+ * (-1 when it never held one). */
+int tb_factor_create( tb_factor ** out );
+int tb_factor_destroy( tb_factor * f );
+int tb_factor_state( tb_factor * f, int32_t * factorized, int32_t * good, int64_t * bytes, int32_t * precision );
+/* SwapNumericalFactorization (Numeric.hpp:228-254): exchanges the handle's
+ * numeric factor with f.  A factor that says factorized but not good, or
+ * whose storage is smaller than the handle's symbolic analysis requires, is
+ * then treated as unfactorized.  The handle takes the incoming factor's
+ * precision; its captured factor and solve graphs are dropped (they hold the
+ * outgoing storage's addresses).  f must be empty or live on the handle's
+ * device. */
+int tb_chol_swap_factor( tb_chol * h, tb_factor * f );
 
 /* Half solves (Solve.hpp:182-310) with the documented meaning:
  * upper: X = alpha * P^T U^{-1} P B + beta X;  lower: X = alpha * P^T U^{-T} P B + beta X. */
@@ -169,7 +204,9 @@ int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
  * the solve's task graph, out[15] its first level, out[16] CTAs of the
  * persistent factorization launch (0 before the device plan exists),
  * out[17] / out[18] host microseconds of the last symbolic analysis / plan
- * build.  Returns the number of entries written (at most cap). */
+ * build, out[19] tensor-core tiles of the mixed-precision path, out[20]
+ * blocks of its operand image (8 KB each).  Returns the number of entries
+ * written (at most cap). */
 int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
 /* Host-side bounds check of every device task of the plan (also run before
  * the plan is first uploaded).  TB_OK or TB_ERR_INVALID_ARGUMENT with the
@@ -275,13 +312,17 @@ int tb_chol_kernel_profile( tb_chol * h, double * ms, int64_t * launches, double
  * info[4i..4i+3] = kind, level, panel step (or child rank), task count and
  * ms[i] its duration; entry 0 is the clear + assembly.  Returns the count. */
 int tb_chol_launch_profile( tb_chol * h, int64_t * info, double * ms, int32_t cap );
-/* Solve (as tb_chol_solve_device) that allocates no device memory: its two
- * permuted work blocks live in a fixed device array of 2 x 4,194,304 doubles
- * (64 MiB) per device, so n * nrhs must not exceed 4,194,304 (else
- * TB_ERR_INVALID_ARGUMENT, nothing launched).  For callers that may not
- * allocate at solve time.  The first call on a device looks the array up
- * (make it outside stream capture); calls that can overlap on one device
- * share the array and must be serialised.  No counterpart in the reference. */
+/* Direct solve with the FP64 factor (tb_chol_solve_device's result on an FP64
+ * handle) that allocates no device memory: its two permuted work blocks live
+ * in a fixed device array of 2 x 4,194,304 doubles (64 MiB) per device, so
+ * n * nrhs must not exceed 4,194,304 (else TB_ERR_INVALID_ARGUMENT, nothing
+ * launched).  For callers that may not allocate at solve time.  Handles that
+ * solve by refinement (mixed precision, or FP64 after a failed refinement) are
+ * rejected with TB_ERR_INVALID_ARGUMENT.  The sweeps run as level launches
+ * (no waits, no timeout).  The first call on a device looks the array up
+ * (make it outside stream capture; the caller's current device is kept);
+ * calls that can overlap on one device share the array and must be
+ * serialised.  No counterpart in the reference. */
 int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B, int32_t ldB,
                                   double beta, double * d_X, int32_t ldX, int32_t nrhs );
 /* Per launch of the last solve run with profiling enabled (at most cap

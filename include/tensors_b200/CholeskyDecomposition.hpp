@@ -1,10 +1,16 @@
 // tensors_b200::Sparse::CholeskyDecomposition -- header-only C++ mirror of
-// Tensors::Sparse::CholeskyDecomposition<double,int32_t,int64_t>
+// Tensors::Sparse::CholeskyDecomposition<Scal,Int,LInt,parQ>
 // (src/Sparse/CholeskyDecomposition.hpp) over the C-ABI of tensors_b200.h.
 //
 // Member names, argument order and argument meaning follow the reference so
 // that code written against it compiles after swapping the include and the
-// namespace.  Differences:
+// namespace.  Template arguments: Scal = double (FP64 factor) or float (FP32
+// factor storage with 3xTF32 tensor-core updates; solves are refined in FP64
+// to the handle's target, so they are at least as accurate as the reference's
+// float solves); Int = int32_t and LInt = int64_t, as the reference's driver
+// instantiates it (Example_SparseCholesky/main.cpp:31-32).  The reference's
+// parQ argument selects host threading and has no counterpart: every
+// numeric phase runs on the GPU.  Differences:
 //  - errors throw tensors_b200::Sparse::Error (the reference prints with
 //    eprint and continues); NumericFactorization still returns 1 for a
 //    non-positive pivot, like the reference (Numeric.hpp:99);
@@ -12,14 +18,16 @@
 //    runs the upper solve, Solve.hpp:290-307);
 //  - the template arguments of the reference's Solve (NRHS, parQ, op) are not
 //    needed: the right-hand-side count is a run-time argument and every solve
-//    runs on the GPU.
-// Link with tensors_b200/_tensors_b200*.so (the library built by
+//    runs on the GPU; the scalar types of B and X are the call's own (float
+//    or double, cast on copy as Solve.hpp:20-27).
+// Link with tensors_b200/libtensors_b200.so (the library built by
 // tensors_b200/build.py).
 #pragma once
 
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -40,12 +48,46 @@ enum class FactorizationMethod_T : int32_t
     Multifrontal = TB_MULTIFRONTAL, LeftLooking = TB_LEFT_LOOKING
 };
 
+namespace detail
+{
+template<typename T> constexpr int32_t dtype_of()
+{
+    static_assert( std::is_same<T, double>::value || std::is_same<T, float>::value, "scalars are double or float" );
+    return std::is_same<T, float>::value ? TB_F32 : TB_F64;
+}
+} // namespace detail
+
+template<typename Scal_ = double, typename Int_ = int32_t, typename LInt_ = int64_t>
 class CholeskyDecomposition
 {
 public:
-    using Scal = double;
-    using Int  = int32_t;
-    using LInt = int64_t;
+    using Scal = Scal_;
+    using Int  = Int_;
+    using LInt = LInt_;
+    static_assert( std::is_same<Scal, double>::value || std::is_same<Scal, float>::value, "Scal is double or float" );
+    static_assert( std::is_same<Int, int32_t>::value && std::is_same<LInt, int64_t>::value,
+                   "Int = int32_t and LInt = int64_t (the reference driver's instantiation)" );
+
+    // NumericalFactorization_T (CholeskyDecomposition.hpp:132-201): a numeric
+    // factor held apart from any decomposition, exchanged by
+    // SwapNumericalFactorization.  Device memory; a new one is empty.
+    class NumericalFactorization_T
+    {
+    public:
+        NumericalFactorization_T() { Check( tb_factor_create( &f_ ) ); }
+        ~NumericalFactorization_T() { if( f_ != nullptr ) { tb_factor_destroy( f_ ); } }
+        NumericalFactorization_T( const NumericalFactorization_T & ) = delete;
+        NumericalFactorization_T & operator=( const NumericalFactorization_T & ) = delete;
+        NumericalFactorization_T( NumericalFactorization_T && o ) noexcept : f_( std::exchange( o.f_, nullptr ) ) {}
+
+        bool NumericallyFactorizedQ() const { int32_t f = 0; Check( tb_factor_state( f_, &f, nullptr, nullptr, nullptr ) ); return f != 0; }
+        bool NumericallyGoodQ() const { int32_t g = 0; Check( tb_factor_state( f_, nullptr, &g, nullptr, nullptr ) ); return g != 0; }
+        size_t AllocatedByteCount() const { int64_t b = 0; Check( tb_factor_state( f_, nullptr, nullptr, &b, nullptr ) ); return static_cast<size_t>( b ); }
+        tb_factor * Handle() const noexcept { return f_; }
+
+    private:
+        tb_factor * f_ = nullptr;
+    };
 
     // Fill-reducing permutation p of size n (Inverse::False), ctor
     // CholeskyDecomposition.hpp:336-346.  thread_count is used by the host
@@ -55,6 +97,7 @@ public:
     : threads_( thread_count )
     {
         Check( tb_chol_create( &h_, n, A_outer, A_inner, p, thread_count ) );
+        SetScalarPrecision();
     }
 
     // Matrix already permuted, ctor CholeskyDecomposition.hpp:350-371.
@@ -62,6 +105,7 @@ public:
     : threads_( thread_count )
     {
         Check( tb_chol_create( &h_, n, A_outer, A_inner, nullptr, thread_count ) );
+        SetScalarPrecision();
     }
 
     ~CholeskyDecomposition() { if( h_ != nullptr ) { tb_chol_destroy( h_ ); } }
@@ -105,41 +149,54 @@ public:
     void SymbolicFactorization() { Check( tb_chol_symbolic( h_ ) ); }
 
     // CholeskyDecomposition/Numeric.hpp:3-24: values in the caller's CSR
-    // order, reg added to the diagonal.  0 = success, 1 = not positive definite.
-    int NumericFactorization( const Scal * A_val, Scal reg = 0 )
+    // order, reg added to the diagonal.  0 = success, 1 = not positive
+    // definite.  ExtScal is the values' own type (float or double), cast on
+    // copy as NumericFactorization<ExtScal> does.
+    template<typename ExtScal>
+    int NumericFactorization( const ExtScal * A_val, ExtScal reg = ExtScal( 0 ) )
     {
-        return Check( tb_chol_numeric( h_, A_val, reg ) );
+        return Check( tb_chol_numeric_ex( h_, A_val, detail::dtype_of<ExtScal>(), static_cast<double>( reg ) ) );
     }
     // Same with A_val in device memory of the handle's GPU.
-    int NumericFactorization_Device( const Scal * d_A_val, Scal reg = 0 )
+    template<typename ExtScal>
+    int NumericFactorization_Device( const ExtScal * d_A_val, ExtScal reg = ExtScal( 0 ) )
     {
-        return Check( tb_chol_numeric_device( h_, d_A_val, reg ) );
+        return Check( tb_chol_numeric_device_ex( h_, d_A_val, detail::dtype_of<ExtScal>(), static_cast<double>( reg ) ) );
     }
 
+    // SwapNumericalFactorization (Numeric.hpp:228-254): exchanges this
+    // object's numeric factor with cont.  A factor that says factorized but
+    // not good, or is smaller than this symbolic analysis requires, is then
+    // treated as unfactorized.
+    void SwapNumericalFactorization( NumericalFactorization_T & cont ) { Check( tb_chol_swap_factor( h_, cont.Handle() ) ); }
+
     // X_out = alpha * A^{-1} B + beta * X_out, row-major n x nrhs
-    // (Solve.hpp:22-80); host pointers.
-    void Solve( Scal alpha, const Scal * B, Int ldB, Scal beta, Scal * X_out, Int ldX, Int nrhs = 1 )
+    // (Solve.hpp:22-80); host pointers.  B and X_out each float or double.
+    template<typename B_T, typename X_T>
+    void Solve( double alpha, const B_T * B, Int ldB, double beta, X_T * X_out, Int ldX, Int nrhs = 1 )
     {
-        Check( tb_chol_solve( h_, alpha, B, ldB, beta, X_out, ldX, nrhs ) );
+        Check( tb_chol_solve_ex( h_, alpha, B, ldB, detail::dtype_of<B_T>(), beta, X_out, ldX, detail::dtype_of<X_T>(), nrhs ) );
     }
     // X_out = A^{-1} B, Solve.hpp:87-99.
-    void Solve( const Scal * B, Scal * X_out, Int nrhs = 1 )
+    template<typename B_T, typename X_T>
+    void Solve( const B_T * B, X_T * X_out, Int nrhs = 1 )
     {
         Solve( 1.0, B, nrhs, 0.0, X_out, nrhs, nrhs );
     }
     // Same on device buffers of the handle's GPU and stream.
-    void Solve_Device( Scal alpha, const Scal * d_B, Int ldB, Scal beta, Scal * d_X, Int ldX, Int nrhs = 1 )
+    template<typename B_T, typename X_T>
+    void Solve_Device( double alpha, const B_T * d_B, Int ldB, double beta, X_T * d_X, Int ldX, Int nrhs = 1 )
     {
-        Check( tb_chol_solve_device( h_, alpha, d_B, ldB, beta, d_X, ldX, nrhs ) );
+        Check( tb_chol_solve_device_ex( h_, alpha, d_B, ldB, detail::dtype_of<B_T>(), beta, d_X, ldX, detail::dtype_of<X_T>(), nrhs ) );
     }
 
     // X_out = alpha * P^T U^{-1} P B + beta * X_out (Solve.hpp:182-245).
-    void UpperSolve( Scal alpha, const Scal * B, Int ldB, Scal beta, Scal * X_out, Int ldX, Int nrhs = 1 )
+    void UpperSolve( double alpha, const double * B, Int ldB, double beta, double * X_out, Int ldX, Int nrhs = 1 )
     {
         Check( tb_chol_upper_solve( h_, alpha, B, ldB, beta, X_out, ldX, nrhs ) );
     }
     // X_out = alpha * P^T U^{-T} P B + beta * X_out (Solve.hpp:251-310, documented meaning).
-    void LowerSolve( Scal alpha, const Scal * B, Int ldB, Scal beta, Scal * X_out, Int ldX, Int nrhs = 1 )
+    void LowerSolve( double alpha, const double * B, Int ldB, double beta, double * X_out, Int ldX, Int nrhs = 1 )
     {
         Check( tb_chol_lower_solve( h_, alpha, B, ldB, beta, X_out, ldX, nrhs ) );
     }
@@ -149,8 +206,8 @@ public:
     // with P = this factor's solve: X_out = alpha x + beta X_out.  A_val: A' in
     // the caller's CSR order (nullptr: the factored values).  Returns whether
     // every column met the relative tolerance; IterationCount() tells the steps.
-    bool ConjugateGradient( const Scal * A_val, Scal reg, Scal alpha, const Scal * B, Int ldB, Scal beta,
-                            Scal * X_out, Int ldX, Int nrhs, Scal relative_tolerance, Int max_iter,
+    bool ConjugateGradient( const double * A_val, double reg, double alpha, const double * B, Int ldB, double beta,
+                            double * X_out, Int ldX, Int nrhs, double relative_tolerance, Int max_iter,
                             bool use_initial_guess = false )
     {
         relres_.assign( static_cast<size_t>( nrhs < 1 ? 1 : nrhs ), 0.0 );
@@ -161,7 +218,7 @@ public:
         return true;
     }
     Int IterationCount() const { return cg_iter_; }
-    const std::vector<Scal> & RelativeResiduals() const { return relres_; }
+    const std::vector<double> & RelativeResiduals() const { return relres_; }
 
     // Queries, CholeskyDecomposition/InputOutput.hpp:85-367 and Numeric.hpp:183-215.
     Int RowCount() const { Int v = 0; Check( tb_chol_row_count( h_, &v ) ); return v; }
@@ -204,11 +261,10 @@ public:
     // copied back from the device in the reference's layout.
     std::pair<std::vector<Scal>, std::vector<Scal>> FactorValues() const
     {
-        std::pair<std::vector<Scal>, std::vector<Scal>> out;
-        out.first.resize( static_cast<size_t>( RequiredTriangularSize() ) );
-        out.second.resize( static_cast<size_t>( RequiredRectangularSize() ) );
-        Check( tb_chol_factor_values( h_, out.first.data(), out.second.data() ) );
-        return out;
+        std::vector<double> tri( static_cast<size_t>( RequiredTriangularSize() ) );
+        std::vector<double> rec( static_cast<size_t>( RequiredRectangularSize() ) );
+        Check( tb_chol_factor_values( h_, tri.data(), rec.data() ) );
+        return { std::vector<Scal>( tri.begin(), tri.end() ), std::vector<Scal>( rec.begin(), rec.end() ) };
     }
 
     // GetU (InputOutput.hpp:116-217): U in the permuted ordering as CSR.
@@ -219,16 +275,21 @@ public:
         const Int n = RowCount();
         std::vector<LInt> outer( static_cast<size_t>( n ) + 1 );
         std::vector<Int> inner( static_cast<size_t>( nnz ) );
-        std::vector<Scal> values( static_cast<size_t>( nnz ) );
+        std::vector<double> values( static_cast<size_t>( nnz ) );
         Check( tb_chol_get_u( h_, outer.data(), inner.data(), values.data() ) );
         return MatrixCSR( outer.data(), inner.data(), values.data(), n, n, 1 );
     }
 
     // LogDeterminant (InputOutput.hpp:294-297), WriteFactorDiagonal (:238-257).
-    Scal LogDeterminant() const { Scal v = 0; Check( tb_chol_log_det( h_, &v ) ); return v; }
+    Scal LogDeterminant() const { double v = 0; Check( tb_chol_log_det( h_, &v ) ); return static_cast<Scal>( v ); }
     // log det U = half of log det A (InputOutput.hpp:259-292).
-    Scal FactorLogDeterminant() const { return 0.5 * LogDeterminant(); }
-    void WriteFactorDiagonal( Scal * diag ) const { Check( tb_chol_factor_diagonal( h_, diag ) ); }
+    Scal FactorLogDeterminant() const { return static_cast<Scal>( 0.5 ) * LogDeterminant(); }
+    void WriteFactorDiagonal( Scal * diag ) const
+    {
+        std::vector<double> d( static_cast<size_t>( RowCount() ) );
+        Check( tb_chol_factor_diagonal( h_, d.data() ) );
+        for( size_t i = 0; i < d.size(); ++i ) { diag[i] = static_cast<Scal>( d[i] ); }
+    }
 
     // Stream of the handle (a cudaStream_t).
     void SetStream( void * stream ) { Check( tb_chol_set_stream( h_, stream ) ); }
@@ -236,6 +297,12 @@ public:
     tb_chol * Handle() const noexcept { return h_; }
 
 private:
+    // Scal = float: FP32 factor storage (the mixed-precision mode)
+    void SetScalarPrecision()
+    {
+        if( std::is_same<Scal, float>::value ) { Check( tb_chol_set_precision( h_, TB_PRECISION_MIXED ) ); }
+    }
+
     template<typename T>
     std::vector<T> Array( int32_t which ) const
     {
@@ -252,7 +319,7 @@ private:
     FactorizationMethod_T method_ = FactorizationMethod_T::Multifrontal;
     Int threads_ = 1;
     Int cg_iter_ = 0;
-    std::vector<Scal> relres_;
+    std::vector<double> relres_;
 };
 
 } // namespace Sparse

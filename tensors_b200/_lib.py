@@ -35,6 +35,14 @@ SIGNATURES = {
     "tb_chol_solve": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_solve_device": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_solve_device_noalloc": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
+    "tb_chol_numeric_ex": (ctypes.c_int, [_vp, _vp, _i32, _d]),
+    "tb_chol_numeric_device_ex": (ctypes.c_int, [_vp, _vp, _i32, _d]),
+    "tb_chol_solve_ex": (ctypes.c_int, [_vp, _d, _vp, _i32, _i32, _d, _vp, _i32, _i32, _i32]),
+    "tb_chol_solve_device_ex": (ctypes.c_int, [_vp, _d, _vp, _i32, _i32, _d, _vp, _i32, _i32, _i32]),
+    "tb_factor_create": (ctypes.c_int, [ctypes.POINTER(_vp)]),
+    "tb_factor_destroy": (ctypes.c_int, [_vp]),
+    "tb_factor_state": (ctypes.c_int, [_vp, _pi32, _pi32, _pi64, _pi32]),
+    "tb_chol_swap_factor": (ctypes.c_int, [_vp, _vp]),
     "tb_chol_upper_solve": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_lower_solve": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_residual_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, _i32]),

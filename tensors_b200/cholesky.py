@@ -62,6 +62,55 @@ def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+# scalar types at the boundary (tb_dtype)
+TB_F64, TB_F32 = 0, 1
+
+
+def _dtype_code(dt) -> int:
+    return TB_F32 if np.dtype(dt) == np.float32 else TB_F64
+
+
+class NumericalFactorization:
+    """A numeric factor held apart from any decomposition (``NumericalFactorization_T``,
+    CholeskyDecomposition.hpp:132-201): device storage exchanged with a decomposition's by
+    ``CholeskyDecomposition.SwapNumericalFactorization``.  A new one is empty."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        _check(lib().tb_factor_create(ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tb_factor_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _state(self):
+        f, g, b, p = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32()
+        _check(lib().tb_factor_state(self._h, ctypes.byref(f), ctypes.byref(g), ctypes.byref(b), ctypes.byref(p)))
+        return bool(f.value), bool(g.value), int(b.value), int(p.value)
+
+    def NumericallyFactorizedQ(self) -> bool:
+        return self._state()[0]
+
+    def NumericallyGoodQ(self) -> bool:
+        return self._state()[1]
+
+    def AllocatedByteCount(self) -> int:
+        return self._state()[2]
+
+    def Precision(self):
+        """'fp64' | 'mixed' of the stored factor, None when it never held one."""
+        p = self._state()[3]
+        return None if p < 0 else ("mixed" if p == 1 else "fp64")
+
+
 class CholeskyDecomposition:
     """Supernodal Cholesky A = U^T U of a sparse SPD matrix on the GPU.
 
@@ -229,28 +278,50 @@ class CholeskyDecomposition:
         _check(lib().tb_chol_symbolic(self._h))
 
     def NumericFactorization(self, values, reg: float = 0.0) -> int:
-        """Values in the caller's CSR order (host array or CUDA torch tensor)."""
+        """Values in the caller's CSR order (host array or CUDA torch tensor), float64 or float32
+        (``NumericFactorization<ExtScal>``, Numeric.hpp:3-8: converted to FP64 on copy)."""
         if _is_cuda_tensor(values):
-            return _check(lib().tb_chol_numeric_device(self._h, values.data_ptr(), float(reg)))
-        v = _f64(values)
+            import torch
+
+            v = values.contiguous()
+            if v.dtype == torch.float64:
+                return _check(lib().tb_chol_numeric_device(self._h, v.data_ptr(), float(reg)))
+            if v.dtype != torch.float32:
+                raise TBError(-1, "NumericFactorization: values must be float64 or float32")
+            return _check(lib().tb_chol_numeric_device_ex(self._h, v.data_ptr(), TB_F32, float(reg)))
+        v = np.asarray(values)
+        if v.dtype == np.float32:
+            v = np.ascontiguousarray(v)
+            code = TB_F32
+        else:
+            v = _f64(v)
+            code = TB_F64
         if v.shape != (self.NonzeroCount(),):
             raise TBError(-1, "NumericFactorization: wrong number of values")
-        return _check(lib().tb_chol_numeric(self._h, v.ctypes.data, float(reg)))
+        return _check(lib().tb_chol_numeric_ex(self._h, v.ctypes.data, code, float(reg)))
 
     def _solve(self, which: str, B, X=None, alpha=1.0, beta=0.0):
         if _is_cuda_tensor(B):
             return self._solve_device(which, B, X, alpha, beta)
-        B = _f64(B)
+        B = np.asarray(B)
+        B = np.ascontiguousarray(B) if B.dtype == np.float32 else _f64(B)
         one_d = B.ndim == 1
         k = 1 if one_d else B.shape[1]
         if B.shape[0] != self._n:
             raise TBError(-1, "Solve: B has the wrong number of rows")
         if X is None:
-            X = np.zeros_like(B)
+            X = np.zeros(B.shape, dtype=B.dtype)
             beta = 0.0
-        elif not (X.flags.c_contiguous and X.dtype == np.float64 and X.shape == B.shape):
-            raise TBError(-1, "Solve: X must be a C-contiguous float64 array shaped like B")
-        fn = {"full": lib().tb_chol_solve, "upper": lib().tb_chol_upper_solve, "lower": lib().tb_chol_lower_solve}[which]
+        elif not (X.flags.c_contiguous and X.dtype in (np.float64, np.float32) and X.shape == B.shape):
+            raise TBError(-1, "Solve: X must be a C-contiguous float64 or float32 array shaped like B")
+        if which == "full":
+            # B and X may differ in type: each is cast on copy (Solve.hpp:20-27)
+            _check(lib().tb_chol_solve_ex(self._h, float(alpha), B.ctypes.data, k, _dtype_code(B.dtype), float(beta),
+                                          X.ctypes.data, k, _dtype_code(X.dtype), k))
+            return X
+        if B.dtype != np.float64 or X.dtype != np.float64:
+            raise TBError(-1, "half solves take float64 arrays")
+        fn = {"upper": lib().tb_chol_upper_solve, "lower": lib().tb_chol_lower_solve}[which]
         _check(fn(self._h, float(alpha), B.ctypes.data, k, float(beta), X.ctypes.data, k, k))
         return X
 
@@ -264,8 +335,21 @@ class CholeskyDecomposition:
         if X is None:
             X = torch.empty_like(B)
             beta = 0.0
-        _check(lib().tb_chol_solve_device(self._h, float(alpha), B.data_ptr(), k, float(beta), X.data_ptr(), k, k))
+        codes = {torch.float64: TB_F64, torch.float32: TB_F32}
+        if B.dtype not in codes or X.dtype not in codes:
+            raise TBError(-1, "Solve: B and X must be float64 or float32 tensors")
+        if B.dtype == torch.float64 and X.dtype == torch.float64:
+            _check(lib().tb_chol_solve_device(self._h, float(alpha), B.data_ptr(), k, float(beta), X.data_ptr(), k, k))
+        else:
+            _check(lib().tb_chol_solve_device_ex(self._h, float(alpha), B.data_ptr(), k, codes[B.dtype], float(beta),
+                                                 X.data_ptr(), k, codes[X.dtype], k))
         return X
+
+    def SwapNumericalFactorization(self, factor: "NumericalFactorization") -> None:
+        """Exchanges this object's numeric factor with ``factor`` (Numeric.hpp:228-254).  A factor that
+        says factorized but not good, or is too small for this symbolic analysis, is then treated as
+        unfactorized; the object takes the incoming factor's precision."""
+        _check(lib().tb_chol_swap_factor(self._h, factor._h))
 
     def Solve(self, B, X=None, alpha: float = 1.0, beta: float = 0.0):
         """X = alpha * A^{-1} B + beta * X  (Solve.hpp:22-80); B is n or n x nrhs."""
@@ -462,7 +546,8 @@ class CholeskyDecomposition:
         m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 24))
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
                 "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks",
-                "solve_graph_tasks", "solve_split_level", "graph_ctas", "analyze_us", "plan_us"]
+                "solve_graph_tasks", "solve_split_level", "graph_ctas", "analyze_us", "plan_us", "tc_tiles",
+                "image_blocks"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

@@ -3,6 +3,7 @@
 
 #include "common.hpp"
 #include "kernels.cuh"
+#include "parallel.hpp"
 #include "plan.hpp"
 #include "plan_check.hpp"
 #include "schedule.hpp"
@@ -21,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace
@@ -140,6 +142,9 @@ struct tb_chol
     DeviceArray<tb::ExportTask>     exports;
     DeviceArray<double>             exported;    // reference-layout factor (tri then rec)
     DeviceArray<tb::GemmTask>       gemm;
+    DeviceArray<tb::TcTask>         tc;          // mixed precision: the GEMM updates as tensor-core tiles
+    DeviceArray<float>              img;         // mixed precision: the tiles' operand image (TF32 hi / lo)
+    tb::ImageMap                    img_map{};   // its tensor map
     DeviceArray<tb::PanelTask>      potrf, panel;
     DeviceArray<tb::ExtendTask>     extend;
     DeviceArray<tb::SolveDiagTask>  sdiag;
@@ -301,6 +306,7 @@ int ensure_device( tb_chol * h )
     if( !h->kernels_configured )
     {
         TB_CUDA( tb::configure_kernels() );
+        TB_CUDA( tb::configure_tc_tiles() );
         h->kernels_configured = true;
     }
     if( h->device_ready ) { return TB_OK; }
@@ -345,7 +351,17 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->status.reserve( 3 ) );
     TB_TRY( h->diag_off.upload( pl.diag_offset, st_ ) );
     TB_TRY( h->diag_vals.reserve( s.n ) );
-    if( h->precision == TB_PRECISION_MIXED ) { TB_TRY( h->pivot_floor.reserve( static_cast<std::int64_t>( s.n ) + 1 ) ); }
+    if( h->precision == TB_PRECISION_MIXED )
+    {
+        TB_TRY( h->pivot_floor.reserve( static_cast<std::int64_t>( s.n ) + 1 ) );
+        TB_TRY( h->tc.upload( pl.tc, st_ ) );
+        if( pl.img_blocks > 0 )
+        {
+            TB_TRY( h->img.reserve( pl.img_blocks * tb::kImgRows * tb::kImgK ) );
+            const int e = tb::encode_image_map( &h->img_map, h->img.ptr, pl.img_blocks );
+            if( e != 0 ) { return fail( TB_ERR_CUDA, "encoding the operand image's tensor map failed (" + std::to_string( e ) + ")" ); }
+        }
+    }
     TB_TRY( h->tinv.reserve( static_cast<std::int64_t>( pl.sdiag.size() ) * tb::kPanel * tb::kPanel ) );
     TB_TRY( h->dag.upload( pl.dag, st_ ) );
     TB_TRY( h->dag_state.reserve( static_cast<std::int64_t>( pl.dag_counters ) + 2 ) );
@@ -368,6 +384,23 @@ int ensure_device( tb_chol * h )
 
 template<typename T> T * arena_as( tb_chol * h ) { return reinterpret_cast<T *>( h->arena.ptr ); }
 
+// One GEMM launch of the level schedule.  FP64: its 64 x 64 DMMA tiles.
+// FP32: the 64 x 64 tiles of the fronts without an operand image (the launch's
+// first small_count tiles), then the tensor-core tiles of the others.
+template<typename T>
+void issue_gemm( tb_chol * h, const tb::Launch & L, T * A, cudaStream_t s )
+{
+    if constexpr ( sizeof(T) == 8 )
+    {
+        tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, s );
+    }
+    else
+    {
+        tb::launch_gemm( h->gemm.ptr + L.first, L.small_count, A, h->status.ptr, s );
+        tb::launch_gemm_tc_tiles( h->tc.ptr + L.tc_first, L.tc_count, A, h->img_map, h->status.ptr, s );
+    }
+}
+
 // Issues the numeric factorization on h->stream (capturable).  With
 // `timed`, every launch is bracketed by events (kind index in `kinds`).
 template<typename T>
@@ -376,6 +409,7 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
     const tb::Plan & pl = h->plan;
     cudaStream_t st = h->stream;
     T * A = arena_as<T>( h );
+    float * img = (sizeof(T) == 4 && h->img.ptr != nullptr) ? h->img.ptr : nullptr;
     std::int64_t launches = 0;
     std::size_t ev = 0;
     auto mark = [&]( int kind )
@@ -408,8 +442,8 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
                 case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
                 case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
                 case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, h->tinv.ptr, st ); break;
-                case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, st ); break;
-                case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, st ); break;
+                case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, st, img ); break;
+                case tb::LaunchKind::Gemm:   issue_gemm( h, L, A, st ); break;
                 default: break;
             }
             ++launches;
@@ -470,8 +504,8 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
             case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, s ); break;
             case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, s ); break;
             case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, h->tinv.ptr, s ); break;
-            case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, s ); break;
-            case tb::LaunchKind::Gemm:   tb::launch_gemm( h->gemm.ptr + L.first, L.count, A, h->status.ptr, s ); break;
+            case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, s, img ); break;
+            case tb::LaunchKind::Gemm:   issue_gemm( h, L, A, s ); break;
             default: break;
         }
         if( overlap && L.kind == tb::LaunchKind::Trsm ) { cudaEventRecord( h->ev_trsm, st ); }
@@ -589,7 +623,10 @@ int require_factor( tb_chol * h )
 // which it clears first.
 // With `timed`, every launch is bracketed by the handle's solve events and
 // described in solve_info (the events must exist).
-std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::int32_t k, bool timed = false )
+// levels_only: every level as a step launch, whatever the solve schedule (no
+// persistent launch, so no wait that can run out of time).
+std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::int32_t k, bool timed = false,
+                           bool levels_only = false )
 {
     const tb::Plan & pl = h->plan;
     cudaStream_t st = h->stream;
@@ -605,7 +642,7 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
     if( timed ) { h->solve_info.clear(); }
     const bool mixed = h->precision == TB_PRECISION_MIXED;
     // the levels from solve_split_level up: one persistent launch per sweep
-    bool graph = !pl.solve_fwd_order.empty();
+    bool graph = !levels_only && !pl.solve_fwd_order.empty();
     for( std::int32_t c0 = 0; c0 < k && graph; c0 += tb::kSolveMaxRhs )
     {
         const auto it = h->solve_grid.find( std::min( tb::kSolveMaxRhs, k - c0 ) );
@@ -956,10 +993,79 @@ int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, 
 }
 
 // Host-buffer solve through pinned staging buffers.
-int run_solve_host( tb_chol * h, int which, double alpha, const double * B, std::int32_t ldB,
-                    double beta, double * X, std::int32_t ldX, std::int32_t nrhs )
+// Host buffers of either scalar type (the reference casts on copy,
+// Solve.hpp:20-27, ReadNonzeroValues Numeric.hpp:165-180).
+int dtype_size( std::int32_t dtype ) { return dtype == TB_F32 ? 4 : dtype == TB_F64 ? 8 : 0; }
+
+// body(b, e) over rows [0, n) on all host threads once a copy is large
+// enough to be bound by one thread's memory bandwidth (about 4 MB a thread).
+template<typename Body>
+void host_rows( std::int64_t n, std::int64_t row_bytes, Body && body )
+{
+    const std::int64_t total = n * std::max<std::int64_t>( row_bytes, 1 );
+    const unsigned hw = std::max( 1u, std::thread::hardware_concurrency() );
+    const std::int64_t threads = std::min<std::int64_t>( std::min<std::int64_t>( hw, 16 ), std::max<std::int64_t>( 1, total >> 22 ) );
+    if( threads <= 1 || n < 2 ) { body( std::int64_t( 0 ), n ); return; }
+    std::vector<std::thread> pool;
+    for( std::int64_t t = 0; t < threads; ++t )
+    {
+        const std::int64_t b = n * t / threads, e = n * (t + 1) / threads;
+        pool.emplace_back( [&body, b, e]() { body( b, e ); } );
+    }
+    for( auto & th : pool ) { th.join(); }
+}
+
+// Packed n x k doubles <- caller rows of type dtype (leading dimension ld).
+void stage_rows_in( double * dst, const void * src, std::int32_t dtype, std::int64_t n, std::int32_t k, std::int32_t ld )
+{
+    host_rows( n, static_cast<std::int64_t>( k ) * 8, [&]( std::int64_t b, std::int64_t e )
+    {
+        if( dtype == TB_F64 )
+        {
+            const double * s = static_cast<const double *>( src );
+            if( ld == k ) { std::memcpy( dst + b * k, s + b * k, sizeof(double) * static_cast<size_t>( (e - b) * k ) ); return; }
+            for( std::int64_t i = b; i < e; ++i ) { std::memcpy( dst + i * k, s + i * ld, sizeof(double) * static_cast<size_t>( k ) ); }
+        }
+        else
+        {
+            const float * s = static_cast<const float *>( src );
+            for( std::int64_t i = b; i < e; ++i )
+            {
+                for( std::int32_t c = 0; c < k; ++c ) { dst[i * k + c] = static_cast<double>( s[i * ld + c] ); }
+            }
+        }
+    } );
+}
+
+// Caller rows of type dtype (leading dimension ld) <- packed n x k doubles.
+void stage_rows_out( void * dst, std::int32_t dtype, std::int32_t ld, const double * src, std::int64_t n, std::int32_t k )
+{
+    host_rows( n, static_cast<std::int64_t>( k ) * 8, [&]( std::int64_t b, std::int64_t e )
+    {
+        if( dtype == TB_F64 )
+        {
+            double * d = static_cast<double *>( dst );
+            if( ld == k ) { std::memcpy( d + b * k, src + b * k, sizeof(double) * static_cast<size_t>( (e - b) * k ) ); return; }
+            for( std::int64_t i = b; i < e; ++i ) { std::memcpy( d + i * ld, src + i * k, sizeof(double) * static_cast<size_t>( k ) ); }
+        }
+        else
+        {
+            float * d = static_cast<float *>( dst );
+            for( std::int64_t i = b; i < e; ++i )
+            {
+                for( std::int32_t c = 0; c < k; ++c ) { d[i * ld + c] = static_cast<float>( src[i * k + c] ); }
+            }
+        }
+    } );
+}
+
+// Host buffers of either type: staged through pinned memory on all host
+// threads (cast on copy), solved on the device, copied back.
+int run_solve_host( tb_chol * h, int which, double alpha, const void * B, std::int32_t ldB, std::int32_t b_dtype,
+                    double beta, void * X, std::int32_t ldX, std::int32_t x_dtype, std::int32_t nrhs )
 {
     if( B == nullptr || X == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: null buffer" ); }
+    if( dtype_size( b_dtype ) == 0 || dtype_size( x_dtype ) == 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: unknown scalar type" ); }
     const std::int32_t n = h->n;
     const std::int32_t k = std::max( 1, nrhs );
     if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
@@ -971,22 +1077,25 @@ int run_solve_host( tb_chol * h, int which, double alpha, const double * B, std:
     TB_TRY( h->out.reserve( static_cast<std::int64_t>(n) * k ) );
     double * pi = h->pin_in.as<double>();
     double * po = h->pin_out.as<double>();
-    if( ldB == k ) { std::memcpy( pi, B, bytes ); }
-    else { for( std::int64_t i = 0; i < n; ++i ) { std::memcpy( pi + i * k, B + i * ldB, sizeof(double) * k ); } }
+    stage_rows_in( pi, B, b_dtype, n, k, ldB );
     TB_CUDA( cudaMemcpyAsync( h->in.ptr, pi, bytes, cudaMemcpyHostToDevice, st ) );
     if( beta != 0.0 )
     {
-        if( ldX == k ) { std::memcpy( po, X, bytes ); }
-        else { for( std::int64_t i = 0; i < n; ++i ) { std::memcpy( po + i * k, X + i * ldX, sizeof(double) * k ); } }
+        stage_rows_in( po, X, x_dtype, n, k, ldX );
         TB_CUDA( cudaMemcpyAsync( h->out.ptr, po, bytes, cudaMemcpyHostToDevice, st ) );
     }
     TB_TRY( run_solve_device( h, which, alpha, h->in.ptr, k, beta, h->out.ptr, k, k ) );
     TB_CUDA( cudaMemcpyAsync( po, h->out.ptr, bytes, cudaMemcpyDeviceToHost, st ) );
     TB_CUDA( cudaStreamSynchronize( st ) );
     TB_TRY( check_solve_error( h ) );
-    if( ldX == k ) { std::memcpy( X, po, bytes ); }
-    else { for( std::int64_t i = 0; i < n; ++i ) { std::memcpy( X + i * ldX, po + i * k, sizeof(double) * k ); } }
+    stage_rows_out( X, x_dtype, ldX, po, n, k );
     return TB_OK;
+}
+
+int run_solve_host( tb_chol * h, int which, double alpha, const double * B, std::int32_t ldB,
+                    double beta, double * X, std::int32_t ldX, std::int32_t nrhs )
+{
+    return run_solve_host( h, which, alpha, B, ldB, TB_F64, beta, X, ldX, TB_F64, nrhs );
 }
 
 int fetch_diagonal( tb_chol * h, std::vector<double> & d )
@@ -1111,13 +1220,31 @@ int tb_chol_symbolic( tb_chol * h )
 
 int tb_chol_numeric( tb_chol * h, const double * values, double reg )
 {
+    return tb_chol_numeric_ex( h, values, TB_F64, reg );
+}
+
+int tb_chol_numeric_ex( tb_chol * h, const void * values, std::int32_t dtype, double reg )
+{
     TB_TRY( check_handle( h ) );
     if( values == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "NumericFactorization: null values" ); }
+    if( dtype_size( dtype ) == 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "NumericFactorization: unknown scalar type" ); }
     TB_TRY( ensure_device( h ) );
     const size_t bytes = sizeof(double) * static_cast<size_t>( h->sym.nnz );
     TB_TRY( h->pin_in.reserve( bytes ) );
-    std::memcpy( h->pin_in.ptr, values, bytes );
+    stage_rows_in( h->pin_in.as<double>(), values, dtype, h->sym.nnz, 1, 1 );
     TB_CUDA( cudaMemcpyAsync( h->values.ptr, h->pin_in.ptr, bytes, cudaMemcpyHostToDevice, h->stream ) );
+    return run_factor( h, reg );
+}
+
+int tb_chol_numeric_device_ex( tb_chol * h, const void * d_values, std::int32_t dtype, double reg )
+{
+    TB_TRY( check_handle( h ) );
+    if( d_values == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "NumericFactorization: null values" ); }
+    if( dtype == TB_F64 ) { return tb_chol_numeric_device( h, static_cast<const double *>( d_values ), reg ); }
+    if( dtype != TB_F32 ) { return fail( TB_ERR_INVALID_ARGUMENT, "NumericFactorization: unknown scalar type" ); }
+    TB_TRY( ensure_device( h ) );
+    tb::launch_widen( static_cast<const float *>( d_values ), 1, h->values.ptr, 1, h->sym.nnz, 1, h->stream );
+    TB_CUDA( cudaGetLastError() );
     return run_factor( h, reg );
 }
 
@@ -1520,7 +1647,8 @@ int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
         static_cast<std::int64_t>( pl.upper_launches.size() ), h->sym.sn_count, pl.front_count,
         static_cast<std::int64_t>( pl.front_flops ), static_cast<std::int64_t>( pl.dag_makespan_us ),
         static_cast<std::int64_t>( pl.dag.size() ), static_cast<std::int64_t>( pl.solve_fwd_order.size() ),
-        pl.solve_split_level, h->dag_grid, h->analyze_us, h->plan_us };
+        pl.solve_split_level, h->dag_grid, h->analyze_us, h->plan_us,
+        static_cast<std::int64_t>( pl.tc.size() ), pl.img_blocks };
     const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
     for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
     return m;
@@ -1866,6 +1994,166 @@ int tb_chol_launch_counts( tb_chol * h, std::int64_t * factor_launches, std::int
 } // extern "C"
 
 // ---------------------------------------------------------------------------
+// Scalar types at the boundary and the numeric-factor container.
+// ---------------------------------------------------------------------------
+
+// NumericalFactorization_T (CholeskyDecomposition.hpp:132-201): a numeric
+// factor held apart from any handle.  Here it is the device state a
+// factorization leaves behind: the front storage (FP64, or FP32 in the
+// mixed-precision mode), the inverse diagonal blocks the solves use, the
+// matrix values and shift the mixed mode's refinement needs, and the
+// factorized / good flags.
+struct tb_factor
+{
+    int device = -1;
+    DeviceArray<double> arena, tinv, values;
+    int precision = -1;                          // of the stored factor; -1: never held one
+    double last_reg = 0.0;
+    bool factorized = false, good = false, fell_back = false;
+    std::int32_t failed_sn = -1, perturbed_pivots = 0;
+};
+
+namespace
+{
+
+template<typename T> void swap_arrays( DeviceArray<T> & a, DeviceArray<T> & b )
+{
+    std::swap( a.ptr, b.ptr );
+    std::swap( a.size, b.size );
+}
+
+// Device sizes a factor of the handle's symbolic analysis needs, for a precision.
+std::int64_t required_arena( const tb_chol * h, int precision )
+{
+    return precision == TB_PRECISION_MIXED ? (h->plan.arena_size() + 1) / 2 : h->plan.arena_size();
+}
+
+} // namespace
+
+extern "C" {
+
+int tb_factor_create( tb_factor ** out )
+{
+    if( out == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null output" ); }
+    *out = new tb_factor();
+    return TB_OK;
+}
+
+int tb_factor_destroy( tb_factor * f )
+{
+    int caller = -1;
+    if( f != nullptr && f->device >= 0 && cudaGetDevice( &caller ) == cudaSuccess ) { cudaSetDevice( f->device ); }
+    delete f;
+    if( caller >= 0 ) { cudaSetDevice( caller ); }
+    return TB_OK;
+}
+
+int tb_factor_state( tb_factor * f, std::int32_t * factorized, std::int32_t * good, std::int64_t * bytes,
+                     std::int32_t * precision )
+{
+    if( f == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "null factor" ); }
+    if( factorized ) { *factorized = f->factorized ? 1 : 0; }
+    if( good ) { *good = f->good ? 1 : 0; }
+    if( bytes ) { *bytes = 8 * (f->arena.size + f->tinv.size + f->values.size); }
+    if( precision ) { *precision = f->precision; }
+    return TB_OK;
+}
+
+int tb_chol_swap_factor( tb_chol * h, tb_factor * f )
+{
+    TB_TRY( check_handle( h ) );
+    if( f == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "SwapNumericalFactorization: null factor" ); }
+    if( f->device >= 0 && f->device != h->device )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "SwapNumericalFactorization: the factor lives on another device" );
+    }
+    TB_TRY( ensure_symbolic( h ) );
+    // captured factor and solve graphs hold the outgoing storage's addresses
+    if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    h->drop_solve_graphs();
+    if( h->device_ready ) { TB_CUDA( cudaSetDevice( h->device ) ); TB_CUDA( cudaStreamSynchronize( h->stream ) ); }
+    const int incoming = f->precision;
+    swap_arrays( h->arena, f->arena );
+    swap_arrays( h->tinv, f->tinv );
+    swap_arrays( h->values, f->values );
+    std::swap( h->last_reg, f->last_reg );
+    std::swap( h->factorized, f->factorized );
+    std::swap( h->good, f->good );
+    std::swap( h->fell_back, f->fell_back );
+    std::swap( h->failed_sn, f->failed_sn );
+    std::swap( h->perturbed_pivots, f->perturbed_pivots );
+    f->precision = h->precision;
+    f->device = h->device;
+    if( incoming >= 0 && incoming != h->precision )
+    {
+        // the factor's storage width: the next factorization re-creates the device plan for it
+        h->precision = incoming;
+        h->device_ready = false;
+    }
+    // Numeric.hpp:232-253: a factor marked factorized but not good, or too
+    // small for this symbolic analysis, is treated as unfactorized
+    if( h->factorized && !h->good ) { h->factorized = false; }
+    const std::int64_t need_tinv = static_cast<std::int64_t>( h->plan.sdiag.size() ) * tb::kPanel * tb::kPanel;
+    if( h->factorized && (h->arena.size < required_arena( h, h->precision ) || h->tinv.size < need_tinv
+                          || h->values.size < h->sym.nnz || h->arena.ptr == nullptr) )
+    {
+        h->factorized = false;
+        h->good = false;
+    }
+    if( h->device_ready )
+    {
+        // the device plan stays: storage too small for it is grown (its contents are then moot)
+        TB_TRY( h->arena.reserve( required_arena( h, h->precision ) ) );
+        TB_TRY( h->tinv.reserve( need_tinv ) );
+        TB_TRY( h->values.reserve( h->sym.nnz ) );
+    }
+    return TB_OK;
+}
+
+int tb_chol_solve_ex( tb_chol * h, double alpha, const void * B, std::int32_t ldB, std::int32_t b_dtype,
+                      double beta, void * X, std::int32_t ldX, std::int32_t x_dtype, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    return run_solve_host( h, 2, alpha, B, ldB, b_dtype, beta, X, ldX, x_dtype, nrhs );
+}
+
+int tb_chol_solve_device_ex( tb_chol * h, double alpha, const void * d_B, std::int32_t ldB, std::int32_t b_dtype,
+                             double beta, void * d_X, std::int32_t ldX, std::int32_t x_dtype, std::int32_t nrhs )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    if( d_B == nullptr || d_X == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: null buffer" ); }
+    if( dtype_size( b_dtype ) == 0 || dtype_size( x_dtype ) == 0 ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: unknown scalar type" ); }
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    if( b_dtype == TB_F64 && x_dtype == TB_F64 )
+    {
+        return run_solve_device( h, 2, alpha, static_cast<const double *>( d_B ), ldB, beta, static_cast<double *>( d_X ), ldX, nrhs );
+    }
+    cudaStream_t st = h->stream;
+    const double * B = static_cast<const double *>( d_B );
+    std::int32_t ldb = ldB;
+    if( b_dtype == TB_F32 )
+    {
+        TB_TRY( h->in.reserve( static_cast<std::int64_t>( n ) * k ) );
+        tb::launch_widen( static_cast<const float *>( d_B ), ldB, h->in.ptr, k, n, k, st );
+        B = h->in.ptr;
+        ldb = k;
+    }
+    if( x_dtype == TB_F64 ) { return run_solve_device( h, 2, alpha, B, ldb, beta, static_cast<double *>( d_X ), ldX, nrhs ); }
+    TB_TRY( h->out.reserve( static_cast<std::int64_t>( n ) * k ) );
+    if( beta != 0.0 ) { tb::launch_widen( static_cast<const float *>( d_X ), ldX, h->out.ptr, k, n, k, st ); }
+    TB_TRY( run_solve_device( h, 2, alpha, B, ldb, beta, h->out.ptr, k, nrhs ) );
+    tb::launch_narrow( h->out.ptr, k, static_cast<float *>( d_X ), ldX, n, k, st );
+    TB_CUDA( cudaGetLastError() );
+    return TB_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
 // Solve without any device allocation.
 //
 // Some callers cannot allocate device memory at solve time: a real-time loop
@@ -1889,6 +2177,16 @@ int tb_chol_launch_counts( tb_chol * h, std::int64_t * factor_launches, std::int
 //  - There is one array per device, shared by every handle: calls whose
 //    solves can overlap on the device (other streams, other host threads)
 //    race on it and must be serialised by the caller.
+//  - It applies the FP64 factor once (the direct solve).  A mixed-precision
+//    handle, or one that fell back to FP64 after a failed refinement, is
+//    solved by refinement with more work vectors than this array holds, so
+//    such handles are rejected with TB_ERR_INVALID_ARGUMENT.
+//  - The sweeps always run as level launches, whatever the handle's solve
+//    schedule: they contain no waits, so this path cannot time out.
+//  - The array is part of the library's device code: with lazy module
+//    loading (the CUDA default) it takes device memory once the first call
+//    looks it up; with CUDA_MODULE_LOADING=EAGER every context that loads the
+//    library holds the 64 MiB from the start.
 // ---------------------------------------------------------------------------
 namespace
 {
@@ -1907,9 +2205,22 @@ int noalloc_scratch( int device, double ** out )
     std::lock_guard<std::mutex> lock( g_noalloc_mutex );
     if( g_noalloc_ptr[device] == nullptr )
     {
+        // the symbol resolves on the current device: make it the handle's,
+        // then give the caller back the device it had current
+        int caller = 0;
+        TB_CUDA( cudaGetDevice( &caller ) );
         void * p = nullptr;
-        TB_CUDA( cudaSetDevice( device ) );
-        TB_CUDA( cudaGetSymbolAddress( &p, g_noalloc_scratch ) );
+        cudaError_t e = cudaSetDevice( device );
+        if( e == cudaSuccess ) { e = cudaGetSymbolAddress( &p, g_noalloc_scratch ); }
+        const cudaError_t back = cudaSetDevice( caller );
+        if( e != cudaSuccess )
+        {
+            return fail( TB_ERR_CUDA, std::string( "solve_device_noalloc: looking up the fixed scratch: " ) + cudaGetErrorString( e ) );
+        }
+        if( back != cudaSuccess )
+        {
+            return fail( TB_ERR_CUDA, std::string( "solve_device_noalloc: restoring the current device: " ) + cudaGetErrorString( back ) );
+        }
         g_noalloc_ptr[device] = static_cast<double *>( p );
     }
     *out = g_noalloc_ptr[device];
@@ -1926,6 +2237,12 @@ int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B,
     TB_TRY( check_handle( h ) );
     TB_TRY( require_factor( h ) );
     if( d_B == nullptr || d_X == nullptr ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: null buffer" ); }
+    if( h->precision == TB_PRECISION_MIXED || h->fell_back )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "solve_device_noalloc: the handle solves by refinement (mixed precision, "
+                     "or FP64 after a failed refinement), which needs work vectors beyond the fixed scratch; "
+                     "use tb_chol_solve_device" );
+    }
     const std::int32_t n = h->n;
     const std::int32_t k = std::max( 1, nrhs );
     if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
@@ -1937,12 +2254,11 @@ int tb_chol_solve_device_noalloc( tb_chol * h, double alpha, const double * d_B,
     }
     double * W = nullptr;
     TB_TRY( noalloc_scratch( h->device, &W ) );
-    TB_TRY( prepare_solve_grid( h, k ) );
     double * Y = W + kNoAllocScratchEntries;
     cudaStream_t st = h->stream;
     std::int64_t launches = 2;
     tb::launch_gather_rows( d_B, ldB, h->p.ptr, W, k, n, k, st );
-    launches += issue_sweeps( h, 2, W, Y, k );
+    launches += issue_sweeps( h, 2, W, Y, k, false, true );
     tb::launch_scatter_rows( W, k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );
     h->solve_launch_count = launches;
     TB_CUDA( cudaGetLastError() );

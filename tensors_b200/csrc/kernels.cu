@@ -217,6 +217,14 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
     extend_body( tasks[blockIdx.x], lut_all, arena );
 }
 
+// TF32 rounding (round to nearest, ties away) of an FP32 value, as bits.
+__device__ __forceinline__ unsigned to_tf32( float x )
+{
+    unsigned r;
+    asm( "cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x) );
+    return r;
+}
+
 // ------------------------------------------------------------------ panel
 // Cholesky of a panel's nb x nb diagonal block, in shared memory and then
 // in place (LAPACK potrf of FactorizeSupernode, Multifrontal.hpp:438-449).
@@ -491,9 +499,19 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
 // takes the K blocks 0..rb.  Warp w computes the output tiles (rb, ct) with
 // rb = (w + ct) mod 8, one of every block row, so every warp does the same
 // 36 8 x 8 x 8 DMMA steps (when nb = 64); no step waits on another.
+// Operand-image entry of U row k, rest column `col` of a panel whose rest
+// columns start at U0 column r1 (m of them in U0, the rest U1 columns).
+__device__ __forceinline__ std::int64_t img_offset( const PanelTask & t, int k, int col, int r1, int m )
+{
+    const int ucol = col < m ? r1 + col : col - m;
+    const int ct = col < m ? ucol / kImgRows : t.img_t0 + ucol / kImgRows;
+    const std::int64_t blk = t.img + static_cast<std::int64_t>( k / kImgK ) * 2 * t.img_tf + ct;
+    return blk * (kImgRows * kImgK) + (ucol % kImgRows) * kImgK + (k % kImgK);
+}
+
 template<typename T>
 __device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__ arena, const double * __restrict__ tinv,
-                                           double * tsm )
+                                           double * tsm, float * __restrict__ img = nullptr )
 {
     double (*Ti)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm );
     double (*X)[kXld] = reinterpret_cast<double (*)[kXld]>( tsm + kPanel * kXld );
@@ -552,8 +570,36 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__
             if( r < nb && cc < cw )
             {
                 const int col = t.c0 + cc;
-                if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = static_cast<T>( acc[e] ); }
-                else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = static_cast<T>( acc[e] ); }
+                const T v = static_cast<T>( acc[e] );
+                if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = v; }
+                else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = v; }
+                if constexpr ( sizeof(T) == 4 )
+                {
+                    if( img != nullptr && t.img >= 0 )
+                    {
+                        // the stored FP32 value split into TF32 hi + lo, for the tensor-core tiles
+                        const unsigned hi = to_tf32( v );
+                        const std::int64_t o = img_offset( t, t.r0 + r, col, r1, m );
+                        img[o] = __uint_as_float( hi );
+                        img[o + static_cast<std::int64_t>( t.img_tf ) * (kImgRows * kImgK)] = __uint_as_float( to_tf32( v - __uint_as_float( hi ) ) );
+                    }
+                }
+            }
+        }
+    }
+    if constexpr ( sizeof(T) == 4 )
+    {
+        // the last panel: image rows n0 .. (n0 rounded up to the 32-row k-chunk) are zero, so
+        // that the update matrix's tiles (K = n0) can read whole chunks
+        if( img != nullptr && t.img >= 0 && t.r0 + nb == t.n0 )
+        {
+            const int pad = (kImgK - t.n0 % kImgK) % kImgK;
+            for( int idx = threadIdx.x; idx < pad * cw; idx += kTrsmThreads )
+            {
+                const int k = t.n0 + idx / cw, col = t.c0 + idx % cw;
+                const std::int64_t o = img_offset( t, k, col, r1, m );
+                img[o] = 0.0f;
+                img[o + static_cast<std::int64_t>( t.img_tf ) * (kImgRows * kImgK)] = 0.0f;
             }
         }
     }
@@ -561,10 +607,11 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__
 
 template<typename T>
 __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * __restrict__ tasks,
-                                                             T * __restrict__ arena, const double * __restrict__ tinv )
+                                                             T * __restrict__ arena, const double * __restrict__ tinv,
+                                                             float * __restrict__ img )
 {
     extern __shared__ __align__(16) double tsm[];
-    trsm_body( tasks[blockIdx.x], arena, tinv, tsm );
+    trsm_body( tasks[blockIdx.x], arena, tinv, tsm, img );
 }
 
 // ------------------------------------------------------------------- gemm
@@ -704,13 +751,6 @@ constexpr unsigned kTcMaxPolls = 1u << 24;             // bound on the polls of 
 constexpr unsigned long long kTcTimeoutNs = 1000000000ull;
 constexpr int kStatusTcTimeout = 2;                    // status[0] bit: a tensor-core completion wait ran out
 static_assert( kGemmSmemBytesF >= sizeof(float) * kTile * kTcSld, "result staging does not fit" );
-
-__device__ __forceinline__ unsigned to_tf32( float x )
-{
-    unsigned r;
-    asm( "cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x) );
-    return r;
-}
 
 __device__ __forceinline__ std::uint32_t smem_u32( const void * p )
 {
@@ -1659,9 +1699,9 @@ void launch_pivot_floor( const std::int64_t * offsets, const float * arena, doub
 }
 
 template<typename T>
-void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st )
+void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st, float * img )
 {
-    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, kTrsmSmemBytes, st>>>( tasks, arena, tinv ); }
+    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, kTrsmSmemBytes, st>>>( tasks, arena, tinv, img ); }
 }
 
 template<typename T>
@@ -1781,7 +1821,7 @@ void launch_gather_diag( const std::int64_t * offsets, const T * arena, double *
                                     cudaStream_t );                                                                \
     template void launch_extend<T>( const ExtendTask *, int, const std::int32_t *, T *, cudaStream_t );             \
     template void launch_potrf<T>( const PanelTask *, int, T *, int *, const double *, double *, cudaStream_t );     \
-    template void launch_trsm<T>( const PanelTask *, int, T *, const double *, cudaStream_t );                       \
+    template void launch_trsm<T>( const PanelTask *, int, T *, const double *, cudaStream_t, float * );              \
     template void launch_gemm<T>( const GemmTask *, int, T *, int *, cudaStream_t );                                 \
     template void launch_solve_dag<T>( const SolveDagArgs &, int, const T *, double *, double *, int, int, cudaStream_t );                                        \
     template void launch_factor_dag<T>( const DagArgs &, int, cudaStream_t );                                        \
@@ -1879,6 +1919,31 @@ void launch_axpy( std::int64_t n, double a, const double * x, double * y, cudaSt
 void launch_combine( int n, int k, double alpha, const double * X, int ldx, double beta, double * Y, int ldy, cudaStream_t st )
 {
     combine_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( n, k, alpha, X, ldx, beta, Y, ldy );
+}
+
+// Row-major n x k blocks between the two scalar types (the reference casts
+// right-hand sides and solutions on copy, Solve.hpp:20-27).
+template<typename S, typename D>
+__global__ void convert_rows_kernel( const S * __restrict__ src, int lds, D * __restrict__ dst, int ldd, std::int64_t n, int k )
+{
+    const std::int64_t total = n * k;
+    for( std::int64_t i = blockIdx.x * static_cast<std::int64_t>( blockDim.x ) + threadIdx.x; i < total;
+         i += static_cast<std::int64_t>( gridDim.x ) * blockDim.x )
+    {
+        const std::int64_t r = i / k;
+        const int c = static_cast<int>( i - r * k );
+        dst[r * ldd + c] = static_cast<D>( src[r * lds + c] );
+    }
+}
+
+void launch_widen( const float * src, int lds, double * dst, int ldd, std::int64_t n, int k, cudaStream_t st )
+{
+    if( n * k > 0 ) { convert_rows_kernel<float, double><<<grid_for( std::min<std::int64_t>( n * k, std::int64_t( 1 ) << 24 ), 256 ), 256, 0, st>>>( src, lds, dst, ldd, n, k ); }
+}
+
+void launch_narrow( const double * src, int lds, float * dst, int ldd, std::int64_t n, int k, cudaStream_t st )
+{
+    if( n * k > 0 ) { convert_rows_kernel<double, float><<<grid_for( std::min<std::int64_t>( n * k, std::int64_t( 1 ) << 24 ), 256 ), 256, 0, st>>>( src, lds, dst, ldd, n, k ); }
 }
 
 void launch_init_status( int * status, cudaStream_t st )

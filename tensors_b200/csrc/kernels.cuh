@@ -32,11 +32,25 @@ template<typename T> void launch_potrf( const PanelTask * tasks, int count, T * 
                                         const double * pivot_floor, double * tinv, cudaStream_t st );
 // out (n + 1 doubles): the pivot floors in the layout of launch_potrf's pivot_floor.
 void launch_pivot_floor( const std::int64_t * offsets, const float * arena, double rel, double * out, int n, cudaStream_t st );
-// Uses the inverse diagonal blocks the panels' potrf wrote to tinv.
-template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st );
+// Uses the inverse diagonal blocks the panels' potrf wrote to tinv.  img
+// (FP32 path, else null): the operand image the trsm also writes its panel
+// rows into, split into TF32 hi and lo (tasks with PanelTask::img >= 0).
+template<typename T> void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st,
+                                       float * img = nullptr );
 // status[0] gets kStatusTcTimeout (2) when a tensor-core completion wait of
 // the FP32 path ran out (its tile is then not updated).
 template<typename T> void launch_gemm( const GemmTask * tasks, int count, T * arena, int * status, cudaStream_t st );
+
+// The tensor map (CUtensorMap, 128 bytes) of the operand image, held by the
+// host and passed to the tile kernel by value.
+struct alignas(64) ImageMap { unsigned char bytes[128]; };
+// Encodes the map of an operand image of `blocks` blocks at img; 0 on success.
+int encode_image_map( ImageMap * out, const float * img, std::int64_t blocks );
+// The FP32 path's tensor-core tiles (TcTask) of one launch: persistent CTAs,
+// one per SM.  status[0] gets bit 2 when a wait of the kernel ran out.
+void launch_gemm_tc_tiles( const TcTask * tasks, int count, float * arena, const ImageMap & map, int * status,
+                           cudaStream_t st );
+cudaError_t configure_tc_tiles();
 
 // The numeric factorization as one persistent launch over the plan's task
 // graph (Plan::dag).  counters (dag_counters ints), next and error must be
@@ -115,6 +129,9 @@ void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv,
 void launch_residual( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
                       const double * X, const double * B, double * R, int k, cudaStream_t st );
 void launch_init_status( int * status, cudaStream_t st );
+// dst (n x k, leading dimension ldd) = src (leading dimension lds), converted.
+void launch_widen( const float * src, int lds, double * dst, int ldd, std::int64_t n, int k, cudaStream_t st );
+void launch_narrow( const double * src, int lds, float * dst, int ldd, std::int64_t n, int k, cudaStream_t st );
 // R = B - (A + shift I) X, or (A + shift I) X when B is null;
 // out[c] += X(:, c) . Y(:, c); the two CG updates with per-column scalars on
 // the device; y += a x; Y = alpha X + beta Y.

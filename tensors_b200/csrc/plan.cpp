@@ -40,6 +40,30 @@ void push_tiles( std::vector<GemmTask> & out, I64 a, I32 lda, I64 b, I32 ldb, I6
     }
 }
 
+// The tensor-core tiles of the fronts with an operand image (see TcTask):
+// kTcM x nt tiles (nt up to kTcNMax) over C's M x N entries (symmetric: the
+// tiles on and right of the diagonal).  next_rows: the call updates the next
+// panel's rows, which the tiles of the first tile row contain.
+void push_tc( std::vector<TcTask> & out, std::vector<char> & next, bool next_rows, I64 blk, I32 tf,
+              I32 ta0, I32 tb0, I32 K, I64 c, I32 ldc, I32 M, I32 N, bool symmetric )
+{
+    for( I32 m0 = 0; m0 < M; m0 += kTcM )
+    {
+        for( I32 c0 = symmetric ? m0 : 0; c0 < N; c0 += kTcNMax )
+        {
+            TcTask t{};
+            t.c = c; t.blk = blk;
+            t.ldc = ldc; t.M = M; t.N = N;
+            t.m0 = m0; t.c0 = c0; t.K = K;
+            t.ta = ta0 + m0 / kImgRows; t.tb = tb0 + c0 / kImgRows; t.tf = tf;
+            t.nt = static_cast<I32>( std::min<I64>( kTcNMax, ceil_div( N - c0, kImgRows ) * kImgRows ) );
+            t.upper = symmetric ? 1 : 0;
+            out.push_back( t );
+            next.push_back( next_rows && m0 == 0 ? 1 : 0 );
+        }
+    }
+}
+
 // Best-fit allocator over [0, capacity) with a coalescing free list; grows
 // the capacity when nothing fits.  Free blocks are indexed both by address
 // (for coalescing) and by (size, address) (for the O(log n) best-fit lookup),
@@ -357,8 +381,26 @@ void Plan::build( const Symbolic & sym )
         }
     }
 
+    // ------------------------------------------------ operand image
+    // Fronts whose widest update has at least 128 columns (and >= 16 pivot
+    // rows) get an operand image and tensor-core tiles on the FP32 path; the
+    // updates of the smaller ones stay 64 x 64 tiles (an image block holds 32
+    // rows of k and 64 columns, mostly empty for them).
+    front_img.assign( static_cast<size_t>(F), -1 );
+    img_blocks = 0;
+    std::vector<I32> img_t0( static_cast<size_t>(F), 0 ), img_tf( static_cast<size_t>(F), 0 );
+    for( I32 f = 0; f < F; ++f )
+    {
+        const I32 n0 = front_n0[f], n1 = front_n1[f];
+        if( n0 < 16 || std::max<I32>( n0 - kPanel, 0 ) + n1 < 2 * kImgRows ) { continue; }
+        img_t0[f] = static_cast<I32>( ceil_div( n0, kImgRows ) );
+        img_tf[f] = img_t0[f] + static_cast<I32>( ceil_div( n1, kImgRows ) );
+        front_img[f] = img_blocks;
+        img_blocks += ceil_div( n0, kImgK ) * 2 * img_tf[f];
+    }
+
     // -------------------------------------------------- launch sequences
-    gemm.clear(); potrf.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
+    gemm.clear(); tc.clear(); potrf.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
     gemm_flops = 0.0;
     factor_launches.clear(); lower_launches.clear(); upper_launches.clear();
     dag.clear();
@@ -508,7 +550,9 @@ void Plan::build( const Symbolic & sym )
             const I64 rfirst = static_cast<I64>(srest.size());
             std::vector<GemmTask> tiles;
             std::vector<I32> tile_panel, tile_prev;
-            std::vector<char> tile_next;
+            std::vector<char> tile_next, tile_small;
+            std::vector<TcTask> tct;
+            std::vector<char> tct_next;
             for( I32 f : L )
             {
                 const I32 n0 = front_n0[f], n1 = front_n1[f];
@@ -535,6 +579,7 @@ void Plan::build( const Symbolic & sym )
                 t.row0 = front_row0[f];
                 t.single_rows = singles;
                 t.panel = pi;                   // == sdiag.size(): one potrf task and one SolveDiagTask per panel
+                t.img = front_img[f]; t.img_t0 = img_t0[f]; t.img_tf = img_tf[f];
                 {
                     PendingTask d = make( LaunchKind::Potrf, static_cast<I64>(potrf.size()) );
                     // the first panel starts once the children's contributions are in and
@@ -580,12 +625,31 @@ void Plan::build( const Symbolic & sym )
                     }
                     // tiles of rows [r1, r1 + 64) feed the next panel
                     for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_next.push_back( tiles[i].m0 == 0 ? 1 : 0 ); }
+                    if( front_img[f] >= 0 )
+                    {
+                        // r1 and k0 are multiples of 64: whole image column tiles and k-chunks
+                        const I64 blk = front_img[f] + static_cast<I64>( k0 / kImgK ) * 2 * img_tf[f];
+                        const I32 ta = r1 / kImgRows;
+                        push_tc( tct, tct_next, true, blk, img_tf[f], ta, ta, K,
+                                 front_u0[f] + static_cast<I64>(r1) * ld0 + r1, ld0, rows, m, true );
+                        if( n1 > 0 )
+                        {
+                            push_tc( tct, tct_next, true, blk, img_tf[f], ta, img_t0[f], K,
+                                     front_u1[f] + static_cast<I64>(r1) * ld1, ld1, rows, n1, false );
+                        }
+                    }
                 }
                 else if( n1 > 0 && front_parent[f] < F )
                 {
                     push_tiles( tiles, front_u1[f], ld1, front_u1[f], ld1, front_v[f], ld1, n0, n1, n1, true );
                     for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_next.push_back( 0 ); }
+                    if( front_img[f] >= 0 )
+                    {
+                        push_tc( tct, tct_next, false, front_img[f], img_tf[f], img_t0[f], img_t0[f], n0,
+                                 front_v[f], ld1, n1, n1, true );
+                    }
                 }
+                for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_small.push_back( front_img[f] < 0 ? 1 : 0 ); }
                 for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_panel.push_back( pi ); tile_prev.push_back( prev ); }
                 {
                     SolveRestTask t{};
@@ -611,6 +675,7 @@ void Plan::build( const Symbolic & sym )
             for( size_t i = 0; i < order.size(); ++i ) { order[i] = i; }
             std::stable_sort( order.begin(), order.end(), [&]( size_t x, size_t y ) {
                 if( tile_next[x] != tile_next[y] ) { return tile_next[x] > tile_next[y]; }
+                if( tile_small[x] != tile_small[y] ) { return tile_small[x] > tile_small[y]; }
                 return tiles[x].K > tiles[y].K;
             } );
             for( size_t i : order )
@@ -637,11 +702,37 @@ void Plan::build( const Symbolic & sym )
             if( oc > 0 ) { factor_launches.push_back( { LaunchKind::Potrf, oc, ofirst, h, q } ); }
             if( pc > 0 ) { factor_launches.push_back( { LaunchKind::Trsm, pc, pfirst, h, q } ); }
             {
-                // the step's tiles are in the order of `order`: the next panel's rows first
-                I32 gn = 0;
-                for( size_t i : order ) { gn += tile_next[i] ? 1 : 0; }
-                if( gn > 0 ) { factor_launches.push_back( { LaunchKind::Gemm, gn, gfirst, h, q, 0 } ); }
-                if( gc > gn ) { factor_launches.push_back( { LaunchKind::Gemm, gc - gn, gfirst + gn, h, q, 1 } ); }
+                // the step's tiles are in the order of `order`: the next panel's rows first,
+                // within each part the tiles of fronts without an operand image first
+                I32 gn = 0, sn0 = 0, sn1 = 0;
+                for( size_t i : order )
+                {
+                    gn += tile_next[i] ? 1 : 0;
+                    if( tile_small[i] ) { (tile_next[i] ? sn0 : sn1) += 1; }
+                }
+                // the same updates as tensor-core tiles: next-row tiles first, deepest first
+                std::vector<size_t> tord( tct.size() );
+                for( size_t i = 0; i < tord.size(); ++i ) { tord[i] = i; }
+                std::stable_sort( tord.begin(), tord.end(), [&]( size_t x, size_t y ) {
+                    if( tct_next[x] != tct_next[y] ) { return tct_next[x] > tct_next[y]; }
+                    return tct[x].K > tct[y].K;
+                } );
+                const I64 tfirst = static_cast<I64>( tc.size() );
+                I32 tn = 0;
+                for( size_t i : tord ) { tc.push_back( tct[i] ); tn += tct_next[i] ? 1 : 0; }
+                const I32 tcount = static_cast<I32>( tct.size() );
+                if( gn > 0 )
+                {
+                    Launch L{ LaunchKind::Gemm, gn, gfirst, h, q, 0 };
+                    L.small_count = sn0; L.tc_first = tfirst; L.tc_count = tn;
+                    factor_launches.push_back( L );
+                }
+                if( gc > gn )
+                {
+                    Launch L{ LaunchKind::Gemm, gc - gn, gfirst + gn, h, q, 1 };
+                    L.small_count = sn1; L.tc_first = tfirst + tn; L.tc_count = tcount - tn;
+                    factor_launches.push_back( L );
+                }
             }
             rest_ranges[h][q] = { rfirst, static_cast<I32>( static_cast<I64>(srest.size()) - rfirst ) };
         }

@@ -89,6 +89,41 @@ struct PanelTask
     std::int32_t row0;
     std::int32_t panel;            // index of the panel (its potrf task, SolveDiagTask and inverse block)
     std::int64_t single_rows;      // bit r set: panel row r is a 1 x 1 reference supernode
+    std::int64_t img;              // FP32 path: the front's first operand-image block (see TcTask)
+    std::int32_t img_t0, img_tf;   // its U0 column tiles, and U0 + U1 column tiles per k-chunk segment
+};
+
+// The FP32 path's Schur-complement tiles on the 5th-generation tensor cores
+// read their operands from an *operand image*: every panel row of a front,
+// once its trsm is done, split into TF32 hi and lo parts (x = hi + lo) and
+// stored transposed in blocks of kImgRows U columns x kImgK U rows (row-major
+// inside the block: the 32 k values of one U column are 128 contiguous bytes,
+// one 128-byte-swizzled row of a K-major tensor-core operand).  Block
+// (k-chunk kc, part hl, column tile ct) of front f is
+//     img + (kc * 2 + hl) * tf + ct,
+// where column tiles 0 .. t0-1 are U0 columns and t0 .. tf-1 are U1 columns
+// (each 64-aligned), so every operand tile is a few whole blocks: one tensor
+// map over the whole image serves every front.
+constexpr int kImgRows = 64;
+constexpr int kImgK    = 32;
+constexpr int kTcM     = 128;     // tensor-core tile rows
+constexpr int kTcNMax  = 256;     // widest tensor-core tile
+
+// C[m0 : m0+kTcM, c0 : c0+nt] -= A^T B for K panel rows: A's columns are
+// operand-image column tiles ta, ta+1 (the C rows), B's are tb .. tb+nt/64-1,
+// over the k-chunks blk, blk + 2 tf, ... (hi; lo at + tf).  Rows >= M and
+// columns >= N are not written; upper: only (row <= col) entries.
+struct TcTask
+{
+    std::int64_t c;                // arena offset of C[0][0]
+    std::int64_t blk;              // image block of (first k-chunk, hi, column tile 0)
+    std::int32_t ldc, M, N;
+    std::int32_t m0, c0;
+    std::int32_t K;
+    std::int32_t ta, tb, tf;
+    std::int32_t nt;               // tile width: 64, 128, 192 or 256
+    std::int32_t upper;
+    std::int32_t pad;
 };
 
 // Add rows [row_begin, row_end) of child update W (m1 x m1, upper) into the
@@ -184,6 +219,12 @@ struct Launch
     std::int32_t level;
     std::int32_t step;
     std::int32_t part = 0;
+    // Gemm launches, FP32 path: the first small_count tiles belong to fronts
+    // without an operand image (64 x 64 tiles); the updates of the other
+    // tiles are the tensor-core tiles [tc_first, tc_first + tc_count)
+    std::int64_t tc_first = 0;
+    std::int32_t tc_count = 0;
+    std::int32_t small_count = 0;
 };
 
 struct Plan
@@ -225,6 +266,9 @@ struct Plan
     std::vector<std::int64_t> diag_offset;  // per row: arena offset of U(i,i)
 
     std::vector<GemmTask>      gemm;
+    std::vector<TcTask>        tc;             // the GEMM updates as tensor-core tiles (FP32 path, level launches)
+    std::vector<std::int64_t>  front_img;      // per front: first operand-image block
+    std::int64_t img_blocks = 0;               // operand-image size in blocks of kImgRows x kImgK floats
     std::vector<PanelTask>     potrf;          // one per (front, panel)
     std::vector<PanelTask>     panel;          // trsm chunks
     std::vector<ExtendTask>    extend;

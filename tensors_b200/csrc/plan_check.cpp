@@ -215,6 +215,85 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         const I64 bad = first_bad( static_cast<I64>( pl.gemm.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
         if( bad >= 0 ) { return task( bad ); }
     }
+    {
+        // tensor-core tiles (FP32 path): C in the arena, 16-byte aligned rows;
+        // the image blocks of their valid rows, columns and k-chunks inside the
+        // image (the copies of the blocks past a front's end read other
+        // fronts' data or zeros, used only for rows and columns not written)
+        auto task = [&]( I64 k ) -> std::string
+        {
+            const TcTask & t = pl.tc[static_cast<size_t>( k )];
+            auto at = [&]() { return " (tensor-core tile " + std::to_string( k ) + ")"; };   // built only on failure
+            if( t.K <= 0 || t.M <= 0 || t.N <= 0 || t.m0 < 0 || t.m0 >= t.M || t.c0 < 0 || t.c0 >= t.N ) { return "bad tile dimensions" + at(); }
+            if( t.nt < kImgRows || t.nt > kTcNMax || t.nt % kImgRows != 0 || t.m0 % kTcM != 0 || t.c0 % kImgRows != 0 ) { return "bad tile shape" + at(); }
+            if( t.N > t.ldc || t.c % 4 != 0 || t.ldc % 4 != 0 ) { return "tile C leading dimension or alignment" + at(); }
+            if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "tile C out of range" + at(); }
+            const I64 nk = (t.K + kImgK - 1) / kImgK;
+            const I32 rows = std::min( kTcM, t.M - t.m0 ), cols = std::min( t.nt, t.N - t.c0 );
+            if( t.tf <= 0 || t.ta < 0 || t.tb < 0 || t.ta + (rows - 1) / kImgRows >= t.tf || t.tb + (cols - 1) / kImgRows >= t.tf ) { return "tile column tiles out of range" + at(); }
+            if( t.blk < 0 || t.blk + (nk - 1) * 2 * t.tf + 2 * t.tf > pl.img_blocks ) { return "tile k-chunks outside the operand image" + at(); }
+            return std::string();
+        };
+        const I64 bad = first_bad( static_cast<I64>( pl.tc.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
+        if( bad >= 0 ) { return task( bad ); }
+        // each panel step: its GEMM launches' small-front tiles and tensor-core tiles do the step's
+        // updates (a tensor-core tile of the first tile row spans both launches' rows)
+        for( const std::vector<Launch> * list : { &pl.factor_launches, &pl.pre_dag_launches } )
+        {
+            std::map<std::pair<I32, I32>, std::pair<double, double>> steps;   // (level, step) -> (want, got)
+            for( const Launch & L : *list )
+            {
+                if( L.kind != LaunchKind::Gemm ) { continue; }
+                if( L.small_count < 0 || L.small_count > L.count || L.tc_count < 0 || L.tc_first < 0
+                    || L.tc_first + L.tc_count > static_cast<I64>( pl.tc.size() ) ) { return "tensor-core tile range out of bounds"; }
+                double want = 0.0, got = 0.0;
+                for( I64 i = L.first; i < L.first + L.count; ++i )
+                {
+                    const GemmTask & t = pl.gemm[static_cast<size_t>( i )];
+                    const double r = std::min( kTile, t.M - t.m0 ), c = std::min( kTile, t.N - t.c0 );
+                    const double f = 2.0 * t.K * (t.upper ? r * (r + 1.0) / 2.0 + r * (c - r) : r * c);
+                    want += f;
+                    if( i < L.first + L.small_count ) { got += f; }
+                }
+                for( I64 i = L.tc_first; i < L.tc_first + L.tc_count; ++i )
+                {
+                    const TcTask & t = pl.tc[static_cast<size_t>( i )];
+                    const I64 r = std::min( kTcM, t.M - t.m0 ), c = std::min( t.nt, t.N - t.c0 );
+                    double e = 0.0;
+                    if( !t.upper ) { e = static_cast<double>( r ) * c; }
+                    else
+                    {
+                        // entries (m0 + i, c0 + j) with m0 + i <= c0 + j
+                        for( I64 i2 = 0; i2 < r; ++i2 ) { e += static_cast<double>( std::max<I64>( 0, c - std::max<I64>( 0, t.m0 + i2 - t.c0 ) ) ); }
+                    }
+                    got += 2.0 * t.K * e;
+                }
+                auto & acc = steps[{ L.level, L.step }];
+                acc.first += want;
+                acc.second += got;
+            }
+            for( const auto & kv : steps )
+            {
+                const double want = kv.second.first, got = kv.second.second;
+                if( std::abs( want - got ) > 1e-12 * std::max( 1.0, want ) )
+                {
+                    return "tensor-core tiles do not do their step's updates (level " + std::to_string( kv.first.first ) + ", step "
+                           + std::to_string( kv.first.second ) + ": " + std::to_string( got ) + " of " + std::to_string( want ) + " flops)";
+                }
+            }
+        }
+        // the trsm's image writes stay inside the front's image segments
+        for( size_t k = 0; k < pl.panel.size(); ++k )
+        {
+            const PanelTask & t = pl.panel[k];
+            if( t.img < 0 ) { continue; }
+            const I64 t0 = (t.n0 + kImgRows - 1) / kImgRows, tf = t0 + (t.n1 + kImgRows - 1) / kImgRows;
+            if( t.img_t0 != t0 || t.img_tf != tf || t.img + (t.n0 + kImgK - 1) / kImgK * 2 * tf > pl.img_blocks )
+            {
+                return "trsm image segment out of range (panel task " + std::to_string( k ) + ")";
+            }
+        }
+    }
     for( size_t k = 0; k < pl.sdiag.size(); ++k )
     {
         const SolveDiagTask & t = pl.sdiag[k];

@@ -15,7 +15,9 @@
 #include "tensors_b200/CholeskyDecomposition.hpp"
 #include "tensors_b200/MatrixCSR.hpp"
 
-using tensors_b200::Sparse::CholeskyDecomposition;
+// the reference driver's instantiation (Example_SparseCholesky/main.cpp:31-32)
+using CholeskyDecomposition = tensors_b200::Sparse::CholeskyDecomposition<double, int32_t, int64_t>;
+using CholeskyDecompositionF = tensors_b200::Sparse::CholeskyDecomposition<float, int32_t, int64_t>;
 using tensors_b200::Sparse::MatrixCSR;
 
 int main( int argc, char ** argv )
@@ -96,5 +98,56 @@ int main( int argc, char ** argv )
     }
     const bool ok = S.ConjugateGradient( val2.data(), 0.0, 1.0, B.data(), nrhs, 0.0, X.data(), nrhs, nrhs, 1e-12, 200 );
     std::printf( "cg_ok %d\ncg_iter %d\n", ok ? 1 : 0, S.IterationCount() );
+
+    auto relres_of = [&]( const std::vector<double> & Y ) {
+        double r2 = 0.0, b2 = 0.0;
+        for( int r = 0; r < n; ++r )
+        {
+            for( int k = 0; k < nrhs; ++k )
+            {
+                double ax = 0.0;
+                for( int64_t l = outer[r]; l < outer[r + 1]; ++l ) { ax += val[l] * Y[inner[l] * nrhs + k]; }
+                const double d = B[r * nrhs + k] - ax;
+                r2 += d * d;
+                b2 += B[r * nrhs + k] * B[r * nrhs + k];
+            }
+        }
+        return std::sqrt( r2 / b2 );
+    };
+    // float right-hand sides, double solution (cast on copy, Solve.hpp:20-27)
+    std::vector<float> Bf( B.begin(), B.end() );
+    std::vector<double> Xd( B.size() );
+    S.Solve( Bf.data(), Xd.data(), nrhs );
+    double rn2 = 0.0, bn2 = 0.0;
+    for( int r = 0; r < n; ++r )
+    {
+        for( int k = 0; k < nrhs; ++k )
+        {
+            double ax = 0.0;
+            for( int64_t l = outer[r]; l < outer[r + 1]; ++l ) { ax += val[l] * Xd[inner[l] * nrhs + k]; }
+            const double d = static_cast<double>( Bf[r * nrhs + k] ) - ax;
+            rn2 += d * d;
+            bn2 += static_cast<double>( Bf[r * nrhs + k] ) * Bf[r * nrhs + k];
+        }
+    }
+    std::printf( "relres_f32_in %.3e\n", std::sqrt( rn2 / bn2 ) );
+
+    // Scal = float: FP32 factor of float values, refined solves
+    CholeskyDecompositionF F( outer.data(), inner.data(), p.data(), n, 1 );
+    std::vector<float> valf( val.begin(), val.end() );
+    std::printf( "status_f32 %d\n", F.NumericFactorization( valf.data(), 0.0f ) );
+    std::vector<double> Xf( B.size() );
+    F.Solve( B.data(), Xf.data(), nrhs );
+    std::printf( "relres_f32_factor %.3e\n", relres_of( Xf ) );
+
+    // SwapNumericalFactorization: S's factor moves to a second decomposition of the same pattern
+    CholeskyDecomposition S2( outer.data(), inner.data(), p.data(), n, 1 );
+    CholeskyDecomposition::NumericalFactorization_T cont;
+    S.SwapNumericalFactorization( cont );
+    const bool moved = cont.NumericallyFactorizedQ() && cont.NumericallyGoodQ() && !S.NumericallyFactorizedQ();
+    S2.SwapNumericalFactorization( cont );
+    std::vector<double> X2( B.size() );
+    S2.Solve( B.data(), X2.data(), nrhs );
+    std::printf( "swap_moved %d\nrelres_swapped %.3e\n", moved ? 1 : 0, relres_of( X2 ) );
     return 0;
 }
