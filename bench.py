@@ -267,11 +267,10 @@ def run_for_profiler(args):
 C3_GRID, C3_SEED, C3_SHIFT, C3_NRHS = 48, 0x5EED0003, 1e-2, 8
 C4_COUNT, C4_SEED, C4_MIN, C4_MAX = 2000, 0x5EED0004, 500, 20000
 # The random Delaunay meshes carry near-flat hull triangles whose cotangent
-# weights reach ~1e6 while the lumped mass is ~1e-8: kappa ~1e12-1e14.  The
-# plain FP64 direct solve attains a relative residual of ~2e-8 on them, so the
-# batch's refinement target is 1e-7 (the 1e-10 target of C3 / C5 is out of
-# reach of any FP64 solver here).
-C4_TARGET = 1e-7
+# weights reach ~1e6 while the lumped mass is ~1e-8: kappa ~1e12-1e14.  A plain
+# FP64 direct solve attains a relative residual of only ~2e-8 on them, so the
+# batch's refinement target is max(1e-10, 2 x what the reference's own FP64
+# code attains on the same systems).
 TARGET_RELRES = 1e-10
 
 
@@ -414,7 +413,7 @@ def shard_by_work(work, world):
 
 def run_c4(args):
     """2,000 independent Delaunay systems factored as one batch (level launches over the merged task lists),
-    FP32 factor + FP64 refinement to max(C4_TARGET, 2 x the residual a plain FP64 solve attains on the
+    FP32 factor + FP64 refinement to max(1e-10, 2 x the residual the reference's FP64 code attains on the
     batch), 1 RHS each.  When the refinement breaks down on a system
     whose conditioning is beyond FP32, the handle falls back to an FP64 factor (reported in the line)."""
     count = args.batch or C4_COUNT
@@ -450,14 +449,17 @@ def run_c4(args):
     stream = torch.cuda.Stream(dev)
     b.handle.SetStream(stream)
     torch.cuda.set_stream(stream)
-    # Untimed: the residual a plain FP64 factor + solve attains on this batch.  On the worst
-    # meshes (kappa ~1e14) the FP64 floor u |A| |x| / |b| lies above 1e-7, so the refinement
-    # target is max(C4_TARGET, 2 x that attainable residual).
+    # Untimed: the residual a plain FP64 factor + solve attains on this batch, on the GPU and with the
+    # reference's own CPU code.  On the worst meshes (kappa ~1e14) the FP64 floor u |A| |x| / |b| lies
+    # far above 1e-10, so the refinement target is max(1e-10, 2 x the reference's attainable residual).
     b.handle.SetPrecision("fp64")
     assert b.NumericFactorization(vals, 0.0) == 0
     b.Solve(B, X)
     attainable = float(torch.linalg.norm(b.handle.Residual(B, X)) / torch.linalg.norm(B))
-    target = max(C4_TARGET, 2.0 * attainable)
+    ref = None
+    if not args.no_cpu_baseline and world == 1:
+        ref = c4_reference(systems, B.cpu().numpy(), np.asarray(b.row_offsets), X.cpu().numpy())
+    target = max(TARGET_RELRES, 2.0 * (ref["relres"] if ref else attainable))
     b.handle.SetPrecision("mixed")
     b.handle.SetRefinement(target, 60)
 
@@ -491,7 +493,7 @@ def run_c4(args):
             return 0
     line = {
         "metric": f"batched factor+solve GFLOP/s, {n_systems} Delaunay systems, FP32 factor + FP64 refinement "
-                  f"to max({C4_TARGET:g}, 2 x the FP64 direct residual)",
+                  f"to max({TARGET_RELRES:g}, 2 x the reference's FP64 residual)",
         "value": flops / (t * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic (seeded)",
@@ -500,14 +502,56 @@ def run_c4(args):
                    "parallelism": f"{world} GPU(s), systems sharded by estimated factor work, no collective",
                    "rows": n, "factor_gflop": F / 1e9, "factor_ms": tf, "solve_ms": t - tf,
                    "systems_per_s": n_systems / (t * 1e-3), "refinement": [it, rr], "relres": relres,
-                   "target": target, "fp64_direct_relres": attainable,
+                   "target": target, "target_from": "reference CPU residual" if ref else "GPU FP64 residual",
+                   "fp64_direct_relres": attainable,
+                   "reference_relres": ref["relres"] if ref else None,
+                   "worst_gpu_over_reference_relres": ref["worst_ratio"] if ref else None,
                    "perturbed_pivots": b.handle.PerturbedPivots(),
                    "precision_in_use": list(b.handle.PrecisionInUse()),
                    "schedule": args.schedule or "levels", "setup_s": t_setup,
                    "plan": b.handle.PlanStats(), "clocks": clocks.summary()},
+        "cpu_baseline": None if ref is None else {
+            "value": flops / ref["seconds"] / 1e9, "unit": "GFLOP/s", "cores": ref["cores"], "kind": "reference",
+            "sample": "the reference's own code on every system of the batch, one factor + solve each "
+                      "(all host threads per system)", "seconds": ref["seconds"]},
     }
     print(json.dumps(line))
     return 0
+
+
+def c4_reference(systems, B, offsets, X_gpu):
+    """The reference's own CPU factor + solve of every system of the batch: the stacked relative residual it
+    attains, the worst ratio of the GPU FP64 solution's per-system residual to the reference's, and its time."""
+    import scipy.sparse as sp
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not oracle.ref_available():
+        return None
+    threads = os.cpu_count() or 1
+    r2 = b2 = 0.0
+    secs = 0.0
+    worst = 0.0
+    for s, (outer, inner, values, perm) in enumerate(systems):
+        n = len(outer) - 1
+        o0, o1 = int(offsets[s]), int(offsets[s + 1])
+        bs = np.ascontiguousarray(B[o0:o1])
+        ref = oracle.RefCholesky(n, outer, inner, perm, "maximal", threads=threads, blas_threads=1)
+        ref.symbolic()
+        t0 = time.perf_counter()
+        ref.factor(values, 0.0)
+        xs = ref.solve(bs, parallel=False)
+        secs += time.perf_counter() - t0
+        A = sp.csr_matrix((values, inner, outer), shape=(n, n))
+        rr = float(np.linalg.norm(bs - A @ xs) ** 2)
+        rg = float(np.linalg.norm(bs - A @ X_gpu[o0:o1]) ** 2)
+        r2 += rr
+        b2 += float(np.linalg.norm(bs) ** 2)
+        if rr > 0.0:
+            worst = max(worst, np.sqrt(rg / rr))
+        del ref
+    return {"relres": float(np.sqrt(r2 / b2)), "worst_ratio": float(worst), "seconds": secs, "cores": threads}
 
 
 # Arrival rate below the measured service capacity (about 43 requests/s with 4
@@ -522,15 +566,57 @@ def _c5_matrix(args):
     j, kind, g = args
     from tensors_b200 import matrices, ordering
 
-    A = (matrices.grid_laplacian_2d(int(g), 1e-2) if kind == "2d"
+    # 2D: a quality mesh of about g^2 points (jittered grid, Delaunay, cotangent Laplacian + 1e-3
+    # lumped mass); 3D: the 7-point grid Laplacian of a g^3 grid with lognormal conductivities
+    A = (matrices.mesh_laplacian(int(g) * int(g), C5_SEED + j, 1e-3) if kind == "2d"
          else matrices.grid_laplacian_3d(int(g), C5_SEED + j, 1e-2))
     return kind, int(g), A.outer, A.inner, A.values, ordering.nested_dissection(A)
 
 
+def c5_reference_time(mats, which, repeat, nrhs, reqs):
+    """The reference's own CPU code on the served requests: each pool matrix factored once and solved
+    with 1 and with 64 right-hand sides on all host threads (symbolic analysis untimed, as the server's
+    warm-up); a request costs its matrix's factor time (unless it is a repeat solve) plus its solve time
+    interpolated linearly in its RHS count.  Returns the summed busy time and the throughput it allows."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    if not oracle.ref_available():
+        return None
+    threads = os.cpu_count() or 1
+    per = {}
+    for j, (kind, g, outer, inner, values, perm) in mats.items():
+        n = len(outer) - 1
+        ref = oracle.RefCholesky(n, outer, inner, perm, "maximal", threads=threads, blas_threads=1)
+        ref.symbolic()
+        t0 = time.perf_counter()
+        ref.factor(values, 0.0)
+        tf = time.perf_counter() - t0
+        ts = []
+        for k in (1, 64):
+            B = np.random.default_rng(j).standard_normal((n, k))
+            t0 = time.perf_counter()
+            ref.solve(B, parallel=False)
+            ts.append(time.perf_counter() - t0)
+        per[j] = (tf, ts[0], ts[1])
+        del ref
+    total = 0.0
+    for r in reqs:
+        tf, s1, s64 = per[int(which[r])]
+        k = int(nrhs[r])
+        total += (0.0 if repeat[r] else tf) + s1 + (s64 - s1) * (k - 1) / 63.0
+    return {"value": len(reqs) / total, "unit": "requests/s", "cores": threads, "kind": "reference",
+            "sample": "the reference's own code: every pool matrix factored once and solved with 1 and 64 RHS, "
+                      "summed over the stream's requests (factor unless a repeat solve, solve interpolated in k)",
+            "busy_s": total, "factor_s_per_matrix": {str(j): v[0] for j, v in per.items()}}
+
+
 def run_c5(args):
-    """Serving: a Poisson stream of factor / solve requests over a pool of 2D grid Laplacians
-    (n 1k-50k) and 3D 7-point grids (32^3-64^3), 1-64 RHS each, 30% solves on resident factors,
-    150 GB HBM cap, FP32 factor + FP64 refinement to 1e-10; reports p50 / p99 latency and throughput."""
+    """Serving: a Poisson stream of factor / solve requests over a pool of 2D mesh Laplacians
+    (quality meshes, n 1k-50k) and 3D 7-point grids (32^3-64^3), 1-64 RHS each, 30% solves on
+    resident factors, 150 GB HBM cap, FP32 factor + FP64 refinement to 1e-10; reports p50 / p99
+    latency and throughput, and the reference's CPU time for the same requests (each matrix's
+    factor and solve timed once on the host, summed over the stream's requests)."""
     import multiprocessing as mp
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -624,6 +710,9 @@ def run_c5(args):
         if rank != 0:
             return 0
     lat = np.array(lat)
+    ref = None
+    if not args.no_cpu_baseline and world == 1:
+        ref = c5_reference_time(mats, which, repeat, nrhs, reqs)
     line = {
         "metric": "serving latency p50/p99 (ms) and throughput, Poisson stream of factor/solve requests, "
                   "FP32 factor + FP64 refinement to 1e-10",
@@ -631,13 +720,14 @@ def run_c5(args):
         "warmup": len(specs), "ms_per_step": float(np.mean(runs)), "higher_is_better": False, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
         "config": {"workload": f"{n_req} requests, Poisson arrivals at {C5_RATE:g}/s over {len(specs)} matrices "
-                               "(2D grid Laplacians n 1k-50k, 3D 7-point grids 32^3-64^3), 1-64 RHS, 30% solves on "
-                               "resident factors, 150 GB HBM cap, 4 slots",
+                               "(2D quality-mesh Laplacians n 1k-50k, 3D 7-point grids 32^3-64^3), 1-64 RHS, 30% "
+                               "solves on resident factors, 150 GB HBM cap, 4 slots",
                    "p50_ms": float(np.percentile(lat, 50)), "p90_ms": float(np.percentile(lat, 90)),
                    "p99_ms": float(np.percentile(lat, 99)), "mean_run_ms": float(np.mean(runs)),
                    "parallelism": f"{world} GPU(s), matrices and their requests sharded by estimated factor work",
                    "throughput_req_per_s": n_req / wall, "wall_s": wall, "failures": fails,
                    "worst_relres": worst, "mean_refinement_steps": float(np.mean(iters)), "server": st},
+        "cpu_baseline": ref,
     }
     print(json.dumps(line))
     return 0
