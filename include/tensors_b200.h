@@ -87,6 +87,17 @@ typedef struct tb_factor tb_factor;
 /* Message of the last failing call on this thread (never NULL). */
 const char * tb_last_error( void );
 
+/* Phase ranges.  Every phase of the path (symbolic analysis and its steps,
+ * numeric factorization, ReadNonzeroValues, ClearFactors, solves and their
+ * sweeps) is an NVTX range named with the reference's TOOLS_PTIMER tag of
+ * that phase (e.g. "CholeskyDecomposition::NumericFactorization",
+ * Numeric.hpp:34), visible in timeline tools.  tb_trace_record(1) clears and
+ * starts a host-side list of the ranges entered (0 stops it);
+ * tb_trace_names copies it, one name per line, into buf (at most cap bytes,
+ * NUL-terminated) and returns the bytes the whole list needs. */
+int tb_trace_record( int32_t enabled );
+int64_t tb_trace_names( char * buf, int64_t cap );
+
 /* Library / device information: CUDA device ordinal used by new handles. */
 int tb_set_device( int device );
 

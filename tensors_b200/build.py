@@ -17,8 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtensors_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["symbolic.cpp", "plan.cpp", "plan_check.cpp", "schedule.cpp", "batch.cpp", "serve.cpp", "matrix_market.cpp", "ordering.cpp", "kernels.cu", "gemm_tc.cu", "handle.cu"]
-HEADERS = ["common.hpp", "parallel.hpp", "symbolic.hpp", "plan.hpp", "plan_check.hpp", "schedule.hpp", "kernels.cuh"]
+SOURCES = ["trace.cpp", "symbolic.cpp", "plan.cpp", "plan_check.cpp", "schedule.cpp", "batch.cpp", "serve.cpp", "matrix_market.cpp", "ordering.cpp", "kernels.cu", "gemm_tc.cu", "handle.cu"]
+HEADERS = ["trace.hpp", "common.hpp", "parallel.hpp", "symbolic.hpp", "plan.hpp", "plan_check.hpp", "schedule.hpp", "kernels.cuh"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

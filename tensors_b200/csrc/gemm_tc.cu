@@ -15,7 +15,7 @@
 // Persistent, warp-specialised CTAs (one per SM: 192 KB of shared memory):
 //   warp 0    TMA producer: fills a 2-stage ring (A hi/lo, B hi/lo per stage)
 //   warp 1    MMA issuer (one thread) and tensor-memory owner
-//   warps 2-5 epilogue: tensor memory -> registers, C -= acc in global memory
+//   warps 2-5 epilogue: tensor memory -> registers, C -= acc by reductions in L2
 // Two 256-column accumulators (all 512 tensor-memory columns) alternate
 // between tiles, so the epilogue of one tile overlaps the MMAs of the next.
 // Every mbarrier wait is bounded (polls and time); a wait that runs out sets
@@ -162,6 +162,18 @@ __device__ __forceinline__ void tmem_ld32( std::uint32_t addr, std::uint32_t (&v
     asm volatile( "tcgen05.wait::ld.sync.aligned;\n" ::: "memory" );
 }
 
+// Fire-and-forget additions into global memory (the read-modify-write runs in
+// the L2 cache; the thread does not wait for it).
+__device__ __forceinline__ void red_add_v4( float * p, float a, float b, float c, float d )
+{
+    asm volatile( "red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" :: "l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory" );
+}
+
+__device__ __forceinline__ void red_add( float * p, float a )
+{
+    asm volatile( "red.global.add.f32 [%0], %1;\n" :: "l"(p), "f"(a) : "memory" );
+}
+
 __device__ __forceinline__ int tc_chunks( const TcTask & t ) { return (t.K + kImgK - 1) / kImgK; }
 __device__ __forceinline__ int tc_b_boxes( const TcTask & t ) { return (t.nt + 2 * kImgRows - 1) / (2 * kImgRows); }
 
@@ -305,6 +317,8 @@ __global__ __launch_bounds__(kTcThreads, 1) void gemm_tc_tile_kernel( const TcTa
                 tmem_ld32( acc + static_cast<std::uint32_t>( j ), v );
                 if( row >= t.M ) { continue; }
                 const int col0 = t.c0 + j;
+                // C -= acc as reductions in the memory system (no load round trip): every C entry
+                // gets exactly one contribution per launch, so the result is the plain C - acc
 #pragma unroll
                 for( int u = 0; u < 8; ++u )
                 {
@@ -313,19 +327,15 @@ __global__ __launch_bounds__(kTcThreads, 1) void gemm_tc_tile_kernel( const TcTa
                     float * p = crow + col;
                     if( col + 3 < t.N && (!t.upper || row <= col) )
                     {
-                        float4 x = *reinterpret_cast<float4 *>( p );
-                        x.x -= __uint_as_float( v[4 * u] );
-                        x.y -= __uint_as_float( v[4 * u + 1] );
-                        x.z -= __uint_as_float( v[4 * u + 2] );
-                        x.w -= __uint_as_float( v[4 * u + 3] );
-                        *reinterpret_cast<float4 *>( p ) = x;
+                        red_add_v4( p, -__uint_as_float( v[4 * u] ), -__uint_as_float( v[4 * u + 1] ),
+                                    -__uint_as_float( v[4 * u + 2] ), -__uint_as_float( v[4 * u + 3] ) );
                     }
                     else
                     {
 #pragma unroll
                         for( int e = 0; e < 4; ++e )
                         {
-                            if( col + e < t.N && (!t.upper || row <= col + e) ) { p[e] -= __uint_as_float( v[4 * u + e] ); }
+                            if( col + e < t.N && (!t.upper || row <= col + e) ) { red_add( p + e, -__uint_as_float( v[4 * u + e] ) ); }
                         }
                     }
                 }

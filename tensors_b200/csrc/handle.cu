@@ -8,6 +8,7 @@
 #include "plan_check.hpp"
 #include "schedule.hpp"
 #include "symbolic.hpp"
+#include "trace.hpp"
 
 #include <cuda_runtime.h>
 
@@ -261,6 +262,7 @@ int ensure_symbolic( tb_chol * h )
     in.perm = h->has_perm ? h->perm.data() : nullptr;
     in.strategy = h->strategy;
     in.amalgamation_threshold = h->amalgamation_threshold;
+    tb::TraceRange range( "Sparse::CholeskyDecomposition::SymbolicFactorization" );
     const auto t0 = std::chrono::steady_clock::now();
     const int st = h->sym.analyze( in );
     const auto t1 = std::chrono::steady_clock::now();
@@ -272,6 +274,7 @@ int ensure_symbolic( tb_chol * h )
         return fail( st, std::string( "SymbolicFactorization: " ) + what );
     }
     h->plan.dag_min_steps = h->schedule == TB_SCHEDULE_TASK_GRAPH_ALL ? 0 : tb::kDagMinSteps;
+    tb::TraceRange plan_range( "tensors_b200::DevicePlan" );
     h->plan.build( h->sym );
     if( h->solve_schedule == TB_SCHEDULE_LEVELS ) { h->plan.build_solve_graph( h->sym, h->plan.levels ); }
     else if( h->solve_schedule == TB_SCHEDULE_TASK_GRAPH_ALL ) { h->plan.build_solve_graph( h->sym, 0 ); }
@@ -419,11 +422,17 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         if( kind >= 0 ) { kinds->push_back( kind ); }
     };
     mark( -1 );
-    // ClearFactors (Numeric.hpp:256-268); update matrices are zeroed per level
-    cudaMemsetAsync( A, 0, sizeof(T) * static_cast<size_t>( pl.u0_size + pl.u1_size ), st );
-    tb::launch_init_status( h->status.ptr, st );
-    tb::launch_assemble( h->values.ptr, h->asm_src.ptr, h->asm_dst.ptr,
-                         static_cast<std::int64_t>( pl.asm_src.size() ), h->reg.ptr, A, st );
+    {
+        // ClearFactors (Numeric.hpp:256-268); update matrices are zeroed per level
+        tb::TraceRange range( "Sparse::CholeskyDecomposition::ClearFactors" );
+        cudaMemsetAsync( A, 0, sizeof(T) * static_cast<size_t>( pl.u0_size + pl.u1_size ), st );
+        tb::launch_init_status( h->status.ptr, st );
+    }
+    {
+        tb::TraceRange range( "Sparse::CholeskyDecomposition::ReadNonzeroValues" );
+        tb::launch_assemble( h->values.ptr, h->asm_src.ptr, h->asm_dst.ptr,
+                             static_cast<std::int64_t>( pl.asm_src.size() ), h->reg.ptr, A, st );
+    }
     const double * floor = nullptr;
     if constexpr ( sizeof(T) == 4 )
     {
@@ -524,6 +533,7 @@ std::int64_t issue_factor( tb_chol * h, bool timed = false, std::vector<int> * k
 
 int run_factor( tb_chol * h, double reg )
 {
+    tb::TraceRange range( "Sparse::CholeskyDecomposition::NumericFactorization_Multifrontal" );
     cudaStream_t st = h->stream;
     TB_TRY( h->pin_small.reserve( 64 ) );
     double * pr = h->pin_small.as<double>();
@@ -699,6 +709,7 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
     };
     if( which != 1 )
     {
+        tb::TraceRange range( "Sparse::CholeskyDecomposition::SN_LowerSolve" );
         for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
             const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
@@ -708,6 +719,7 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
     }
     if( which != 0 )
     {
+        tb::TraceRange range( "Sparse::CholeskyDecomposition::SN_UpperSolve" );
         cudaMemsetAsync( W, 0, sizeof(double) * static_cast<size_t>( h->n ) * k, st );
         for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
@@ -865,6 +877,7 @@ int solve_fp64_fallback( tb_chol * h, double alpha, const double * d_B, std::int
 int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
                        double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
 {
+    tb::TraceRange range( "tensors_b200::Refinement" );
     cudaStream_t st = h->stream;
     const std::int32_t n = h->n;
     const std::int32_t k = std::max( 1, nrhs );
@@ -984,6 +997,8 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
 int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, std::int32_t ldB,
                       double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
 {
+    tb::TraceRange range( which == 2 ? "Sparse::CholeskyDecomposition::Solve"
+                        : which == 1 ? "Sparse::CholeskyDecomposition::UpperSolve" : "Sparse::CholeskyDecomposition::LowerSolve" );
     // refined: mixed precision, and a handle that fell back to FP64 from it (its target still holds)
     if( (h->precision == TB_PRECISION_MIXED || h->fell_back) && which == 2 )
     {
@@ -2100,6 +2115,9 @@ int tb_chol_swap_factor( tb_chol * h, tb_factor * f )
         h->factorized = false;
         h->good = false;
     }
+    // a factor to solve with needs the device plan (built here for a handle that never factored);
+    // its storage is large enough for it and is kept
+    if( h->factorized ) { TB_TRY( ensure_device( h ) ); }
     if( h->device_ready )
     {
         // the device plan stays: storage too small for it is grown (its contents are then moot)

@@ -217,6 +217,18 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
     extend_body( tasks[blockIdx.x], lut_all, arena );
 }
 
+// Fire-and-forget additions into global memory: the read-modify-write runs in
+// the L2 cache and the thread does not wait for it.
+__device__ __forceinline__ void red_add_f64( double * p, double a )
+{
+    asm volatile( "red.global.add.f64 [%0], %1;\n" :: "l"(p), "d"(a) : "memory" );
+}
+
+__device__ __forceinline__ void red_add_v4f32( float * p, float a, float b, float c, float d )
+{
+    asm volatile( "red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" :: "l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory" );
+}
+
 // TF32 rounding (round to nearest, ties away) of an FP32 value, as bits.
 __device__ __forceinline__ unsigned to_tf32( float x )
 {
@@ -697,6 +709,8 @@ __device__ __forceinline__ void gemm_body( const GemmTask & t, double * __restri
     // the ring is reused by the next task of a persistent CTA
     __syncthreads();
 
+    // C -= acc as reductions in the memory system (no load round trip); every C
+    // entry gets one contribution per launch, so the result is the plain C - acc
     double * C = arena + t.c;
 #pragma unroll
     for( int i = 0; i < 4; ++i )
@@ -708,20 +722,8 @@ __device__ __forceinline__ void gemm_body( const GemmTask & t, double * __restri
         for( int j = 0; j < 2; ++j )
         {
             const int col = t.c0 + wn * 16 + j * 8 + (lane & 3) * 2;
-            const bool ok0 = col < t.N && (!t.upper || row <= col);
-            const bool ok1 = col + 1 < t.N && (!t.upper || row <= col + 1);
-            if( ok0 && ok1 )
-            {
-                double2 v = *reinterpret_cast<const double2 *>( Crow + col );
-                v.x -= acc[i][j][0];
-                v.y -= acc[i][j][1];
-                *reinterpret_cast<double2 *>( Crow + col ) = v;
-            }
-            else
-            {
-                if( ok0 ) { Crow[col] -= acc[i][j][0]; }
-                if( ok1 ) { Crow[col + 1] -= acc[i][j][1]; }
-            }
+            if( col < t.N && (!t.upper || row <= col) ) { red_add_f64( Crow + col, -acc[i][j][0] ); }
+            if( col + 1 < t.N && (!t.upper || row <= col + 1) ) { red_add_f64( Crow + col + 1, -acc[i][j][1] ); }
         }
     }
 }
@@ -981,9 +983,7 @@ __device__ __forceinline__ void gemm_body( const GemmTask & t, float * __restric
         float * Cp = C + (std::int64_t)row * t.ldc + col;
         if( col + 3 < t.N && (!t.upper || row <= col) )
         {
-            float4 x = *reinterpret_cast<float4 *>( Cp );
-            x.x -= d.x; x.y -= d.y; x.z -= d.z; x.w -= d.w;
-            *reinterpret_cast<float4 *>( Cp ) = x;
+            red_add_v4f32( Cp, -d.x, -d.y, -d.z, -d.w );
         }
         else
         {
@@ -991,7 +991,7 @@ __device__ __forceinline__ void gemm_body( const GemmTask & t, float * __restric
 #pragma unroll
             for( int j = 0; j < 4; ++j )
             {
-                if( col + j < t.N && (!t.upper || row <= col + j) ) { Cp[j] -= dv[j]; }
+                if( col + j < t.N && (!t.upper || row <= col + j) ) { atomicAdd( Cp + j, -dv[j] ); }
             }
         }
     }

@@ -6,6 +6,7 @@
 // supernode sweep parameterised by the merge rule.
 
 #include "symbolic.hpp"
+#include "trace.hpp"
 #include "parallel.hpp"
 #include "common.hpp"
 
@@ -302,6 +303,7 @@ int Symbolic::analyze( const SymbolicInput & in )
     p_inv.assign( static_cast<size_t>(n), -1 );
     if( in.perm != nullptr )
     {
+        TraceRange range( "Sparse::CholeskyDecomposition::Init" );
         for( I32 i = 0; i < n; ++i )
         {
             const I32 v = in.perm[i];
@@ -332,11 +334,15 @@ int Symbolic::analyze( const SymbolicInput & in )
     }
 
     // CholeskyDecomposition.hpp:427-472: make the elimination tree postordered.
-    elimination_tree();
+    {
+        TraceRange range( "Sparse::CholeskyDecomposition::EliminationTree" );
+        elimination_tree();
+    }
     Forest et;
     forest_of( etree_parent, et, true );
     if( !postordered( etree_parent, et.desc ) )
     {
+        TraceRange range( "Sparse::CholeskyDecomposition::PostOrdering" );
         const std::vector<I32> & post = et.postorder;
         std::vector<I32> post_inv( static_cast<size_t>(n) );
         for( I32 i = 0; i < n; ++i ) { post_inv[post[i]] = i; }
@@ -353,8 +359,16 @@ int Symbolic::analyze( const SymbolicInput & in )
         forest_of( etree_parent, et, false );
     }
 
-    supernodes( in.strategy, in.amalgamation_threshold, et );
-    assembly_tree();
+    {
+        TraceRange range( in.strategy == SupernodeStrategy::Fundamental ? "Sparse::CholeskyDecomposition::FindFundamentalSupernodes"
+                        : in.strategy == SupernodeStrategy::Amalgamated ? "Sparse::CholeskyDecomposition::FindAmalgamatedSupernodes"
+                                                                        : "Sparse::CholeskyDecomposition::FindMaximalSupernodes" );
+        supernodes( in.strategy, in.amalgamation_threshold, et );
+    }
+    {
+        TraceRange range( "Sparse::CholeskyDecomposition::CreateAssemblyTree" );
+        assembly_tree();
+    }
     return TB_OK;
 }
 

@@ -124,6 +124,20 @@ def test_swap_moves_factors_between_decompositions():
     assert close(h2.Solve(B), X2)
 
 
+def test_swap_into_a_decomposition_that_never_factored():
+    A, perm = _system()
+    h1 = CholeskyDecomposition(A.outer, A.inner, perm)
+    assert h1.NumericFactorization(A.values, 0.0) == 0
+    B = np.random.default_rng(37).standard_normal((A.n, 4))
+    X1 = h1.Solve(B)
+    f = NumericalFactorization()
+    h1.SwapNumericalFactorization(f)
+    fresh = CholeskyDecomposition(A.outer, A.inner, perm)    # no symbolic phase, no device plan yet
+    fresh.SwapNumericalFactorization(f)
+    assert fresh.NumericallyFactorizedQ()
+    assert close(fresh.Solve(B), X1)
+
+
 def test_swap_treats_a_too_small_factor_as_unfactorized():
     small, ps = _system(g=6)
     big, pb = _system(g=12)

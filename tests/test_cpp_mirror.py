@@ -51,7 +51,9 @@ def test_cpp_mirror_symbolic_matches_python_binding(mirror_exe):
 
 @pytest.mark.gpu
 def test_cpp_mirror_factor_and_solve(mirror_exe):
-    out = subprocess.run([mirror_exe, "24", "numeric"], check=True, capture_output=True, text=True).stdout
+    run = subprocess.run([mirror_exe, "24", "numeric"], capture_output=True, text=True)
+    assert run.returncode == 0, run.stdout + run.stderr
+    out = run.stdout
     vals = dict(line.split() for line in out.strip().splitlines())
     assert int(vals["status"]) == 0
     assert float(vals["relres"]) < 1e-13
