@@ -189,6 +189,10 @@ __global__ __launch_bounds__(kTcThreads, 1) void gemm_tc_tile_kernel( const TcTa
     __shared__ int s_abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // programmatic dependent launch: let the next kernel launch once every CTA
+    // runs, and wait for the previous one (which wrote the operands and C)
+    asm volatile( "griddepcontrol.launch_dependents;\n" ::: "memory" );
+    asm volatile( "griddepcontrol.wait;\n" ::: "memory" );
     // the 128-byte swizzle repeats every 1024 bytes: operand parts start on 1024-byte boundaries
     const std::uint32_t base = (smem_addr( tc_smem_raw ) + 1023u) & ~1023u;
     volatile int * abort = &s_abort;
@@ -367,7 +371,17 @@ void launch_gemm_tc_tiles( const TcTask * tasks, int count, float * arena, const
     cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
     const int grid = std::min( count, std::max( sms, 1 ) );
     const CUtensorMap * m = reinterpret_cast<const CUtensorMap *>( map.bytes );
-    gemm_tc_tile_kernel<<<grid, kTcThreads, kTcSmemBytes, st>>>( tasks, count, arena, *m, status );
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3( static_cast<unsigned>( grid ) );
+    cfg.blockDim = dim3( kTcThreads );
+    cfg.dynamicSmemBytes = kTcSmemBytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx( &cfg, gemm_tc_tile_kernel, tasks, count, arena, *m, status );
 }
 
 cudaError_t configure_tc_tiles()

@@ -98,6 +98,37 @@ __device__ __forceinline__ void stage_finish( Src src, Dst dst )
     }
 }
 
+// Programmatic dependent launch (sm_90+).  Kernels of the level schedule are
+// launched with programmatic stream serialization: a kernel lets the next one
+// in its stream launch as soon as all of its own CTAs are running
+// (pdl_allow_next), and the next one's CTAs do the work that does not read
+// the previous kernel's results (their own task records, factor blocks) and
+// then wait for that kernel to complete with its memory visible (pdl_wait),
+// so launch latency and independent loads overlap the previous kernel.
+// Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_allow_next() { asm volatile( "griddepcontrol.launch_dependents;\n" ::: "memory" ); }
+__device__ __forceinline__ void pdl_wait() { asm volatile( "griddepcontrol.wait;\n" ::: "memory" ); }
+
+// Fire-and-forget additions into global memory: the read-modify-write runs in
+// the L2 cache and the thread does not wait for it.
+__device__ __forceinline__ void red_add_f64( double * p, double a )
+{
+    asm volatile( "red.global.add.f64 [%0], %1;\n" :: "l"(p), "d"(a) : "memory" );
+}
+
+__device__ __forceinline__ void red_add_f32( float * p, float a )
+{
+    asm volatile( "red.global.add.f32 [%0], %1;\n" :: "l"(p), "f"(a) : "memory" );
+}
+
+__device__ __forceinline__ void red_add_v4f32( float * p, float a, float b, float c, float d )
+{
+    asm volatile( "red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" :: "l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory" );
+}
+
+__device__ __forceinline__ void red_add_any( double * p, double a ) { red_add_f64( p, a ); }
+__device__ __forceinline__ void red_add_any( float * p, float a ) { red_add_f32( p, a ); }
+
 // ---------------------------------------------------------------- assembly
 // arena[dst] = values[src] (+ reg on the diagonal): ReadNonzeroValues
 // (Numeric.hpp:165-180) fused with FetchFromA (Multifrontal.hpp:249-321).
@@ -133,6 +164,8 @@ __device__ __forceinline__ void zero_body( const ZeroTask & t, T * __restrict__ 
 template<typename T>
 __global__ void zero_kernel( const ZeroTask * __restrict__ tasks, T * __restrict__ arena )
 {
+    pdl_allow_next();
+    pdl_wait();
     zero_body( tasks[blockIdx.x], arena );
 }
 
@@ -173,9 +206,11 @@ __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::in
     const T * W = arena + t.w;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    constexpr int kU = 4;     // entries per lane in flight: the lut entries, W values and targets of a
-                              // group are loaded before any target is written (lut is injective within
-                              // a row, so the targets of a group are distinct)
+    constexpr int kU = 4;     // entries per lane in flight: the lut entries and W values of a group are
+                              // loaded before any target is added to.  The targets get their additions
+                              // as reductions in the memory system (no load round trip): a launch adds
+                              // at most one child into any parent entry (one child rank per pass), so
+                              // the sum is the plain target + W in the passes' order.
     for( int i = t.row_begin + warp; i < t.row_end; i += 8 )
     {
         const std::int64_t li = lut[i];
@@ -186,7 +221,7 @@ __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::in
         const bool upper_part = i < t.mid;
         for( int j0 = i + lane; j0 < t.m1; j0 += 32 * kU )
         {
-            T v[kU], old[kU];
+            T v[kU];
             T * dst[kU];
 #pragma unroll
             for( int u = 0; u < kU; ++u )
@@ -202,9 +237,7 @@ __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::in
                 }
             }
 #pragma unroll
-            for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : T( 0 ); }
-#pragma unroll
-            for( int u = 0; u < kU; ++u ) { if( dst[u] ) { *dst[u] = old[u] + v[u]; } }
+            for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
         }
     }
 }
@@ -214,19 +247,10 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
                                                       const std::int32_t * __restrict__ lut_all,
                                                       T * __restrict__ arena )
 {
-    extend_body( tasks[blockIdx.x], lut_all, arena );
-}
-
-// Fire-and-forget additions into global memory: the read-modify-write runs in
-// the L2 cache and the thread does not wait for it.
-__device__ __forceinline__ void red_add_f64( double * p, double a )
-{
-    asm volatile( "red.global.add.f64 [%0], %1;\n" :: "l"(p), "d"(a) : "memory" );
-}
-
-__device__ __forceinline__ void red_add_v4f32( float * p, float a, float b, float c, float d )
-{
-    asm volatile( "red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n" :: "l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory" );
+    pdl_allow_next();
+    const ExtendTask t = tasks[blockIdx.x];
+    pdl_wait();
+    extend_body( t, lut_all, arena );
 }
 
 // TF32 rounding (round to nearest, ties away) of an FP32 value, as bits.
@@ -381,7 +405,7 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
         // (b) rows o..o+7 of the columns right of the sub-block: U_b,c = L_bb^{-1} A_b,c
         {
             const int col = o + kSub + tid;
-            if( col < kPanel )
+            if( col < kSub * nsub )
             {
                 double x[kSub];
 #pragma unroll
@@ -398,9 +422,10 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
             }
         }
         __syncthreads();
-        // (c) trailing sub-blocks (b2, b3), b < b2 <= b3: D -= U_b,b2^T U_b,b3
+        // (c) trailing sub-blocks (b2, b3), b < b2 <= b3 < nsub: D -= U_b,b2^T U_b,b3 (the
+        // identity padding beyond nb rounded up to 8 is neither updated nor read)
         {
-            const int rem = kSubs - 1 - b;
+            const int rem = nsub - 1 - b;
             const int tiles = rem * (rem + 1) / 2;
             for( int tile = warp; tile < tiles; tile += kPotrfThreads / 32 )
             {
@@ -442,10 +467,13 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
         }
         __syncthreads();
     }
-    // reciprocal pivots of the (possibly rounded) block, one division per thread
-    if( tid < kPanel ) { inv_d[tid] = 1.0 / D[tid][tid]; }
+    // reciprocal pivots of the (possibly rounded) block, one division per thread;
+    // only the leading nsub x nsub blocks of T are formed (the trsm and the
+    // solves read no more)
+    const int nbp = kSub * nsub;
+    if( tid < nbp ) { inv_d[tid] = 1.0 / D[tid][tid]; }
     __syncthreads();
-    if( tid < kPanel )
+    if( tid < nbp )
     {
         const int o = (tid >> 3) * kSub, j = tid & (kSub - 1);
         double col[kSub];
@@ -461,9 +489,9 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
         for( int i = 0; i < kSub; ++i ) { Ti[o + i][o + j] = col[i]; }
     }
     __syncthreads();
-    for( int d = 1; d < kSubs; ++d )
+    for( int d = 1; d < nsub; ++d )
     {
-        if( warp < kSubs - d )
+        if( warp < nsub - d )
         {
             const int ib = warp, jb = warp + d;
             double acc[2] = { 0.0, 0.0 };
@@ -488,10 +516,10 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
         __syncthreads();
     }
     double * out = tinv + (std::int64_t)t.panel * (kPanel * kPanel);
-    for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
+    for( int idx = tid; idx < nbp * kPanel; idx += kPotrfThreads )
     {
         const int r = idx / kPanel, c = idx % kPanel;
-        out[idx] = (r <= c) ? Ti[r][c] : 0.0;
+        if( c < nbp ) { out[idx] = (r <= c) ? Ti[r][c] : 0.0; }
     }
 }
 
@@ -502,7 +530,10 @@ __global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask *
                                                                double * __restrict__ tinv )
 {
     extern __shared__ __align__(16) double psm[];
-    potrf_body( tasks[blockIdx.x], arena, status, psm, pivot_floor, tinv );
+    pdl_allow_next();
+    const PanelTask t = tasks[blockIdx.x];
+    pdl_wait();
+    potrf_body( t, arena, status, psm, pivot_floor, tinv );
 }
 
 // X = D^{-T} U for the rest columns [c0, c0 + kRestChunk) of a panel (trsm of
@@ -623,7 +654,10 @@ __global__ __launch_bounds__(kTrsmThreads) void trsm_kernel( const PanelTask * _
                                                              float * __restrict__ img )
 {
     extern __shared__ __align__(16) double tsm[];
-    trsm_body( tasks[blockIdx.x], arena, tinv, tsm, img );
+    pdl_allow_next();
+    const PanelTask t = tasks[blockIdx.x];
+    pdl_wait();
+    trsm_body( t, arena, tinv, tsm, img );
 }
 
 // ------------------------------------------------------------------- gemm
@@ -1007,6 +1041,8 @@ __global__ __launch_bounds__(kGemmThreads, 3) void gemm_tc_kernel( const GemmTas
     extern __shared__ __align__(16) double gsm[];
     __shared__ std::uint64_t bars[2];
     __shared__ std::uint32_t s_tmem;
+    pdl_allow_next();
+    pdl_wait();
     TcState tc = tc_setup( bars, &s_tmem );
     for( int i = blockIdx.x; i < count; i += gridDim.x ) { gemm_body( tasks[i], arena, gsm, tc, status ); }
     tc_teardown( tc );
@@ -1016,7 +1052,10 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
                                                                 double * __restrict__ arena )
 {
     extern __shared__ __align__(16) double gsm[];
-    gemm_body( tasks[blockIdx.x], arena, gsm );
+    pdl_allow_next();
+    const GemmTask t = tasks[blockIdx.x];
+    pdl_wait();
+    gemm_body( t, arena, gsm );
 }
 
 // ------------------------------------------------------------------ solves
@@ -1062,7 +1101,11 @@ __device__ __forceinline__ void warp_rows_product( double (&acc)[NCT][2], int kb
 //
 // atomic_own: rows of the task's own front are updated with atomics too (the
 // task-graph solve, where panels of one front can run concurrently).
-template<typename T, int KP>
+//
+// kPdl: launched with programmatic stream serialization; the factor blocks (T,
+// the rest block) and the rest rows' indices are loaded before pdl_wait, the
+// vectors the previous step writes only after it.
+template<typename T, int KP, bool kPdl = false>
 __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int upper, const T * __restrict__ arena,
                                                  const double * __restrict__ tinv,
                                                  const std::int32_t * __restrict__ sn_inner,
@@ -1100,6 +1143,25 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
             cp_async_16( &sT[idx >> 6][idx & 63], used ? Tg + idx : Tg, used ? 16 : 0 );
         }
     }
+    if( tid < kSolveRest )
+    {
+        const int col = t.c0 + tid;
+        trow[tid] = (tid < cw) ? ((col < m) ? (std::int64_t)t.row0 + r1 + col
+                                            : (std::int64_t)sn_inner[t.inner + (col - m)]) : -1;
+    }
+    // the panel's rest block (factor data: final before any solve step)
+    const T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
+    const T * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
+    auto stage_src = [&]( int idx, double & ) -> const T *
+    {
+        const int i = idx >> 6, jj = idx & 63;
+        const int col = t.c0 + jj;
+        if( i >= nb || jj >= cw ) { return nullptr; }
+        return (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col : U1 + (std::int64_t)i * t.ld1 + (col - m);
+    };
+    auto stage_dst = [&]( int idx ) { return &sP[idx >> 6][idx & 63]; };
+    if( has_rest ) { stage_block<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( U0, stage_src, stage_dst ); }
+    if constexpr ( kPdl ) { pdl_wait(); }
     // y_q: the panel's rows of `in` (forward: every task; backward: the owner)
     const bool need_y = !upper || owner;
 #pragma unroll 4
@@ -1108,12 +1170,6 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         const int i = idx >> lkp, c = idx & (kp - 1);
         const bool valid = need_y && i < nb && c < k;
         cp_async_8( &sY[i * ldv + c], valid ? in + (prow + i) * ld + c : in, valid );
-    }
-    if( tid < kSolveRest )
-    {
-        const int col = t.c0 + tid;
-        trow[tid] = (tid < cw) ? ((col < m) ? (std::int64_t)t.row0 + r1 + col
-                                            : (std::int64_t)sn_inner[t.inner + (col - m)]) : -1;
     }
     __syncthreads();
     if( upper )
@@ -1127,25 +1183,8 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
             cp_async_8( &sX[i * ldv + c], valid ? out + trow[i] * ld + c : out, valid );
         }
     }
-    // the panel's rest block last: with FP32 storage its converting loads then
-    // overlap the copies above
-    if( has_rest )
-    {
-        const T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
-        const T * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
-        auto stage_src = [&]( int idx, double & ) -> const T *
-        {
-            const int i = idx >> 6, jj = idx & 63;
-            const int col = t.c0 + jj;
-            if( i >= nb || jj >= cw ) { return nullptr; }
-            return (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col : U1 + (std::int64_t)i * t.ld1 + (col - m);
-        };
-        auto stage_dst = [&]( int idx ) { return &sP[idx >> 6][idx & 63]; };
-        stage_block<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( U0, stage_src, stage_dst );
-        cp_async_wait_all();
-        stage_finish<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( stage_src, stage_dst );
-    }
     cp_async_wait_all();
+    if( has_rest ) { stage_finish<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( stage_src, stage_dst ); }
     __syncthreads();
 
     const int fi = lane >> 2, fj = 2 * (lane & 3);     // accumulator fragment: row fi, columns fj, fj + 1
@@ -1254,7 +1293,8 @@ __global__ __launch_bounds__(kSolveThreads) void solve_step_kernel( const SolveR
                                                                     double * in, double * out, int ld, int k )
 {
     extern __shared__ __align__(16) double ssm[];
-    solve_step_body<T, KP>( tasks[blockIdx.x], upper, arena, tinv, sn_inner, in, out, ld, k, false, ssm );
+    pdl_allow_next();
+    solve_step_body<T, KP, true>( tasks[blockIdx.x], upper, arena, tinv, sn_inner, in, out, ld, k, false, ssm );
 }
 
 // The solve's task graph (Plan::solve_*) as one persistent launch per sweep:
@@ -1627,6 +1667,23 @@ __global__ void init_status_kernel( int * status )
     status[2] = 0;
 }
 
+// Launch with programmatic stream serialization (see pdl_allow_next).
+template<typename... KArgs, typename... Args>
+void launch_pdl( void (*kernel)( KArgs... ), unsigned grid, unsigned block, size_t smem, cudaStream_t st, Args... args )
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3( grid );
+    cfg.blockDim = dim3( block );
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx( &cfg, kernel, static_cast<KArgs>( args )... );
+}
+
 int grid_for( std::int64_t work, int threads )
 {
     const std::int64_t blocks = (work + threads - 1) / threads;
@@ -1646,7 +1703,7 @@ void launch_assemble( const double * values, const std::int64_t * src, const std
 template<typename T>
 void launch_zero( const ZeroTask * tasks, int count, T * arena, cudaStream_t st )
 {
-    if( count > 0 ) { zero_kernel<<<count, 256, 0, st>>>( tasks, arena ); }
+    if( count > 0 ) { launch_pdl( zero_kernel<T>, count, 256, 0, st, tasks, arena ); }
 }
 
 template<typename T>
@@ -1659,14 +1716,14 @@ void launch_export( const ExportTask * tasks, int count, const std::int32_t * co
 template<typename T>
 void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, T * arena, cudaStream_t st )
 {
-    if( count > 0 ) { extend_kernel<<<count, 256, 0, st>>>( tasks, lut, arena ); }
+    if( count > 0 ) { launch_pdl( extend_kernel<T>, count, 256, 0, st, tasks, lut, arena ); }
 }
 
 template<typename T>
 void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, const double * pivot_floor, double * tinv,
                    cudaStream_t st )
 {
-    if( count > 0 ) { potrf_kernel<<<count, kPotrfThreads, kPotrfSmemBytes, st>>>( tasks, arena, status, pivot_floor, tinv ); }
+    if( count > 0 ) { launch_pdl( potrf_kernel<T>, count, kPotrfThreads, kPotrfSmemBytes, st, tasks, arena, status, pivot_floor, tinv ); }
 }
 
 // floor[i] = rel * |diagonal entry of row i| after assembly (FP32 storage).
@@ -1701,7 +1758,7 @@ void launch_pivot_floor( const std::int64_t * offsets, const float * arena, doub
 template<typename T>
 void launch_trsm( const PanelTask * tasks, int count, T * arena, const double * tinv, cudaStream_t st, float * img )
 {
-    if( count > 0 ) { trsm_kernel<<<count, kTrsmThreads, kTrsmSmemBytes, st>>>( tasks, arena, tinv, img ); }
+    if( count > 0 ) { launch_pdl( trsm_kernel<T>, count, kTrsmThreads, kTrsmSmemBytes, st, tasks, arena, tinv, img ); }
 }
 
 template<typename T>
@@ -1711,7 +1768,7 @@ void launch_gemm( const GemmTask * tasks, int count, T * arena, int * status, cu
     if constexpr ( sizeof(T) == 8 )
     {
         (void)status;
-        gemm_tn_kernel<<<count, kGemmThreads, kGemmSmemBytes, st>>>( tasks, arena );
+        launch_pdl( gemm_tn_kernel, count, kGemmThreads, kGemmSmemBytes, st, tasks, arena );
     }
     else
     {
@@ -1719,7 +1776,7 @@ void launch_gemm( const GemmTask * tasks, int count, T * arena, int * status, cu
         cudaGetDevice( &dev );
         cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev );
         const int grid = std::min( count, 3 * std::max( sms, 1 ) );
-        gemm_tc_kernel<<<grid, kGemmThreads, kGemmSmemBytesF, st>>>( tasks, count, arena, status );
+        launch_pdl( gemm_tc_kernel, grid, kGemmThreads, kGemmSmemBytesF, st, tasks, count, arena, status );
     }
 }
 
@@ -1800,10 +1857,10 @@ void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, cons
     const int u = upper ? 1 : 0;
     switch( solve_lkp( k ) )
     {
-        case 3:  solve_step_kernel<T, 8><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
-        case 4:  solve_step_kernel<T, 16><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
-        case 5:  solve_step_kernel<T, 32><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
-        default: solve_step_kernel<T, 64><<<count, kSolveThreads, sm, st>>>( tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+        case 3:  launch_pdl( solve_step_kernel<T, 8>, count, kSolveThreads, sm, st, tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+        case 4:  launch_pdl( solve_step_kernel<T, 16>, count, kSolveThreads, sm, st, tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+        case 5:  launch_pdl( solve_step_kernel<T, 32>, count, kSolveThreads, sm, st, tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
+        default: launch_pdl( solve_step_kernel<T, 64>, count, kSolveThreads, sm, st, tasks, u, arena, tinv, sn_inner, in, out, ld, k ); break;
     }
 }
 
