@@ -298,6 +298,19 @@ int tb_chol_set_solve_schedule( tb_chol * h, int32_t schedule );
  * times_ms (4 entries, may be NULL): factor levels, factor task graph, solve
  * levels, solve task graph. */
 int tb_chol_autotune( tb_chol * h, int32_t nrhs, int32_t * choice, double * times_ms );
+/* Plan options (no counterpart in the reference): defer_steps (1-4) panel
+ * steps over which a front's trailing update is deferred (default 3); relax,
+ * the fronts' amalgamation relaxation: 0 tight, 1 default, 2 loose; tc_width,
+ * the widest tensor-core tile of the mixed-precision path (128 or 256).  A
+ * change rebuilds the device plan (the symbolic analysis stands) and leaves
+ * the handle unfactorized.  tb_chol_autotune_plan: after a factorization,
+ * factors the same values under each candidate set (deferral 2-4 x the three
+ * relaxations, x both tile widths in mixed precision), timed, keeps the
+ * fastest and refactors under it; choice[0..2] the kept options, times_ms[i]
+ * (at most cap) each candidate's ms.  Returns the number of candidates. */
+int tb_chol_set_plan_options( tb_chol * h, int32_t defer_steps, int32_t relax, int32_t tc_width );
+int tb_chol_plan_options( tb_chol * h, int32_t * defer_steps, int32_t * relax, int32_t * tc_width );
+int tb_chol_autotune_plan( tb_chol * h, int32_t * choice, double * times_ms, int32_t cap );
 /* Execution trace of the persistent factorization launch: when enabled,
  * each task records when it was taken, when its inputs were ready, when it
  * was done (%globaltimer ns) and which CTA ran it.  tb_chol_trace writes 6

@@ -258,6 +258,25 @@ class CholeskyDecomposition:
                 "times_ms": {"factor_levels": times[0], "factor_task_graph": times[1],
                              "solve_levels": times[2], "solve_task_graph": times[3]}}
 
+    def SetPlanOptions(self, defer_steps: int = 3, relax: int = 1, tc_width: int = 256) -> None:
+        """Device-plan options: trailing-update deferral (1-4 panel steps), front relaxation (0 tight,
+        1 default, 2 loose), widest tensor-core tile of the mixed path (128 / 256).  Leaves the object
+        unfactorized."""
+        _check(lib().tb_chol_set_plan_options(self._h, int(defer_steps), int(relax), int(tc_width)))
+
+    def PlanOptions(self):
+        d, r, w = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().tb_chol_plan_options(self._h, ctypes.byref(d), ctypes.byref(r), ctypes.byref(w)))
+        return d.value, r.value, w.value
+
+    def AutotunePlan(self) -> dict:
+        """After a factorization: factor the same values under every candidate plan-option set, keep the
+        fastest (the object ends factored under it).  Returns {'choice': (defer, relax, width), 'times_ms': [...]}."""
+        choice = (ctypes.c_int32 * 3)()
+        times = np.full(64, np.inf)
+        m = _check(lib().tb_chol_autotune_plan(self._h, choice, times.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 64))
+        return {"choice": tuple(choice), "times_ms": times[:m].tolist()}
+
     def SetTrace(self, enabled: bool) -> None:
         _check(lib().tb_chol_set_trace(self._h, 1 if enabled else 0))
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <utility>
 #include <climits>
@@ -129,6 +130,10 @@ struct tb_chol
     std::int32_t method = TB_MULTIFRONTAL;
 
     bool symbolic_done = false;
+    // plan options (tb_chol_set_plan_options): trailing-update deferral, front
+    // relaxation preset, widest tensor-core tile; plan_dirty: rebuild the plan
+    std::int32_t opt_defer = tb::kDeferSteps, opt_relax = 1, opt_tc_width = tb::kTcNMax;
+    bool plan_dirty = false;
     std::int64_t analyze_us = 0, plan_us = 0;   // host time of the last symbolic analysis and plan build
     bool device_ready = false;
     bool kernels_configured = false;
@@ -252,8 +257,42 @@ int check_handle( tb_chol * h )
     return TB_OK;
 }
 
+// The plan options' relaxation presets: tight, default (CHOLMOD-like), loose.
+tb::Relaxation relaxation_preset( std::int32_t which )
+{
+    tb::Relaxation r;
+    if( which == 0 ) { r.nrelax[0] = 4;  r.nrelax[1] = 16; r.nrelax[2] = 32;  r.zrelax[0] = 0.8; r.zrelax[1] = 0.1; r.zrelax[2] = 0.05; }
+    if( which == 2 ) { r.nrelax[0] = 16; r.nrelax[1] = 48; r.nrelax[2] = 128; r.zrelax[0] = 0.9; r.zrelax[1] = 0.3; r.zrelax[2] = 0.15; }
+    return r;
+}
+
+// Builds the device plan of the symbolic analysis with the handle's plan options.
+void build_plan( tb_chol * h )
+{
+    tb::TraceRange plan_range( "tensors_b200::DevicePlan" );
+    h->plan.dag_min_steps = h->schedule == TB_SCHEDULE_TASK_GRAPH_ALL ? 0 : tb::kDagMinSteps;
+    h->plan.defer_steps = h->opt_defer;
+    h->plan.tc_nmax = h->opt_tc_width;
+    h->plan.relax = relaxation_preset( h->opt_relax );
+    h->plan.build( h->sym );
+    if( h->solve_schedule == TB_SCHEDULE_LEVELS ) { h->plan.build_solve_graph( h->sym, h->plan.levels ); }
+    else if( h->solve_schedule == TB_SCHEDULE_TASK_GRAPH_ALL ) { h->plan.build_solve_graph( h->sym, 0 ); }
+    h->plan_dirty = false;
+}
+
 int ensure_symbolic( tb_chol * h )
 {
+    if( h->symbolic_done && h->plan_dirty )
+    {
+        // new plan options: the symbolic analysis stands, the device plan is rebuilt
+        const auto t1 = std::chrono::steady_clock::now();
+        build_plan( h );
+        h->plan_us = std::chrono::duration_cast<std::chrono::microseconds>( std::chrono::steady_clock::now() - t1 ).count();
+        h->device_ready = false;
+        h->factorized = false;
+        h->good = false;
+        return TB_OK;
+    }
     if( h->symbolic_done ) { return TB_OK; }
     tb::SymbolicInput in;
     in.n = h->n;
@@ -273,11 +312,7 @@ int ensure_symbolic( tb_chol * h )
                           : "invalid CSR pattern";
         return fail( st, std::string( "SymbolicFactorization: " ) + what );
     }
-    h->plan.dag_min_steps = h->schedule == TB_SCHEDULE_TASK_GRAPH_ALL ? 0 : tb::kDagMinSteps;
-    tb::TraceRange plan_range( "tensors_b200::DevicePlan" );
-    h->plan.build( h->sym );
-    if( h->solve_schedule == TB_SCHEDULE_LEVELS ) { h->plan.build_solve_graph( h->sym, h->plan.levels ); }
-    else if( h->solve_schedule == TB_SCHEDULE_TASK_GRAPH_ALL ) { h->plan.build_solve_graph( h->sym, 0 ); }
+    build_plan( h );
     const auto t2 = std::chrono::steady_clock::now();
     h->analyze_us = std::chrono::duration_cast<std::chrono::microseconds>( t1 - t0 ).count();
     h->plan_us = std::chrono::duration_cast<std::chrono::microseconds>( t2 - t1 ).count();
@@ -1833,6 +1868,87 @@ int tb_chol_autotune( tb_chol * h, std::int32_t nrhs, std::int32_t * choice, dou
     if( choice ) { choice[0] = t[1] < t[0] ? sched[1] : sched[0]; choice[1] = t[3] < t[2] ? sched[1] : sched[0]; }
     if( times_ms ) { for( int i = 0; i < 4; ++i ) { times_ms[i] = t[i]; } }
     return TB_OK;
+}
+
+int tb_chol_set_plan_options( tb_chol * h, std::int32_t defer_steps, std::int32_t relax, std::int32_t tc_width )
+{
+    TB_TRY( check_handle( h ) );
+    if( defer_steps < 1 || defer_steps > 4 || relax < 0 || relax > 2 || (tc_width != 128 && tc_width != 256) )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "plan options: defer_steps 1-4, relax 0-2, tc_width 128 or 256" );
+    }
+    if( defer_steps == h->opt_defer && relax == h->opt_relax && tc_width == h->opt_tc_width ) { return TB_OK; }
+    h->opt_defer = defer_steps;
+    h->opt_relax = relax;
+    h->opt_tc_width = tc_width;
+    if( h->symbolic_done ) { h->plan_dirty = true; }
+    h->device_ready = false;
+    h->factorized = false;
+    h->good = false;
+    if( h->factor_graph ) { cudaGraphExecDestroy( h->factor_graph ); h->factor_graph = nullptr; }
+    h->drop_solve_graphs();
+    return TB_OK;
+}
+
+int tb_chol_plan_options( tb_chol * h, std::int32_t * defer_steps, std::int32_t * relax, std::int32_t * tc_width )
+{
+    TB_TRY( check_handle( h ) );
+    if( defer_steps ) { *defer_steps = h->opt_defer; }
+    if( relax ) { *relax = h->opt_relax; }
+    if( tc_width ) { *tc_width = h->opt_tc_width; }
+    return TB_OK;
+}
+
+// Times the factorization of the last values under every candidate plan
+// option set (two runs each, the second timed) and keeps the fastest; the
+// handle ends factored under it.
+int tb_chol_autotune_plan( tb_chol * h, std::int32_t * choice, double * times_ms, std::int32_t cap )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    std::vector<std::array<std::int32_t, 3>> cand;
+    for( std::int32_t d : { 2, 3, 4 } )
+    {
+        for( std::int32_t r : { 0, 1, 2 } )
+        {
+            if( h->precision == TB_PRECISION_MIXED ) { for( std::int32_t w : { 128, 256 } ) { cand.push_back( { d, r, w } ); } }
+            else { cand.push_back( { d, r, h->opt_tc_width } ); }
+        }
+    }
+    const double reg = h->last_reg;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TB_CUDA( cudaEventCreate( &e0 ) );
+    TB_CUDA( cudaEventCreate( &e1 ) );
+    double best = std::numeric_limits<double>::infinity();
+    size_t pick = 0;
+    int status = TB_OK;
+    for( size_t c = 0; c < cand.size() && status == TB_OK; ++c )
+    {
+        status = tb_chol_set_plan_options( h, cand[c][0], cand[c][1], cand[c][2] );
+        if( status == TB_OK ) { status = ensure_device( h ); }
+        double t = std::numeric_limits<double>::infinity();
+        for( int rep = 0; rep < 2 && status == TB_OK; ++rep )
+        {
+            cudaEventRecord( e0, h->stream );
+            status = run_factor( h, reg );
+            cudaEventRecord( e1, h->stream );
+            cudaEventSynchronize( e1 );
+            float ms = 0.0f;
+            cudaEventElapsedTime( &ms, e0, e1 );
+            if( rep == 1 ) { t = ms; }
+        }
+        if( times_ms && static_cast<std::int32_t>( c ) < cap ) { times_ms[c] = t; }
+        if( status == TB_OK && t < best ) { best = t; pick = c; }
+    }
+    cudaEventDestroy( e0 );
+    cudaEventDestroy( e1 );
+    if( status != TB_OK ) { return status; }
+    TB_TRY( tb_chol_set_plan_options( h, cand[pick][0], cand[pick][1], cand[pick][2] ) );
+    TB_TRY( ensure_device( h ) );
+    const int st = run_factor( h, reg );
+    if( st < 0 ) { return st; }
+    if( choice ) { choice[0] = cand[pick][0]; choice[1] = cand[pick][1]; choice[2] = cand[pick][2]; }
+    return static_cast<int>( cand.size() );
 }
 
 int tb_chol_set_precision( tb_chol * h, std::int32_t precision )

@@ -41,22 +41,22 @@ void push_tiles( std::vector<GemmTask> & out, I64 a, I32 lda, I64 b, I32 ldb, I6
 }
 
 // The tensor-core tiles of the fronts with an operand image (see TcTask):
-// kTcM x nt tiles (nt up to kTcNMax) over C's M x N entries (symmetric: the
+// kTcM x nt tiles (nt up to nmax <= kTcNMax) over C's M x N entries (symmetric: the
 // tiles on and right of the diagonal).  next_rows: the call updates the next
 // panel's rows, which the tiles of the first tile row contain.
 void push_tc( std::vector<TcTask> & out, std::vector<char> & next, bool next_rows, I64 blk, I32 tf,
-              I32 ta0, I32 tb0, I32 K, I64 c, I32 ldc, I32 M, I32 N, bool symmetric )
+              I32 ta0, I32 tb0, I32 K, I64 c, I32 ldc, I32 M, I32 N, bool symmetric, I32 nmax )
 {
     for( I32 m0 = 0; m0 < M; m0 += kTcM )
     {
-        for( I32 c0 = symmetric ? m0 : 0; c0 < N; c0 += kTcNMax )
+        for( I32 c0 = symmetric ? m0 : 0; c0 < N; c0 += nmax )
         {
             TcTask t{};
             t.c = c; t.blk = blk;
             t.ldc = ldc; t.M = M; t.N = N;
             t.m0 = m0; t.c0 = c0; t.K = K;
             t.ta = ta0 + m0 / kImgRows; t.tb = tb0 + c0 / kImgRows; t.tf = tf;
-            t.nt = static_cast<I32>( std::min<I64>( kTcNMax, ceil_div( N - c0, kImgRows ) * kImgRows ) );
+            t.nt = static_cast<I32>( std::min<I64>( nmax, ceil_div( N - c0, kImgRows ) * kImgRows ) );
             t.upper = symmetric ? 1 : 0;
             out.push_back( t );
             next.push_back( next_rows && m0 == 0 ? 1 : 0 );
@@ -604,18 +604,18 @@ void Plan::build( const Symbolic & sym )
                 const size_t tfirst = tiles.size();
                 if( m > 0 )
                 {
-                    // Trailing updates are deferred over kDeferSteps panel steps: the
+                    // Trailing updates are deferred over defer_steps panel steps: the
                     // next panel's rows [r1, r1 + 64) get every pending panel at once,
-                    // and the whole trailing matrix is updated at every kDeferSteps-th
+                    // and the whole trailing matrix is updated at every defer_steps-th
                     // step, with the rows of the panels since the last such update
-                    // (contiguous in U0 / U1, K up to 64 kDeferSteps).  Each C entry is
-                    // read and written kDeferSteps times less often and the tiles are
+                    // (contiguous in U0 / U1, K up to 64 defer_steps).  Each C entry is
+                    // read and written defer_steps times less often and the tiles are
                     // that much deeper; the next panel still sees every update before
                     // its potrf, and every contribution is applied exactly once.
-                    const I32 j = q % kDeferSteps;
+                    const I32 j = q % defer_steps;
                     const I32 k0 = r0 - j * kPanel;
                     const I32 K = r1 - k0;
-                    const I32 rows = (j + 1 < kDeferSteps) ? std::min( kPanel, m ) : m;
+                    const I32 rows = (j + 1 < defer_steps) ? std::min( kPanel, m ) : m;
                     const I64 pa = front_u0[f] + static_cast<I64>(k0) * ld0 + r1;        // U0[k0:r1, r1:n0]
                     push_tiles( tiles, pa, ld0, pa, ld0, front_u0[f] + static_cast<I64>(r1) * ld0 + r1, ld0, K, rows, m, true );
                     if( n1 > 0 )
@@ -631,11 +631,11 @@ void Plan::build( const Symbolic & sym )
                         const I64 blk = front_img[f] + static_cast<I64>( k0 / kImgK ) * 2 * img_tf[f];
                         const I32 ta = r1 / kImgRows;
                         push_tc( tct, tct_next, true, blk, img_tf[f], ta, ta, K,
-                                 front_u0[f] + static_cast<I64>(r1) * ld0 + r1, ld0, rows, m, true );
+                                 front_u0[f] + static_cast<I64>(r1) * ld0 + r1, ld0, rows, m, true, tc_nmax );
                         if( n1 > 0 )
                         {
                             push_tc( tct, tct_next, true, blk, img_tf[f], ta, img_t0[f], K,
-                                     front_u1[f] + static_cast<I64>(r1) * ld1, ld1, rows, n1, false );
+                                     front_u1[f] + static_cast<I64>(r1) * ld1, ld1, rows, n1, false, tc_nmax );
                         }
                     }
                 }
@@ -646,7 +646,7 @@ void Plan::build( const Symbolic & sym )
                     if( front_img[f] >= 0 )
                     {
                         push_tc( tct, tct_next, false, front_img[f], img_tf[f], img_t0[f], img_t0[f], n0,
-                                 front_v[f], ld1, n1, n1, true );
+                                 front_v[f], ld1, n1, n1, true, tc_nmax );
                     }
                 }
                 for( size_t i = tfirst; i < tiles.size(); ++i ) { tile_small.push_back( front_img[f] < 0 ? 1 : 0 ); }
