@@ -373,6 +373,27 @@ int tb_chol_cg_device( tb_chol * h, const double * values, double reg, double al
                        int32_t use_initial_guess, int32_t * iterations, double * relres );
 /* Number of kernel launches the last numeric factorization / solve issued. */
 int tb_chol_launch_counts( tb_chol * h, int64_t * factor_launches, int64_t * solve_launches );
+/* GMRES preconditioned by the factor: the reference's GMRES::operator()
+ * (GMRES.hpp:124-330), left preconditioning, restarted after max_iter Arnoldi
+ * steps (two Gram-Schmidt passes each, Givens rotations), one Krylov space
+ * per column, with the operator (A' + reg I) (values: A' in the caller's CSR
+ * order, NULL = the factored values) and P = this factor's solve.
+ * X = alpha x + beta X; with use_initial_guess the iteration starts from X.
+ * Converged when every column's |P (b - A x)| <= rel_tol |P b| (its
+ * CheckResiduals); relres[c] reports that ratio.  TB_ERR_NOT_CONVERGED after
+ * max_restarts restarts without it (X still written). */
+int tb_chol_gmres( tb_chol * h, const double * values, double reg, double alpha, const double * B, int32_t ldB,
+                   double beta, double * X, int32_t ldX, int32_t nrhs, double rel_tol, int32_t max_iter,
+                   int32_t max_restarts, int32_t use_initial_guess, int32_t * iterations, int32_t * restarts, double * relres );
+int tb_chol_gmres_device( tb_chol * h, const double * d_values, double reg, double alpha, const double * d_B, int32_t ldB,
+                          double beta, double * d_X, int32_t ldX, int32_t nrhs, double rel_tol, int32_t max_iter,
+                          int32_t max_restarts, int32_t use_initial_guess, int32_t * iterations, int32_t * restarts,
+                          double * relres );
+/* Mixed precision: when the conjugate-gradient refinement of a solve breaks
+ * down or stalls, the solve runs GMRES-IR (GMRES on the FP64 system,
+ * preconditioned by the FP32 factor) before refactoring in FP64.  The GMRES
+ * steps of the last solve, or -1 when it was not needed. */
+int tb_chol_gmres_ir_iterations( tb_chol * h, int32_t * out );
 
 /* ------------------------------------------------------------------------
  * Batches of independent systems (no counterpart in the reference, which

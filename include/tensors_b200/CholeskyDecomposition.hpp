@@ -114,7 +114,7 @@ public:
     CholeskyDecomposition & operator=( const CholeskyDecomposition & ) = delete;
     CholeskyDecomposition( CholeskyDecomposition && o ) noexcept
     :   h_( std::exchange( o.h_, nullptr ) ), strategy_( o.strategy_ ), threshold_( o.threshold_ ), method_( o.method_ ),
-        threads_( o.threads_ ), cg_iter_( o.cg_iter_ ), relres_( std::move( o.relres_ ) ) {}
+        threads_( o.threads_ ), cg_iter_( o.cg_iter_ ), restarts_( o.restarts_ ), relres_( std::move( o.relres_ ) ) {}
     CholeskyDecomposition & operator=( CholeskyDecomposition && o ) noexcept
     {
         if( this != &o )
@@ -122,7 +122,7 @@ public:
             if( h_ != nullptr ) { tb_chol_destroy( h_ ); }
             h_ = std::exchange( o.h_, nullptr );
             strategy_ = o.strategy_; threshold_ = o.threshold_; method_ = o.method_; threads_ = o.threads_;
-            cg_iter_ = o.cg_iter_; relres_ = std::move( o.relres_ );
+            cg_iter_ = o.cg_iter_; restarts_ = o.restarts_; relres_ = std::move( o.relres_ );
         }
         return *this;
     }
@@ -217,6 +217,22 @@ public:
         Check( st );
         return true;
     }
+    // GMRES on (A' + reg I) X = B preconditioned from the left by this factor,
+    // the reference's GMRES::operator() (GMRES.hpp:124-330): max_iter Arnoldi
+    // steps per restart, at most max_restarts restarts.  Returns whether every
+    // column met |P r| <= relative_tolerance |P b|.
+    bool GMRES( const double * A_val, double reg, double alpha, const double * B, Int ldB, double beta,
+                double * X_out, Int ldX, Int nrhs, double relative_tolerance, Int max_iter, Int max_restarts,
+                bool use_initial_guess = false )
+    {
+        relres_.assign( static_cast<size_t>( nrhs < 1 ? 1 : nrhs ), 0.0 );
+        const int st = tb_chol_gmres( h_, A_val, reg, alpha, B, ldB, beta, X_out, ldX, nrhs, relative_tolerance, max_iter,
+                                      max_restarts, use_initial_guess ? 1 : 0, &cg_iter_, &restarts_, relres_.data() );
+        if( st == TB_ERR_NOT_CONVERGED ) { return false; }
+        Check( st );
+        return true;
+    }
+    Int RestartCount() const { return restarts_; }
     Int IterationCount() const { return cg_iter_; }
     const std::vector<double> & RelativeResiduals() const { return relres_; }
 
@@ -319,6 +335,7 @@ private:
     FactorizationMethod_T method_ = FactorizationMethod_T::Multifrontal;
     Int threads_ = 1;
     Int cg_iter_ = 0;
+    Int restarts_ = 0;
     std::vector<double> relres_;
 };
 

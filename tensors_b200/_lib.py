@@ -39,6 +39,9 @@ SIGNATURES = {
     "tb_chol_solve_device_noalloc": (ctypes.c_int, [_vp, _d, _vp, _i32, _d, _vp, _i32, _i32]),
     "tb_chol_numeric_ex": (ctypes.c_int, [_vp, _vp, _i32, _d]),
     "tb_chol_set_plan_options": (ctypes.c_int, [_vp, _i32, _i32, _i32]),
+    "tb_chol_gmres": (ctypes.c_int, [_vp, _vp, _d, _d, _vp, _i32, _d, _vp, _i32, _i32, _d, _i32, _i32, _i32, _pi32, _pi32, _vp]),
+    "tb_chol_gmres_device": (ctypes.c_int, [_vp, _vp, _d, _d, _vp, _i32, _d, _vp, _i32, _i32, _d, _i32, _i32, _i32, _pi32, _pi32, _vp]),
+    "tb_chol_gmres_ir_iterations": (ctypes.c_int, [_vp, _pi32]),
     "tb_chol_plan_options": (ctypes.c_int, [_vp, _pi32, _pi32, _pi32]),
     "tb_chol_autotune_plan": (ctypes.c_int, [_vp, _pi32, _pd, _i32]),
     "tb_chol_numeric_device_ex": (ctypes.c_int, [_vp, _vp, _i32, _d]),

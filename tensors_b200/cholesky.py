@@ -435,6 +435,57 @@ class CholeskyDecomposition:
         _check(st)
         return X, True
 
+    def GMRES(self, B, X=None, values=None, reg: float = 0.0, alpha: float = 1.0, beta: float = 0.0,
+              relative_tolerance: float = 1e-10, max_iter: int = 30, max_restarts: int = 10,
+              use_initial_guess: bool = False):
+        """Restarted GMRES on (A' + reg I) X = B, preconditioned from the left by this factor, as the
+        reference's ``GMRES::operator()`` (GMRES.hpp:124-330): ``max_iter`` Arnoldi steps per restart.
+        Returns ``(X, succeeded)``; ``IterationCount()``, ``GMRESRestarts()`` and ``RelativeResiduals()``
+        (per column |P r| / |P b|) report the end state.  Host arrays or CUDA tensors."""
+        cuda = _is_cuda_tensor(B)
+        k = 1 if B.ndim == 1 else B.shape[1]
+        rel = np.zeros(k, dtype=np.float64)
+        iters, rests = ctypes.c_int32(), ctypes.c_int32()
+        if cuda:
+            import torch
+
+            B = B.contiguous()
+            if X is None:
+                X = torch.zeros_like(B)
+                beta = 0.0
+                torch.cuda.current_stream().synchronize()
+            v = 0 if values is None else values.contiguous().data_ptr()
+            st = lib().tb_chol_gmres_device(self._h, v, float(reg), float(alpha), B.data_ptr(), k, float(beta),
+                                            X.data_ptr(), k, k, float(relative_tolerance), int(max_iter),
+                                            int(max_restarts), int(bool(use_initial_guess)), ctypes.byref(iters),
+                                            ctypes.byref(rests), rel.ctypes.data)
+        else:
+            B = _f64(B)
+            if X is None:
+                X = np.zeros_like(B)
+                beta = 0.0
+            elif not (X.flags.c_contiguous and X.dtype == np.float64 and X.shape == B.shape):
+                raise TBError(-1, "GMRES: X must be a C-contiguous float64 array shaped like B")
+            v = None if values is None else _f64(values)
+            st = lib().tb_chol_gmres(self._h, None if v is None else v.ctypes.data, float(reg), float(alpha),
+                                     B.ctypes.data, k, float(beta), X.ctypes.data, k, k, float(relative_tolerance),
+                                     int(max_iter), int(max_restarts), int(bool(use_initial_guess)),
+                                     ctypes.byref(iters), ctypes.byref(rests), rel.ctypes.data)
+        self._cg_iterations, self._cg_relres, self._gmres_restarts = iters.value, rel, rests.value
+        if st == -10:
+            return X, False
+        _check(st)
+        return X, True
+
+    def GMRESRestarts(self) -> int:
+        return getattr(self, "_gmres_restarts", 0)
+
+    def GMRESIRIterations(self) -> int:
+        """GMRES-IR steps of the last mixed-precision solve (-1: its CG refinement sufficed)."""
+        v = ctypes.c_int32()
+        _check(lib().tb_chol_gmres_ir_iterations(self._h, ctypes.byref(v)))
+        return v.value
+
     def IterationCount(self) -> int:
         """Steps of the last ConjugateGradient call (ConjugateGradient.hpp:442)."""
         return getattr(self, "_cg_iterations", 0)

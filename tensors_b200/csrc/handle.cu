@@ -183,8 +183,11 @@ struct tb_chol
     std::int32_t ir_max = 30;
     std::int32_t ir_iters = 0;
     double ir_relres = 0.0;
+    std::int32_t gmres_iters = -1;               // GMRES-IR steps of the last refined solve (-1: not used)
     DeviceArray<double> ir_x, ir_r, ir_norms;
     DeviceArray<double> cg_buf, cg_scal, cg_host;   // tb_chol_cg: vectors, per-column scalars, host-call copies
+    DeviceArray<double> gm_buf, gm_scal;            // GMRES: Krylov basis and work vectors, per-column scalars
+    PinnedBuffer pin_gm;
     DeviceArray<double> pivot_floor;             // mixed precision: static-pivot floor per row
     std::int32_t perturbed_pivots = 0;
     bool fell_back = false;                      // a mixed solve's refinement failed: refactored in FP64
@@ -909,6 +912,194 @@ int solve_fp64_fallback( tb_chol * h, double alpha, const double * d_B, std::int
     return run_solve_refined( h, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
 }
 
+// Restarted GMRES preconditioned from the left by the handle's factor: the
+// reference's GMRES::operator() (GMRES.hpp:124-330, Solve :333-485,
+// ArnoldiStep :529-590 with two Gram-Schmidt passes, Givens rotations
+// :592-655, CheckResiduals :802-818), one Krylov space per right-hand side
+// column, vectors on the device, the small Hessenberg systems on the host.
+// Operator: (A' + shift I) with values `vals` (caller order).  sol (n x k,
+// packed) holds the initial guess when use_x0 and receives the solution.
+// Stops when every column's preconditioned residual |P (b - A x)| is at most
+// rel_tol |P b| (the reference's TOL) or after max_restarts restarts of m
+// Arnoldi steps.  relres (k entries) gets |P r| / |P b| per column.
+struct GmresOutcome
+{
+    std::int32_t iterations = 0, restarts = 0;
+    bool converged = false;
+};
+
+int run_gmres( tb_chol * h, const double * vals, double shift, const double * d_B, std::int32_t ldB, std::int32_t k,
+               double * sol, bool use_x0, double rel_tol, std::int32_t m, std::int32_t max_restarts, double * relres,
+               GmresOutcome & out )
+{
+    tb::TraceRange range( "GMRES::operator()" );
+    const std::int32_t n = h->n;
+    cudaStream_t st = h->stream;
+    m = std::max<std::int32_t>( 1, std::min<std::int32_t>( m, n ) );
+    const std::int64_t nk = static_cast<std::int64_t>( n ) * k;
+    TB_TRY( h->gm_buf.reserve( (static_cast<std::int64_t>( m ) + 2) * nk ) );        // Q_0..Q_m, z
+    TB_TRY( h->gm_scal.reserve( (2 * (static_cast<std::int64_t>( m ) + 1) + 2) * k ) ); // two dot passes, |q|^2, |Pb|^2
+    const size_t hcount = static_cast<size_t>( 2 * (m + 1) + 2 ) * static_cast<size_t>( k );
+    TB_TRY( h->pin_gm.reserve( sizeof(double) * hcount ) );
+    double * Q = h->gm_buf.ptr;
+    double * z = Q + (static_cast<std::int64_t>( m ) + 1) * nk;
+    double * hd = h->gm_scal.ptr;                                   // [2][m+1][k]
+    double * qsq = hd + 2 * (static_cast<std::int64_t>( m ) + 1) * k;
+    double * bsq = qsq + k;
+    double * hp = h->pin_gm.as<double>();
+    auto precondition = [&]( const double * in, std::int32_t ld, double * o ) -> int {
+        return run_solve_core( h, 2, 1.0, in, ld, 0.0, o, k, k );
+    };
+    auto sqnorms = [&]( const double * x, double * o ) -> int {
+        TB_CUDA( cudaMemsetAsync( o, 0, sizeof(double) * static_cast<size_t>( k ), st ) );
+        tb::launch_column_dots( x, k, x, k, n, k, o, st );
+        return TB_OK;
+    };
+    auto fetch = [&]( const double * d, size_t count ) -> int {
+        TB_CUDA( cudaMemcpyAsync( hp, d, sizeof(double) * count, cudaMemcpyDeviceToHost, st ) );
+        TB_CUDA( cudaStreamSynchronize( st ) );
+        return check_solve_error( h );
+    };
+
+    // |P b| per column: the tolerance reference (GMRES.hpp:174-186)
+    TB_TRY( precondition( d_B, ldB, z ) );
+    TB_TRY( sqnorms( z, bsq ) );
+    TB_TRY( fetch( bsq, static_cast<size_t>( k ) ) );
+    std::vector<double> tol( static_cast<size_t>( k ) ), bn( static_cast<size_t>( k ) );
+    double bmax = 0.0;
+    for( std::int32_t c = 0; c < k; ++c )
+    {
+        if( std::isnan( hp[c] ) ) { return fail( TB_ERR_INVALID_ARGUMENT, "GMRES: right-hand side contains NaNs" ); }
+        bn[static_cast<size_t>( c )] = std::sqrt( hp[c] );
+        tol[static_cast<size_t>( c )] = rel_tol * bn[static_cast<size_t>( c )];
+        bmax = std::max( bmax, bn[static_cast<size_t>( c )] );
+    }
+    if( !(bmax > 0.0) )
+    {
+        TB_CUDA( cudaMemsetAsync( sol, 0, sizeof(double) * static_cast<size_t>( nk ), st ) );
+        for( std::int32_t c = 0; c < k; ++c ) { relres[c] = 0.0; }
+        out.converged = true;
+        return TB_OK;
+    }
+    const size_t mk = static_cast<size_t>( m );
+    std::vector<double> H( (mk + 1) * mk * static_cast<size_t>( k ) ), cs( mk * k ), sn( mk * k ), beta( (mk + 1) * k );
+    auto Hat = [&]( size_t i, size_t j, std::int32_t c ) -> double & { return H[(i * mk + j) * k + static_cast<size_t>( c )]; };
+    bool first = true;
+    for( std::int32_t restart = 0; restart <= max_restarts; ++restart )
+    {
+        // r = b - A x (x = 0 at a start without a guess); Q_0 = P r / |P r|
+        if( first && !use_x0 )
+        {
+            TB_CUDA( cudaMemsetAsync( sol, 0, sizeof(double) * static_cast<size_t>( nk ), st ) );
+            TB_TRY( precondition( d_B, ldB, Q ) );
+        }
+        else
+        {
+            tb::launch_apply_shifted( n, h->a_outer.ptr, h->a_inner.ptr, vals, shift, sol, k, d_B, ldB, z, k, k, st );
+            TB_TRY( precondition( z, k, Q ) );
+        }
+        first = false;
+        TB_TRY( sqnorms( Q, qsq ) );
+        tb::launch_col_normalize( Q, n, k, qsq, st );
+        TB_TRY( fetch( qsq, static_cast<size_t>( k ) ) );
+        std::fill( H.begin(), H.end(), 0.0 );
+        std::fill( beta.begin(), beta.end(), 0.0 );
+        bool succ = true;
+        for( std::int32_t c = 0; c < k; ++c )
+        {
+            beta[static_cast<size_t>( c )] = std::sqrt( hp[c] );
+            succ = succ && beta[static_cast<size_t>( c )] <= tol[static_cast<size_t>( c )];
+        }
+        std::int32_t iter = 0;
+        while( !succ && iter < m )
+        {
+            double * qn = Q + (static_cast<std::int64_t>( iter ) + 1) * nk;
+            tb::launch_apply_shifted( n, h->a_outer.ptr, h->a_inner.ptr, vals, shift, Q + static_cast<std::int64_t>( iter ) * nk,
+                                      k, nullptr, k, z, k, k, st );                      // z = A Q_iter
+            TB_TRY( precondition( z, k, qn ) );                                          // Q_iter+1 = P A Q_iter
+            for( int g = 0; g < 2; ++g )
+            {
+                // classical Gram-Schmidt against Q_0..Q_iter, twice
+                double * hg = hd + static_cast<std::int64_t>( g ) * (static_cast<std::int64_t>( m ) + 1) * k;
+                TB_CUDA( cudaMemsetAsync( hg, 0, sizeof(double) * static_cast<size_t>( iter + 1 ) * k, st ) );
+                tb::launch_multi_dots( Q, nk, iter + 1, qn, n, k, hg, st );
+                tb::launch_multi_axpy( Q, nk, iter + 1, hg, -1.0, qn, n, k, st );
+            }
+            TB_TRY( sqnorms( qn, qsq ) );
+            tb::launch_col_normalize( qn, n, k, qsq, st );
+            // both passes' coefficients and |q|^2 to the host: hp = [pass 0][pass 1][|q|^2]
+            const size_t it = static_cast<size_t>( iter );
+            TB_CUDA( cudaMemcpyAsync( hp, hd, sizeof(double) * (it + 1) * k, cudaMemcpyDeviceToHost, st ) );
+            TB_CUDA( cudaMemcpyAsync( hp + (it + 1) * k, hd + (static_cast<std::int64_t>( m ) + 1) * k,
+                                      sizeof(double) * (it + 1) * k, cudaMemcpyDeviceToHost, st ) );
+            TB_CUDA( cudaMemcpyAsync( hp + 2 * (it + 1) * k, qsq, sizeof(double) * static_cast<size_t>( k ), cudaMemcpyDeviceToHost, st ) );
+            TB_CUDA( cudaStreamSynchronize( st ) );
+            TB_TRY( check_solve_error( h ) );
+            for( std::int32_t c = 0; c < k; ++c )
+            {
+                const size_t cc = static_cast<size_t>( c );
+                for( size_t i = 0; i <= it; ++i ) { Hat( i, it, c ) = hp[i * k + cc] + hp[(it + 1 + i) * k + cc]; }
+                Hat( it + 1, it, c ) = std::sqrt( std::max( hp[2 * (it + 1) * k + cc], 0.0 ) );
+                // Givens rotations (GMRES.hpp:592-655)
+                for( size_t i = 0; i < it; ++i )
+                {
+                    const double xi = Hat( i, it, c ), eta = Hat( i + 1, it, c );
+                    const double co = cs[i * k + cc], si = sn[i * k + cc];
+                    Hat( i, it, c ) = co * xi + si * eta;
+                    Hat( i + 1, it, c ) = -si * xi + co * eta;
+                }
+                const double xi = Hat( it, it, c ), eta = Hat( it + 1, it, c );
+                const double r = std::sqrt( xi * xi + eta * eta );
+                double co, si;
+                if( std::abs( xi ) <= std::numeric_limits<double>::epsilon() * r ) { co = 0.0; si = 1.0; }
+                else { co = std::abs( xi ) / r; si = (xi / std::abs( xi )) * eta / r; }
+                cs[it * k + cc] = co;
+                sn[it * k + cc] = si;
+                Hat( it, it, c ) = co * xi + si * eta;
+                Hat( it + 1, it, c ) = 0.0;
+                beta[(it + 1) * k + cc] = -si * beta[it * k + cc];
+                beta[it * k + cc] = co * beta[it * k + cc];
+            }
+            ++iter;
+            succ = true;
+            for( std::int32_t c = 0; c < k; ++c )
+            {
+                succ = succ && std::abs( beta[static_cast<size_t>( iter ) * k + static_cast<size_t>( c )] ) <= tol[static_cast<size_t>( c )];
+            }
+        }
+        // least squares: H y = beta (upper triangular, iter x iter), then x += Q y
+        if( iter > 0 )
+        {
+            std::vector<double> y( static_cast<size_t>( iter ) * k );
+            for( std::int32_t c = 0; c < k; ++c )
+            {
+                const size_t cc = static_cast<size_t>( c );
+                for( std::int32_t i = iter - 1; i >= 0; --i )
+                {
+                    double v = beta[static_cast<size_t>( i ) * k + cc];
+                    for( std::int32_t j = i + 1; j < iter; ++j ) { v -= Hat( static_cast<size_t>( i ), static_cast<size_t>( j ), c ) * y[static_cast<size_t>( j ) * k + cc]; }
+                    const double d = Hat( static_cast<size_t>( i ), static_cast<size_t>( i ), c );
+                    y[static_cast<size_t>( i ) * k + cc] = d != 0.0 ? v / d : 0.0;
+                }
+            }
+            std::copy( y.begin(), y.end(), hp );
+            TB_CUDA( cudaMemcpyAsync( hd, hp, sizeof(double) * y.size(), cudaMemcpyHostToDevice, st ) );
+            tb::launch_multi_axpy( Q, nk, iter, hd, 1.0, sol, n, k, st );
+            TB_CUDA( cudaStreamSynchronize( st ) );          // hp is reused by the next restart
+        }
+        out.iterations += iter;
+        out.restarts = restart;
+        for( std::int32_t c = 0; c < k; ++c )
+        {
+            const size_t cc = static_cast<size_t>( c );
+            relres[c] = bn[cc] > 0.0 ? std::abs( beta[static_cast<size_t>( iter ) * k + cc] ) / bn[cc] : 0.0;
+        }
+        if( succ ) { out.converged = true; break; }
+    }
+    TB_CUDA( cudaGetLastError() );
+    return TB_OK;
+}
+
 int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32_t ldB,
                        double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs )
 {
@@ -951,6 +1142,7 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
         return TB_OK;
     };
 
+    h->gmres_iters = -1;
     TB_TRY( dots( d_B, ldB, d_B, ldB, bb ) );
     TB_TRY( run_solve_core( h, 2, 1.0, d_B, ldB, 0.0, X, k, k ) );   // x0 = F^{-1} b
     launches += h->solve_launch_count;
@@ -1010,6 +1202,36 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
     }
     if( (broke_down || !(h->ir_relres <= h->ir_tol)) && h->precision == TB_PRECISION_MIXED )
     {
+        // GMRES-IR (Carson & Higham 2018): GMRES on the FP64 system, preconditioned by the same
+        // FP32 factor, from the refinement's iterate (from zero if that broke down); accepted when
+        // the true residual meets the target, else the matrix is refactored in FP64
+        std::vector<double> rel( static_cast<size_t>( k ) );
+        GmresOutcome go;
+        // (its stopping rule bounds the preconditioned residual: a tenth of the target leaves room for the true one)
+        const int gst = run_gmres( h, h->values.ptr, shift, d_B, ldB, k, X, !broke_down, 0.1 * h->ir_tol, 30, 3, rel.data(), go );
+        if( gst == TB_OK )
+        {
+            apply( X, d_B, R );
+            TB_TRY( dots( R, k, R, k, rr ) );
+            TB_CUDA( cudaMemcpyAsync( hn, rr, sizeof(double) * 2 * static_cast<size_t>( k ), cudaMemcpyDeviceToHost, st ) );
+            TB_CUDA( cudaStreamSynchronize( st ) );
+            double rel_true = 0.0;
+            for( std::int32_t c = 0; c < k; ++c )
+            {
+                const double bn = std::sqrt( hn[k + c] ), rn = std::sqrt( hn[c] );
+                const double v = bn > 0.0 ? rn / bn : rn;
+                if( !(v <= rel_true) ) { rel_true = v; }
+            }
+            h->gmres_iters = go.iterations;
+            if( rel_true <= h->ir_tol )
+            {
+                h->ir_relres = rel_true;
+                tb::launch_combine( n, k, alpha, X, k, beta, d_X, ldX, st );
+                h->solve_launch_count = launches + 1;
+                TB_CUDA( cudaGetLastError() );
+                return TB_OK;
+            }
+        }
         return solve_fp64_fallback( h, alpha, d_B, ldB, beta, d_X, ldX, nrhs );
     }
     if( broke_down )
@@ -1517,6 +1739,97 @@ int tb_chol_cg( tb_chol * h, const double * values, double reg, double alpha, co
     TB_CUDA( cudaStreamSynchronize( st ) );
     if( status != TB_OK ) { g_error = msg; }
     return status;
+}
+
+// GMRES preconditioned by the factor: the reference's GMRES::operator()
+// (GMRES.hpp:124-330) with the operator (A' + reg I) and P = the factor's
+// solve; X = alpha x + beta X.  Device buffers.
+int tb_chol_gmres_device( tb_chol * h, const double * d_values, double reg, double alpha, const double * d_B, std::int32_t ldB,
+                          double beta, double * d_X, std::int32_t ldX, std::int32_t nrhs, double rel_tol, std::int32_t max_iter,
+                          std::int32_t max_restarts, std::int32_t use_initial_guess, std::int32_t * iterations,
+                          std::int32_t * restarts, double * relres )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    const std::int32_t n = h->n;
+    const std::int32_t k = std::max( 1, nrhs );
+    if( d_B == nullptr || d_X == nullptr || ldB < k || ldX < k || max_iter < 1 || max_restarts < 0 || !(rel_tol >= 0.0) )
+    {
+        return fail( TB_ERR_INVALID_ARGUMENT, "GMRES: bad argument" );
+    }
+    cudaStream_t st = h->stream;
+    const std::int64_t nk = static_cast<std::int64_t>( n ) * k;
+    TB_TRY( h->cg_buf.reserve( nk ) );
+    double * x = h->cg_buf.ptr;
+    std::vector<double> rel( static_cast<size_t>( k ), 0.0 );
+    GmresOutcome go;
+    if( alpha != 0.0 )
+    {
+        if( use_initial_guess ) { tb::launch_combine( n, k, 1.0, d_X, ldX, 0.0, x, k, st ); }
+        const double * vals = d_values != nullptr ? d_values : h->values.ptr;
+        TB_TRY( run_gmres( h, vals, reg, d_B, ldB, k, x, use_initial_guess != 0, rel_tol, max_iter, max_restarts, rel.data(), go ) );
+        tb::launch_combine( n, k, alpha, x, k, beta, d_X, ldX, st );          // X = alpha x + beta X
+    }
+    else
+    {
+        go.converged = true;
+        tb::launch_combine( n, k, beta, d_X, ldX, 0.0, d_X, ldX, st );
+    }
+    TB_CUDA( cudaGetLastError() );
+    TB_CUDA( cudaStreamSynchronize( st ) );
+    if( iterations ) { *iterations = go.iterations; }
+    if( restarts ) { *restarts = go.restarts; }
+    if( relres ) { for( std::int32_t c = 0; c < k; ++c ) { relres[c] = rel[static_cast<size_t>( c )]; } }
+    if( !go.converged )
+    {
+        return fail( TB_ERR_NOT_CONVERGED, "GMRES: not converged after " + std::to_string( go.restarts ) + " restarts ("
+                     + std::to_string( go.iterations ) + " steps)" );
+    }
+    return TB_OK;
+}
+
+// Host-buffer form of tb_chol_gmres_device (values NULL: those of the last factorization).
+int tb_chol_gmres( tb_chol * h, const double * values, double reg, double alpha, const double * B, std::int32_t ldB,
+                   double beta, double * X, std::int32_t ldX, std::int32_t nrhs, double rel_tol, std::int32_t max_iter,
+                   std::int32_t max_restarts, std::int32_t use_initial_guess, std::int32_t * iterations,
+                   std::int32_t * restarts, double * relres )
+{
+    TB_TRY( check_handle( h ) );
+    TB_TRY( require_factor( h ) );
+    const std::int32_t k = std::max( 1, nrhs );
+    if( B == nullptr || X == nullptr || ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "GMRES: bad argument" ); }
+    const std::int64_t nnz = h->outer[h->n];
+    const std::int64_t nk = static_cast<std::int64_t>( h->n ) * k;
+    cudaStream_t st = h->stream;
+    TB_TRY( h->cg_host.reserve( (values != nullptr ? nnz : 0) + 2 * nk ) );
+    double * dB = h->cg_host.ptr;
+    double * dX = dB + nk;
+    double * dv = values != nullptr ? dX + nk : nullptr;
+    TB_CUDA( cudaMemcpy2DAsync( dB, sizeof(double) * k, B, sizeof(double) * ldB, sizeof(double) * k, h->n, cudaMemcpyHostToDevice, st ) );
+    if( use_initial_guess || beta != 0.0 )
+    {
+        TB_CUDA( cudaMemcpy2DAsync( dX, sizeof(double) * k, X, sizeof(double) * ldX, sizeof(double) * k, h->n, cudaMemcpyHostToDevice, st ) );
+    }
+    else
+    {
+        TB_CUDA( cudaMemsetAsync( dX, 0, sizeof(double) * static_cast<size_t>( nk ), st ) );
+    }
+    if( dv != nullptr ) { TB_CUDA( cudaMemcpyAsync( dv, values, sizeof(double) * static_cast<size_t>( nnz ), cudaMemcpyHostToDevice, st ) ); }
+    const int status = tb_chol_gmres_device( h, dv, reg, alpha, dB, k, beta, dX, k, nrhs, rel_tol, max_iter, max_restarts,
+                                             use_initial_guess, iterations, restarts, relres );
+    if( status < 0 && status != TB_ERR_NOT_CONVERGED ) { return status; }
+    const std::string msg = g_error;
+    TB_CUDA( cudaMemcpy2DAsync( X, sizeof(double) * ldX, dX, sizeof(double) * k, sizeof(double) * k, h->n, cudaMemcpyDeviceToHost, st ) );
+    TB_CUDA( cudaStreamSynchronize( st ) );
+    if( status != TB_OK ) { g_error = msg; }
+    return status;
+}
+
+int tb_chol_gmres_ir_iterations( tb_chol * h, std::int32_t * out )
+{
+    TB_TRY( check_handle( h ) );
+    if( out ) { *out = h->gmres_iters; }
+    return TB_OK;
 }
 
 int tb_chol_sn_count( tb_chol * h, std::int32_t * out )

@@ -1627,6 +1627,50 @@ __global__ void cg_update_p_kernel( int n, int k, const double * __restrict__ rz
     }
 }
 
+// GMRES (GMRES.hpp): out[i k + c] += Q_i(:, c) . q(:, c) for the nq Krylov
+// vectors Q_i (n x k each, nk apart); blockIdx.y = i.
+__global__ void multi_dots_kernel( const double * __restrict__ Q, std::int64_t nk, const double * __restrict__ q,
+                                   int n, int k, double * __restrict__ out )
+{
+    const double * Qi = Q + blockIdx.y * nk;
+    for( int c = 0; c < k; ++c )
+    {
+        double s = 0.0;
+        for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
+        {
+            s += Qi[i * k + c] * q[i * k + c];
+        }
+#pragma unroll
+        for( int o = 16; o > 0; o >>= 1 ) { s += __shfl_xor_sync( 0xffffffffu, s, o ); }
+        if( (threadIdx.x & 31) == 0 && s != 0.0 ) { atomicAdd( out + blockIdx.y * k + c, s ); }
+    }
+}
+
+// q += sign * sum_{i < nq} coef[i k + c] Q_i(:, c).
+__global__ void multi_axpy_kernel( const double * __restrict__ Q, std::int64_t nk, int nq, const double * __restrict__ coef,
+                                   double sign, double * __restrict__ q, int n, int k )
+{
+    const std::int64_t total = (std::int64_t)n * k;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total; e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const int c = static_cast<int>( e % k );
+        double s = 0.0;
+        for( int i = 0; i < nq; ++i ) { s += coef[i * k + c] * Q[i * nk + e]; }
+        q[e] += sign * s;
+    }
+}
+
+// x(:, c) /= sqrt(sq[c]) where sq[c] > 0 (normalises by squared column norms).
+__global__ void col_normalize_kernel( double * __restrict__ x, int n, int k, const double * __restrict__ sq )
+{
+    const std::int64_t total = (std::int64_t)n * k;
+    for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total; e += (std::int64_t)gridDim.x * blockDim.x )
+    {
+        const int c = static_cast<int>( e % k );
+        if( sq[c] > 0.0 ) { x[e] /= sqrt( sq[c] ); }
+    }
+}
+
 __global__ void axpy_kernel( std::int64_t n, double a, const double * __restrict__ x, double * __restrict__ y )
 {
     for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
@@ -1966,6 +2010,24 @@ void launch_cg_update_p( int n, int k, const double * rz_new, const double * rz_
                          cudaStream_t st )
 {
     cg_update_p_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( n, k, rz_new, rz_old, z, p );
+}
+
+void launch_multi_dots( const double * Q, std::int64_t nk, int nq, const double * q, int n, int k, double * out, cudaStream_t st )
+{
+    if( nq <= 0 ) { return; }
+    multi_dots_kernel<<<dim3( static_cast<unsigned>( grid_for( n, 256 ) ), static_cast<unsigned>( nq ) ), 256, 0, st>>>( Q, nk, q, n, k, out );
+}
+
+void launch_multi_axpy( const double * Q, std::int64_t nk, int nq, const double * coef, double sign, double * q, int n, int k,
+                        cudaStream_t st )
+{
+    if( nq <= 0 ) { return; }
+    multi_axpy_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( Q, nk, nq, coef, sign, q, n, k );
+}
+
+void launch_col_normalize( double * x, int n, int k, const double * sq, cudaStream_t st )
+{
+    col_normalize_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( x, n, k, sq );
 }
 
 void launch_axpy( std::int64_t n, double a, const double * x, double * y, cudaStream_t st )

@@ -144,6 +144,12 @@ void launch_cg_update_xr( int n, int k, const double * rz, const double * pq, co
 void launch_cg_update_p( int n, int k, const double * rz_new, const double * rz_old, const double * z, double * p,
                          cudaStream_t st );
 void launch_axpy( std::int64_t n, double a, const double * x, double * y, cudaStream_t st );
+// GMRES: out[i k + c] += Q_i(:, c) . q(:, c) for the nq vectors Q_i = Q + i nk;
+// q += sign sum_i coef[i k + c] Q_i(:, c); x(:, c) /= sqrt(sq[c]) where sq[c] > 0.
+void launch_multi_dots( const double * Q, std::int64_t nk, int nq, const double * q, int n, int k, double * out, cudaStream_t st );
+void launch_multi_axpy( const double * Q, std::int64_t nk, int nq, const double * coef, double sign, double * q, int n, int k,
+                        cudaStream_t st );
+void launch_col_normalize( double * x, int n, int k, const double * sq, cudaStream_t st );
 void launch_combine( int n, int k, double alpha, const double * X, int ldx, double beta, double * Y, int ldy, cudaStream_t st );
 template<typename T>
 void launch_gather_diag( const std::int64_t * offsets, const T * arena, double * out, int n, cudaStream_t st );

@@ -98,15 +98,18 @@ int main( int argc, char ** argv )
     }
     const bool ok = S.ConjugateGradient( val2.data(), 0.0, 1.0, B.data(), nrhs, 0.0, X.data(), nrhs, nrhs, 1e-12, 200 );
     std::printf( "cg_ok %d\ncg_iter %d\n", ok ? 1 : 0, S.IterationCount() );
+    const bool gok = S.GMRES( val2.data(), 0.0, 1.0, B.data(), nrhs, 0.0, X.data(), nrhs, nrhs, 1e-12, 30, 10 );
+    std::printf( "gmres_ok %d\ngmres_iter %d\n", gok ? 1 : 0, S.IterationCount() );
 
-    auto relres_of = [&]( const std::vector<double> & Y ) {
+    // relative residual of Y for the matrix with values vv
+    auto relres_of = [&]( const std::vector<double> & vv, const std::vector<double> & Y ) {
         double r2 = 0.0, b2 = 0.0;
         for( int r = 0; r < n; ++r )
         {
             for( int k = 0; k < nrhs; ++k )
             {
                 double ax = 0.0;
-                for( int64_t l = outer[r]; l < outer[r + 1]; ++l ) { ax += val[l] * Y[inner[l] * nrhs + k]; }
+                for( int64_t l = outer[r]; l < outer[r + 1]; ++l ) { ax += vv[l] * Y[inner[l] * nrhs + k]; }
                 const double d = B[r * nrhs + k] - ax;
                 r2 += d * d;
                 b2 += B[r * nrhs + k] * B[r * nrhs + k];
@@ -132,13 +135,13 @@ int main( int argc, char ** argv )
     }
     std::printf( "relres_f32_in %.3e\n", std::sqrt( rn2 / bn2 ) );
 
-    // Scal = float: FP32 factor of float values, refined solves
+    // Scal = float: FP32 factor of float values, solves refined against those values (as FP64)
     CholeskyDecompositionF F( outer.data(), inner.data(), p.data(), n, 1 );
     std::vector<float> valf( val.begin(), val.end() );
     std::printf( "status_f32 %d\n", F.NumericFactorization( valf.data(), 0.0f ) );
     std::vector<double> Xf( B.size() );
     F.Solve( B.data(), Xf.data(), nrhs );
-    std::printf( "relres_f32_factor %.3e\n", relres_of( Xf ) );
+    std::printf( "relres_f32_factor %.3e\n", relres_of( std::vector<double>( valf.begin(), valf.end() ), Xf ) );
 
     // SwapNumericalFactorization: S's factor moves to a second decomposition of the same pattern
     CholeskyDecomposition S2( outer.data(), inner.data(), p.data(), n, 1 );
@@ -148,6 +151,6 @@ int main( int argc, char ** argv )
     S2.SwapNumericalFactorization( cont );
     std::vector<double> X2( B.size() );
     S2.Solve( B.data(), X2.data(), nrhs );
-    std::printf( "swap_moved %d\nrelres_swapped %.3e\n", moved ? 1 : 0, relres_of( X2 ) );
+    std::printf( "swap_moved %d\nrelres_swapped %.3e\n", moved ? 1 : 0, relres_of( val, X2 ) );
     return 0;
 }

@@ -58,9 +58,11 @@ def test_cpp_mirror_factor_and_solve(mirror_exe):
     assert int(vals["status"]) == 0
     assert float(vals["relres"]) < 1e-13
     assert int(vals["cg_ok"]) == 1 and 1 <= int(vals["cg_iter"]) <= 200
+    assert int(vals["gmres_ok"]) == 1 and 1 <= int(vals["gmres_iter"]) <= 330
     assert float(vals["relres_f32_in"]) < 1e-13                        # float B, double X
     assert int(vals["status_f32"]) == 0
     assert float(vals["relres_f32_factor"]) <= 1e-12                   # Scal = float: refined to the default 1e-12
+                                                                       # (for the float values it was given)
     assert int(vals["swap_moved"]) == 1
     assert float(vals["relres_swapped"]) < 1e-13
 
