@@ -208,6 +208,7 @@ struct tb_chol
     double kind_ms[8] = {};
     std::int64_t kind_launches[8] = {};
     std::vector<cudaEvent_t> events;
+    std::vector<cudaEvent_t> chunk_events;   // host solves: completion of each chunk copied back
     std::vector<float> launch_ms;          // per factor launch of the last profiled run (0 = clear + assembly)
     std::vector<cudaEvent_t> solve_events;
     std::vector<std::int64_t> solve_info;  // per solve launch of the last profiled solve: upper, level, step, tasks
@@ -231,6 +232,7 @@ struct tb_chol
     ~tb_chol()
     {
         for( cudaEvent_t e : events ) { cudaEventDestroy( e ); }
+        for( cudaEvent_t e : chunk_events ) { cudaEventDestroy( e ); }
         for( cudaEvent_t e : solve_events ) { cudaEventDestroy( e ); }
         drop_solve_graphs();
         if( factor_graph ) { cudaGraphExecDestroy( factor_graph ); }
@@ -990,8 +992,9 @@ int run_gmres( tb_chol * h, const double * vals, double shift, const double * d_
         // r = b - A x (x = 0 at a start without a guess); Q_0 = P r / |P r|
         if( first && !use_x0 )
         {
+            // x = 0: P r = P b, which z still holds
             TB_CUDA( cudaMemsetAsync( sol, 0, sizeof(double) * static_cast<size_t>( nk ), st ) );
-            TB_TRY( precondition( d_B, ldB, Q ) );
+            TB_CUDA( cudaMemcpyAsync( Q, z, sizeof(double) * static_cast<size_t>( nk ), cudaMemcpyDeviceToDevice, st ) );
         }
         else
         {
@@ -1269,14 +1272,13 @@ int run_solve_device( tb_chol * h, int which, double alpha, const double * d_B, 
 // Solve.hpp:20-27, ReadNonzeroValues Numeric.hpp:165-180).
 int dtype_size( std::int32_t dtype ) { return dtype == TB_F32 ? 4 : dtype == TB_F64 ? 8 : 0; }
 
-// body(b, e) over rows [0, n) on all host threads once a copy is large
-// enough to be bound by one thread's memory bandwidth (about 4 MB a thread).
+// body(b, e) over rows [0, n) on up to 16 host threads, one per MB of copy.
 template<typename Body>
 void host_rows( std::int64_t n, std::int64_t row_bytes, Body && body )
 {
     const std::int64_t total = n * std::max<std::int64_t>( row_bytes, 1 );
     const unsigned hw = std::max( 1u, std::thread::hardware_concurrency() );
-    const std::int64_t threads = std::min<std::int64_t>( std::min<std::int64_t>( hw, 16 ), std::max<std::int64_t>( 1, total >> 22 ) );
+    const std::int64_t threads = std::min<std::int64_t>( std::min<std::int64_t>( hw, 16 ), std::max<std::int64_t>( 1, total >> 20 ) );
     if( threads <= 1 || n < 2 ) { body( std::int64_t( 0 ), n ); return; }
     std::vector<std::thread> pool;
     for( std::int64_t t = 0; t < threads; ++t )
@@ -1349,18 +1351,48 @@ int run_solve_host( tb_chol * h, int which, double alpha, const void * B, std::i
     TB_TRY( h->out.reserve( static_cast<std::int64_t>(n) * k ) );
     double * pi = h->pin_in.as<double>();
     double * po = h->pin_out.as<double>();
-    stage_rows_in( pi, B, b_dtype, n, k, ldB );
-    TB_CUDA( cudaMemcpyAsync( h->in.ptr, pi, bytes, cudaMemcpyHostToDevice, st ) );
-    if( beta != 0.0 )
+    // in chunks of rows: the copy of chunk c to the device runs while the host stages chunk c + 1
+    const std::int64_t rows_per_chunk = std::max<std::int64_t>( 1, (std::int64_t( 16 ) << 20) / (8 * std::int64_t( k )) );
+    const int esz = dtype_size( b_dtype ), xsz = dtype_size( x_dtype );
+    for( std::int64_t r0 = 0; r0 < n; r0 += rows_per_chunk )
     {
-        stage_rows_in( po, X, x_dtype, n, k, ldX );
-        TB_CUDA( cudaMemcpyAsync( h->out.ptr, po, bytes, cudaMemcpyHostToDevice, st ) );
+        const std::int64_t rc = std::min<std::int64_t>( rows_per_chunk, n - r0 );
+        stage_rows_in( pi + r0 * k, static_cast<const char *>( B ) + r0 * ldB * esz, b_dtype, rc, k, ldB );
+        TB_CUDA( cudaMemcpyAsync( h->in.ptr + r0 * k, pi + r0 * k, sizeof(double) * static_cast<size_t>( rc * k ),
+                                  cudaMemcpyHostToDevice, st ) );
+        if( beta != 0.0 )
+        {
+            stage_rows_in( po + r0 * k, static_cast<const char *>( X ) + r0 * ldX * xsz, x_dtype, rc, k, ldX );
+            TB_CUDA( cudaMemcpyAsync( h->out.ptr + r0 * k, po + r0 * k, sizeof(double) * static_cast<size_t>( rc * k ),
+                                      cudaMemcpyHostToDevice, st ) );
+        }
     }
     TB_TRY( run_solve_device( h, which, alpha, h->in.ptr, k, beta, h->out.ptr, k, k ) );
-    TB_CUDA( cudaMemcpyAsync( po, h->out.ptr, bytes, cudaMemcpyDeviceToHost, st ) );
+    // back in chunks: the host unstages chunk c while chunk c + 1 is copied
+    std::vector<cudaEvent_t> done;
+    for( std::int64_t r0 = 0; r0 < n; r0 += rows_per_chunk )
+    {
+        const std::int64_t rc = std::min<std::int64_t>( rows_per_chunk, n - r0 );
+        TB_CUDA( cudaMemcpyAsync( po + r0 * k, h->out.ptr + r0 * k, sizeof(double) * static_cast<size_t>( rc * k ),
+                                  cudaMemcpyDeviceToHost, st ) );
+        if( h->chunk_events.size() <= done.size() )
+        {
+            cudaEvent_t e;
+            TB_CUDA( cudaEventCreateWithFlags( &e, cudaEventDisableTiming ) );
+            h->chunk_events.push_back( e );
+        }
+        TB_CUDA( cudaEventRecord( h->chunk_events[done.size()], st ) );
+        done.push_back( h->chunk_events[done.size()] );
+    }
+    size_t c = 0;
+    for( std::int64_t r0 = 0; r0 < n; r0 += rows_per_chunk, ++c )
+    {
+        const std::int64_t rc = std::min<std::int64_t>( rows_per_chunk, n - r0 );
+        TB_CUDA( cudaEventSynchronize( done[c] ) );
+        if( c == 0 ) { TB_TRY( check_solve_error( h ) ); }
+        stage_rows_out( static_cast<char *>( X ) + r0 * ldX * xsz, x_dtype, ldX, po + r0 * k, rc, k );
+    }
     TB_CUDA( cudaStreamSynchronize( st ) );
-    TB_TRY( check_solve_error( h ) );
-    stage_rows_out( X, x_dtype, ldX, po, n, k );
     return TB_OK;
 }
 
@@ -1503,8 +1535,16 @@ int tb_chol_numeric_ex( tb_chol * h, const void * values, std::int32_t dtype, do
     TB_TRY( ensure_device( h ) );
     const size_t bytes = sizeof(double) * static_cast<size_t>( h->sym.nnz );
     TB_TRY( h->pin_in.reserve( bytes ) );
-    stage_rows_in( h->pin_in.as<double>(), values, dtype, h->sym.nnz, 1, 1 );
-    TB_CUDA( cudaMemcpyAsync( h->values.ptr, h->pin_in.ptr, bytes, cudaMemcpyHostToDevice, h->stream ) );
+    // in chunks: the copy of chunk c to the device runs while the host stages chunk c + 1
+    const std::int64_t chunk = std::int64_t( 2 ) << 20;          // values per chunk (16 MB of FP64)
+    const int esz = dtype_size( dtype );
+    double * pin = h->pin_in.as<double>();
+    for( std::int64_t i0 = 0; i0 < h->sym.nnz; i0 += chunk )
+    {
+        const std::int64_t c = std::min<std::int64_t>( chunk, h->sym.nnz - i0 );
+        stage_rows_in( pin + i0, static_cast<const char *>( values ) + i0 * esz, dtype, c, 1, 1 );
+        TB_CUDA( cudaMemcpyAsync( h->values.ptr + i0, pin + i0, sizeof(double) * static_cast<size_t>( c ), cudaMemcpyHostToDevice, h->stream ) );
+    }
     return run_factor( h, reg );
 }
 
