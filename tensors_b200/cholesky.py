@@ -617,7 +617,7 @@ class CholeskyDecomposition:
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
                 "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks",
                 "solve_graph_tasks", "solve_split_level", "graph_ctas", "analyze_us", "plan_us", "tc_tiles",
-                "image_blocks"]
+                "image_blocks", "gemm_flops", "gemm_tile_flops"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

@@ -2051,7 +2051,8 @@ int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
         static_cast<std::int64_t>( pl.front_flops ), static_cast<std::int64_t>( pl.dag_makespan_us ),
         static_cast<std::int64_t>( pl.dag.size() ), static_cast<std::int64_t>( pl.solve_fwd_order.size() ),
         pl.solve_split_level, h->dag_grid, h->analyze_us, h->plan_us,
-        static_cast<std::int64_t>( pl.tc.size() ), pl.img_blocks };
+        static_cast<std::int64_t>( pl.tc.size() ), pl.img_blocks, static_cast<std::int64_t>( pl.gemm_flops ),
+        static_cast<std::int64_t>( pl.gemm_tile_flops ) };
     const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
     for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
     return m;

@@ -402,6 +402,7 @@ void Plan::build( const Symbolic & sym )
     // -------------------------------------------------- launch sequences
     gemm.clear(); tc.clear(); potrf.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
     gemm_flops = 0.0;
+    gemm_tile_flops = 0.0;
     factor_launches.clear(); lower_launches.clear(); upper_launches.clear();
     dag.clear();
 
@@ -683,6 +684,7 @@ void Plan::build( const Symbolic & sym )
                 const GemmTask & t = tiles[i];
                 const double rows = std::min( kTile, t.M - t.m0 ), cols = std::min( kTile, t.N - t.c0 );
                 gemm_flops += 2.0 * t.K * (t.upper ? rows * (rows + 1.0) / 2.0 + rows * (cols - rows) : rows * cols);
+                gemm_tile_flops += 2.0 * t.K * kTile * kTile;
                 const I32 pi = tile_panel[i];
                 const I32 prev = tile_prev[i];
                 PendingTask d = make( LaunchKind::Gemm, static_cast<I64>(gemm.size()) );

@@ -309,6 +309,7 @@ struct Plan
     std::vector<std::int32_t> solve_panel_tasks;  // per graph panel
 
     double gemm_flops = 0.0;                // useful flops of all GEMM tiles (upper part of diagonal tiles)
+    double gemm_tile_flops = 0.0;           // the flops the 64 x 64 tiles execute (full tiles, full depth)
     double factor_flops = 0.0;              // reference supernodes: Sum [n0^3/3 + n0^2 n1 + n0 n1^2]
     double front_flops  = 0.0;              // the same sum over fronts (work actually executed)
     double nnz_u = 0.0;                     // reference supernodes: Sum [n0(n0+1)/2 + n0 n1]
