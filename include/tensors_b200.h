@@ -217,7 +217,9 @@ int tb_chol_flop_count( tb_chol * h, double * factor_flops, double * nnz_u );
  * out[17] / out[18] host microseconds of the last symbolic analysis / plan
  * build, out[19] tensor-core tiles of the mixed-precision path, out[20]
  * blocks of its operand image (8 KB each), out[21] useful flops of the
- * 64 x 64 GEMM tiles, out[22] the flops those tiles execute (full tiles).  Returns the number of entries
+ * 64 x 64 GEMM tiles, out[22] the flops those tiles execute (full tiles),
+ * out[23] super-panels of the large fronts' solves, out[24] / out[25] the
+ * forward / back sweep launches with them.  Returns the number of entries
  * written (at most cap). */
 int tb_chol_plan_stats( tb_chol * h, int64_t * out, int32_t cap );
 /* Host-side bounds check of every device task of the plan (also run before

@@ -612,12 +612,13 @@ class CholeskyDecomposition:
         return f.value, z.value
 
     def PlanStats(self) -> dict:
-        out = np.zeros(24, dtype=np.int64)
-        m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 24))
+        out = np.zeros(32, dtype=np.int64)
+        m = _check(lib().tb_chol_plan_stats(self._h, out.ctypes.data, 32))
         keys = ["arena_doubles", "update_doubles", "levels", "factor_launches", "gemm_tasks", "panel_tasks",
                 "extend_tasks", "lower_launches", "upper_launches", "supernodes", "fronts", "front_flops", "graph_makespan_us", "graph_tasks",
                 "solve_graph_tasks", "solve_split_level", "graph_ctas", "analyze_us", "plan_us", "tc_tiles",
-                "image_blocks", "gemm_flops", "gemm_tile_flops"]
+                "image_blocks", "gemm_flops", "gemm_tile_flops", "super_panels", "lower_launches_super",
+                "upper_launches_super"]
         return {k: int(out[i]) for i, k in enumerate(keys[:m])}
 
     def CheckPlan(self) -> None:

@@ -155,12 +155,16 @@ struct tb_chol
     DeviceArray<tb::ExtendTask>     extend;
     DeviceArray<tb::SolveDiagTask>  sdiag;
     DeviceArray<tb::SolveRestTask>  srest;
+    DeviceArray<tb::SuperPanel>     spanels;     // super-panel solve of the large fronts (Plan::spanels)
+    DeviceArray<tb::SuperInvTask>   sinv;
+    DeviceArray<tb::SuperSolveTask> ssolve;
+    DeviceArray<double>             tsuper;      // their 512 x 512 inverses
     DeviceArray<std::int64_t>       a_outer;     // caller-order pattern, for residuals
     DeviceArray<std::int32_t>       a_inner;
     DeviceArray<double>             values;      // caller-order values of the last factorization
     DeviceArray<double>             reg;
     DeviceArray<int>                status;
-    DeviceArray<double>             work, work2, in, out, diag_vals;
+    DeviceArray<double>             work, work2, work3, in, out, diag_vals;   // work3: the super-panel back sweep's sums
     DeviceArray<double>             tinv;        // inverse diagonal block of every panel (64 x 64 each)
     DeviceArray<tb::DagTask>        dag;         // the factorization as one dependency-ordered task list
     DeviceArray<int>                dag_state;   // task-graph counters, then the ticket and the error word
@@ -202,6 +206,7 @@ struct tb_chol
     std::map<std::pair<int,int>, cudaGraphExec_t> solve_graphs;
     double * solve_graph_work = nullptr;
     double * solve_graph_work2 = nullptr;
+    double * solve_graph_work3 = nullptr;
 
     // optional per-kernel timing of direct (non-graph) factorizations
     bool profiling = false;
@@ -227,6 +232,7 @@ struct tb_chol
         solve_graphs.clear();
         solve_graph_work = nullptr;
         solve_graph_work2 = nullptr;
+        solve_graph_work3 = nullptr;
     }
 
     ~tb_chol()
@@ -384,6 +390,10 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->extend.upload( pl.extend, st_ ) );
     TB_TRY( h->sdiag.upload( pl.sdiag, st_ ) );
     TB_TRY( h->srest.upload( pl.srest, st_ ) );
+    TB_TRY( h->spanels.upload( pl.spanels, st_ ) );
+    TB_TRY( h->sinv.upload( pl.sinv, st_ ) );
+    TB_TRY( h->ssolve.upload( pl.ssolve, st_ ) );
+    if( pl.super_inv_size > 0 ) { TB_TRY( h->tsuper.reserve( pl.super_inv_size ) ); }
     TB_TRY( h->zero.upload( pl.zero, st_ ) );
     TB_TRY( h->exports.upload( pl.exports, st_ ) );
     TB_TRY( h->colmap.upload( pl.colmap, st_ ) );
@@ -509,7 +519,13 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         a.timeout_ns = kDagTimeoutNs;
         a.trace = h->trace ? h->trace_buf.ptr : nullptr;
         tb::launch_factor_dag<T>( a, h->dag_grid, st );
-        return launches + (pl.dag.empty() ? 0 : 1);
+        launches += pl.dag.empty() ? 0 : 1;
+        for( const tb::Launch & L : pl.sinv_launches )
+        {
+            tb::launch_super_inv( h->sinv.ptr + L.first, L.count, h->spanels.ptr, A, h->tinv.ptr, h->tsuper.ptr, st );
+            ++launches;
+        }
+        return launches;
     }
     // One panel of look-ahead over two streams (the profiled path keeps one,
     // so that every launch is timed alone).  Main stream: potrf(q), trsm(q),
@@ -562,6 +578,13 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         ++launches;
     }
     if( overlap ) { join(); }
+    // the large fronts' super-panel inverses for the solves (after every panel inverse exists)
+    for( const tb::Launch & L : pl.sinv_launches )
+    {
+        tb::launch_super_inv( h->sinv.ptr + L.first, L.count, h->spanels.ptr, A, h->tinv.ptr, h->tsuper.ptr, st );
+        mark( static_cast<int>( tb::LaunchKind::Invert ) );
+        ++launches;
+    }
     return launches;
 }
 
@@ -582,7 +605,7 @@ int run_factor( tb_chol * h, double reg )
     TB_CUDA( cudaMemcpyAsync( h->reg.ptr, pr, sizeof(double), cudaMemcpyHostToDevice, st ) );
     if( h->profiling )
     {
-        const std::size_t need = h->plan.factor_launches.size() + 2;
+        const std::size_t need = h->plan.factor_launches.size() + h->plan.sinv_launches.size() + 2;
         while( h->events.size() < need )
         {
             cudaEvent_t e;
@@ -699,13 +722,29 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
         graph = it != h->solve_grid.end() && it->second > 0;
     }
     const std::int32_t split = graph ? pl.solve_split_level : pl.levels;
+    // the large fronts step by super-panels when every level runs as launches
+    const bool super = !graph && !levels_only && !pl.spanels.empty() && h->work3.ptr != nullptr;
+    const std::vector<tb::Launch> & lower = super ? pl.lower_launches_sp : pl.lower_launches;
+    const std::vector<tb::Launch> & upper_list = super ? pl.upper_launches_sp : pl.upper_launches;
+    double * Z = h->work3.ptr;
     const std::int32_t np = static_cast<std::int32_t>( pl.solve_panel_tasks.size() );
     int * err = h->solve_state.ptr + np + 1;
     if( graph ) { cudaMemsetAsync( err, 0, sizeof(int), st ); }
-    auto step = [&]( const tb::Launch & L, bool upper, double * in, double * out, std::int32_t kc )
+    auto step = [&]( const tb::Launch & L, bool upper, double * in, double * out, std::int32_t kc, std::int32_t c0 )
     {
         begin();
-        if( mixed )
+        if( L.kind == tb::LaunchKind::SuperDiag )
+        {
+            tb::launch_super_diag( h->ssolve.ptr + L.first, L.count, h->spanels.ptr, h->tsuper.ptr, upper, in, Z + c0, out, k, kc, st );
+        }
+        else if( L.kind == tb::LaunchKind::SuperRest )
+        {
+            if( mixed ) { tb::launch_super_rest( h->ssolve.ptr + L.first, L.count, h->spanels.ptr, arena_as<float>( h ), h->sn_inner.ptr,
+                                                 upper, in, Z + c0, out, k, kc, st ); }
+            else        { tb::launch_super_rest( h->ssolve.ptr + L.first, L.count, h->spanels.ptr, arena_as<double>( h ), h->sn_inner.ptr,
+                                                 upper, in, Z + c0, out, k, kc, st ); }
+        }
+        else if( mixed )
         {
             tb::launch_solve_step( h->srest.ptr + L.first, L.count, upper, arena_as<float>( h ), h->tinv.ptr,
                                    h->sn_inner.ptr, in, out, k, kc, st );
@@ -753,7 +792,7 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
         for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
             const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
-            for( const tb::Launch & L : pl.lower_launches ) { if( L.level < split ) { step( L, false, W + c0, Y + c0, kc ); } }
+            for( const tb::Launch & L : lower ) { if( L.level < split ) { step( L, false, W + c0, Y + c0, kc, c0 ); } }
             if( graph ) { persistent( false, W + c0, Y + c0, kc, c0 ); }
         }
     }
@@ -761,11 +800,12 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
     {
         tb::TraceRange range( "Sparse::CholeskyDecomposition::SN_UpperSolve" );
         cudaMemsetAsync( W, 0, sizeof(double) * static_cast<size_t>( h->n ) * k, st );
+        if( super ) { cudaMemsetAsync( Z, 0, sizeof(double) * static_cast<size_t>( h->n ) * k, st ); }
         for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
             const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );
             if( graph ) { persistent( true, Y + c0, W + c0, kc, c0 ); }
-            for( const tb::Launch & L : pl.upper_launches ) { if( L.level < split ) { step( L, true, Y + c0, W + c0, kc ); } }
+            for( const tb::Launch & L : upper_list ) { if( L.level < split ) { step( L, true, Y + c0, W + c0, kc, c0 ); } }
         }
     }
     if( graph ) { cudaMemcpyAsync( h->pin_solve_err.ptr, err, sizeof(int), cudaMemcpyDeviceToHost, st ); }
@@ -820,13 +860,15 @@ int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, st
     if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
     TB_TRY( h->work.reserve( static_cast<std::int64_t>(n) * k ) );
     TB_TRY( h->work2.reserve( static_cast<std::int64_t>(n) * k ) );
+    if( !h->plan.spanels.empty() ) { TB_TRY( h->work3.reserve( static_cast<std::int64_t>(n) * k ) ); }
     double * W = h->work.ptr;
     double * Y = h->work2.ptr;
-    if( h->solve_graph_work != W || h->solve_graph_work2 != Y )
+    if( h->solve_graph_work != W || h->solve_graph_work2 != Y || h->solve_graph_work3 != h->work3.ptr )
     {
         h->drop_solve_graphs();
         h->solve_graph_work = W;
         h->solve_graph_work2 = Y;
+        h->solve_graph_work3 = h->work3.ptr;
     }
     TB_TRY( prepare_solve_grid( h, k ) );
     std::int64_t launches = 0;
@@ -852,7 +894,9 @@ int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, st
     else if( h->profiling )
     {
         const std::int32_t chunks = (k + tb::kSolveMaxRhs - 1) / tb::kSolveMaxRhs;
-        const std::size_t need = 2 * static_cast<std::size_t>( chunks ) * (h->plan.lower_launches.size() + h->plan.upper_launches.size());
+        const std::size_t need = 2 * static_cast<std::size_t>( chunks )
+                               * std::max( h->plan.lower_launches.size() + h->plan.upper_launches.size(),
+                                           h->plan.lower_launches_sp.size() + h->plan.upper_launches_sp.size() );
         while( h->solve_events.size() < need )
         {
             cudaEvent_t e;
@@ -2052,7 +2096,8 @@ int tb_chol_plan_stats( tb_chol * h, std::int64_t * out, std::int32_t cap )
         static_cast<std::int64_t>( pl.dag.size() ), static_cast<std::int64_t>( pl.solve_fwd_order.size() ),
         pl.solve_split_level, h->dag_grid, h->analyze_us, h->plan_us,
         static_cast<std::int64_t>( pl.tc.size() ), pl.img_blocks, static_cast<std::int64_t>( pl.gemm_flops ),
-        static_cast<std::int64_t>( pl.gemm_tile_flops ) };
+        static_cast<std::int64_t>( pl.gemm_tile_flops ), static_cast<std::int64_t>( pl.spanels.size() ),
+        static_cast<std::int64_t>( pl.lower_launches_sp.size() ), static_cast<std::int64_t>( pl.upper_launches_sp.size() ) };
     const std::int32_t m = std::min<std::int32_t>( cap, static_cast<std::int32_t>( sizeof(v) / sizeof(v[0]) ) );
     for( std::int32_t i = 0; i < m; ++i ) { out[i] = v[i]; }
     return m;

@@ -1734,6 +1734,315 @@ int grid_for( std::int64_t work, int threads )
     return static_cast<int>( blocks < 1 ? 1 : (blocks > 148 * 32 ? 148 * 32 : blocks) );
 }
 
+// ------------------------------------------------------ super-panel solve
+// Large fronts solve 512 pivot rows per step (SuperPanel, plan.hpp): the
+// inverse T of the 512 x 512 diagonal block, formed after the factorization
+// from the 64-row panel inverses, replaces eight sequential panel steps by
+// one product with T.  64 x 64 blocks throughout; warp w owns output rows
+// 8w..8w+7 as 8 x 8 DMMA tiles.
+constexpr int kSld = kPanel + 1;                        // padded smem row of a 64 x 64 block
+constexpr size_t kSuperInvSmem = sizeof(double) * 4 * kPanel * kSld;
+
+__device__ __forceinline__ int super_block_rows( const SuperPanel & sp, int b ) { return min( kPanel, sp.rows - b * kPanel ); }
+
+// acc[ct] (this warp's rows of 8 x 8 tile ct) += A(64 x 64) B(64 x 64) with A through a(i, k), B through b(k, j).
+template<typename FA, typename FB>
+__device__ __forceinline__ void block_product_64( double (&acc)[8][2], FA a, FB b )
+{
+    const int warp = threadIdx.x >> 5;
+    for( int kb = 0; kb < kSubs; ++kb )
+    {
+#pragma unroll
+        for( int ct = 0; ct < 8; ++ct )
+        {
+            dmma_8x8x8( acc[ct], [&]( int i, int k ) { return a( 8 * warp + i, 8 * kb + k ); },
+                                 [&]( int k, int j ) { return b( 8 * kb + k, 8 * ct + j ); } );
+        }
+    }
+}
+
+// One block (i, j) of a super-panel's inverse (round j - i; rounds run in
+// order, so the blocks T_kj with k > i are complete): T_ii is panel i's
+// inverse (its nb x nb part), T_ij = -T_ii sum_{k=i+1..j} U_ik T_kj.
+template<typename T>
+__global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __restrict__ tasks, const SuperPanel * __restrict__ sps,
+                                                         const T * __restrict__ arena, const double * __restrict__ tinv,
+                                                         double * __restrict__ tbuf )
+{
+    extern __shared__ __align__(16) double ism[];
+    pdl_allow_next();
+    const SuperInvTask task = tasks[blockIdx.x];
+    const SuperPanel sp = sps[task.sp];
+    pdl_wait();
+    double (*A)[kSld] = reinterpret_cast<double (*)[kSld]>( ism );
+    double (*Bm)[kSld] = A + kPanel;
+    double (*S)[kSld] = Bm + kPanel;
+    double (*Tii)[kSld] = S + kPanel;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i = task.i, j = task.j;
+    const int nbi = super_block_rows( sp, i ), nbj = super_block_rows( sp, j );
+    double * out = tbuf + sp.t + (std::int64_t)(kPanel * i) * kSuperRows + kPanel * j;
+    auto load_tinv = [&]( double (*D)[kSld], int b, int nbb )
+    {
+        const double * src = tinv + (std::int64_t)sp.panel[b] * (kPanel * kPanel);
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 )
+        {
+            const int r = idx >> 6, c = idx & 63;
+            D[r][c] = (r < nbb && c < nbb) ? src[idx] : 0.0;
+        }
+    };
+    if( i == j )
+    {
+        load_tinv( Tii, i, nbi );
+        __syncthreads();
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { out[(idx >> 6) * kSuperRows + (idx & 63)] = Tii[idx >> 6][idx & 63]; }
+        return;
+    }
+    double acc[8][2];
+#pragma unroll
+    for( int ct = 0; ct < 8; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+    const T * U0 = arena + sp.u0;
+    for( int k = i + 1; k <= j; ++k )
+    {
+        const int nbk = super_block_rows( sp, k );
+        const double * tk = tbuf + sp.t + (std::int64_t)(kPanel * k) * kSuperRows + kPanel * j;
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 )
+        {
+            const int r = idx >> 6, c = idx & 63;
+            A[r][c] = (r < nbi && c < nbk) ? static_cast<double>( U0[(std::int64_t)(sp.r0 + kPanel * i + r) * sp.ld0 + sp.r0 + kPanel * k + c] ) : 0.0;
+            Bm[r][c] = (r < nbk && c < nbj) ? tk[r * kSuperRows + c] : 0.0;
+        }
+        __syncthreads();
+        block_product_64( acc, [&]( int r, int c ) { return A[r][c]; }, [&]( int r, int c ) { return Bm[r][c]; } );
+        __syncthreads();
+    }
+#pragma unroll
+    for( int ct = 0; ct < 8; ++ct )
+    {
+        S[8 * warp + (lane >> 2)][8 * ct + 2 * (lane & 3)] = acc[ct][0];
+        S[8 * warp + (lane >> 2)][8 * ct + 2 * (lane & 3) + 1] = acc[ct][1];
+        acc[ct][0] = 0.0; acc[ct][1] = 0.0;
+    }
+    load_tinv( Tii, i, nbi );
+    __syncthreads();
+    block_product_64( acc, [&]( int r, int c ) { return Tii[r][c]; }, [&]( int r, int c ) { return S[r][c]; } );
+#pragma unroll
+    for( int ct = 0; ct < 8; ++ct )
+    {
+        const int r = 8 * warp + (lane >> 2), c = 8 * ct + 2 * (lane & 3);
+        out[r * kSuperRows + c] = -acc[ct][0];
+        out[r * kSuperRows + c + 1] = -acc[ct][1];
+    }
+}
+
+// Diag step of a super-panel: forward x_o = sum_{i<=o} T_io^T y_i (y: `in`,
+// x written to `out`); back x_o = sum_{j>=o} T_oj (y_j + z_j) (y: `in`, z: the
+// rest launch's sums in `zbuf`; x written to `out`).  KP = k rounded up to a
+// power of two >= 8; T blocks and vectors staged in shared memory.
+template<int KP>
+__global__ __launch_bounds__(256) void super_diag_kernel( const SuperSolveTask * __restrict__ tasks, const SuperPanel * __restrict__ sps,
+                                                          const double * __restrict__ tbuf, int upper, const double * in,
+                                                          const double * zbuf, double * out, int ld, int k )
+{
+    extern __shared__ __align__(16) double dsm[];
+    pdl_allow_next();
+    const SuperSolveTask task = tasks[blockIdx.x];
+    const SuperPanel sp = sps[task.sp];
+    constexpr int nct = KP / 8;
+    constexpr int ldv = KP + 4;
+    double (*Tb)[kSld] = reinterpret_cast<double (*)[kSld]>( dsm );
+    double * V = dsm + kPanel * kSld;                  // [64][ldv]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int o = task.blk;
+    const int nblk = (sp.rows + kPanel - 1) / kPanel;
+    const std::int64_t brow = (std::int64_t)sp.row0 + sp.r0;
+    pdl_wait();
+    double acc[nct][2];
+#pragma unroll
+    for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+    const int b0 = upper ? o : 0, b1 = upper ? nblk : o + 1;
+    for( int b = b0; b < b1; ++b )
+    {
+        const int nbb = super_block_rows( sp, b );
+        // forward: block (b, o) of T, read transposed; back: block (o, b)
+        const double * tb = upper ? tbuf + sp.t + (std::int64_t)(kPanel * o) * kSuperRows + kPanel * b
+                                  : tbuf + sp.t + (std::int64_t)(kPanel * b) * kSuperRows + kPanel * o;
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { Tb[idx >> 6][idx & 63] = tb[(idx >> 6) * kSuperRows + (idx & 63)]; }
+        for( int idx = tid; idx < kPanel * KP; idx += 256 )
+        {
+            const int r = idx / KP, c = idx % KP;
+            double v = 0.0;
+            if( r < nbb && c < k )
+            {
+                const std::int64_t row = brow + kPanel * b + r;
+                v = in[row * ld + c];
+                if( upper ) { v += zbuf[row * ld + c]; }
+            }
+            V[r * ldv + c] = v;
+        }
+        __syncthreads();
+        for( int kb = 0; kb < kSubs; ++kb )
+        {
+#pragma unroll
+            for( int ct = 0; ct < nct; ++ct )
+            {
+                if( upper ) { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return Tb[8 * warp + i][8 * kb + kk]; },
+                                                   [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
+                else        { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return Tb[8 * kb + kk][8 * warp + i]; },
+                                                   [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
+            }
+        }
+        __syncthreads();
+    }
+    const int nbo = super_block_rows( sp, o );
+    const int r = 8 * warp + (lane >> 2);
+    if( r < nbo )
+    {
+        double * dst = out + (brow + kPanel * o + r) * ld;
+#pragma unroll
+        for( int ct = 0; ct < nct; ++ct )
+        {
+            const int c = 8 * ct + 2 * (lane & 3);
+            if( c < k ) { dst[c] = acc[ct][0]; }
+            if( c + 1 < k ) { dst[c + 1] = acc[ct][1]; }
+        }
+    }
+}
+
+// Rest step of a super-panel over rest rows [c0, c1).  Forward: y_rest -=
+// sum_b U_{b,rest}^T x_b (x: `out` rows of the block; own rest rows of `in`
+// plain, ancestor rows by atomics).  Back: z_b -= U_{b,rest} x_rest for every
+// block b (x_rest: `out`, final; z: atomics into `zbuf`).
+template<typename T, int KP>
+__global__ __launch_bounds__(256) void super_rest_kernel( const SuperSolveTask * __restrict__ tasks, const SuperPanel * __restrict__ sps,
+                                                          const T * __restrict__ arena, const std::int32_t * __restrict__ sn_inner,
+                                                          int upper, double * in, double * zbuf, const double * out, int ld, int k )
+{
+    extern __shared__ __align__(16) double rsm[];
+    pdl_allow_next();
+    const SuperSolveTask task = tasks[blockIdx.x];
+    const SuperPanel sp = sps[task.sp];
+    constexpr int nct = KP / 8;
+    constexpr int ldv = KP + 4;
+    __shared__ std::int64_t trow[kSolveRest];
+    double (*P)[kSld] = reinterpret_cast<double (*)[kSld]>( rsm );
+    double * V = rsm + kPanel * kSld;                   // [64][ldv]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r1 = sp.r0 + sp.rows;
+    const int m = sp.n0 - r1;
+    const int cw = task.c1 - task.c0;
+    const int nblk = (sp.rows + kPanel - 1) / kPanel;
+    const std::int64_t brow = (std::int64_t)sp.row0 + sp.r0;
+    if( tid < kSolveRest )
+    {
+        const int col = task.c0 + tid;
+        trow[tid] = (tid < cw) ? ((col < m) ? (std::int64_t)sp.row0 + r1 + col : (std::int64_t)sn_inner[sp.inner + (col - m)]) : -1;
+    }
+    const T * U0 = arena + sp.u0;
+    const T * U1 = arena + sp.u1;
+    pdl_wait();
+    __syncthreads();
+    double acc[nct][2];
+#pragma unroll
+    for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
+    if( upper )
+    {
+        // x_rest into shared memory once
+        for( int idx = tid; idx < kPanel * KP; idx += 256 )
+        {
+            const int r = idx / KP, c = idx % KP;
+            V[r * ldv + c] = (r < cw && c < k) ? out[trow[r] * ld + c] : 0.0;
+        }
+    }
+    for( int b = 0; b < nblk; ++b )
+    {
+        const int nbb = super_block_rows( sp, b );
+        // P: rows of block b (U rows r0 + 64 b + rr), the chunk's rest columns
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 )
+        {
+            const int rr = idx >> 6, jj = idx & 63;
+            const int col = task.c0 + jj;
+            const std::int64_t urow = sp.r0 + kPanel * b + rr;
+            double v = 0.0;
+            if( rr < nbb && jj < cw )
+            {
+                v = static_cast<double>( col < m ? U0[urow * sp.ld0 + r1 + col] : U1[urow * sp.ld1 + (col - m)] );
+            }
+            P[rr][jj] = v;
+        }
+        if( !upper )
+        {
+            for( int idx = tid; idx < kPanel * KP; idx += 256 )
+            {
+                const int r = idx / KP, c = idx % KP;
+                V[r * ldv + c] = (r < nbb && c < k) ? out[(brow + kPanel * b + r) * ld + c] : 0.0;
+            }
+        }
+        __syncthreads();
+        if( !upper )
+        {
+            // acc(jj, c) += sum_rr P[rr][jj] x_b[rr][c]
+            for( int kb = 0; kb < kSubs; ++kb )
+            {
+#pragma unroll
+                for( int ct = 0; ct < nct; ++ct )
+                {
+                    dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return P[8 * kb + kk][8 * warp + i]; },
+                                         [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } );
+                }
+            }
+        }
+        else
+        {
+            // z_b(rr, c) -= sum_jj P[rr][jj] x_rest[jj][c]
+            double zb[nct][2];
+#pragma unroll
+            for( int ct = 0; ct < nct; ++ct ) { zb[ct][0] = 0.0; zb[ct][1] = 0.0; }
+            for( int kb = 0; kb < kSubs; ++kb )
+            {
+#pragma unroll
+                for( int ct = 0; ct < nct; ++ct )
+                {
+                    dmma_8x8x8( zb[ct], [&]( int i, int kk ) { return P[8 * warp + i][8 * kb + kk]; },
+                                        [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } );
+                }
+            }
+            const int rr = 8 * warp + (lane >> 2);
+            if( rr < nbb )
+            {
+                double * dst = zbuf + (brow + kPanel * b + rr) * ld;
+#pragma unroll
+                for( int ct = 0; ct < nct; ++ct )
+                {
+                    const int c = 8 * ct + 2 * (lane & 3);
+                    if( c < k ) { atomicAdd( dst + c, -zb[ct][0] ); }
+                    if( c + 1 < k ) { atomicAdd( dst + c + 1, -zb[ct][1] ); }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if( !upper )
+    {
+        const int jj = 8 * warp + (lane >> 2);
+        if( jj < cw )
+        {
+            double * dst = in + trow[jj] * ld;
+            const bool own = task.c0 + jj < m;
+#pragma unroll
+            for( int ct = 0; ct < nct; ++ct )
+            {
+#pragma unroll
+                for( int e = 0; e < 2; ++e )
+                {
+                    const int c = 8 * ct + 2 * (lane & 3) + e;
+                    if( c < k ) { if( own ) { dst[c] -= acc[ct][e]; } else { atomicAdd( dst + c, -acc[ct][e] ); } }
+                }
+            }
+        }
+    }
+}
+
 } // namespace
 
 template<typename T>
@@ -1909,6 +2218,50 @@ void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, cons
 }
 
 template<typename T>
+void launch_super_inv( const SuperInvTask * tasks, int count, const SuperPanel * sps, const T * arena, const double * tinv,
+                       double * tbuf, cudaStream_t st )
+{
+    if( count > 0 ) { launch_pdl( super_inv_kernel<T>, count, 256, kSuperInvSmem, st, tasks, sps, arena, tinv, tbuf ); }
+}
+
+static size_t super_solve_smem( int k )
+{
+    return sizeof(double) * (kPanel * kSld + kPanel * ((1 << solve_lkp( k )) + 4));
+}
+
+void launch_super_diag( const SuperSolveTask * tasks, int count, const SuperPanel * sps, const double * tbuf, bool upper,
+                        const double * in, const double * zbuf, double * out, int ld, int k, cudaStream_t st )
+{
+    if( count <= 0 ) { return; }
+    const size_t sm = super_solve_smem( k );
+    const int u = upper ? 1 : 0;
+    switch( solve_lkp( k ) )
+    {
+        case 3:  launch_pdl( super_diag_kernel<8>, count, 256, sm, st, tasks, sps, tbuf, u, in, zbuf, out, ld, k ); break;
+        case 4:  launch_pdl( super_diag_kernel<16>, count, 256, sm, st, tasks, sps, tbuf, u, in, zbuf, out, ld, k ); break;
+        case 5:  launch_pdl( super_diag_kernel<32>, count, 256, sm, st, tasks, sps, tbuf, u, in, zbuf, out, ld, k ); break;
+        default: launch_pdl( super_diag_kernel<64>, count, 256, sm, st, tasks, sps, tbuf, u, in, zbuf, out, ld, k ); break;
+    }
+}
+
+template<typename T>
+void launch_super_rest( const SuperSolveTask * tasks, int count, const SuperPanel * sps, const T * arena,
+                        const std::int32_t * sn_inner, bool upper, double * in, double * zbuf, const double * out, int ld, int k,
+                        cudaStream_t st )
+{
+    if( count <= 0 ) { return; }
+    const size_t sm = super_solve_smem( k );
+    const int u = upper ? 1 : 0;
+    switch( solve_lkp( k ) )
+    {
+        case 3:  launch_pdl( super_rest_kernel<T, 8>, count, 256, sm, st, tasks, sps, arena, sn_inner, u, in, zbuf, out, ld, k ); break;
+        case 4:  launch_pdl( super_rest_kernel<T, 16>, count, 256, sm, st, tasks, sps, arena, sn_inner, u, in, zbuf, out, ld, k ); break;
+        case 5:  launch_pdl( super_rest_kernel<T, 32>, count, 256, sm, st, tasks, sps, arena, sn_inner, u, in, zbuf, out, ld, k ); break;
+        default: launch_pdl( super_rest_kernel<T, 64>, count, 256, sm, st, tasks, sps, arena, sn_inner, u, in, zbuf, out, ld, k ); break;
+    }
+}
+
+template<typename T>
 void launch_gather_diag( const std::int64_t * offsets, const T * arena, double * out, int n, cudaStream_t st )
 {
     gather_diag_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( offsets, arena, out, n );
@@ -1928,7 +2281,12 @@ void launch_gather_diag( const std::int64_t * offsets, const T * arena, double *
     template void launch_factor_dag<T>( const DagArgs &, int, cudaStream_t );                                        \
     template void launch_solve_step<T>( const SolveRestTask *, int, bool, const T *, const double *,                \
                                         const std::int32_t *, double *, double *, int, int, cudaStream_t );         \
-    template void launch_gather_diag<T>( const std::int64_t *, const T *, double *, int, cudaStream_t );
+    template void launch_gather_diag<T>( const std::int64_t *, const T *, double *, int, cudaStream_t );          \
+    template void launch_super_inv<T>( const SuperInvTask *, int, const SuperPanel *, const T *, const double *,      \
+                                       double *, cudaStream_t );                                                    \
+    template void launch_super_rest<T>( const SuperSolveTask *, int, const SuperPanel *, const T *,                 \
+                                        const std::int32_t *, bool, double *, double *, const double *, int, int,   \
+                                        cudaStream_t );
 TB_INSTANTIATE( double )
 TB_INSTANTIATE( float )
 #undef TB_INSTANTIATE
@@ -1978,6 +2336,20 @@ cudaError_t configure_kernels()
         { reinterpret_cast<const void *>( solve_dag_kernel<float, 16> ), solve_smem_bytes( 16 ) },
         { reinterpret_cast<const void *>( solve_dag_kernel<float, 32> ), solve_smem_bytes( 32 ) },
         { reinterpret_cast<const void *>( solve_dag_kernel<float, 64> ), solve_smem_bytes( 64 ) },
+        { reinterpret_cast<const void *>( super_inv_kernel<double> ), kSuperInvSmem },
+        { reinterpret_cast<const void *>( super_inv_kernel<float> ), kSuperInvSmem },
+        { reinterpret_cast<const void *>( super_diag_kernel<8> ), super_solve_smem( 8 ) },
+        { reinterpret_cast<const void *>( super_diag_kernel<16> ), super_solve_smem( 16 ) },
+        { reinterpret_cast<const void *>( super_diag_kernel<32> ), super_solve_smem( 32 ) },
+        { reinterpret_cast<const void *>( super_diag_kernel<64> ), super_solve_smem( 64 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 8> ), super_solve_smem( 8 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 16> ), super_solve_smem( 16 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 32> ), super_solve_smem( 32 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 64> ), super_solve_smem( 64 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 8> ), super_solve_smem( 8 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 16> ), super_solve_smem( 16 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 32> ), super_solve_smem( 32 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 64> ), super_solve_smem( 64 ) },
     };
     for( const auto & a : attrs )
     {

@@ -122,6 +122,20 @@ void launch_solve_dag( const SolveDagArgs & args, int grid, const T * arena, dou
 // Resident CTAs per SM of the persistent solve kernel for k right-hand sides (0 on error).
 int solve_dag_blocks_per_sm( int k );
 
+// Super-panel solve (plan.hpp, SuperPanel): the inverses' round launches
+// (after the factorization; tbuf: Plan::super_inv_size doubles), and the diag
+// and rest steps of the sweeps (zbuf: n x ld doubles, zero before the back
+// sweep; in / out as launch_solve_step's).
+template<typename T>
+void launch_super_inv( const SuperInvTask * tasks, int count, const SuperPanel * sps, const T * arena, const double * tinv,
+                       double * tbuf, cudaStream_t st );
+void launch_super_diag( const SuperSolveTask * tasks, int count, const SuperPanel * sps, const double * tbuf, bool upper,
+                        const double * in, const double * zbuf, double * out, int ld, int k, cudaStream_t st );
+template<typename T>
+void launch_super_rest( const SuperSolveTask * tasks, int count, const SuperPanel * sps, const T * arena,
+                        const std::int32_t * sn_inner, bool upper, double * in, double * zbuf, const double * out, int ld, int k,
+                        cudaStream_t st );
+
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
                          int n, int k, cudaStream_t st );
 void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv, double alpha, double beta,

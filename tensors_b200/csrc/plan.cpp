@@ -408,6 +408,7 @@ void Plan::build( const Symbolic & sym )
 
     struct Range { I64 first; I32 count; };
     std::vector<std::vector<Range>> rest_ranges( static_cast<size_t>(levels) );
+    std::vector<std::vector<I32>> front_panels( static_cast<size_t>(F) );   // sdiag index of each panel, in step order
 
     // Dependency counters of the task graph (see DagTask): per level the
     // finished extend-add tasks, per front the extend-adds received and
@@ -669,6 +670,7 @@ void Plan::build( const Symbolic & sym )
                         srest.push_back( t );
                     }
                 }
+                front_panels[static_cast<size_t>( f )].push_back( static_cast<I32>( sdiag.size() ) );
                 sdiag.push_back( { front_u0[f], n0, r0, front_row0[f], ld0 } );
             }
             // tiles of the step: next-row tiles first, each group by K descending
@@ -820,7 +822,143 @@ void Plan::build( const Symbolic & sym )
     I32 solve_split = levels;
     for( I32 h = 0; h < levels; ++h ) { if( level_steps[static_cast<size_t>(h)] >= kSolveDagMinSteps ) { solve_split = h; break; } }
     solve_default_split = solve_split;
+    build_super( front_panels, [&]( I32 h, size_t q ) { return std::make_pair( rest_ranges[static_cast<size_t>(h)][q].first,
+                                                                              rest_ranges[static_cast<size_t>(h)][q].count ); },
+                 [&]( I32 h ) { return rest_ranges[static_cast<size_t>(h)].size(); }, by_level );
     build_solve_graph( sym, solve_split );
+}
+
+// The super-panel solve: super-panels of the large fronts, the rounds of their
+// inverses, and the solve launch lists in which their panel steps are replaced.
+// Within each (level, step) range of srest the tasks of the large fronts are
+// moved behind the others (the order inside a range is free: its tasks are
+// independent, and each panel keeps its own tasks' order), so the step
+// launches of the super-panel lists cover the range's leading part.
+template<typename RangeOf, typename RangeCount>
+void Plan::build_super( const std::vector<std::vector<I32>> & front_panels, RangeOf range_of, RangeCount ranges,
+                        const std::vector<std::vector<I32>> & by_level )
+{
+    spanels.clear(); sinv.clear(); sinv_launches.clear(); ssolve.clear();
+    lower_launches_sp.clear(); upper_launches_sp.clear();
+    super_inv_size = 0;
+    const I32 F = front_count;
+    std::vector<char> big( static_cast<size_t>(F), 0 );
+    std::vector<std::vector<I32>> front_sp( static_cast<size_t>(F) );
+    if( use_super )
+    {
+        for( I32 f = 0; f < F; ++f ) { big[static_cast<size_t>(f)] = front_n0[f] >= kSuperMinRows ? 1 : 0; }
+    }
+    for( I32 f = 0; f < F; ++f )
+    {
+        if( !big[static_cast<size_t>(f)] ) { continue; }
+        const std::vector<I32> & pan = front_panels[static_cast<size_t>(f)];
+        for( I32 r0 = 0; r0 < front_n0[f]; r0 += kSuperRows )
+        {
+            SuperPanel sp{};
+            sp.u0 = front_u0[f]; sp.u1 = front_u1[f]; sp.inner = front_cols[f];
+            sp.t = super_inv_size;
+            sp.n0 = front_n0[f]; sp.n1 = front_n1[f]; sp.ld0 = front_ld0[f]; sp.ld1 = front_ld1[f];
+            sp.r0 = r0; sp.rows = std::min( kSuperRows, front_n0[f] - r0 ); sp.row0 = front_row0[f];
+            for( I32 b = 0; b < kSuperPanels; ++b )
+            {
+                const size_t q = static_cast<size_t>( r0 / kPanel + b );
+                sp.panel[b] = (b * kPanel < sp.rows && q < pan.size()) ? pan[q] : -1;
+            }
+            front_sp[static_cast<size_t>(f)].push_back( static_cast<I32>( spanels.size() ) );
+            spanels.push_back( sp );
+            super_inv_size += static_cast<I64>( kSuperRows ) * kSuperRows;
+        }
+    }
+    if( spanels.empty() ) { return; }
+    // the inverses: round d forms the blocks at distance d from the diagonal
+    for( I32 d = 0; d < kSuperPanels; ++d )
+    {
+        const I64 first = static_cast<I64>( sinv.size() );
+        for( I32 p = 0; p < static_cast<I32>( spanels.size() ); ++p )
+        {
+            const I32 nblk = static_cast<I32>( ceil_div( spanels[static_cast<size_t>(p)].rows, kPanel ) );
+            for( I32 i = 0; i + d < nblk; ++i ) { sinv.push_back( { p, i, i + d, 0 } ); }
+        }
+        const I32 count = static_cast<I32>( static_cast<I64>( sinv.size() ) - first );
+        if( count > 0 ) { sinv_launches.push_back( { LaunchKind::SuperInv, count, first, levels, d } ); }
+    }
+    // srest ranges: the large fronts' tasks last
+    // (a task's front is large exactly when its n0 is: the criterion is the front's pivot-row count)
+    auto is_big_task = [&]( const SolveRestTask & t ) { return use_super && t.n0 >= kSuperMinRows; };
+    std::vector<std::vector<I32>> regular( static_cast<size_t>(levels) );
+    for( I32 h = 0; h < levels; ++h )
+    {
+        for( size_t q = 0; q < ranges( h ); ++q )
+        {
+            const auto r = range_of( h, q );
+            auto b = srest.begin() + r.first, e = b + r.second;
+            std::stable_partition( b, e, [&]( const SolveRestTask & t ) { return !is_big_task( t ); } );
+            I32 nreg = 0;
+            for( auto it = b; it != e; ++it ) { nreg += is_big_task( *it ) ? 0 : 1; }
+            regular[static_cast<size_t>(h)].push_back( nreg );
+        }
+    }
+    // per level: the step launches of the other fronts, then the super-panel steps
+    auto super_steps = [&]( I32 h ) {
+        size_t m = 0;
+        for( I32 f : by_level[static_cast<size_t>(h)] ) { m = std::max( m, front_sp[static_cast<size_t>(f)].size() ); }
+        return m;
+    };
+    auto push_super = [&]( std::vector<Launch> & list, I32 h, size_t s, bool diag, bool forward )
+    {
+        const I64 first = static_cast<I64>( ssolve.size() );
+        for( I32 f : by_level[static_cast<size_t>(h)] )
+        {
+            const std::vector<I32> & v = front_sp[static_cast<size_t>(f)];
+            if( s >= v.size() ) { continue; }
+            const I32 p = v[s];
+            const SuperPanel & sp = spanels[static_cast<size_t>(p)];
+            if( diag )
+            {
+                for( I32 o = 0; o * kPanel < sp.rows; ++o ) { ssolve.push_back( { p, o, 0, 0 } ); }
+            }
+            else
+            {
+                const I32 rest = (sp.n0 - sp.r0 - sp.rows) + sp.n1;
+                for( I32 c0 = 0; c0 < rest; c0 += kSolveRest ) { ssolve.push_back( { p, 0, c0, std::min( rest, c0 + kSolveRest ) } ); }
+            }
+        }
+        const I32 count = static_cast<I32>( static_cast<I64>( ssolve.size() ) - first );
+        if( count > 0 )
+        {
+            Launch L{ diag ? LaunchKind::SuperDiag : LaunchKind::SuperRest, count, first, h, static_cast<I32>( s ) };
+            L.part = forward ? 0 : 1;
+            list.push_back( L );
+        }
+    };
+    for( I32 h = 0; h < levels; ++h )
+    {
+        for( size_t q = 0; q < ranges( h ); ++q )
+        {
+            const auto r = range_of( h, q );
+            const I32 nreg = regular[static_cast<size_t>(h)][q];
+            if( nreg > 0 ) { lower_launches_sp.push_back( { LaunchKind::Solve, nreg, r.first, h, static_cast<I32>(q) } ); }
+        }
+        for( size_t st = 0; st < super_steps( h ); ++st )
+        {
+            push_super( lower_launches_sp, h, st, true, true );
+            push_super( lower_launches_sp, h, st, false, true );
+        }
+    }
+    for( I32 h = levels; h-- > 0; )
+    {
+        for( size_t st = super_steps( h ); st-- > 0; )
+        {
+            push_super( upper_launches_sp, h, st, false, false );
+            push_super( upper_launches_sp, h, st, true, false );
+        }
+        for( size_t q = ranges( h ); q-- > 0; )
+        {
+            const auto r = range_of( h, q );
+            const I32 nreg = regular[static_cast<size_t>(h)][q];
+            if( nreg > 0 ) { upper_launches_sp.push_back( { LaunchKind::Solve, nreg, r.first, h, static_cast<I32>(q) } ); }
+        }
+    }
 }
 
 void Plan::build_solve_graph( const Symbolic & sym, I32 split )

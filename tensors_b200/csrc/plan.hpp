@@ -205,7 +205,46 @@ struct DagTask
     std::int32_t target[kDagWaits];
 };
 
-enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, Invert = 4, Solve = 5, Potrf = 6 };
+enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, Invert = 4, Solve = 5, Potrf = 6,
+                                       SuperInv = 8, SuperDiag = 9, SuperRest = 10 };
+
+// The solve of a large front steps through its pivot rows 512 at a time
+// (super-panels) instead of 64 at a time: the inverse of each 512 x 512
+// diagonal block of U0 (T, FP64, upper triangular, row-major, built from
+// the 64-row panel inverses after the factorization by block back
+// substitution) turns eight sequential panel steps into one.  A front uses
+// super-panels when it has at least kSuperMinRows pivot rows.
+constexpr int kSuperPanels  = 8;
+constexpr int kSuperRows    = kSuperPanels * kPanel;   // 512
+constexpr int kSuperMinRows = 1024;
+
+struct SuperPanel
+{
+    std::int64_t u0, u1, inner;    // the front's U0 / U1 arena offsets and its SN_inner offset
+    std::int64_t t;                // offset of the inverse (kSuperRows x kSuperRows doubles)
+    std::int32_t n0, n1, ld0, ld1;
+    std::int32_t r0, rows;         // first pivot row of the block (a multiple of 512) and its row count
+    std::int32_t row0;             // the front's first global row
+    std::int32_t panel[kSuperPanels];   // inverse-block index of each 64-row panel (-1 beyond rows)
+    std::int32_t pad;
+};
+
+// Block (i, j = i + d) of a super-panel's inverse, formed in round d:
+// d = 0 copies panel i's inverse; d > 0: T_ij = -T_ii sum_{k=i+1..j} U_ik T_kj.
+struct SuperInvTask
+{
+    std::int32_t sp, i, j, pad;
+};
+
+// A super-panel solve task.  Diag: output block `blk` (64 rows) of the
+// block's solution, x_blk = sum_{i<=blk} T_{i,blk}^T y_i (forward) or
+// sum_{j>=blk} T_{blk,j} (y_j + z_j) (back).  Rest: rest rows [c0, c1) of the
+// front after the block (U0 rows, then its U1 columns): forward y_rest -=
+// U_{block,rest}^T x_block; back z_block -= U_{block,rest} x_rest.
+struct SuperSolveTask
+{
+    std::int32_t sp, blk, c0, c1;
+};
 
 // One launch: `count` tasks starting at `first` in the array of its kind.
 // A panel step's GEMM tiles come as two launches: part 0 updates the next
@@ -289,6 +328,19 @@ struct Plan
     std::vector<Launch> lower_launches;     // forward solve U^T y = b
     std::vector<Launch> upper_launches;     // back solve U x = y
 
+    // Super-panel solve (see SuperPanel): the launch lists with the large
+    // fronts' panel steps replaced by super-panel steps (per level: the other
+    // fronts' step launches, then per super-panel step a diag and a rest
+    // launch); the inverses are formed by the launches of sinv_launches after
+    // the factorization.  Empty lists: no front is large enough.
+    bool use_super = true;                  // set before build(): false keeps every front on panel steps
+    std::vector<SuperPanel> spanels;
+    std::vector<SuperInvTask> sinv;
+    std::vector<Launch> sinv_launches;
+    std::vector<SuperSolveTask> ssolve;
+    std::vector<Launch> lower_launches_sp, upper_launches_sp;
+    std::int64_t super_inv_size = 0;        // doubles of all inverses
+
     // Solve task graph: the levels from solve_split_level up run as one
     // persistent launch per sweep, the levels below as the launches above.
     // A graph task is an srest task; its targets are the panels its rest
@@ -318,6 +370,9 @@ struct Plan
     std::int64_t arena_size() const { return u0_size + u1_size + v_size; }
 
     void build( const Symbolic & sym );
+    template<typename RangeOf, typename RangeCount>
+    void build_super( const std::vector<std::vector<std::int32_t>> & front_panels, RangeOf range_of, RangeCount ranges,
+                      const std::vector<std::vector<std::int32_t>> & by_level );
     // Fills the solve task graph for the levels from `split` up (levels: none).
     void build_solve_graph( const Symbolic & sym, std::int32_t split );
 };

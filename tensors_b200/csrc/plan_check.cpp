@@ -395,6 +395,98 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
     }
     for( const Launch & L : pl.lower_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the forward solve"; } }
     for( const Launch & L : pl.upper_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the back solve"; } }
+    if( !pl.spanels.empty() )
+    {
+        // super-panels: blocks inside their fronts and the arena, inverses inside their buffer, the
+        // panel inverses they start from belong to their rows
+        const I64 nsp = static_cast<I64>( pl.spanels.size() );
+        std::vector<I32> nblk( static_cast<size_t>( nsp ) ), nrest( static_cast<size_t>( nsp ) );
+        for( I64 p = 0; p < nsp; ++p )
+        {
+            const SuperPanel & sp = pl.spanels[static_cast<size_t>( p )];
+            const std::string at = " (super-panel " + std::to_string( p ) + ")";
+            if( sp.rows <= 0 || sp.rows > kSuperRows || sp.r0 < 0 || sp.r0 % kSuperRows != 0 || sp.r0 + sp.rows > sp.n0 ) { return "bad super-panel rows" + at; }
+            if( sp.ld0 < sp.n0 || sp.ld1 < sp.n1 || sp.n1 < 0 ) { return "bad super-panel dimensions" + at; }
+            if( !in_range( sp.u0, sp.u0 + static_cast<I64>( sp.n0 ) * sp.ld0 - 1, arena ) ) { return "super-panel U0 out of range" + at; }
+            if( sp.n1 > 0 && !in_range( sp.u1, sp.u1 + static_cast<I64>( sp.n0 ) * sp.ld1 - 1, arena ) ) { return "super-panel U1 out of range" + at; }
+            if( sp.n1 > 0 && (sp.inner < 0 || sp.inner + sp.n1 > inner_size) ) { return "super-panel columns out of range" + at; }
+            if( sp.row0 < 0 || sp.row0 + sp.n0 > sym.n ) { return "super-panel rows out of the matrix" + at; }
+            if( sp.t < 0 || sp.t + static_cast<I64>( kSuperRows ) * kSuperRows > pl.super_inv_size ) { return "super-panel inverse out of range" + at; }
+            nblk[static_cast<size_t>( p )] = (sp.rows + kPanel - 1) / kPanel;
+            nrest[static_cast<size_t>( p )] = (sp.n0 - sp.r0 - sp.rows) + sp.n1;
+            for( I32 b = 0; b < kSuperPanels; ++b )
+            {
+                if( b < nblk[static_cast<size_t>( p )] )
+                {
+                    const I32 q = sp.panel[b];
+                    if( q < 0 || q >= static_cast<I32>( pl.sdiag.size() ) ) { return "super-panel panel out of range" + at; }
+                    const SolveDiagTask & d = pl.sdiag[static_cast<size_t>( q )];
+                    if( d.u0 != sp.u0 || d.r0 != sp.r0 + b * kPanel || d.n0 != sp.n0 ) { return "super-panel panel mismatch" + at; }
+                }
+                else if( sp.panel[b] != -1 ) { return "super-panel panel beyond its rows" + at; }
+            }
+        }
+        for( size_t t = 0; t < pl.sinv.size(); ++t )
+        {
+            const SuperInvTask & v = pl.sinv[t];
+            if( v.sp < 0 || v.sp >= nsp || v.i < 0 || v.j < v.i || v.j >= nblk[static_cast<size_t>( v.sp )] ) { return "super-panel inverse task out of range"; }
+        }
+        for( const Launch & L : pl.sinv_launches )
+        {
+            if( L.kind != LaunchKind::SuperInv || L.count <= 0 || L.first < 0 || L.first + L.count > static_cast<I64>( pl.sinv.size() ) )
+            {
+                return "super-panel inverse launch out of bounds";
+            }
+            for( I64 t = L.first; t < L.first + L.count; ++t ) { if( pl.sinv[static_cast<size_t>( t )].j - pl.sinv[static_cast<size_t>( t )].i != L.step ) { return "super-panel inverse round mismatch"; } }
+        }
+        // each sweep: every other front's tasks once, every super-panel's diag blocks and rest rows once
+        for( const std::vector<Launch> * list : { &pl.lower_launches_sp, &pl.upper_launches_sp } )
+        {
+            I64 regular = 0;
+            std::vector<I64> diag( static_cast<size_t>( nsp ), 0 ), rest( static_cast<size_t>( nsp ), 0 );
+            for( const Launch & L : *list )
+            {
+                if( L.kind == LaunchKind::Solve )
+                {
+                    if( L.count <= 0 || L.first < 0 || L.first + L.count > static_cast<I64>( pl.srest.size() ) ) { return "super solve list: step launch out of bounds"; }
+                    for( I64 t = L.first; t < L.first + L.count; ++t ) { if( pl.srest[static_cast<size_t>( t )].n0 >= kSuperMinRows ) { return "super solve list: a large front's panel step"; } }
+                    regular += L.count;
+                    continue;
+                }
+                if( (L.kind != LaunchKind::SuperDiag && L.kind != LaunchKind::SuperRest) || L.count <= 0 || L.first < 0
+                    || L.first + L.count > static_cast<I64>( pl.ssolve.size() ) )
+                {
+                    return "super solve list: launch out of bounds";
+                }
+                for( I64 t = L.first; t < L.first + L.count; ++t )
+                {
+                    const SuperSolveTask & v = pl.ssolve[static_cast<size_t>( t )];
+                    if( v.sp < 0 || v.sp >= nsp ) { return "super solve task out of range"; }
+                    const size_t p = static_cast<size_t>( v.sp );
+                    if( L.kind == LaunchKind::SuperDiag )
+                    {
+                        if( v.blk < 0 || v.blk >= nblk[p] ) { return "super solve diag block out of range"; }
+                        ++diag[p];
+                    }
+                    else
+                    {
+                        if( v.c0 < 0 || v.c1 > nrest[p] || v.c0 >= v.c1 || v.c1 - v.c0 > kSolveRest ) { return "super solve rest rows out of range"; }
+                        rest[p] += v.c1 - v.c0;
+                    }
+                }
+            }
+            I64 small = 0;
+            for( const SolveRestTask & t : pl.srest ) { small += t.n0 >= kSuperMinRows ? 0 : 1; }
+            if( regular != small ) { return "super solve list: the other fronts' steps are not covered once"; }
+            for( I64 p = 0; p < nsp; ++p )
+            {
+                if( diag[static_cast<size_t>( p )] != nblk[static_cast<size_t>( p )] || rest[static_cast<size_t>( p )] != nrest[static_cast<size_t>( p )] )
+                {
+                    return "super solve list: super-panel " + std::to_string( p ) + " not covered once";
+                }
+            }
+        }
+    }
     {
         // solve task graph: sizes, ranges, and deadlock freedom: in the forward
         // list every task that updates a panel's rows comes before the panel's
