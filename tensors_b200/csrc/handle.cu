@@ -789,6 +789,8 @@ std::int64_t issue_sweeps( tb_chol * h, int which, double * W, double * Y, std::
     if( which != 1 )
     {
         tb::TraceRange range( "Sparse::CholeskyDecomposition::SN_LowerSolve" );
+        // the super-panels' diag steps add their block pairs into zeroed rows
+        if( super ) { cudaMemsetAsync( Y, 0, sizeof(double) * static_cast<size_t>( h->n ) * k, st ); }
         for( std::int32_t c0 = 0; c0 < k; c0 += tb::kSolveMaxRhs )
         {
             const std::int32_t kc = std::min( tb::kSolveMaxRhs, k - c0 );

@@ -1780,7 +1780,7 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     double (*Tii)[kSld] = S + kPanel;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int i = task.i, j = task.j;
-    const int nbi = super_block_rows( sp, i ), nbj = super_block_rows( sp, j );
+    const int nbi = super_block_rows( sp, i );
     double * out = tbuf + sp.t + (std::int64_t)(kPanel * i) * kSuperRows + kPanel * j;
     auto load_tinv = [&]( double (*D)[kSld], int b, int nbb )
     {
@@ -1806,12 +1806,19 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     {
         const int nbk = super_block_rows( sp, k );
         const double * tk = tbuf + sp.t + (std::int64_t)(kPanel * k) * kSuperRows + kPanel * j;
-        for( int idx = tid; idx < kPanel * kPanel; idx += 256 )
+        auto src = [&]( int idx, double & fill ) -> const T *
         {
+            fill = 0.0;
             const int r = idx >> 6, c = idx & 63;
-            A[r][c] = (r < nbi && c < nbk) ? static_cast<double>( U0[(std::int64_t)(sp.r0 + kPanel * i + r) * sp.ld0 + sp.r0 + kPanel * k + c] ) : 0.0;
-            Bm[r][c] = (r < nbk && c < nbj) ? tk[r * kSuperRows + c] : 0.0;
-        }
+            return (r < nbi && c < nbk) ? U0 + (std::int64_t)(sp.r0 + kPanel * i + r) * sp.ld0 + sp.r0 + kPanel * k + c : nullptr;
+        };
+        auto dst = [&]( int idx ) { return &A[idx >> 6][idx & 63]; };
+        stage_block<T, kPanel * kPanel / 256, 256>( U0, src, dst );
+        // T_kj is zero outside its valid rows and columns
+#pragma unroll 4
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { cp_async_8( &Bm[idx >> 6][idx & 63], tk + (idx >> 6) * kSuperRows + (idx & 63), true ); }
+        cp_async_wait_all();
+        stage_finish<T, kPanel * kPanel / 256, 256>( src, dst );
         __syncthreads();
         block_product_64( acc, [&]( int r, int c ) { return A[r][c]; }, [&]( int r, int c ) { return Bm[r][c]; } );
         __syncthreads();
@@ -1835,10 +1842,28 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     }
 }
 
-// Diag step of a super-panel: forward x_o = sum_{i<=o} T_io^T y_i (y: `in`,
-// x written to `out`); back x_o = sum_{j>=o} T_oj (y_j + z_j) (y: `in`, z: the
-// rest launch's sums in `zbuf`; x written to `out`).  KP = k rounded up to a
-// power of two >= 8; T blocks and vectors staged in shared memory.
+// Stages x rows [row, row + nr) (leading dimension ld, k columns) of a sweep
+// vector into V (64 x KP, leading dimension KP + 4) with 8-byte asynchronous
+// copies; cells outside nr x k are zero.
+template<int KP>
+__device__ __forceinline__ void stage_rows( double * V, const double * x, std::int64_t row, int nr, int ld, int k )
+{
+    constexpr int ldv = KP + 4;
+#pragma unroll 4
+    for( int idx = threadIdx.x; idx < kPanel * KP; idx += 256 )
+    {
+        const int r = idx / KP, c = idx % KP;
+        const bool ok = r < nr && c < k;
+        cp_async_8( V + r * ldv + c, ok ? x + (row + r) * ld + c : x, ok );
+    }
+}
+
+// One block pair of a super-panel's diag step.  Forward (task (o, b), b <= o):
+// x_o += T_bo^T y_b; back (b >= o): x_o += T_ob (y_b + z_b).  y: `in`, z: the
+// rest steps' sums in `zbuf`, x: `out`, whose block rows are zero before the
+// step (the pairs of one block row add into it).  KP = k rounded up to a power
+// of two >= 8.  One 64 x 64 block of T and one 64 x k block of vectors per
+// CTA, all copies in flight together.
 template<int KP>
 __global__ __launch_bounds__(256) void super_diag_kernel( const SuperSolveTask * __restrict__ tasks, const SuperPanel * __restrict__ sps,
                                                           const double * __restrict__ tbuf, int upper, const double * in,
@@ -1852,47 +1877,39 @@ __global__ __launch_bounds__(256) void super_diag_kernel( const SuperSolveTask *
     constexpr int ldv = KP + 4;
     double (*Tb)[kSld] = reinterpret_cast<double (*)[kSld]>( dsm );
     double * V = dsm + kPanel * kSld;                  // [64][ldv]
+    double * Z = V + kPanel * ldv;                     // [64][ldv], back sweep only
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int o = task.blk;
-    const int nblk = (sp.rows + kPanel - 1) / kPanel;
+    const int o = task.blk, b = task.c0;
+    const int nbb = super_block_rows( sp, b );
     const std::int64_t brow = (std::int64_t)sp.row0 + sp.r0;
+    // forward: block (b, o) of T, read transposed; back: block (o, b).  The
+    // blocks are zero outside their valid rows and columns.
+    const double * tb = upper ? tbuf + sp.t + (std::int64_t)(kPanel * o) * kSuperRows + kPanel * b
+                              : tbuf + sp.t + (std::int64_t)(kPanel * b) * kSuperRows + kPanel * o;
+#pragma unroll 4
+    for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { cp_async_8( &Tb[idx >> 6][idx & 63], tb + (idx >> 6) * kSuperRows + (idx & 63), true ); }
     pdl_wait();
+    stage_rows<KP>( V, in, brow + kPanel * b, nbb, ld, k );
+    if( upper ) { stage_rows<KP>( Z, zbuf, brow + kPanel * b, nbb, ld, k ); }
+    cp_async_wait_all();
+    if( upper )
+    {
+        for( int idx = tid; idx < kPanel * KP; idx += 256 ) { V[(idx / KP) * ldv + idx % KP] += Z[(idx / KP) * ldv + idx % KP]; }
+    }
+    __syncthreads();
     double acc[nct][2];
 #pragma unroll
     for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
-    const int b0 = upper ? o : 0, b1 = upper ? nblk : o + 1;
-    for( int b = b0; b < b1; ++b )
+    for( int kb = 0; kb < kSubs; ++kb )
     {
-        const int nbb = super_block_rows( sp, b );
-        // forward: block (b, o) of T, read transposed; back: block (o, b)
-        const double * tb = upper ? tbuf + sp.t + (std::int64_t)(kPanel * o) * kSuperRows + kPanel * b
-                                  : tbuf + sp.t + (std::int64_t)(kPanel * b) * kSuperRows + kPanel * o;
-        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { Tb[idx >> 6][idx & 63] = tb[(idx >> 6) * kSuperRows + (idx & 63)]; }
-        for( int idx = tid; idx < kPanel * KP; idx += 256 )
-        {
-            const int r = idx / KP, c = idx % KP;
-            double v = 0.0;
-            if( r < nbb && c < k )
-            {
-                const std::int64_t row = brow + kPanel * b + r;
-                v = in[row * ld + c];
-                if( upper ) { v += zbuf[row * ld + c]; }
-            }
-            V[r * ldv + c] = v;
-        }
-        __syncthreads();
-        for( int kb = 0; kb < kSubs; ++kb )
-        {
 #pragma unroll
-            for( int ct = 0; ct < nct; ++ct )
-            {
-                if( upper ) { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return Tb[8 * warp + i][8 * kb + kk]; },
-                                                   [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
-                else        { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return Tb[8 * kb + kk][8 * warp + i]; },
-                                                   [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
-            }
+        for( int ct = 0; ct < nct; ++ct )
+        {
+            if( upper ) { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return Tb[8 * warp + i][8 * kb + kk]; },
+                                               [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
+            else        { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return Tb[8 * kb + kk][8 * warp + i]; },
+                                               [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
         }
-        __syncthreads();
     }
     const int nbo = super_block_rows( sp, o );
     const int r = 8 * warp + (lane >> 2);
@@ -1903,16 +1920,17 @@ __global__ __launch_bounds__(256) void super_diag_kernel( const SuperSolveTask *
         for( int ct = 0; ct < nct; ++ct )
         {
             const int c = 8 * ct + 2 * (lane & 3);
-            if( c < k ) { dst[c] = acc[ct][0]; }
-            if( c + 1 < k ) { dst[c + 1] = acc[ct][1]; }
+            if( c < k ) { red_add_f64( dst + c, acc[ct][0] ); }
+            if( c + 1 < k ) { red_add_f64( dst + c + 1, acc[ct][1] ); }
         }
     }
 }
 
-// Rest step of a super-panel over rest rows [c0, c1).  Forward: y_rest -=
-// sum_b U_{b,rest}^T x_b (x: `out` rows of the block; own rest rows of `in`
-// plain, ancestor rows by atomics).  Back: z_b -= U_{b,rest} x_rest for every
-// block b (x_rest: `out`, final; z: atomics into `zbuf`).
+// One (block, rest chunk) pair of a super-panel's rest step, rest columns
+// [c0, c1) of block b.  Forward: y_rest -= U_{b,rest}^T x_b (x_b: `out`, final
+// after the diag step; y: `in`, every row by reductions, as the eight blocks
+// add into the same rows).  Back: z_b -= U_{b,rest} x_rest (x_rest: `out`,
+// final; z: reductions into `zbuf`).
 template<typename T, int KP>
 __global__ __launch_bounds__(256) void super_rest_kernel( const SuperSolveTask * __restrict__ tasks, const SuperPanel * __restrict__ sps,
                                                           const T * __restrict__ arena, const std::int32_t * __restrict__ sn_inner,
@@ -1931,114 +1949,70 @@ __global__ __launch_bounds__(256) void super_rest_kernel( const SuperSolveTask *
     const int r1 = sp.r0 + sp.rows;
     const int m = sp.n0 - r1;
     const int cw = task.c1 - task.c0;
-    const int nblk = (sp.rows + kPanel - 1) / kPanel;
+    const int b = task.blk;
+    const int nbb = super_block_rows( sp, b );
     const std::int64_t brow = (std::int64_t)sp.row0 + sp.r0;
     if( tid < kSolveRest )
     {
         const int col = task.c0 + tid;
         trow[tid] = (tid < cw) ? ((col < m) ? (std::int64_t)sp.row0 + r1 + col : (std::int64_t)sn_inner[sp.inner + (col - m)]) : -1;
     }
+    // P: rows of block b (U rows r0 + 64 b + rr), the chunk's rest columns
     const T * U0 = arena + sp.u0;
     const T * U1 = arena + sp.u1;
+    auto src = [&]( int idx, double & fill ) -> const T *
+    {
+        fill = 0.0;
+        const int rr = idx >> 6, jj = idx & 63;
+        if( rr >= nbb || jj >= cw ) { return nullptr; }
+        const int col = task.c0 + jj;
+        const std::int64_t urow = sp.r0 + kPanel * b + rr;
+        return col < m ? U0 + urow * sp.ld0 + r1 + col : U1 + urow * sp.ld1 + (col - m);
+    };
+    auto dst = [&]( int idx ) { return &P[idx >> 6][idx & 63]; };
+    stage_block<T, kPanel * kPanel / 256, 256>( U0, src, dst );
     pdl_wait();
+    __syncthreads();                                    // trow
+    if( upper )
+    {
+        // x_rest: the chunk's rows of `out`
+#pragma unroll 4
+        for( int idx = tid; idx < kPanel * KP; idx += 256 )
+        {
+            const int r = idx / KP, c = idx % KP;
+            const bool ok = r < cw && c < k;
+            cp_async_8( V + r * ldv + c, ok ? out + trow[r] * ld + c : out, ok );
+        }
+    }
+    else { stage_rows<KP>( V, out, brow + kPanel * b, nbb, ld, k ); }
+    cp_async_wait_all();
+    stage_finish<T, kPanel * kPanel / 256, 256>( src, dst );
     __syncthreads();
     double acc[nct][2];
 #pragma unroll
     for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
-    if( upper )
+    for( int kb = 0; kb < kSubs; ++kb )
     {
-        // x_rest into shared memory once
-        for( int idx = tid; idx < kPanel * KP; idx += 256 )
+#pragma unroll
+        for( int ct = 0; ct < nct; ++ct )
         {
-            const int r = idx / KP, c = idx % KP;
-            V[r * ldv + c] = (r < cw && c < k) ? out[trow[r] * ld + c] : 0.0;
+            // forward: acc(jj, c) = sum_rr P[rr][jj] x_b[rr][c]; back: acc(rr, c) = sum_jj P[rr][jj] x_rest[jj][c]
+            if( upper ) { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return P[8 * warp + i][8 * kb + kk]; },
+                                               [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
+            else        { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return P[8 * kb + kk][8 * warp + i]; },
+                                               [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
         }
     }
-    for( int b = 0; b < nblk; ++b )
+    const int r = 8 * warp + (lane >> 2);
+    if( upper ? r < nbb : r < cw )
     {
-        const int nbb = super_block_rows( sp, b );
-        // P: rows of block b (U rows r0 + 64 b + rr), the chunk's rest columns
-        for( int idx = tid; idx < kPanel * kPanel; idx += 256 )
+        double * row = upper ? zbuf + (brow + kPanel * b + r) * ld : in + trow[r] * ld;
+#pragma unroll
+        for( int ct = 0; ct < nct; ++ct )
         {
-            const int rr = idx >> 6, jj = idx & 63;
-            const int col = task.c0 + jj;
-            const std::int64_t urow = sp.r0 + kPanel * b + rr;
-            double v = 0.0;
-            if( rr < nbb && jj < cw )
-            {
-                v = static_cast<double>( col < m ? U0[urow * sp.ld0 + r1 + col] : U1[urow * sp.ld1 + (col - m)] );
-            }
-            P[rr][jj] = v;
-        }
-        if( !upper )
-        {
-            for( int idx = tid; idx < kPanel * KP; idx += 256 )
-            {
-                const int r = idx / KP, c = idx % KP;
-                V[r * ldv + c] = (r < nbb && c < k) ? out[(brow + kPanel * b + r) * ld + c] : 0.0;
-            }
-        }
-        __syncthreads();
-        if( !upper )
-        {
-            // acc(jj, c) += sum_rr P[rr][jj] x_b[rr][c]
-            for( int kb = 0; kb < kSubs; ++kb )
-            {
-#pragma unroll
-                for( int ct = 0; ct < nct; ++ct )
-                {
-                    dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return P[8 * kb + kk][8 * warp + i]; },
-                                         [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } );
-                }
-            }
-        }
-        else
-        {
-            // z_b(rr, c) -= sum_jj P[rr][jj] x_rest[jj][c]
-            double zb[nct][2];
-#pragma unroll
-            for( int ct = 0; ct < nct; ++ct ) { zb[ct][0] = 0.0; zb[ct][1] = 0.0; }
-            for( int kb = 0; kb < kSubs; ++kb )
-            {
-#pragma unroll
-                for( int ct = 0; ct < nct; ++ct )
-                {
-                    dmma_8x8x8( zb[ct], [&]( int i, int kk ) { return P[8 * warp + i][8 * kb + kk]; },
-                                        [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } );
-                }
-            }
-            const int rr = 8 * warp + (lane >> 2);
-            if( rr < nbb )
-            {
-                double * dst = zbuf + (brow + kPanel * b + rr) * ld;
-#pragma unroll
-                for( int ct = 0; ct < nct; ++ct )
-                {
-                    const int c = 8 * ct + 2 * (lane & 3);
-                    if( c < k ) { atomicAdd( dst + c, -zb[ct][0] ); }
-                    if( c + 1 < k ) { atomicAdd( dst + c + 1, -zb[ct][1] ); }
-                }
-            }
-        }
-        __syncthreads();
-    }
-    if( !upper )
-    {
-        const int jj = 8 * warp + (lane >> 2);
-        if( jj < cw )
-        {
-            double * dst = in + trow[jj] * ld;
-            const bool own = task.c0 + jj < m;
-#pragma unroll
-            for( int ct = 0; ct < nct; ++ct )
-            {
-#pragma unroll
-                for( int e = 0; e < 2; ++e )
-                {
-                    const int c = 8 * ct + 2 * (lane & 3) + e;
-                    if( c < k ) { if( own ) { dst[c] -= acc[ct][e]; } else { atomicAdd( dst + c, -acc[ct][e] ); } }
-                }
-            }
+            const int c = 8 * ct + 2 * (lane & 3);
+            if( c < k ) { red_add_f64( row + c, -acc[ct][0] ); }
+            if( c + 1 < k ) { red_add_f64( row + c + 1, -acc[ct][1] ); }
         }
     }
 }
@@ -2226,7 +2200,7 @@ void launch_super_inv( const SuperInvTask * tasks, int count, const SuperPanel *
 
 static size_t super_solve_smem( int k )
 {
-    return sizeof(double) * (kPanel * kSld + kPanel * ((1 << solve_lkp( k )) + 4));
+    return sizeof(double) * (kPanel * kSld + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
 }
 
 void launch_super_diag( const SuperSolveTask * tasks, int count, const SuperPanel * sps, const double * tbuf, bool upper,

@@ -913,14 +913,22 @@ void Plan::build_super( const std::vector<std::vector<I32>> & front_panels, Rang
             if( s >= v.size() ) { continue; }
             const I32 p = v[s];
             const SuperPanel & sp = spanels[static_cast<size_t>(p)];
+            const I32 nblk = static_cast<I32>( ceil_div( sp.rows, kPanel ) );
             if( diag )
             {
-                for( I32 o = 0; o * kPanel < sp.rows; ++o ) { ssolve.push_back( { p, o, 0, 0 } ); }
+                // block pairs (o, b): forward b <= o, back b >= o
+                for( I32 o = 0; o < nblk; ++o )
+                {
+                    for( I32 b = forward ? 0 : o; b < (forward ? o + 1 : nblk); ++b ) { ssolve.push_back( { p, o, b, 0 } ); }
+                }
             }
             else
             {
                 const I32 rest = (sp.n0 - sp.r0 - sp.rows) + sp.n1;
-                for( I32 c0 = 0; c0 < rest; c0 += kSolveRest ) { ssolve.push_back( { p, 0, c0, std::min( rest, c0 + kSolveRest ) } ); }
+                for( I32 b = 0; b < nblk; ++b )
+                {
+                    for( I32 c0 = 0; c0 < rest; c0 += kSolveRest ) { ssolve.push_back( { p, b, c0, std::min( rest, c0 + kSolveRest ) } ); }
+                }
             }
         }
         const I32 count = static_cast<I32>( static_cast<I64>( ssolve.size() ) - first );

@@ -236,11 +236,12 @@ struct SuperInvTask
     std::int32_t sp, i, j, pad;
 };
 
-// A super-panel solve task.  Diag: output block `blk` (64 rows) of the
-// block's solution, x_blk = sum_{i<=blk} T_{i,blk}^T y_i (forward) or
-// sum_{j>=blk} T_{blk,j} (y_j + z_j) (back).  Rest: rest rows [c0, c1) of the
-// front after the block (U0 rows, then its U1 columns): forward y_rest -=
-// U_{block,rest}^T x_block; back z_block -= U_{block,rest} x_rest.
+// A super-panel solve task.  Diag: the pair (blk, c0) of 64-row blocks, one
+// term of the block's solution x_blk = sum_{i<=blk} T_{i,blk}^T y_i (forward,
+// i = c0 <= blk) or sum_{j>=blk} T_{blk,j} (y_j + z_j) (back, j = c0 >= blk).
+// Rest: block blk and rest rows [c0, c1) of the front after the super-panel
+// (U0 rows, then its U1 columns): forward y_rest -= U_{blk,rest}^T x_blk; back
+// z_blk -= U_{blk,rest} x_rest.
 struct SuperSolveTask
 {
     std::int32_t sp, blk, c0, c1;

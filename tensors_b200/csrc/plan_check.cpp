@@ -442,6 +442,7 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         // each sweep: every other front's tasks once, every super-panel's diag blocks and rest rows once
         for( const std::vector<Launch> * list : { &pl.lower_launches_sp, &pl.upper_launches_sp } )
         {
+            const bool forward = list == &pl.lower_launches_sp;
             I64 regular = 0;
             std::vector<I64> diag( static_cast<size_t>( nsp ), 0 ), rest( static_cast<size_t>( nsp ), 0 );
             for( const Launch & L : *list )
@@ -463,9 +464,11 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
                     const SuperSolveTask & v = pl.ssolve[static_cast<size_t>( t )];
                     if( v.sp < 0 || v.sp >= nsp ) { return "super solve task out of range"; }
                     const size_t p = static_cast<size_t>( v.sp );
+                    if( v.blk < 0 || v.blk >= nblk[p] ) { return "super solve block out of range"; }
                     if( L.kind == LaunchKind::SuperDiag )
                     {
-                        if( v.blk < 0 || v.blk >= nblk[p] ) { return "super solve diag block out of range"; }
+                        // block pair (blk, c0): forward c0 <= blk, back c0 >= blk
+                        if( v.c0 < 0 || v.c0 >= nblk[p] || (forward ? v.c0 > v.blk : v.c0 < v.blk) ) { return "super solve diag pair out of range"; }
                         ++diag[p];
                     }
                     else
@@ -480,7 +483,8 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             if( regular != small ) { return "super solve list: the other fronts' steps are not covered once"; }
             for( I64 p = 0; p < nsp; ++p )
             {
-                if( diag[static_cast<size_t>( p )] != nblk[static_cast<size_t>( p )] || rest[static_cast<size_t>( p )] != nrest[static_cast<size_t>( p )] )
+                const I64 nb = nblk[static_cast<size_t>( p )];
+                if( diag[static_cast<size_t>( p )] != nb * (nb + 1) / 2 || rest[static_cast<size_t>( p )] != nb * nrest[static_cast<size_t>( p )] )
                 {
                     return "super solve list: super-panel " + std::to_string( p ) + " not covered once";
                 }
