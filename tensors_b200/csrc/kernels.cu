@@ -293,12 +293,159 @@ __device__ __forceinline__ void dmma_8x8x8( double (&acc)[2], FA a, FB b )
 
 constexpr size_t kPotrfSmemBytes = sizeof(double) * (2 * kPanel * (kPanel + 1) + 2 * kPanel + 1);
 
-// Cholesky of one panel's 64 x 64 diagonal block D (identity beyond nb), in
-// shared memory by 8 x 8 sub-blocks, written back in place; then the inverse
-// T = D^{-1} (upper triangular, zero below the diagonal) into tinv block
-// t.panel, which the panel's trsm and the solves use.  With FP32 storage the
-// block is rounded to FP32 before the inversion, so that T inverts the stored
-// factor.
+template<typename T> __device__ __forceinline__ double round_to( double v ) { return static_cast<double>( static_cast<T>( v ) ); }
+
+// Panel factorization state in shared memory.  D: the 64 x 64 block; its
+// upper triangle holds A (updated right-looking) and, in the diagonal 8 x 8
+// tiles, U; the strictly lower tile (c, b) receives U_bc^T once row block b
+// is formed.  Ti: the inverse T = U^{-1} (upper tiles; diagonal tiles zero
+// below the diagonal); its strictly lower tiles serve as per-warp scratch.
+struct PotrfShared
+{
+    double (*D)[kPanel + 1];
+    double (*Ti)[kPanel + 1];
+    double * floor_s;
+    int * fail;
+    int * redo;
+};
+
+// The warp's scratch tile `slot` (0 or 1): one of the strictly lower 8 x 8
+// tiles of Ti in its rows 40..63 (16 of them, two per warp).
+__device__ __forceinline__ double (*potrf_scratch( const PotrfShared & sh, int slot ))[kPanel + 1]
+{
+    const int idx = 2 * (threadIdx.x >> 5) + slot;
+    const int r = idx < 7 ? 7 : (idx < 13 ? 6 : 5);
+    const int q = idx < 7 ? idx : (idx < 13 ? idx - 7 : idx - 13);
+    return reinterpret_cast<double (*)[kPanel + 1]>( &sh.Ti[kSub * r][kSub * q] );
+}
+
+// U_bc = W_b^T A_bc (W_b = U_bb^{-1}, tile (b, b) of Ti), rounded to the
+// storage type, into the scratch tile S (warp-wide).
+template<typename T>
+__device__ __forceinline__ void potrf_u_tile( const PotrfShared & sh, int b, int c, double (*S)[kPanel + 1] )
+{
+    const int lane = threadIdx.x & 31;
+    double acc[2] = { 0.0, 0.0 };
+    dmma_8x8x8( acc, [&]( int i, int k ) { return sh.Ti[kSub * b + k][kSub * b + i]; },
+                     [&]( int k, int j ) { return sh.D[kSub * b + k][kSub * c + j]; } );
+    const int i = lane >> 2, j = 2 * (lane & 3);
+    S[i][j] = round_to<T>( acc[0] );
+    S[i][j + 1] = round_to<T>( acc[1] );
+    __syncwarp();
+}
+
+// Cholesky of the diagonal tile q of D and the inverse W_q of its factor
+// (one warp; lane c < 8 holds column c).  Speculative: the tile's row block
+// right of it may still be changing, so a pivot at or below its floor (mixed
+// precision), whose raised value depends on that row, stops the tile with
+// nothing written and returns false.  Otherwise U_qq (rounded to the storage
+// type) replaces the tile's upper triangle and W_q = U_qq^{-1} goes to tile
+// (q, q) of Ti with zeros below its diagonal.
+template<typename T>
+__device__ bool potrf_diag_tile( const PotrfShared & sh, const PanelTask & t, int q, int nb, const T * __restrict__ arena,
+                                 int * __restrict__ status, const double * __restrict__ pivot_floor, bool speculative )
+{
+    const int lane = threadIdx.x & 31;
+    const int o = kSub * q;
+    const double beta2 = pivot_floor != nullptr ? pivot_floor[0] : 0.0;
+    double a[kSub];
+#pragma unroll
+    for( int r = 0; r < kSub; ++r ) { a[r] = (lane < kSub && r <= lane) ? sh.D[o + r][o + lane] : 0.0; }
+#pragma unroll
+    for( int r = 0; r < kSub; ++r )
+    {
+        double d = __shfl_sync( 0xffffffffu, a[r], r );
+        const bool single = (t.single_rows >> (o + r)) & 1;
+        if( single ) { d = fabs( d ); }                     // 1 x 1 reference supernodes: sqrt(|a|)
+        if( pivot_floor != nullptr && o + r < nb )
+        {
+            // mixed precision: a pivot lost to FP32 rounding (for a 1 x 1
+            // supernode too: |a| can cancel to 0) is raised to its floor
+            // (static pivoting); the FP64 refinement corrects it.  The raised
+            // pivot also bounds the row's entries in the block by beta =
+            // sqrt(max |a_ii|), the growth bound of the modified Cholesky of
+            // Gill, Murray and Wright: a small pivot under a large row would
+            // otherwise make the next pivots of the block hugely negative,
+            // floored in turn, until FP32 overflows.
+            const double tau = sh.floor_s[o + r];
+            if( !(d > tau) )
+            {
+                if( speculative ) { return false; }
+                // the row's largest entry: this tile's columns (registers), the
+                // rest of the block (shared memory) and the row's rest columns in
+                // U0 and U1, which the trsm divides by the pivot
+                double m = (lane > r && lane < kSub) ? fabs( a[r] ) : 0.0;
+                for( int c = o + kSub + lane; c < kPanel; c += 32 ) { m = fmax( m, fabs( sh.D[o + r][c] ) ); }
+                const std::int64_t grow = t.r0 + o + r;
+                for( int c = t.r0 + nb + lane; c < t.n0; c += 32 )
+                {
+                    m = fmax( m, fabs( static_cast<double>( arena[t.u0 + grow * t.ld0 + c] ) ) );
+                }
+                for( int c = lane; c < t.n1; c += 32 )
+                {
+                    m = fmax( m, fabs( static_cast<double>( arena[t.u1 + grow * t.ld1 + c] ) ) );
+                }
+#pragma unroll
+                for( int s2 = 16; s2 > 0; s2 >>= 1 ) { m = fmax( m, __shfl_xor_sync( 0xffffffffu, m, s2 ) ); }
+                if( lane == 0 ) { atomicAdd( status + 2, 1 ); }
+                d = fmax( tau, beta2 > 0.0 ? m * m / beta2 : 0.0 );
+            }
+        }
+        if( lane == 0 && !single && o + r < nb && !(d > 0.0) && *sh.fail < 0 ) { *sh.fail = o + r; }
+        // reciprocal square root and one product instead of sqrt and a
+        // division: both are long dependent sequences on the FP64 pipe
+        const double inv = rsqrt( d );
+        const double piv = d * inv;
+        if( lane == r ) { a[r] = piv; }
+        if( lane > r ) { a[r] *= inv; }                     // U(r, lane)
+#pragma unroll
+        for( int r2 = r + 1; r2 < kSub; ++r2 )
+        {
+            const double urr2 = __shfl_sync( 0xffffffffu, a[r], r2 );   // U(r, r2)
+            if( lane >= r2 ) { a[r2] -= urr2 * a[r]; }
+        }
+    }
+#pragma unroll
+    for( int r = 0; r < kSub; ++r ) { a[r] = round_to<T>( a[r] ); }
+    // W = U^{-1}, lane j its column j: w_j = 1 / u_jj, then for k = j, j-1, ..:
+    // w_i = -(sum_{k=i+1..j} u_ik w_k) / u_ii
+    double rec[kSub], w[kSub], sum[kSub];
+#pragma unroll
+    for( int i = 0; i < kSub; ++i ) { rec[i] = 1.0 / __shfl_sync( 0xffffffffu, a[i], i ); sum[i] = 0.0; }
+#pragma unroll
+    for( int k = kSub - 1; k >= 0; --k )
+    {
+        w[k] = lane == k ? rec[k] : (lane > k ? -rec[k] * sum[k] : 0.0);
+#pragma unroll
+        for( int i = 0; i < k; ++i ) { sum[i] += __shfl_sync( 0xffffffffu, a[i], k ) * w[k]; }   // u_ik w_k
+    }
+    if( lane < kSub )
+    {
+#pragma unroll
+        for( int r = 0; r < kSub; ++r )
+        {
+            if( r <= lane ) { sh.D[o + r][o + lane] = a[r]; }
+            sh.Ti[o + r][o + lane] = w[r];
+        }
+    }
+    __syncwarp();
+    return true;
+}
+
+// Cholesky of one panel's 64 x 64 diagonal block D (identity beyond nb) and
+// the inverse T = D^{-1} of its factor (LAPACK potrf of FactorizeSupernode,
+// Multifrontal.hpp:438-449, plus the inverse the panel's trsm and the solves
+// use).  A row that forms a 1 x 1 reference supernode takes sqrt(|a|) as the
+// reference does (:471) and never reports failure.
+//
+// Right-looking by 8 x 8 tiles with one barrier per tile step b.  Warp 0
+// forms U_{b,b+1}, applies its update to tile (b+1, b+1) and factors that
+// tile ahead (its Cholesky and inverse W_{b+1}); the other warps update the
+// remaining trailing tiles (b2, c), each forming the U_{b,b2} = W_b^T A_{b,b2}
+// and U_{b,c} it needs in its own registers, and form column block b of T,
+// T_ib = -(sum_{k=i..b-1} T_ik U_kb) W_b.  Every 8 x 8 x 8 product runs on
+// the FP64 tensor cores (two DMMA m8n8k4).  With FP32 storage every U value
+// is rounded to FP32 when formed, so the updates and T use the stored factor.
 template<typename T>
 __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict__ arena, int * __restrict__ status,
                                             double * smem, const double * __restrict__ pivot_floor, double * __restrict__ tinv )
@@ -306,220 +453,135 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int nb = min( kPanel, t.n0 - t.r0 );
-    double (*D)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem );
-    double (*Ti)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( smem + kPanel * (kPanel + 1) );
-    double * inv_d = smem + 2 * kPanel * (kPanel + 1);
-    double * floor_s = inv_d + kPanel;                  // the panel's pivot floors (mixed precision)
-    int & fail = *reinterpret_cast<int *>( floor_s + kPanel );
+    PotrfShared sh;
+    sh.D = reinterpret_cast<double (*)[kPanel + 1]>( smem );
+    sh.Ti = reinterpret_cast<double (*)[kPanel + 1]>( smem + kPanel * (kPanel + 1) );
+    sh.floor_s = smem + 2 * kPanel * (kPanel + 1);      // the panel's pivot floors (mixed precision)
+    sh.fail = reinterpret_cast<int *>( sh.floor_s + kPanel );
+    sh.redo = sh.fail + 1;
 
     T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    if( pivot_floor != nullptr && tid < nb ) { floor_s[tid] = pivot_floor[1 + t.row0 + t.r0 + tid]; }
-    const double beta2 = pivot_floor != nullptr ? pivot_floor[0] : 0.0;
+    if( pivot_floor != nullptr && tid < nb ) { sh.floor_s[tid] = pivot_floor[1 + t.row0 + t.r0 + tid]; }
     auto stage_src = [&]( int idx, double & fill ) -> const T *
     {
         const int r = idx / kPanel, c = idx % kPanel;
         fill = (r >= nb && r == c) ? 1.0 : 0.0;      // identity padding beyond nb
         return (r < nb && c < nb && r <= c) ? U0 + (std::int64_t)r * t.ld0 + c : nullptr;
     };
-    auto stage_dst = [&]( int idx ) { return &D[idx / kPanel][idx % kPanel]; };
+    auto stage_dst = [&]( int idx ) { return &sh.D[idx / kPanel][idx % kPanel]; };
     stage_block<T, kPanel * kPanel / kPotrfThreads, kPotrfThreads>( U0, stage_src, stage_dst );
-    if( tid == 0 ) { fail = -1; }
+    if( tid == 0 ) { *sh.fail = -1; *sh.redo = 0; }
     cp_async_wait_all();
     stage_finish<T, kPanel * kPanel / kPotrfThreads, kPotrfThreads>( stage_src, stage_dst );
     __syncthreads();
 
     const int nsub = (nb + kSub - 1) / kSub;
+    if( warp == 0 ) { potrf_diag_tile<T>( sh, t, 0, nb, arena, status, pivot_floor, false ); }
+    __syncthreads();
     for( int b = 0; b < nsub; ++b )
     {
-        const int o = b * kSub;
-        // (a) Cholesky of the 8 x 8 diagonal sub-block: lane c < 8 holds column c
+        const int rem = nsub - 1 - b;                   // trailing tile rows / columns
         if( warp == 0 )
         {
-            double a[kSub];
-#pragma unroll
-            for( int r = 0; r < kSub; ++r ) { a[r] = (lane < kSub && r <= lane) ? D[o + r][o + lane] : 0.0; }
-#pragma unroll
-            for( int r = 0; r < kSub; ++r )
+            if( rem > 0 )
             {
-                double d = __shfl_sync( 0xffffffffu, a[r], r );
-                const bool single = (t.single_rows >> (o + r)) & 1;
-                if( single ) { d = fabs( d ); }                     // 1 x 1 reference supernodes: sqrt(|a|)
-                if( pivot_floor != nullptr && o + r < nb )
-                {
-                    // mixed precision: a pivot lost to FP32 rounding (for a 1 x 1
-                    // supernode too: |a| can cancel to 0) is raised to its floor
-                    // (static pivoting); the FP64 refinement corrects it.  The
-                    // raised pivot also bounds the row's entries in the block by
-                    // beta = sqrt(max |a_ii|), the growth bound of the modified
-                    // Cholesky of Gill, Murray and Wright: a small pivot under a
-                    // large row would otherwise make the next pivots of the block
-                    // hugely negative, floored in turn, until FP32 overflows.
-                    const double tau = floor_s[o + r];
-                    if( !(d > tau) )
-                    {
-                        // the row's largest entry: this sub-block's columns (registers),
-                        // the rest of the block (shared memory) and the row's rest
-                        // columns in U0 and U1, which the trsm divides by the pivot
-                        double m = (lane > r && lane < kSub) ? fabs( a[r] ) : 0.0;
-                        for( int c = o + kSub + lane; c < kPanel; c += 32 ) { m = fmax( m, fabs( D[o + r][c] ) ); }
-                        const std::int64_t grow = t.r0 + o + r;
-                        for( int c = t.r0 + nb + lane; c < t.n0; c += 32 )
-                        {
-                            m = fmax( m, fabs( static_cast<double>( arena[t.u0 + grow * t.ld0 + c] ) ) );
-                        }
-                        for( int c = lane; c < t.n1; c += 32 )
-                        {
-                            m = fmax( m, fabs( static_cast<double>( arena[t.u1 + grow * t.ld1 + c] ) ) );
-                        }
-#pragma unroll
-                        for( int s2 = 16; s2 > 0; s2 >>= 1 ) { m = fmax( m, __shfl_xor_sync( 0xffffffffu, m, s2 ) ); }
-                        if( lane == 0 ) { atomicAdd( status + 2, 1 ); }
-                        d = fmax( tau, beta2 > 0.0 ? m * m / beta2 : 0.0 );
-                    }
-                }
-                if( lane == 0 )
-                {
-                    if( single ) { }
-                    else if( o + r < nb && !(d > 0.0) && fail < 0 ) { fail = o + r; }
-                }
-                // reciprocal square root and one product instead of sqrt and a
-                // division: both are long dependent sequences on the FP64 pipe
-                const double inv = rsqrt( d );
-                const double piv = d * inv;
-                if( lane == r ) { a[r] = piv; inv_d[o + r] = inv; }
-                if( lane > r ) { a[r] *= inv; }                     // U(r, lane)
-#pragma unroll
-                for( int r2 = r + 1; r2 < kSub; ++r2 )
-                {
-                    const double urr2 = __shfl_sync( 0xffffffffu, a[r], r2 );   // U(r, r2)
-                    if( lane >= r2 ) { a[r2] -= urr2 * a[r]; }
-                }
-            }
-            if( lane < kSub )
-            {
-#pragma unroll
-                for( int r = 0; r < kSub; ++r ) { if( r <= lane ) { D[o + r][o + lane] = a[r]; } }
-            }
-        }
-        __syncthreads();
-        // (b) rows o..o+7 of the columns right of the sub-block: U_b,c = L_bb^{-1} A_b,c
-        {
-            const int col = o + kSub + tid;
-            if( col < kSub * nsub )
-            {
-                double x[kSub];
-#pragma unroll
-                for( int r = 0; r < kSub; ++r ) { x[r] = D[o + r][col]; }
-#pragma unroll
-                for( int r = 0; r < kSub; ++r )
-                {
-                    x[r] *= inv_d[o + r];
-#pragma unroll
-                    for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= D[o + r][o + r2] * x[r]; }
-                }
-#pragma unroll
-                for( int r = 0; r < kSub; ++r ) { D[o + r][col] = x[r]; }
-            }
-        }
-        __syncthreads();
-        // (c) trailing sub-blocks (b2, b3), b < b2 <= b3 < nsub: D -= U_b,b2^T U_b,b3 (the
-        // identity padding beyond nb rounded up to 8 is neither updated nor read)
-        {
-            const int rem = nsub - 1 - b;
-            const int tiles = rem * (rem + 1) / 2;
-            for( int tile = warp; tile < tiles; tile += kPotrfThreads / 32 )
-            {
-                int b2 = 0, acc_t = tile;
-                while( acc_t >= rem - b2 ) { acc_t -= rem - b2; ++b2; }
-                const int b3 = b2 + acc_t;
-                const int o2 = o + kSub + b2 * kSub, o3 = o + kSub + b3 * kSub;
-                double acc[2] = { 0.0, 0.0 };
-                dmma_8x8x8( acc, [&]( int i, int k ) { return D[o + k][o2 + i]; },
-                                 [&]( int k, int j ) { return D[o + k][o3 + j]; } );
+                // U_{b,b+1}: the lower tile (b+1, b) and the update of tile (b+1, b+1)
+                double (*S)[kPanel + 1] = potrf_scratch( sh, 0 );
+                potrf_u_tile<T>( sh, b, b + 1, S );
                 const int i = lane >> 2, j = 2 * (lane & 3);
-                D[o2 + i][o3 + j]     -= acc[0];
-                D[o2 + i][o3 + j + 1] -= acc[1];
+                sh.D[kSub * (b + 1) + j][kSub * b + i] = S[i][j];
+                sh.D[kSub * (b + 1) + j + 1][kSub * b + i] = S[i][j + 1];
+                double acc[2] = { 0.0, 0.0 };
+                dmma_8x8x8( acc, [&]( int ii, int k ) { return S[k][ii]; }, [&]( int k, int jj ) { return S[k][jj]; } );
+                sh.D[kSub * (b + 1) + i][kSub * (b + 1) + j] -= acc[0];
+                sh.D[kSub * (b + 1) + i][kSub * (b + 1) + j + 1] -= acc[1];
+                __syncwarp();
+                if( !potrf_diag_tile<T>( sh, t, b + 1, nb, arena, status, pivot_floor, true ) && lane == 0 ) { *sh.redo = 1; }
+            }
+        }
+        else
+        {
+            // trailing tiles (b2, c), b < b2 <= c < nsub, but (b+1, b+1); then T's column block b
+            const int tiles = rem * (rem + 1) / 2 - (rem > 0 ? 1 : 0);
+            for( int job = warp - 1; job < tiles + b; job += kPotrfThreads / 32 - 1 )
+            {
+                const int i = lane >> 2, j = 2 * (lane & 3);
+                if( job < tiles )
+                {
+                    // job -> (b2, c) in column-major order of the trailing triangle after (b+1, b+1)
+                    int c = b + 2, left = job;
+                    while( left >= c - b ) { left -= c - b; ++c; }
+                    const int b2 = b + 1 + left;
+                    double (*Sc)[kPanel + 1] = potrf_scratch( sh, 0 );
+                    double (*Sr)[kPanel + 1] = potrf_scratch( sh, 1 );
+                    potrf_u_tile<T>( sh, b, c, Sc );
+                    if( b2 == c )
+                    {
+                        // the tile (c, c) job also stores U_bc into the lower tile (c, b)
+                        sh.D[kSub * c + j][kSub * b + i] = Sc[i][j];
+                        sh.D[kSub * c + j + 1][kSub * b + i] = Sc[i][j + 1];
+                    }
+                    else { potrf_u_tile<T>( sh, b, b2, Sr ); }
+                    double (*Sb)[kPanel + 1] = b2 == c ? Sc : Sr;
+                    double acc[2] = { 0.0, 0.0 };
+                    dmma_8x8x8( acc, [&]( int ii, int k ) { return Sb[k][ii]; }, [&]( int k, int jj ) { return Sc[k][jj]; } );
+                    sh.D[kSub * b2 + i][kSub * c + j] -= acc[0];
+                    sh.D[kSub * b2 + i][kSub * c + j + 1] -= acc[1];
+                    __syncwarp();
+                }
+                else
+                {
+                    // T_ib, i = job - tiles < b
+                    const int ib = job - tiles;
+                    double acc[2] = { 0.0, 0.0 };
+                    for( int k = ib; k < b; ++k )
+                    {
+                        dmma_8x8x8( acc, [&]( int ii, int kk ) { return sh.Ti[kSub * ib + ii][kSub * k + kk]; },
+                                         [&]( int kk, int jj ) { return sh.D[kSub * b + jj][kSub * k + kk]; } );   // U_kb = (lower tile (b, k))^T
+                    }
+                    double (*S)[kPanel + 1] = potrf_scratch( sh, 0 );
+                    S[i][j] = acc[0];
+                    S[i][j + 1] = acc[1];
+                    __syncwarp();
+                    double acc2[2] = { 0.0, 0.0 };
+                    dmma_8x8x8( acc2, [&]( int ii, int k ) { return S[ii][k]; },
+                                      [&]( int k, int jj ) { return sh.Ti[kSub * b + k][kSub * b + jj]; } );
+                    sh.Ti[kSub * ib + i][kSub * b + j] = -acc2[0];
+                    sh.Ti[kSub * ib + i][kSub * b + j + 1] = -acc2[1];
+                    __syncwarp();
+                }
             }
         }
         __syncthreads();
+        if( *sh.redo )
+        {
+            // a pivot of tile (b+1, b+1) needed its floor: factor the tile again
+            // now that its row block is complete
+            if( warp == 0 ) { potrf_diag_tile<T>( sh, t, b + 1, nb, arena, status, pivot_floor, false ); }
+            __syncthreads();
+            if( tid == 0 ) { *sh.redo = 0; }
+            __syncthreads();
+        }
     }
+    // U: the diagonal tiles' upper triangles and the transposed lower tiles
     for( int idx = tid; idx < nb * nb; idx += kPotrfThreads )
     {
         const int r = idx / nb, c = idx % nb;
-        if( r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = static_cast<T>( D[r][c] ); }
+        if( r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = static_cast<T>( (r >> 3) == (c >> 3) ? sh.D[r][c] : sh.D[c][r] ); }
     }
-    if( tid == 0 && fail >= 0 )
+    if( tid == 0 && *sh.fail >= 0 )
     {
         atomicOr( status, 1 );
-        atomicMin( status + 1, t.row0 + t.r0 + fail );
+        atomicMin( status + 1, t.row0 + t.r0 + *sh.fail );
     }
-
-    // T = D^{-1} by 8 x 8 blocks: (a) the 8 diagonal blocks, one thread per
-    // column; (b) the blocks at distance d = 1..7 from the diagonal, one warp
-    // per block: T_ij = -T_ii sum_{k=i+1..j} D_ik T_kj (T_kj at smaller
-    // distances, so each distance is one round).
-    if constexpr ( sizeof(T) == 4 )
-    {
-        for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
-        {
-            double & v = D[idx / kPanel][idx % kPanel];
-            v = static_cast<double>( static_cast<float>( v ) );
-        }
-        __syncthreads();
-    }
-    // reciprocal pivots of the (possibly rounded) block, one division per thread;
-    // only the leading nsub x nsub blocks of T are formed (the trsm and the
+    // only the leading nsub x nsub tiles of T are formed (the trsm and the
     // solves read no more)
     const int nbp = kSub * nsub;
-    if( tid < nbp ) { inv_d[tid] = 1.0 / D[tid][tid]; }
-    __syncthreads();
-    if( tid < nbp )
-    {
-        const int o = (tid >> 3) * kSub, j = tid & (kSub - 1);
-        double col[kSub];
-#pragma unroll
-        for( int i = kSub - 1; i >= 0; --i )
-        {
-            double s = (i == j) ? 1.0 : 0.0;
-#pragma unroll
-            for( int k = i + 1; k < kSub; ++k ) { if( k <= j ) { s -= D[o + i][o + k] * col[k]; } }
-            col[i] = (i <= j) ? s * inv_d[o + i] : 0.0;
-        }
-#pragma unroll
-        for( int i = 0; i < kSub; ++i ) { Ti[o + i][o + j] = col[i]; }
-    }
-    __syncthreads();
-    for( int d = 1; d < nsub; ++d )
-    {
-        if( warp < nsub - d )
-        {
-            const int ib = warp, jb = warp + d;
-            double acc[2] = { 0.0, 0.0 };
-            for( int kb = ib + 1; kb <= jb; ++kb )
-            {
-                dmma_8x8x8( acc, [&]( int i, int k ) { return D[kSub * ib + i][kSub * kb + k]; },
-                                 [&]( int k, int j ) { return Ti[kSub * kb + k][kSub * jb + j]; } );
-            }
-            // the sum goes through the warp's strictly lower block (7, warp) of
-            // Ti, which nothing else reads, into the B operand layout
-            double (*S)[kPanel + 1] = reinterpret_cast<double (*)[kPanel + 1]>( &Ti[kPanel - kSub][kSub * warp] );
-            const int ri = lane >> 2, cj = 2 * (lane & 3);
-            S[ri][cj] = acc[0];
-            S[ri][cj + 1] = acc[1];
-            __syncwarp();
-            double acc2[2] = { 0.0, 0.0 };
-            dmma_8x8x8( acc2, [&]( int i, int k ) { return Ti[kSub * ib + i][kSub * ib + k]; },
-                              [&]( int k, int j ) { return S[k][j]; } );
-            Ti[kSub * ib + ri][kSub * jb + cj]     = -acc2[0];
-            Ti[kSub * ib + ri][kSub * jb + cj + 1] = -acc2[1];
-        }
-        __syncthreads();
-    }
     double * out = tinv + (std::int64_t)t.panel * (kPanel * kPanel);
     for( int idx = tid; idx < nbp * kPanel; idx += kPotrfThreads )
     {
         const int r = idx / kPanel, c = idx % kPanel;
-        if( c < nbp ) { out[idx] = (r <= c) ? Ti[r][c] : 0.0; }
+        if( c < nbp ) { out[idx] = (r <= c) ? sh.Ti[r][c] : 0.0; }
     }
 }
 
