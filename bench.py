@@ -237,13 +237,21 @@ def run_reference(args):
 
 
 def run_for_profiler(args):
-    """The plain workload for ncu: (warmup + steps) x (factor + solve), direct launches."""
+    """The plain workload for ncu: (warmup + steps) x (factor + solve), direct launches; the
+    headline Laplacian, or with --workload c3 the vector Laplacian (--grid: its edge)."""
     import torch
     from tensors_b200 import build as tb_build
     from tensors_b200.cholesky import CholeskyDecomposition
 
     tb_build.build()
-    A, perm, B_host = build_problem(args.grid)
+    if args.workload == "c3":
+        from tensors_b200 import matrices, ordering
+
+        A = matrices.vector_laplacian_3d(args.grid or C3_GRID, C3_SEED, C3_SHIFT)
+        perm = ordering.nested_dissection(A)
+        B_host = np.random.default_rng(C3_SEED + 1).standard_normal((A.n, C3_NRHS))
+    else:
+        A, perm, B_host = build_problem(args.grid)
     chol = CholeskyDecomposition(A.outer, A.inner, perm)
     chol.SetPrecision(args.precision)
     chol.SymbolicFactorization()
@@ -257,7 +265,7 @@ def run_for_profiler(args):
     torch.cuda.synchronize()
     R = chol.Residual(B, X)
     torch.cuda.synchronize()
-    print(json.dumps({"grid": args.grid, "precision": args.precision,
+    print(json.dumps({"workload": args.workload or "c2", "grid": args.grid, "precision": args.precision,
                       "relres": float(torch.linalg.norm(R) / torch.linalg.norm(B)),
                       "launches": chol.LaunchCounts(), "plan": chol.PlanStats()}))
     return 0

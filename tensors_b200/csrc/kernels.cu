@@ -295,157 +295,182 @@ constexpr size_t kPotrfSmemBytes = sizeof(double) * (2 * kPanel * (kPanel + 1) +
 
 template<typename T> __device__ __forceinline__ double round_to( double v ) { return static_cast<double>( static_cast<T>( v ) ); }
 
-// Panel factorization state in shared memory.  D: the 64 x 64 block; its
-// upper triangle holds A (updated right-looking) and, in the diagonal 8 x 8
-// tiles, U; the strictly lower tile (c, b) receives U_bc^T once row block b
-// is formed.  Ti: the inverse T = U^{-1} (upper tiles; diagonal tiles zero
-// below the diagonal); its strictly lower tiles serve as per-warp scratch.
+// Panel factorization state in shared memory.  D: the 64 x 64 block, upper
+// triangle (A, overwritten by U row block by row block); Ti: the inverse
+// T = U^{-1} (upper tiles; diagonal tiles zero below the diagonal; its
+// strictly lower tiles serve as per-warp scratch); inv_d: the reciprocal
+// pivots the row-block solves use.
 struct PotrfShared
 {
     double (*D)[kPanel + 1];
     double (*Ti)[kPanel + 1];
+    double * inv_d;
     double * floor_s;
     int * fail;
     int * redo;
 };
 
-// The warp's scratch tile `slot` (0 or 1): one of the strictly lower 8 x 8
-// tiles of Ti in its rows 40..63 (16 of them, two per warp).
-__device__ __forceinline__ double (*potrf_scratch( const PotrfShared & sh, int slot ))[kPanel + 1]
+// The scratch tile of warp w = 1..7: the strictly lower tile (7, w - 1) of Ti.
+__device__ __forceinline__ double (*potrf_scratch( const PotrfShared & sh ))[kPanel + 1]
 {
-    const int idx = 2 * (threadIdx.x >> 5) + slot;
-    const int r = idx < 7 ? 7 : (idx < 13 ? 6 : 5);
-    const int q = idx < 7 ? idx : (idx < 13 ? idx - 7 : idx - 13);
-    return reinterpret_cast<double (*)[kPanel + 1]>( &sh.Ti[kSub * r][kSub * q] );
+    return reinterpret_cast<double (*)[kPanel + 1]>( &sh.Ti[kPanel - kSub][kSub * ((threadIdx.x >> 5) - 1)] );
 }
 
-// U_bc = W_b^T A_bc (W_b = U_bb^{-1}, tile (b, b) of Ti), rounded to the
-// storage type, into the scratch tile S (warp-wide).
-template<typename T>
-__device__ __forceinline__ void potrf_u_tile( const PotrfShared & sh, int b, int c, double (*S)[kPanel + 1] )
+// Stores a factored diagonal tile: U_qq over the tile's upper triangle and
+// its reciprocal pivots into inv_d.
+__device__ __forceinline__ void potrf_store_tile( const PotrfShared & sh, int o, const double (&a)[kSub][kSub], const double (&iv)[kSub] )
 {
-    const int lane = threadIdx.x & 31;
-    double acc[2] = { 0.0, 0.0 };
-    dmma_8x8x8( acc, [&]( int i, int k ) { return sh.Ti[kSub * b + k][kSub * b + i]; },
-                     [&]( int k, int j ) { return sh.D[kSub * b + k][kSub * c + j]; } );
-    const int i = lane >> 2, j = 2 * (lane & 3);
-    S[i][j] = round_to<T>( acc[0] );
-    S[i][j + 1] = round_to<T>( acc[1] );
+    if( (threadIdx.x & 31) == 0 )
+    {
+#pragma unroll
+        for( int r = 0; r < kSub; ++r )
+        {
+#pragma unroll
+            for( int c = r; c < kSub; ++c ) { sh.D[o + r][o + c] = a[r][c]; }
+            sh.inv_d[o + r] = iv[r];
+        }
+    }
     __syncwarp();
 }
 
-// Cholesky of the diagonal tile q of D and the inverse W_q of its factor
-// (one warp; lane c < 8 holds column c).  Speculative: the tile's row block
-// right of it may still be changing, so a pivot at or below its floor (mixed
-// precision), whose raised value depends on that row, stops the tile with
-// nothing written and returns false.  Otherwise U_qq (rounded to the storage
-// type) replaces the tile's upper triangle and W_q = U_qq^{-1} goes to tile
-// (q, q) of Ti with zeros below its diagonal.
+// The diagonal tile's Cholesky with pivot floors (mixed precision): a pivot
+// lost to FP32 rounding (for a 1 x 1 supernode too: |a| can cancel to 0) is
+// raised to its floor (static pivoting); the FP64 refinement corrects it.
+// The raised pivot also bounds the row's entries in the block by beta =
+// sqrt(max |a_ii|), the growth bound of the modified Cholesky of Gill, Murray
+// and Wright: a small pivot under a large row would otherwise make the next
+// pivots of the block hugely negative, floored in turn, until FP32
+// overflows.  Runs only for tiles with a pivot at or below its floor, after
+// the tile's row block is complete.
+template<typename T>
+__device__ __noinline__ void potrf_tile_floored( const PotrfShared & sh, const PanelTask & t, int q, int nb, const T * __restrict__ arena,
+                                                 int * __restrict__ status, const double * __restrict__ pivot_floor )
+{
+    const int lane = threadIdx.x & 31;
+    const int o = kSub * q;
+    double a[kSub][kSub], iv[kSub];
+#pragma unroll
+    for( int r = 0; r < kSub; ++r )
+    {
+#pragma unroll
+        for( int c = r; c < kSub; ++c ) { a[r][c] = sh.D[o + r][o + c]; }
+    }
+#pragma unroll
+    for( int r = 0; r < kSub; ++r )
+    {
+        double d = a[r][r];
+        const bool single = (t.single_rows >> (o + r)) & 1;
+        if( single ) { d = fabs( d ); }                     // 1 x 1 reference supernodes: sqrt(|a|)
+        const double tau = sh.floor_s[o + r];
+        if( o + r < nb && !(d > tau) )
+        {
+            // the row's largest entry: this tile's columns, the rest of the
+            // block and the row's rest columns in U0 and U1, which the trsm
+            // divides by the pivot
+            double m = 0.0;
+#pragma unroll
+            for( int c = r + 1; c < kSub; ++c ) { m = fmax( m, fabs( a[r][c] ) ); }
+            for( int c = o + kSub + lane; c < kPanel; c += 32 ) { m = fmax( m, fabs( sh.D[o + r][c] ) ); }
+            const std::int64_t grow = t.r0 + o + r;
+            for( int c = t.r0 + nb + lane; c < t.n0; c += 32 ) { m = fmax( m, fabs( static_cast<double>( arena[t.u0 + grow * t.ld0 + c] ) ) ); }
+            for( int c = lane; c < t.n1; c += 32 ) { m = fmax( m, fabs( static_cast<double>( arena[t.u1 + grow * t.ld1 + c] ) ) ); }
+#pragma unroll
+            for( int s2 = 16; s2 > 0; s2 >>= 1 ) { m = fmax( m, __shfl_xor_sync( 0xffffffffu, m, s2 ) ); }
+            if( lane == 0 ) { atomicAdd( status + 2, 1 ); }
+            const double beta2 = pivot_floor[0];
+            d = fmax( tau, beta2 > 0.0 ? m * m / beta2 : 0.0 );
+        }
+        iv[r] = rsqrt( d );
+        a[r][r] = d * iv[r];
+#pragma unroll
+        for( int c = r + 1; c < kSub; ++c ) { a[r][c] *= iv[r]; }
+#pragma unroll
+        for( int r2 = r + 1; r2 < kSub; ++r2 )
+        {
+#pragma unroll
+            for( int c = r2; c < kSub; ++c ) { a[r2][c] -= a[r][r2] * a[r][c]; }
+        }
+    }
+    potrf_store_tile( sh, o, a, iv );
+}
+
+// Cholesky of the diagonal tile q of D by one warp.  Every lane holds the
+// whole tile in registers and runs the same branch-free recurrence, so that
+// a pivot's chain is one reciprocal square root, one product and one fused
+// multiply-add; pivot checks come after the tile.  A non-positive pivot (FP64)
+// records the first failing row and lets NaNs run on, as before.  With pivot
+// floors (mixed precision), a tile that has a pivot at or below its floor is
+// factored again by potrf_tile_floored, whose raised pivots depend on the
+// whole row: speculative (the tile's row block right of it may still be
+// changing) returns false instead, with nothing written.
 template<typename T>
 __device__ bool potrf_diag_tile( const PotrfShared & sh, const PanelTask & t, int q, int nb, const T * __restrict__ arena,
                                  int * __restrict__ status, const double * __restrict__ pivot_floor, bool speculative )
 {
     const int lane = threadIdx.x & 31;
     const int o = kSub * q;
-    const double beta2 = pivot_floor != nullptr ? pivot_floor[0] : 0.0;
-    double a[kSub];
-#pragma unroll
-    for( int r = 0; r < kSub; ++r ) { a[r] = (lane < kSub && r <= lane) ? sh.D[o + r][o + lane] : 0.0; }
+    const unsigned singles = static_cast<unsigned>( (t.single_rows >> o) & 0xff );
+    double a[kSub][kSub], iv[kSub], piv[kSub];
 #pragma unroll
     for( int r = 0; r < kSub; ++r )
     {
-        double d = __shfl_sync( 0xffffffffu, a[r], r );
-        const bool single = (t.single_rows >> (o + r)) & 1;
-        if( single ) { d = fabs( d ); }                     // 1 x 1 reference supernodes: sqrt(|a|)
-        if( pivot_floor != nullptr && o + r < nb )
-        {
-            // mixed precision: a pivot lost to FP32 rounding (for a 1 x 1
-            // supernode too: |a| can cancel to 0) is raised to its floor
-            // (static pivoting); the FP64 refinement corrects it.  The raised
-            // pivot also bounds the row's entries in the block by beta =
-            // sqrt(max |a_ii|), the growth bound of the modified Cholesky of
-            // Gill, Murray and Wright: a small pivot under a large row would
-            // otherwise make the next pivots of the block hugely negative,
-            // floored in turn, until FP32 overflows.
-            const double tau = sh.floor_s[o + r];
-            if( !(d > tau) )
-            {
-                if( speculative ) { return false; }
-                // the row's largest entry: this tile's columns (registers), the
-                // rest of the block (shared memory) and the row's rest columns in
-                // U0 and U1, which the trsm divides by the pivot
-                double m = (lane > r && lane < kSub) ? fabs( a[r] ) : 0.0;
-                for( int c = o + kSub + lane; c < kPanel; c += 32 ) { m = fmax( m, fabs( sh.D[o + r][c] ) ); }
-                const std::int64_t grow = t.r0 + o + r;
-                for( int c = t.r0 + nb + lane; c < t.n0; c += 32 )
-                {
-                    m = fmax( m, fabs( static_cast<double>( arena[t.u0 + grow * t.ld0 + c] ) ) );
-                }
-                for( int c = lane; c < t.n1; c += 32 )
-                {
-                    m = fmax( m, fabs( static_cast<double>( arena[t.u1 + grow * t.ld1 + c] ) ) );
-                }
 #pragma unroll
-                for( int s2 = 16; s2 > 0; s2 >>= 1 ) { m = fmax( m, __shfl_xor_sync( 0xffffffffu, m, s2 ) ); }
-                if( lane == 0 ) { atomicAdd( status + 2, 1 ); }
-                d = fmax( tau, beta2 > 0.0 ? m * m / beta2 : 0.0 );
-            }
-        }
-        if( lane == 0 && !single && o + r < nb && !(d > 0.0) && *sh.fail < 0 ) { *sh.fail = o + r; }
-        // reciprocal square root and one product instead of sqrt and a
-        // division: both are long dependent sequences on the FP64 pipe
-        const double inv = rsqrt( d );
-        const double piv = d * inv;
-        if( lane == r ) { a[r] = piv; }
-        if( lane > r ) { a[r] *= inv; }                     // U(r, lane)
+        for( int c = r; c < kSub; ++c ) { a[r][c] = sh.D[o + r][o + c]; }
+    }
+#pragma unroll
+    for( int r = 0; r < kSub; ++r )
+    {
+        const double d = ((singles >> r) & 1) ? fabs( a[r][r] ) : a[r][r];   // 1 x 1 reference supernodes: sqrt(|a|)
+        piv[r] = d;
+        iv[r] = rsqrt( d );
+        a[r][r] = d * iv[r];
+#pragma unroll
+        for( int c = r + 1; c < kSub; ++c ) { a[r][c] *= iv[r]; }
 #pragma unroll
         for( int r2 = r + 1; r2 < kSub; ++r2 )
         {
-            const double urr2 = __shfl_sync( 0xffffffffu, a[r], r2 );   // U(r, r2)
-            if( lane >= r2 ) { a[r2] -= urr2 * a[r]; }
+#pragma unroll
+            for( int c = r2; c < kSub; ++c ) { a[r2][c] -= a[r][r2] * a[r][c]; }
         }
     }
-#pragma unroll
-    for( int r = 0; r < kSub; ++r ) { a[r] = round_to<T>( a[r] ); }
-    // W = U^{-1}, lane j its column j: w_j = 1 / u_jj, then for k = j, j-1, ..:
-    // w_i = -(sum_{k=i+1..j} u_ik w_k) / u_ii
-    double rec[kSub], w[kSub], sum[kSub];
-#pragma unroll
-    for( int i = 0; i < kSub; ++i ) { rec[i] = 1.0 / __shfl_sync( 0xffffffffu, a[i], i ); sum[i] = 0.0; }
-#pragma unroll
-    for( int k = kSub - 1; k >= 0; --k )
+    if constexpr ( sizeof(T) == 4 )
     {
-        w[k] = lane == k ? rec[k] : (lane > k ? -rec[k] * sum[k] : 0.0);
+        bool low = false;
 #pragma unroll
-        for( int i = 0; i < k; ++i ) { sum[i] += __shfl_sync( 0xffffffffu, a[i], k ) * w[k]; }   // u_ik w_k
+        for( int r = 0; r < kSub; ++r ) { low |= o + r < nb && !(piv[r] > sh.floor_s[o + r]); }
+        if( low && pivot_floor != nullptr )
+        {
+            if( speculative ) { return false; }
+            potrf_tile_floored<T>( sh, t, q, nb, arena, status, pivot_floor );
+            return true;
+        }
     }
-    if( lane < kSub )
+    if( lane == 0 )
     {
 #pragma unroll
         for( int r = 0; r < kSub; ++r )
         {
-            if( r <= lane ) { sh.D[o + r][o + lane] = a[r]; }
-            sh.Ti[o + r][o + lane] = w[r];
+            if( !((singles >> r) & 1) && o + r < nb && !(piv[r] > 0.0) && *sh.fail < 0 ) { *sh.fail = o + r; }
         }
     }
-    __syncwarp();
+    potrf_store_tile( sh, o, a, iv );
     return true;
 }
 
 // Cholesky of one panel's 64 x 64 diagonal block D (identity beyond nb) and
 // the inverse T = D^{-1} of its factor (LAPACK potrf of FactorizeSupernode,
 // Multifrontal.hpp:438-449, plus the inverse the panel's trsm and the solves
-// use).  A row that forms a 1 x 1 reference supernode takes sqrt(|a|) as the
-// reference does (:471) and never reports failure.
-//
-// Right-looking by 8 x 8 tiles with one barrier per tile step b.  Warp 0
-// forms U_{b,b+1}, applies its update to tile (b+1, b+1) and factors that
-// tile ahead (its Cholesky and inverse W_{b+1}); the other warps update the
-// remaining trailing tiles (b2, c), each forming the U_{b,b2} = W_b^T A_{b,b2}
-// and U_{b,c} it needs in its own registers, and form column block b of T,
-// T_ib = -(sum_{k=i..b-1} T_ik U_kb) W_b.  Every 8 x 8 x 8 product runs on
-// the FP64 tensor cores (two DMMA m8n8k4).  With FP32 storage every U value
-// is rounded to FP32 when formed, so the updates and T use the stored factor.
+// use), right-looking by 8 x 8 tiles, two barriers per tile step b:
+//   1. U_bc = U_bb^{-T} A_bc for the columns right of tile b, one column per
+//      thread; one warp forms W_b = U_bb^{-1} (tile (b, b) of T).
+//   2. warp 0 applies row block b's update to tile (b+1, b+1) and factors
+//      that tile ahead; the other warps update the other trailing tiles and
+//      form column block b of T, T_ib = -(sum_{k=i..b-1} T_ik U_kb) W_b.
+// Tile products run on the FP64 tensor cores (two DMMA m8n8k4 each).  A row
+// that forms a 1 x 1 reference supernode takes sqrt(|a|) as the reference
+// does (:471) and never reports failure.  With FP32 storage the block is
+// factored in FP64 and rounded when stored; W and T are formed from the
+// rounded values, so that T inverts the stored factor.
 template<typename T>
 __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict__ arena, int * __restrict__ status,
                                             double * smem, const double * __restrict__ pivot_floor, double * __restrict__ tinv )
@@ -456,7 +481,8 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     PotrfShared sh;
     sh.D = reinterpret_cast<double (*)[kPanel + 1]>( smem );
     sh.Ti = reinterpret_cast<double (*)[kPanel + 1]>( smem + kPanel * (kPanel + 1) );
-    sh.floor_s = smem + 2 * kPanel * (kPanel + 1);      // the panel's pivot floors (mixed precision)
+    sh.inv_d = smem + 2 * kPanel * (kPanel + 1);
+    sh.floor_s = sh.inv_d + kPanel;                     // the panel's pivot floors (mixed precision)
     sh.fail = reinterpret_cast<int *>( sh.floor_s + kPanel );
     sh.redo = sh.fail + 1;
 
@@ -478,76 +504,102 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     const int nsub = (nb + kSub - 1) / kSub;
     if( warp == 0 ) { potrf_diag_tile<T>( sh, t, 0, nb, arena, status, pivot_floor, false ); }
     __syncthreads();
+    const int i8 = lane >> 2, j8 = 2 * (lane & 3);        // this lane's entries of an 8 x 8 DMMA result
     for( int b = 0; b < nsub; ++b )
     {
+        const int o = kSub * b;
         const int rem = nsub - 1 - b;                   // trailing tile rows / columns
+        // 1. row block b right of its diagonal tile; W_b
+        if( tid < kSub * rem )
+        {
+            const int col = o + kSub + tid;
+            double x[kSub];
+#pragma unroll
+            for( int r = 0; r < kSub; ++r ) { x[r] = sh.D[o + r][col]; }
+#pragma unroll
+            for( int r = 0; r < kSub; ++r )
+            {
+                x[r] *= sh.inv_d[o + r];
+#pragma unroll
+                for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= sh.D[o + r][o + r2] * x[r]; }
+            }
+#pragma unroll
+            for( int r = 0; r < kSub; ++r ) { sh.D[o + r][col] = x[r]; }
+        }
+        else if( warp == 7 && lane < kSub )
+        {
+            // column j = lane of W_b: w_jj = 1 / u_jj, w_ij = -(sum_{k=i+1..j} u_ik w_kj) / u_ii
+            const int j = lane;
+            double w[kSub], sum[kSub];
+#pragma unroll
+            for( int i = 0; i < kSub; ++i ) { sum[i] = 0.0; }
+#pragma unroll
+            for( int k = kSub - 1; k >= 0; --k )
+            {
+                w[k] = 0.0;
+                if( k <= j )
+                {
+                    const double rk = 1.0 / round_to<T>( sh.D[o + k][o + k] );
+                    w[k] = k == j ? rk : -rk * sum[k];
+#pragma unroll
+                    for( int i = 0; i < k; ++i ) { sum[i] += round_to<T>( sh.D[o + i][o + k] ) * w[k]; }
+                }
+            }
+#pragma unroll
+            for( int i = 0; i < kSub; ++i ) { sh.Ti[o + i][o + j] = w[i]; }
+        }
+        __syncthreads();
+        // 2. trailing tiles and T's column block b
         if( warp == 0 )
         {
             if( rem > 0 )
             {
-                // U_{b,b+1}: the lower tile (b+1, b) and the update of tile (b+1, b+1)
-                double (*S)[kPanel + 1] = potrf_scratch( sh, 0 );
-                potrf_u_tile<T>( sh, b, b + 1, S );
-                const int i = lane >> 2, j = 2 * (lane & 3);
-                sh.D[kSub * (b + 1) + j][kSub * b + i] = S[i][j];
-                sh.D[kSub * (b + 1) + j + 1][kSub * b + i] = S[i][j + 1];
+                const int o1 = o + kSub;
                 double acc[2] = { 0.0, 0.0 };
-                dmma_8x8x8( acc, [&]( int ii, int k ) { return S[k][ii]; }, [&]( int k, int jj ) { return S[k][jj]; } );
-                sh.D[kSub * (b + 1) + i][kSub * (b + 1) + j] -= acc[0];
-                sh.D[kSub * (b + 1) + i][kSub * (b + 1) + j + 1] -= acc[1];
+                dmma_8x8x8( acc, [&]( int ii, int k ) { return sh.D[o + k][o1 + ii]; }, [&]( int k, int jj ) { return sh.D[o + k][o1 + jj]; } );
+                sh.D[o1 + i8][o1 + j8] -= acc[0];
+                sh.D[o1 + i8][o1 + j8 + 1] -= acc[1];
                 __syncwarp();
                 if( !potrf_diag_tile<T>( sh, t, b + 1, nb, arena, status, pivot_floor, true ) && lane == 0 ) { *sh.redo = 1; }
             }
         }
         else
         {
-            // trailing tiles (b2, c), b < b2 <= c < nsub, but (b+1, b+1); then T's column block b
-            const int tiles = rem * (rem + 1) / 2 - (rem > 0 ? 1 : 0);
-            for( int job = warp - 1; job < tiles + b; job += kPotrfThreads / 32 - 1 )
+            const int tiles = rem * (rem + 1) / 2 - (rem > 0 ? 1 : 0);     // all but (b+1, b+1)
+            // warp 4 shares warp 0's SM sub-partition (warp index mod 4) and
+            // stays idle, so that the tile factorization's FP64 chain does not
+            // wait behind tile products
+            for( int job = warp - (warp < 4 ? 1 : 2); warp != 4 && job < tiles + b; job += kPotrfThreads / 32 - 2 )
             {
-                const int i = lane >> 2, j = 2 * (lane & 3);
                 if( job < tiles )
                 {
-                    // job -> (b2, c) in column-major order of the trailing triangle after (b+1, b+1)
+                    // job -> (b2, c), column by column of the trailing triangle after (b+1, b+1)
                     int c = b + 2, left = job;
                     while( left >= c - b ) { left -= c - b; ++c; }
-                    const int b2 = b + 1 + left;
-                    double (*Sc)[kPanel + 1] = potrf_scratch( sh, 0 );
-                    double (*Sr)[kPanel + 1] = potrf_scratch( sh, 1 );
-                    potrf_u_tile<T>( sh, b, c, Sc );
-                    if( b2 == c )
-                    {
-                        // the tile (c, c) job also stores U_bc into the lower tile (c, b)
-                        sh.D[kSub * c + j][kSub * b + i] = Sc[i][j];
-                        sh.D[kSub * c + j + 1][kSub * b + i] = Sc[i][j + 1];
-                    }
-                    else { potrf_u_tile<T>( sh, b, b2, Sr ); }
-                    double (*Sb)[kPanel + 1] = b2 == c ? Sc : Sr;
+                    const int o2 = kSub * (b + 1 + left), oc = kSub * c;
                     double acc[2] = { 0.0, 0.0 };
-                    dmma_8x8x8( acc, [&]( int ii, int k ) { return Sb[k][ii]; }, [&]( int k, int jj ) { return Sc[k][jj]; } );
-                    sh.D[kSub * b2 + i][kSub * c + j] -= acc[0];
-                    sh.D[kSub * b2 + i][kSub * c + j + 1] -= acc[1];
-                    __syncwarp();
+                    dmma_8x8x8( acc, [&]( int ii, int k ) { return sh.D[o + k][o2 + ii]; }, [&]( int k, int jj ) { return sh.D[o + k][oc + jj]; } );
+                    sh.D[o2 + i8][oc + j8] -= acc[0];
+                    sh.D[o2 + i8][oc + j8 + 1] -= acc[1];
                 }
                 else
                 {
                     // T_ib, i = job - tiles < b
-                    const int ib = job - tiles;
+                    const int oi = kSub * (job - tiles);
                     double acc[2] = { 0.0, 0.0 };
-                    for( int k = ib; k < b; ++k )
+                    for( int ok = oi; ok < o; ok += kSub )
                     {
-                        dmma_8x8x8( acc, [&]( int ii, int kk ) { return sh.Ti[kSub * ib + ii][kSub * k + kk]; },
-                                         [&]( int kk, int jj ) { return sh.D[kSub * b + jj][kSub * k + kk]; } );   // U_kb = (lower tile (b, k))^T
+                        dmma_8x8x8( acc, [&]( int ii, int kk ) { return sh.Ti[oi + ii][ok + kk]; },
+                                         [&]( int kk, int jj ) { return round_to<T>( sh.D[ok + kk][o + jj] ); } );
                     }
-                    double (*S)[kPanel + 1] = potrf_scratch( sh, 0 );
-                    S[i][j] = acc[0];
-                    S[i][j + 1] = acc[1];
+                    double (*S)[kPanel + 1] = potrf_scratch( sh );
+                    S[i8][j8] = acc[0];
+                    S[i8][j8 + 1] = acc[1];
                     __syncwarp();
                     double acc2[2] = { 0.0, 0.0 };
-                    dmma_8x8x8( acc2, [&]( int ii, int k ) { return S[ii][k]; },
-                                      [&]( int k, int jj ) { return sh.Ti[kSub * b + k][kSub * b + jj]; } );
-                    sh.Ti[kSub * ib + i][kSub * b + j] = -acc2[0];
-                    sh.Ti[kSub * ib + i][kSub * b + j + 1] = -acc2[1];
+                    dmma_8x8x8( acc2, [&]( int ii, int k ) { return S[ii][k]; }, [&]( int k, int jj ) { return sh.Ti[o + k][o + jj]; } );
+                    sh.Ti[oi + i8][o + j8] = -acc2[0];
+                    sh.Ti[oi + i8][o + j8 + 1] = -acc2[1];
                     __syncwarp();
                 }
             }
@@ -563,11 +615,10 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
             __syncthreads();
         }
     }
-    // U: the diagonal tiles' upper triangles and the transposed lower tiles
-    for( int idx = tid; idx < nb * nb; idx += kPotrfThreads )
+    for( int idx = tid; idx < kPanel * kPanel; idx += kPotrfThreads )
     {
-        const int r = idx / nb, c = idx % nb;
-        if( r <= c ) { U0[(std::int64_t)r * t.ld0 + c] = static_cast<T>( (r >> 3) == (c >> 3) ? sh.D[r][c] : sh.D[c][r] ); }
+        const int r = idx >> 6, c = idx & 63;
+        if( r <= c && c < nb ) { U0[(std::int64_t)r * t.ld0 + c] = static_cast<T>( sh.D[r][c] ); }
     }
     if( tid == 0 && *sh.fail >= 0 )
     {
@@ -580,13 +631,13 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     double * out = tinv + (std::int64_t)t.panel * (kPanel * kPanel);
     for( int idx = tid; idx < nbp * kPanel; idx += kPotrfThreads )
     {
-        const int r = idx / kPanel, c = idx % kPanel;
+        const int r = idx >> 6, c = idx & 63;
         if( c < nbp ) { out[idx] = (r <= c) ? sh.Ti[r][c] : 0.0; }
     }
 }
 
 template<typename T>
-__global__ __launch_bounds__(kPotrfThreads) void potrf_kernel( const PanelTask * __restrict__ tasks,
+__global__ __launch_bounds__(kPotrfThreads, 1) void potrf_kernel( const PanelTask * __restrict__ tasks,
                                                                T * __restrict__ arena, int * __restrict__ status,
                                                                const double * __restrict__ pivot_floor,
                                                                double * __restrict__ tinv )
