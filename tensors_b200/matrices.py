@@ -179,7 +179,7 @@ def delaunay_laplacian(m: int, seed: int, shift: float = 1e-3) -> CSRMatrix:
     return _cotangent_laplacian(pts, tri, shift, {"kind": "delaunay", "m": m, "seed": seed, "shift": shift})
 
 
-def _cotangent_laplacian(pts, tri, shift, meta) -> CSRMatrix:
+def _cotangent_laplacian(pts, tri, shift, meta, relative: bool = False) -> CSRMatrix:
     m = len(pts)
     P = pts[tri]                                  # (t, 3, 2)
     rows, cols, vals = [], [], []
@@ -202,15 +202,18 @@ def _cotangent_laplacian(pts, tri, shift, meta) -> CSRMatrix:
         np.add.at(mass, tri[:, k], area / 3.0)
     rows.append(np.arange(m))
     cols.append(np.arange(m))
-    vals.append(shift * mass)
+    vals.append(shift * mass / (mass.mean() if relative else 1.0))
     return from_coo(m, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals), coords=pts, meta=meta)
 
 
-def mesh_laplacian(m: int, seed: int, shift: float = 1e-3) -> CSRMatrix:
+def mesh_laplacian(m: int, seed: int, shift: float = 1e-3, relative: bool = False) -> CSRMatrix:
     """Cotangent Laplacian + shift * lumped mass of a quality 2D mesh: the Delaunay
     triangulation of about m points on a jittered grid (every point moved by up to
     a quarter cell), which keeps the angles bounded away from 0 and pi -- unlike
-    uniform random points, whose hull slivers give cotangent weights of ~1e6."""
+    uniform random points, whose hull slivers give cotangent weights of ~1e6.
+    relative: the lumped mass is scaled to mean 1, so the diagonal shift averages
+    `shift` at any resolution (an absolute shift times a mass of ~1/m makes kappa
+    grow like m / shift)."""
     from scipy.spatial import Delaunay
 
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -219,7 +222,8 @@ def mesh_laplacian(m: int, seed: int, shift: float = 1e-3) -> CSRMatrix:
     yy, xx = np.meshgrid(np.arange(g) * h, np.arange(g) * h, indexing="ij")
     pts = np.stack([xx.ravel(), yy.ravel()], 1) + rng.uniform(-0.25 * h, 0.25 * h, size=(g * g, 2))
     tri = Delaunay(pts).simplices.astype(np.int64)
-    return _cotangent_laplacian(pts, tri, shift, {"kind": "mesh", "m": g * g, "seed": seed, "shift": shift})
+    return _cotangent_laplacian(pts, tri, shift, {"kind": "mesh", "m": g * g, "seed": seed, "shift": shift,
+                                                  "relative": relative}, relative)
 
 
 def csr_matvec(A: CSRMatrix, X: np.ndarray) -> np.ndarray:
