@@ -132,6 +132,11 @@ class CholeskyDecomposition:
         self._perm = None if perm is None else np.ascontiguousarray(perm, dtype=np.int32)
         if self._perm is not None and self._perm.shape != (self._n,):
             raise TBError(-1, "permutation has the wrong length")
+        # the C-ABI reads outer[0..n] and inner[0..outer[n]): the arrays must hold that many
+        if self._n < 0 or len(self._outer) < self._n + 1:
+            raise TBError(-1, "row pointers shorter than n + 1")
+        if self._n > 0 and not (0 <= int(self._outer[self._n]) <= len(self._inner)):
+            raise TBError(-2, "row pointers run past the column indices")
         h = ctypes.c_void_p()
         _check(lib().tb_chol_create(ctypes.byref(h), self._n, self._outer.ctypes.data, self._inner.ctypes.data,
                                     None if self._perm is None else self._perm.ctypes.data, int(thread_count)))
@@ -725,6 +730,10 @@ class BatchedCholesky:
             o = np.ascontiguousarray(outer, dtype=np.int64)
             i = np.ascontiguousarray(inner, dtype=np.int32)
             n[s] = len(o) - 1
+            if n[s] > 0 and not (0 <= int(o[-1]) <= len(i)):
+                raise TBError(-2, f"system {s}: row pointers run past the column indices")
+            if perm is not None and len(perm) != n[s]:
+                raise TBError(-1, f"system {s}: permutation has the wrong length")
             outer_p[s] = o.ctypes.data
             inner_p[s] = i.ctypes.data
             self._keep += [o, i]

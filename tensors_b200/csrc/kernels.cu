@@ -9,7 +9,9 @@
 
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <climits>
+#include <type_traits>
 
 namespace tb
 {
@@ -1632,82 +1634,116 @@ __global__ void scatter_rows_kernel( const double * __restrict__ W, int ldw, con
 }
 
 // R = B - A X, one warp per row, lanes over the row's entries.
-__global__ void residual_kernel( int n, const std::int64_t * __restrict__ outer, const std::int32_t * __restrict__ inner,
-                                 const double * __restrict__ vals, const double * __restrict__ X,
-                                 const double * __restrict__ B, double * __restrict__ R, int k )
-{
-    const int lane = threadIdx.x & 31;
-    const std::int64_t warp = (blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x) >> 5;
-    const std::int64_t warps = ((std::int64_t)gridDim.x * blockDim.x) >> 5;
-    for( std::int64_t i = warp; i < n; i += warps )
-    {
-        for( int c = 0; c < k; ++c )
-        {
-            double s = 0.0;
-            for( std::int64_t e = outer[i] + lane; e < outer[i+1]; e += 32 ) { s += vals[e] * X[(std::int64_t)inner[e] * k + c]; }
-#pragma unroll
-            for( int o = 16; o > 0; o >>= 1 ) { s += __shfl_xor_sync( 0xffffffffu, s, o ); }
-            if( lane == 0 ) { R[i * k + c] = B[i * k + c] - s; }
-        }
-    }
-}
-
 // R = B - (A + shift I) X (B != nullptr) or R = (A + shift I) X (B == nullptr)
-// for row-major blocks with leading dimensions: one warp per row, lanes over
-// the row's entries, 8 right-hand sides per pass over the row.
-__global__ void apply_shifted_kernel( int n, const std::int64_t * __restrict__ outer, const std::int32_t * __restrict__ inner,
-                                      const double * __restrict__ vals, double shift,
-                                      const double * __restrict__ X, int ldx, const double * __restrict__ B, int ldb,
-                                      double * __restrict__ R, int ldr, int k )
+// for row-major blocks with leading dimensions.  One warp per row: the lanes
+// form 32 / KP groups of KP columns (KP = k rounded up to a power of two, at
+// most 32); group g takes the row's entries g, g + G, ... (one broadcast load
+// of the entry, one contiguous load of KP values of x's row), the groups'
+// sums meet by log2(G) shuffles, and group 0 writes the row.  Blocks of 32
+// columns when k > 32.
+template<int KP>
+__global__ __launch_bounds__(256) void spmv_rows_kernel( int n, const std::int64_t * __restrict__ outer, const std::int32_t * __restrict__ inner,
+                                                         const double * __restrict__ vals, double shift,
+                                                         const double * __restrict__ X, int ldx, const double * __restrict__ B, int ldb,
+                                                         double * __restrict__ R, int ldr, int k )
 {
+    constexpr int G = 32 / KP;
     const int lane = threadIdx.x & 31;
+    const int g = lane / KP, c = lane % KP;
     const std::int64_t warp = (blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x) >> 5;
     const std::int64_t warps = ((std::int64_t)gridDim.x * blockDim.x) >> 5;
     for( std::int64_t i = warp; i < n; i += warps )
     {
-        for( int c0 = 0; c0 < k; c0 += 8 )
+        const std::int64_t e0 = outer[i], e1 = outer[i + 1];
+        for( int c0 = 0; c0 < k; c0 += KP )
         {
-            double s[8] = { 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0 };
-            for( std::int64_t e = outer[i] + lane; e < outer[i+1]; e += 32 )
+            const int col = c0 + c;
+            const bool live = col < k;
+            double s = 0.0;
+#pragma unroll 4
+            for( std::int64_t e = e0 + g; e < e1; e += G )
             {
                 const double v = vals[e];
-                const double * xr = X + (std::int64_t)inner[e] * ldx;
-#pragma unroll
-                for( int u = 0; u < 8; ++u ) { if( c0 + u < k ) { s[u] += v * xr[c0 + u]; } }
+                const std::int64_t j = inner[e];
+                if( live ) { s = fma( v, X[j * ldx + col], s ); }
             }
 #pragma unroll
-            for( int u = 0; u < 8; ++u )
+            for( int o = KP; o < 32; o <<= 1 ) { s += __shfl_xor_sync( 0xffffffffu, s, o ); }
+            if( g == 0 && live )
             {
-#pragma unroll
-                for( int o = 16; o > 0; o >>= 1 ) { s[u] += __shfl_xor_sync( 0xffffffffu, s[u], o ); }
-            }
-            if( lane < 8 && c0 + lane < k )
-            {
-                double v = 0.0;
-#pragma unroll
-                for( int u = 0; u < 8; ++u ) { if( u == lane ) { v = s[u]; } }
-                const int c = c0 + lane;
-                const double ax = v + shift * X[i * ldx + c];
-                R[i * ldr + c] = B ? B[i * ldb + c] - ax : ax;
+                const double ax = s + shift * X[i * ldx + col];
+                R[i * ldr + col] = B ? B[i * ldb + col] - ax : ax;
             }
         }
     }
 }
 
-// out[c] += sum_i X[i][c] Y[i][c] (out zeroed by the caller).
-__global__ void column_dots_kernel( const double * __restrict__ X, int ldx, const double * __restrict__ Y, int ldy,
-                                    int n, int k, double * __restrict__ out )
+// The same product for k >= 3: a group of KP lanes takes a whole row (KP
+// columns of it, blocks of 32 when k > 32), 32 / KP rows per warp, with no
+// cross-lane sum; the rows a warp holds together are consecutive, so rows
+// with the same pattern (the dofs of one node) share their x loads in L1.
+template<int KP>
+__global__ __launch_bounds__(256) void spmv_group_kernel( int n, const std::int64_t * __restrict__ outer, const std::int32_t * __restrict__ inner,
+                                                          const double * __restrict__ vals, double shift,
+                                                          const double * __restrict__ X, int ldx, const double * __restrict__ B, int ldb,
+                                                          double * __restrict__ R, int ldr, int k )
 {
-    for( int c = 0; c < k; ++c )
+    constexpr int G = 32 / KP;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / KP, c = lane % KP;
+    const std::int64_t grp = ((blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x) >> 5) * G + g;
+    const std::int64_t groups = (((std::int64_t)gridDim.x * blockDim.x) >> 5) * G;
+    for( std::int64_t i = grp; i < n; i += groups )
     {
-        double s = 0.0;
-        for( std::int64_t i = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; i < n; i += (std::int64_t)gridDim.x * blockDim.x )
+        const std::int64_t e0 = outer[i], e1 = outer[i + 1];
+        for( int c0 = 0; c0 < k; c0 += KP )
         {
-            s += X[i * ldx + c] * Y[i * ldy + c];
+            const int col = c0 + c;
+            if( col >= k ) { continue; }
+            double s = 0.0;
+#pragma unroll 8
+            for( std::int64_t e = e0; e < e1; ++e ) { s = fma( vals[e], X[(std::int64_t)inner[e] * ldx + col], s ); }
+            const double ax = s + shift * X[i * ldx + col];
+            R[i * ldr + col] = B ? B[i * ldb + col] - ax : ax;
+        }
+    }
+}
+
+// out[c] += sum_i X[i][c] Y[i][c] (out zeroed by the caller).  The lanes form
+// groups of KP columns as in spmv_rows_kernel, so that a warp reads whole
+// rows; per block the columns' sums meet in shared memory and go out with one
+// atomic addition per column.
+template<int KP>
+__global__ __launch_bounds__(256) void column_dots_kernel( const double * __restrict__ X, int ldx, const double * __restrict__ Y, int ldy,
+                                                           int n, int k, double * __restrict__ out )
+{
+    constexpr int G = 32 / KP;
+    __shared__ double part[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / KP, c = lane % KP;
+    const std::int64_t gw = (blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x) >> 5;
+    const std::int64_t warps = ((std::int64_t)gridDim.x * blockDim.x) >> 5;
+    for( int c0 = 0; c0 < k; c0 += KP )
+    {
+        const int col = c0 + c;
+        double s = 0.0;
+        if( col < k )
+        {
+#pragma unroll 4
+            for( std::int64_t i = gw * G + g; i < n; i += warps * G ) { s = fma( X[i * ldx + col], Y[i * ldy + col], s ); }
         }
 #pragma unroll
-        for( int o = 16; o > 0; o >>= 1 ) { s += __shfl_xor_sync( 0xffffffffu, s, o ); }
-        if( (threadIdx.x & 31) == 0 && s != 0.0 ) { atomicAdd( out + c, s ); }
+        for( int o = KP; o < 32; o <<= 1 ) { s += __shfl_xor_sync( 0xffffffffu, s, o ); }
+        if( g == 0 ) { part[warp][c] = s; }
+        __syncthreads();
+        if( threadIdx.x < KP && c0 + threadIdx.x < k )
+        {
+            double t = 0.0;
+#pragma unroll
+            for( int w = 0; w < 8; ++w ) { t += part[w][threadIdx.x]; }
+            if( t != 0.0 ) { atomicAdd( out + c0 + threadIdx.x, t ); }
+        }
+        __syncthreads();
     }
 }
 
@@ -1894,7 +1930,7 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int i = task.i, j = task.j;
     const int nbi = super_block_rows( sp, i );
-    double * out = tbuf + sp.t + (std::int64_t)(kPanel * i) * kSuperRows + kPanel * j;
+    double * out = tbuf + sp.t + (std::int64_t)(kPanel * i) * sp.ldt + kPanel * j;
     auto load_tinv = [&]( double (*D)[kSld], int b, int nbb )
     {
         const double * src = tinv + (std::int64_t)sp.panel[b] * (kPanel * kPanel);
@@ -1908,7 +1944,7 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     {
         load_tinv( Tii, i, nbi );
         __syncthreads();
-        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { out[(idx >> 6) * kSuperRows + (idx & 63)] = Tii[idx >> 6][idx & 63]; }
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { out[(idx >> 6) * sp.ldt + (idx & 63)] = Tii[idx >> 6][idx & 63]; }
         return;
     }
     double acc[8][2];
@@ -1918,7 +1954,7 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     for( int k = i + 1; k <= j; ++k )
     {
         const int nbk = super_block_rows( sp, k );
-        const double * tk = tbuf + sp.t + (std::int64_t)(kPanel * k) * kSuperRows + kPanel * j;
+        const double * tk = tbuf + sp.t + (std::int64_t)(kPanel * k) * sp.ldt + kPanel * j;
         auto src = [&]( int idx, double & fill ) -> const T *
         {
             fill = 0.0;
@@ -1929,7 +1965,7 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
         stage_block<T, kPanel * kPanel / 256, 256>( U0, src, dst );
         // T_kj is zero outside its valid rows and columns
 #pragma unroll 4
-        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { cp_async_8( &Bm[idx >> 6][idx & 63], tk + (idx >> 6) * kSuperRows + (idx & 63), true ); }
+        for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { cp_async_8( &Bm[idx >> 6][idx & 63], tk + (idx >> 6) * sp.ldt + (idx & 63), true ); }
         cp_async_wait_all();
         stage_finish<T, kPanel * kPanel / 256, 256>( src, dst );
         __syncthreads();
@@ -1950,8 +1986,8 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     for( int ct = 0; ct < 8; ++ct )
     {
         const int r = 8 * warp + (lane >> 2), c = 8 * ct + 2 * (lane & 3);
-        out[r * kSuperRows + c] = -acc[ct][0];
-        out[r * kSuperRows + c + 1] = -acc[ct][1];
+        out[r * sp.ldt + c] = -acc[ct][0];
+        out[r * sp.ldt + c + 1] = -acc[ct][1];
     }
 }
 
@@ -1997,10 +2033,10 @@ __global__ __launch_bounds__(256) void super_diag_kernel( const SuperSolveTask *
     const std::int64_t brow = (std::int64_t)sp.row0 + sp.r0;
     // forward: block (b, o) of T, read transposed; back: block (o, b).  The
     // blocks are zero outside their valid rows and columns.
-    const double * tb = upper ? tbuf + sp.t + (std::int64_t)(kPanel * o) * kSuperRows + kPanel * b
-                              : tbuf + sp.t + (std::int64_t)(kPanel * b) * kSuperRows + kPanel * o;
+    const double * tb = upper ? tbuf + sp.t + (std::int64_t)(kPanel * o) * sp.ldt + kPanel * b
+                              : tbuf + sp.t + (std::int64_t)(kPanel * b) * sp.ldt + kPanel * o;
 #pragma unroll 4
-    for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { cp_async_8( &Tb[idx >> 6][idx & 63], tb + (idx >> 6) * kSuperRows + (idx & 63), true ); }
+    for( int idx = tid; idx < kPanel * kPanel; idx += 256 ) { cp_async_8( &Tb[idx >> 6][idx & 63], tb + (idx >> 6) * sp.ldt + (idx & 63), true ); }
     pdl_wait();
     stage_rows<KP>( V, in, brow + kPanel * b, nbb, ld, k );
     if( upper ) { stage_rows<KP>( Z, zbuf, brow + kPanel * b, nbb, ld, k ); }
@@ -2390,10 +2426,21 @@ void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv,
     scatter_rows_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( W, ldw, p_inv, alpha, beta, Y, ldY, n, k );
 }
 
+template<typename Launch>
+static void by_column_width( int k, Launch launch )
+{
+    if( k <= 1 ) { launch( std::integral_constant<int, 1>{} ); }
+    else if( k <= 2 ) { launch( std::integral_constant<int, 2>{} ); }
+    else if( k <= 4 ) { launch( std::integral_constant<int, 4>{} ); }
+    else if( k <= 8 ) { launch( std::integral_constant<int, 8>{} ); }
+    else if( k <= 16 ) { launch( std::integral_constant<int, 16>{} ); }
+    else { launch( std::integral_constant<int, 32>{} ); }
+}
+
 void launch_residual( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
                       const double * X, const double * B, double * R, int k, cudaStream_t st )
 {
-    residual_kernel<<<grid_for( (std::int64_t)n * 32, 256 ), 256, 0, st>>>( n, outer, inner, vals, X, B, R, k );
+    launch_apply_shifted( n, outer, inner, vals, 0.0, X, k, B, k, R, k, k, st );
 }
 
 cudaError_t configure_kernels()
@@ -2450,13 +2497,33 @@ void launch_apply_shifted( int n, const std::int64_t * outer, const std::int32_t
                            double shift, const double * X, int ldx, const double * B, int ldb, double * R, int ldr,
                            int k, cudaStream_t st )
 {
-    apply_shifted_kernel<<<grid_for( (std::int64_t)n * 32, 256 ), 256, 0, st>>>( n, outer, inner, vals, shift, X, ldx,
-                                                                                B, ldb, R, ldr, k );
+    if( n <= 0 ) { return; }
+    if( k >= 3 )
+    {
+        // 8 blocks per SM (measured best on a 3-dof 27-point stencil)
+        const int grid = static_cast<int>( std::min<std::int64_t>( 148 * 8, ((std::int64_t)n * 32 + 255) / 256 ) );
+        by_column_width( k, [&]( auto kp ) {
+            if constexpr ( decltype( kp )::value >= 4 )
+            {
+                spmv_group_kernel<decltype( kp )::value><<<grid, 256, 0, st>>>( n, outer, inner, vals, shift, X, ldx, B, ldb, R, ldr, k );
+            }
+        } );
+        return;
+    }
+    const int grid = grid_for( (std::int64_t)n * 32, 256 );
+    by_column_width( k, [&]( auto kp ) {
+        spmv_rows_kernel<decltype( kp )::value><<<grid, 256, 0, st>>>( n, outer, inner, vals, shift, X, ldx, B, ldb, R, ldr, k );
+    } );
 }
 
 void launch_column_dots( const double * X, int ldx, const double * Y, int ldy, int n, int k, double * out, cudaStream_t st )
 {
-    column_dots_kernel<<<grid_for( n, 256 ), 256, 0, st>>>( X, ldx, Y, ldy, n, k, out );
+    if( n <= 0 ) { return; }
+    // two blocks per SM: few atomics per column, every row read once
+    const int grid = static_cast<int>( std::min<std::int64_t>( 296, ((std::int64_t)n + 255) / 256 ) );
+    by_column_width( k, [&]( auto kp ) {
+        column_dots_kernel<decltype( kp )::value><<<grid, 256, 0, st>>>( X, ldx, Y, ldy, n, k, out );
+    } );
 }
 
 void launch_cg_update_xr( int n, int k, const double * rz, const double * pq, const double * p, const double * q,

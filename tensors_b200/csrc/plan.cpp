@@ -859,6 +859,7 @@ void Plan::build_super( const std::vector<std::vector<I32>> & front_panels, Rang
             sp.t = super_inv_size;
             sp.n0 = front_n0[f]; sp.n1 = front_n1[f]; sp.ld0 = front_ld0[f]; sp.ld1 = front_ld1[f];
             sp.r0 = r0; sp.rows = std::min( kSuperRows, front_n0[f] - r0 ); sp.row0 = front_row0[f];
+            sp.ldt = kPanel * static_cast<I32>( ceil_div( sp.rows, kPanel ) );
             for( I32 b = 0; b < kSuperPanels; ++b )
             {
                 const size_t q = static_cast<size_t>( r0 / kPanel + b );
@@ -866,7 +867,7 @@ void Plan::build_super( const std::vector<std::vector<I32>> & front_panels, Rang
             }
             front_sp[static_cast<size_t>(f)].push_back( static_cast<I32>( spanels.size() ) );
             spanels.push_back( sp );
-            super_inv_size += static_cast<I64>( kSuperRows ) * kSuperRows;
+            super_inv_size += static_cast<I64>( sp.ldt ) * sp.ldt;
         }
     }
     if( spanels.empty() ) { return; }
@@ -979,8 +980,13 @@ void Plan::build_solve_graph( const Symbolic & sym, I32 split )
     {
         if( L.level >= solve_split_level ) { solve_first_task = std::min( solve_first_task, L.first ); }
     }
-    solve_first_panel = solve_first_task < static_cast<I64>( srest.size() ) ? srest[static_cast<size_t>( solve_first_task )].panel
-                                                                            : static_cast<I32>( sdiag.size() );
+    // the lowest panel of the graph's tasks (the super-panel lists reorder the tasks inside a
+    // (level, step) range, so the first task need not hold it)
+    solve_first_panel = static_cast<I32>( sdiag.size() );
+    for( I64 t = solve_first_task; t < static_cast<I64>( srest.size() ); ++t )
+    {
+        solve_first_panel = std::min( solve_first_panel, srest[static_cast<size_t>( t )].panel );
+    }
     const I64 nt = static_cast<I64>( srest.size() ) - solve_first_task;
     const I32 np = static_cast<I32>( sdiag.size() ) - solve_first_panel;
     solve_target_ptr.assign( static_cast<size_t>( nt ) + 1, 0 );

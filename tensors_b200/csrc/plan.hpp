@@ -216,17 +216,17 @@ enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3,
 // super-panels when it has at least kSuperMinRows pivot rows.
 constexpr int kSuperPanels  = 8;
 constexpr int kSuperRows    = kSuperPanels * kPanel;   // 512
-constexpr int kSuperMinRows = 1024;
+constexpr int kSuperMinRows = 256;
 
 struct SuperPanel
 {
     std::int64_t u0, u1, inner;    // the front's U0 / U1 arena offsets and its SN_inner offset
-    std::int64_t t;                // offset of the inverse (kSuperRows x kSuperRows doubles)
+    std::int64_t t;                // offset of the inverse (ldt x ldt doubles, row-major)
     std::int32_t n0, n1, ld0, ld1;
     std::int32_t r0, rows;         // first pivot row of the block (a multiple of 512) and its row count
     std::int32_t row0;             // the front's first global row
     std::int32_t panel[kSuperPanels];   // inverse-block index of each 64-row panel (-1 beyond rows)
-    std::int32_t pad;
+    std::int32_t ldt;              // the inverse's edge: rows rounded up to 64
 };
 
 // Block (i, j = i + d) of a super-panel's inverse, formed in round d:

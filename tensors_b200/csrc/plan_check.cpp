@@ -411,7 +411,8 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             if( sp.n1 > 0 && !in_range( sp.u1, sp.u1 + static_cast<I64>( sp.n0 ) * sp.ld1 - 1, arena ) ) { return "super-panel U1 out of range" + at; }
             if( sp.n1 > 0 && (sp.inner < 0 || sp.inner + sp.n1 > inner_size) ) { return "super-panel columns out of range" + at; }
             if( sp.row0 < 0 || sp.row0 + sp.n0 > sym.n ) { return "super-panel rows out of the matrix" + at; }
-            if( sp.t < 0 || sp.t + static_cast<I64>( kSuperRows ) * kSuperRows > pl.super_inv_size ) { return "super-panel inverse out of range" + at; }
+            if( sp.ldt != kPanel * ((sp.rows + kPanel - 1) / kPanel) ) { return "super-panel inverse edge" + at; }
+            if( sp.t < 0 || sp.t + static_cast<I64>( sp.ldt ) * sp.ldt > pl.super_inv_size ) { return "super-panel inverse out of range" + at; }
             nblk[static_cast<size_t>( p )] = (sp.rows + kPanel - 1) / kPanel;
             nrest[static_cast<size_t>( p )] = (sp.n0 - sp.r0 - sp.rows) + sp.n1;
             for( I32 b = 0; b < kSuperPanels; ++b )

@@ -1,4 +1,4 @@
-"""The super-panel solve of large fronts: fronts with at least 1024 pivot rows step through
+"""The super-panel solve of large fronts: fronts with at least 256 pivot rows step through
 their rows 512 at a time with the inverse of each 512 x 512 diagonal block (formed after the
 factorization from the 64-row panel inverses).  On the CPU: the plan has super-panels for such
 fronts, and the checked launch lists cover every task once.  On the GPU: solves match the oracle
