@@ -153,6 +153,8 @@ struct tb_chol
     tb::ImageMap                    img_map{};   // its tensor map
     DeviceArray<tb::PanelTask>      potrf, panel;
     DeviceArray<tb::ExtendTask>     extend;
+    DeviceArray<tb::ExtendPullTask> extend_pull;
+    DeviceArray<tb::ExtendTask>     extend_segs;
     DeviceArray<tb::SolveDiagTask>  sdiag;
     DeviceArray<tb::SolveRestTask>  srest;
     DeviceArray<tb::SuperPanel>     spanels;     // super-panel solve of the large fronts (Plan::spanels)
@@ -388,6 +390,8 @@ int ensure_device( tb_chol * h )
     TB_TRY( h->potrf.upload( pl.potrf, st_ ) );
     TB_TRY( h->panel.upload( pl.panel, st_ ) );
     TB_TRY( h->extend.upload( pl.extend, st_ ) );
+    TB_TRY( h->extend_pull.upload( pl.extend_pull, st_ ) );
+    TB_TRY( h->extend_segs.upload( pl.extend_segs, st_ ) );
     TB_TRY( h->sdiag.upload( pl.sdiag, st_ ) );
     TB_TRY( h->srest.upload( pl.srest, st_ ) );
     TB_TRY( h->spanels.upload( pl.spanels, st_ ) );
@@ -500,6 +504,9 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
             {
                 case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, st ); break;
                 case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, st ); break;
+                case tb::LaunchKind::ExtendPull:
+                    tb::launch_extend_pull( h->extend_pull.ptr + L.first, L.count, h->extend_segs.ptr, h->lut.ptr, A, st );
+                    break;
                 case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, h->tinv.ptr, st ); break;
                 case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, st, img ); break;
                 case tb::LaunchKind::Gemm:   issue_gemm( h, L, A, st ); break;
@@ -568,13 +575,16 @@ std::int64_t issue_factor_t( tb_chol * h, bool timed, std::vector<int> * kinds )
         {
             case tb::LaunchKind::Zero:   tb::launch_zero( h->zero.ptr + L.first, L.count, A, s ); break;
             case tb::LaunchKind::Extend: tb::launch_extend( h->extend.ptr + L.first, L.count, h->lut.ptr, A, s ); break;
+            case tb::LaunchKind::ExtendPull:
+                tb::launch_extend_pull( h->extend_pull.ptr + L.first, L.count, h->extend_segs.ptr, h->lut.ptr, A, s );
+                break;
             case tb::LaunchKind::Potrf:  tb::launch_potrf( h->potrf.ptr + L.first, L.count, A, h->status.ptr, floor, h->tinv.ptr, s ); break;
             case tb::LaunchKind::Trsm:   tb::launch_trsm( h->panel.ptr + L.first, L.count, A, h->tinv.ptr, s, img ); break;
             case tb::LaunchKind::Gemm:   issue_gemm( h, L, A, s ); break;
             default: break;
         }
         if( overlap && L.kind == tb::LaunchKind::Trsm ) { cudaEventRecord( h->ev_trsm, st ); }
-        mark( static_cast<int>( L.kind ) );
+        mark( static_cast<int>( L.kind == tb::LaunchKind::ExtendPull ? tb::LaunchKind::Extend : L.kind ) );
         ++launches;
     }
     if( overlap ) { join(); }
@@ -2121,7 +2131,8 @@ int tb_chol_device_bytes( tb_chol * h, std::int64_t * out )
     b += h->arena.size * 8 + h->asm_src.size * 8 + h->asm_dst.size * 8 + h->diag_off.size * 8;
     b += (h->lut.size + h->sn_inner.size + h->p.size + h->p_inv.size + h->a_inner.size) * 4;
     b += h->gemm.size * (std::int64_t)sizeof(tb::GemmTask) + (h->panel.size + h->potrf.size) * (std::int64_t)sizeof(tb::PanelTask);
-    b += h->extend.size * (std::int64_t)sizeof(tb::ExtendTask) + h->sdiag.size * (std::int64_t)sizeof(tb::SolveDiagTask);
+    b += (h->extend.size + h->extend_segs.size) * (std::int64_t)sizeof(tb::ExtendTask) + h->sdiag.size * (std::int64_t)sizeof(tb::SolveDiagTask);
+    b += h->extend_pull.size * (std::int64_t)sizeof(tb::ExtendPullTask);
     b += h->srest.size * (std::int64_t)sizeof(tb::SolveRestTask) + h->a_outer.size * 8;
     b += h->zero.size * (std::int64_t)sizeof(tb::ZeroTask) + h->exports.size * (std::int64_t)sizeof(tb::ExportTask);
     b += h->colmap.size * 4 + h->exported.size * 8;
@@ -2493,7 +2504,7 @@ int tb_chol_launch_profile( tb_chol * h, std::int64_t * info, double * ms, std::
         else if( info )
         {
             const tb::Launch & L = h->plan.factor_launches[static_cast<size_t>( i - 1 )];
-            info[4 * i + 0] = static_cast<std::int64_t>( L.kind );
+            info[4 * i + 0] = static_cast<std::int64_t>( L.kind == tb::LaunchKind::ExtendPull ? tb::LaunchKind::Extend : L.kind );
             info[4 * i + 1] = L.level;
             info[4 * i + 2] = L.step;
             info[4 * i + 3] = L.count;

@@ -200,7 +200,7 @@ __global__ void export_kernel( const ExportTask * __restrict__ tasks, const std:
 // ------------------------------------------------------------- extend-add
 // One warp per row of the child's update W; lanes walk the row's upper part
 // (coalesced reads of W, lut-indexed adds into the parent front).
-template<typename T>
+template<typename T, bool kPlainAdd = false>
 __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::int32_t * __restrict__ lut_all,
                                              T * __restrict__ arena )
 {
@@ -238,8 +238,20 @@ __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::in
                     dst[u] = upper_part ? ((j < t.mid) ? row0 + lj : row1 + lj) : rowv + lj;
                 }
             }
+            if constexpr ( kPlainAdd )
+            {
+                // one CTA owns the targets (extend_pull_kernel): load, add, store
+                T old[kU];
 #pragma unroll
-            for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
+                for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : T( 0 ); }
+#pragma unroll
+                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { *dst[u] = old[u] + v[u]; } }
+            }
+            else
+            {
+#pragma unroll
+                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
+            }
         }
     }
 }
@@ -253,6 +265,24 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
     const ExtendTask t = tasks[blockIdx.x];
     pdl_wait();
     extend_body( t, lut_all, arena );
+}
+
+// Extend-add by parent rows (ExtendPullTask): the CTA adds its segments one
+// child after the other; the barrier between two children orders their
+// additions into the rows they share, so every entry gets the sum of the
+// passes by child rank, in the same order.
+template<typename T>
+__global__ __launch_bounds__(256) void extend_pull_kernel( const ExtendPullTask * __restrict__ tasks, const ExtendTask * __restrict__ segs,
+                                                           const std::int32_t * __restrict__ lut_all, T * __restrict__ arena )
+{
+    pdl_allow_next();
+    const ExtendPullTask t = tasks[blockIdx.x];
+    pdl_wait();
+    for( std::int64_t g = t.seg_first; g < t.seg_first + t.seg_count; ++g )
+    {
+        if( g > t.seg_first ) { __syncthreads(); }
+        extend_body<T, true>( segs[g], lut_all, arena );
+    }
 }
 
 // TF32 rounding (round to nearest, ties away) of an FP32 value, as bits.
@@ -2196,6 +2226,13 @@ void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lu
 }
 
 template<typename T>
+void launch_extend_pull( const ExtendPullTask * tasks, int count, const ExtendTask * segs, const std::int32_t * lut, T * arena,
+                         cudaStream_t st )
+{
+    if( count > 0 ) { launch_pdl( extend_pull_kernel<T>, count, 256, 0, st, tasks, segs, lut, arena ); }
+}
+
+template<typename T>
 void launch_potrf( const PanelTask * tasks, int count, T * arena, int * status, const double * pivot_floor, double * tinv,
                    cudaStream_t st )
 {
@@ -2397,6 +2434,7 @@ void launch_gather_diag( const std::int64_t * offsets, const T * arena, double *
     template void launch_export<T>( const ExportTask *, int, const std::int32_t *, const T *, double *, double *,    \
                                     cudaStream_t );                                                                \
     template void launch_extend<T>( const ExtendTask *, int, const std::int32_t *, T *, cudaStream_t );             \
+    template void launch_extend_pull<T>( const ExtendPullTask *, int, const ExtendTask *, const std::int32_t *, T *, cudaStream_t ); \
     template void launch_potrf<T>( const PanelTask *, int, T *, int *, const double *, double *, cudaStream_t );     \
     template void launch_trsm<T>( const PanelTask *, int, T *, const double *, cudaStream_t, float * );              \
     template void launch_gemm<T>( const GemmTask *, int, T *, int *, cudaStream_t );                                 \

@@ -24,6 +24,10 @@ template<typename T>
 void launch_export( const ExportTask * tasks, int count, const std::int32_t * colmap, const T * arena,
                     double * tri, double * rec, cudaStream_t st );
 template<typename T> void launch_extend( const ExtendTask * tasks, int count, const std::int32_t * lut, T * arena, cudaStream_t st );
+// Extend-add by parent rows (plan.hpp, ExtendPullTask): one launch per level.
+template<typename T>
+void launch_extend_pull( const ExtendPullTask * tasks, int count, const ExtendTask * segs, const std::int32_t * lut, T * arena,
+                         cudaStream_t st );
 // pivot_floor (mixed precision only, else null): element 0 the largest |a_ii|,
 // element 1 + i the value a non-positive or lost pivot of permuted row i is
 // raised to instead of failing; status[2] counts them.

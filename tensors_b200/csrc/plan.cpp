@@ -401,6 +401,7 @@ void Plan::build( const Symbolic & sym )
 
     // -------------------------------------------------- launch sequences
     gemm.clear(); tc.clear(); potrf.clear(); panel.clear(); extend.clear(); zero.clear(); sdiag.clear(); srest.clear();
+    extend_pull.clear(); extend_segs.clear();
     gemm_flops = 0.0;
     gemm_tile_flops = 0.0;
     factor_launches.clear(); lower_launches.clear(); upper_launches.clear();
@@ -487,6 +488,7 @@ void Plan::build( const Symbolic & sym )
         // no two tasks of a pass touch the same parent entries)
         I32 max_children = 0;
         for( I32 f : L ) { max_children = std::max( max_children, child_ptr[f+1] - child_ptr[f] ); }
+        const I64 level_ext_first = static_cast<I64>( extend.size() );
         for( I32 r = 0; r < max_children; ++r )
         {
             const I64 first = static_cast<I64>(extend.size());
@@ -530,8 +532,56 @@ void Plan::build( const Symbolic & sym )
                     row = end;
                 }
             }
-            const I32 count = static_cast<I32>( static_cast<I64>(extend.size()) - first );
-            if( count > 0 ) { factor_launches.push_back( { LaunchKind::Extend, count, first, h, r } ); }
+            (void)first;
+        }
+        // the level launch: the same additions by blocks of parent rows (ExtendPullTask)
+        {
+            const I64 pull_first = static_cast<I64>( extend_pull.size() );
+            for( I32 p : L )
+            {
+                const I32 cb = child_ptr[p], ce = child_ptr[p+1];
+                for( int space = 0; space < 2 && cb < ce; ++space )
+                {
+                    const I32 prow = space == 0 ? front_n0[p] : front_n1[p];
+                    for( I32 b0 = 0; b0 < prow; b0 += kExtendPullRows )
+                    {
+                        const I32 b1 = std::min( prow, b0 + kExtendPullRows );
+                        const I64 seg_first = static_cast<I64>( extend_segs.size() );
+                        for( I32 c = cb; c < ce; ++c )
+                        {
+                            const I32 t = child_idx[c];
+                            const I32 m1 = front_n1[t];
+                            if( m1 == 0 ) { continue; }
+                            // the child's rows in this space map to increasing parent rows
+                            const I32 * lt = lut.data() + front_lut[t];
+                            const I32 lo = space == 0 ? 0 : mid[t], hi = space == 0 ? mid[t] : m1;
+                            const I32 ia = static_cast<I32>( std::lower_bound( lt + lo, lt + hi, b0 ) - lt );
+                            const I32 ib = static_cast<I32>( std::lower_bound( lt + lo, lt + hi, b1 ) - lt );
+                            if( ia >= ib ) { continue; }
+                            ExtendTask e{};
+                            e.w = front_v[t];
+                            e.u0 = front_u0[p]; e.u1 = front_u1[p]; e.v = front_v[p];
+                            e.lut = front_lut[t];
+                            e.m1 = m1; e.mid = mid[t];
+                            e.n0p = front_n0[p]; e.n1p = front_n1[p];
+                            e.ldw = front_ld1[t];
+                            e.ld0p = front_ld0[p]; e.ld1p = front_ld1[p]; e.ldvp = front_ld1[p];
+                            e.row_begin = ia; e.row_end = ib;
+                            extend_segs.push_back( e );
+                        }
+                        const I32 nseg = static_cast<I32>( static_cast<I64>( extend_segs.size() ) - seg_first );
+                        if( nseg > 0 ) { extend_pull.push_back( { seg_first, nseg, 0 } ); }
+                    }
+                }
+            }
+            const I32 npull = static_cast<I32>( static_cast<I64>( extend_pull.size() ) - pull_first );
+            if( npull > 0 )
+            {
+                Launch Lp{ LaunchKind::ExtendPull, npull, pull_first, h, 0 };
+                Lp.tc_first = level_ext_first;
+                Lp.tc_count = static_cast<I32>( static_cast<I64>( extend.size() ) - level_ext_first );
+                factor_launches.push_back( Lp );
+            }
         }
 
         // panel steps; in the task graph a step's GEMM tiles that update the

@@ -206,7 +206,21 @@ struct DagTask
 };
 
 enum class LaunchKind : std::int32_t { Zero = 0, Extend = 1, Trsm = 2, Gemm = 3, Invert = 4, Solve = 5, Potrf = 6,
-                                       SuperInv = 8, SuperDiag = 9, SuperRest = 10 };
+                                       SuperInv = 8, SuperDiag = 9, SuperRest = 10, ExtendPull = 11 };
+
+// Extend-add by parent rows (the level launches): one CTA adds, child by
+// child in rank order, the rows of every child that map into one block of
+// a parent's rows (pivot rows: U0 / U1; update rows: V).  The segments are
+// ExtendTasks whose [row_begin, row_end) are those child rows.  Every parent
+// entry receives the same additions in the same order as in the passes by
+// child rank (the persistent schedule's extend tasks), in one launch per
+// level instead of one per child rank.
+struct ExtendPullTask
+{
+    std::int64_t seg_first;        // its segments in Plan::extend_segs
+    std::int32_t seg_count, pad;
+};
+constexpr int kExtendPullRows = 32;     // parent rows per pull task
 
 // The solve of a large front steps through its pivot rows 512 at a time
 // (super-panels) instead of 64 at a time: the inverse of each 512 x 512
@@ -265,6 +279,9 @@ struct Launch
     std::int64_t tc_first = 0;
     std::int32_t tc_count = 0;
     std::int32_t small_count = 0;
+    // ExtendPull launches: the level's extend tasks in pass order are
+    // [tc_first, tc_first + tc_count) of Plan::extend (what the persistent
+    // schedule runs instead)
 };
 
 struct Plan
@@ -339,6 +356,8 @@ struct Plan
     std::vector<SuperInvTask> sinv;
     std::vector<Launch> sinv_launches;
     std::vector<SuperSolveTask> ssolve;
+    std::vector<ExtendPullTask> extend_pull;
+    std::vector<ExtendTask> extend_segs;
     std::vector<Launch> lower_launches_sp, upper_launches_sp;
     std::int64_t super_inv_size = 0;        // doubles of all inverses
 

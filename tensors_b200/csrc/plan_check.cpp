@@ -86,10 +86,12 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         if( !in_range( z.offset, z.offset + static_cast<I64>( z.row_end - 1 ) * z.ld + z.n - 1, arena ) ) { return "zero task out of range"; }
     }
     std::vector<I32> lut_seen( pl.lut.size() + 1, 0 );
-    for( size_t k = 0; k < pl.extend.size(); ++k )
+    const size_t n_ext = pl.extend.size();
+    for( size_t k = 0; k < n_ext + pl.extend_segs.size(); ++k )
     {
-        const ExtendTask & t = pl.extend[k];
-        auto at = [&]() { return " (extend task " + std::to_string( k ) + ")"; };   // built only on failure
+        const ExtendTask & t = k < n_ext ? pl.extend[k] : pl.extend_segs[k - n_ext];
+        auto at = [&]() { return k < n_ext ? " (extend task " + std::to_string( k ) + ")"
+                                           : " (extend segment " + std::to_string( k - n_ext ) + ")"; };   // built only on failure
         if( t.m1 <= 0 || t.mid < 0 || t.mid > t.m1 ) { return "bad extend dimensions" + at(); }
         if( t.row_begin < 0 || t.row_end > t.m1 || t.row_begin >= t.row_end ) { return "bad extend rows" + at(); }
         if( t.ldw < t.m1 || t.ld0p < t.n0p || t.ld1p < t.n1p || t.ldvp < t.n1p ) { return "extend leading dimension too small" + at(); }
@@ -108,6 +110,47 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             const I32 lim = (i < t.mid) ? t.n0p : t.n1p;
             if( l < 0 || l >= lim ) { return "extend lut value out of range" + at(); }
             if( i > 0 && i != t.mid && l <= pl.lut[t.lut + i - 1] ) { return "extend lut not increasing" + at(); }
+        }
+    }
+    // extend-add by parent rows: per level launch, the segments cover every row of the level's
+    // extend tasks once; a task's segments share one parent and one block of its pivot or update
+    // rows, in child-rank order (the order of the children's first tasks in the passes)
+    for( const Launch & L : pl.factor_launches )
+    {
+        if( L.kind != LaunchKind::ExtendPull ) { continue; }
+        if( L.tc_first < 0 || L.tc_count < 0 || L.tc_first + L.tc_count > static_cast<I64>( pl.extend.size() ) ) { return "extend pull launch: task range"; }
+        std::map<I64, std::pair<I64, std::vector<I32>>> rows;          // child W -> (rank, rows left to add)
+        for( I64 k = L.tc_first; k < L.tc_first + L.tc_count; ++k )
+        {
+            const ExtendTask & t = pl.extend[static_cast<size_t>( k )];
+            auto it = rows.find( t.w );
+            if( it == rows.end() ) { it = rows.emplace( t.w, std::make_pair( k, std::vector<I32>( static_cast<size_t>( t.m1 ), 0 ) ) ).first; }
+            for( I32 i = t.row_begin; i < t.row_end; ++i ) { ++it->second.second[static_cast<size_t>( i )]; }
+        }
+        for( I64 q = L.first; q < L.first + L.count; ++q )
+        {
+            const ExtendPullTask & u = pl.extend_pull[static_cast<size_t>( q )];
+            if( u.seg_count <= 0 || u.seg_first < 0 || u.seg_first + u.seg_count > static_cast<I64>( pl.extend_segs.size() ) ) { return "extend pull task out of range"; }
+            const ExtendTask & s0 = pl.extend_segs[static_cast<size_t>( u.seg_first )];
+            const bool upper = s0.row_begin < s0.mid;
+            const I32 b0 = pl.lut[s0.lut + s0.row_begin] / kExtendPullRows * kExtendPullRows;
+            I64 rank = -1;
+            for( I64 g = u.seg_first; g < u.seg_first + u.seg_count; ++g )
+            {
+                const ExtendTask & t = pl.extend_segs[static_cast<size_t>( g )];
+                if( t.u0 != s0.u0 || t.u1 != s0.u1 || t.v != s0.v ) { return "extend pull task spans parents"; }
+                if( (t.row_end <= t.mid) != upper || (t.row_begin < t.mid) != upper ) { return "extend pull segment spans row spaces"; }
+                if( pl.lut[t.lut + t.row_begin] < b0 || pl.lut[t.lut + t.row_end - 1] >= b0 + kExtendPullRows ) { return "extend pull segment outside its row block"; }
+                auto it = rows.find( t.w );
+                if( it == rows.end() ) { return "extend pull segment of a child not in its level"; }
+                if( it->second.first <= rank ) { return "extend pull segments not in child-rank order"; }
+                rank = it->second.first;
+                for( I32 i = t.row_begin; i < t.row_end; ++i ) { --it->second.second[static_cast<size_t>( i )]; }
+            }
+        }
+        for( const auto & kv : rows )
+        {
+            for( I32 c : kv.second.second ) { if( c != 0 ) { return "extend pull launch does not add every child row once"; } }
         }
     }
     for( int which = 0; which < 2; ++which )
@@ -352,6 +395,8 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             case LaunchKind::Invert: return static_cast<I64>( pl.sdiag.size() );
             case LaunchKind::Solve:  return static_cast<I64>( pl.srest.size() );
             case LaunchKind::Potrf:  return static_cast<I64>( pl.potrf.size() );
+            case LaunchKind::ExtendPull: return static_cast<I64>( pl.extend_pull.size() );
+            default: break;
         }
         return -1;
     };
@@ -389,8 +434,9 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             }
         }
         I64 expect = 0, pre = 0;
-        for( const Launch & L : pl.factor_launches ) { expect += L.count; }
-        for( const Launch & L : pl.pre_dag_launches ) { pre += L.count; }
+        // an ExtendPull launch stands for its level's extend tasks
+        for( const Launch & L : pl.factor_launches ) { expect += L.kind == LaunchKind::ExtendPull ? L.tc_count : L.count; }
+        for( const Launch & L : pl.pre_dag_launches ) { pre += L.kind == LaunchKind::ExtendPull ? L.tc_count : L.count; }
         if( work + pre != expect ) { return "task graph and preceding launches do not cover the factorization tasks"; }
     }
     for( const Launch & L : pl.lower_launches ) { if( L.kind != LaunchKind::Solve ) { return "unexpected launch kind in the forward solve"; } }
