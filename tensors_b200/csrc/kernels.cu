@@ -200,7 +200,7 @@ __global__ void export_kernel( const ExportTask * __restrict__ tasks, const std:
 // ------------------------------------------------------------- extend-add
 // One warp per row of the child's update W; lanes walk the row's upper part
 // (coalesced reads of W, lut-indexed adds into the parent front).
-template<typename T, bool kPlainAdd = false>
+template<typename T>
 __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::int32_t * __restrict__ lut_all,
                                              T * __restrict__ arena )
 {
@@ -238,20 +238,8 @@ __device__ __forceinline__ void extend_body( const ExtendTask & t, const std::in
                     dst[u] = upper_part ? ((j < t.mid) ? row0 + lj : row1 + lj) : rowv + lj;
                 }
             }
-            if constexpr ( kPlainAdd )
-            {
-                // one CTA owns the targets (extend_pull_kernel): load, add, store
-                T old[kU];
 #pragma unroll
-                for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : T( 0 ); }
-#pragma unroll
-                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { *dst[u] = old[u] + v[u]; } }
-            }
-            else
-            {
-#pragma unroll
-                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
-            }
+            for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
         }
     }
 }
@@ -270,18 +258,63 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
 // Extend-add by parent rows (ExtendPullTask): the CTA adds its segments one
 // child after the other; the barrier between two children orders their
 // additions into the rows they share, so every entry gets the sum of the
-// passes by child rank, in the same order.
+// passes by child rank, in the same order.  Inside a segment the (row, 128
+// columns) chunks go round-robin to the warps, so long rows of large update
+// matrices spread over the CTA; every target is loaded, added to and stored
+// (the CTA owns its parent rows for the launch).
 template<typename T>
 __global__ __launch_bounds__(256) void extend_pull_kernel( const ExtendPullTask * __restrict__ tasks, const ExtendTask * __restrict__ segs,
                                                            const std::int32_t * __restrict__ lut_all, T * __restrict__ arena )
 {
+    constexpr int kU = 4, kChunk = 32 * kU, kWarps = 8;
     pdl_allow_next();
     const ExtendPullTask t = tasks[blockIdx.x];
     pdl_wait();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for( std::int64_t g = t.seg_first; g < t.seg_first + t.seg_count; ++g )
     {
         if( g > t.seg_first ) { __syncthreads(); }
-        extend_body<T, true>( segs[g], lut_all, arena );
+        const ExtendTask e = segs[g];
+        const std::int32_t * lut = lut_all + e.lut;
+        const T * W = arena + e.w;
+        int unit = 0;                                   // chunks before row i, over the segment
+        for( int i = e.row_begin; i < e.row_end; ++i )
+        {
+            const int nch = (e.m1 - i + kChunk - 1) / kChunk;
+            int k = (warp - unit % kWarps + kWarps) % kWarps;
+            unit += nch;
+            if( k >= nch ) { continue; }
+            const std::int64_t li = lut[i];
+            const T * Wi = W + (std::int64_t)i * e.ldw;
+            T * row0 = arena + e.u0 + li * e.ld0p;
+            T * row1 = arena + e.u1 + li * e.ld1p;
+            T * rowv = arena + e.v + li * e.ldvp;
+            const bool upper_part = i < e.mid;
+            for( ; k < nch; k += kWarps )
+            {
+                const int j0 = i + k * kChunk + lane;
+                T v[kU];
+                T * dst[kU];
+#pragma unroll
+                for( int u = 0; u < kU; ++u )
+                {
+                    const int j = j0 + 32 * u;
+                    dst[u] = nullptr;
+                    v[u] = T( 0 );
+                    if( j < e.m1 )
+                    {
+                        const int lj = lut[j];
+                        v[u] = Wi[j];
+                        dst[u] = upper_part ? ((j < e.mid) ? row0 + lj : row1 + lj) : rowv + lj;
+                    }
+                }
+                T old[kU];
+#pragma unroll
+                for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : T( 0 ); }
+#pragma unroll
+                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { *dst[u] = old[u] + v[u]; } }
+            }
+        }
     }
 }
 

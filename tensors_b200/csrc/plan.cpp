@@ -534,43 +534,63 @@ void Plan::build( const Symbolic & sym )
             }
             (void)first;
         }
-        // the level launch: the same additions by blocks of parent rows (ExtendPullTask)
+        // the level launch: the same additions by blocks of parent rows (ExtendPullTask), a block
+        // growing while its children's entries stay within kExtendPullEntries
         {
             const I64 pull_first = static_cast<I64>( extend_pull.size() );
+            std::vector<I64> row_work;
             for( I32 p : L )
             {
                 const I32 cb = child_ptr[p], ce = child_ptr[p+1];
                 for( int space = 0; space < 2 && cb < ce; ++space )
                 {
                     const I32 prow = space == 0 ? front_n0[p] : front_n1[p];
-                    for( I32 b0 = 0; b0 < prow; b0 += kExtendPullRows )
+                    row_work.assign( static_cast<size_t>( prow ), 0 );
+                    for( I32 c = cb; c < ce; ++c )
                     {
-                        const I32 b1 = std::min( prow, b0 + kExtendPullRows );
-                        const I64 seg_first = static_cast<I64>( extend_segs.size() );
-                        for( I32 c = cb; c < ce; ++c )
+                        const I32 t = child_idx[c];
+                        const I32 m1 = front_n1[t];
+                        const I32 lo = space == 0 ? 0 : mid[t], hi = space == 0 ? mid[t] : m1;
+                        for( I32 i = lo; i < hi; ++i ) { row_work[static_cast<size_t>( lut[front_lut[t] + i] )] += m1 - i; }
+                    }
+                    for( I32 b0 = 0; b0 < prow; )
+                    {
+                        I32 b1 = b0;
+                        I64 work = 0;
+                        while( b1 < prow && (b1 == b0 || work + row_work[static_cast<size_t>( b1 )] <= kExtendPullEntries) )
                         {
-                            const I32 t = child_idx[c];
-                            const I32 m1 = front_n1[t];
-                            if( m1 == 0 ) { continue; }
-                            // the child's rows in this space map to increasing parent rows
-                            const I32 * lt = lut.data() + front_lut[t];
-                            const I32 lo = space == 0 ? 0 : mid[t], hi = space == 0 ? mid[t] : m1;
-                            const I32 ia = static_cast<I32>( std::lower_bound( lt + lo, lt + hi, b0 ) - lt );
-                            const I32 ib = static_cast<I32>( std::lower_bound( lt + lo, lt + hi, b1 ) - lt );
-                            if( ia >= ib ) { continue; }
-                            ExtendTask e{};
-                            e.w = front_v[t];
-                            e.u0 = front_u0[p]; e.u1 = front_u1[p]; e.v = front_v[p];
-                            e.lut = front_lut[t];
-                            e.m1 = m1; e.mid = mid[t];
-                            e.n0p = front_n0[p]; e.n1p = front_n1[p];
-                            e.ldw = front_ld1[t];
-                            e.ld0p = front_ld0[p]; e.ld1p = front_ld1[p]; e.ldvp = front_ld1[p];
-                            e.row_begin = ia; e.row_end = ib;
-                            extend_segs.push_back( e );
+                            work += row_work[static_cast<size_t>( b1 )];
+                            ++b1;
                         }
-                        const I32 nseg = static_cast<I32>( static_cast<I64>( extend_segs.size() ) - seg_first );
-                        if( nseg > 0 ) { extend_pull.push_back( { seg_first, nseg, 0 } ); }
+                        if( work > 0 )
+                        {
+                            const I64 seg_first = static_cast<I64>( extend_segs.size() );
+                            for( I32 c = cb; c < ce; ++c )
+                            {
+                                const I32 t = child_idx[c];
+                                const I32 m1 = front_n1[t];
+                                if( m1 == 0 ) { continue; }
+                                // the child's rows in this space map to increasing parent rows
+                                const I32 * lt = lut.data() + front_lut[t];
+                                const I32 lo = space == 0 ? 0 : mid[t], hi = space == 0 ? mid[t] : m1;
+                                const I32 ia = static_cast<I32>( std::lower_bound( lt + lo, lt + hi, b0 ) - lt );
+                                const I32 ib = static_cast<I32>( std::lower_bound( lt + lo, lt + hi, b1 ) - lt );
+                                if( ia >= ib ) { continue; }
+                                ExtendTask e{};
+                                e.w = front_v[t];
+                                e.u0 = front_u0[p]; e.u1 = front_u1[p]; e.v = front_v[p];
+                                e.lut = front_lut[t];
+                                e.m1 = m1; e.mid = mid[t];
+                                e.n0p = front_n0[p]; e.n1p = front_n1[p];
+                                e.ldw = front_ld1[t];
+                                e.ld0p = front_ld0[p]; e.ld1p = front_ld1[p]; e.ldvp = front_ld1[p];
+                                e.row_begin = ia; e.row_end = ib;
+                                extend_segs.push_back( e );
+                            }
+                            const I32 nseg = static_cast<I32>( static_cast<I64>( extend_segs.size() ) - seg_first );
+                            extend_pull.push_back( { seg_first, nseg, space, b0, b1 } );
+                        }
+                        b0 = b1;
                     }
                 }
             }

@@ -132,15 +132,15 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             const ExtendPullTask & u = pl.extend_pull[static_cast<size_t>( q )];
             if( u.seg_count <= 0 || u.seg_first < 0 || u.seg_first + u.seg_count > static_cast<I64>( pl.extend_segs.size() ) ) { return "extend pull task out of range"; }
             const ExtendTask & s0 = pl.extend_segs[static_cast<size_t>( u.seg_first )];
-            const bool upper = s0.row_begin < s0.mid;
-            const I32 b0 = pl.lut[s0.lut + s0.row_begin] / kExtendPullRows * kExtendPullRows;
+            const bool upper = u.space == 0;
+            if( (u.space != 0 && u.space != 1) || u.b0 < 0 || u.b1 <= u.b0 || u.b1 > (upper ? s0.n0p : s0.n1p) ) { return "extend pull task rows out of range"; }
             I64 rank = -1;
             for( I64 g = u.seg_first; g < u.seg_first + u.seg_count; ++g )
             {
                 const ExtendTask & t = pl.extend_segs[static_cast<size_t>( g )];
                 if( t.u0 != s0.u0 || t.u1 != s0.u1 || t.v != s0.v ) { return "extend pull task spans parents"; }
                 if( (t.row_end <= t.mid) != upper || (t.row_begin < t.mid) != upper ) { return "extend pull segment spans row spaces"; }
-                if( pl.lut[t.lut + t.row_begin] < b0 || pl.lut[t.lut + t.row_end - 1] >= b0 + kExtendPullRows ) { return "extend pull segment outside its row block"; }
+                if( pl.lut[t.lut + t.row_begin] < u.b0 || pl.lut[t.lut + t.row_end - 1] >= u.b1 ) { return "extend pull segment outside its row block"; }
                 auto it = rows.find( t.w );
                 if( it == rows.end() ) { return "extend pull segment of a child not in its level"; }
                 if( it->second.first <= rank ) { return "extend pull segments not in child-rank order"; }
