@@ -256,12 +256,12 @@ __global__ __launch_bounds__(256) void extend_kernel( const ExtendTask * __restr
 }
 
 // Extend-add by parent rows (ExtendPullTask): the CTA adds its segments one
-// child after the other; the barrier between two children orders their
-// additions into the rows they share, so every entry gets the sum of the
-// passes by child rank, in the same order.  Inside a segment the (row, 128
-// columns) chunks go round-robin to the warps, so long rows of large update
-// matrices spread over the CTA; every target is loaded, added to and stored
-// (the CTA owns its parent rows for the launch).
+// child after the other, as reductions in the memory system; a fence and a
+// barrier between two children make every reduction of the first performed
+// before any of the next is issued, so every entry gets the sum of the passes
+// by child rank, in the same order (the CTA owns its parent rows for the
+// launch).  Inside a segment the (row, 128 columns) chunks go round-robin to
+// the warps, so long rows of large update matrices spread over the CTA.
 template<typename T>
 __global__ __launch_bounds__(256) void extend_pull_kernel( const ExtendPullTask * __restrict__ tasks, const ExtendTask * __restrict__ segs,
                                                            const std::int32_t * __restrict__ lut_all, T * __restrict__ arena )
@@ -273,7 +273,11 @@ __global__ __launch_bounds__(256) void extend_pull_kernel( const ExtendPullTask 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for( std::int64_t g = t.seg_first; g < t.seg_first + t.seg_count; ++g )
     {
-        if( g > t.seg_first ) { __syncthreads(); }
+        if( g > t.seg_first )
+        {
+            __threadfence();
+            __syncthreads();
+        }
         const ExtendTask e = segs[g];
         const std::int32_t * lut = lut_all + e.lut;
         const T * W = arena + e.w;
@@ -308,11 +312,8 @@ __global__ __launch_bounds__(256) void extend_pull_kernel( const ExtendPullTask 
                         dst[u] = upper_part ? ((j < e.mid) ? row0 + lj : row1 + lj) : rowv + lj;
                     }
                 }
-                T old[kU];
 #pragma unroll
-                for( int u = 0; u < kU; ++u ) { old[u] = dst[u] ? *dst[u] : T( 0 ); }
-#pragma unroll
-                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { *dst[u] = old[u] + v[u]; } }
+                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
             }
         }
     }
