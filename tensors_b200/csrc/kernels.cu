@@ -382,8 +382,10 @@ __device__ __forceinline__ double (*potrf_scratch( const PotrfShared & sh ))[kPa
     return reinterpret_cast<double (*)[kPanel + 1]>( &sh.Ti[kPanel - kSub][kSub * ((threadIdx.x >> 5) - 1)] );
 }
 
-// Stores a factored diagonal tile: U_qq over the tile's upper triangle and
-// its reciprocal pivots into inv_d.
+// Stores a factored diagonal tile: U_qq, rounded to the storage type, over
+// the tile's upper triangle and its reciprocal pivots (of the unrounded
+// pivots) into inv_d.
+template<typename T>
 __device__ __forceinline__ void potrf_store_tile( const PotrfShared & sh, int o, const double (&a)[kSub][kSub], const double (&iv)[kSub] )
 {
     if( (threadIdx.x & 31) == 0 )
@@ -392,7 +394,7 @@ __device__ __forceinline__ void potrf_store_tile( const PotrfShared & sh, int o,
         for( int r = 0; r < kSub; ++r )
         {
 #pragma unroll
-            for( int c = r; c < kSub; ++c ) { sh.D[o + r][o + c] = a[r][c]; }
+            for( int c = r; c < kSub; ++c ) { sh.D[o + r][o + c] = round_to<T>( a[r][c] ); }
             sh.inv_d[o + r] = iv[r];
         }
     }
@@ -457,7 +459,7 @@ __device__ __noinline__ void potrf_tile_floored( const PotrfShared & sh, const P
             for( int c = r2; c < kSub; ++c ) { a[r2][c] -= a[r][r2] * a[r][c]; }
         }
     }
-    potrf_store_tile( sh, o, a, iv );
+    potrf_store_tile<T>( sh, o, a, iv );
 }
 
 // Cholesky of the diagonal tile q of D by one warp.  Every lane holds the
@@ -519,7 +521,7 @@ __device__ bool potrf_diag_tile( const PotrfShared & sh, const PanelTask & t, in
             if( !((singles >> r) & 1) && o + r < nb && !(piv[r] > 0.0) && *sh.fail < 0 ) { *sh.fail = o + r; }
         }
     }
-    potrf_store_tile( sh, o, a, iv );
+    potrf_store_tile<T>( sh, o, a, iv );
     return true;
 }
 
@@ -534,9 +536,9 @@ __device__ bool potrf_diag_tile( const PotrfShared & sh, const PanelTask & t, in
 //      form column block b of T, T_ib = -(sum_{k=i..b-1} T_ik U_kb) W_b.
 // Tile products run on the FP64 tensor cores (two DMMA m8n8k4 each).  A row
 // that forms a 1 x 1 reference supernode takes sqrt(|a|) as the reference
-// does (:471) and never reports failure.  With FP32 storage the block is
-// factored in FP64 and rounded when stored; W and T are formed from the
-// rounded values, so that T inverts the stored factor.
+// does (:471) and never reports failure.  With FP32 storage every U value is
+// rounded to FP32 as it is formed, so the in-panel updates, W and T use the
+// stored factor (T inverts it), as the updates of later panels do.
 template<typename T>
 __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict__ arena, int * __restrict__ status,
                                             double * smem, const double * __restrict__ pivot_floor, double * __restrict__ tinv )
@@ -590,29 +592,35 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
                 for( int r2 = r + 1; r2 < kSub; ++r2 ) { x[r2] -= sh.D[o + r][o + r2] * x[r]; }
             }
 #pragma unroll
-            for( int r = 0; r < kSub; ++r ) { sh.D[o + r][col] = x[r]; }
+            for( int r = 0; r < kSub; ++r ) { sh.D[o + r][col] = round_to<T>( x[r] ); }
         }
-        else if( warp == 7 && lane < kSub )
+        else if( warp == 7 )
         {
-            // column j = lane of W_b: w_jj = 1 / u_jj, w_ij = -(sum_{k=i+1..j} u_ik w_kj) / u_ii
-            const int j = lane;
-            double w[kSub], sum[kSub];
+            // column j = lane of W_b = U_bb^{-1} (lanes 8-31 repeat lanes 0-7 and store nothing):
+            // w_jj = 1 / u_jj, then for k = j-1, .., 0 w_k = -(sum_{i>k} u_ki w_i) / u_kk, as one
+            // branch-free recurrence over k = 7..0.  The reciprocals of the stored pivots come from
+            // one Newton step on the tile's reciprocal square roots, r = v (2 - u v).
+            const int j = lane & (kSub - 1);
+            double rec[kSub], w[kSub], sum[kSub];
 #pragma unroll
-            for( int i = 0; i < kSub; ++i ) { sum[i] = 0.0; }
+            for( int k = 0; k < kSub; ++k )
+            {
+                const double v = sh.inv_d[o + k];
+                rec[k] = v * fma( -sh.D[o + k][o + k], v, 2.0 );
+                sum[k] = 0.0;
+            }
 #pragma unroll
             for( int k = kSub - 1; k >= 0; --k )
             {
-                w[k] = 0.0;
-                if( k <= j )
-                {
-                    const double rk = 1.0 / round_to<T>( sh.D[o + k][o + k] );
-                    w[k] = k == j ? rk : -rk * sum[k];
+                w[k] = j == k ? rec[k] : (j > k ? -rec[k] * sum[k] : 0.0);
 #pragma unroll
-                    for( int i = 0; i < k; ++i ) { sum[i] += round_to<T>( sh.D[o + i][o + k] ) * w[k]; }
-                }
+                for( int i = 0; i < k; ++i ) { sum[i] = fma( sh.D[o + i][o + k], w[k], sum[i] ); }
             }
+            if( lane < kSub )
+            {
 #pragma unroll
-            for( int i = 0; i < kSub; ++i ) { sh.Ti[o + i][o + j] = w[i]; }
+                for( int i = 0; i < kSub; ++i ) { sh.Ti[o + i][o + j] = w[i]; }
+            }
         }
         __syncthreads();
         // 2. trailing tiles and T's column block b
@@ -656,7 +664,7 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
                     for( int ok = oi; ok < o; ok += kSub )
                     {
                         dmma_8x8x8( acc, [&]( int ii, int kk ) { return sh.Ti[oi + ii][ok + kk]; },
-                                         [&]( int kk, int jj ) { return round_to<T>( sh.D[ok + kk][o + jj] ); } );
+                                         [&]( int kk, int jj ) { return sh.D[ok + kk][o + jj]; } );
                     }
                     double (*S)[kPanel + 1] = potrf_scratch( sh );
                     S[i8][j8] = acc[0];
