@@ -273,6 +273,7 @@ def run_for_profiler(args):
 
 # ------------------------------------------------------------ other configs
 C3_GRID, C3_SEED, C3_SHIFT, C3_NRHS, C3_TARGET = 48, 0x5EED0003, 1e-2, 8, 1e-12
+C3_NORTH_STAR_TARGET = 1e-10     # the mixed-vs-FP64 target of the path's goal (the configuration says 1e-12)
 C4_COUNT, C4_SEED, C4_MIN, C4_MAX = 2000, 0x5EED0004, 500, 20000
 # The random Delaunay meshes carry near-flat hull triangles whose cotangent
 # weights reach ~1e6 while the lumped mass is ~1e-8: kappa ~1e12-1e14.  A plain
@@ -309,7 +310,8 @@ def c3_compare(torch, dev, steps, warmup, autotune=True):
     The stiffness sum_e [[B,-B],[-B,B]] with SPD edge blocks B = G G^T + 0.1 I is
     singular (rigid translations are in its null space), so the matrix carries
     a 1e-2 diagonal shift.  Both paths solve to the configuration's 1e-12
-    relative residual target; the FP64 path reaches ~1e-14 directly.  Returns per
+    relative residual target (the mixed path also to 1e-10, the target of the
+    path's 2x goal); the FP64 path reaches ~1e-14 directly.  Returns per
     precision the step, factor and solve times, the relative residual and the
     refinement, plus the speed-up and the forward difference of the mixed
     solution from the FP64 one.
@@ -346,16 +348,21 @@ def c3_compare(torch, dev, steps, warmup, autotune=True):
                 mid.record(stream)
             c.Solve(B, X)
 
-        with ClockSampler(dev.index or 0) as clocks:
-            t, tf = _time_steps(torch, stream, step, steps, warmup)
-        R = c.Residual(B, X)
-        stream.synchronize()
-        rr = float((torch.linalg.norm(R, dim=0) / torch.linalg.norm(B, dim=0)).max())
-        F, nnz_u = c.FlopCount()
-        out[prec] = {"ms": t, "factor_ms": tf, "solve_ms": t - tf, "relres": rr, "plan_options": tuned,
-                     "refinement": c.RefinementInfo() if prec == "mixed" else None,
-                     "precision_in_use": list(c.PrecisionInUse()), "clocks": clocks.summary()}
-        sols[prec] = X
+        # the mixed path also to the north star's 1e-10 (the FP64 path reaches ~1e-14 either way)
+        for target in ((C3_TARGET, C3_NORTH_STAR_TARGET) if prec == "mixed" else (C3_TARGET,)):
+            c.SetRefinement(target, 30)
+            with ClockSampler(dev.index or 0) as clocks:
+                t, tf = _time_steps(torch, stream, step, steps, warmup)
+            R = c.Residual(B, X)
+            stream.synchronize()
+            rr = float((torch.linalg.norm(R, dim=0) / torch.linalg.norm(B, dim=0)).max())
+            F, nnz_u = c.FlopCount()
+            key = prec if target == C3_TARGET else f"{prec}_{target:g}"
+            out[key] = {"ms": t, "factor_ms": tf, "solve_ms": t - tf, "relres": rr, "target": target,
+                        "plan_options": tuned, "refinement": c.RefinementInfo() if prec == "mixed" else None,
+                        "precision_in_use": list(c.PrecisionInUse()), "clocks": clocks.summary()}
+            if target == C3_TARGET:
+                sols[prec] = X.clone()
         del c
     torch.cuda.set_stream(prev)
     flops = F + 4.0 * C3_NRHS * nnz_u
@@ -363,7 +370,9 @@ def c3_compare(torch, dev, steps, warmup, autotune=True):
                         f"G G^T + 0.1 I, shift {C3_SHIFT:g}, geometric nested dissection, {C3_NRHS} RHS, "
                         f"target relres {C3_TARGET:g}",
             "factor_gflop": F / 1e9, "flops": flops, "fp64": out["fp64"], "mixed": out["mixed"],
+            f"mixed_{C3_NORTH_STAR_TARGET:g}": out[f"mixed_{C3_NORTH_STAR_TARGET:g}"],
             "speedup_mixed_over_fp64": out["fp64"]["ms"] / out["mixed"]["ms"],
+            f"speedup_mixed_over_fp64_at_{C3_NORTH_STAR_TARGET:g}": out["fp64"]["ms"] / out[f"mixed_{C3_NORTH_STAR_TARGET:g}"]["ms"],
             "forward_diff_mixed_vs_fp64": float(torch.linalg.norm(sols["mixed"] - sols["fp64"])
                                                 / torch.linalg.norm(sols["fp64"])),
             "l2": "factor and matrix exceed L2"}
