@@ -478,12 +478,14 @@ __device__ bool potrf_diag_tile( const PotrfShared & sh, const PanelTask & t, in
     const int lane = threadIdx.x & 31;
     const int o = kSub * q;
     const unsigned singles = static_cast<unsigned>( (t.single_rows >> o) & 0xff );
-    double a[kSub][kSub], iv[kSub], piv[kSub];
+    double a[kSub][kSub], iv[kSub], piv[kSub], fl[kSub];
 #pragma unroll
     for( int r = 0; r < kSub; ++r )
     {
 #pragma unroll
         for( int c = r; c < kSub; ++c ) { a[r][c] = sh.D[o + r][o + c]; }
+        // the pivot floors are read with the tile, off the pivot chain
+        if constexpr ( sizeof(T) == 4 ) { fl[r] = sh.floor_s[o + r]; }
     }
 #pragma unroll
     for( int r = 0; r < kSub; ++r )
@@ -505,7 +507,7 @@ __device__ bool potrf_diag_tile( const PotrfShared & sh, const PanelTask & t, in
     {
         bool low = false;
 #pragma unroll
-        for( int r = 0; r < kSub; ++r ) { low |= o + r < nb && !(piv[r] > sh.floor_s[o + r]); }
+        for( int r = 0; r < kSub; ++r ) { low |= o + r < nb && !(piv[r] > fl[r]); }
         if( low && pivot_floor != nullptr )
         {
             if( speculative ) { return false; }
@@ -555,7 +557,6 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     sh.redo = sh.fail + 1;
 
     T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0 + t.r0;
-    if( pivot_floor != nullptr && tid < nb ) { sh.floor_s[tid] = pivot_floor[1 + t.row0 + t.r0 + tid]; }
     auto stage_src = [&]( int idx, double & fill ) -> const T *
     {
         const int r = idx / kPanel, c = idx % kPanel;
@@ -564,6 +565,8 @@ __device__ __forceinline__ void potrf_body( const PanelTask & t, T * __restrict_
     };
     auto stage_dst = [&]( int idx ) { return &sh.D[idx / kPanel][idx % kPanel]; };
     stage_block<T, kPanel * kPanel / kPotrfThreads, kPotrfThreads>( U0, stage_src, stage_dst );
+    // the pivot floors after the block's copies are in flight (their loads overlap)
+    if( pivot_floor != nullptr && tid < nb ) { sh.floor_s[tid] = pivot_floor[1 + t.row0 + t.r0 + tid]; }
     if( tid == 0 ) { *sh.fail = -1; *sh.redo = 0; }
     cp_async_wait_all();
     stage_finish<T, kPanel * kPanel / kPotrfThreads, kPotrfThreads>( stage_src, stage_dst );
