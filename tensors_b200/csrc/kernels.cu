@@ -1256,6 +1256,8 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 // solution itself and no CTA waits for another.
 
 constexpr int kTld = kPanel + 4;   // padded shared-memory row of 64-wide blocks (conflict-free DMMA fragments)
+// Doubles of shared memory the solve step's staged rest block takes (64 x kTld of T, rounded up).
+template<typename T> __host__ __device__ constexpr int solve_block_doubles() { return (kPanel * kTld * static_cast<int>( sizeof(T) ) + 7) / 8; }
 
 // acc[ct] (8 x 8 tile ct of this warp's 8 output rows, NCT tiles) += sum over
 // the K blocks [kb0, kb1) of A(i, kk) * B(kk, ct * 8 + j).
@@ -1304,9 +1306,11 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
     constexpr int kp = KP;
     constexpr int lkp = KP == 8 ? 3 : KP == 16 ? 4 : KP == 32 ? 5 : 6;
     constexpr int ldv = kp + 4;
+    // the rest block stays in the factor's type (FP32 storage: half the shared memory, so
+    // that three CTAs fit an SM) and is widened as the products read it
     double (*sT)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm );
-    double (*sP)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm + kPanel * kTld );
-    double * sX = ssm + 2 * kPanel * kTld;          // [64][ldv]: x_q (forward) / x_r (backward)
+    T (*sP)[kTld] = reinterpret_cast<T (*)[kTld]>( ssm + kPanel * kTld );
+    double * sX = ssm + kPanel * kTld + solve_block_doubles<T>();   // [64][ldv]: x_q (forward) / x_r (backward)
     double * sY = sX + kPanel * ldv;                // [64][ldv]: y_q
     __shared__ std::int64_t trow[kSolveRest];
     const int tid = threadIdx.x;
@@ -1342,15 +1346,21 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
     // the panel's rest block (factor data: final before any solve step)
     const T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
     const T * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
-    auto stage_src = [&]( int idx, double & ) -> const T *
+    if( has_rest )
     {
-        const int i = idx >> 6, jj = idx & 63;
-        const int col = t.c0 + jj;
-        if( i >= nb || jj >= cw ) { return nullptr; }
-        return (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col : U1 + (std::int64_t)i * t.ld1 + (col - m);
-    };
-    auto stage_dst = [&]( int idx ) { return &sP[idx >> 6][idx & 63]; };
-    if( has_rest ) { stage_block<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( U0, stage_src, stage_dst ); }
+#pragma unroll 4
+        for( int u = 0; u < kPanel * kPanel / kSolveThreads; ++u )
+        {
+            const int idx = tid + u * kSolveThreads;
+            const int i = idx >> 6, jj = idx & 63;
+            const int col = t.c0 + jj;
+            const bool valid = i < nb && jj < cw;
+            const T * src = !valid ? U0 : (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col
+                                                    : U1 + (std::int64_t)i * t.ld1 + (col - m);
+            if constexpr ( sizeof(T) == 8 ) { cp_async_8( reinterpret_cast<double *>( &sP[i][jj] ), reinterpret_cast<const double *>( src ), valid ); }
+            else { cp_async_4( &sP[i][jj], src, valid ); }
+        }
+    }
     if constexpr ( kPdl ) { pdl_wait(); }
     // y_q: the panel's rows of `in` (forward: every task; backward: the owner)
     const bool need_y = !upper || owner;
@@ -1374,7 +1384,6 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         }
     }
     cp_async_wait_all();
-    if( has_rest ) { stage_finish<T, kPanel * kPanel / kSolveThreads, kSolveThreads>( stage_src, stage_dst ); }
     __syncthreads();
 
     const int fi = lane >> 2, fj = 2 * (lane & 3);     // accumulator fragment: row fi, columns fj, fj + 1
@@ -1409,7 +1418,7 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         // rest rows: y_r -= P^T x_q
 #pragma unroll
         for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
-        warp_rows_product<nct>( acc, 0, nbb, [&]( int i, int kk ) { return sP[kk][o + i]; },
+        warp_rows_product<nct>( acc, 0, nbb, [&]( int i, int kk ) { return static_cast<double>( sP[kk][o + i] ); },
                                              [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
         const int jj = o + fi;
         if( jj < cw )
@@ -1436,7 +1445,7 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         // sY rows of this warp <- (owner ? y_q : 0) - P x_r
         if( has_rest && o < nb )
         {
-            warp_rows_product<nct>( acc, 0, (cw + 7) >> 3, [&]( int i, int kk ) { return sP[o + i][kk]; },
+            warp_rows_product<nct>( acc, 0, (cw + 7) >> 3, [&]( int i, int kk ) { return static_cast<double>( sP[o + i][kk] ); },
                                                            [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
 #pragma unroll
             for( int ct = 0; ct < nct; ++ct )
@@ -2365,9 +2374,10 @@ static int solve_lkp( int k )
     return l;
 }
 
+template<typename T>
 static size_t solve_smem_bytes( int k )
 {
-    return sizeof(double) * (2 * kPanel * kTld + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
+    return sizeof(double) * (kPanel * kTld + solve_block_doubles<T>() + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
 }
 
 template<typename T>
@@ -2375,7 +2385,7 @@ void launch_solve_dag( const SolveDagArgs & args, int grid, const T * arena, dou
                        cudaStream_t st )
 {
     if( args.ntasks <= 0 || grid <= 0 ) { return; }
-    const size_t sm = solve_smem_bytes( k );
+    const size_t sm = solve_smem_bytes<T>( k );
     switch( solve_lkp( k ) )
     {
         case 3:  solve_dag_kernel<T, 8><<<grid, kSolveThreads, sm, st>>>( args, arena, in, out, ld, k ); break;
@@ -2388,7 +2398,7 @@ void launch_solve_dag( const SolveDagArgs & args, int grid, const T * arena, dou
 template<typename T>
 int solve_dag_occupancy( int k )
 {
-    const size_t sm = solve_smem_bytes( k );
+    const size_t sm = solve_smem_bytes<T>( k );
     int n = 0;
     cudaError_t e = cudaSuccess;
     switch( solve_lkp( k ) )
@@ -2411,7 +2421,7 @@ void launch_solve_step( const SolveRestTask * tasks, int count, bool upper, cons
                         const std::int32_t * sn_inner, double * in, double * out, int ld, int k, cudaStream_t st )
 {
     if( count <= 0 ) { return; }
-    const size_t sm = solve_smem_bytes( k );
+    const size_t sm = solve_smem_bytes<T>( k );
     const int u = upper ? 1 : 0;
     switch( solve_lkp( k ) )
     {
@@ -2537,22 +2547,22 @@ cudaError_t configure_kernels()
         { reinterpret_cast<const void *>( gemm_tc_kernel ), kGemmSmemBytesF },
         { reinterpret_cast<const void *>( factor_dag_kernel<double> ), kDagSmemBytes },
         { reinterpret_cast<const void *>( factor_dag_kernel<float> ), kDagSmemBytes },
-        { reinterpret_cast<const void *>( solve_step_kernel<double, 8> ), solve_smem_bytes( 8 ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<double, 16> ), solve_smem_bytes( 16 ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<double, 32> ), solve_smem_bytes( 32 ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<double, 64> ), solve_smem_bytes( 64 ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<float, 8> ), solve_smem_bytes( 8 ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<float, 16> ), solve_smem_bytes( 16 ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<float, 32> ), solve_smem_bytes( 32 ) },
-        { reinterpret_cast<const void *>( solve_step_kernel<float, 64> ), solve_smem_bytes( 64 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<double, 8> ), solve_smem_bytes( 8 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<double, 16> ), solve_smem_bytes( 16 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<double, 32> ), solve_smem_bytes( 32 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<double, 64> ), solve_smem_bytes( 64 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<float, 8> ), solve_smem_bytes( 8 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<float, 16> ), solve_smem_bytes( 16 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<float, 32> ), solve_smem_bytes( 32 ) },
-        { reinterpret_cast<const void *>( solve_dag_kernel<float, 64> ), solve_smem_bytes( 64 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 8> ), solve_smem_bytes<double>( 8 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 16> ), solve_smem_bytes<double>( 16 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 32> ), solve_smem_bytes<double>( 32 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<double, 64> ), solve_smem_bytes<double>( 64 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 8> ), solve_smem_bytes<float>( 8 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 16> ), solve_smem_bytes<float>( 16 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 32> ), solve_smem_bytes<float>( 32 ) },
+        { reinterpret_cast<const void *>( solve_step_kernel<float, 64> ), solve_smem_bytes<float>( 64 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 8> ), solve_smem_bytes<double>( 8 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 16> ), solve_smem_bytes<double>( 16 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 32> ), solve_smem_bytes<double>( 32 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<double, 64> ), solve_smem_bytes<double>( 64 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 8> ), solve_smem_bytes<float>( 8 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 16> ), solve_smem_bytes<float>( 16 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 32> ), solve_smem_bytes<float>( 32 ) },
+        { reinterpret_cast<const void *>( solve_dag_kernel<float, 64> ), solve_smem_bytes<float>( 64 ) },
         { reinterpret_cast<const void *>( super_inv_kernel<double> ), kSuperInvSmem },
         { reinterpret_cast<const void *>( super_inv_kernel<float> ), kSuperInvSmem },
         { reinterpret_cast<const void *>( super_diag_kernel<8> ), super_solve_smem( 8 ) },
