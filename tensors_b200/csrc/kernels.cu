@@ -1974,6 +1974,8 @@ int grid_for( std::int64_t work, int threads )
 // one product with T.  64 x 64 blocks throughout; warp w owns output rows
 // 8w..8w+7 as 8 x 8 DMMA tiles.
 constexpr int kSld = kPanel + 1;                        // padded smem row of a 64 x 64 block
+// Doubles of shared memory a 64 x kSld block of T takes (rounded up to 16 bytes).
+template<typename T> __host__ __device__ constexpr int super_block_doubles() { return ((kPanel * kSld * static_cast<int>( sizeof(T) ) + 15) / 16) * 2; }
 constexpr size_t kSuperInvSmem = sizeof(double) * 4 * kPanel * kSld;
 
 __device__ __forceinline__ int super_block_rows( const SuperPanel & sp, int b ) { return min( kPanel, sp.rows - b * kPanel ); }
@@ -2176,8 +2178,9 @@ __global__ __launch_bounds__(256) void super_rest_kernel( const SuperSolveTask *
     constexpr int nct = KP / 8;
     constexpr int ldv = KP + 4;
     __shared__ std::int64_t trow[kSolveRest];
-    double (*P)[kSld] = reinterpret_cast<double (*)[kSld]>( rsm );
-    double * V = rsm + kPanel * kSld;                   // [64][ldv]
+    // the factor block in the factor's type (FP32 storage: half the shared memory), widened as read
+    T (*P)[kSld] = reinterpret_cast<T (*)[kSld]>( rsm );
+    double * V = rsm + super_block_doubles<T>();        // [64][ldv]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r1 = sp.r0 + sp.rows;
     const int m = sp.n0 - r1;
@@ -2193,17 +2196,17 @@ __global__ __launch_bounds__(256) void super_rest_kernel( const SuperSolveTask *
     // P: rows of block b (U rows r0 + 64 b + rr), the chunk's rest columns
     const T * U0 = arena + sp.u0;
     const T * U1 = arena + sp.u1;
-    auto src = [&]( int idx, double & fill ) -> const T *
+#pragma unroll 4
+    for( int idx = tid; idx < kPanel * kPanel; idx += 256 )
     {
-        fill = 0.0;
         const int rr = idx >> 6, jj = idx & 63;
-        if( rr >= nbb || jj >= cw ) { return nullptr; }
+        const bool valid = rr < nbb && jj < cw;
         const int col = task.c0 + jj;
         const std::int64_t urow = sp.r0 + kPanel * b + rr;
-        return col < m ? U0 + urow * sp.ld0 + r1 + col : U1 + urow * sp.ld1 + (col - m);
-    };
-    auto dst = [&]( int idx ) { return &P[idx >> 6][idx & 63]; };
-    stage_block<T, kPanel * kPanel / 256, 256>( U0, src, dst );
+        const T * src = !valid ? U0 : col < m ? U0 + urow * sp.ld0 + r1 + col : U1 + urow * sp.ld1 + (col - m);
+        if constexpr ( sizeof(T) == 8 ) { cp_async_8( reinterpret_cast<double *>( &P[rr][jj] ), reinterpret_cast<const double *>( src ), valid ); }
+        else { cp_async_4( &P[rr][jj], src, valid ); }
+    }
     pdl_wait();
     __syncthreads();                                    // trow
     if( upper )
@@ -2219,7 +2222,6 @@ __global__ __launch_bounds__(256) void super_rest_kernel( const SuperSolveTask *
     }
     else { stage_rows<KP>( V, out, brow + kPanel * b, nbb, ld, k ); }
     cp_async_wait_all();
-    stage_finish<T, kPanel * kPanel / 256, 256>( src, dst );
     __syncthreads();
     double acc[nct][2];
 #pragma unroll
@@ -2230,9 +2232,9 @@ __global__ __launch_bounds__(256) void super_rest_kernel( const SuperSolveTask *
         for( int ct = 0; ct < nct; ++ct )
         {
             // forward: acc(jj, c) = sum_rr P[rr][jj] x_b[rr][c]; back: acc(rr, c) = sum_jj P[rr][jj] x_rest[jj][c]
-            if( upper ) { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return P[8 * warp + i][8 * kb + kk]; },
+            if( upper ) { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return static_cast<double>( P[8 * warp + i][8 * kb + kk] ); },
                                                [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
-            else        { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return P[8 * kb + kk][8 * warp + i]; },
+            else        { dmma_8x8x8( acc[ct], [&]( int i, int kk ) { return static_cast<double>( P[8 * kb + kk][8 * warp + i] ); },
                                                [&]( int kk, int j ) { return V[(8 * kb + kk) * ldv + 8 * ct + j]; } ); }
         }
     }
@@ -2444,6 +2446,12 @@ static size_t super_solve_smem( int k )
     return sizeof(double) * (kPanel * kSld + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
 }
 
+template<typename T>
+static size_t super_rest_smem( int k )
+{
+    return sizeof(double) * (super_block_doubles<T>() + kPanel * ((1 << solve_lkp( k )) + 4));
+}
+
 void launch_super_diag( const SuperSolveTask * tasks, int count, const SuperPanel * sps, const double * tbuf, bool upper,
                         const double * in, const double * zbuf, double * out, int ld, int k, cudaStream_t st )
 {
@@ -2465,7 +2473,7 @@ void launch_super_rest( const SuperSolveTask * tasks, int count, const SuperPane
                         cudaStream_t st )
 {
     if( count <= 0 ) { return; }
-    const size_t sm = super_solve_smem( k );
+    const size_t sm = super_rest_smem<T>( k );
     const int u = upper ? 1 : 0;
     switch( solve_lkp( k ) )
     {
@@ -2569,14 +2577,14 @@ cudaError_t configure_kernels()
         { reinterpret_cast<const void *>( super_diag_kernel<16> ), super_solve_smem( 16 ) },
         { reinterpret_cast<const void *>( super_diag_kernel<32> ), super_solve_smem( 32 ) },
         { reinterpret_cast<const void *>( super_diag_kernel<64> ), super_solve_smem( 64 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<double, 8> ), super_solve_smem( 8 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<double, 16> ), super_solve_smem( 16 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<double, 32> ), super_solve_smem( 32 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<double, 64> ), super_solve_smem( 64 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<float, 8> ), super_solve_smem( 8 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<float, 16> ), super_solve_smem( 16 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<float, 32> ), super_solve_smem( 32 ) },
-        { reinterpret_cast<const void *>( super_rest_kernel<float, 64> ), super_solve_smem( 64 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 8> ), super_rest_smem<double>( 8 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 16> ), super_rest_smem<double>( 16 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 32> ), super_rest_smem<double>( 32 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<double, 64> ), super_rest_smem<double>( 64 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 8> ), super_rest_smem<float>( 8 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 16> ), super_rest_smem<float>( 16 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 32> ), super_rest_smem<float>( 32 ) },
+        { reinterpret_cast<const void *>( super_rest_kernel<float, 64> ), super_rest_smem<float>( 64 ) },
     };
     for( const auto & a : attrs )
     {
