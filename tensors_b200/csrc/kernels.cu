@@ -1784,10 +1784,20 @@ __global__ __launch_bounds__(256) void spmv_group_kernel( int n, const std::int6
         {
             const int col = c0 + c;
             if( col >= k ) { continue; }
-            double s = 0.0;
-#pragma unroll 8
-            for( std::int64_t e = e0; e < e1; ++e ) { s = fma( vals[e], X[(std::int64_t)inner[e] * ldx + col], s ); }
-            const double ax = s + shift * X[i * ldx + col];
+            // four independent sums keep four gathers of x in flight per lane
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            std::int64_t e = e0;
+            for( ; e + 4 <= e1; e += 4 )
+            {
+                const double v0 = vals[e], v1 = vals[e + 1], v2 = vals[e + 2], v3 = vals[e + 3];
+                const std::int64_t j0 = inner[e], j1 = inner[e + 1], j2 = inner[e + 2], j3 = inner[e + 3];
+                s0 = fma( v0, X[j0 * ldx + col], s0 );
+                s1 = fma( v1, X[j1 * ldx + col], s1 );
+                s2 = fma( v2, X[j2 * ldx + col], s2 );
+                s3 = fma( v3, X[j3 * ldx + col], s3 );
+            }
+            for( ; e < e1; ++e ) { s0 = fma( vals[e], X[(std::int64_t)inner[e] * ldx + col], s0 ); }
+            const double ax = ((s0 + s1) + (s2 + s3)) + shift * X[i * ldx + col];
             R[i * ldr + col] = B ? B[i * ldb + col] - ax : ax;
         }
     }
@@ -2601,8 +2611,8 @@ void launch_apply_shifted( int n, const std::int64_t * outer, const std::int32_t
     if( n <= 0 ) { return; }
     if( k >= 3 )
     {
-        // 8 blocks per SM (measured best on a 3-dof 27-point stencil)
-        const int grid = static_cast<int>( std::min<std::int64_t>( 148 * 8, ((std::int64_t)n * 32 + 255) / 256 ) );
+        // one warp per 32 / KP rows, up to 32 blocks per SM (measured best on a 3-dof 27-point stencil)
+        const int grid = grid_for( (std::int64_t)n * 32, 256 );
         by_column_width( k, [&]( auto kp ) {
             if constexpr ( decltype( kp )::value >= 4 )
             {
