@@ -1979,9 +1979,9 @@ int grid_for( std::int64_t work, int threads )
 
 // ------------------------------------------------------ super-panel solve
 // Large fronts solve up to 1024 pivot rows per step (SuperPanel, plan.hpp): the
-// inverse T of the diagonal block, formed after the factorization from the
-// 64-row panel inverses, replaces up to sixteen sequential panel steps by one
-// product with T.  64 x 64 blocks throughout; warp w owns output rows
+// inverse T of the 512 x 512 diagonal block, formed after the factorization
+// from the 64-row panel inverses, replaces eight sequential panel steps by
+// one product with T.  64 x 64 blocks throughout; warp w owns output rows
 // 8w..8w+7 as 8 x 8 DMMA tiles.
 constexpr int kSld = kPanel + 1;                        // padded smem row of a 64 x 64 block
 // Doubles of shared memory a 64 x kSld block of T takes (rounded up to 16 bytes).
