@@ -160,7 +160,7 @@ struct tb_chol
     DeviceArray<tb::SuperPanel>     spanels;     // super-panel solve of the large fronts (Plan::spanels)
     DeviceArray<tb::SuperInvTask>   sinv;
     DeviceArray<tb::SuperSolveTask> ssolve;
-    DeviceArray<double>             tsuper;      // their diagonal-block inverses (up to 1024 x 1024)
+    DeviceArray<double>             tsuper;      // their 512 x 512 inverses
     DeviceArray<std::int64_t>       a_outer;     // caller-order pattern, for residuals
     DeviceArray<std::int32_t>       a_inner;
     DeviceArray<double>             values;      // caller-order values of the last factorization

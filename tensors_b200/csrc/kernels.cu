@@ -1978,7 +1978,7 @@ int grid_for( std::int64_t work, int threads )
 }
 
 // ------------------------------------------------------ super-panel solve
-// Large fronts solve up to 1024 pivot rows per step (SuperPanel, plan.hpp): the
+// Large fronts solve 512 pivot rows per step (SuperPanel, plan.hpp): the
 // inverse T of the 512 x 512 diagonal block, formed after the factorization
 // from the 64-row panel inverses, replaces eight sequential panel steps by
 // one product with T.  64 x 64 blocks throughout; warp w owns output rows

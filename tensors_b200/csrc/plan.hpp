@@ -224,14 +224,14 @@ struct ExtendPullTask
 };
 constexpr std::int64_t kExtendPullEntries = 16384;   // target child entries per pull task
 
-// The solve of a large front steps through its pivot rows 1024 at a time
-// (super-panels) instead of 64 at a time: the inverse of each 1024 x 1024
+// The solve of a large front steps through its pivot rows 512 at a time
+// (super-panels) instead of 64 at a time: the inverse of each 512 x 512
 // diagonal block of U0 (T, FP64, upper triangular, row-major, built from
 // the 64-row panel inverses after the factorization by block back
-// substitution) turns up to sixteen sequential panel steps into one.  A front uses
+// substitution) turns eight sequential panel steps into one.  A front uses
 // super-panels when it has at least kSuperMinRows pivot rows.
-constexpr int kSuperPanels  = 16;
-constexpr int kSuperRows    = kSuperPanels * kPanel;   // 1024
+constexpr int kSuperPanels  = 8;
+constexpr int kSuperRows    = kSuperPanels * kPanel;   // 512
 constexpr int kSuperMinRows = 256;
 
 struct SuperPanel
@@ -239,7 +239,7 @@ struct SuperPanel
     std::int64_t u0, u1, inner;    // the front's U0 / U1 arena offsets and its SN_inner offset
     std::int64_t t;                // offset of the inverse (ldt x ldt doubles, row-major)
     std::int32_t n0, n1, ld0, ld1;
-    std::int32_t r0, rows;         // first pivot row of the block (a multiple of kSuperRows) and its row count
+    std::int32_t r0, rows;         // first pivot row of the block (a multiple of 512) and its row count
     std::int32_t row0;             // the front's first global row
     std::int32_t panel[kSuperPanels];   // inverse-block index of each 64-row panel (-1 beyond rows)
     std::int32_t ldt;              // the inverse's edge: rows rounded up to 64
