@@ -2503,11 +2503,21 @@ int tb_chol_launch_profile( tb_chol * h, std::int64_t * info, double * ms, std::
         }
         else if( info )
         {
-            const tb::Launch & L = h->plan.factor_launches[static_cast<size_t>( i - 1 )];
-            info[4 * i + 0] = static_cast<std::int64_t>( L.kind == tb::LaunchKind::ExtendPull ? tb::LaunchKind::Extend : L.kind );
-            info[4 * i + 1] = L.level;
-            info[4 * i + 2] = L.step;
-            info[4 * i + 3] = L.count;
+            // the factor launches, then the super-panel inverse rounds (reported as Invert)
+            const std::size_t nf = h->plan.factor_launches.size();
+            const std::size_t j = static_cast<std::size_t>( i - 1 );
+            const tb::Launch * L = j < nf ? &h->plan.factor_launches[j]
+                                          : (j - nf < h->plan.sinv_launches.size() ? &h->plan.sinv_launches[j - nf] : nullptr);
+            if( L == nullptr ) { info[4 * i] = -1; info[4 * i + 1] = -1; info[4 * i + 2] = -1; info[4 * i + 3] = 0; }
+            else
+            {
+                const tb::LaunchKind kind = L->kind == tb::LaunchKind::ExtendPull ? tb::LaunchKind::Extend
+                                          : L->kind == tb::LaunchKind::SuperInv ? tb::LaunchKind::Invert : L->kind;
+                info[4 * i + 0] = static_cast<std::int64_t>( kind );
+                info[4 * i + 1] = L->level;
+                info[4 * i + 2] = L->step;
+                info[4 * i + 3] = L->count;
+            }
         }
         if( ms ) { ms[i] = h->launch_ms[static_cast<size_t>( i )]; }
     }
