@@ -296,24 +296,56 @@ __global__ __launch_bounds__(256) void extend_pull_kernel( const ExtendPullTask 
             const bool upper_part = i < e.mid;
             for( ; k < nch; k += kWarps )
             {
-                const int j0 = i + k * kChunk + lane;
-                T v[kU];
-                T * dst[kU];
-#pragma unroll
-                for( int u = 0; u < kU; ++u )
+                if constexpr ( sizeof(T) == 4 )
                 {
-                    const int j = j0 + 32 * u;
-                    dst[u] = nullptr;
-                    v[u] = T( 0 );
-                    if( j < e.m1 )
+                    // FP32: lane quads of consecutive columns; a quad whose targets are four
+                    // consecutive, 16-byte aligned entries goes out as one vector reduction
+                    const int j0 = i + k * kChunk + 4 * lane;
+                    T v[4];
+                    T * dst[4];
+#pragma unroll
+                    for( int u = 0; u < 4; ++u )
                     {
-                        const int lj = lut[j];
-                        v[u] = Wi[j];
-                        dst[u] = upper_part ? ((j < e.mid) ? row0 + lj : row1 + lj) : rowv + lj;
+                        const int j = j0 + u;
+                        dst[u] = nullptr;
+                        v[u] = T( 0 );
+                        if( j < e.m1 )
+                        {
+                            const int lj = lut[j];
+                            v[u] = Wi[j];
+                            dst[u] = upper_part ? ((j < e.mid) ? row0 + lj : row1 + lj) : rowv + lj;
+                        }
+                    }
+                    const bool quad = dst[3] != nullptr && dst[1] == dst[0] + 1 && dst[2] == dst[0] + 2 && dst[3] == dst[0] + 3
+                                      && (reinterpret_cast<std::uintptr_t>( dst[0] ) & 15u) == 0;
+                    if( quad ) { red_add_v4f32( reinterpret_cast<float *>( dst[0] ), v[0], v[1], v[2], v[3] ); }
+                    else
+                    {
+#pragma unroll
+                        for( int u = 0; u < 4; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
                     }
                 }
+                else
+                {
+                    const int j0 = i + k * kChunk + lane;
+                    T v[kU];
+                    T * dst[kU];
 #pragma unroll
-                for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
+                    for( int u = 0; u < kU; ++u )
+                    {
+                        const int j = j0 + 32 * u;
+                        dst[u] = nullptr;
+                        v[u] = T( 0 );
+                        if( j < e.m1 )
+                        {
+                            const int lj = lut[j];
+                            v[u] = Wi[j];
+                            dst[u] = upper_part ? ((j < e.mid) ? row0 + lj : row1 + lj) : rowv + lj;
+                        }
+                    }
+#pragma unroll
+                    for( int u = 0; u < kU; ++u ) { if( dst[u] ) { red_add_any( dst[u], v[u] ); } }
+                }
             }
         }
     }
