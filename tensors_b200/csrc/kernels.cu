@@ -2018,7 +2018,7 @@ int grid_for( std::int64_t work, int threads )
 constexpr int kSld = kPanel + 1;                        // padded smem row of a 64 x 64 block
 // Doubles of shared memory a 64 x kSld block of T takes (rounded up to 16 bytes).
 template<typename T> __host__ __device__ constexpr int super_block_doubles() { return ((kPanel * kSld * static_cast<int>( sizeof(T) ) + 15) / 16) * 2; }
-constexpr size_t kSuperInvSmem = sizeof(double) * 4 * kPanel * kSld;
+constexpr size_t kSuperInvSmem = sizeof(double) * 2 * kPanel * kSld;
 
 __device__ __forceinline__ int super_block_rows( const SuperPanel & sp, int b ) { return min( kPanel, sp.rows - b * kPanel ); }
 
@@ -2051,10 +2051,11 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     const SuperInvTask task = tasks[blockIdx.x];
     const SuperPanel sp = sps[task.sp];
     pdl_wait();
+    // two 64 x 64 blocks: the products' operands, then S (in A's place) and T_ii (in Bm's)
     double (*A)[kSld] = reinterpret_cast<double (*)[kSld]>( ism );
     double (*Bm)[kSld] = A + kPanel;
-    double (*S)[kSld] = Bm + kPanel;
-    double (*Tii)[kSld] = S + kPanel;
+    double (*S)[kSld] = A;
+    double (*Tii)[kSld] = Bm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int i = task.i, j = task.j;
     const int nbi = super_block_rows( sp, i );
@@ -2062,11 +2063,14 @@ __global__ __launch_bounds__(256) void super_inv_kernel( const SuperInvTask * __
     auto load_tinv = [&]( double (*D)[kSld], int b, int nbb )
     {
         const double * src = tinv + (std::int64_t)sp.panel[b] * (kPanel * kPanel);
+#pragma unroll 4
         for( int idx = tid; idx < kPanel * kPanel; idx += 256 )
         {
             const int r = idx >> 6, c = idx & 63;
-            D[r][c] = (r < nbb && c < nbb) ? src[idx] : 0.0;
+            const bool valid = r < nbb && c < nbb;
+            cp_async_8( &D[r][c], valid ? src + idx : src, valid );
         }
+        cp_async_wait_all();
     };
     if( i == j )
     {
