@@ -155,11 +155,22 @@ __global__ void assemble_kernel( const double * __restrict__ values, const std::
 template<typename T>
 __device__ __forceinline__ void zero_body( const ZeroTask & t, T * __restrict__ arena )
 {
+    // a row's upper part [r, n): the entries up to the first 16-byte boundary, then 16-byte
+    // stores, then the tail
+    constexpr int kV = 16 / static_cast<int>( sizeof(T) );
     const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     for( int r = t.row_begin + static_cast<int>( threadIdx.x >> 5 ); r < t.row_end; r += warps )
     {
-        T * row = arena + t.offset + static_cast<std::int64_t>( r ) * t.ld;
-        for( int c = r + lane; c < t.n; c += 32 ) { row[c] = T( 0 ); }
+        T * p = arena + t.offset + static_cast<std::int64_t>( r ) * t.ld + r;
+        const int len = t.n - r;
+        int head = static_cast<int>( ((16u - (reinterpret_cast<std::uintptr_t>( p ) & 15u)) & 15u) / sizeof(T) );
+        head = min( head, len );
+        if( lane < head ) { p[lane] = T( 0 ); }
+        T * q = p + head;
+        const int nv = (len - head) / kV;
+        float4 * qv = reinterpret_cast<float4 *>( q );
+        for( int v = lane; v < nv; v += 32 ) { qv[v] = make_float4( 0.f, 0.f, 0.f, 0.f ); }
+        for( int c = nv * kV + lane; c < len - head; c += 32 ) { q[c] = T( 0 ); }
     }
 }
 
