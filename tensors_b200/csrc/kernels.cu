@@ -828,38 +828,58 @@ __device__ __forceinline__ void trsm_body( const PanelTask & t, T * __restrict__
     stage_finish<T, kPanel * kRestChunk / kTrsmThreads, kTrsmThreads>( stage_src, stage_dst );
     __syncthreads();
     const int nct = (cw + kSub - 1) / kSub;
+    double res[kRestChunk / kSub][2];
+#pragma unroll
+    for( int ct = 0; ct < kRestChunk / kSub; ++ct )
+    {
+        res[ct][0] = 0.0; res[ct][1] = 0.0;
+        const int rb = (warp + ct) & (kSubs - 1);
+        if( rb >= nbb || ct >= nct ) { continue; }
+        for( int kb = 0; kb <= rb; ++kb )
+        {
+            dmma_8x8x8( res[ct], [&]( int i, int k ) { return Ti[kSub * kb + k][kSub * rb + i]; },
+                                 [&]( int k, int j ) { return X[kSub * kb + k][kSub * ct + j]; } );
+        }
+    }
+    // the products are done: the results replace the staged block, then go out coalesced
+    __syncthreads();
+#pragma unroll
     for( int ct = 0; ct < kRestChunk / kSub; ++ct )
     {
         const int rb = (warp + ct) & (kSubs - 1);
         if( rb >= nbb || ct >= nct ) { continue; }
-        double acc[2] = { 0.0, 0.0 };
-        for( int kb = 0; kb <= rb; ++kb )
+        const int r = kSub * rb + (lane >> 2), cc = kSub * ct + 2 * (lane & 3);
+        X[r][cc] = static_cast<double>( static_cast<T>( res[ct][0] ) );
+        X[r][cc + 1] = static_cast<double>( static_cast<T>( res[ct][1] ) );
+    }
+    __syncthreads();
+    // U rows: consecutive threads, consecutive columns
+    for( int idx = tid; idx < kPanel * kRestChunk; idx += kTrsmThreads )
+    {
+        const int r = idx >> 6, cc = idx & 63;
+        if( r >= nb || cc >= cw ) { continue; }
+        const int col = t.c0 + cc;
+        const T v = static_cast<T>( X[r][cc] );
+        if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = v; }
+        else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = v; }
+    }
+    if constexpr ( sizeof(T) == 4 )
+    {
+        if( img != nullptr && t.img >= 0 )
         {
-            dmma_8x8x8( acc, [&]( int i, int k ) { return Ti[kSub * kb + k][kSub * rb + i]; },
-                             [&]( int k, int j ) { return X[kSub * kb + k][kSub * ct + j]; } );
-        }
-        const int r = kSub * rb + (lane >> 2);
-#pragma unroll
-        for( int e = 0; e < 2; ++e )
-        {
-            const int cc = kSub * ct + 2 * (lane & 3) + e;
-            if( r < nb && cc < cw )
+            // the stored FP32 values split into TF32 hi + lo, for the tensor-core tiles: the
+            // image is K-major, so a warp writes one column's 32 k values of a k-chunk at once
+            // (128 contiguous bytes per part)
+            const std::int64_t lo_off = static_cast<std::int64_t>( t.img_tf ) * (kImgRows * kImgK);
+            for( int pair = warp; pair < 2 * cw; pair += kTrsmThreads / 32 )
             {
-                const int col = t.c0 + cc;
-                const T v = static_cast<T>( acc[e] );
-                if( col < m ) { U0[(std::int64_t)(t.r0 + r) * t.ld0 + r1 + col] = v; }
-                else          { U1[(std::int64_t)(t.r0 + r) * t.ld1 + (col - m)] = v; }
-                if constexpr ( sizeof(T) == 4 )
-                {
-                    if( img != nullptr && t.img >= 0 )
-                    {
-                        // the stored FP32 value split into TF32 hi + lo, for the tensor-core tiles
-                        const unsigned hi = to_tf32( v );
-                        const std::int64_t o = img_offset( t, t.r0 + r, col, r1, m );
-                        img[o] = __uint_as_float( hi );
-                        img[o + static_cast<std::int64_t>( t.img_tf ) * (kImgRows * kImgK)] = __uint_as_float( to_tf32( v - __uint_as_float( hi ) ) );
-                    }
-                }
+                const int cc = pair >> 1, r = 32 * (pair & 1) + lane;
+                if( r >= nb ) { continue; }
+                const float v = static_cast<float>( X[r][cc] );
+                const unsigned hi = to_tf32( v );
+                const std::int64_t o = img_offset( t, t.r0 + r, t.c0 + cc, r1, m );
+                img[o] = __uint_as_float( hi );
+                img[o + lo_off] = __uint_as_float( to_tf32( v - __uint_as_float( hi ) ) );
             }
         }
     }
