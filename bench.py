@@ -635,6 +635,68 @@ def c5_reference_time(mats, which, repeat, nrhs, reqs):
             "busy_s": total, "factor_s_per_matrix": {str(j): v[0] for j, v in per.items()}}
 
 
+def run_setup(args):
+    """Host set-up of the C2 and C3 systems (no GPU): both nested-dissection orderings, the
+    symbolic analysis by phase (the phase ranges' host times), the device plan and the plan
+    check, each the median of --steps runs.  One JSON line."""
+    import statistics
+
+    from tensors_b200 import build as tb_build
+    from tensors_b200 import matrices, ordering, trace
+    from tensors_b200.cholesky import CholeskyDecomposition
+
+    tb_build.build()
+    P = "Sparse::CholeskyDecomposition::"
+    phases = [("init", P + "Init"), ("elimination_tree", P + "EliminationTree"), ("postordering", P + "PostOrdering"),
+              ("supernodes", P + "FindMaximalSupernodes"), ("supernode_starts", "tensors_b200::SupernodeStarts"),
+              ("assembly_tree", P + "CreateAssemblyTree"),
+              ("analysis", P + "SymbolicFactorization"), ("plan", "tensors_b200::DevicePlan")]
+    systems = {"c2": (f"3D 7-point Laplacian {GRID}^3", lambda: matrices.grid_laplacian_3d(GRID, SEED, SHIFT)),
+               "c3": (f"3-dof 27-point vector Laplacian {C3_GRID}^3",
+                      lambda: matrices.vector_laplacian_3d(C3_GRID, C3_SEED, C3_SHIFT))}
+    steps = max(1, args.steps)
+    out = {}
+    for key, (name, make) in systems.items():
+        A = make()
+        rec = {"n": A.n, "nnz": int(A.outer[-1])}
+        for oname, fn in (("geometric", ordering.nested_dissection), ("graph", ordering.graph_nested_dissection)):
+            ts = []
+            for _ in range(steps):
+                t0 = time.perf_counter()
+                perm = fn(A)
+                ts.append(1e3 * (time.perf_counter() - t0))
+            rec[f"ordering_{oname}_ms"] = statistics.median(ts)
+        perm = ordering.graph_nested_dissection(A) if key == "c2" else ordering.nested_dissection(A)
+        got = {k: [] for k, _ in phases}
+        got["plan_check"] = []
+        for _ in range(steps):
+            trace.record(True)
+            try:
+                c = CholeskyDecomposition(A.outer, A.inner, perm)
+                c.SymbolicFactorization()
+                times = dict(trace.times())
+            finally:
+                trace.record(False)
+            for k, tag in phases:
+                got[k].append(times.get(tag, float("nan")))
+            t0 = time.perf_counter()
+            c.CheckPlan()
+            got["plan_check"].append(1e3 * (time.perf_counter() - t0))
+        stats = c.PlanStats()
+        # the SymbolicFactorization range holds the plan build: analysis = the range less the plan;
+        # a phase that did not run (PostOrdering of an ordering already postordered) is null
+        got["analysis"] = [a - p for a, p in zip(got["analysis"], got["plan"])]
+        rec.update({f"{k}_ms": (None if any(x != x for x in v) else statistics.median(v)) for k, v in got.items()})
+        rec.update({"fronts": stats["fronts"], "gemm_tasks": stats["gemm_tasks"], "supernodes": stats["supernodes"]})
+        out[key] = rec
+    line = {"metric": "host set-up time (ordering, symbolic analysis, device plan, plan check)", "unit": "ms",
+            "value": out["c2"]["analysis_ms"] + out["c2"]["plan_ms"], "higher_is_better": False,
+            "steps": steps, "cores": os.cpu_count(), "data": "synthetic (seeded)",
+            "config": {"workload": "C2 and C3 systems, median of steps", "systems": out}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_c5(args):
     """Serving: a Poisson stream of factor / solve requests over a pool of 2D mesh Laplacians
     (quality meshes, n 1k-50k) and 3D 7-point grids (32^3-64^3), 1-64 RHS each, 30% solves on
@@ -781,9 +843,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=GRID, help="grid edge (profiling runs on smaller cases)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "setup"],
                     help="c2 (default): the headline FP64 64^3 Laplacian; c3: mixed vs FP64 vector Laplacian; "
-                         "c4: batched Delaunay systems; c5: serving stream")
+                         "c4: batched Delaunay systems; c5: serving stream; setup: host set-up phases (no GPU)")
     ap.add_argument("--batch", type=int, default=0, help="c4: number of systems (default 2000)")
     ap.add_argument("--requests", type=int, default=0, help="c5: number of requests (default 2000 of the 10000)")
     ap.add_argument("--schedule", default=None, help="c4: factorization schedule of the batch")
@@ -813,6 +875,8 @@ def main():
         return run_c4(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload == "setup":
+        return run_setup(args)
 
     import torch
     import torch.distributed as dist

@@ -94,9 +94,14 @@ const char * tb_last_error( void );
  * Numeric.hpp:34), visible in timeline tools.  tb_trace_record(1) clears and
  * starts a host-side list of the ranges entered (0 stops it);
  * tb_trace_names copies it, one name per line, into buf (at most cap bytes,
- * NUL-terminated) and returns the bytes the whole list needs. */
+ * NUL-terminated) and returns the bytes the whole list needs.
+ * tb_trace_times writes the host wall time of each recorded range, in the
+ * same order, in milliseconds (-1 for a range still open), into ms (at most
+ * cap entries) and returns the number of recorded ranges: the durations the
+ * reference's TOOLS_PTIMER logs for the same phases. */
 int tb_trace_record( int32_t enabled );
 int64_t tb_trace_names( char * buf, int64_t cap );
+int64_t tb_trace_times( double * ms, int64_t cap );
 
 /* Library / device information: CUDA device ordinal used by new handles. */
 int tb_set_device( int device );
@@ -105,7 +110,8 @@ int tb_set_device( int device );
  * perm == NULL: the matrix is already permuted (ctor :350).  Otherwise
  * perm[i] is the original index placed at position i (ctor :336,
  * Inverse::False).  thread_count is the host thread count of the symbolic
- * phase (the reference's thread_count). */
+ * phase and the device plan (the reference's thread_count); 0 or less: every
+ * hardware thread.  The result does not depend on it. */
 int tb_chol_create( tb_chol ** out, int32_t n, const int64_t * outer, const int32_t * inner,
                     const int32_t * perm, int32_t thread_count );
 int tb_chol_destroy( tb_chol * h );

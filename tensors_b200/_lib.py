@@ -25,6 +25,7 @@ SIGNATURES = {
     "tb_last_error": (ctypes.c_char_p, []),
     "tb_trace_record": (ctypes.c_int, [_i32]),
     "tb_trace_names": (ctypes.c_int64, [ctypes.c_char_p, ctypes.c_int64]),
+    "tb_trace_times": (ctypes.c_int64, [ctypes.POINTER(ctypes.c_double), ctypes.c_int64]),
     "tb_set_device": (ctypes.c_int, [ctypes.c_int]),
     "tb_chol_create": (ctypes.c_int, [ctypes.POINTER(_vp), _i32, _vp, _vp, _vp, _i32]),
     "tb_chol_destroy": (ctypes.c_int, [_vp]),

@@ -124,7 +124,7 @@ class CholeskyDecomposition:
     SupernodeStrategy_T = SupernodeStrategy
     FactorizationMethod_T = FactorizationMethod
 
-    def __init__(self, outer, inner, perm=None, n: int | None = None, thread_count: int = 1):
+    def __init__(self, outer, inner, perm=None, n: int | None = None, thread_count: int = 0):
         self._outer = np.ascontiguousarray(outer, dtype=np.int64)
         self._inner = np.ascontiguousarray(inner, dtype=np.int32)
         self._n = int(n) if n is not None else len(self._outer) - 1
@@ -719,7 +719,7 @@ class BatchedCholesky:
     :class:`CholeskyDecomposition` for precision, refinement and statistics.
     """
 
-    def __init__(self, systems, thread_count: int = 1):
+    def __init__(self, systems, thread_count: int = 0):
         self._keep = []
         count = len(systems)
         n = np.zeros(count, dtype=np.int32)

@@ -287,6 +287,7 @@ void build_plan( tb_chol * h )
     h->plan.defer_steps = h->opt_defer;
     h->plan.tc_nmax = h->opt_tc_width;
     h->plan.relax = relaxation_preset( h->opt_relax );
+    h->plan.threads = h->threads;
     h->plan.build( h->sym );
     if( h->solve_schedule == TB_SCHEDULE_LEVELS ) { h->plan.build_solve_graph( h->sym, h->plan.levels ); }
     else if( h->solve_schedule == TB_SCHEDULE_TASK_GRAPH_ALL ) { h->plan.build_solve_graph( h->sym, 0 ); }
@@ -314,6 +315,7 @@ int ensure_symbolic( tb_chol * h )
     in.perm = h->has_perm ? h->perm.data() : nullptr;
     in.strategy = h->strategy;
     in.amalgamation_threshold = h->amalgamation_threshold;
+    in.threads = h->threads;
     tb::TraceRange range( "Sparse::CholeskyDecomposition::SymbolicFactorization" );
     const auto t0 = std::chrono::steady_clock::now();
     const int st = h->sym.analyze( in );
@@ -1537,7 +1539,7 @@ int tb_chol_create( tb_chol ** out, std::int32_t n, const std::int64_t * outer, 
     h->outer.assign( outer, outer + n + 1 );
     h->inner.assign( inner, inner + outer[n] );
     if( perm != nullptr ) { h->perm.assign( perm, perm + n ); h->has_perm = true; }
-    h->threads = std::max( 1, thread_count );
+    h->threads = thread_count;                 // <= 0: every hardware thread
     *out = h;
     return TB_OK;
 }

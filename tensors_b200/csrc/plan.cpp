@@ -339,7 +339,7 @@ void Plan::build( const Symbolic & sym )
                     asm_dst[static_cast<size_t>(out)] = static_cast<I64>( static_cast<std::uint64_t>(dst) | (j == i ? kDiagFlag : 0ull) );
                 }
             }
-        } );
+        }, threads );
     }
 
     // ------------------------------------------ export to reference layout

@@ -291,6 +291,7 @@ struct Plan
     Relaxation relax;
     std::int32_t defer_steps = kDeferSteps;   // panel steps over which a front's trailing update is deferred (1-4)
     std::int32_t tc_nmax = kTcNMax;           // widest tensor-core tile of the FP32 path (128 or 256)
+    std::int32_t threads = 0;                 // host threads of the build and the check (<= 0: every hardware thread)
 
     // fronts: runs [sn_first, sn_last] of reference supernodes
     std::int32_t front_count = 0;

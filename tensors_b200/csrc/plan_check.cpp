@@ -30,10 +30,10 @@ bool in_range( I64 first, I64 last_inclusive, I64 size )
 }
 
 // The lowest index in [0, count) for which bad(i) holds, or -1; the range is
-// split over the host threads (the message is then rebuilt for that index, so
+// split over `threads` host threads (<= 0: all) (the message is then rebuilt for that index, so
 // the report does not depend on the threads).
 template<typename Bad>
-I64 first_bad( I64 count, Bad && bad )
+I64 first_bad( I64 threads, I64 count, Bad && bad )
 {
     std::atomic<I64> first{ count };
     parallel_rows( count, [&]( I64 b, I64 e )
@@ -45,7 +45,7 @@ I64 first_bad( I64 count, Bad && bad )
             while( i < cur && !first.compare_exchange_weak( cur, i ) ) {}
             break;
         }
-    } );
+    }, threads );
     const I64 f = first.load();
     return f < count ? f : -1;
 }
@@ -70,7 +70,7 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             if( d < 0 || d >= pl.u0_size + pl.u1_size ) { return "assembly target out of range at " + std::to_string( e ); }
             return std::string();
         };
-        const I64 bad = first_bad( static_cast<I64>( pl.asm_src.size() ), [&]( I64 e ) { return !entry( e ).empty(); } );
+        const I64 bad = first_bad( pl.threads, static_cast<I64>( pl.asm_src.size() ), [&]( I64 e ) { return !entry( e ).empty(); } );
         if( bad >= 0 ) { return entry( bad ); }
     }
     for( size_t i = 0; i < pl.diag_offset.size(); ++i )
@@ -255,7 +255,7 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             if( !in_range( t.c, t.c + static_cast<I64>(t.M - 1) * t.ldc + t.N - 1, arena ) ) { return "gemm C out of range" + at(); }
             return std::string();
         };
-        const I64 bad = first_bad( static_cast<I64>( pl.gemm.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
+        const I64 bad = first_bad( pl.threads, static_cast<I64>( pl.gemm.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
         if( bad >= 0 ) { return task( bad ); }
     }
     {
@@ -277,7 +277,7 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
             if( t.blk < 0 || t.blk + (nk - 1) * 2 * t.tf + 2 * t.tf > pl.img_blocks ) { return "tile k-chunks outside the operand image" + at(); }
             return std::string();
         };
-        const I64 bad = first_bad( static_cast<I64>( pl.tc.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
+        const I64 bad = first_bad( pl.threads, static_cast<I64>( pl.tc.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
         if( bad >= 0 ) { return task( bad ); }
         // each panel step: its GEMM launches' small-front tiles and tensor-core tiles do the step's
         // updates (a tensor-core tile of the first tile row spans both launches' rows)

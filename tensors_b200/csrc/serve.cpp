@@ -154,7 +154,7 @@ struct tb_server
         if( mx->h == nullptr )
         {
             st = tb_chol_create( &mx->h, mx->n, mx->outer.data(), mx->inner.data(),
-                                 mx->has_perm ? mx->perm.data() : nullptr, 1 );
+                                 mx->has_perm ? mx->perm.data() : nullptr, 0 );
             if( st == TB_OK ) { st = tb_chol_set_precision( mx->h, precision ); }
             mx->factored = false;
         }

@@ -11,6 +11,7 @@
 #include "common.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <numeric>
 #include <thread>
 
@@ -44,21 +45,25 @@ void Symbolic::permute_pattern( const std::vector<I32> & rows, const std::vector
     moved_from.assign( static_cast<size_t>(nnz), 0 );
     parallel_rows( n, [&]( I64 b, I64 e )
     {
-        std::vector<std::pair<I32,I64>> buf;
+        // one 64-bit key per entry: new column (high word), slot within the old row (low word)
+        std::vector<std::uint64_t> buf;
         for( I64 i = b; i < e; ++i )
         {
             const I64 src = outer[rows[i]];
             const I64 len = new_outer[i+1] - new_outer[i];
             buf.resize( static_cast<size_t>(len) );
-            for( I64 k = 0; k < len; ++k ) { buf[k] = { cols_inv[inner[src+k]], src + k }; }
+            for( I64 k = 0; k < len; ++k )
+            {
+                buf[k] = (static_cast<std::uint64_t>( static_cast<std::uint32_t>( cols_inv[inner[src+k]] ) ) << 32) | static_cast<std::uint64_t>( k );
+            }
             std::sort( buf.begin(), buf.end() );
             for( I64 k = 0; k < len; ++k )
             {
-                new_inner [new_outer[i] + k] = buf[k].first;
-                moved_from[new_outer[i] + k] = buf[k].second;
+                new_inner [new_outer[i] + k] = static_cast<I32>( buf[k] >> 32 );
+                moved_from[new_outer[i] + k] = src + static_cast<I64>( buf[k] & 0xffffffffu );
             }
         }
-    } );
+    }, threads_ );
     outer.swap( new_outer );
     inner.swap( new_inner );
 }
@@ -76,27 +81,88 @@ void Symbolic::locate_diagonal()
             const I32 * last  = inner.data() + outer[i+1];
             diag[i] = outer[i] + ( std::lower_bound( first, last, static_cast<I32>(i) ) - first );
         }
-    } );
+    }, threads_ );
 }
 
 // Liu's elimination-tree algorithm with path compression over the full
 // pattern (EliminationTreeParents.hpp:8-63); n marks a root.
+//
+// On several host threads the rows split into contiguous chunks.  Each chunk
+// runs Liu's algorithm on its own rows and columns alone (its entries left of
+// the chunk are set aside), which gives the elimination forest of the chunk's
+// diagonal block.  A serial pass then runs Liu's algorithm once more over a
+// smaller graph: every chunk forest's edges plus the set-aside entries.  For
+// every k the vertices 0..k split into the same connected components in both
+// graphs (the chunk forest restricted to a chunk's first rows spans the
+// components of its diagonal block restricted to those rows), and the
+// elimination tree depends on nothing else, so the tree is the same.
 void Symbolic::elimination_tree()
 {
     etree_parent.assign( static_cast<size_t>(n), n );
     std::vector<I32> ancestor( static_cast<size_t>(n), n );
-    for( I32 k = 1; k < n; ++k )
+    // row k's entries left of k, from column `from` on
+    auto liu_rows = [&]( I32 kb, I32 ke, I32 from, std::vector<std::pair<I32,I32>> * aside )
     {
-        for( I64 l = outer[k]; l < outer[k+1]; ++l )
+        for( I32 k = std::max( kb, 1 ); k < ke; ++k )
         {
-            I32 i = inner[l];
-            while( i != n && i < k )
+            for( I64 l = outer[k]; l < outer[k+1]; ++l )
             {
-                const I32 next = ancestor[i];
-                ancestor[i] = k;
-                if( next == n ) { etree_parent[i] = k; }
-                i = next;
+                I32 i = inner[l];
+                if( i >= k ) { break; }
+                if( i < from ) { aside->emplace_back( k, i ); continue; }
+                while( i != n && i < k )
+                {
+                    const I32 next = ancestor[i];
+                    ancestor[i] = k;
+                    if( next == n ) { etree_parent[i] = k; }
+                    i = next;
+                }
             }
+        }
+    };
+    const I64 chunks = std::min<I64>( host_threads( threads_ ), std::max<I64>( 1, n / 65536 ) );
+    if( chunks <= 1 ) { liu_rows( 0, n, 0, nullptr ); return; }
+
+    std::vector<std::vector<std::pair<I32,I32>>> aside( static_cast<size_t>(chunks) );
+    {
+        std::vector<std::thread> pool;
+        for( I64 t = 0; t < chunks; ++t )
+        {
+            const I32 b = static_cast<I32>( n * t / chunks ), e = static_cast<I32>( n * (t + 1) / chunks );
+            pool.emplace_back( [&, t, b, e]() { liu_rows( b, e, b, &aside[static_cast<size_t>(t)] ); } );
+        }
+        for( auto & th : pool ) { th.join(); }
+    }
+    // the chunk forests' edges, by parent
+    std::vector<I32> child_ptr( static_cast<size_t>(n) + 2, 0 ), child_idx;
+    for( I32 i = 0; i < n; ++i ) { ++child_ptr[static_cast<size_t>( etree_parent[i] ) + 1]; }
+    std::partial_sum( child_ptr.begin(), child_ptr.end(), child_ptr.begin() );
+    child_idx.resize( static_cast<size_t>( child_ptr[static_cast<size_t>(n)] ) );
+    {
+        std::vector<I32> next( child_ptr.begin(), child_ptr.end() - 1 );
+        for( I32 i = 0; i < n; ++i ) { if( etree_parent[i] < n ) { child_idx[static_cast<size_t>( next[etree_parent[i]]++ )] = i; } }
+    }
+    etree_parent.assign( static_cast<size_t>(n), n );
+    ancestor.assign( static_cast<size_t>(n), n );
+    auto climb = [&]( I32 i, I32 k )
+    {
+        while( i != n && i < k )
+        {
+            const I32 next = ancestor[i];
+            ancestor[i] = k;
+            if( next == n ) { etree_parent[i] = k; }
+            i = next;
+        }
+    };
+    for( I64 t = 0; t < chunks; ++t )
+    {
+        const I32 b = static_cast<I32>( n * t / chunks ), e = static_cast<I32>( n * (t + 1) / chunks );
+        const auto & side = aside[static_cast<size_t>(t)];
+        size_t q = 0;
+        for( I32 k = b; k < e; ++k )
+        {
+            for( I32 c = child_ptr[k]; c < child_ptr[k+1]; ++c ) { climb( child_idx[static_cast<size_t>(c)], k ); }
+            for( ; q < side.size() && side[q].first == k; ++q ) { climb( side[q].second, k ); }
         }
     }
 }
@@ -163,9 +229,46 @@ bool Symbolic::postordered( const std::vector<I32> & parent, const std::vector<I
 // or beyond the closing row, united with the column sets of the first row's
 // elimination-tree children (restricted to the same range).  The merge rule
 // then decides whether the closed supernode joins its predecessor.
+//
+// Whether row i starts a supernode depends only on the pattern and the tree, so
+// it is decided for all rows first, in parallel: row i (1 <= i < n) starts one
+// if it has more than one child, or if some column j of its upper pattern was
+// last seen, among the rows before i that record their columns (rows 1.. with
+// at most one child; the sweep's early exit skips the others), before i's
+// subtree.  The rows with column j in their upper pattern are the entries of
+// row j's lower pattern (the pattern is symmetric), so one ascending pass over
+// every row's lower pattern visits each (recording row, column) pair with the
+// recording row before it; the flags it sets are only ever set to 1.
+void Symbolic::supernode_starts( const Forest & et, std::vector<std::uint8_t> & fresh ) const
+{
+    fresh.assign( static_cast<size_t>(n) + 1, 0 );
+    auto records = [&]( I32 r ) { return r >= 1 && et.child_ptr[r+1] - et.child_ptr[r] <= 1; };
+    for( I32 i = 0; i < n; ++i ) { if( !records( i ) ) { fresh[static_cast<size_t>(i)] = 1; } }
+    fresh[static_cast<size_t>(n)] = 1;
+    std::uint8_t * flag = fresh.data();
+    parallel_rows( n, [&]( I64 b, I64 e )
+    {
+        for( I64 j = b; j < e; ++j )
+        {
+            I32 last = -1;
+            for( I64 k = outer[j]; k < diag[j]; ++k )
+            {
+                const I32 i = inner[k];
+                if( !records( i ) ) { continue; }
+                if( last < i - et.desc[i] + 1 ) { __atomic_store_n( flag + i, std::uint8_t(1), __ATOMIC_RELAXED ); }
+                last = i;
+            }
+        }
+    }, threads_ );
+}
+
 void Symbolic::supernodes( SupernodeStrategy strategy, I32 threshold, const Forest & et )
 {
-    std::vector<I32> last_row_with_col( static_cast<size_t>(n), -1 );
+    std::vector<std::uint8_t> fresh;
+    {
+        TraceRange range( "tensors_b200::SupernodeStarts" );
+        supernode_starts( et, fresh );
+    }
     row_to_sn.assign( static_cast<size_t>(n), 0 );
     sn_rp.assign( 1, 0 );
     sn_outer.assign( 1, 0 );
@@ -176,20 +279,7 @@ void Symbolic::supernodes( SupernodeStrategy strategy, I32 threshold, const Fore
     I32 first = 0;        // first row of the open supernode
     I32 prev_rows = 0, prev_cols = 0;
 
-    auto starts_supernode = [&]( I32 i ) -> bool
-    {
-        if( i == n ) { return true; }
-        if( et.child_ptr[i+1] - et.child_ptr[i] > 1 ) { return true; }   // early exit, columns unrecorded
-        const I32 subtree_first = i - et.desc[i] + 1;
-        bool fresh = false;
-        for( I64 k = diag[i] + 1; k < outer[i+1]; ++k )
-        {
-            const I32 j = inner[k];
-            if( last_row_with_col[j] < subtree_first ) { fresh = true; }
-            last_row_with_col[j] = i;
-        }
-        return fresh;
-    };
+    auto starts_supernode = [&]( I32 i ) -> bool { return fresh[static_cast<size_t>(i)] != 0; };
 
     // Trailing part (columns >= bound) of closed supernode k's column set.
     auto tail_of = [&]( I32 k, I32 bound ) -> std::pair<I64,I64>
@@ -282,22 +372,32 @@ void Symbolic::assembly_tree()
 int Symbolic::analyze( const SymbolicInput & in )
 {
     n = in.n;
+    threads_ = in.threads;
     if( n <= 0 || in.outer == nullptr || in.inner == nullptr ) { return TB_ERR_INVALID_ARGUMENT; }
     nnz = in.outer[n];
     if( in.outer[0] != 0 || nnz < n ) { return TB_ERR_INVALID_PATTERN; }
     outer.assign( in.outer, in.outer + n + 1 );
-    inner.assign( in.inner, in.inner + nnz );
+    for( I32 i = 0; i < n; ++i ) { if( outer[i+1] < outer[i] ) { return TB_ERR_INVALID_PATTERN; } }
+    inner.resize( static_cast<size_t>(nnz) );
     // Rows must be sorted unless a permutation is given, in which case the
     // permuted pattern is sorted here (as the reference's Permute does).
-    for( I32 i = 0; i < n; ++i )
+    std::atomic<bool> bad{ false };
+    parallel_rows( n, [&]( I64 b, I64 e )
     {
-        if( outer[i+1] < outer[i] ) { return TB_ERR_INVALID_PATTERN; }
-        for( I64 k = outer[i]; k < outer[i+1]; ++k )
+        std::copy( in.inner + outer[b], in.inner + outer[e], inner.begin() + outer[b] );
+        for( I64 i = b; i < e && !bad.load( std::memory_order_relaxed ); ++i )
         {
-            if( inner[k] < 0 || inner[k] >= n ) { return TB_ERR_INVALID_PATTERN; }
-            if( in.perm == nullptr && k > outer[i] && inner[k] <= inner[k-1] ) { return TB_ERR_INVALID_PATTERN; }
+            for( I64 k = outer[i]; k < outer[i+1]; ++k )
+            {
+                if( inner[k] < 0 || inner[k] >= n || (in.perm == nullptr && k > outer[i] && inner[k] <= inner[k-1]) )
+                {
+                    bad.store( true );
+                    break;
+                }
+            }
         }
-    }
+    }, threads_ );
+    if( bad.load() ) { return TB_ERR_INVALID_PATTERN; }
 
     p.resize( static_cast<size_t>(n) );
     p_inv.assign( static_cast<size_t>(n), -1 );
@@ -312,13 +412,17 @@ int Symbolic::analyze( const SymbolicInput & in )
             p_inv[v] = i;
         }
         permute_pattern( p, p_inv, value_perm );         // CholeskyDecomposition.hpp:313-331
-        for( I32 i = 0; i < n; ++i )                      // duplicates are not a CSR pattern
+        parallel_rows( n, [&]( I64 b, I64 e )             // duplicates are not a CSR pattern
         {
-            for( I64 k = outer[i] + 1; k < outer[i+1]; ++k )
+            for( I64 i = b; i < e && !bad.load( std::memory_order_relaxed ); ++i )
             {
-                if( inner[k] == inner[k-1] ) { return TB_ERR_INVALID_PATTERN; }
+                for( I64 k = outer[i] + 1; k < outer[i+1]; ++k )
+                {
+                    if( inner[k] == inner[k-1] ) { bad.store( true ); break; }
+                }
             }
-        }
+        }, threads_ );
+        if( bad.load() ) { return TB_ERR_INVALID_PATTERN; }
     }
     else
     {

@@ -27,6 +27,7 @@ struct SymbolicInput
     const std::int32_t * perm  = nullptr;   // perm[i] = original index at position i; null = identity
     SupernodeStrategy    strategy = SupernodeStrategy::Maximal;
     std::int32_t         amalgamation_threshold = 4;
+    std::int32_t         threads = 0;         // host threads of the analysis; <= 0: every hardware thread
 };
 
 class Symbolic
@@ -69,6 +70,8 @@ public:
     std::int32_t n1( std::int32_t s ) const { return static_cast<std::int32_t>( sn_outer[s+1] - sn_outer[s] ); }
 
 private:
+    std::int32_t threads_ = 0;
+
     struct Forest
     {
         std::vector<std::int32_t> child_ptr, child_idx, desc;
@@ -81,6 +84,7 @@ private:
     void elimination_tree();
     static void forest_of( const std::vector<std::int32_t> & parent, Forest & f, bool with_order );
     static bool postordered( const std::vector<std::int32_t> & parent, const std::vector<std::int32_t> & desc );
+    void supernode_starts( const Forest & et, std::vector<std::uint8_t> & fresh ) const;
     void supernodes( SupernodeStrategy strategy, std::int32_t threshold, const Forest & et );
     void assembly_tree();
 };

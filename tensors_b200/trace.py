@@ -21,6 +21,16 @@ def names() -> list[str]:
     return [s for s in buf.value.decode().split("\n") if s]
 
 
+def times() -> list[tuple[str, float]]:
+    """(name, host wall milliseconds) of every phase range entered since recording started, in
+    order (-1.0 for a range still open)."""
+    got = names()
+    n = int(lib().tb_trace_times(None, 0))
+    ms = (ctypes.c_double * max(n, 1))()
+    lib().tb_trace_times(ms, n)
+    return list(zip(got, [float(ms[i]) for i in range(min(n, len(got)))]))
+
+
 @contextmanager
 def recording():
     """with recording() as got: ... ; got holds the ranges entered inside the block."""

@@ -167,3 +167,22 @@ def test_settings_getters_follow_the_setters():
     c.SetFactorizationMethod(FactorizationMethod.LeftLooking)
     assert (c.GetSupernodeStrategy(), c.AmalgamationThreshold(), c.GetFactorizationMethod()) == \
         (SupernodeStrategy.Amalgamated, 7, FactorizationMethod.LeftLooking)
+
+
+@pytest.mark.parametrize("order", ["geometric", "pattern"])
+def test_analysis_is_the_same_on_any_number_of_threads(order):
+    # the elimination tree runs in row chunks (one per thread, from 2 x 65,536 rows on) merged
+    # by a serial pass, and the supernode starts are decided row-parallel: the symbolic arrays
+    # are those of one thread, for an ordering that is already postordered (the geometric
+    # dissection) and one that is not (the dissection from the pattern alone)
+    A = M.grid_laplacian_2d(730, 1.0)         # 532,900 rows: up to 8 chunks
+    perm = O.nested_dissection(A, 64) if order == "geometric" else O.graph_nested_dissection(A, 64)
+    got = {}
+    for threads in (1, 2, 3, 8):
+        c = CholeskyDecomposition(A.outer, A.inner, perm, thread_count=threads)
+        c.SymbolicFactorization()
+        got[threads] = (c.EliminationTreeParents(), c.GetPermutation(), c.GetValuePermutation(), c.SN_RowPointers(),
+                        c.SN_Outer(), c.SN_Inner(), c.AssemblyTreeParents())
+    for threads in (2, 3, 8):
+        for a, b in zip(got[1], got[threads]):
+            assert np.array_equal(a, b), threads

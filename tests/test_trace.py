@@ -31,6 +31,25 @@ def test_symbolic_phases_are_ranges():
     assert trace.names() == []
 
 
+def test_phase_times_nest():
+    # every closed range has a host duration, and the enclosing SymbolicFactorization range
+    # lasts at least as long as the steps inside it
+    A = M.grid_laplacian_2d(40, 1.0)
+    trace.record(True)
+    try:
+        c = CholeskyDecomposition(A.outer, A.inner, O.nested_dissection(A, 8))
+        c.SymbolicFactorization()
+        got = trace.times()
+    finally:
+        trace.record(False)
+    d = dict(got)
+    assert all(t >= 0.0 for _, t in got)
+    inner = sum(d[P + tag] for tag in ("Init", "EliminationTree", "PostOrdering", "FindMaximalSupernodes",
+                                       "CreateAssemblyTree") if P + tag in d)
+    assert d[P + "SymbolicFactorization"] >= inner
+    assert trace.times() == []
+
+
 def test_strategy_names_its_supernode_range():
     A = M.grid_laplacian_2d(10, 1.0)
     for strategy, tag in ((1, "FindFundamentalSupernodes"), (2, "FindAmalgamatedSupernodes")):
