@@ -416,7 +416,7 @@ def c4_systems(count=C4_COUNT, which=None):
 
     ms = c4_sizes(count)
     jobs = [(s, ms[s]) for s in (range(count) if which is None else which)]
-    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
         return pool.map(_c4_system, jobs, chunksize=8)
 
 
@@ -717,7 +717,7 @@ def run_c5(args):
     # on the data path, latencies gathered at the end
     mine = (shard_by_work([float(g) ** (3 if kind == "2d" else 6) for _, kind, g in specs], world)[rank]
             if world > 1 else list(range(len(specs))))
-    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:     # before any GPU call
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, len(mine), 16)) as pool:     # before any GPU call
         mats = dict(zip(mine, pool.map(_c5_matrix, [specs[j] for j in mine])))
     from tensors_b200 import build as tb_build
     from tensors_b200.serving import Server

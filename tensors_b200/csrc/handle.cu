@@ -858,6 +858,15 @@ int check_solve_error( tb_chol * h )
                  + " ran out of time" );
 }
 
+// Right-hand-side columns a buffer is reserved for when nrhs are needed: the
+// width class (8, 16, 32, 64; wider: as given), so that calls with varying
+// nrhs regrow (free and reallocate, which waits for the whole device) at most
+// once per class.
+std::int64_t rhs_capacity( std::int32_t nrhs )
+{
+    return nrhs <= 8 ? 8 : nrhs <= 16 ? 16 : nrhs <= 32 ? 32 : nrhs <= tb::kSolveMaxRhs ? tb::kSolveMaxRhs : nrhs;
+}
+
 double * sweep_input( int which, double * W, double * Y ) { return which == 1 ? Y : W; }
 double * sweep_result( int which, double * W, double * Y ) { return which == 0 ? Y : W; }
 
@@ -870,8 +879,13 @@ int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, st
 {
     cudaStream_t st = h->stream;
     const std::int32_t n = h->n;
-    const std::int32_t k = std::max( 1, nrhs );
-    if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    const std::int32_t kb = std::max( 1, nrhs );
+    if( ldB < kb || ldX < kb ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
+    // The sweeps run on the width class of nrhs (8, 16, 32 or 64 columns; wider: as given), the
+    // extra columns zero: the kernels compute that many columns in any case, every column's
+    // result depends on that column alone, and one captured graph and one set of work buffers
+    // then serve every nrhs of the class instead of one per nrhs.
+    const std::int32_t k = static_cast<std::int32_t>( rhs_capacity( kb ) );
     TB_TRY( h->work.reserve( static_cast<std::int64_t>(n) * k ) );
     TB_TRY( h->work2.reserve( static_cast<std::int64_t>(n) * k ) );
     if( !h->plan.spanels.empty() ) { TB_TRY( h->work3.reserve( static_cast<std::int64_t>(n) * k ) ); }
@@ -886,7 +900,7 @@ int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, st
     }
     TB_TRY( prepare_solve_grid( h, k ) );
     std::int64_t launches = 0;
-    tb::launch_gather_rows( d_B, ldB, h->p.ptr, sweep_input( which, W, Y ), k, n, k, st );   // ReadRightHandSide
+    tb::launch_gather_rows( d_B, ldB, h->p.ptr, sweep_input( which, W, Y ), k, n, kb, st, k );   // ReadRightHandSide
     ++launches;
     if( h->use_graph && !h->profiling )
     {
@@ -931,7 +945,7 @@ int run_solve_core( tb_chol * h, int which, double alpha, const double * d_B, st
     {
         launches += issue_sweeps( h, which, W, Y, k );
     }
-    tb::launch_scatter_rows( sweep_result( which, W, Y ), k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, k, st );   // WriteSolution
+    tb::launch_scatter_rows( sweep_result( which, W, Y ), k, h->p_inv.ptr, alpha, beta, d_X, ldX, n, kb, st );   // WriteSolution
     ++launches;
     h->solve_launch_count = launches;
     TB_CUDA( cudaGetLastError() );
@@ -1170,10 +1184,11 @@ int run_solve_refined( tb_chol * h, double alpha, const double * d_B, std::int32
     const std::int32_t k = std::max( 1, nrhs );
     if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
     const std::int64_t nk = static_cast<std::int64_t>( n ) * k;
-    TB_TRY( h->ir_x.reserve( 4 * nk ) );               // x, r, z (and q), p
-    TB_TRY( h->ir_r.reserve( nk ) );
-    TB_TRY( h->ir_norms.reserve( 5 * k ) );            // |r|^2, |b|^2, rz, rz_new, pq
-    TB_TRY( h->pin_norms.reserve( sizeof(double) * 2 * static_cast<size_t>( k ) ) );
+    const std::int64_t kcap = rhs_capacity( k );
+    TB_TRY( h->ir_x.reserve( 4 * n * kcap ) );         // x, r, z (and q), p
+    TB_TRY( h->ir_r.reserve( n * kcap ) );
+    TB_TRY( h->ir_norms.reserve( 5 * kcap ) );         // |r|^2, |b|^2, rz, rz_new, pq
+    TB_TRY( h->pin_norms.reserve( sizeof(double) * 2 * static_cast<size_t>( kcap ) ) );
     double * hn = h->pin_norms.as<double>();
     double * X = h->ir_x.ptr;
     double * P = X + nk;
@@ -1401,12 +1416,12 @@ int run_solve_host( tb_chol * h, int which, double alpha, const void * B, std::i
     const std::int32_t n = h->n;
     const std::int32_t k = std::max( 1, nrhs );
     if( ldB < k || ldX < k ) { return fail( TB_ERR_INVALID_ARGUMENT, "Solve: leading dimension smaller than nrhs" ); }
-    const size_t bytes = sizeof(double) * static_cast<size_t>(n) * k;
+    const std::int64_t kcap = rhs_capacity( k );
     cudaStream_t st = h->stream;
-    TB_TRY( h->pin_in.reserve( bytes ) );
-    TB_TRY( h->pin_out.reserve( bytes ) );
-    TB_TRY( h->in.reserve( static_cast<std::int64_t>(n) * k ) );
-    TB_TRY( h->out.reserve( static_cast<std::int64_t>(n) * k ) );
+    TB_TRY( h->pin_in.reserve( sizeof(double) * static_cast<size_t>(n) * kcap ) );
+    TB_TRY( h->pin_out.reserve( sizeof(double) * static_cast<size_t>(n) * kcap ) );
+    TB_TRY( h->in.reserve( static_cast<std::int64_t>(n) * kcap ) );
+    TB_TRY( h->out.reserve( static_cast<std::int64_t>(n) * kcap ) );
     double * pi = h->pin_in.as<double>();
     double * po = h->pin_out.as<double>();
     // in chunks of rows: the copy of chunk c to the device runs while the host stages chunk c + 1

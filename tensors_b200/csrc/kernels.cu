@@ -1752,16 +1752,17 @@ __global__ __launch_bounds__(kDagThreads, 3) void factor_dag_kernel( const DagAr
 }
 
 // ------------------------------------------------------ permutations, SpMV
+// W rows (kw columns) <- rows p[i] of B (k columns), columns k..kw-1 zero.
 __global__ void gather_rows_kernel( const double * __restrict__ B, int ldB, const std::int32_t * __restrict__ p,
-                                    double * __restrict__ W, int ldw, int n, int k )
+                                    double * __restrict__ W, int ldw, int n, int k, int kw )
 {
-    const std::int64_t total = (std::int64_t)n * k;
+    const std::int64_t total = (std::int64_t)n * kw;
     for( std::int64_t e = blockIdx.x * (std::int64_t)blockDim.x + threadIdx.x; e < total;
          e += (std::int64_t)gridDim.x * blockDim.x )
     {
-        const std::int64_t i = e / k;
-        const int c = static_cast<int>( e % k );
-        W[i * ldw + c] = B[(std::int64_t)p[i] * ldB + c];
+        const std::int64_t i = e / kw;
+        const int c = static_cast<int>( e % kw );
+        W[i * ldw + c] = c < k ? B[(std::int64_t)p[i] * ldB + c] : 0.0;
     }
 }
 
@@ -2593,9 +2594,10 @@ TB_INSTANTIATE( float )
 #undef TB_INSTANTIATE
 
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
-                         int n, int k, cudaStream_t st )
+                         int n, int k, cudaStream_t st, int kw )
 {
-    gather_rows_kernel<<<grid_for( (std::int64_t)n * k, 256 ), 256, 0, st>>>( B, ldB, p, W, ldw, n, k );
+    kw = std::max( kw, k );
+    gather_rows_kernel<<<grid_for( (std::int64_t)n * kw, 256 ), 256, 0, st>>>( B, ldB, p, W, ldw, n, k, kw );
 }
 
 void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv, double alpha, double beta,

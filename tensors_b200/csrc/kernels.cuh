@@ -140,8 +140,9 @@ void launch_super_rest( const SuperSolveTask * tasks, int count, const SuperPane
                         const std::int32_t * sn_inner, bool upper, double * in, double * zbuf, const double * out, int ld, int k,
                         cudaStream_t st );
 
+// W (ldw) <- rows p[i] of B (ldB), k columns; columns k..kw-1 of W are zeroed.
 void launch_gather_rows( const double * B, int ldB, const std::int32_t * p, double * W, int ldw,
-                         int n, int k, cudaStream_t st );
+                         int n, int k, cudaStream_t st, int kw = 0 );
 void launch_scatter_rows( const double * W, int ldw, const std::int32_t * p_inv, double alpha, double beta,
                           double * Y, int ldY, int n, int k, cudaStream_t st );
 void launch_residual( int n, const std::int64_t * outer, const std::int32_t * inner, const double * vals,
