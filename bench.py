@@ -736,9 +736,16 @@ def run_c5(args):
     ids = {j: srv.add_matrix(m[2], m[3], m[5]) for j, m in mats.items()}
     blocks = {j: np.random.default_rng(C5_SEED + 100 + j).standard_normal((len(m[2]) - 1, 64)) for j, m in mats.items()}
     # warm-up: symbolic analysis, device plan and first factor of every matrix (the reference's
-    # SymbolicFactorization precedes NumericFactorization in the same way)
+    # SymbolicFactorization precedes NumericFactorization in the same way), then one solve per
+    # right-hand-side width class (the solves run on 8, 16, 32 or 64 columns: each class's
+    # graph is captured and its buffers sized once); its time is reported as cold_start_s
+    t_cold = time.perf_counter()
     for t in [srv.submit(ids[j], values=mats[j][4], B=blocks[j][:, :1].copy(), tol=TARGET_RELRES) for j in mine]:
         srv.wait(t)
+    for width in (16, 32, 64):
+        for t in [srv.submit(ids[j], B=np.ascontiguousarray(blocks[j][:, :width]), tol=TARGET_RELRES) for j in mine]:
+            srv.wait(t)
+    cold_start = time.perf_counter() - t_cold
     arrivals = np.cumsum(rng.exponential(1.0 / C5_RATE, size=n_req))
     which = rng.integers(0, len(specs), size=n_req)
     repeat = rng.random(n_req) < 0.3
@@ -784,13 +791,14 @@ def run_c5(args):
     if dist is not None:
         # the job's latency distribution: every rank's requests, over the slowest rank's wall time
         parts = [None] * world
-        dist.all_gather_object(parts, (lat, runs, iters, worst, fails, wall))
+        dist.all_gather_object(parts, (lat, runs, iters, worst, fails, wall, cold_start))
         lat = [x for p in parts for x in p[0]]
         runs = [x for p in parts for x in p[1]]
         iters = [x for p in parts for x in p[2]]
         worst = max(p[3] for p in parts)
         fails = sum(p[4] for p in parts)
         wall = max(p[5] for p in parts)
+        cold_start = max(p[6] for p in parts)
         dist.barrier()
         dist.destroy_process_group()
         if rank != 0:
@@ -803,7 +811,7 @@ def run_c5(args):
         "metric": "serving latency p50/p99 (ms) and throughput, Poisson stream of factor/solve requests, "
                   "FP32 factor + FP64 refinement to 1e-10",
         "value": float(np.percentile(lat, 99)), "unit": "ms (p99 latency)", "n_gpus": world, "steps": n_req,
-        "warmup": len(specs), "ms_per_step": float(np.mean(runs)), "higher_is_better": False, "scaling": "strong",
+        "warmup": 4 * len(specs), "ms_per_step": float(np.mean(runs)), "higher_is_better": False, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
         "config": {"workload": f"{n_req} requests, Poisson arrivals at {C5_RATE:g}/s over {len(specs)} matrices "
                                "(2D quality-mesh cotangent Laplacians n 1k-50k + mass-weighted shift of mean 1e-2, 3D 7-point "
@@ -813,6 +821,9 @@ def run_c5(args):
                    "p99_ms": float(np.percentile(lat, 99)), "mean_run_ms": float(np.mean(runs)),
                    "parallelism": f"{world} GPU(s), matrices and their requests sharded by estimated factor work",
                    "throughput_req_per_s": n_req / wall, "wall_s": wall, "failures": fails,
+                   "cold_start_s": cold_start,
+                   "warmup_note": "untimed: per matrix the symbolic analysis, plan and first factor, then one solve "
+                                  "per right-hand-side width class (16, 32, 64 columns)",
                    "worst_relres": worst, "mean_refinement_steps": float(np.mean(iters)), "server": st},
         "cpu_baseline": ref,
     }

@@ -1320,7 +1320,6 @@ __global__ __launch_bounds__(kGemmThreads) void gemm_tn_kernel( const GemmTask *
 
 constexpr int kTld = kPanel + 4;   // padded shared-memory row of 64-wide blocks (conflict-free DMMA fragments)
 // Doubles of shared memory the solve step's staged rest block takes (64 x kTld of T, rounded up).
-template<typename T> __host__ __device__ constexpr int solve_block_doubles() { return (kPanel * kTld * static_cast<int>( sizeof(T) ) + 7) / 8; }
 
 // acc[ct] (8 x 8 tile ct of this warp's 8 output rows, NCT tiles) += sum over
 // the K blocks [kb0, kb1) of A(i, kk) * B(kk, ct * 8 + j).
@@ -1369,11 +1368,8 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
     constexpr int kp = KP;
     constexpr int lkp = KP == 8 ? 3 : KP == 16 ? 4 : KP == 32 ? 5 : 6;
     constexpr int ldv = kp + 4;
-    // the rest block stays in the factor's type (FP32 storage: half the shared memory, so
-    // that three CTAs fit an SM) and is widened as the products read it
     double (*sT)[kTld] = reinterpret_cast<double (*)[kTld]>( ssm );
-    T (*sP)[kTld] = reinterpret_cast<T (*)[kTld]>( ssm + kPanel * kTld );
-    double * sX = ssm + kPanel * kTld + solve_block_doubles<T>();   // [64][ldv]: x_q (forward) / x_r (backward)
+    double * sX = ssm + kPanel * kTld;              // [64][ldv]: x_q (forward) / x_r (backward)
     double * sY = sX + kPanel * ldv;                // [64][ldv]: y_q
     __shared__ std::int64_t trow[kSolveRest];
     const int tid = threadIdx.x;
@@ -1406,22 +1402,33 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         trow[tid] = (tid < cw) ? ((col < m) ? (std::int64_t)t.row0 + r1 + col
                                             : (std::int64_t)sn_inner[t.inner + (col - m)]) : -1;
     }
-    // the panel's rest block (factor data: final before any solve step)
+    // The panel's rest block P (factor data: final before any solve step) goes straight into
+    // registers as this warp's DMMA A fragments (lane: row lane / 4 of the 8-row tile, K index
+    // lane % 4 + 4 s of each 8-wide K block kb), loaded before the wait on the previous launch.
+    // Forward: A(i, K) = P[K][o + i] (K over the panel's rows); back: A(i, K) = P[o + i][K]
+    // (K over the rest columns).  Without a staged copy of P a CTA needs 35 KB (FP64) or
+    // 17 KB (FP32) less shared memory, so more CTAs share an SM.
     const T * U0 = arena + t.u0 + (std::int64_t)t.r0 * t.ld0;
     const T * U1 = arena + t.u1 + (std::int64_t)t.r0 * t.ld1;
-    if( has_rest )
+    const int o = warp * 8;
+    T pf[kPanel / 8][2];
     {
-#pragma unroll 4
-        for( int u = 0; u < kPanel * kPanel / kSolveThreads; ++u )
+        auto rest_at = [&]( int i, int cc ) -> T
         {
-            const int idx = tid + u * kSolveThreads;
-            const int i = idx >> 6, jj = idx & 63;
-            const int col = t.c0 + jj;
-            const bool valid = i < nb && jj < cw;
-            const T * src = !valid ? U0 : (col < m) ? U0 + (std::int64_t)i * t.ld0 + r1 + col
-                                                    : U1 + (std::int64_t)i * t.ld1 + (col - m);
-            if constexpr ( sizeof(T) == 8 ) { cp_async_8( reinterpret_cast<double *>( &sP[i][jj] ), reinterpret_cast<const double *>( src ), valid ); }
-            else { cp_async_4( &sP[i][jj], src, valid ); }
+            const int col = t.c0 + cc;
+            return (col < m) ? U0[(std::int64_t)i * t.ld0 + r1 + col] : U1[(std::int64_t)i * t.ld1 + (col - m)];
+        };
+#pragma unroll
+        for( int kb = 0; kb < kPanel / 8; ++kb )
+        {
+#pragma unroll
+            for( int s = 0; s < 2; ++s )
+            {
+                const int kk = 8 * kb + (lane & 3) + 4 * s;
+                const int i = upper ? o + (lane >> 2) : kk;          // panel row
+                const int cc = upper ? kk : o + (lane >> 2);         // rest column
+                pf[kb][s] = (has_rest && i < nb && cc < cw) ? rest_at( i, cc ) : T( 0 );
+            }
         }
     }
     if constexpr ( kPdl ) { pdl_wait(); }
@@ -1450,8 +1457,26 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
     __syncthreads();
 
     const int fi = lane >> 2, fj = 2 * (lane & 3);     // accumulator fragment: row fi, columns fj, fj + 1
-    const int o = warp * 8;
     double acc[nct][2];
+    // acc += P-part (A fragments in pf) times rows of sX, K blocks [0, kbn)
+    auto rest_product = [&]( int kbn )
+    {
+#pragma unroll
+        for( int kb = 0; kb < kPanel / 8; ++kb )
+        {
+            if( kb >= kbn ) { break; }
+#pragma unroll
+            for( int ct = 0; ct < nct; ++ct )
+            {
+#pragma unroll
+                for( int s = 0; s < 2; ++s )
+                {
+                    dmma_8x8x4( acc[ct], static_cast<double>( pf[kb][s] ),
+                                sX[(8 * kb + (lane & 3) + 4 * s) * ldv + ct * 8 + (lane >> 2)] );
+                }
+            }
+        }
+    };
 #pragma unroll
     for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
     if( !upper )
@@ -1481,8 +1506,7 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         // rest rows: y_r -= P^T x_q
 #pragma unroll
         for( int ct = 0; ct < nct; ++ct ) { acc[ct][0] = 0.0; acc[ct][1] = 0.0; }
-        warp_rows_product<nct>( acc, 0, nbb, [&]( int i, int kk ) { return static_cast<double>( sP[kk][o + i] ); },
-                                             [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
+        rest_product( nbb );
         const int jj = o + fi;
         if( jj < cw )
         {
@@ -1508,8 +1532,7 @@ __device__ __forceinline__ void solve_step_body( const SolveRestTask & t, int up
         // sY rows of this warp <- (owner ? y_q : 0) - P x_r
         if( has_rest && o < nb )
         {
-            warp_rows_product<nct>( acc, 0, (cw + 7) >> 3, [&]( int i, int kk ) { return static_cast<double>( sP[o + i][kk] ); },
-                                                           [&]( int kk, int c ) { return sX[kk * ldv + c]; } );
+            rest_product( (cw + 7) >> 3 );
 #pragma unroll
             for( int ct = 0; ct < nct; ++ct )
             {
@@ -2457,7 +2480,7 @@ static int solve_lkp( int k )
 template<typename T>
 static size_t solve_smem_bytes( int k )
 {
-    return sizeof(double) * (kPanel * kTld + solve_block_doubles<T>() + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
+    return sizeof(double) * (kPanel * kTld + 2 * kPanel * ((1 << solve_lkp( k )) + 4));
 }
 
 template<typename T>

@@ -222,7 +222,7 @@ struct ExtendPullTask
     std::int32_t space;            // 0: pivot rows (U0 / U1), 1: update rows (V)
     std::int32_t b0, b1;           // its parent rows [b0, b1) in that space
 };
-constexpr std::int64_t kExtendPullEntries = 16384;   // target child entries per pull task
+constexpr std::int64_t kExtendPullEntries = 4096;    // target child entries per pull task
 
 // The solve of a large front steps through its pivot rows 512 at a time
 // (super-panels) instead of 64 at a time: the inverse of each 512 x 512
