@@ -366,23 +366,36 @@ std::string check_plan( const Symbolic & sym, const Plan & pl )
         if( t.row0 < 0 || t.row0 + t.n0 > sym.n ) { return "solve-rest rows out of range" + at(); }
     }
     for( I32 v : sym.sn_inner ) { if( v < 0 || v >= sym.n ) { return "SN_inner value out of range"; } }
-    for( size_t k = 0; k < pl.exports.size(); ++k )
     {
-        const ExportTask & t = pl.exports[k];
-        auto at = [&]() { return " (export task " + std::to_string( k ) + ")"; };   // built only on failure
-        if( t.n0s <= 0 || t.r_begin < 0 || t.r_end > t.n0s || t.r_begin >= t.r_end ) { return "bad export rows" + at(); }
-        if( t.roff < 0 || t.roff + t.n0s > t.fn0 ) { return "export rows outside the front" + at(); }
-        if( !in_range( t.tri, t.tri + static_cast<I64>(t.n0s) * t.n0s - 1, tri_size ) ) { return "export tri out of range" + at(); }
-        if( t.n1s > 0 && !in_range( t.rec, t.rec + static_cast<I64>(t.n0s) * t.n1s - 1, rec_size ) ) { return "export rec out of range" + at(); }
-        if( t.fld0 < t.fn0 || t.fld1 < t.fn1 ) { return "export leading dimension too small" + at(); }
-        if( !in_range( t.fu0, t.fu0 + static_cast<I64>(t.fn0) * t.fld0 - 1, arena ) ) { return "export front U0 out of range" + at(); }
-        if( t.fn1 > 0 && !in_range( t.fu1, t.fu1 + static_cast<I64>(t.fn0) * t.fld1 - 1, arena ) ) { return "export front U1 out of range" + at(); }
-        if( t.colmap < 0 || t.colmap + t.n1s > static_cast<I64>( pl.colmap.size() ) ) { return "export colmap out of range" + at(); }
-        for( I32 l = 0; l < t.n1s; ++l )
+        auto task = [&]( I64 k ) -> std::string
         {
-            const I32 cm = pl.colmap[t.colmap + l];
-            if( cm >= 0 ? cm >= t.fn0 : (-cm - 1) >= t.fn1 ) { return "export colmap value out of range" + at(); }
-        }
+            const ExportTask & t = pl.exports[static_cast<size_t>( k )];
+            auto at = [&]() { return " (export task " + std::to_string( k ) + ")"; };   // built only on failure
+            if( t.n0s <= 0 || t.r_begin < 0 || t.r_end > t.n0s || t.r_begin >= t.r_end ) { return "bad export rows" + at(); }
+            if( t.roff < 0 || t.roff + t.n0s > t.fn0 ) { return "export rows outside the front" + at(); }
+            if( !in_range( t.tri, t.tri + static_cast<I64>(t.n0s) * t.n0s - 1, tri_size ) ) { return "export tri out of range" + at(); }
+            if( t.n1s > 0 && !in_range( t.rec, t.rec + static_cast<I64>(t.n0s) * t.n1s - 1, rec_size ) ) { return "export rec out of range" + at(); }
+            if( t.fld0 < t.fn0 || t.fld1 < t.fn1 ) { return "export leading dimension too small" + at(); }
+            if( !in_range( t.fu0, t.fu0 + static_cast<I64>(t.fn0) * t.fld0 - 1, arena ) ) { return "export front U0 out of range" + at(); }
+            if( t.fn1 > 0 && !in_range( t.fu1, t.fu1 + static_cast<I64>(t.fn0) * t.fld1 - 1, arena ) ) { return "export front U1 out of range" + at(); }
+            if( t.colmap < 0 || t.colmap + t.n1s > static_cast<I64>( pl.colmap.size() ) ) { return "export colmap out of range" + at(); }
+            if( k > 0 )
+            {
+                // the row blocks of one supernode share its column map: the previous task
+                // checked the same entries against the same limits (and failed first if any is bad)
+                const ExportTask & p = pl.exports[static_cast<size_t>( k - 1 )];
+                if( p.colmap == t.colmap && p.n1s == t.n1s && p.fn0 == t.fn0 && p.fn1 == t.fn1 ) { return std::string(); }
+            }
+            for( I32 l = 0; l < t.n1s; ++l )
+            {
+                const I32 cm = pl.colmap[t.colmap + l];
+                if( cm >= 0 ? cm >= t.fn0 : (-cm - 1) >= t.fn1 ) { return "export colmap value out of range" + at(); }
+            }
+            return std::string();
+        };
+        // checked on all host threads, the first failing task reported
+        const I64 bad = first_bad( pl.threads, static_cast<I64>( pl.exports.size() ), [&]( I64 k ) { return !task( k ).empty(); } );
+        if( bad >= 0 ) { return task( bad ); }
     }
     auto size_of = [&]( LaunchKind kind ) -> I64
     {
